@@ -1,0 +1,334 @@
+"""Throughput benchmark of the hybrid DG residual-and-update path on B200.
+
+Workload (the headline configuration): Mach-3 viscous flow past a sphere of radius
+0.5 in the box [-4,12]x[-6,6]^2, body-fitted O/H hex grid of ~200k elements, P3
+(64 nodes per element), perfect gas gamma=1.4, Re_D=1e5, T_inf=220 K, no-slip
+isothermal wall T_w=300 K (non-dimensional as the reference driver does:
+rho=p=1, U=3*sqrt(1.4), mu=U/Re, T_w=300/220).  One step = one checked SSP-RK3
+step (three stages of inviscid HLLC + BR2 viscous residual, blend, Zhang-Shu
+positivity limiter and admissibility check), float64.  Synthetic seeded mesh
+(numpy generator); the state starts as the uniform free stream.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Metric: DOF-updates/s = sum_b E_b*Np_b * steps / seconds (Np = element nodes).
+--impl reference times the CPU oracle (a float64 numpy restatement of the
+reference's JAX code, which cannot be installed here) on a bounded sample mesh
+with all host threads.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "P3 DOF-updates/s at fixed L2 error, learned+mixed vs plain; % HBM roofline"
+UNIT = "DOF-updates/s"
+GAMMA, MACH, RE, T_INF, T_WALL = 1.4, 3.0, 1.0e5, 220.0, 300.0
+
+
+def peaks():
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text()), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    def __init__(self, index=0):
+        self.index, self.samples, self.proc = index, [], None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=5)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[3 + k] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(self.samples[0][1]) if self.samples[0][1].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def workload(scale="full"):
+    from jax_fluid_sim_b200 import meshgen
+    if scale == "full":
+        return meshgen.sphere_oh_grid()
+    if scale == "small":
+        return meshgen.sphere_oh_grid(n=8, n_radial=6, outer=((3, 10), (4, 4), (4, 4)))
+    return meshgen.sphere_oh_grid(n=4, n_radial=2, outer=((1, 3), (1, 1), (1, 1)))
+
+
+def freestream(degree):
+    u = MACH * np.sqrt(GAMMA)
+    return u, u * 1.0 / RE, np.array([1.0, u, 0.0, 0.0, 1.0])
+
+
+def rhs_bytes(op, nv, sizeof=8):
+    """Algorithmic HBM bytes of one RHS evaluation (each input read once, outputs written once)."""
+    total = 0
+    for bp in op.plan.blocks:
+        total += 2 * sizeof * nv * bp.E * bp.Np             # U in, R out
+        total += sizeof * 10 * bp.E * bp.Nq                 # J^-1 (9) + w|J| (1) per volume point
+        total += sizeof * bp.E * bp.Np * bp.Np              # dense inverse mass
+    for fp in op.plan.faces.values():
+        total += fp.F * (sizeof * fp.nq * (2 * nv + 4 + nv) + 8)
+    return total
+
+
+def volume_kernel_bytes(op, nv, viscous, sizeof=8):
+    """Algorithmic bytes of k_volume: U, metrics, M^-1 (viscous lift), jumps in, lifts and residuals out."""
+    total = 0
+    for bp in op.plan.blocks:
+        per = nv * bp.Np + 10 * bp.Nq + nv * bp.Np
+        if viscous:
+            nq = max(fp.nq for fp in op.plan.faces.values())
+            per += bp.Np * bp.Np + bp.nlf * nq * 12 * 2 + nv * bp.Np
+        total += sizeof * bp.E * per
+    return total
+
+
+def run_ours(args):
+    import ctypes
+
+    import torch
+    import torch.distributed as dist
+
+    import jax_fluid_sim_b200 as jfs
+    from jax_fluid_sim_b200 import _native as N
+    from jax_fluid_sim_b200.operators import _stream_ptr
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    t_setup = time.time()
+    src = workload(args.scale)
+    u, mu, farfield = freestream(3)
+    solver = jfs.HybridCompressibleSolver(jfs.HybridMesh(src), polynomial_degree=args.degree, dynamic_viscosity=mu)
+    op = jfs.HybridNavierStokesOperator(solver)
+    bc = jfs.FarfieldWallBoundary(solver, farfield, wall_temperature=T_WALL / T_INF)
+    pos = jfs.HybridPositivityLimiter(op)
+    integ = jfs.HybridSSPRK3(op, cfl=0.3, limiter=pos)
+    U0 = solver.uniform_state_blocks(1.0, [u, 0.0, 0.0], 1.0)
+    U = {k: v.clone() for k, v in U0.items()}
+    dofs = sum(bp.E * bp.Np for bp in op.plan.blocks)
+    nv = solver.layout.number_of_variables
+    setup_s = time.time() - t_setup
+    dt = integ.stable_dt(U, bc)
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        integ.checked_step_inplace(U, dt, bc)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        start.record()
+        for _ in range(args.steps):
+            status = integ.checked_step_inplace(U, dt, bc)
+        stop.record()
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(stop)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    valid, rmin, pmin = integ._status_tuple()
+    value = dofs * args.steps * world / (ms / 1e3)
+
+    # per-stage kernel durations of one RHS (CUDA events on the launching stream)
+    stage_ms = (ctypes.c_float * 5)()
+    st = op.native.state(op._blocks(U))
+    for _ in range(3):
+        N.check(N.lib().dgb_rhs_profile(op.native.handle, ctypes.byref(st), stage_ms, _stream_ptr()))
+    stages = dict(zip(["traces", "face_flux", "volume_lift", "face_visc", "finalize"], list(stage_ms)))
+    dominant = max(stages, key=stages.get)
+    pk, pk_kind = peaks()
+    hbm = float(pk["hbm_gbs"])
+    vol_bytes = volume_kernel_bytes(op, nv, op.viscous)
+    achieved = vol_bytes / (stages["volume_lift"] / 1e3) / 1e9
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic.json"
+    if tfile.exists():
+        try:
+            traffic = json.loads(tfile.read_text()).get("volume_lift_bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    # end to end through the public API with host buffers: H2D state, step, D2H state
+    host_in = {k: v.cpu().pin_memory() for k, v in U0.items()}
+    host_out = {k: torch.empty_like(v) .pin_memory() for k, v in host_in.items()}
+    dev = {k: torch.empty_like(v) for k, v in U0.items()}
+    e_steps = max(1, min(args.steps, 5))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(e_steps):
+        for k in dev:
+            dev[k].copy_(host_in[k], non_blocking=True)
+        integ.checked_step_inplace(dev, dt, bc)
+        for k in dev:
+            host_out[k].copy_(dev[k], non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e_steps
+    state_bytes = sum(v.numel() * 8 for v in host_in.values())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.cpu_seconds)
+    # launches per checked step: per stage the five RHS stages (per block / face type),
+    # positivity and admissibility per block, one final admissibility reduction
+    nb, nf = len(op.plan.blocks), len(op.plan.faces)
+    per_stage = nb * 3 + nf * (2 if op.viscous else 1) + nb * 2 + 1
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"Mach-3 viscous sphere, O/H hex grid, {sum(bp.E for bp in op.plan.blocks)} "
+                               f"elements, P{args.degree} ({dofs} DOF), plain float64 SSP-RK3 + positivity",
+                   "elements": int(sum(bp.E for bp in op.plan.blocks)), "degree": args.degree, "dofs": int(dofs),
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs larger than L2 (state 0.5 GB, inverse mass 6.5 GB per pass)",
+                   "mood": "off (subcell recompute not in this build)", "setup_s": round(setup_s, 1)},
+        "gpu_launches": per_stage * 3 * args.steps,
+        "step_status": {"valid": valid, "rho_min": rmin, "p_min": pmin, "dt": dt},
+        "stage_ms": stages,
+        "roofline": {"bound": "hbm", "kernel": "volume_lift", "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": achieved / hbm, "peak_kind": pk_kind, "traffic": traffic,
+                     "dominant_stage": dominant, "algorithmic_bytes": vol_bytes,
+                     "rhs_algorithmic_bytes": rhs_bytes(op, nv),
+                     "rhs_achieved_gbs": rhs_bytes(op, nv) / (sum(stages.values()) / 1e3) / 1e9},
+        "clocks": clocks.summary(),
+        "e2e": {"value": dofs / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": state_bytes,
+                "d2h_bytes_per_step": state_bytes},
+    }
+    if cpu:
+        line["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+class CpuSample:
+    """Oracle (numpy float64 restatement of the reference) on a bounded sample of the workload:
+    a coarse sphere O/H grid at P3, whole checked SSP-RK3 steps, all host threads for BLAS."""
+
+    def __init__(self):
+        from oracle.dg import Operator, PositivityLimiter, TimeIntegrator
+        from oracle.mesh import Mesh, MeshSource
+        from oracle.physics import FarfieldWallBoundary, Gas
+        src = workload("tiny")
+        u, mu, farfield = freestream(3)
+        mesh = Mesh(MeshSource(src.points, src.cells, src.physical, src.field_data))
+        gas = Gas(dynamic_viscosity=mu)
+        op = Operator(mesh, gas, 3)
+        self.bc = FarfieldWallBoundary(gas, mesh.physical_names, farfield, wall_temperature=T_WALL / T_INF)
+        self.integ = TimeIntegrator(op, cfl=0.3, limiter=PositivityLimiter(op))
+        U = gas.to_conserved(np.array([1.0, u, 0.0, 0.0, 1.0]))
+        self.states = {b.element_type: np.broadcast_to(U, (len(b.connectivity), 64, 5)).copy()
+                       for b in mesh.element_blocks}
+        self.dt = self.integ.stable_dt(self.states)
+        self.elements = sum(len(b.connectivity) for b in mesh.element_blocks)
+        self.dofs = self.elements * 64
+
+    def step(self):
+        t0 = time.time()
+        self.states = self.integ.checked_step(self.states, self.dt, self.bc)[0]
+        return time.time() - t0
+
+
+def cpu_baseline(budget_s=15.0):
+    sample = CpuSample()
+    steps, sec = 0, 0.0
+    while steps == 0 or sec < budget_s:
+        sec += sample.step()
+        steps += 1
+    return {"value": sample.dofs * steps / sec, "unit": UNIT, "cores": len(os.sched_getaffinity(0)),
+            "kind": "port",
+            "sample": f"oracle checked SSP-RK3 steps on a {sample.elements}-element P3 sphere O/H grid, "
+                      f"{steps} steps in {sec:.1f} s, float64 numpy"}
+
+
+def run_reference(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    sample = CpuSample()
+    for _ in range(args.warmup):
+        sample.step()
+    sec = sum(sample.step() for _ in range(args.steps))
+    value = sample.dofs * args.steps / sec
+    cb = {"value": value, "unit": UNIT, "cores": len(os.sched_getaffinity(0)), "kind": "port",
+          "sample": f"oracle checked SSP-RK3 steps on a {sample.elements}-element P3 sphere O/H grid, "
+                    f"{args.steps} timed steps in {sec:.1f} s, float64 numpy (the reference is Python/JAX; "
+                    f"JAX is not installable here, so its numpy restatement is timed)"}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "Mach-3 viscous sphere O/H hex grid, P3: bounded coarse sample on host cores"},
+            "cpu_baseline": cb,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--degree", type=int, default=3)
+    ap.add_argument("--scale", default="full", choices=["full", "small", "tiny"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,160 @@
+/*
+ * dgb200 -- B200 (sm_100a) hybrid-mesh DG residual-and-update path, C ABI.
+ *
+ * Drop-in boundary for the Python entry points of superboss2300/jax-fluid-sim
+ * (a pure Python/JAX project: there is no FFI in the reference; each entry
+ * point below names the Python method whose behaviour it replaces).
+ *
+ * Conventions
+ *   - All state arrays are DEVICE pointers owned by the caller, one per element
+ *     block in the reference's block order (hexahedron, wedge, tetra), each a
+ *     contiguous float64 array (elements, nodes, variables) -- the reference's
+ *     state layout (hybrid/state.py:7-37, hybrid/mesh.py:253-286).
+ *   - Plan tables are HOST pointers; dgb_plan_* copies them to the device and
+ *     the plan owns the copies.
+ *   - Return 0 on success, a negative dgb_error code on failure; the message of
+ *     the last failure on this thread is in dgb_last_error().
+ *   - A plan is not thread-safe; every call takes the CUDA stream to run on.
+ */
+#ifndef DGB200_H
+#define DGB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum dgb_error {
+  DGB_OK = 0,
+  DGB_ERR_ARGUMENT = -1,   /* invalid argument or plan state (reference raises ValueError) */
+  DGB_ERR_CUDA = -2,       /* CUDA runtime failure */
+  DGB_ERR_UNSUPPORTED = -3 /* configuration outside what the kernels implement */
+};
+
+enum { DGB_MAX_BLOCKS = 3, DGB_MAX_TAGS = 8, DGB_MAX_VARS = 16 };
+
+typedef struct dgb_plan dgb_plan;
+
+/* Physics, boundary and limiter constants.
+ *   HybridCompressibleSolver.__init__   hybrid/solver.py:20-61
+ *   FarfieldWallBoundary.__init__        hybrid/boundary.py:13-46
+ *   HybridPositivityLimiter.__init__     hybrid/limiter.py:14-26
+ *   HybridSSPRK3.__init__                hybrid/time_integration.py:9-25
+ *   HybridTroubledCellSensor.__init__    hybrid/limiter.py:153-163 */
+typedef struct {
+  int degree;                 /* 1..3 */
+  int nvars;                  /* 5 + species (5 or 16) */
+  int num_blocks;             /* 1..3 */
+  int viscous;                /* 1 when dynamic_viscosity > 0 */
+  double gamma, gas_constant, dynamic_viscosity, thermal_conductivity, br2_penalty;
+  int has_boundary;           /* 0: boundary_state=None (ghost = interior trace) */
+  double farfield_primitive[DGB_MAX_VARS];
+  int inlet_tags[DGB_MAX_TAGS], n_inlet;
+  int wall_tags[DGB_MAX_TAGS], n_wall;
+  int no_slip_tags[DGB_MAX_TAGS], n_no_slip;
+  int slip_tags[DGB_MAX_TAGS], n_slip;
+  int has_wall_temperature;
+  double wall_temperature;
+  double pos_density_floor, pos_pressure_floor, pos_relative_floor;
+  double adm_density_floor, adm_pressure_floor;
+  double sensor_threshold;
+  int limiter;                /* stage limiter of dgb_ssprk3_step: 0 none, 1 positivity */
+} dgb_params;
+
+/* One element block (hybrid/geometry.py:139-203 metrics, precomputed by the host). */
+typedef struct {
+  int element_type;           /* 0 hexahedron, 1 wedge, 2 tetra */
+  int num_elements, num_nodes, num_qp, num_local_faces;
+  const double* basis;        /* [Nq][Np]      basis at volume points          */
+  const double* basis_grad;   /* [Nq][Np][3]   reference gradients              */
+  const double* inv_jacobian; /* [E][Nq][3][3] dxi_r/dx_d                       */
+  const double* wdet;         /* [E][Nq]       w |det J|                        */
+  const double* inv_mass;     /* [E][Np][Np]   sliver-scaled inverse mass       */
+  const int32_t* elem_face;   /* [E][nlf]      (face type<<30)|(face<<1)|side   */
+  const double* length;       /* [E]           characteristic length (CFL)      */
+  int num_face_samples;
+  const double* face_sample_basis; /* [Ns][Np] basis at distinct face points    */
+  const double* p1_projector;      /* [Np][Np] sensor projector (P>=2)          */
+} dgb_block_desc;
+
+/* One face type (hybrid/mesh.py:378-459 topology, hybrid/geometry.py:226-362 metrics). */
+typedef struct {
+  int face_type;              /* 0 triangle, 1 quad */
+  int num_faces, num_qp;
+  const int32_t* owner_block; const int32_t* owner_local; const int32_t* owner_code;
+  const int32_t* nbr_block;   const int32_t* nbr_local;   const int32_t* nbr_code;  /* -1: boundary */
+  const int32_t* tags;        /* physical tag, -1 internal */
+  const double* normals;      /* [F][nq][3] */
+  const double* weights;      /* [F][nq]    */
+  const double* side_inv_jacobian; /* [F][2][nq][3][3] at owner / neighbour face points */
+} dgb_face_desc;
+
+/* Per-block device state pointers, (E_b, Np_b, nvars) float64 each. */
+typedef struct {
+  double* block[DGB_MAX_BLOCKS];
+} dgb_state;
+
+/* Admissibility of a stage/step (time_integration.py:291-312) in device memory. */
+typedef struct {
+  int32_t valid;
+  int32_t pad;
+  double rho_min;
+  double p_min;
+} dgb_status;
+
+const char* dgb_last_error(void);
+int dgb_version(void);
+
+/* Plan lifetime. */
+int dgb_plan_create(const dgb_params* params, dgb_plan** out);
+int dgb_plan_set_block(dgb_plan* plan, int block, const dgb_block_desc* desc);
+int dgb_plan_set_faces(dgb_plan* plan, const dgb_face_desc* desc);
+/* Trace tables for (element type, face type): basis [C][nq][Np] and gradients [C][nq][Np][3]
+ * at each code's reference face points. */
+int dgb_plan_set_trace(dgb_plan* plan, int element_type, int face_type, int num_codes, int num_qp,
+                       int num_nodes, const double* basis, const double* basis_grad);
+int dgb_plan_finalize(dgb_plan* plan);
+int dgb_plan_destroy(dgb_plan* plan);
+/* Replace the physics/boundary/limiter constants of a finalized plan (same mesh and degree);
+ * the reference passes boundary_state per call (hybrid/spatial.py:236). */
+int dgb_plan_update_params(dgb_plan* plan, const dgb_params* params);
+
+/* HybridEulerOperator.rhs (hybrid/spatial.py:236-249) -> inviscid_out;
+ * HybridNavierStokesOperator.viscous_rhs (hybrid/navier_stokes.py:326-336) -> viscous_out.
+ * Either output may be NULL (not computed / not written). */
+int dgb_rhs(dgb_plan* plan, const dgb_state* U, const dgb_state* inviscid_out,
+            const dgb_state* viscous_out, void* stream);
+
+/* HybridSSPRK3.stable_dt (hybrid/time_integration.py:93-169): writes the clipped dt
+ * to the device double *dt_out. */
+int dgb_stable_dt(dgb_plan* plan, const dgb_state* U, double cfl, double* dt_out, void* stream);
+
+/* HybridPositivityLimiter.__call__ (hybrid/limiter.py:100-147), in place. */
+int dgb_positivity(dgb_plan* plan, const dgb_state* U, void* stream);
+
+/* HybridTroubledCellSensor.__call__ (hybrid/limiter.py:165-185): sensor values [E_b] per block
+ * (device doubles, may be NULL) and HybridMOODSubcellLimiter.troubled (hybrid/limiter.py:285-300)
+ * flags [E_b] per block (device uint8, may be NULL). */
+int dgb_troubled(dgb_plan* plan, const dgb_state* U, double* const* sensor_out,
+                 uint8_t* const* flags_out, void* stream);
+
+/* HybridSSPRK3.state_admissibility (hybrid/time_integration.py:291-312) into *status (device). */
+int dgb_admissibility(dgb_plan* plan, const dgb_state* U, dgb_status* status, void* stream);
+
+/* HybridSSPRK3.checked_step without MOOD (hybrid/time_integration.py:404-439,556-583):
+ * three SSP-RK3 stages, each RHS -> blend -> positivity limiter -> admissibility, in place
+ * on U; *status (device) receives valid1&valid2&valid3 and the minima over the stages. */
+int dgb_ssprk3_step(dgb_plan* plan, const dgb_state* U, double dt, dgb_status* status, void* stream);
+
+/* Tracing (no reference counterpart; the reference only prints wall-clock progress,
+ * run_hybrid_sphere.py:366-390): runs one dgb_rhs with CUDA events around each kernel
+ * stage and writes the stage durations in milliseconds to host ms_out[DGB_RHS_STAGES]
+ * (traces, face flux, volume+lift, viscous face flux, finalize).  Synchronises the stream. */
+enum { DGB_RHS_STAGES = 5 };
+int dgb_rhs_profile(dgb_plan* plan, const dgb_state* U, float* ms_out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DGB200_H */

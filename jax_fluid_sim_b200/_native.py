@@ -1,0 +1,124 @@
+"""ctypes binding of ``libdgb200.so`` (declarations in ``include/dgb200.h``).
+
+There is no CPU fallback: if the library cannot be loaded, every entry point
+raises.  PyTorch is used only for device allocations and streams; the library
+receives raw pointers.
+"""
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+MAX_BLOCKS, MAX_TAGS, MAX_VARS = 3, 8, 16
+LIB_PATH = Path(__file__).resolve().parent / "libdgb200.so"
+
+c_int, c_double, c_void_p = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
+P_double = ctypes.POINTER(ctypes.c_double)
+P_int32 = ctypes.POINTER(ctypes.c_int32)
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("degree", c_int), ("nvars", c_int), ("num_blocks", c_int), ("viscous", c_int),
+        ("gamma", c_double), ("gas_constant", c_double), ("dynamic_viscosity", c_double),
+        ("thermal_conductivity", c_double), ("br2_penalty", c_double),
+        ("has_boundary", c_int),
+        ("farfield_primitive", c_double * MAX_VARS),
+        ("inlet_tags", c_int * MAX_TAGS), ("n_inlet", c_int),
+        ("wall_tags", c_int * MAX_TAGS), ("n_wall", c_int),
+        ("no_slip_tags", c_int * MAX_TAGS), ("n_no_slip", c_int),
+        ("slip_tags", c_int * MAX_TAGS), ("n_slip", c_int),
+        ("has_wall_temperature", c_int), ("wall_temperature", c_double),
+        ("pos_density_floor", c_double), ("pos_pressure_floor", c_double), ("pos_relative_floor", c_double),
+        ("adm_density_floor", c_double), ("adm_pressure_floor", c_double),
+        ("sensor_threshold", c_double),
+        ("limiter", c_int),
+    ]
+
+
+class BlockDesc(ctypes.Structure):
+    _fields_ = [
+        ("element_type", c_int), ("num_elements", c_int), ("num_nodes", c_int), ("num_qp", c_int),
+        ("num_local_faces", c_int),
+        ("basis", P_double), ("basis_grad", P_double), ("inv_jacobian", P_double), ("wdet", P_double),
+        ("inv_mass", P_double), ("elem_face", P_int32), ("length", P_double),
+        ("num_face_samples", c_int), ("face_sample_basis", P_double), ("p1_projector", P_double),
+    ]
+
+
+class FaceDesc(ctypes.Structure):
+    _fields_ = [
+        ("face_type", c_int), ("num_faces", c_int), ("num_qp", c_int),
+        ("owner_block", P_int32), ("owner_local", P_int32), ("owner_code", P_int32),
+        ("nbr_block", P_int32), ("nbr_local", P_int32), ("nbr_code", P_int32),
+        ("tags", P_int32), ("normals", P_double), ("weights", P_double), ("side_inv_jacobian", P_double),
+    ]
+
+
+class State(ctypes.Structure):
+    _fields_ = [("block", c_void_p * MAX_BLOCKS)]
+
+
+class Status(ctypes.Structure):
+    _fields_ = [("valid", ctypes.c_int32), ("pad", ctypes.c_int32), ("rho_min", c_double), ("p_min", c_double)]
+
+
+_lib = None
+
+
+def lib():
+    """Load the library once; raise loudly when it is missing (no CPU fallback)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m jax_fluid_sim_b200.build`")
+        L = ctypes.CDLL(str(LIB_PATH))
+        L.dgb_last_error.restype = ctypes.c_char_p
+        L.dgb_version.restype = c_int
+        sigs = {
+            "dgb_plan_create": [ctypes.POINTER(Params), ctypes.POINTER(c_void_p)],
+            "dgb_plan_set_block": [c_void_p, c_int, ctypes.POINTER(BlockDesc)],
+            "dgb_plan_set_faces": [c_void_p, ctypes.POINTER(FaceDesc)],
+            "dgb_plan_set_trace": [c_void_p, c_int, c_int, c_int, c_int, c_int, P_double, P_double],
+            "dgb_plan_finalize": [c_void_p],
+            "dgb_plan_destroy": [c_void_p],
+            "dgb_plan_update_params": [c_void_p, ctypes.POINTER(Params)],
+            "dgb_rhs": [c_void_p, ctypes.POINTER(State), ctypes.POINTER(State), ctypes.POINTER(State), c_void_p],
+            "dgb_stable_dt": [c_void_p, ctypes.POINTER(State), c_double, c_void_p, c_void_p],
+            "dgb_positivity": [c_void_p, ctypes.POINTER(State), c_void_p],
+            "dgb_troubled": [c_void_p, ctypes.POINTER(State), c_void_p, c_void_p, c_void_p],
+            "dgb_admissibility": [c_void_p, ctypes.POINTER(State), c_void_p, c_void_p],
+            "dgb_ssprk3_step": [c_void_p, ctypes.POINTER(State), c_double, c_void_p, c_void_p],
+            "dgb_rhs_profile": [c_void_p, ctypes.POINTER(State), ctypes.POINTER(ctypes.c_float), c_void_p],
+        }
+        for name, args in sigs.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = c_int
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    if rc != 0:
+        msg = lib().dgb_last_error().decode()
+        if rc == -1:
+            raise ValueError(msg)
+        if rc == -3:
+            raise NotImplementedError(msg)
+        raise RuntimeError(f"dgb200 error {rc}: {msg}")
+
+
+def dptr(a, ctype=ctypes.c_double):
+    """Pointer to a C-contiguous numpy array (the caller keeps the array alive)."""
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def as_f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def as_i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)

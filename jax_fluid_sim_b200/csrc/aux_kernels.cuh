@@ -1,0 +1,367 @@
+// Element-local limiter, detector and reduction kernels (float64).
+//
+//   k_positivity    Zhang-Shu scaling toward the cell mean: density theta in closed form,
+//                   pressure theta by 30 bisection steps over node, volume-point and
+//                   face-point samples (hybrid/limiter.py:69-147).
+//   k_troubled      Persson-type high-mode sensor on (rho, p) plus the MOOD admissibility
+//                   test at samples and the mean (hybrid/limiter.py:165-185, 285-300).
+//   k_rate / k_dt   CFL rate per element, max by warp shuffles then one final CTA
+//                   (hybrid/time_integration.py:93-169).
+//   k_adm / k_adm_final   finite check and min rho / min p over all nodes
+//                   (hybrid/time_integration.py:291-312), combined across stages.
+#pragma once
+#include "dg_kernels.cuh"
+
+namespace dgb {
+
+struct LimiterConst {
+  double density_floor, pressure_floor, relative_floor;   // positivity limiter
+  double adm_density_floor, adm_pressure_floor;           // integrator admissibility
+  double sensor_threshold;
+};
+
+template <int NV>
+__device__ __forceinline__ double pressure_of(const Physics& ph, const double* U) {
+  const double srho = fmax(U[0], kRhoFloor);
+  const double ke = 0.5 * (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / srho;
+  return (ph.gamma - 1.0) * (U[4] - ke);
+}
+
+// samples = [U at nodes; B U at volume points; Bfs U at face points]  -> S[Ns_total][NV]
+template <int NV>
+__device__ void build_samples(const BlockDev& B, const double* U, double* S) {
+  const int Np = B.Np, Nq = B.Nq, Ns = B.Ns;
+  const int total = (Np + Nq + Ns) * NV;
+  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+    const int r = idx / NV, v = idx % NV;
+    double val;
+    if (r < Np) {
+      val = U[r * NV + v];
+    } else {
+      const double* row = r < Np + Nq ? B.B + (size_t)(r - Np) * Np : B.fsB + (size_t)(r - Np - Nq) * Np;
+      double s = 0.0;
+      for (int i = 0; i < Np; ++i) s += row[i] * U[i * NV + v];
+      val = s;
+    }
+    S[idx] = val;
+  }
+}
+
+// Cell mean: sum_q wdet (B U) / sum_q wdet, from the volume samples.
+template <int NV>
+__device__ void cell_mean(const BlockDev& B, int e, const double* Svol, double* mean) {
+  const double* wdet = B.wdet + (size_t)e * B.Nq;
+  for (int v = threadIdx.x; v < NV; v += blockDim.x) {
+    double s = 0.0, wsum = 0.0;
+    for (int q = 0; q < B.Nq; ++q) {
+      s += Svol[q * NV + v] * wdet[q];
+      wsum += wdet[q];
+    }
+    mean[v] = s / wsum;
+  }
+}
+
+template <int NV>
+__global__ void __launch_bounds__(kThreads) k_positivity(const DevPlan P, const StatePtrs S, int b,
+                                                        const LimiterConst L) {
+  extern __shared__ double smem[];
+  __shared__ double mean[NV];
+  __shared__ double sh_theta_rho;
+  const BlockDev& B = P.blk[b];
+  const int e = blockIdx.x;
+  const int Np = B.Np, Nq = B.Nq;
+  const int Nt = Np + Nq + B.Ns;
+  double* U = smem;
+  double* Smp = U + Np * NV;
+  double* Ug = S.b[b] + (size_t)e * Np * NV;
+  for (int i = threadIdx.x; i < Np * NV; i += blockDim.x) U[i] = Ug[i];
+  __syncthreads();
+  build_samples<NV>(B, U, Smp);
+  __syncthreads();
+  cell_mean<NV>(B, e, Smp + Np * NV, mean);
+  __syncthreads();
+  double Wm[NV];
+  primitive<NV>(P.ph, mean, Wm);
+  const double rfloor = fmax(L.density_floor, L.relative_floor * Wm[0]);
+  const double pfloor = fmax(L.pressure_floor, L.relative_floor * Wm[4]);
+  // minimum sampled density
+  double rmin = INFINITY;
+  bool nan_seen = false;
+  for (int r = threadIdx.x; r < Nt; r += blockDim.x) {
+    const double d = Smp[r * NV];
+    nan_seen |= isnan(d);
+    rmin = fmin(rmin, d);
+  }
+  // block min (NaN propagates like a jnp.min)
+  __shared__ double red[kThreads / 32];
+  __shared__ int red_nan;
+  if (threadIdx.x == 0) red_nan = 0;
+  for (int o = 16; o > 0; o >>= 1) rmin = fmin(rmin, __shfl_xor_sync(0xffffffff, rmin, o));
+  __syncthreads();
+  if (nan_seen) atomicOr(&red_nan, 1);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = rmin;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = red[0];
+    for (int k = 1; k < kThreads / 32; ++k) m = fmin(m, red[k]);
+    if (red_nan) m = NAN;
+    const double denom = mean[0] - m;
+    const double th = (m < rfloor) ? (mean[0] - rfloor) / fmax(denom, 1.0e-30) : 1.0;
+    // jnp.clip(x, 0, 1) keeps NaN as NaN
+    sh_theta_rho = isnan(th) ? th : fmin(fmax(th, 0.0), 1.0);
+  }
+  __syncthreads();
+  const double upper = sh_theta_rho;
+  // pressure admissibility of mean + theta*(sample - mean) at every sample
+  auto pressure_ok = [&](double theta) -> bool {
+    bool ok = true;
+    for (int r = threadIdx.x; r < Nt; r += blockDim.x) {
+      double s[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) s[v] = mean[v] + theta * (Smp[r * NV + v] - mean[v]);
+      ok &= (pressure_of<NV>(P.ph, s) >= pfloor);
+    }
+    return __syncthreads_and(ok);
+  };
+  double lo = 0.0, hi = upper;
+  for (int it = 0; it < 30; ++it) {
+    const double mid = 0.5 * (lo + hi);
+    const bool ok = pressure_ok(mid);
+    lo = ok ? mid : lo;
+    hi = ok ? hi : mid;
+  }
+  const double theta = pressure_ok(upper) ? upper : lo;
+  for (int idx = threadIdx.x; idx < Np * NV; idx += blockDim.x) {
+    const int v = idx % NV;
+    Ug[idx] = mean[v] + theta * (U[idx] - mean[v]);
+  }
+}
+
+template <int NV>
+__global__ void __launch_bounds__(kThreads) k_troubled(const DevPlan P, const StatePtrs S, int b, const LimiterConst L,
+                                                      double* sensor_out, uint8_t* flag_out) {
+  extern __shared__ double smem[];
+  __shared__ double mean[NV];
+  __shared__ double red[4][kThreads / 32];
+  const BlockDev& B = P.blk[b];
+  const int e = blockIdx.x;
+  const int Np = B.Np, Nq = B.Nq;
+  const int Nt = Np + Nq + B.Ns;
+  double* U = smem;
+  double* Smp = U + Np * NV;
+  double* Mon = Smp + Nt * NV;   // [Np][2] monitored (rho, p)
+  const double* Ug = S.b[b] + (size_t)e * Np * NV;
+  for (int i = threadIdx.x; i < Np * NV; i += blockDim.x) U[i] = Ug[i];
+  __syncthreads();
+  build_samples<NV>(B, U, Smp);
+  for (int i = threadIdx.x; i < Np; i += blockDim.x) {
+    double W[NV];
+    primitive<NV>(P.ph, U + i * NV, W);
+    Mon[i * 2 + 0] = W[0];
+    Mon[i * 2 + 1] = W[4];
+  }
+  __syncthreads();
+  cell_mean<NV>(B, e, Smp + Np * NV, mean);
+  // sensor: sum_i (m - Pi m)^2 / max(sum_i m^2, 1e-12), max over (rho, p)
+  double hi0 = 0.0, hi1 = 0.0, sc0 = 0.0, sc1 = 0.0;
+  if (P.degree >= 2) {
+    for (int i = threadIdx.x; i < Np; i += blockDim.x) {
+      double l0 = 0.0, l1 = 0.0;
+      for (int j = 0; j < Np; ++j) {
+        l0 += B.p1proj[(size_t)i * Np + j] * Mon[j * 2 + 0];
+        l1 += B.p1proj[(size_t)i * Np + j] * Mon[j * 2 + 1];
+      }
+      const double d0 = Mon[i * 2 + 0] - l0, d1 = Mon[i * 2 + 1] - l1;
+      hi0 += d0 * d0;
+      hi1 += d1 * d1;
+      sc0 += Mon[i * 2 + 0] * Mon[i * 2 + 0];
+      sc1 += Mon[i * 2 + 1] * Mon[i * 2 + 1];
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    hi0 += __shfl_xor_sync(0xffffffff, hi0, o);
+    hi1 += __shfl_xor_sync(0xffffffff, hi1, o);
+    sc0 += __shfl_xor_sync(0xffffffff, sc0, o);
+    sc1 += __shfl_xor_sync(0xffffffff, sc1, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = hi0;
+    red[1][threadIdx.x >> 5] = hi1;
+    red[2][threadIdx.x >> 5] = sc0;
+    red[3][threadIdx.x >> 5] = sc1;
+  }
+  __syncthreads();
+  // invalid samples (including the cell mean)
+  bool bad = false;
+  for (int r = threadIdx.x; r <= Nt; r += blockDim.x) {
+    const double* s = r < Nt ? Smp + r * NV : mean;
+    double W[NV];
+    primitive<NV>(P.ph, s, W);
+    bool finite = true;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) finite &= isfinite(W[v]);
+    bad |= !finite || (W[0] < L.density_floor) || (W[4] < L.pressure_floor);
+  }
+  const bool any_bad = __syncthreads_or(bad);
+  if (threadIdx.x == 0) {
+    double h0 = 0, h1 = 0, s0 = 0, s1 = 0;
+    for (int k = 0; k < kThreads / 32; ++k) {
+      h0 += red[0][k]; h1 += red[1][k]; s0 += red[2][k]; s1 += red[3][k];
+    }
+    double value = 0.0;
+    if (P.degree >= 2) {
+      const double r0 = h0 / fmax(s0, 1.0e-12), r1 = h1 / fmax(s1, 1.0e-12);
+      value = (isnan(r0) || isnan(r1)) ? NAN : fmax(r0, r1);
+    }
+    if (sensor_out) sensor_out[e] = value;
+    if (flag_out) flag_out[e] = (uint8_t)((value > L.sensor_threshold) || any_bad);
+  }
+}
+
+// ---------------------------------------------------------------- reductions
+struct Partial {
+  double a, b;   // (max rate) or (rho_min, p_min)
+  int flag;      // finite / nan seen
+  int pad;
+};
+
+template <int NV>
+__global__ void __launch_bounds__(kThreads) k_rate(const DevPlan P, const StatePtrs S, int b, double cp,
+                                                  Partial* partials, int offset) {
+  // one warp per element; grid-stride over elements
+  const BlockDev& B = P.blk[b];
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const double df = 2.0 * P.degree + 1.0;
+  double best = -INFINITY;
+  for (int e = warp; e < B.E; e += nwarps) {
+    const double* U = S.b[b] + (size_t)e * B.Np * NV;
+    double smax = -INFINITY, rsum = 0.0;
+    bool en = false;
+    for (int i = lane; i < B.Np; i += 32) {
+      double W[NV];
+      primitive<NV>(P.ph, U + i * NV, W);
+      const double rho = fmax(W[0], 1.0e-14), p = fmax(W[4], 1.0e-14);
+      const double sp = sqrt(W[1] * W[1] + W[2] * W[2] + W[3] * W[3]) + sqrt(P.ph.gamma * p / rho);
+      en |= isnan(sp);
+      smax = fmax(smax, sp);
+      rsum += rho;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      smax = fmax(smax, __shfl_xor_sync(0xffffffff, smax, o));
+      rsum += __shfl_xor_sync(0xffffffff, rsum, o);
+    }
+    en = __any_sync(0xffffffff, en);
+    const double h = B.length[e];
+    double rate = en ? NAN : df * smax / h;
+    if (P.viscous) {
+      const double rmin = fmax(rsum / B.Np, 0.1);
+      const double diff = fmax((4.0 / 3.0) * P.ph.mu / rmin, P.ph.kappa / (rmin * cp));
+      const double vl = fmax(h, 0.01);
+      rate = rate + 2.0 * P.ph.br2 * df * df * diff / (vl * vl);
+    }
+    // jnp.nan_to_num(rate, nan=1e7, posinf=1e7)
+    if (isnan(rate) || (isinf(rate) && rate > 0.0)) rate = 1.0e7;
+    else if (isinf(rate)) rate = -1.7976931348623157e308;
+    best = fmax(best, rate);
+  }
+  __shared__ double red[kThreads / 32];
+  if (lane == 0) red[threadIdx.x >> 5] = best;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = red[0];
+    for (int k = 1; k < kThreads / 32; ++k) m = fmax(m, red[k]);
+    partials[offset + blockIdx.x].a = m;
+  }
+}
+
+__global__ void k_dt(const Partial* partials, int n, double cfl, double* dt_out) {
+  __shared__ double red[kThreads];
+  double m = -INFINITY;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, partials[i].a);
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double dt = cfl / fmax(red[0], 1.0e-12);
+    *dt_out = fmin(fmax(dt, 1.0e-7), 1.0e-3);
+  }
+}
+
+template <int NV>
+__global__ void __launch_bounds__(kThreads) k_adm(const DevPlan P, const StatePtrs S, int b, Partial* partials,
+                                                 int offset) {
+  const BlockDev& B = P.blk[b];
+  const size_t nodes = (size_t)B.E * B.Np;
+  double rmin = INFINITY, pmin = INFINITY;
+  int finite = 1, rnan = 0, pnan = 0;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nodes; k += (size_t)gridDim.x * blockDim.x) {
+    const double* U = S.b[b] + k * NV;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) finite &= isfinite(U[v]) ? 1 : 0;
+    const double p = pressure_of<NV>(P.ph, U);
+    rnan |= isnan(U[0]);
+    pnan |= isnan(p);
+    rmin = fmin(rmin, U[0]);
+    pmin = fmin(pmin, p);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    rmin = fmin(rmin, __shfl_xor_sync(0xffffffff, rmin, o));
+    pmin = fmin(pmin, __shfl_xor_sync(0xffffffff, pmin, o));
+  }
+  finite = __syncthreads_and(finite);
+  rnan = __syncthreads_or(rnan);
+  pnan = __syncthreads_or(pnan);
+  __shared__ double r1[kThreads / 32], r2[kThreads / 32];
+  if ((threadIdx.x & 31) == 0) {
+    r1[threadIdx.x >> 5] = rmin;
+    r2[threadIdx.x >> 5] = pmin;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = r1[0], c = r2[0];
+    for (int k = 1; k < kThreads / 32; ++k) {
+      a = fmin(a, r1[k]);
+      c = fmin(c, r2[k]);
+    }
+    Partial out;
+    out.a = rnan ? NAN : a;
+    out.b = pnan ? NAN : c;
+    out.flag = finite;
+    out.pad = 0;
+    partials[offset + blockIdx.x] = out;
+  }
+}
+
+// combine: first stage overwrites the status, later stages AND / min into it
+__global__ void k_adm_final(const Partial* partials, int n, double rho_floor, double p_floor, int combine,
+                            dgb_status* status) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double rmin = INFINITY, pmin = INFINITY;
+  int finite = 1, rnan = 0, pnan = 0;
+  for (int i = 0; i < n; ++i) {
+    rnan |= isnan(partials[i].a);
+    pnan |= isnan(partials[i].b);
+    rmin = fmin(rmin, partials[i].a);
+    pmin = fmin(pmin, partials[i].b);
+    finite &= partials[i].flag;
+  }
+  if (rnan) rmin = NAN;
+  if (pnan) pmin = NAN;
+  const int valid = finite && (rmin >= rho_floor) && (pmin >= p_floor);
+  if (combine) {
+    status->valid = status->valid && valid;
+    status->rho_min = (isnan(status->rho_min) || isnan(rmin)) ? NAN : fmin(status->rho_min, rmin);
+    status->p_min = (isnan(status->p_min) || isnan(pmin)) ? NAN : fmin(status->p_min, pmin);
+  } else {
+    status->valid = valid;
+    status->rho_min = rmin;
+    status->p_min = pmin;
+  }
+}
+
+}  // namespace dgb

@@ -1,0 +1,507 @@
+// C ABI of the dgb200 library: plan construction and the hot-path entry points.
+// Declarations and the reference method each entry point replaces: include/dgb200.h.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "aux_kernels.cuh"
+
+using namespace dgb;
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string& msg) {
+  g_error = msg;
+  return code;
+}
+
+#define CK(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t err__ = (call);                                                           \
+    if (err__ != cudaSuccess)                                                             \
+      return fail(DGB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(err__));   \
+  } while (0)
+
+}  // namespace
+
+struct dgb_plan {
+  dgb_params prm;
+  DevPlan dev;
+  LimiterConst lim;
+  std::vector<void*> allocations;
+  bool block_set[DGB_MAX_BLOCKS] = {false, false, false};
+  bool finalized = false;
+  bool face_present[2] = {false, false};
+  // stage buffers for SSP-RK3
+  double* stage1[DGB_MAX_BLOCKS] = {nullptr, nullptr, nullptr};
+  double* stage2[DGB_MAX_BLOCKS] = {nullptr, nullptr, nullptr};
+  Partial* partials = nullptr;
+  int rate_grid[DGB_MAX_BLOCKS] = {0, 0, 0};
+  int adm_grid[DGB_MAX_BLOCKS] = {0, 0, 0};
+  int npartials = 0;
+  double* dt_scratch = nullptr;
+  size_t smem_traces[DGB_MAX_BLOCKS], smem_volume[DGB_MAX_BLOCKS], smem_final[DGB_MAX_BLOCKS];
+  size_t smem_pos[DGB_MAX_BLOCKS], smem_troubled[DGB_MAX_BLOCKS];
+};
+
+namespace {
+
+template <typename T>
+int upload(dgb_plan* p, const T* host, size_t count, const T** out) {
+  if (count == 0) {
+    *out = nullptr;
+    return DGB_OK;
+  }
+  if (!host) return fail(DGB_ERR_ARGUMENT, "null host table");
+  void* d = nullptr;
+  CK(cudaMalloc(&d, count * sizeof(T)));
+  p->allocations.push_back(d);
+  CK(cudaMemcpy(d, host, count * sizeof(T), cudaMemcpyHostToDevice));
+  *out = static_cast<const T*>(d);
+  return DGB_OK;
+}
+
+int alloc(dgb_plan* p, size_t count, double** out) {
+  void* d = nullptr;
+  if (count == 0) count = 1;
+  CK(cudaMalloc(&d, count * sizeof(double)));
+  p->allocations.push_back(d);
+  CK(cudaMemset(d, 0, count * sizeof(double)));
+  *out = static_cast<double*>(d);
+  return DGB_OK;
+}
+
+StatePtrs to_ptrs(const dgb_state* s) {
+  StatePtrs out;
+  for (int b = 0; b < DGB_MAX_BLOCKS; ++b) out.b[b] = s ? s->block[b] : nullptr;
+  return out;
+}
+
+template <typename K>
+int prepare(K kernel, size_t smem) {
+  if (smem > 48 * 1024) CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  return DGB_OK;
+}
+
+int blocks_for(long n, int per) { return (int)((n + per - 1) / per); }
+
+// ------------------------------------------------------------------ RHS pipeline
+// events: optional array of DGB_RHS_STAGES + 1 events recorded around the stages
+template <int NV>
+int run_rhs(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStream_t st, cudaEvent_t* ev = nullptr) {
+  const DevPlan& P = p->dev;
+  int rc;
+  if (ev) CK(cudaEventRecord(ev[0], st));
+  for (int b = 0; b < P.nblocks; ++b) {
+    if ((rc = prepare(k_traces<NV>, p->smem_traces[b]))) return rc;
+    k_traces<NV><<<P.blk[b].E, kThreads, p->smem_traces[b], st>>>(P, S, b);
+  }
+  if (ev) CK(cudaEventRecord(ev[1], st));
+  for (int ft = 0; ft < 2; ++ft)
+    if (p->face_present[ft])
+      k_face_flux<NV><<<blocks_for((long)P.face[ft].F * P.face[ft].nq, kThreads), kThreads, 0, st>>>(P, S, ft);
+  if (ev) CK(cudaEventRecord(ev[2], st));
+  for (int b = 0; b < P.nblocks; ++b) {
+    if ((rc = prepare(k_volume<NV>, p->smem_volume[b]))) return rc;
+    k_volume<NV><<<P.blk[b].E, kThreads, p->smem_volume[b], st>>>(P, S, b);
+  }
+  if (ev) CK(cudaEventRecord(ev[3], st));
+  if (P.viscous)
+    for (int ft = 0; ft < 2; ++ft)
+      if (p->face_present[ft])
+        k_face_visc<NV><<<blocks_for((long)P.face[ft].F * P.face[ft].nq, kThreads), kThreads, 0, st>>>(P, ft);
+  if (ev) CK(cudaEventRecord(ev[4], st));
+  for (int b = 0; b < P.nblocks; ++b) {
+    if ((rc = prepare(k_finalize<NV>, p->smem_final[b]))) return rc;
+    k_finalize<NV><<<P.blk[b].E, kThreads, p->smem_final[b], st>>>(P, S, b, A);
+  }
+  if (ev) CK(cudaEventRecord(ev[5], st));
+  CK(cudaGetLastError());
+  return DGB_OK;
+}
+
+template <int NV>
+int run_positivity(dgb_plan* p, const StatePtrs& S, cudaStream_t st) {
+  int rc;
+  for (int b = 0; b < p->dev.nblocks; ++b) {
+    if ((rc = prepare(k_positivity<NV>, p->smem_pos[b]))) return rc;
+    k_positivity<NV><<<p->dev.blk[b].E, kThreads, p->smem_pos[b], st>>>(p->dev, S, b, p->lim);
+  }
+  CK(cudaGetLastError());
+  return DGB_OK;
+}
+
+template <int NV>
+int run_admissibility(dgb_plan* p, const StatePtrs& S, dgb_status* status, int combine, cudaStream_t st) {
+  int off = 0;
+  for (int b = 0; b < p->dev.nblocks; ++b) {
+    k_adm<NV><<<p->adm_grid[b], kThreads, 0, st>>>(p->dev, S, b, p->partials, off);
+    off += p->adm_grid[b];
+  }
+  k_adm_final<<<1, 32, 0, st>>>(p->partials, off, p->lim.adm_density_floor, p->lim.adm_pressure_floor, combine,
+                                status);
+  CK(cudaGetLastError());
+  return DGB_OK;
+}
+
+template <int NV>
+int run_stable_dt(dgb_plan* p, const StatePtrs& S, double cfl, double* dt_out, cudaStream_t st) {
+  int off = 0;
+  const double cp = p->prm.gamma * p->prm.gas_constant / (p->prm.gamma - 1.0);
+  for (int b = 0; b < p->dev.nblocks; ++b) {
+    k_rate<NV><<<p->rate_grid[b], kThreads, 0, st>>>(p->dev, S, b, cp, p->partials, off);
+    off += p->rate_grid[b];
+  }
+  k_dt<<<1, kThreads, 0, st>>>(p->partials, off, cfl, dt_out);
+  CK(cudaGetLastError());
+  return DGB_OK;
+}
+
+template <int NV>
+int run_troubled(dgb_plan* p, const StatePtrs& S, double* const* sensor, uint8_t* const* flags, cudaStream_t st) {
+  int rc;
+  for (int b = 0; b < p->dev.nblocks; ++b) {
+    if ((rc = prepare(k_troubled<NV>, p->smem_troubled[b]))) return rc;
+    k_troubled<NV><<<p->dev.blk[b].E, kThreads, p->smem_troubled[b], st>>>(
+        p->dev, S, b, p->lim, sensor ? sensor[b] : nullptr, flags ? flags[b] : nullptr);
+  }
+  CK(cudaGetLastError());
+  return DGB_OK;
+}
+
+template <int NV>
+int run_step(dgb_plan* p, const StatePtrs& U0, double dt, dgb_status* status, cudaStream_t st) {
+  const DevPlan& P = p->dev;
+  StatePtrs S1, S2;
+  for (int b = 0; b < DGB_MAX_BLOCKS; ++b) {
+    S1.b[b] = p->stage1[b];
+    S2.b[b] = p->stage2[b];
+  }
+  const double alphas[3] = {0.0, 0.75, 1.0 / 3.0};
+  const double betas[3] = {1.0, 0.25, 2.0 / 3.0};
+  const StatePtrs* cur[3] = {&U0, &S1, &S2};
+  const StatePtrs* dst[3] = {&S1, &S2, &U0};
+  int rc;
+  for (int s = 0; s < 3; ++s) {
+    FinalizeArgs A;
+    memset(&A, 0, sizeof(A));
+    A.stage = 1;
+    A.alpha = alphas[s];
+    A.beta = betas[s];
+    A.dt = dt;
+    for (int b = 0; b < P.nblocks; ++b) {
+      A.base[b] = U0.b[b];
+      A.dst[b] = dst[s]->b[b];
+    }
+    if ((rc = run_rhs<NV>(p, *cur[s], A, st))) return rc;
+    if (p->prm.limiter == 1 && (rc = run_positivity<NV>(p, *dst[s], st))) return rc;
+    if ((rc = run_admissibility<NV>(p, *dst[s], status, s > 0, st))) return rc;
+  }
+  return DGB_OK;
+}
+
+int check_ready(dgb_plan* p) {
+  if (!p) return fail(DGB_ERR_ARGUMENT, "null plan");
+  if (!p->finalized) return fail(DGB_ERR_ARGUMENT, "plan not finalized");
+  return DGB_OK;
+}
+
+int check_state(dgb_plan* p, const dgb_state* s, const char* what) {
+  if (!s) return fail(DGB_ERR_ARGUMENT, std::string(what) + " is null");
+  for (int b = 0; b < p->dev.nblocks; ++b)
+    if (!s->block[b]) return fail(DGB_ERR_ARGUMENT, std::string(what) + ": null block pointer");
+  return DGB_OK;
+}
+
+}  // namespace
+
+static void set_params(dgb_plan* p, const dgb_params* prm);
+
+extern "C" {
+
+const char* dgb_last_error(void) { return g_error.c_str(); }
+
+int dgb_version(void) { return 1; }
+
+int dgb_plan_create(const dgb_params* prm, dgb_plan** out) {
+  if (!prm || !out) return fail(DGB_ERR_ARGUMENT, "null argument");
+  if (prm->degree < 1 || prm->degree > 3) return fail(DGB_ERR_ARGUMENT, "Only P1, P2, and P3 are currently implemented");
+  if (prm->nvars != 5 && prm->nvars != 16) return fail(DGB_ERR_UNSUPPORTED, "nvars must be 5 or 16");
+  if (prm->num_blocks < 1 || prm->num_blocks > DGB_MAX_BLOCKS) return fail(DGB_ERR_ARGUMENT, "num_blocks out of range");
+  if (prm->n_inlet > DGB_MAX_TAGS || prm->n_wall > DGB_MAX_TAGS || prm->n_no_slip > DGB_MAX_TAGS ||
+      prm->n_slip > DGB_MAX_TAGS)
+    return fail(DGB_ERR_ARGUMENT, "too many boundary tags");
+  dgb_plan* p = new dgb_plan();
+  memset(&p->dev, 0, sizeof(p->dev));
+  p->dev.nv = prm->nvars;
+  p->dev.nblocks = prm->num_blocks;
+  p->dev.viscous = prm->viscous;
+  p->dev.degree = prm->degree;
+  set_params(p, prm);
+  *out = p;
+  return DGB_OK;
+}
+
+int dgb_plan_update_params(dgb_plan* p, const dgb_params* prm) {
+  if (!p || !prm) return fail(DGB_ERR_ARGUMENT, "null argument");
+  if (prm->degree != p->dev.degree || prm->nvars != p->dev.nv || prm->num_blocks != p->dev.nblocks ||
+      prm->viscous != p->dev.viscous)
+    return fail(DGB_ERR_ARGUMENT, "degree, nvars, blocks and viscous flag are fixed for a plan");
+  if (prm->n_inlet > DGB_MAX_TAGS || prm->n_wall > DGB_MAX_TAGS || prm->n_no_slip > DGB_MAX_TAGS ||
+      prm->n_slip > DGB_MAX_TAGS)
+    return fail(DGB_ERR_ARGUMENT, "too many boundary tags");
+  set_params(p, prm);
+  return DGB_OK;
+}
+
+}  // extern "C"
+
+static void set_params(dgb_plan* p, const dgb_params* prm) {
+  p->prm = *prm;
+  Physics& ph = p->dev.ph;
+  ph.gamma = prm->gamma;
+  ph.R = prm->gas_constant;
+  ph.mu = prm->dynamic_viscosity;
+  ph.kappa = prm->thermal_conductivity;
+  ph.br2 = prm->br2_penalty;
+  ph.has_boundary = prm->has_boundary;
+  for (int v = 0; v < DGB_MAX_VARS; ++v) ph.farfield_W[v] = prm->farfield_primitive[v];
+  ph.n_inlet = prm->n_inlet;
+  ph.n_wall = prm->n_wall;
+  ph.n_no_slip = prm->n_no_slip;
+  ph.n_slip = prm->n_slip;
+  for (int k = 0; k < DGB_MAX_TAGS; ++k) {
+    ph.inlet[k] = prm->inlet_tags[k];
+    ph.wall[k] = prm->wall_tags[k];
+    ph.no_slip[k] = prm->no_slip_tags[k];
+    ph.slip[k] = prm->slip_tags[k];
+  }
+  ph.has_wall_T = prm->has_wall_temperature;
+  ph.wall_T = prm->wall_temperature;
+  p->lim.density_floor = prm->pos_density_floor;
+  p->lim.pressure_floor = prm->pos_pressure_floor;
+  p->lim.relative_floor = prm->pos_relative_floor;
+  p->lim.adm_density_floor = prm->adm_density_floor;
+  p->lim.adm_pressure_floor = prm->adm_pressure_floor;
+  p->lim.sensor_threshold = prm->sensor_threshold;
+}
+
+extern "C" {
+
+int dgb_plan_set_block(dgb_plan* p, int b, const dgb_block_desc* d) {
+  if (!p || !d || b < 0 || b >= p->dev.nblocks) return fail(DGB_ERR_ARGUMENT, "bad block argument");
+  if (p->finalized) return fail(DGB_ERR_ARGUMENT, "plan already finalized");
+  BlockDev& B = p->dev.blk[b];
+  B.type = d->element_type;
+  B.E = d->num_elements;
+  B.Np = d->num_nodes;
+  B.Nq = d->num_qp;
+  B.nlf = d->num_local_faces;
+  B.Ns = d->num_face_samples;
+  const size_t E = B.E, Np = B.Np, Nq = B.Nq;
+  int rc;
+  if ((rc = upload(p, d->basis, Nq * Np, &B.B))) return rc;
+  if ((rc = upload(p, d->basis_grad, Nq * Np * 3, &B.dB))) return rc;
+  if ((rc = upload(p, d->inv_jacobian, E * Nq * 9, &B.jinv))) return rc;
+  if ((rc = upload(p, d->wdet, E * Nq, &B.wdet))) return rc;
+  if ((rc = upload(p, d->inv_mass, E * Np * Np, &B.minv))) return rc;
+  if ((rc = upload(p, d->length, E, &B.length))) return rc;
+  if ((rc = upload(p, d->face_sample_basis, (size_t)B.Ns * Np, &B.fsB))) return rc;
+  if ((rc = upload(p, d->p1_projector, Np * Np, &B.p1proj))) return rc;
+  if ((rc = upload(p, d->elem_face, E * B.nlf, &B.elem_face))) return rc;
+  p->block_set[b] = true;
+  return DGB_OK;
+}
+
+int dgb_plan_set_faces(dgb_plan* p, const dgb_face_desc* d) {
+  if (!p || !d || d->face_type < 0 || d->face_type > 1) return fail(DGB_ERR_ARGUMENT, "bad face argument");
+  if (p->finalized) return fail(DGB_ERR_ARGUMENT, "plan already finalized");
+  FaceDev& F = p->dev.face[d->face_type];
+  F.F = d->num_faces;
+  F.nq = d->num_qp;
+  const size_t n = F.F, nq = F.nq;
+  int rc;
+  if ((rc = upload(p, d->owner_block, n, &F.ob))) return rc;
+  if ((rc = upload(p, d->owner_local, n, &F.ol))) return rc;
+  if ((rc = upload(p, d->owner_code, n, &F.oc))) return rc;
+  if ((rc = upload(p, d->nbr_block, n, &F.nb))) return rc;
+  if ((rc = upload(p, d->nbr_local, n, &F.nl))) return rc;
+  if ((rc = upload(p, d->nbr_code, n, &F.nc))) return rc;
+  if ((rc = upload(p, d->tags, n, &F.tag))) return rc;
+  if ((rc = upload(p, d->normals, n * nq * 3, &F.n))) return rc;
+  if ((rc = upload(p, d->weights, n * nq, &F.w))) return rc;
+  if ((rc = upload(p, d->side_inv_jacobian, n * 2 * nq * 9, &F.jinv))) return rc;
+  p->face_present[d->face_type] = n > 0;
+  return DGB_OK;
+}
+
+int dgb_plan_set_trace(dgb_plan* p, int etype, int ftype, int ncodes, int nq, int np, const double* B,
+                       const double* dB) {
+  if (!p || ftype < 0 || ftype > 1) return fail(DGB_ERR_ARGUMENT, "bad trace argument");
+  int found = 0;
+  for (int b = 0; b < p->dev.nblocks; ++b) {
+    BlockDev& blk = p->dev.blk[b];
+    if (!p->block_set[b] || blk.type != etype) continue;
+    if (blk.Np != np) return fail(DGB_ERR_ARGUMENT, "trace table node count mismatch");
+    int rc;
+    if ((rc = upload(p, B, (size_t)ncodes * nq * np, &blk.trB[ftype]))) return rc;
+    if ((rc = upload(p, dB, (size_t)ncodes * nq * np * 3, &blk.trdB[ftype]))) return rc;
+    found = 1;
+  }
+  if (!found) return fail(DGB_ERR_ARGUMENT, "trace table for an element type without a block");
+  return DGB_OK;
+}
+
+int dgb_plan_finalize(dgb_plan* p) {
+  if (!p) return fail(DGB_ERR_ARGUMENT, "null plan");
+  const int NV = p->dev.nv;
+  int rc;
+  for (int b = 0; b < p->dev.nblocks; ++b)
+    if (!p->block_set[b]) return fail(DGB_ERR_ARGUMENT, "block descriptor missing");
+  for (int ft = 0; ft < 2; ++ft) {
+    FaceDev& F = p->dev.face[ft];
+    if (!p->face_present[ft]) continue;
+    const size_t n = F.F, nq = F.nq;
+    if ((rc = alloc(p, n * 2 * nq * NV, &F.trA))) return rc;
+    if ((rc = alloc(p, n * 2 * nq * NV, &F.fluxI))) return rc;
+    if (p->dev.viscous) {
+      if ((rc = alloc(p, n * 2 * nq * NV, &F.trP))) return rc;
+      if ((rc = alloc(p, n * 2 * nq * 4, &F.trV))) return rc;
+      if ((rc = alloc(p, n * 2 * nq * 12, &F.trG))) return rc;
+      if ((rc = alloc(p, n * nq * 12, &F.jumpW))) return rc;
+      if ((rc = alloc(p, n * 2 * nq * 12, &F.liftF))) return rc;
+      if ((rc = alloc(p, n * nq * NV, &F.fluxV))) return rc;
+    }
+  }
+  p->npartials = 0;
+  for (int b = 0; b < p->dev.nblocks; ++b) {
+    BlockDev& B = p->dev.blk[b];
+    for (int ft = 0; ft < 2; ++ft) {
+      // every face type this block touches needs its trace table
+      (void)ft;
+    }
+    const size_t state = (size_t)B.E * B.Np * NV;
+    if ((rc = alloc(p, state, &B.Rinv))) return rc;
+    if ((rc = alloc(p, p->dev.viscous ? state : 1, &B.Rvis))) return rc;
+    if ((rc = alloc(p, state, &p->stage1[b]))) return rc;
+    if ((rc = alloc(p, state, &p->stage2[b]))) return rc;
+    int max_nq = 0;
+    for (int ft = 0; ft < 2; ++ft)
+      if (p->face_present[ft] && p->dev.face[ft].nq > max_nq) max_nq = p->dev.face[ft].nq;
+    (void)max_nq;
+    p->smem_traces[b] = sizeof(double) * (size_t)B.Np * (NV + 4);
+    p->smem_volume[b] = sizeof(double) * (size_t)VolumeSmem(B.Np, B.Nq, B.nlf, NV, p->dev.viscous).total;
+    p->smem_final[b] = sizeof(double) * (size_t)B.Np * NV * 2;
+    p->smem_pos[b] = sizeof(double) * (size_t)(B.Np + B.Np + B.Nq + B.Ns) * NV;
+    p->smem_troubled[b] = sizeof(double) * ((size_t)(B.Np + B.Np + B.Nq + B.Ns) * NV + 2 * B.Np);
+    p->rate_grid[b] = blocks_for(B.E, kThreads / 32) < 2 * 148 * 8 ? blocks_for(B.E, kThreads / 32) : 2 * 148 * 8;
+    const long nodes = (long)B.E * B.Np;
+    p->adm_grid[b] = blocks_for(nodes, kThreads) < 148 * 8 ? blocks_for(nodes, kThreads) : 148 * 8;
+    p->npartials += (p->rate_grid[b] > p->adm_grid[b] ? p->rate_grid[b] : p->adm_grid[b]);
+    if (p->smem_volume[b] > 227 * 1024 || p->smem_pos[b] > 227 * 1024)
+      return fail(DGB_ERR_UNSUPPORTED, "element too large for the shared-memory kernels");
+  }
+  {
+    void* d = nullptr;
+    CK(cudaMalloc(&d, sizeof(Partial) * (size_t)(p->npartials + 1)));
+    p->allocations.push_back(d);
+    p->partials = static_cast<Partial*>(d);
+  }
+  if ((rc = alloc(p, 1, &p->dt_scratch))) return rc;
+  p->finalized = true;
+  return DGB_OK;
+}
+
+int dgb_plan_destroy(dgb_plan* p) {
+  if (!p) return DGB_OK;
+  for (void* d : p->allocations) cudaFree(d);
+  delete p;
+  return DGB_OK;
+}
+
+int dgb_rhs(dgb_plan* p, const dgb_state* U, const dgb_state* inv_out, const dgb_state* vis_out, void* stream) {
+  int rc;
+  if ((rc = check_ready(p)) || (rc = check_state(p, U, "U"))) return rc;
+  FinalizeArgs A;
+  memset(&A, 0, sizeof(A));
+  for (int b = 0; b < DGB_MAX_BLOCKS; ++b) {
+    A.out_inv[b] = inv_out ? inv_out->block[b] : nullptr;
+    A.out_vis[b] = vis_out ? vis_out->block[b] : nullptr;
+  }
+  const StatePtrs S = to_ptrs(U);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  return p->dev.nv == 5 ? run_rhs<5>(p, S, A, st) : run_rhs<16>(p, S, A, st);
+}
+
+int dgb_rhs_profile(dgb_plan* p, const dgb_state* U, float* ms_out, void* stream) {
+  int rc;
+  if ((rc = check_ready(p)) || (rc = check_state(p, U, "U"))) return rc;
+  if (!ms_out) return fail(DGB_ERR_ARGUMENT, "ms_out is null");
+  FinalizeArgs A;
+  memset(&A, 0, sizeof(A));
+  for (int b = 0; b < DGB_MAX_BLOCKS; ++b) {
+    A.out_inv[b] = p->stage1[b];      // scratch outputs
+    A.out_vis[b] = p->stage2[b];
+  }
+  cudaEvent_t ev[DGB_RHS_STAGES + 1];
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  const StatePtrs S = to_ptrs(U);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  rc = p->dev.nv == 5 ? run_rhs<5>(p, S, A, st, ev) : run_rhs<16>(p, S, A, st, ev);
+  if (!rc) {
+    CK(cudaEventSynchronize(ev[DGB_RHS_STAGES]));
+    for (int k = 0; k < DGB_RHS_STAGES; ++k) CK(cudaEventElapsedTime(&ms_out[k], ev[k], ev[k + 1]));
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  return rc;
+}
+
+int dgb_stable_dt(dgb_plan* p, const dgb_state* U, double cfl, double* dt_out, void* stream) {
+  int rc;
+  if ((rc = check_ready(p)) || (rc = check_state(p, U, "U"))) return rc;
+  if (!dt_out) return fail(DGB_ERR_ARGUMENT, "dt_out is null");
+  const StatePtrs S = to_ptrs(U);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  return p->dev.nv == 5 ? run_stable_dt<5>(p, S, cfl, dt_out, st) : run_stable_dt<16>(p, S, cfl, dt_out, st);
+}
+
+int dgb_positivity(dgb_plan* p, const dgb_state* U, void* stream) {
+  int rc;
+  if ((rc = check_ready(p)) || (rc = check_state(p, U, "U"))) return rc;
+  const StatePtrs S = to_ptrs(U);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  return p->dev.nv == 5 ? run_positivity<5>(p, S, st) : run_positivity<16>(p, S, st);
+}
+
+int dgb_troubled(dgb_plan* p, const dgb_state* U, double* const* sensor, uint8_t* const* flags, void* stream) {
+  int rc;
+  if ((rc = check_ready(p)) || (rc = check_state(p, U, "U"))) return rc;
+  const StatePtrs S = to_ptrs(U);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  return p->dev.nv == 5 ? run_troubled<5>(p, S, sensor, flags, st) : run_troubled<16>(p, S, sensor, flags, st);
+}
+
+int dgb_admissibility(dgb_plan* p, const dgb_state* U, dgb_status* status, void* stream) {
+  int rc;
+  if ((rc = check_ready(p)) || (rc = check_state(p, U, "U"))) return rc;
+  if (!status) return fail(DGB_ERR_ARGUMENT, "status is null");
+  const StatePtrs S = to_ptrs(U);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  return p->dev.nv == 5 ? run_admissibility<5>(p, S, status, 0, st) : run_admissibility<16>(p, S, status, 0, st);
+}
+
+int dgb_ssprk3_step(dgb_plan* p, const dgb_state* U, double dt, dgb_status* status, void* stream) {
+  int rc;
+  if ((rc = check_ready(p)) || (rc = check_state(p, U, "U"))) return rc;
+  if (!status) return fail(DGB_ERR_ARGUMENT, "status is null");
+  const StatePtrs S = to_ptrs(U);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  return p->dev.nv == 5 ? run_step<5>(p, S, dt, status, st) : run_step<16>(p, S, dt, status, st);
+}
+
+}  // extern "C"

@@ -227,3 +227,105 @@ def mixed_block(jitter=0.1, seed=0):
     bcells, bphys = _boundary_cells(vol, np.arange(len(points)), tagger)
     phys = [np.ones(len(v[1]), np.int32) for v in vol]
     return MeshSource(points, vol + bcells, phys + bphys, field)
+
+
+def sphere_oh_grid(radius=0.5, box=((-4.0, 12.0), (-6.0, 6.0), (-6.0, 6.0)), cube=1.5, n=24, n_radial=20,
+                   outer=((8, 32), (12, 12), (12, 12)), clustering=1.6):
+    """Body-fitted O/H hex grid around a sphere centred at the origin.
+
+    A structured H-grid fills the box outside the cube [-cube, cube]^3 (n cells per cube
+    edge); inside, n_radial layers of an O-grid connect the cube's surface grid to the
+    sphere, each surface node moving along the straight line from its projection on the
+    sphere (layer spacing clustered toward the wall by ``clustering``).  Tags: inlet
+    (x min), outlet (x max), walls (y and z planes, slip), sphere_wall (no-slip body).
+    """
+    segs = []
+    for d in range(3):
+        lo, hi = box[d]
+        segs.append(np.concatenate([np.linspace(lo, -cube, outer[d][0] + 1),
+                                    np.linspace(-cube, cube, n + 1)[1:],
+                                    np.linspace(cube, hi, outer[d][1] + 1)[1:]]))
+    nxn, nyn, nzn = (len(s) for s in segs)
+    Z, Y, X = np.meshgrid(segs[2], segs[1], segs[0], indexing="ij")
+    points = [np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)]
+
+    def bid(i, j, k):
+        return (k * nyn + j) * nxn + i
+
+    c0 = (outer[0][0], outer[1][0], outer[2][0])
+    inside = lambda i, j, k: (c0[0] <= i < c0[0] + n) and (c0[1] <= j < c0[1] + n) and (c0[2] <= k < c0[2] + n)
+    hexes = []
+    for k in range(nzn - 1):
+        for j in range(nyn - 1):
+            for i in range(nxn - 1):
+                if inside(i, j, k):
+                    continue
+                hexes.append([bid(i, j, k), bid(i + 1, j, k), bid(i + 1, j + 1, k), bid(i, j + 1, k),
+                              bid(i, j, k + 1), bid(i + 1, j, k + 1), bid(i + 1, j + 1, k + 1), bid(i, j + 1, k + 1)])
+    # O-grid nodes: one radial line per cube-surface node
+    base = points[0]
+    line_of = {}
+    next_id = len(base)
+    extra = []
+    s = (np.arange(n_radial) / n_radial) ** clustering          # layer l fraction toward the cube
+    rng_ = range(n + 1)
+    for a in rng_:
+        for b in rng_:
+            for c in rng_:
+                if 0 < a < n and 0 < b < n and 0 < c < n:
+                    continue
+                node = bid(c0[0] + a, c0[1] + b, c0[2] + c)
+                p = base[node]
+                q = radius * p / np.linalg.norm(p)
+                ids = []
+                for l in range(n_radial):
+                    extra.append((1.0 - s[l]) * q + s[l] * p)
+                    ids.append(next_id)
+                    next_id += 1
+                ids.append(node)
+                line_of[(a, b, c)] = ids
+    points.append(np.asarray(extra))
+    points = np.concatenate(points)
+    # six cube faces: (fixed axis, value), in-plane axes
+    wall_quads = []
+    for axis in range(3):
+        for val in (0, n):
+            u_ax, v_ax = [d for d in range(3) if d != axis]
+            for u in range(n):
+                for v in range(n):
+                    def key(du, dv):
+                        idx = [0, 0, 0]
+                        idx[axis] = val
+                        idx[u_ax] = u + du
+                        idx[v_ax] = v + dv
+                        return tuple(idx)
+                    quad = [line_of[key(0, 0)], line_of[key(1, 0)], line_of[key(1, 1)], line_of[key(0, 1)]]
+                    for l in range(n_radial):
+                        cell = [quad[m][l] for m in range(4)] + [quad[m][l + 1] for m in range(4)]
+                        hexes.append(cell)
+                    wall_quads.append([quad[m][0] for m in range(4)])
+    hexes = np.asarray(hexes, np.int64)
+    # positive orientation: swap the two quads of any inverted cell
+    v = points[hexes]
+    det = np.einsum("ij,ij->i", np.cross(v[:, 1] - v[:, 0], v[:, 3] - v[:, 0]), v[:, 4] - v[:, 0])
+    flip = det < 0
+    hexes[flip] = hexes[flip][:, [4, 5, 6, 7, 0, 1, 2, 3]]
+    field = {"fluid": (1, 3), "inlet": (10, 2), "outlet": (11, 2), "walls": (12, 2), "sphere_wall": (13, 2)}
+    lo = np.asarray([b[0] for b in box])
+    hi = np.asarray([b[1] for b in box])
+    tagger = _box_tagger(points, lo, hi, [(10, 11), (12, 12), (12, 12), 13])
+    vol = [("hexahedron", hexes.astype(np.int32))]
+    bcells, bphys = _boundary_cells_fast(vol, points, tagger)
+    return MeshSource(points, vol + bcells, [np.ones(len(hexes), np.int32)] + bphys, field)
+
+
+def _boundary_cells_fast(volume_cells, points, tagger):
+    """Vectorised unpaired-face search for large hex meshes (same result as _boundary_cells)."""
+    ctype, conn = volume_cells[0]
+    faces = np.concatenate([conn[:, list(loc)] for loc in FACES[ctype]])
+    key = np.sort(faces, axis=1)
+    _, inv, counts = np.unique(key, axis=0, return_inverse=True, return_counts=True)
+    single = counts[inv.ravel()] == 1
+    bq = faces[single]
+    tags = np.asarray([tagger(q) for q in bq], np.int32)
+    return [("quad", bq.astype(np.int32))], [tags]

@@ -1,0 +1,196 @@
+"""DG spatial operators on the GPU (reference-named API).
+
+``HybridEulerOperator`` and ``HybridNavierStokesOperator`` mirror
+hybrid/spatial.py:10-249 and hybrid/navier_stokes.py:9-352 of
+superboss2300/jax-fluid-sim: ``rhs``, ``inviscid_rhs`` and ``viscous_rhs`` take
+a dict ``{element_type: (E, Np, nvars)}`` and an optional boundary descriptor
+and return a new dict.  States are float64 CUDA tensors (numpy arrays are
+copied to the device); all arithmetic runs in ``libdgb200.so``.
+"""
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _native as N
+from .plan import Plan
+from .reference import FACE_TYPE_ID, TYPE_ID
+
+
+def _stream_ptr():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class NativePlan:
+    """Owns one ``dgb_plan``: uploads the host plan tables and keeps the parameter block."""
+
+    def __init__(self, plan: Plan, solver, viscous: bool, br2: float):
+        L = N.lib()
+        self.plan = plan
+        self.nblocks = len(plan.blocks)
+        prm = N.Params()
+        prm.degree = plan.degree
+        prm.nvars = solver.layout.number_of_variables
+        prm.num_blocks = self.nblocks
+        prm.viscous = int(viscous)
+        prm.gamma, prm.gas_constant = solver.gamma, solver.gas_constant
+        prm.dynamic_viscosity, prm.thermal_conductivity = solver.dynamic_viscosity, solver.thermal_conductivity
+        prm.br2_penalty = br2
+        prm.has_boundary = 0
+        prm.pos_density_floor = prm.pos_pressure_floor = 1e-10
+        prm.pos_relative_floor = 0.05
+        prm.adm_density_floor = prm.adm_pressure_floor = 1e-7
+        prm.sensor_threshold = 5e-2
+        prm.limiter = 0
+        self.params = prm
+        handle = ctypes.c_void_p()
+        N.check(L.dgb_plan_create(ctypes.byref(prm), ctypes.byref(handle)))
+        self.handle = handle
+        keep = []
+        for b, bp in enumerate(plan.blocks):
+            arrays = dict(basis=N.as_f64(bp.ref.B), basis_grad=N.as_f64(bp.ref.dB),
+                          inv_jacobian=N.as_f64(bp.jinv), wdet=N.as_f64(bp.wdet), inv_mass=N.as_f64(bp.minv),
+                          length=N.as_f64(bp.length), face_sample_basis=N.as_f64(bp.face_sample_B),
+                          p1_projector=N.as_f64(bp.p1_projector))
+            ef = N.as_i32(bp.elem_face)
+            keep += list(arrays.values()) + [ef]
+            d = N.BlockDesc(element_type=TYPE_ID[bp.etype], num_elements=bp.E, num_nodes=bp.Np, num_qp=bp.Nq,
+                            num_local_faces=bp.nlf, elem_face=N.dptr(ef, ctypes.c_int32),
+                            num_face_samples=len(bp.face_sample_B))
+            for k, a in arrays.items():
+                setattr(d, k, N.dptr(a))
+            N.check(L.dgb_plan_set_block(handle, b, ctypes.byref(d)))
+        for ftype, fp in plan.faces.items():
+            ints = {k: N.as_i32(v) for k, v in dict(owner_block=fp.owner_block, owner_local=fp.owner_local,
+                                                      owner_code=fp.ocode, nbr_block=fp.nbr_block,
+                                                      nbr_local=fp.nbr_local, nbr_code=fp.ncode,
+                                                      tags=fp.tags).items()}
+            dbl = dict(normals=N.as_f64(fp.normals), weights=N.as_f64(fp.weights),
+                       side_inv_jacobian=N.as_f64(fp.jinv_side))
+            keep += list(ints.values()) + list(dbl.values())
+            d = N.FaceDesc(face_type=FACE_TYPE_ID[ftype], num_faces=fp.F, num_qp=fp.nq)
+            for k, a in ints.items():
+                setattr(d, k, N.dptr(a, ctypes.c_int32))
+            for k, a in dbl.items():
+                setattr(d, k, N.dptr(a))
+            N.check(L.dgb_plan_set_faces(handle, ctypes.byref(d)))
+        for (etype, ftype), (B, dB) in plan.trace.items():
+            B, dB = N.as_f64(B), N.as_f64(dB)
+            keep += [B, dB]
+            N.check(L.dgb_plan_set_trace(handle, TYPE_ID[etype], FACE_TYPE_ID[ftype], B.shape[0], B.shape[1],
+                                         B.shape[2], N.dptr(B), N.dptr(dB)))
+        N.check(L.dgb_plan_finalize(handle))
+        self._pushed = self._snapshot()
+
+    def _snapshot(self):
+        return bytes(self.params)
+
+    def sync_params(self):
+        snap = self._snapshot()
+        if snap != self._pushed:
+            N.check(N.lib().dgb_plan_update_params(self.handle, ctypes.byref(self.params)))
+            self._pushed = snap
+
+    def set_boundary(self, bc):
+        if bc is None:
+            self.params.has_boundary = 0
+        else:
+            bc.fill_params(self.params)
+        self.sync_params()
+
+    def state(self, blocks):
+        st = N.State()
+        for b, t in enumerate(blocks):
+            st.block[b] = t.data_ptr() if t is not None else None
+        return st
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None):
+                N.lib().dgb_plan_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
+class HybridEulerOperator:
+    """Anchor-form DG Euler residual (hybrid/spatial.py:10-249)."""
+
+    _viscous = False
+
+    def __init__(self, solver, br2_stabilization=None):
+        self.solver = solver
+        self.mesh = solver.mesh
+        P = solver.polynomial_degree
+        self.br2_stabilization = float((P + 1) * (P + 2) / 2 if br2_stabilization is None else br2_stabilization)
+        self.plan = Plan(self.mesh, P)
+        self.names = [b.element_type for b in self.mesh.element_blocks]
+        viscous = self._viscous and solver.dynamic_viscosity > 0.0
+        self.native = NativePlan(self.plan, solver, viscous, self.br2_stabilization)
+        self.viscous = viscous
+        self.solution_node_coordinates = {bp.etype: bp.node_xyz for bp in self.plan.blocks}
+
+    # -- state plumbing
+    def to_device(self, states):
+        out = {}
+        nv = self.solver.layout.number_of_variables
+        for k, bp in zip(self.names, self.plan.blocks):
+            t = states[k]
+            if not isinstance(t, torch.Tensor):
+                t = torch.as_tensor(np.asarray(t), device="cuda")
+            if t.device.type != "cuda":
+                t = t.cuda()
+            t = t.to(torch.float64).contiguous()
+            if tuple(t.shape) != (bp.E, bp.Np, nv):
+                raise ValueError(f"{k} state has shape {tuple(t.shape)}; expected {(bp.E, bp.Np, nv)}")
+            out[k] = t
+        return out
+
+    def _blocks(self, states):
+        return [states[k] for k in self.names]
+
+    def _run_rhs(self, states, boundary_state, want_inv, want_vis):
+        U = self.to_device(states)
+        self.native.set_boundary(boundary_state)
+        inv = {k: torch.empty_like(U[k]) for k in self.names} if want_inv else None
+        vis = {k: torch.empty_like(U[k]) for k in self.names} if want_vis else None
+        s_in = self.native.state(self._blocks(U))
+        s_inv = self.native.state(self._blocks(inv)) if inv else None
+        s_vis = self.native.state(self._blocks(vis)) if vis else None
+        N.check(N.lib().dgb_rhs(self.native.handle, ctypes.byref(s_in),
+                                ctypes.byref(s_inv) if s_inv else None,
+                                ctypes.byref(s_vis) if s_vis else None, _stream_ptr()))
+        return inv, vis
+
+    def rhs(self, states, boundary_state=None):
+        inv, _ = self._run_rhs(states, boundary_state, True, False)
+        return inv
+
+
+class HybridNavierStokesOperator(HybridEulerOperator):
+    """BR2 viscous operator on top of the Euler residual (hybrid/navier_stokes.py:9-352)."""
+
+    _viscous = True
+
+    def inviscid_rhs(self, states, boundary_state=None):
+        inv, _ = self._run_rhs(states, boundary_state, True, False)
+        return inv
+
+    def viscous_rhs(self, states, boundary_state=None):
+        if not self.viscous:
+            U = self.to_device(states)
+            return {k: torch.zeros_like(v) for k, v in U.items()}
+        _, vis = self._run_rhs(states, boundary_state, False, True)
+        return vis
+
+    def rhs(self, states, boundary_state=None):
+        if not self.viscous:
+            return self.inviscid_rhs(states, boundary_state)
+        inv, vis = self._run_rhs(states, boundary_state, True, True)
+        return {k: inv[k] + vis[k] for k in inv}
+
+
+def polynomial_br2_penalty(degree):
+    """hybrid/navier_stokes.py:350-352."""
+    return (degree + 1) * (degree + 2) / 2

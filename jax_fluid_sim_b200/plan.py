@@ -1,0 +1,250 @@
+"""Host-side construction of the device plan (all tables the kernels read).
+
+Geometry follows the reference's isoparametric, first-order mapping
+(``hybrid/geometry.py:139-362``): per element and volume point the inverse
+Jacobian and w|det J|; per element the dense inverse mass matrix with the
+sliver scale ``min(1, V/1e-4)``; per face and face point the unit normal and
+w*dA from the owner mapping; per face side the reference points (owner:
+its local-face corners, neighbour: corners matched by node id), from which a
+small set of distinct "trace codes" per element type is built.  Each code owns
+a trace matrix (basis at the side's face points) and its reference-gradient
+counterpart.  Faces are stored per face type (triangle, quad).
+"""
+
+import numpy as np
+
+from .mesh import HybridMesh
+from .reference import CORNERS, FACE_TYPE_ID, LOCAL_FACES, TYPE_ID, RefElement, face_quadrature
+
+FACE_TYPES = ("triangle", "quad")
+
+
+def _p1_jacobian(etype, xyz, points):
+    """J[..., d, r] = sum_k x_k[d] dN_k/dxi_r at reference points (first-order geometry)."""
+    g = RefElement(etype, 1).basis_gradients(points)          # (..., 8, 3)
+    return np.einsum("...kd,...kr->...dr", xyz, g)
+
+
+class ElementPlan:
+    pass
+
+
+class FacePlan:
+    pass
+
+
+class Plan:
+    """All numpy arrays for one mesh at one polynomial degree."""
+
+    def __init__(self, mesh: HybridMesh, degree: int):
+        self.mesh, self.degree = mesh, degree
+        self.blocks = [self._element_plan(b, k) for k, b in enumerate(mesh.element_blocks)]
+        self.codes = {}          # (etype, ftype) -> list of reference point arrays
+        self.faces = {}
+        for ftype in FACE_TYPES:
+            if ftype in mesh.face_blocks:
+                self.faces[ftype] = self._face_plan(ftype, mesh.face_blocks[ftype])
+        self._trace_tables()
+        self._element_face_links()
+        self._lengths()
+        self._face_samples()
+
+    # ------------------------------------------------------------ elements
+    def _element_plan(self, block, k):
+        ref = RefElement(block.element_type, self.degree)
+        xyz = self.mesh.points[block.connectivity]               # (E, nc, 3)
+        J = _p1_jacobian(block.element_type, xyz[:, None, :, :], ref.points[None])    # (E, Nq, 3, 3)
+        det = np.linalg.det(J)
+        jinv = np.linalg.inv(J)                                   # [r][d] = dxi_r/dx_d
+        wdet = ref.weights[None, :] * np.abs(det)
+        vol = wdet.sum(axis=1)
+        minv = _inverse_mass(wdet, ref.B)
+        minv *= np.minimum(1.0, vol / 1.0e-4)[:, None, None]
+        p = ElementPlan()
+        p.etype, p.type_id, p.ref = block.element_type, TYPE_ID[block.element_type], ref
+        p.E, p.Np, p.Nq = len(block.connectivity), ref.np, ref.nq
+        p.nlf = len(LOCAL_FACES[block.element_type])
+        p.jinv, p.wdet, p.minv, p.volume = jinv, wdet, minv, vol
+        p.node_xyz = np.einsum("qi,eid->eqd", RefElement(block.element_type, 1).basis(ref.nodes), xyz)
+        p.affine = bool(np.all(np.ptp(det, axis=1) <= 1e-13 * np.abs(det).max(axis=1)))
+        return p
+
+    # ------------------------------------------------------------ faces
+    def _code(self, etype, ftype, pts):
+        lst = self.codes.setdefault((etype, ftype), [])
+        for c, q in enumerate(lst):
+            if q.shape == pts.shape and np.array_equal(q, pts):
+                return c
+        lst.append(pts)
+        return len(lst) - 1
+
+    def _face_plan(self, ftype, fb):
+        mesh = self.mesh
+        shapes, nweights = face_quadrature(ftype, self.degree)
+        F, nq = len(fb.nodes), len(shapes)
+        canon = mesh.canon
+        fp = FacePlan()
+        fp.ftype, fp.F, fp.nq = ftype, F, nq
+        fp.owner_block, fp.owner_local = fb.owner_block.copy(), fb.owner_local.copy()
+        fp.nbr_block, fp.nbr_local = fb.neighbor_block.copy(), fb.neighbor_local.copy()
+        fp.tags = fb.boundary_tags.copy()
+        own_pts = np.empty((F, nq, 3))
+        nbr_pts = np.full((F, nq, 3), np.nan)
+        ocode = np.empty(F, np.int32)
+        ncode = np.full(F, -1, np.int32)
+        tu_ref = np.empty((F, nq, 3))
+        tv_ref = np.empty((F, nq, 3))
+        # owner side: one point set per (owner type, local face)
+        for b, block in enumerate(mesh.element_blocks):
+            for lf, loc in enumerate(LOCAL_FACES[block.element_type]):
+                sel = np.flatnonzero((fb.owner_block == b) & (fb.owner_face == lf))
+                if not len(sel):
+                    continue
+                corners = CORNERS[block.element_type][list(loc)]
+                pts = shapes @ corners
+                own_pts[sel] = pts
+                ocode[sel] = self._code(block.element_type, ftype, pts)
+                if ftype == "triangle":
+                    tu = np.broadcast_to(corners[1] - corners[0], pts.shape)
+                    tv = np.broadcast_to(corners[2] - corners[0], pts.shape)
+                else:
+                    u = shapes[:, 1] + shapes[:, 2]
+                    v = shapes[:, 2] + shapes[:, 3]
+                    c0, c1, c2, c3 = corners
+                    tu = -(1 - v)[:, None] * c0 + (1 - v)[:, None] * c1 + v[:, None] * c2 - v[:, None] * c3
+                    tv = -(1 - u)[:, None] * c0 - u[:, None] * c1 + u[:, None] * c2 + (1 - u)[:, None] * c3
+                tu_ref[sel], tv_ref[sel] = tu, tv
+        # neighbour side: corners matched by canonical node id (geometry.py:205-224)
+        internal = np.flatnonzero(fb.neighbor_block >= 0)
+        if len(internal):
+            k = fb.nodes.shape[1]
+            onodes = canon[fb.nodes[internal]]
+            nnodes = canon[fb.neighbor_nodes[internal]]
+            perm = np.argmax(onodes[:, :, None] == nnodes[:, None, :], axis=2)   # owner corner j -> nbr corner perm[j]
+            keys = np.concatenate([fb.neighbor_block[internal][:, None], fb.neighbor_face[internal][:, None],
+                                   perm], axis=1)
+            uniq, inverse = np.unique(keys, axis=0, return_inverse=True)
+            inverse = inverse.ravel()
+            for u, (b, lf, *pm) in enumerate(uniq.tolist()):
+                etype = mesh.element_blocks[b].element_type
+                corners = CORNERS[etype][list(LOCAL_FACES[etype][lf])][list(pm)]
+                pts = shapes @ corners
+                faces = internal[inverse == u]
+                nbr_pts[faces] = pts
+                ncode[faces] = self._code(etype, ftype, pts)
+        fp.own_pts, fp.nbr_pts, fp.ocode, fp.ncode = own_pts, nbr_pts, ocode, ncode
+        # metrics from the owner mapping (geometry.py:299-353)
+        normals = np.empty((F, nq, 3))
+        weights = np.empty((F, nq))
+        jinv_side = np.zeros((F, 2, nq, 3, 3))
+        measure = 0.5 if ftype == "triangle" else 1.0
+        for b, block in enumerate(mesh.element_blocks):
+            sel = np.flatnonzero(fb.owner_block == b)
+            if len(sel):
+                xyz = mesh.points[block.connectivity[fb.owner_local[sel]]]
+                J = _p1_jacobian(block.element_type, xyz[:, None], own_pts[sel])
+                tu = np.einsum("fqdr,fqr->fqd", J, tu_ref[sel])
+                tv = np.einsum("fqdr,fqr->fqd", J, tv_ref[sel])
+                area = np.cross(tu, tv)
+                sign = np.where(np.sum(area * fb.normals[sel][:, None, :], axis=-1) >= 0, 1.0, -1.0)
+                area = area * sign[..., None]
+                mag = np.linalg.norm(area, axis=-1)
+                normals[sel] = area / mag[..., None]
+                weights[sel] = nweights[None, :] * measure * mag
+                jinv_side[sel, 0] = np.linalg.inv(J)
+            seln = np.flatnonzero(fb.neighbor_block == b)
+            if len(seln):
+                xyz = mesh.points[block.connectivity[fb.neighbor_local[seln]]]
+                J = _p1_jacobian(block.element_type, xyz[:, None], nbr_pts[seln])
+                jinv_side[seln, 1] = np.linalg.inv(J)
+        fp.normals, fp.weights, fp.jinv_side = normals, weights, jinv_side
+        return fp
+
+    def _trace_tables(self):
+        """Per (element type, face type): basis and reference gradients at each code's points,
+        with entries of nodes off the face set to exactly zero."""
+        self.trace = {}
+        for (etype, ftype), pts_list in self.codes.items():
+            ref = RefElement(etype, self.degree)
+            B = np.stack([ref.basis(p) for p in pts_list])                  # (C, nq, Np)
+            dB = np.stack([ref.basis_gradients(p) for p in pts_list])       # (C, nq, Np, 3)
+            for c, p in enumerate(pts_list):
+                on_face = _nodes_on_plane(ref.nodes, p)
+                B[c][:, ~on_face] = 0.0
+            self.trace[(etype, ftype)] = (B, dB)
+
+    def _element_face_links(self):
+        """elem_face[e][lf] = (face type << 30) | (face index << 1) | side."""
+        for bp in self.blocks:
+            bp.elem_face = np.full((bp.E, bp.nlf), -1, np.int64)
+        for ftype, fp in self.faces.items():
+            ft = FACE_TYPE_ID[ftype]
+            fb = self.mesh.face_blocks[ftype]
+            f = np.arange(fp.F)
+            for side, blk, loc, lf in ((0, fb.owner_block, fb.owner_local, fb.owner_face),
+                                       (1, fb.neighbor_block, fb.neighbor_local, fb.neighbor_face)):
+                for b, bp in enumerate(self.blocks):
+                    sel = np.flatnonzero(blk == b)
+                    bp.elem_face[loc[sel], lf[sel]] = (ft << 30) | (f[sel] << 1) | side
+        for bp in self.blocks:
+            if np.any(bp.elem_face < 0):
+                raise ValueError("element face without a face record")
+            bp.elem_face = bp.elem_face.astype(np.int32)
+
+    def _lengths(self):
+        """time_integration.py:49-91: h = max(2V / sum of face areas, V^(1/3) / (4 (P+1)))."""
+        sums = [np.zeros(bp.E) for bp in self.blocks]
+        for ftype, fp in self.faces.items():
+            area = fp.weights.sum(axis=1)
+            for b in range(len(self.blocks)):
+                o = np.flatnonzero(fp.owner_block == b)
+                np.add.at(sums[b], fp.owner_local[o], area[o])
+                n = np.flatnonzero(fp.nbr_block == b)
+                np.add.at(sums[b], fp.nbr_local[n], area[n])
+        for b, bp in enumerate(self.blocks):
+            bp.length = np.maximum(2.0 * bp.volume / sums[b], 0.25 * bp.volume ** (1.0 / 3.0) / (self.degree + 1))
+
+    def _face_samples(self):
+        """Distinct face points per element type for the positivity limiter (limiter.py:28-67).
+
+        Every face point of an element type is a point of one of its trace codes, so the
+        distinct points are taken over the codes instead of over all faces."""
+        for bp in self.blocks:
+            chunks = [p for (etype, _), plist in self.codes.items() if etype == bp.etype for p in plist]
+            uniq = np.unique(np.round(np.concatenate(chunks), decimals=12), axis=0)
+            bp.face_sample_B = bp.ref.basis(uniq)
+            p1 = RefElement(bp.etype, 1).basis(bp.ref.nodes)
+            bp.p1_projector = p1 @ np.linalg.pinv(p1) if self.degree >= 2 else np.zeros((bp.Np, bp.Np))
+
+
+def _inverse_mass(wdet, B, chunk=8192):
+    """Per-element inverse of M_e = B^T diag(w|J|) B (hybrid/geometry.py:181-188).
+
+    Float64 throughout; large meshes are inverted in chunks on the GPU (torch.linalg,
+    set-up only) when one is present, else with numpy."""
+    E = wdet.shape[0]
+    out = np.empty((E, B.shape[1], B.shape[1]))
+    try:
+        import torch
+        use_gpu = torch.cuda.is_available() and E > 4096
+    except Exception:
+        use_gpu = False
+    if use_gpu:
+        Bt = torch.as_tensor(B, device="cuda")
+        for s in range(0, E, chunk):
+            w = torch.as_tensor(wdet[s:s + chunk], device="cuda")
+            M = torch.einsum("eq,qi,qj->eij", w, Bt, Bt)
+            out[s:s + chunk] = torch.linalg.inv(M).cpu().numpy()
+        return out
+    for s in range(0, E, chunk):
+        M = np.einsum("eq,qi,qj->eij", wdet[s:s + chunk], B, B, optimize=True)
+        out[s:s + chunk] = np.linalg.inv(M)
+    return out
+
+
+def _nodes_on_plane(nodes, pts):
+    """Nodes lying on the plane through the face points (all points share one face)."""
+    c = pts.mean(axis=0)
+    u, s, vt = np.linalg.svd(pts - c)
+    normal = vt[-1]
+    return np.abs((nodes - c) @ normal) < 1e-9
