@@ -89,6 +89,8 @@ def workload(scale="full"):
     from jax_fluid_sim_b200 import meshgen
     if scale == "full":
         return meshgen.sphere_oh_grid()
+    if scale == "medium":
+        return meshgen.sphere_oh_grid(n=16, n_radial=10, outer=((4, 16), (6, 6), (6, 6)))
     if scale == "small":
         return meshgen.sphere_oh_grid(n=8, n_radial=6, outer=((3, 10), (4, 4), (4, 4)))
     return meshgen.sphere_oh_grid(n=4, n_radial=2, outer=((1, 3), (1, 1), (1, 1)))
@@ -320,7 +322,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--degree", type=int, default=3)
-    ap.add_argument("--scale", default="full", choices=["full", "small", "tiny"])
+    ap.add_argument("--scale", default="full", choices=["full", "medium", "small", "tiny"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -70,7 +70,8 @@ typedef struct {
   const double* basis_grad;   /* [Nq][Np][3]   reference gradients              */
   const double* inv_jacobian; /* [E][Nq][3][3] dxi_r/dx_d                       */
   const double* wdet;         /* [E][Nq]       w |det J|                        */
-  const double* inv_mass;     /* [E][Np][Np]   sliver-scaled inverse mass       */
+  const double* inv_mass;     /* [E][Np][Np]   sliver-scaled inverse mass; stored transposed
+                                 ([E][j][i] = M^-1[i][j]) when dgb_plan_set_hex is used */
   const int32_t* elem_face;   /* [E][nlf]      (face type<<30)|(face<<1)|side   */
   const double* length;       /* [E]           characteristic length (CFL)      */
   int num_face_samples;
@@ -114,6 +115,16 @@ int dgb_plan_set_faces(dgb_plan* plan, const dgb_face_desc* desc);
  * at each code's reference face points. */
 int dgb_plan_set_trace(dgb_plan* plan, int element_type, int face_type, int num_codes, int num_qp,
                        int num_nodes, const double* basis, const double* basis_grad);
+/* Optional sum-factorised path for a mesh of one hexahedron block (hexahedron bases are
+ * tensor products of the 1-D Lagrange basis on the nodes 0, 1, interior: hybrid/elements.py:
+ * 199-274, 325-456).  line_tables: 136 doubles, in order bq[5][4], dq[5][4] (1-D basis and
+ * derivative at the volume Gauss points), bqT[4][5], dqT[4][5] (transposes), bf[4][4], df[4][4]
+ * (at the face Gauss points), bfT[4][4], d0[4], d1[4] (derivatives at 0 and 1), each block
+ * using its leading (points x nodes) entries; lex2node: 64 ints mapping lexicographic
+ * (x fastest) node positions to element node indices; perm: [codes][face_points] map from the
+ * owner's face-point order to the side element's canonical face grid. */
+int dgb_plan_set_hex(dgb_plan* plan, const double* line_tables, const int32_t* lex2node, int num_codes,
+                     int face_points, const uint8_t* perm);
 int dgb_plan_finalize(dgb_plan* plan);
 int dgb_plan_destroy(dgb_plan* plan);
 /* Replace the physics/boundary/limiter constants of a finalized plan (same mesh and degree);

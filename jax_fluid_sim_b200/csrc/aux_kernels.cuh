@@ -123,14 +123,19 @@ __global__ void __launch_bounds__(kThreads) k_positivity(const DevPlan P, const 
     }
     return __syncthreads_and(ok);
   };
-  double lo = 0.0, hi = upper;
-  for (int it = 0; it < 30; ++it) {
-    const double mid = 0.5 * (lo + hi);
-    const bool ok = pressure_ok(mid);
-    lo = ok ? mid : lo;
-    hi = ok ? hi : mid;
+  // theta = upper when the pressure is admissible there; only otherwise is the reference's
+  // 30-step bisection result used, so it is computed only in that case (same theta)
+  double theta = upper;
+  if (!pressure_ok(upper)) {
+    double lo = 0.0, hi = upper;
+    for (int it = 0; it < 30; ++it) {
+      const double mid = 0.5 * (lo + hi);
+      const bool ok = pressure_ok(mid);
+      lo = ok ? mid : lo;
+      hi = ok ? hi : mid;
+    }
+    theta = lo;
   }
-  const double theta = pressure_ok(upper) ? upper : lo;
   for (int idx = threadIdx.x; idx < Np * NV; idx += blockDim.x) {
     const int v = idx % NV;
     Ug[idx] = mean[v] + theta * (U[idx] - mean[v]);

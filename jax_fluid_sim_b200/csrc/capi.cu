@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "aux_kernels.cuh"
+#include "hex_kernels.cuh"
 
 using namespace dgb;
 
@@ -47,6 +48,11 @@ struct dgb_plan {
   double* dt_scratch = nullptr;
   size_t smem_traces[DGB_MAX_BLOCKS], smem_volume[DGB_MAX_BLOCKS], smem_final[DGB_MAX_BLOCKS];
   size_t smem_pos[DGB_MAX_BLOCKS], smem_troubled[DGB_MAX_BLOCKS];
+  // sum-factorised hexahedron path (single hexahedron block)
+  bool hex = false;
+  HexTables hex_tables;
+  HexCodes hex_codes = {nullptr, nullptr};
+  double* hex_lift = nullptr;     // [E][12][N3] nodal BR2 lift scratch
 };
 
 namespace {
@@ -91,11 +97,52 @@ int prepare(K kernel, size_t smem) {
 int blocks_for(long n, int per) { return (int)((n + per - 1) / per); }
 
 // ------------------------------------------------------------------ RHS pipeline
+template <int P, int NV, bool SPLIT>
+int run_rhs_hex(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStream_t st, cudaEvent_t* ev) {
+  using L = HexSmem<P, NV>;
+  const DevPlan& D = p->dev;
+  const int E = D.blk[0].E;
+  const size_t sm_tr = sizeof(double) * (size_t)L::TRACES, sm_li = sizeof(double) * (size_t)L::LIFT;
+  const size_t sm_vo = sizeof(double) * (size_t)L::template VOLUME<SPLIT>, sm_fi = sizeof(double) * (size_t)L::FINAL;
+  int rc;
+  if (ev) CK(cudaEventRecord(ev[0], st));
+  if ((rc = prepare(k_hex_traces<P, NV>, sm_tr))) return rc;
+  k_hex_traces<P, NV><<<E, kThreads, sm_tr, st>>>(D, S, 0, p->hex_tables, p->hex_codes);
+  if (ev) CK(cudaEventRecord(ev[1], st));
+  k_face_flux<NV><<<blocks_for((long)D.face[1].F * D.face[1].nq, kThreads), kThreads, 0, st>>>(D, S, 1);
+  if (ev) CK(cudaEventRecord(ev[2], st));
+  if (D.viscous) {
+    if ((rc = prepare(k_hex_lift<P, NV>, sm_li))) return rc;
+    k_hex_lift<P, NV><<<E, kThreads, sm_li, st>>>(D, 0, p->hex_tables, p->hex_codes, p->hex_lift);
+  }
+  if ((rc = prepare(k_hex_volume<P, NV, SPLIT>, sm_vo))) return rc;
+  k_hex_volume<P, NV, SPLIT><<<E, kThreads, sm_vo, st>>>(D, S, 0, p->hex_tables, p->hex_lift);
+  if (ev) CK(cudaEventRecord(ev[3], st));
+  if (D.viscous)
+    k_face_visc<NV><<<blocks_for((long)D.face[1].F * D.face[1].nq, kThreads), kThreads, 0, st>>>(D, 1);
+  if (ev) CK(cudaEventRecord(ev[4], st));
+  if ((rc = prepare(k_hex_finalize<P, NV, SPLIT>, sm_fi))) return rc;
+  k_hex_finalize<P, NV, SPLIT><<<E, kThreads, sm_fi, st>>>(D, S, 0, p->hex_tables, p->hex_codes, A);
+  if (ev) CK(cudaEventRecord(ev[5], st));
+  CK(cudaGetLastError());
+  return DGB_OK;
+}
+
+template <int NV, bool SPLIT>
+int run_rhs_hex_deg(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStream_t st, cudaEvent_t* ev) {
+  switch (p->dev.degree) {
+    case 1: return run_rhs_hex<1, NV, SPLIT>(p, S, A, st, ev);
+    case 2: return run_rhs_hex<2, NV, SPLIT>(p, S, A, st, ev);
+    default: return run_rhs_hex<3, NV, SPLIT>(p, S, A, st, ev);
+  }
+}
+
 // events: optional array of DGB_RHS_STAGES + 1 events recorded around the stages
 template <int NV>
 int run_rhs(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStream_t st, cudaEvent_t* ev = nullptr) {
   const DevPlan& P = p->dev;
   int rc;
+  if (p->hex) return A.stage ? run_rhs_hex_deg<NV, false>(p, S, A, st, ev) : run_rhs_hex_deg<NV, true>(p, S, A, st, ev);
   if (ev) CK(cudaEventRecord(ev[0], st));
   for (int b = 0; b < P.nblocks; ++b) {
     if ((rc = prepare(k_traces<NV>, p->smem_traces[b]))) return rc;
@@ -125,9 +172,26 @@ int run_rhs(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStream_t
   return DGB_OK;
 }
 
+template <int P, int NV>
+int run_positivity_hex(dgb_plan* p, const StatePtrs& S, cudaStream_t st) {
+  const size_t sm = sizeof(double) * (size_t)hex_positivity_smem<P, NV>();
+  int rc;
+  if ((rc = prepare(k_hex_positivity<P, NV>, sm))) return rc;
+  k_hex_positivity<P, NV><<<p->dev.blk[0].E, kThreads, sm, st>>>(p->dev, S, 0, p->hex_tables, p->lim);
+  CK(cudaGetLastError());
+  return DGB_OK;
+}
+
 template <int NV>
 int run_positivity(dgb_plan* p, const StatePtrs& S, cudaStream_t st) {
   int rc;
+  if (p->hex) {
+    switch (p->dev.degree) {
+      case 1: return run_positivity_hex<1, NV>(p, S, st);
+      case 2: return run_positivity_hex<2, NV>(p, S, st);
+      default: return run_positivity_hex<3, NV>(p, S, st);
+    }
+  }
   for (int b = 0; b < p->dev.nblocks; ++b) {
     if ((rc = prepare(k_positivity<NV>, p->smem_pos[b]))) return rc;
     k_positivity<NV><<<p->dev.blk[b].E, kThreads, p->smem_pos[b], st>>>(p->dev, S, b, p->lim);
@@ -357,6 +421,33 @@ int dgb_plan_set_trace(dgb_plan* p, int etype, int ftype, int ncodes, int nq, in
   return DGB_OK;
 }
 
+int dgb_plan_set_hex(dgb_plan* p, const double* line_tables, const int32_t* lex2node, int num_codes, int face_points,
+                     const uint8_t* perm) {
+  if (!p || !line_tables || !lex2node || !perm) return fail(DGB_ERR_ARGUMENT, "null argument");
+  if (p->finalized) return fail(DGB_ERR_ARGUMENT, "plan already finalized");
+  if (p->dev.nblocks != 1 || !p->block_set[0] || p->dev.blk[0].type != 0)
+    return fail(DGB_ERR_UNSUPPORTED, "the sum-factorised path needs exactly one hexahedron block");
+  const int qf = p->dev.degree == 1 ? 2 : (p->dev.degree == 2 ? 3 : 4);
+  if (face_points != qf * qf) return fail(DGB_ERR_ARGUMENT, "face point count does not match the degree");
+  HexTables& t = p->hex_tables;
+  memset(&t, 0, sizeof(t));
+  const double* src = line_tables;
+  memcpy(t.bq, src, sizeof(t.bq)); src += 20;
+  memcpy(t.dq, src, sizeof(t.dq)); src += 20;
+  memcpy(t.bqT, src, sizeof(t.bqT)); src += 20;
+  memcpy(t.dqT, src, sizeof(t.dqT)); src += 20;
+  memcpy(t.bf, src, sizeof(t.bf)); src += 16;
+  memcpy(t.df, src, sizeof(t.df)); src += 16;
+  memcpy(t.bfT, src, sizeof(t.bfT)); src += 16;
+  memcpy(t.d0, src, sizeof(t.d0)); src += 4;
+  memcpy(t.d1, src, sizeof(t.d1)); src += 4;
+  for (int i = 0; i < 64; ++i) t.lex2node[i] = lex2node[i];
+  int rc;
+  if ((rc = upload(p, perm, (size_t)num_codes * face_points, &p->hex_codes.perm))) return rc;
+  p->hex = true;
+  return DGB_OK;
+}
+
 int dgb_plan_finalize(dgb_plan* p) {
   if (!p) return fail(DGB_ERR_ARGUMENT, "null plan");
   const int NV = p->dev.nv;
@@ -370,7 +461,8 @@ int dgb_plan_finalize(dgb_plan* p) {
     if ((rc = alloc(p, n * 2 * nq * NV, &F.trA))) return rc;
     if ((rc = alloc(p, n * 2 * nq * NV, &F.fluxI))) return rc;
     if (p->dev.viscous) {
-      if ((rc = alloc(p, n * 2 * nq * NV, &F.trP))) return rc;
+      if (p->hex) F.trP = F.trA;   // the sum-factorised path uses the anchor-form trace for both
+      else if ((rc = alloc(p, n * 2 * nq * NV, &F.trP))) return rc;
       if ((rc = alloc(p, n * 2 * nq * 4, &F.trV))) return rc;
       if ((rc = alloc(p, n * 2 * nq * 12, &F.trG))) return rc;
       if ((rc = alloc(p, n * nq * 12, &F.jumpW))) return rc;
@@ -413,6 +505,8 @@ int dgb_plan_finalize(dgb_plan* p) {
     p->partials = static_cast<Partial*>(d);
   }
   if ((rc = alloc(p, 1, &p->dt_scratch))) return rc;
+  if (p->hex && p->dev.viscous)
+    if ((rc = alloc(p, (size_t)p->dev.blk[0].E * 12 * p->dev.blk[0].Np, &p->hex_lift))) return rc;
   p->finalized = true;
   return DGB_OK;
 }

@@ -1,0 +1,760 @@
+// Sum-factorised hexahedron kernels (float64, P1-P3).
+//
+// The reference builds hexahedron bases as tensor products of 1-D Lagrange
+// polynomials on the nodes (0, 1, interior...) and integrates with tensor Gauss
+// rules (hybrid/elements.py:199-274, 325-456; volume rule :60-98; quad face rule
+// hybrid/geometry.py:74-87), but contracts them as dense (Nq x Np) matrices.
+// Here every contraction is applied one axis at a time:
+//   nodes -> volume points   N^3 -> N^2 Q -> N Q^2 -> Q^3  (and the transpose),
+//   face slab -> face points N^2 -> N Qf -> Qf^2           (and the transpose),
+// so a P3 element costs ~1.2k multiply-adds per field per contraction instead of
+// 8k, and a face trace touches only the (P+1)^2 nodes of its face plus, for the
+// normal derivative, one line of nodes per face node.
+//
+// Face points are produced in the element's canonical face grid (free axes in
+// increasing order, first axis fastest) and mapped to the owner's face-point order
+// through a per-trace-code permutation, so the face-point kernels and buffers are
+// shared with the generic path (dg_kernels.cuh).
+#pragma once
+#include "dg_kernels.cuh"
+
+namespace dgb {
+
+struct HexTables {
+  // volume Gauss points (Q) and face Gauss points (QF); nodes in 1-D order (0, 1, interior)
+  double bq[5 * 4], dq[5 * 4];     // [Q][N]
+  double bqT[4 * 5], dqT[4 * 5];   // [N][Q]
+  double bf[4 * 4], df[4 * 4];     // [QF][N]
+  double bfT[4 * 4];               // [N][QF]
+  double d0[4], d1[4];             // 1-D basis derivatives at xi = 0 and xi = 1
+  int lex2node[64];                // lexicographic (x fastest) -> element node index
+};
+
+struct HexCodes {
+  const uint8_t* perm;   // [codes][QF*QF]: owner face-point order -> canonical face grid index
+  const int8_t* face;    // [codes]: local face of the code
+};
+
+template <int P>
+struct HexDims {
+  static constexpr int N = P + 1;
+  static constexpr int Q = P == 1 ? 2 : (P == 2 ? 3 : 5);
+  static constexpr int QF = P == 1 ? 2 : (P == 2 ? 3 : 4);
+  static constexpr int N3 = N * N * N, Q3 = Q * Q * Q, N2 = N * N, QF2 = QF * QF;
+};
+
+// local face -> (normal axis, end) for the reference's hexahedron face list (hybrid/mesh.py:51-58)
+__device__ __forceinline__ void hex_face_axes(int lf, int& a0, int& end, int& a1, int& a2) {
+  // faces 0,1: z = 0,1; 2,4: y = 0,1; 5,3: x = 0,1
+  a0 = lf < 2 ? 2 : ((lf == 2 || lf == 4) ? 1 : 0);
+  end = (lf == 1 || lf == 3 || lf == 4) ? 1 : 0;
+  a1 = a0 == 0 ? 1 : 0;
+  a2 = a0 == 2 ? 1 : 2;
+}
+
+// lexicographic index of (axis coordinates c[3]) with x fastest
+template <int N>
+__device__ __forceinline__ int lex3(int cx, int cy, int cz) { return (cz * N + cy) * N + cx; }
+
+// stride of axis a in the lexicographic node numbering (x fastest)
+template <int N>
+__device__ __forceinline__ int axis_stride(int a) { return a == 0 ? 1 : (a == 1 ? N : N * N); }
+
+// One 1-D contraction along an axis, in pencil form: every work item (a line of IN values
+// at stride `stride` between consecutive entries) keeps its inputs and the (OUT x IN) matrix in
+// registers and produces the whole output line.  lines = number of lines; a line's first input
+// sits at in_base(line), its first output at out_base(line); outputs also at stride ostride.
+template <int IN, int OUT, bool ACC, typename InBase, typename OutBase>
+__device__ __forceinline__ void pencil(const double* in, double* out, const double* M, int lines, int istride,
+                                       int ostride, InBase in_base, OutBase out_base) {
+  double m[OUT * IN];
+#pragma unroll
+  for (int k = 0; k < OUT * IN; ++k) m[k] = M[k];
+  for (int line = threadIdx.x; line < lines; line += blockDim.x) {
+    const double* src = in + in_base(line);
+    double x[IN];
+#pragma unroll
+    for (int i = 0; i < IN; ++i) x[i] = src[i * istride];
+    double* dst = out + out_base(line);
+#pragma unroll
+    for (int o = 0; o < OUT; ++o) {
+      double s = 0.0;
+#pragma unroll
+      for (int i = 0; i < IN; ++i) s += m[o * IN + i] * x[i];
+      if (ACC) dst[o * ostride] += s; else dst[o * ostride] = s;
+    }
+  }
+}
+
+// out[c][oz][oy][ox] (+)= sum Mz[oz][iz] My[oy][iy] Mx[ox][ix] in[c][iz][iy][ix]
+template <int C, int IX, int IY, int IZ, int OX, int OY, int OZ, bool ACC>
+__device__ __forceinline__ void tensor3(const double* in, double* out, double* t1, double* t2, const double* Mx,
+                                        const double* My, const double* Mz) {
+  // x: lines (c, iz, iy), contiguous inputs; t1[c][iz][iy][ox]
+  pencil<IX, OX, false>(in, t1, Mx, C * IZ * IY, 1, 1, [](int l) { return l * IX; }, [](int l) { return l * OX; });
+  __syncthreads();
+  // y: lines (c, iz, ox), inputs at stride OX; t2[c][iz][oy][ox]
+  pencil<IY, OY, false>(t1, t2, My, C * IZ * OX, OX, OX,
+                        [](int l) { return (l / OX) * IY * OX + l % OX; },
+                        [](int l) { return (l / OX) * OY * OX + l % OX; });
+  __syncthreads();
+  // z: lines (c, oy, ox), inputs at stride OX*OY; out[c][oz][oy][ox]
+  pencil<IZ, OZ, ACC>(t2, out, Mz, C * OY * OX, OX * OY, OX * OY,
+                      [](int l) { return (l / (OX * OY)) * IZ * OX * OY + l % (OX * OY); },
+                      [](int l) { return (l / (OX * OY)) * OZ * OX * OY + l % (OX * OY); });
+  __syncthreads();
+}
+
+// 2-D: out[c][k2][k1] = sum M2[k2][j2] M1[k1][j1] in[c][j2][j1]
+template <int C, int J1, int J2, int K1, int K2>
+__device__ __forceinline__ void tensor2(const double* in, double* out, double* t, const double* M1, const double* M2) {
+  pencil<J1, K1, false>(in, t, M1, C * J2, 1, 1, [](int l) { return l * J1; }, [](int l) { return l * K1; });
+  __syncthreads();
+  pencil<J2, K2, false>(t, out, M2, C * K1, K1, K1,
+                        [](int l) { return (l / K1) * J2 * K1 + l % K1; },
+                        [](int l) { return (l / K1) * K2 * K1 + l % K1; });
+  __syncthreads();
+}
+
+// Gather the N^2 slab of face (a0, end) from lexicographic nodal data X[c][N^3] into slab[c][j2][j1].
+template <int C, int N>
+__device__ __forceinline__ void face_slab(const double* X, double* slab, int a0, int end, int a1, int a2) {
+  for (int idx = threadIdx.x; idx < C * N * N; idx += blockDim.x) {
+    const int j1 = idx % N, j2 = (idx / N) % N, c = idx / (N * N);
+    // 1-D node 0 sits at xi=0, node 1 at xi=1
+    const int l = end * axis_stride<N>(a0) + j1 * axis_stride<N>(a1) + j2 * axis_stride<N>(a2);
+    slab[idx] = X[c * N * N * N + l];
+  }
+}
+
+// --------------------------------------------------------------------------------------------
+// Shared-memory layouts (doubles) of the hex element kernels; each kernel has its own.
+constexpr int cmax(int a, int b) { return a > b ? a : b; }
+
+template <int P, int NV>
+struct HexSmem {
+  using D = HexDims<P>;
+  static constexpr int N = D::N, Q = D::Q, QF = D::QF, N2 = D::N2, N3 = D::N3, Q3 = D::Q3, QF2 = D::QF2;
+  static constexpr int T = (int)((sizeof(HexTables) + 7) / 8);
+  static constexpr int MS = N3 + 1;                 // padded row stride of the staged M^-1 (transposed)
+  // traces: U, v, then face scratch
+  static constexpr int TR_U = T, TR_V = TR_U + NV * N3, TR_W = TR_V + 4 * N3;
+  static constexpr int TRACES = TR_W + (NV + 8) * N2 + (NV + 8) * N * QF + (NV + 16) * QF2;
+  // lift: staged M^-T, b per face on its slab, b on all nodes, scratch
+  static constexpr int LI_BS = T, LI_B = LI_BS + 6 * 12 * N2, LI_W = LI_B + 12 * N3;
+  static constexpr int LIFT = LI_W + 12 * QF2 + 12 * QF * N + 12 * N2 + 12 * QF2;
+  // volume: U, v, lift nodes, then U and gradients at the points and contraction scratch
+  static constexpr int C1 = NV > 12 ? NV : 12;
+  static constexpr int VO_U = T, VO_V = VO_U + NV * N3, VO_L = VO_V + 4 * N3, VO_W = VO_L + 12 * N3;
+  static constexpr int VOL1 = NV * Q3 + 12 * Q3 + C1 * N * N * Q + C1 * N * Q * Q;
+  template <bool SPLIT>
+  static constexpr int VOL2 =
+      NV * Q3 + 12 * Q3 + (SPLIT ? 6 : 3) * NV * Q3 + NV * Q * Q * N + NV * Q * N * N + (SPLIT ? NV * N3 : 0);
+  template <bool SPLIT>
+  static constexpr int VOLUME = VO_W + cmax(VOL1, VOL2<SPLIT>);
+  // finalize: staged M^-T, residuals, face scratch
+  static constexpr int FI_R = T, FI_W = FI_R + 2 * NV * N3;
+  static constexpr int FINAL = FI_W + 2 * NV * QF2 + 2 * NV * QF * N + 2 * NV * N2;
+};
+
+template <int P>
+__device__ __forceinline__ void load_tables(const HexTables& src, HexTables* dst) {
+  const double* s = reinterpret_cast<const double*>(&src);
+  double* d = reinterpret_cast<double*>(dst);
+  for (int i = threadIdx.x; i < (int)(sizeof(HexTables) / sizeof(double)); i += blockDim.x) d[i] = s[i];
+}
+
+// Stage M^-1 of one element transposed into shared memory, in lexicographic node order:
+// Mt[lj * MS + li] = M^-1[node(li)][node(lj)].  Global reads are coalesced rows.
+template <int N3, int MS>
+__device__ __forceinline__ void stage_minv(const double* Mg, const int* lex2node, const int* node2lex, double* Mt) {
+  for (int idx = threadIdx.x; idx < N3 * N3; idx += blockDim.x) {
+    const int i = idx / N3, j = idx % N3;          // element node indices
+    Mt[node2lex[j] * MS + node2lex[i]] = Mg[idx];
+  }
+}
+
+// --------------------------------------------------------------------------------------------
+// Face traces of one hexahedron: anchor-form U, viscous variables, their raw physical
+// gradients, for each of the six faces, in the owner's face-point order.
+template <int P, int NV>
+__global__ void __launch_bounds__(kThreads) k_hex_traces(const DevPlan P_, const StatePtrs S, int b,
+                                                        const HexTables tables, const HexCodes codes) {
+  using D = HexDims<P>;
+  using L = HexSmem<P, NV>;
+  constexpr int N = D::N, QF = D::QF;
+  extern __shared__ double smem[];
+  HexTables* tb = reinterpret_cast<HexTables*>(smem);
+  double* U = smem + L::TR_U;        // [NV][N3], minus anchor
+  double* V = smem + L::TR_V;        // [4][N3]
+  double* W = smem + L::TR_W;
+  const BlockDev& B = P_.blk[b];
+  const int e = blockIdx.x;
+  load_tables<P>(tables, tb);
+  const double* Ug = S.b[b] + (size_t)e * D::N3 * NV;
+  __shared__ double anchor[NV];
+  if (threadIdx.x < NV) anchor[threadIdx.x] = Ug[threadIdx.x];
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < NV * D::N3; idx += blockDim.x) {
+    const int v = idx / D::N3, l = idx % D::N3;
+    U[idx] = Ug[tb->lex2node[l] * NV + v] - anchor[v];
+  }
+  if (P_.viscous) {
+    for (int l = threadIdx.x; l < D::N3; l += blockDim.x) {
+      const int node = tb->lex2node[l];
+      double u[NV], vv[4];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) u[v] = Ug[node * NV + v];
+      viscous_vars<NV>(P_.ph, u, vv);
+#pragma unroll
+      for (int m = 0; m < 4; ++m) V[m * D::N3 + l] = vv[m];
+    }
+  }
+  __syncthreads();
+  double* slab = W;                              // [NV+4+4][N][N]: U, v, dv/dn
+  double* tmp = slab + (NV + 8) * N * N;         // tensor2 scratch
+  double* fu = tmp + (NV + 8) * N * QF;          // [NV][QF2] U at canonical face points
+  double* fv = fu + NV * QF * QF;                // [4][QF2]
+  double* gn = fv + 4 * QF * QF;                 // [4][QF2] normal derivative
+  double* g1 = gn + 4 * QF * QF;                 // [4][QF2] derivative along a1
+  double* g2 = g1 + 4 * QF * QF;                 // [4][QF2] derivative along a2
+  const FaceDev& fd = P_.face[1];
+  for (int lf = 0; lf < 6; ++lf) {
+    int ft, f, side;
+    decode_face(B.elem_face[e * 6 + lf], ft, f, side);
+    int a0, end, a1, a2;
+    hex_face_axes(lf, a0, end, a1, a2);
+    face_slab<NV, N>(U, slab, a0, end, a1, a2);
+    if (P_.viscous) {
+      face_slab<4, N>(V, slab + NV * N * N, a0, end, a1, a2);
+      const double* dn = end ? tb->d1 : tb->d0;
+      for (int idx = threadIdx.x; idx < 4 * N * N; idx += blockDim.x) {
+        const int j1 = idx % N, j2 = (idx / N) % N, m = idx / (N * N);
+        double s = 0.0;
+#pragma unroll
+        for (int j0 = 0; j0 < N; ++j0) {
+          const int l = j0 * axis_stride<N>(a0) + j1 * axis_stride<N>(a1) + j2 * axis_stride<N>(a2);
+          s += dn[j0] * V[m * D::N3 + l];
+        }
+        slab[(NV + 4) * N * N + idx] = s;
+      }
+    }
+    __syncthreads();
+    if (P_.viscous) {
+      tensor2<NV + 8, N, N, QF, QF>(slab, fu, tmp, tb->bf, tb->bf);
+      tensor2<4, N, N, QF, QF>(slab + NV * N * N, g1, tmp, tb->df, tb->bf);
+      tensor2<4, N, N, QF, QF>(slab + NV * N * N, g2, tmp, tb->bf, tb->df);
+    } else {
+      tensor2<NV, N, N, QF, QF>(slab, fu, tmp, tb->bf, tb->bf);
+    }
+    const int tc = side == 0 ? fd.oc[f] : fd.nc[f];
+    const uint8_t* perm = codes.perm + tc * QF * QF;
+    const size_t slot = ((size_t)f * 2 + side) * (QF * QF);
+    for (int idx = threadIdx.x; idx < QF * QF * NV; idx += blockDim.x) {
+      const int q = idx / NV, v = idx % NV;
+      fd.trA[(slot + q) * NV + v] = anchor[v] + fu[v * QF * QF + perm[q]];
+    }
+    if (P_.viscous) {
+      for (int idx = threadIdx.x; idx < QF * QF * 4; idx += blockDim.x) {
+        const int q = idx / 4, m = idx % 4;
+        fd.trV[(slot + q) * 4 + m] = fv[m * QF * QF + perm[q]];
+      }
+      for (int idx = threadIdx.x; idx < QF * QF * 12; idx += blockDim.x) {
+        const int q = idx / 12, m = (idx % 12) / 3, d = idx % 3;
+        const int c = perm[q];
+        const double gnv = gn[m * QF * QF + c], g1v = g1[m * QF * QF + c], g2v = g2[m * QF * QF + c];
+        // reference gradient component along axis r: normal (a0) or tangential (a1 < a2)
+        const double gx = a0 == 0 ? gnv : g1v;
+        const double gy = a0 == 1 ? gnv : (a0 == 0 ? g1v : g2v);
+        const double gz = a0 == 2 ? gnv : g2v;
+        const double* J = fd.jinv + (slot + q) * 9;
+        fd.trG[(slot + q) * 12 + m * 3 + d] = gx * J[0 * 3 + d] + gy * J[1 * 3 + d] + gz * J[2 * 3 + d];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// --------------------------------------------------------------------------------------------
+// BR2 lifts of one hexahedron (hybrid/navier_stokes.py:138-188), with M^-1 read once:
+//   b_f  = B_f^T jumpW_f on the slab of face f (transposed face interpolation);
+//   lift = M^-1 sum_f b_f                      (= sum_f r_f, r_f = M^-1 b_f);
+//   B_f r_f = B_f M^-1[slab_f, slab_f] b_f     (b_f vanishes off its slab, B_f likewise).
+// Writes the nodal lift [12][N3] (lexicographic) and br2 * B_f r_f at each face's points.
+template <int P, int NV>
+__global__ void __launch_bounds__(kThreads) k_hex_lift(const DevPlan P_, int b, const HexTables tables,
+                                                      const HexCodes codes, double* lift_out) {
+  using D = HexDims<P>;
+  using L = HexSmem<P, NV>;
+  constexpr int N = D::N, QF = D::QF, N2 = D::N2, N3 = D::N3;
+  extern __shared__ double smem[];
+  HexTables* tb = reinterpret_cast<HexTables*>(smem);
+  double* bs = smem + L::LI_BS;         // [6][12][N2]
+  double* ball = smem + L::LI_B;        // [12][N3]
+  double* jc = smem + L::LI_W;          // [12][QF2]
+  double* tmp = jc + 12 * QF * QF;      // [12][QF][N]
+  double* rs = tmp + 12 * QF * N;       // [12][N2]
+  double* lq = rs + 12 * N2;            // [12][QF2]
+  __shared__ int node2lex[64];
+  const BlockDev& B = P_.blk[b];
+  const int e = blockIdx.x;
+  load_tables<P>(tables, tb);
+  __syncthreads();
+  for (int l = threadIdx.x; l < N3; l += blockDim.x) node2lex[tb->lex2node[l]] = l;
+  for (int idx = threadIdx.x; idx < 12 * N3; idx += blockDim.x) ball[idx] = 0.0;
+  // M^-T of this element in element node order: MT[j][i] = M^-1[i][j]
+  const double* MT = B.minv + (size_t)e * N3 * N3;
+  const FaceDev& fd = P_.face[1];
+  int fcode[6];
+  for (int lf = 0; lf < 6; ++lf) {
+    int ft, f, side;
+    decode_face(B.elem_face[e * 6 + lf], ft, f, side);
+    fcode[lf] = (f << 1) | side;
+    const int tc = side == 0 ? fd.oc[f] : fd.nc[f];
+    const uint8_t* perm = codes.perm + tc * QF * QF;
+    const double* jw = fd.jumpW + (size_t)f * QF * QF * 12;
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < QF * QF * 12; idx += blockDim.x) {
+      const int q = idx / 12, c = idx % 12;
+      jc[c * QF * QF + perm[q]] = jw[idx];
+    }
+    __syncthreads();
+    tensor2<12, QF, QF, N, N>(jc, bs + lf * 12 * N2, tmp, tb->bfT, tb->bfT);
+  }
+  // b on all nodes: faces scattered one after another in local-face order (deterministic;
+  // within one face every node appears once)
+  for (int lf = 0; lf < 6; ++lf) {
+    int a0, end, a1, a2;
+    hex_face_axes(lf, a0, end, a1, a2);
+    const int st0 = axis_stride<N>(a0), st1 = axis_stride<N>(a1), st2 = axis_stride<N>(a2);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < 12 * N2; idx += blockDim.x) {
+      const int c = idx / N2, j1 = idx % N, j2 = (idx / N) % N;
+      ball[c * N3 + end * st0 + j1 * st1 + j2 * st2] += bs[(lf * 12 + c) * N2 + j2 * N + j1];
+    }
+  }
+  __syncthreads();
+  // nodal lift = M^-1 b: a thread owns one element node i and half of the 12 components;
+  // MT rows are read coalesced across consecutive nodes
+  double* lg = lift_out + (size_t)e * 12 * N3;
+  for (int idx = threadIdx.x; idx < 2 * N3; idx += blockDim.x) {
+    const int i = idx % N3, c0 = (idx / N3) * 6;
+    double s[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll 4
+    for (int j = 0; j < N3; ++j) {
+      const double m = __ldg(MT + (size_t)j * N3 + i);
+      const int lj = node2lex[j];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) s[k] += m * ball[(c0 + k) * N3 + lj];
+    }
+    const int li = node2lex[i];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) lg[(c0 + k) * N3 + li] = s[k];
+  }
+  // per face: r_f on its slab, then br2 * B_f r_f at the face points
+  for (int lf = 0; lf < 6; ++lf) {
+    int a0, end, a1, a2;
+    hex_face_axes(lf, a0, end, a1, a2);
+    const int st0 = axis_stride<N>(a0), st1 = axis_stride<N>(a1), st2 = axis_stride<N>(a2);
+    for (int idx = threadIdx.x; idx < 2 * N2; idx += blockDim.x) {
+      const int s_i = idx % N2, c0 = (idx / N2) * 6;
+      const int ni = tb->lex2node[end * st0 + (s_i % N) * st1 + (s_i / N) * st2];
+      double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int s_j = 0; s_j < N2; ++s_j) {
+        const int nj = tb->lex2node[end * st0 + (s_j % N) * st1 + (s_j / N) * st2];
+        const double m = __ldg(MT + (size_t)nj * N3 + ni);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) acc[k] += m * bs[(lf * 12 + c0 + k) * N2 + s_j];
+      }
+#pragma unroll
+      for (int k = 0; k < 6; ++k) rs[(c0 + k) * N2 + s_i] = acc[k];
+    }
+    __syncthreads();
+    tensor2<12, N, N, QF, QF>(rs, lq, tmp, tb->bf, tb->bf);
+    const int f = fcode[lf] >> 1, side = fcode[lf] & 1;
+    const int tc = side == 0 ? fd.oc[f] : fd.nc[f];
+    const uint8_t* perm = codes.perm + tc * QF * QF;
+    const size_t slot = ((size_t)f * 2 + side) * (QF * QF);
+    for (int idx = threadIdx.x; idx < QF * QF * 12; idx += blockDim.x) {
+      const int q = idx / 12, c = idx % 12;
+      fd.liftF[(slot + q) * 12 + c] = P_.ph.br2 * lq[c * QF * QF + perm[q]];
+    }
+    __syncthreads();
+  }
+}
+
+// --------------------------------------------------------------------------------------------
+// Volume residuals of one hexahedron: U (anchor form), grad v and the lift at the volume
+// points by sum factorisation; inviscid flux minus the anchor flux and the viscous flux,
+// contracted with w J^-T and the reference gradients (transposed sum factorisation).
+// SPLIT writes inviscid and viscous residuals separately, otherwise their sum into Rinv.
+template <int P, int NV, bool SPLIT>
+__global__ void __launch_bounds__(kThreads) k_hex_volume(const DevPlan P_, const StatePtrs S, int b,
+                                                        const HexTables tables, const double* lift_in) {
+  using D = HexDims<P>;
+  using L = HexSmem<P, NV>;
+  constexpr int N = D::N, Q = D::Q, N3 = D::N3, Q3 = D::Q3;
+  extern __shared__ double smem[];
+  HexTables* tb = reinterpret_cast<HexTables*>(smem);
+  double* U = smem + L::VO_U;        // [NV][N3] minus anchor
+  double* V = smem + L::VO_V;        // [4][N3]
+  double* Lf = smem + L::VO_L;       // [12][N3]
+  double* W = smem + L::VO_W;
+  const BlockDev& B = P_.blk[b];
+  const int e = blockIdx.x;
+  load_tables<P>(tables, tb);
+  const double* Ug = S.b[b] + (size_t)e * N3 * NV;
+  __shared__ double anchor[NV];
+  if (threadIdx.x < NV) anchor[threadIdx.x] = Ug[threadIdx.x];
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
+    const int v = idx / N3, l = idx % N3;
+    U[idx] = Ug[tb->lex2node[l] * NV + v] - anchor[v];
+  }
+  const bool visc = P_.viscous;
+  if (visc) {
+    for (int l = threadIdx.x; l < N3; l += blockDim.x) {
+      const int node = tb->lex2node[l];
+      double u[NV], vv[4];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) u[v] = Ug[node * NV + v];
+      viscous_vars<NV>(P_.ph, u, vv);
+#pragma unroll
+      for (int m = 0; m < 4; ++m) V[m * N3 + l] = vv[m];
+    }
+    const double* lg = lift_in + (size_t)e * 12 * N3;
+    for (int idx = threadIdx.x; idx < 12 * N3; idx += blockDim.x) Lf[idx] = lg[idx];
+  }
+  __syncthreads();
+  double* uq = W;                      // [NV][Q3]   U - anchor at volume points
+  double* gq = uq + NV * Q3;           // [12][Q3]   gradients of v: reference (3 x 4), then physical + lift
+  double* t1 = gq + 12 * Q3;           // contraction scratch
+  double* t2 = t1 + L::C1 * N * N * Q;
+  tensor3<NV, N, N, N, Q, Q, Q, false>(U, uq, t1, t2, tb->bq, tb->bq, tb->bq);
+  const double* jinv = B.jinv + (size_t)e * Q3 * 9;
+  const double* wdet = B.wdet + (size_t)e * Q3;
+  if (visc) {
+    tensor3<4, N, N, N, Q, Q, Q, false>(V, gq + 0 * 4 * Q3, t1, t2, tb->dq, tb->bq, tb->bq);
+    tensor3<4, N, N, N, Q, Q, Q, false>(V, gq + 1 * 4 * Q3, t1, t2, tb->bq, tb->dq, tb->bq);
+    tensor3<4, N, N, N, Q, Q, Q, false>(V, gq + 2 * 4 * Q3, t1, t2, tb->bq, tb->bq, tb->dq);
+    // reference -> physical gradient, in place per point: g[m*3+d] = sum_r dv_m/dxi_r J^-1[r][d]
+    for (int q = threadIdx.x; q < Q3; q += blockDim.x) {
+      double J[9], gr[12];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) J[k] = jinv[q * 9 + k];
+#pragma unroll
+      for (int k = 0; k < 12; ++k) gr[k] = gq[k * Q3 + q];      // [r][m]
+#pragma unroll
+      for (int m = 0; m < 4; ++m)
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+          gq[(m * 3 + d) * Q3 + q] = gr[0 * 4 + m] * J[0 * 3 + d] + gr[1 * 4 + m] * J[1 * 3 + d] +
+                                     gr[2 * 4 + m] * J[2 * 3 + d];
+    }
+    __syncthreads();
+    tensor3<12, N, N, N, Q, Q, Q, true>(Lf, gq, t1, t2, tb->bq, tb->bq, tb->bq);   // + lift
+  }
+  double* Gi = t1;                     // [3][NV][Q3]
+  double* Gv = Gi + 3 * NV * Q3;       // [3][NV][Q3] (SPLIT only)
+  double Fa[3][NV];
+  {
+    const double ex[3] = {1.0, 0.0, 0.0}, ey[3] = {0.0, 1.0, 0.0}, ez[3] = {0.0, 0.0, 1.0};
+    normal_flux<NV>(P_.ph, anchor, ex, Fa[0]);
+    normal_flux<NV>(P_.ph, anchor, ey, Fa[1]);
+    normal_flux<NV>(P_.ph, anchor, ez, Fa[2]);
+  }
+  for (int q = threadIdx.x; q < Q3; q += blockDim.x) {
+    double J[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) J[k] = jinv[q * 9 + k];
+    const double wq = wdet[q];
+    double Uq[NV], F[3][NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) Uq[v] = anchor[v] + uq[v * Q3 + q];
+    {
+      const double ex[3] = {1.0, 0.0, 0.0}, ey[3] = {0.0, 1.0, 0.0}, ez[3] = {0.0, 0.0, 1.0};
+      normal_flux<NV>(P_.ph, Uq, ex, F[0]);
+      normal_flux<NV>(P_.ph, Uq, ey, F[1]);
+      normal_flux<NV>(P_.ph, Uq, ez, F[2]);
+    }
+    double Fv[3 * NV];
+#pragma unroll
+    for (int k = 0; k < 3 * NV; ++k) Fv[k] = 0.0;
+    if (visc) {
+      double grad[12];
+#pragma unroll
+      for (int k = 0; k < 12; ++k) grad[k] = gq[k * Q3 + q];
+      viscous_flux<NV>(P_.ph, Uq, grad, Fv);
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        const double gi = (J[r * 3 + 0] * (F[0][v] - Fa[0][v]) + J[r * 3 + 1] * (F[1][v] - Fa[1][v]) +
+                           J[r * 3 + 2] * (F[2][v] - Fa[2][v])) * wq;
+        const double gv = -(J[r * 3 + 0] * Fv[0 * NV + v] + J[r * 3 + 1] * Fv[1 * NV + v] +
+                            J[r * 3 + 2] * Fv[2 * NV + v]) * wq;
+        if (SPLIT) {
+          Gi[(r * NV + v) * Q3 + q] = gi;
+          Gv[(r * NV + v) * Q3 + q] = gv;
+        } else {
+          Gi[(r * NV + v) * Q3 + q] = gi + gv;
+        }
+      }
+  }
+  __syncthreads();
+  double* Ri = uq;                     // reuse: [NV][N3] (NV*N3 <= NV*Q3)
+  double* s1 = Gi + (SPLIT ? 6 : 3) * NV * Q3;
+  double* s2 = s1 + NV * Q * Q * N;
+  double* Rv = s2 + NV * Q * N * N;    // [NV][N3] (SPLIT only)
+  tensor3<NV, Q, Q, Q, N, N, N, false>(Gi + 0 * NV * Q3, Ri, s1, s2, tb->dqT, tb->bqT, tb->bqT);
+  tensor3<NV, Q, Q, Q, N, N, N, true>(Gi + 1 * NV * Q3, Ri, s1, s2, tb->bqT, tb->dqT, tb->bqT);
+  tensor3<NV, Q, Q, Q, N, N, N, true>(Gi + 2 * NV * Q3, Ri, s1, s2, tb->bqT, tb->bqT, tb->dqT);
+  if (SPLIT && visc) {
+    tensor3<NV, Q, Q, Q, N, N, N, false>(Gv + 0 * NV * Q3, Rv, s1, s2, tb->dqT, tb->bqT, tb->bqT);
+    tensor3<NV, Q, Q, Q, N, N, N, true>(Gv + 1 * NV * Q3, Rv, s1, s2, tb->bqT, tb->dqT, tb->bqT);
+    tensor3<NV, Q, Q, Q, N, N, N, true>(Gv + 2 * NV * Q3, Rv, s1, s2, tb->bqT, tb->bqT, tb->dqT);
+  }
+  // residuals stay in lexicographic [NV][N3] order for k_hex_finalize
+  double* Rig = B.Rinv + (size_t)e * N3 * NV;
+  double* Rvg = B.Rvis + (size_t)e * N3 * NV;
+  for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
+    Rig[idx] = Ri[idx];
+    if (SPLIT && visc) Rvg[idx] = Rv[idx];
+  }
+}
+
+// --------------------------------------------------------------------------------------------
+// Gather face contributions into the nodes (transposed face interpolation per face, in local
+// face order: deterministic), apply M^-1 (staged in shared memory), and write either the
+// right-hand sides or the fused SSP-RK stage.  Rinv holds the total volume residual when !SPLIT.
+template <int P, int NV, bool SPLIT>
+__global__ void __launch_bounds__(kThreads) k_hex_finalize(const DevPlan P_, const StatePtrs S, int b,
+                                                          const HexTables tables, const HexCodes codes,
+                                                          const FinalizeArgs A) {
+  using D = HexDims<P>;
+  using L = HexSmem<P, NV>;
+  constexpr int N = D::N, QF = D::QF, N3 = D::N3, MS = L::MS;
+  extern __shared__ double smem[];
+  HexTables* tb = reinterpret_cast<HexTables*>(smem);
+  double* Ri = smem + L::FI_R;                 // [NV][N3] lexicographic
+  double* Rv = Ri + NV * N3;
+  double* hc = smem + L::FI_W;                 // [2*NV][QF2] face flux at canonical points
+  double* tmp = hc + 2 * NV * QF * QF;         // [2*NV][QF][N]
+  double* hs = tmp + 2 * NV * QF * N;          // [2*NV][N][N]
+  __shared__ int node2lex[64];
+  const BlockDev& B = P_.blk[b];
+  const int e = blockIdx.x;
+  load_tables<P>(tables, tb);
+  __syncthreads();
+  for (int l = threadIdx.x; l < N3; l += blockDim.x) node2lex[tb->lex2node[l]] = l;
+  const size_t base = (size_t)e * N3 * NV;
+  const bool visc = P_.viscous;
+  for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
+    Ri[idx] = B.Rinv[base + idx];
+    Rv[idx] = (SPLIT && visc) ? B.Rvis[base + idx] : 0.0;
+  }
+  __syncthreads();
+  const double* MT = B.minv + (size_t)e * N3 * N3;   // M^-T in element node order
+  const FaceDev& fd = P_.face[1];
+  constexpr int C = SPLIT ? 2 * NV : NV;
+  for (int lf = 0; lf < 6; ++lf) {
+    int ft, f, side;
+    decode_face(B.elem_face[e * 6 + lf], ft, f, side);
+    int a0, end, a1, a2;
+    hex_face_axes(lf, a0, end, a1, a2);
+    const int tc = side == 0 ? fd.oc[f] : fd.nc[f];
+    const uint8_t* perm = codes.perm + tc * QF * QF;
+    const double* fi = fd.fluxI + ((size_t)f * 2 + side) * QF * QF * NV;
+    const double* fv = fd.fluxV + (size_t)f * QF * QF * NV;
+    const double si = side == 0 ? -1.0 : 1.0;
+    for (int idx = threadIdx.x; idx < QF * QF * NV; idx += blockDim.x) {
+      const int q = idx / NV, v = idx % NV;
+      const double hi = si * fi[idx];
+      const double hv = visc ? -si * fv[idx] : 0.0;
+      if (SPLIT) {
+        hc[v * QF * QF + perm[q]] = hi;
+        hc[(NV + v) * QF * QF + perm[q]] = hv;
+      } else {
+        hc[v * QF * QF + perm[q]] = hi + hv;
+      }
+    }
+    __syncthreads();
+    tensor2<C, QF, QF, N, N>(hc, hs, tmp, tb->bfT, tb->bfT);
+    for (int idx = threadIdx.x; idx < C * N * N; idx += blockDim.x) {
+      const int j1 = idx % N, j2 = (idx / N) % N, c = idx / (N * N);
+      const int l = end * axis_stride<N>(a0) + j1 * axis_stride<N>(a1) + j2 * axis_stride<N>(a2);
+      if (c < NV) Ri[c * N3 + l] += hs[idx];
+      else Rv[(c - NV) * N3 + l] += hs[idx];
+    }
+    __syncthreads();
+  }
+  // M^-1: out[node(li)] = sum_lj Mt[lj][li] R[lj]; a thread owns node li and a group of
+  // up to VB variables, consecutive threads take consecutive li (conflict-free staged reads)
+  constexpr int VB = NV < 8 ? NV : 8;
+  constexpr int NG = (NV + VB - 1) / VB;
+  for (int idx = threadIdx.x; idx < NG * N3; idx += blockDim.x) {
+    const int i = idx % N3, v0 = (idx / N3) * VB;      // i: element node index
+    double ri[VB], rv[VB];
+#pragma unroll
+    for (int k = 0; k < VB; ++k) ri[k] = rv[k] = 0.0;
+#pragma unroll 4
+    for (int j = 0; j < N3; ++j) {
+      const double m = __ldg(MT + (size_t)j * N3 + i);
+      const int lj = node2lex[j];
+#pragma unroll
+      for (int k = 0; k < VB; ++k) {
+        if (v0 + k < NV) {
+          ri[k] += m * Ri[(v0 + k) * N3 + lj];
+          if (SPLIT) rv[k] += m * Rv[(v0 + k) * N3 + lj];
+        }
+      }
+    }
+    const size_t ob = base + (size_t)i * NV;
+#pragma unroll
+    for (int k = 0; k < VB; ++k) {
+      const int v = v0 + k;
+      if (v >= NV) continue;
+      const size_t o = ob + v;
+      if (!A.stage) {
+        if (A.out_inv[b]) A.out_inv[b][o] = ri[k];
+        if (SPLIT && A.out_vis[b]) A.out_vis[b][o] = rv[k];
+      } else {
+        const double total = SPLIT ? ri[k] + rv[k] : ri[k];
+        const double eul = S.b[b][o] + A.dt * total;
+        if (A.euler[b]) A.euler[b][o] = eul;
+        A.dst[b][o] = A.alpha * A.base[b][o] + A.beta * eul;
+      }
+    }
+  }
+}
+
+// --------------------------------------------------------------------------------------------
+// Zhang-Shu positivity limiter for hexahedra (hybrid/limiter.py:69-147) with the samples built
+// by sum factorisation: nodes, volume points (tensor Gauss grid) and the Gauss grids of the six
+// faces -- for a hexahedron mesh these are exactly the distinct face points the reference
+// collects from its face groups.
+template <int P, int NV>
+__global__ void __launch_bounds__(kThreads) k_hex_positivity(const DevPlan P_, const StatePtrs S, int b,
+                                                            const HexTables tables, const LimiterConst Lc) {
+  using D = HexDims<P>;
+  constexpr int N = D::N, Q = D::Q, QF = D::QF, N3 = D::N3, Q3 = D::Q3, QF2 = D::QF2;
+  constexpr int NS = N3 + Q3 + 6 * QF2;             // samples per element
+  extern __shared__ double smem[];
+  HexTables* tb = reinterpret_cast<HexTables*>(smem);
+  double* U = smem + HexSmem<P, NV>::T;             // [NV][N3] lexicographic
+  double* Smp = U + NV * N3;                        // [NV][NS]
+  double* t1 = Smp + NV * NS;                       // contraction scratch
+  double* t2 = t1 + NV * N * N * Q;
+  double* slab = t2 + NV * N * Q * Q;               // [NV][N2]
+  __shared__ double mean[NV];
+  __shared__ double red[kThreads / 32];
+  __shared__ int red_nan;
+  __shared__ double sh_upper;
+  const BlockDev& B = P_.blk[b];
+  const int e = blockIdx.x;
+  load_tables<P>(tables, tb);
+  double* Ug = S.b[b] + (size_t)e * N3 * NV;
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
+    const int v = idx / N3, l = idx % N3;
+    const double x = Ug[tb->lex2node[l] * NV + v];
+    U[idx] = x;
+    Smp[v * NS + l] = x;
+  }
+  __syncthreads();
+  // volume points -> Smp[v][N3 + q]  (written through a [NV][Q3] staging in t2's tail region)
+  double* vq = slab + NV * N * N;                   // [NV][Q3]
+  tensor3<NV, N, N, N, Q, Q, Q, false>(U, vq, t1, t2, tb->bq, tb->bq, tb->bq);
+  for (int idx = threadIdx.x; idx < NV * Q3; idx += blockDim.x) {
+    const int v = idx / Q3, q = idx % Q3;
+    Smp[v * NS + N3 + q] = vq[idx];
+  }
+  for (int lf = 0; lf < 6; ++lf) {
+    int a0, end, a1, a2;
+    hex_face_axes(lf, a0, end, a1, a2);
+    __syncthreads();
+    face_slab<NV, N>(U, slab, a0, end, a1, a2);
+    __syncthreads();
+    tensor2<NV, N, N, QF, QF>(slab, t2, t1, tb->bf, tb->bf);
+    for (int idx = threadIdx.x; idx < NV * QF2; idx += blockDim.x) {
+      const int v = idx / QF2, q = idx % QF2;
+      Smp[v * NS + N3 + Q3 + lf * QF2 + q] = t2[idx];
+    }
+  }
+  if (threadIdx.x == 0) red_nan = 0;
+  __syncthreads();
+  // cell mean from the volume samples
+  const double* wdet = B.wdet + (size_t)e * Q3;
+  for (int v = threadIdx.x; v < NV; v += blockDim.x) {
+    double s = 0.0, w = 0.0;
+    for (int q = 0; q < Q3; ++q) {
+      s += vq[v * Q3 + q] * wdet[q];
+      w += wdet[q];
+    }
+    mean[v] = s / w;
+  }
+  __syncthreads();
+  double Wm[NV];
+  primitive<NV>(P_.ph, mean, Wm);
+  const double rfloor = fmax(Lc.density_floor, Lc.relative_floor * Wm[0]);
+  const double pfloor = fmax(Lc.pressure_floor, Lc.relative_floor * Wm[4]);
+  double rmin = INFINITY;
+  bool nan_seen = false;
+  for (int r = threadIdx.x; r < NS; r += blockDim.x) {
+    const double d = Smp[r];
+    nan_seen |= isnan(d);
+    rmin = fmin(rmin, d);
+  }
+  for (int o = 16; o > 0; o >>= 1) rmin = fmin(rmin, __shfl_xor_sync(0xffffffff, rmin, o));
+  if (nan_seen) atomicOr(&red_nan, 1);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = rmin;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = red[0];
+    for (int k = 1; k < kThreads / 32; ++k) m = fmin(m, red[k]);
+    if (red_nan) m = NAN;
+    const double th = (m < rfloor) ? (mean[0] - rfloor) / fmax(mean[0] - m, 1.0e-30) : 1.0;
+    sh_upper = isnan(th) ? th : fmin(fmax(th, 0.0), 1.0);
+  }
+  __syncthreads();
+  const double upper = sh_upper;
+  auto pressure_ok = [&](double theta) -> bool {
+    bool ok = true;
+    for (int r = threadIdx.x; r < NS; r += blockDim.x) {
+      double s[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) s[v] = mean[v] + theta * (Smp[v * NS + r] - mean[v]);
+      ok &= (pressure_of<NV>(P_.ph, s) >= pfloor);
+    }
+    return __syncthreads_and(ok);
+  };
+  // theta = upper when the pressure is admissible there; only otherwise is the reference's
+  // 30-step bisection result used, so it is computed only in that case (same theta)
+  double theta = upper;
+  if (!pressure_ok(upper)) {
+    double lo = 0.0, hi = upper;
+    for (int it = 0; it < 30; ++it) {
+      const double mid = 0.5 * (lo + hi);
+      const bool ok = pressure_ok(mid);
+      lo = ok ? mid : lo;
+      hi = ok ? hi : mid;
+    }
+    theta = lo;
+  }
+  for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
+    const int v = idx / N3, l = idx % N3;
+    Ug[tb->lex2node[l] * NV + v] = mean[v] + theta * (U[idx] - mean[v]);
+  }
+}
+
+template <int P, int NV>
+constexpr int hex_positivity_smem() {
+  using D = HexDims<P>;
+  constexpr int NS = D::N3 + D::Q3 + 6 * D::QF2;
+  return HexSmem<P, NV>::T + NV * D::N3 + NV * NS + NV * D::N * D::N * D::Q + NV * D::N * D::Q * D::Q +
+         NV * D::N2 + NV * D::Q3;
+}
+
+}  // namespace dgb

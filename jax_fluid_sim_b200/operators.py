@@ -14,7 +14,7 @@ import numpy as np
 import torch
 
 from . import _native as N
-from .plan import Plan
+from .plan import Plan, hex_sumfact_tables
 from .reference import FACE_TYPE_ID, TYPE_ID
 
 
@@ -25,7 +25,7 @@ def _stream_ptr():
 class NativePlan:
     """Owns one ``dgb_plan``: uploads the host plan tables and keeps the parameter block."""
 
-    def __init__(self, plan: Plan, solver, viscous: bool, br2: float):
+    def __init__(self, plan: Plan, solver, viscous: bool, br2: float, sum_factorised=None):
         L = N.lib()
         self.plan = plan
         self.nblocks = len(plan.blocks)
@@ -48,9 +48,14 @@ class NativePlan:
         N.check(L.dgb_plan_create(ctypes.byref(prm), ctypes.byref(handle)))
         self.handle = handle
         keep = []
+        single_hex = len(plan.blocks) == 1 and plan.blocks[0].etype == "hexahedron"
+        if sum_factorised is None:
+            sum_factorised = single_hex
         for b, bp in enumerate(plan.blocks):
+            # the sum-factorised kernels stream M^-1 transposed (coalesced across nodes)
+            minv = np.ascontiguousarray(np.swapaxes(bp.minv, 1, 2)) if sum_factorised else bp.minv
             arrays = dict(basis=N.as_f64(bp.ref.B), basis_grad=N.as_f64(bp.ref.dB),
-                          inv_jacobian=N.as_f64(bp.jinv), wdet=N.as_f64(bp.wdet), inv_mass=N.as_f64(bp.minv),
+                          inv_jacobian=N.as_f64(bp.jinv), wdet=N.as_f64(bp.wdet), inv_mass=N.as_f64(minv),
                           length=N.as_f64(bp.length), face_sample_basis=N.as_f64(bp.face_sample_B),
                           p1_projector=N.as_f64(bp.p1_projector))
             ef = N.as_i32(bp.elem_face)
@@ -80,6 +85,15 @@ class NativePlan:
             keep += [B, dB]
             N.check(L.dgb_plan_set_trace(handle, TYPE_ID[etype], FACE_TYPE_ID[ftype], B.shape[0], B.shape[1],
                                          B.shape[2], N.dptr(B), N.dptr(dB)))
+        if sum_factorised:
+            if not single_hex:
+                raise ValueError("the sum-factorised path needs a mesh of one hexahedron block")
+            tables, lex, perm, nfq = hex_sumfact_tables(plan)
+            tables, lex, perm = N.as_f64(tables), N.as_i32(lex), np.ascontiguousarray(perm, np.uint8)
+            keep += [tables, lex, perm]
+            N.check(L.dgb_plan_set_hex(handle, N.dptr(tables), N.dptr(lex, ctypes.c_int32), perm.shape[0], nfq,
+                                       N.dptr(perm, ctypes.c_uint8)))
+        self.sum_factorised = bool(sum_factorised)
         N.check(L.dgb_plan_finalize(handle))
         self._pushed = self._snapshot()
 
@@ -119,7 +133,7 @@ class HybridEulerOperator:
 
     _viscous = False
 
-    def __init__(self, solver, br2_stabilization=None):
+    def __init__(self, solver, br2_stabilization=None, sum_factorised=None):
         self.solver = solver
         self.mesh = solver.mesh
         P = solver.polynomial_degree
@@ -127,7 +141,7 @@ class HybridEulerOperator:
         self.plan = Plan(self.mesh, P)
         self.names = [b.element_type for b in self.mesh.element_blocks]
         viscous = self._viscous and solver.dynamic_viscosity > 0.0
-        self.native = NativePlan(self.plan, solver, viscous, self.br2_stabilization)
+        self.native = NativePlan(self.plan, solver, viscous, self.br2_stabilization, sum_factorised)
         self.viscous = viscous
         self.solution_node_coordinates = {bp.etype: bp.node_xyz for bp in self.plan.blocks}
 

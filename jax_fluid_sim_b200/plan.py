@@ -14,7 +14,7 @@ counterpart.  Faces are stored per face type (triangle, quad).
 import numpy as np
 
 from .mesh import HybridMesh
-from .reference import CORNERS, FACE_TYPE_ID, LOCAL_FACES, TYPE_ID, RefElement, face_quadrature
+from .reference import CORNERS, FACE_TYPE_ID, LOCAL_FACES, TYPE_ID, RefElement, face_quadrature, gauss01
 
 FACE_TYPES = ("triangle", "quad")
 
@@ -248,3 +248,70 @@ def _nodes_on_plane(nodes, pts):
     u, s, vt = np.linalg.svd(pts - c)
     normal = vt[-1]
     return np.abs((nodes - c) @ normal) < 1e-9
+
+
+def _lagrange_1d(nodes, x):
+    """1-D Lagrange basis on `nodes` and its derivative at points x: ([len(x)][N], [len(x)][N])."""
+    nodes, x = np.asarray(nodes, float), np.atleast_1d(np.asarray(x, float))
+    N = len(nodes)
+    L = np.ones((len(x), N))
+    dL = np.zeros((len(x), N))
+    for j in range(N):
+        for k in range(N):
+            if k == j:
+                continue
+            f = (x - nodes[k]) / (nodes[j] - nodes[k])
+            dL[:, j] = dL[:, j] * f + L[:, j] / (nodes[j] - nodes[k])
+            L[:, j] = L[:, j] * f
+    return L, dL
+
+
+def hex_sumfact_tables(plan: Plan):
+    """1-D tables, lexicographic node map and face-point permutations of the sum-factorised
+    hexahedron path (layout of dgb_plan_set_hex)."""
+    P = plan.degree
+    bp = plan.blocks[0]
+    line = {1: (0.0, 1.0), 2: (0.0, 1.0, 0.5), 3: (0.0, 1.0, 1.0 / 3.0, 2.0 / 3.0)}[P]
+    N = P + 1
+    Q = len(np.unique(bp.ref.points[:, 0]))
+    gq = bp.ref.points[:Q, 0]
+    gf, _ = gauss01({1: 2, 2: 3, 3: 4}[P])
+    QF = len(gf)
+    bq, dq = _lagrange_1d(line, gq)
+    bf, df = _lagrange_1d(line, gf)
+    _, d01 = _lagrange_1d(line, [0.0, 1.0])
+
+    def pad(a, rows, cols):
+        out = np.zeros((rows, cols))
+        out[:a.shape[0], :a.shape[1]] = a
+        return out.ravel()
+
+    # each block is stored with its real (points x nodes) shape, zero-padded to the capacity
+    def packed(a, cap):
+        out = np.zeros(cap)
+        out[:a.size] = a.ravel()
+        return out
+
+    tables = np.concatenate([packed(bq, 20), packed(dq, 20), packed(bq.T.copy(), 20), packed(dq.T.copy(), 20),
+                             packed(bf, 16), packed(df, 16), packed(bf.T.copy(), 16),
+                             packed(d01[0], 4), packed(d01[1], 4)])
+    lex = np.full(64, 0, np.int32)
+    for iz in range(N):
+        for iy in range(N):
+            for ix in range(N):
+                target = np.array([line[ix], line[iy], line[iz]])
+                node = int(np.argmin(np.abs(bp.ref.nodes - target).sum(axis=1)))
+                assert np.allclose(bp.ref.nodes[node], target)
+                lex[(iz * N + iy) * N + ix] = node
+    pts_list = plan.codes.get(("hexahedron", "quad"), [])
+    perm = np.zeros((len(pts_list), QF * QF), np.uint8)
+    for c, pts in enumerate(pts_list):
+        fixed = [a for a in range(3) if np.ptp(pts[:, a]) < 1e-12]
+        assert len(fixed) == 1
+        a0 = fixed[0]
+        a1, a2 = [a for a in range(3) if a != a0]
+        k1 = np.argmin(np.abs(pts[:, a1][:, None] - gf[None, :]), axis=1)
+        k2 = np.argmin(np.abs(pts[:, a2][:, None] - gf[None, :]), axis=1)
+        assert np.max(np.abs(gf[k1] - pts[:, a1])) < 1e-12 and np.max(np.abs(gf[k2] - pts[:, a2])) < 1e-12
+        perm[c] = k2 * QF + k1
+    return tables, lex, perm, QF * QF

@@ -25,18 +25,23 @@ def close(a, b, rtol=RTOL):
 
 
 def setup(case):
+    """case may carry a ':dense' suffix to force the generic dense path on a hexahedron mesh."""
     from jax_fluid_sim_b200 import (FarfieldWallBoundary, HybridCompressibleSolver, HybridMesh,
                                     HybridNavierStokesOperator)
-    g = load_golden(case)
+    name, _, path = case.partition(":")
+    g = load_golden(name)
     solver = HybridCompressibleSolver(HybridMesh(g["source"]), polynomial_degree=int(g["degree"]),
                                       dynamic_viscosity=float(g["mu"]))
-    op = HybridNavierStokesOperator(solver)
+    op = HybridNavierStokesOperator(solver, sum_factorised=False if path == "dense" else None)
     wt = float(g["wall_temperature"])
     bc = FarfieldWallBoundary(solver, g["farfield"], wall_temperature=None if np.isnan(wt) else wt)
     return g, solver, op, bc
 
 
-@pytest.mark.parametrize("case", GOLDEN_CASES)
+CASES = GOLDEN_CASES + ["box_p2:dense", "box_p3:dense"]
+
+
+@pytest.mark.parametrize("case", CASES)
 @pytest.mark.parametrize("label", ["smooth", "shocked"])
 def test_rhs_matches_reference(case, label):
     g, solver, op, bc = setup(case)
@@ -48,7 +53,7 @@ def test_rhs_matches_reference(case, label):
         close(vis[k], g[f"rhs_viscous_{label}_{k}"])
 
 
-@pytest.mark.parametrize("case", GOLDEN_CASES)
+@pytest.mark.parametrize("case", CASES)
 @pytest.mark.parametrize("label", ["smooth", "shocked"])
 def test_dt_limiter_flags_step(case, label):
     from jax_fluid_sim_b200 import (HybridMOODSubcellLimiter, HybridPositivityLimiter, HybridSSPRK3,
