@@ -59,7 +59,8 @@ typedef struct {
   double pos_density_floor, pos_pressure_floor, pos_relative_floor;
   double adm_density_floor, adm_pressure_floor;
   double sensor_threshold;
-  int limiter;                /* stage limiter of dgb_ssprk3_step: 0 none, 1 positivity */
+  int limiter;                /* stage limiter of dgb_ssprk3_step: 0 none, 1 positivity, 2 MOOD */
+  int reconstruction;         /* MOOD subcell faces: 0 constant, 1 tvd, 2 weno (CWENO-Z) */
 } dgb_params;
 
 /* One element block (hybrid/geometry.py:139-203 metrics, precomputed by the host). */
@@ -153,10 +154,48 @@ int dgb_troubled(dgb_plan* plan, const dgb_state* U, double* const* sensor_out,
 /* HybridSSPRK3.state_admissibility (hybrid/time_integration.py:291-312) into *status (device). */
 int dgb_admissibility(dgb_plan* plan, const dgb_state* U, dgb_status* status, void* stream);
 
-/* HybridSSPRK3.checked_step without MOOD (hybrid/time_integration.py:404-439,556-583):
- * three SSP-RK3 stages, each RHS -> blend -> positivity limiter -> admissibility, in place
- * on U; *status (device) receives valid1&valid2&valid3 and the minima over the stages. */
+/* HybridSSPRK3.checked_step (hybrid/time_integration.py:441-583), in place on U.
+ * limiter 0/1: three SSP-RK3 stages, each RHS -> blend -> positivity -> admissibility;
+ *   *status (device) receives valid1&valid2&valid3 and the minima over the stages.
+ * limiter 2 (MOOD, needs dgb_plan_enable_mood): each stage RHS (inviscid and viscous) ->
+ *   Euler candidate and unlimited blend -> troubled flags on the unlimited state -> subcell
+ *   recompute -> positivity -> blend -> positivity -> admissibility; *status receives the
+ *   last stage's admissibility, as the reference's MOOD branch returns. */
 int dgb_ssprk3_step(dgb_plan* plan, const dgb_state* U, double dt, dgb_status* status, void* stream);
+
+/* MOOD subcell finite-volume tables of one element block (hybrid/subcell.py:216-396):
+ * 64 subcells, NI internal and NB boundary subfaces of the reference subdivision. */
+typedef struct {
+  int num_subcells, num_internal, num_boundary;
+  const double* projection;       /* [E][S][Np] metric-weighted DG -> subcell means      */
+  const double* reconstruction;   /* [E][Np][S] volume-weighted least-squares inverse    */
+  const double* volumes;          /* [E][S]                                              */
+  const double* centers;          /* [E][S][3]                                           */
+  const double* internal_normals; /* [E][NI][3] owner -> neighbour                       */
+  const double* internal_areas;   /* [E][NI]                                             */
+  const double* boundary_normals; /* [E][NB][3] outward                                  */
+  const double* boundary_areas;   /* [E][NB]                                             */
+  const int32_t* internal_owner;  /* [NI] */
+  const int32_t* internal_neighbor; /* [NI] */
+  const int32_t* csr_ptr;         /* [S+1] internal subfaces of each subcell             */
+  const int32_t* csr_face;        /* [2 NI]                                              */
+  const double* boundary_basis;   /* [NB][Np] DG basis at the boundary subface centres   */
+  const int32_t* gather;          /* [NB] subcell read for a boundary subface            */
+  const int32_t* scatter;         /* [NB] subcell updated by a boundary subface, -1 none */
+} dgb_subcell_block_desc;
+
+/* MOOD tables; may be given before or after dgb_plan_finalize.  osub/nsub: [F][16] boundary
+ * subfaces of the owner and of the neighbour (matched to the owner's), -1 on boundary faces. */
+int dgb_plan_set_subcells(dgb_plan* plan, int block, const dgb_subcell_block_desc* desc);
+int dgb_plan_set_subcell_faces(dgb_plan* plan, int face_type, const int32_t* osub, const int32_t* nsub);
+int dgb_plan_enable_mood(dgb_plan* plan);
+
+/* HybridSubcellFV.recompute (hybrid/subcell.py:855-950): base state, Euler DG candidate,
+ * dt, optional additional rhs (viscous, projected onto the subcells) and troubled flags
+ * [E_b] per block (device uint8) -> out (device state).  No positivity limiting. */
+int dgb_subcell_recompute(dgb_plan* plan, const dgb_state* base, const dgb_state* candidate, double dt,
+                          const dgb_state* additional_rhs, uint8_t* const* troubled, const dgb_state* out,
+                          void* stream);
 
 /* Tracing (no reference counterpart; the reference only prints wall-clock progress,
  * run_hybrid_sphere.py:366-390): runs one dgb_rhs with CUDA events around each kernel

@@ -7,7 +7,8 @@ state layout; the arithmetic runs in hand-written sm_100a CUDA kernels in
 """
 
 from .boundary import FarfieldWallBoundary
-from .limiter import HybridMOODSubcellLimiter, HybridPositivityLimiter, HybridTroubledCellSensor
+from .limiter import (HybridMOODSubcellLimiter, HybridPositivityLimiter, HybridSubcellFV,
+                      HybridTroubledCellSensor)
 from .mesh import HybridMesh
 from .meshgen import MeshSource
 from .operators import HybridEulerOperator, HybridNavierStokesOperator, polynomial_br2_penalty
@@ -17,5 +18,5 @@ from .time_integration import HybridSSPRK3
 __all__ = [
     "CompressibleStateLayout", "FarfieldWallBoundary", "HybridCompressibleSolver", "HybridEulerOperator",
     "HybridMOODSubcellLimiter", "HybridMesh", "HybridNavierStokesOperator", "HybridPositivityLimiter",
-    "HybridSSPRK3", "HybridTroubledCellSensor", "MeshSource", "polynomial_br2_penalty",
+    "HybridSSPRK3", "HybridSubcellFV", "HybridTroubledCellSensor", "MeshSource", "polynomial_br2_penalty",
 ]

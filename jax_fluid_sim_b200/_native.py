@@ -34,6 +34,18 @@ class Params(ctypes.Structure):
         ("adm_density_floor", c_double), ("adm_pressure_floor", c_double),
         ("sensor_threshold", c_double),
         ("limiter", c_int),
+        ("reconstruction", c_int),
+    ]
+
+
+class SubcellBlockDesc(ctypes.Structure):
+    _fields_ = [
+        ("num_subcells", c_int), ("num_internal", c_int), ("num_boundary", c_int),
+        ("projection", P_double), ("reconstruction", P_double), ("volumes", P_double), ("centers", P_double),
+        ("internal_normals", P_double), ("internal_areas", P_double), ("boundary_normals", P_double),
+        ("boundary_areas", P_double), ("internal_owner", P_int32), ("internal_neighbor", P_int32),
+        ("csr_ptr", P_int32), ("csr_face", P_int32), ("boundary_basis", P_double), ("gather", P_int32),
+        ("scatter", P_int32),
     ]
 
 
@@ -92,6 +104,11 @@ def lib():
             "dgb_admissibility": [c_void_p, ctypes.POINTER(State), c_void_p, c_void_p],
             "dgb_ssprk3_step": [c_void_p, ctypes.POINTER(State), c_double, c_void_p, c_void_p],
             "dgb_rhs_profile": [c_void_p, ctypes.POINTER(State), ctypes.POINTER(ctypes.c_float), c_void_p],
+            "dgb_plan_set_subcells": [c_void_p, c_int, ctypes.POINTER(SubcellBlockDesc)],
+            "dgb_plan_set_subcell_faces": [c_void_p, c_int, P_int32, P_int32],
+            "dgb_plan_enable_mood": [c_void_p],
+            "dgb_subcell_recompute": [c_void_p, ctypes.POINTER(State), ctypes.POINTER(State), c_double,
+                                      ctypes.POINTER(State), c_void_p, ctypes.POINTER(State), c_void_p],
         }
         for name, args in sigs.items():
             fn = getattr(L, name)

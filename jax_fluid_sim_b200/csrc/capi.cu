@@ -9,6 +9,7 @@
 
 #include "aux_kernels.cuh"
 #include "hex_kernels.cuh"
+#include "mood_kernels.cuh"
 
 using namespace dgb;
 
@@ -53,6 +54,16 @@ struct dgb_plan {
   HexTables hex_tables;
   HexCodes hex_codes = {nullptr, nullptr};
   double* hex_lift = nullptr;     // [E][12][N3] nodal BR2 lift scratch
+  // MOOD subcell fallback
+  MoodDev mood;
+  bool sub_block_set[DGB_MAX_BLOCKS] = {false, false, false};
+  bool sub_face_set[2] = {false, false};
+  bool mood_ready = false;
+  uint8_t* flags[DGB_MAX_BLOCKS] = {nullptr, nullptr, nullptr};
+  double* unl[DGB_MAX_BLOCKS] = {nullptr, nullptr, nullptr};
+  double* eul[DGB_MAX_BLOCKS] = {nullptr, nullptr, nullptr};
+  double* vis[DGB_MAX_BLOCKS] = {nullptr, nullptr, nullptr};
+  double* rec[DGB_MAX_BLOCKS] = {nullptr, nullptr, nullptr};
 };
 
 namespace {
@@ -142,7 +153,8 @@ template <int NV>
 int run_rhs(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStream_t st, cudaEvent_t* ev = nullptr) {
   const DevPlan& P = p->dev;
   int rc;
-  if (p->hex) return A.stage ? run_rhs_hex_deg<NV, false>(p, S, A, st, ev) : run_rhs_hex_deg<NV, true>(p, S, A, st, ev);
+  const bool split = !A.stage || A.out_vis[0] != nullptr;
+  if (p->hex) return split ? run_rhs_hex_deg<NV, true>(p, S, A, st, ev) : run_rhs_hex_deg<NV, false>(p, S, A, st, ev);
   if (ev) CK(cudaEventRecord(ev[0], st));
   for (int b = 0; b < P.nblocks; ++b) {
     if ((rc = prepare(k_traces<NV>, p->smem_traces[b]))) return rc;
@@ -238,8 +250,94 @@ int run_troubled(dgb_plan* p, const StatePtrs& S, double* const* sensor, uint8_t
   return DGB_OK;
 }
 
+FlagPtrs flag_ptrs(uint8_t* const* f) {
+  FlagPtrs out;
+  for (int b = 0; b < DGB_MAX_BLOCKS; ++b) out.f[b] = f ? f[b] : nullptr;
+  return out;
+}
+
+// Subcell recompute of the candidate `cand` from the base `cur` (traces of `cur` must be in
+// the face buffers): writes `out`.
+template <int NV>
+int run_subcell(dgb_plan* p, const StatePtrs& cur, double* const* cand, double* const* visc, double dt,
+                const FlagPtrs& F, double* const* out, cudaStream_t st) {
+  const DevPlan& P = p->dev;
+  MoodDev M = p->mood;
+  M.recon = p->prm.reconstruction;
+  int rc;
+  for (int b = 0; b < P.nblocks; ++b) {
+    const SubcellBlockDev& C = M.blk[b];
+    const size_t sm = sizeof(double) * ((size_t)P.blk[b].Np * NV + (size_t)C.S * NV * 4 + (size_t)C.NI * NV);
+    if ((rc = prepare(k_mood_fv<NV>, sm))) return rc;
+    k_mood_fv<NV><<<P.blk[b].E, kThreads, sm, st>>>(P, M, cur, b, F);
+  }
+  for (int ft = 0; ft < 2; ++ft)
+    if (p->face_present[ft])
+      k_mood_faces<NV><<<blocks_for((long)P.face[ft].F * 32, kThreads), kThreads, 0, st>>>(P, M, cur, ft, F);
+  for (int b = 0; b < P.nblocks; ++b) {
+    const SubcellBlockDev& C = M.blk[b];
+    const size_t sm = sizeof(double) * ((size_t)C.S * NV * 2 + (size_t)P.blk[b].Np * NV);
+    if ((rc = prepare(k_mood_update<NV>, sm))) return rc;
+    k_mood_update<NV><<<P.blk[b].E, kThreads, sm, st>>>(P, M, b, F, cand[b], visc ? visc[b] : nullptr, dt, out[b]);
+  }
+  CK(cudaGetLastError());
+  return DGB_OK;
+}
+
+template <int NV>
+int run_positivity(dgb_plan* p, const StatePtrs& S, cudaStream_t st);
+template <int NV>
+int run_troubled(dgb_plan* p, const StatePtrs& S, double* const* sensor, uint8_t* const* flags, cudaStream_t st);
+template <int NV>
+int run_admissibility(dgb_plan* p, const StatePtrs& S, dgb_status* status, int combine, cudaStream_t st);
+
+// MOOD branch of checked_step (hybrid/time_integration.py:450-554)
+template <int NV>
+int run_step_mood(dgb_plan* p, const StatePtrs& U0, double dt, dgb_status* status, cudaStream_t st) {
+  const DevPlan& P = p->dev;
+  StatePtrs S1, S2, UNL, REC;
+  for (int b = 0; b < DGB_MAX_BLOCKS; ++b) {
+    S1.b[b] = p->stage1[b];
+    S2.b[b] = p->stage2[b];
+    UNL.b[b] = p->unl[b];
+    REC.b[b] = p->rec[b];
+  }
+  const double alphas[3] = {0.0, 0.75, 1.0 / 3.0};
+  const double betas[3] = {1.0, 0.25, 2.0 / 3.0};
+  const StatePtrs* cur[3] = {&U0, &S1, &S2};
+  const StatePtrs* dst[3] = {&S1, &S2, &U0};
+  const FlagPtrs F = flag_ptrs(p->flags);
+  int rc;
+  for (int s = 0; s < 3; ++s) {
+    FinalizeArgs A;
+    memset(&A, 0, sizeof(A));
+    A.stage = 1;
+    A.alpha = alphas[s];
+    A.beta = betas[s];
+    A.dt = dt;
+    for (int b = 0; b < P.nblocks; ++b) {
+      A.base[b] = U0.b[b];
+      A.dst[b] = p->unl[b];
+      A.euler[b] = p->eul[b];
+      A.out_vis[b] = p->vis[b];
+    }
+    if ((rc = run_rhs<NV>(p, *cur[s], A, st))) return rc;
+    if ((rc = run_troubled<NV>(p, UNL, nullptr, p->flags, st))) return rc;
+    if ((rc = run_subcell<NV>(p, *cur[s], p->eul, p->vis, dt, F, p->rec, st))) return rc;
+    if ((rc = run_positivity<NV>(p, REC, st))) return rc;
+    for (int b = 0; b < P.nblocks; ++b) {
+      const size_t n = (size_t)P.blk[b].E * P.blk[b].Np * NV;
+      k_blend<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(U0.b[b], p->rec[b], alphas[s], betas[s], dst[s]->b[b], n);
+    }
+    if ((rc = run_positivity<NV>(p, *dst[s], st))) return rc;
+    if ((rc = run_admissibility<NV>(p, *dst[s], status, 0, st))) return rc;
+  }
+  return DGB_OK;
+}
+
 template <int NV>
 int run_step(dgb_plan* p, const StatePtrs& U0, double dt, dgb_status* status, cudaStream_t st) {
+  if (p->prm.limiter == 2) return run_step_mood<NV>(p, U0, dt, status, st);
   const DevPlan& P = p->dev;
   StatePtrs S1, S2;
   for (int b = 0; b < DGB_MAX_BLOCKS; ++b) {
@@ -280,6 +378,49 @@ int check_state(dgb_plan* p, const dgb_state* s, const char* what) {
   for (int b = 0; b < p->dev.nblocks; ++b)
     if (!s->block[b]) return fail(DGB_ERR_ARGUMENT, std::string(what) + ": null block pointer");
   return DGB_OK;
+}
+
+}  // namespace
+
+namespace {
+template <int NV>
+int run_subcell_api(dgb_plan* p, const dgb_state* base, const dgb_state* cand, double dt, const dgb_state* arhs,
+                    uint8_t* const* troubled, const dgb_state* out, cudaStream_t st) {
+  // traces of the base state for the DG face flux (the RHS's first stage only)
+  const DevPlan& P = p->dev;
+  const StatePtrs S = to_ptrs(base);
+  int rc;
+  if (p->hex) {
+    switch (P.degree) {
+      case 1: {
+        const size_t sm = sizeof(double) * (size_t)HexSmem<1, NV>::TRACES;
+        if ((rc = prepare(k_hex_traces<1, NV>, sm))) return rc;
+        k_hex_traces<1, NV><<<P.blk[0].E, kThreads, sm, st>>>(P, S, 0, p->hex_tables, p->hex_codes);
+        break;
+      }
+      case 2: {
+        const size_t sm = sizeof(double) * (size_t)HexSmem<2, NV>::TRACES;
+        if ((rc = prepare(k_hex_traces<2, NV>, sm))) return rc;
+        k_hex_traces<2, NV><<<P.blk[0].E, kThreads, sm, st>>>(P, S, 0, p->hex_tables, p->hex_codes);
+        break;
+      }
+      default: {
+        const size_t sm = sizeof(double) * (size_t)HexSmem<3, NV>::TRACES;
+        if ((rc = prepare(k_hex_traces<3, NV>, sm))) return rc;
+        k_hex_traces<3, NV><<<P.blk[0].E, kThreads, sm, st>>>(P, S, 0, p->hex_tables, p->hex_codes);
+      }
+    }
+  } else {
+    for (int b = 0; b < P.nblocks; ++b) {
+      if ((rc = prepare(k_traces<NV>, p->smem_traces[b]))) return rc;
+      k_traces<NV><<<P.blk[b].E, kThreads, p->smem_traces[b], st>>>(P, S, b);
+    }
+  }
+  double* candp[DGB_MAX_BLOCKS] = {cand->block[0], cand->block[1], cand->block[2]};
+  double* visp[DGB_MAX_BLOCKS] = {arhs ? arhs->block[0] : nullptr, arhs ? arhs->block[1] : nullptr,
+                                  arhs ? arhs->block[2] : nullptr};
+  double* outp[DGB_MAX_BLOCKS] = {out->block[0], out->block[1], out->block[2]};
+  return run_subcell<NV>(p, S, candp, arhs ? visp : nullptr, dt, flag_ptrs(troubled), outp, st);
 }
 
 }  // namespace
@@ -532,6 +673,97 @@ int dgb_rhs(dgb_plan* p, const dgb_state* U, const dgb_state* inv_out, const dgb
   return p->dev.nv == 5 ? run_rhs<5>(p, S, A, st) : run_rhs<16>(p, S, A, st);
 }
 
+int dgb_plan_set_subcells(dgb_plan* p, int b, const dgb_subcell_block_desc* d) {
+  if (!p || !d || b < 0 || b >= p->dev.nblocks || !p->block_set[b]) return fail(DGB_ERR_ARGUMENT, "bad subcell block");
+  SubcellBlockDev& C = p->mood.blk[b];
+  const BlockDev& B = p->dev.blk[b];
+  C.S = d->num_subcells;
+  C.NI = d->num_internal;
+  C.NB = d->num_boundary;
+  if (C.S != 64) return fail(DGB_ERR_UNSUPPORTED, "subcell tables need 64 subcells (4 divisions)");
+  const size_t E = B.E, S = C.S, Np = B.Np, NI = C.NI, NB = C.NB;
+  int rc;
+  if ((rc = upload(p, d->projection, E * S * Np, &C.P))) return rc;
+  if ((rc = upload(p, d->reconstruction, E * Np * S, &C.R))) return rc;
+  if ((rc = upload(p, d->volumes, E * S, &C.vol))) return rc;
+  if ((rc = upload(p, d->centers, E * S * 3, &C.cen))) return rc;
+  if ((rc = upload(p, d->internal_normals, E * NI * 3, &C.in_n))) return rc;
+  if ((rc = upload(p, d->internal_areas, E * NI, &C.in_a))) return rc;
+  if ((rc = upload(p, d->boundary_normals, E * NB * 3, &C.bd_n))) return rc;
+  if ((rc = upload(p, d->boundary_areas, E * NB, &C.bd_a))) return rc;
+  if ((rc = upload(p, d->internal_owner, NI, &C.iown))) return rc;
+  if ((rc = upload(p, d->internal_neighbor, NI, &C.inbr))) return rc;
+  if ((rc = upload(p, d->csr_ptr, S + 1, &C.csr_ptr))) return rc;
+  if ((rc = upload(p, d->csr_face, 2 * NI, &C.csr_face))) return rc;
+  if ((rc = upload(p, d->boundary_basis, NB * Np, &C.bbasis))) return rc;
+  if ((rc = upload(p, d->gather, NB, &C.gather))) return rc;
+  if ((rc = upload(p, d->scatter, NB, &C.scatter))) return rc;
+  p->sub_block_set[b] = true;
+  return DGB_OK;
+}
+
+int dgb_plan_set_subcell_faces(dgb_plan* p, int ft, const int32_t* osub, const int32_t* nsub) {
+  if (!p || ft < 0 || ft > 1) return fail(DGB_ERR_ARGUMENT, "bad subcell face type");
+  SubcellFaceDev& SF = p->mood.face[ft];
+  const size_t F = p->dev.face[ft].F;
+  int rc;
+  if ((rc = upload(p, osub, F * kSub, &SF.osub))) return rc;
+  if ((rc = upload(p, nsub, F * kSub, &SF.nsub))) return rc;
+  p->sub_face_set[ft] = true;
+  return DGB_OK;
+}
+
+int dgb_plan_enable_mood(dgb_plan* p) {
+  if (!p || !p->finalized) return fail(DGB_ERR_ARGUMENT, "finalize the plan first");
+  if (p->mood_ready) return DGB_OK;
+  for (int b = 0; b < p->dev.nblocks; ++b)
+    if (!p->sub_block_set[b]) return fail(DGB_ERR_ARGUMENT, "subcell tables missing for a block");
+  for (int ft = 0; ft < 2; ++ft)
+    if (p->face_present[ft] && !p->sub_face_set[ft]) return fail(DGB_ERR_ARGUMENT, "subcell face tables missing");
+  const int NV = p->dev.nv;
+  int rc;
+  for (int b = 0; b < p->dev.nblocks; ++b) {
+    const size_t E = p->dev.blk[b].E, S = p->mood.blk[b].S, state = E * p->dev.blk[b].Np * NV;
+    if ((rc = alloc(p, E * S * NV, &p->mood.blk[b].ubar))) return rc;
+    if ((rc = alloc(p, E * S * NV, &p->mood.blk[b].rsub))) return rc;
+    void* f = nullptr;
+    CK(cudaMalloc(&f, E));
+    p->allocations.push_back(f);
+    CK(cudaMemset(f, 0, E));
+    p->flags[b] = static_cast<uint8_t*>(f);
+    if ((rc = alloc(p, state, &p->unl[b]))) return rc;
+    if ((rc = alloc(p, state, &p->eul[b]))) return rc;
+    if ((rc = alloc(p, state, &p->vis[b]))) return rc;
+    if ((rc = alloc(p, state, &p->rec[b]))) return rc;
+  }
+  for (int ft = 0; ft < 2; ++ft) {
+    if (!p->face_present[ft]) continue;
+    const size_t F = p->dev.face[ft].F;
+    if ((rc = alloc(p, F * kSub * NV, &p->mood.face[ft].fsub))) return rc;
+    if ((rc = alloc(p, F * NV, &p->mood.face[ft].dflux))) return rc;
+    void* a = nullptr;
+    CK(cudaMalloc(&a, F));
+    p->allocations.push_back(a);
+    CK(cudaMemset(a, 0, F));
+    p->mood.face[ft].active = static_cast<uint8_t*>(a);
+  }
+  p->mood_ready = true;
+  return DGB_OK;
+}
+
+int dgb_subcell_recompute(dgb_plan* p, const dgb_state* base, const dgb_state* cand, double dt,
+                          const dgb_state* arhs, uint8_t* const* troubled, const dgb_state* out, void* stream) {
+  int rc;
+  if ((rc = check_ready(p)) || (rc = check_state(p, base, "base")) || (rc = check_state(p, cand, "candidate")) ||
+      (rc = check_state(p, out, "out")))
+    return rc;
+  if (!p->mood_ready) return fail(DGB_ERR_ARGUMENT, "call dgb_plan_enable_mood first");
+  if (!troubled) return fail(DGB_ERR_ARGUMENT, "troubled flags are null");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  return p->dev.nv == 5 ? run_subcell_api<5>(p, base, cand, dt, arhs, troubled, out, st)
+                        : run_subcell_api<16>(p, base, cand, dt, arhs, troubled, out, st);
+}
+
 int dgb_rhs_profile(dgb_plan* p, const dgb_state* U, float* ms_out, void* stream) {
   int rc;
   if ((rc = check_ready(p)) || (rc = check_state(p, U, "U"))) return rc;
@@ -593,6 +825,7 @@ int dgb_ssprk3_step(dgb_plan* p, const dgb_state* U, double dt, dgb_status* stat
   int rc;
   if ((rc = check_ready(p)) || (rc = check_state(p, U, "U"))) return rc;
   if (!status) return fail(DGB_ERR_ARGUMENT, "status is null");
+  if (p->prm.limiter == 2 && !p->mood_ready) return fail(DGB_ERR_ARGUMENT, "MOOD limiter needs dgb_plan_enable_mood");
   const StatePtrs S = to_ptrs(U);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   return p->dev.nv == 5 ? run_step<5>(p, S, dt, status, st) : run_step<16>(p, S, dt, status, st);

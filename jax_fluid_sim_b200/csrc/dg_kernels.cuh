@@ -465,6 +465,7 @@ __global__ void __launch_bounds__(kThreads) k_finalize(const DevPlan P, const St
     } else {
       const double total = P.viscous ? ri + rv : ri;
       const double eul = S.b[b][base + idx] + A.dt * total;
+      if (A.out_vis[b]) A.out_vis[b][base + idx] = rv;
       if (A.euler[b]) A.euler[b][base + idx] = eul;
       A.dst[b][base + idx] = A.alpha * A.base[b][base + idx] + A.beta * eul;
     }

@@ -623,6 +623,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_finalize(const DevPlan P_, con
       } else {
         const double total = SPLIT ? ri[k] + rv[k] : ri[k];
         const double eul = S.b[b][o] + A.dt * total;
+        if (SPLIT && A.out_vis[b]) A.out_vis[b][o] = rv[k];
         if (A.euler[b]) A.euler[b][o] = eul;
         A.dst[b][o] = A.alpha * A.base[b][o] + A.beta * eul;
       }

@@ -64,18 +64,69 @@ class HybridTroubledCellSensor:
         return sens, {k: v > self.threshold for k, v in sens.items()}
 
 
-class HybridMOODSubcellLimiter:
-    """A-posteriori detection (troubled) of hybrid/limiter.py:267-343."""
+RECONSTRUCTIONS = {"constant": 0, "tvd": 1, "weno": 2}
 
-    def __init__(self, operator, threshold=5.0e-2, positivity=None, reconstruction="weno"):
+
+class HybridSubcellFV:
+    """Conservative subcell FV recompute (hybrid/subcell.py:442-950) on the GPU.
+
+    ``coupling="reference"`` reproduces the reference's DG-FV coupling indices exactly
+    (see jax_fluid_sim_b200/subcell.py); ``coupling="subcell"`` couples each boundary
+    subface to the subcell that owns it."""
+
+    def __init__(self, operator, division_count=4, reconstruction="weno", coupling="reference"):
+        if division_count != 4:
+            raise ValueError("P2 subcell coupling currently requires division_count=4")
+        if reconstruction not in RECONSTRUCTIONS:
+            raise ValueError(f"Unknown subcell reconstruction mode: {reconstruction!r}")
+        self.operator = operator
+        self.reconstruction = reconstruction
+        operator.native.enable_mood(coupling)
+
+    def recompute(self, states, dg_candidate, dt, troubled, boundary_state=None, additional_rhs=None):
+        op = self.operator
+        base, cand = op.to_device(states), op.to_device(dg_candidate)
+        arhs = op.to_device(additional_rhs) if additional_rhs is not None else None
+        if isinstance(dt, dict):
+            raise NotImplementedError("local time stepping is outside the CUDA path")
+        flags = {k: torch.as_tensor(troubled[k], device="cuda").to(torch.uint8).contiguous() for k in op.names}
+        op.native.params.reconstruction = RECONSTRUCTIONS[self.reconstruction]
+        op.native.set_boundary(boundary_state)
+        out = {k: torch.empty_like(v) for k, v in base.items()}
+        fp = (ctypes.c_void_p * N.MAX_BLOCKS)(*[flags[k].data_ptr() for k in op.names])
+        sb, sc, so = (op.native.state(op._blocks(x)) for x in (base, cand, out))
+        sa = op.native.state(op._blocks(arhs)) if arhs is not None else None
+        N.check(N.lib().dgb_subcell_recompute(op.native.handle, ctypes.byref(sb), ctypes.byref(sc), float(dt),
+                                              ctypes.byref(sa) if sa is not None else None, fp,
+                                              ctypes.byref(so), _stream_ptr()))
+        return out
+
+
+class HybridMOODSubcellLimiter:
+    """A-posteriori P-DG / subcell-FV recomputation (hybrid/limiter.py:267-343)."""
+
+    def __init__(self, operator, threshold=5.0e-2, positivity=None, reconstruction="weno", coupling="reference"):
         self.operator = operator
         self.sensor = HybridTroubledCellSensor(operator, threshold)
         self.positivity = HybridPositivityLimiter(operator) if positivity is None else positivity
         self.reconstruction = reconstruction
+        self.subcell = HybridSubcellFV(operator, reconstruction=reconstruction, coupling=coupling)
+
+    def configure(self, params):
+        self.positivity.configure(params)
+        params.sensor_threshold = self.sensor.threshold
+        params.reconstruction = RECONSTRUCTIONS[self.reconstruction]
 
     def troubled(self, candidate):
         _, flags = self.sensor._run(candidate, self.positivity)
         return {k: v.bool() for k, v in flags.items()}
+
+    def recompute(self, base, dg_candidate, dt, boundary_state=None, additional_rhs=None, detection_state=None,
+                  troubled_mask=None):
+        troubled = troubled_mask if troubled_mask is not None else self.troubled(
+            dg_candidate if detection_state is None else detection_state)
+        corrected = self.subcell.recompute(base, dg_candidate, dt, troubled, boundary_state, additional_rhs)
+        return self.positivity(corrected)
 
     def __call__(self, states):
         return self.positivity(states)

@@ -97,6 +97,44 @@ class NativePlan:
         N.check(L.dgb_plan_finalize(handle))
         self._pushed = self._snapshot()
 
+    def enable_mood(self, coupling="reference"):
+        """Upload the MOOD subcell tables once (hybrid/subcell.py:442-471)."""
+        if getattr(self, "mood_coupling", None) == coupling:
+            return
+        if getattr(self, "mood_coupling", None) is not None:
+            raise ValueError("the subcell coupling of a plan is fixed once chosen")
+        from .subcell import SubcellPlan
+        L = N.lib()
+        sp = SubcellPlan(self.plan.mesh, self.plan.degree, coupling)
+        keep = []
+        for b, (bp, sb) in enumerate(zip(self.plan.blocks, sp.blocks)):
+            rs = sp.refs[bp.etype]
+            gather, scatter = rs.coupling_indices(coupling)
+            dbl = dict(projection=sb.projection, reconstruction=sb.reconstruction, volumes=sb.volumes,
+                       centers=sb.centers, internal_normals=sb.internal_normals, internal_areas=sb.internal_areas,
+                       boundary_normals=sb.boundary_normals, boundary_areas=sb.boundary_areas,
+                       boundary_basis=sb.boundary_basis)
+            ints = dict(internal_owner=rs.internal_owner, internal_neighbor=rs.internal_neighbor,
+                        csr_ptr=rs.csr_ptr, csr_face=rs.csr_face, gather=gather, scatter=scatter)
+            dbl = {k: N.as_f64(v) for k, v in dbl.items()}
+            ints = {k: N.as_i32(v) for k, v in ints.items()}
+            keep += list(dbl.values()) + list(ints.values())
+            d = N.SubcellBlockDesc(num_subcells=rs.count, num_internal=len(rs.internal_faces),
+                                   num_boundary=len(rs.boundary_faces))
+            for k, a in dbl.items():
+                setattr(d, k, N.dptr(a))
+            for k, a in ints.items():
+                setattr(d, k, N.dptr(a, ctypes.c_int32))
+            N.check(L.dgb_plan_set_subcells(self.handle, b, ctypes.byref(d)))
+        for ftype, (osub, nsub) in sp.faces.items():
+            osub, nsub = N.as_i32(osub), N.as_i32(nsub)
+            keep += [osub, nsub]
+            N.check(L.dgb_plan_set_subcell_faces(self.handle, FACE_TYPE_ID[ftype], N.dptr(osub, ctypes.c_int32),
+                                                 N.dptr(nsub, ctypes.c_int32)))
+        N.check(L.dgb_plan_enable_mood(self.handle))
+        self.mood_coupling = coupling
+        self.subcell_plan = sp
+
     def _snapshot(self):
         return bytes(self.params)
 

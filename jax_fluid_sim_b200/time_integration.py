@@ -30,9 +30,7 @@ class HybridSSPRK3:
         self._status = torch.zeros(3, dtype=torch.float64, device="cuda")   # dgb_status (24 bytes)
         self._dt = torch.zeros(1, dtype=torch.float64, device="cuda")
         if limiter is not None and not isinstance(limiter, (HybridPositivityLimiter, HybridMOODSubcellLimiter)):
-            raise NotImplementedError("supported stage limiters: HybridPositivityLimiter")
-        if isinstance(limiter, HybridMOODSubcellLimiter):
-            raise NotImplementedError("MOOD subcell recompute is not part of the CUDA step yet")
+            raise NotImplementedError("supported stage limiters: HybridPositivityLimiter, HybridMOODSubcellLimiter")
 
     @property
     def characteristic_lengths(self):
@@ -43,7 +41,10 @@ class HybridSSPRK3:
         prm = native.params
         prm.adm_density_floor = self.density_floor
         prm.adm_pressure_floor = self.pressure_floor
-        if isinstance(self.limiter, HybridPositivityLimiter):
+        if isinstance(self.limiter, HybridMOODSubcellLimiter):
+            self.limiter.configure(prm)
+            prm.limiter = 2
+        elif isinstance(self.limiter, HybridPositivityLimiter):
             self.limiter.configure(prm)
             prm.limiter = 1
         else:

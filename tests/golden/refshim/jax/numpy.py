@@ -6,30 +6,80 @@ import types
 import numpy as _np
 
 
+def _normalise(index, shape):
+    """Expand an index to one entry per leading axis it addresses (Ellipsis/None not used here)."""
+    if not isinstance(index, tuple):
+        index = (index,)
+    return index
+
+
+def _clamped(index, shape):
+    """JAX gather semantics: integer-array indices out of bounds are clamped to the edge."""
+    index = _normalise(index, shape)
+    out = []
+    axis = 0
+    for item in index:
+        if item is Ellipsis:
+            out.append(item)
+            axis = len(shape) - (len(index) - len(out))
+            continue
+        if isinstance(item, _np.ndarray) and item.dtype.kind in "iu" and axis < len(shape):
+            dim = shape[axis]
+            item = _np.where(item < 0, item + dim, item)
+            item = _np.clip(item, 0, dim - 1)
+        out.append(item)
+        axis += 1
+    return tuple(out)
+
+
+def _scatter(ufunc, array, index, value):
+    """JAX scatter semantics: updates at out-of-bounds integer-array indices are dropped.
+    Implemented by padding each array-indexed axis so that such updates land outside the
+    cropped result."""
+    index = _normalise(index, array.shape)
+    pads = [0] * array.ndim
+    fixed = []
+    axis = 0
+    for item in index:
+        if isinstance(item, _np.ndarray) and item.dtype.kind in "iu" and axis < array.ndim:
+            dim = array.shape[axis]
+            item = _np.where(item < 0, item + dim, item)
+            over = int(item.max()) - dim + 1 if item.size else 0
+            pads[axis] = max(pads[axis], over)
+        fixed.append(item)
+        axis += 1
+    if any(pads):
+        padded = _np.zeros(tuple(d + p for d, p in zip(array.shape, pads)), dtype=array.dtype)
+        padded[tuple(slice(0, d) for d in array.shape)] = array
+        if ufunc is None:
+            padded[tuple(fixed)] = value
+        else:
+            ufunc.at(padded, tuple(fixed), value)
+        return padded[tuple(slice(0, d) for d in array.shape)].copy()
+    out = _np.array(array, copy=True)
+    if ufunc is None:
+        out[tuple(fixed)] = value
+    else:
+        ufunc.at(out, tuple(fixed), value)
+    return out
+
+
 class _AtIndexer:
     def __init__(self, array, index):
-        self.array = array
+        self.array = _np.asarray(array)
         self.index = index
 
     def set(self, value):
-        out = _np.array(self.array, copy=True)
-        out[self.index] = _np.asarray(value)
-        return _wrap(out)
+        return _wrap(_scatter(None, self.array, self.index, _np.asarray(value)))
 
     def add(self, value):
-        out = _np.array(self.array, copy=True)
-        _np.add.at(out, self.index, _np.asarray(value))
-        return _wrap(out)
+        return _wrap(_scatter(_np.add, self.array, self.index, _np.asarray(value)))
 
     def min(self, value):
-        out = _np.array(self.array, copy=True)
-        _np.minimum.at(out, self.index, _np.asarray(value))
-        return _wrap(out)
+        return _wrap(_scatter(_np.minimum, self.array, self.index, _np.asarray(value)))
 
     def max(self, value):
-        out = _np.array(self.array, copy=True)
-        _np.maximum.at(out, self.index, _np.asarray(value))
-        return _wrap(out)
+        return _wrap(_scatter(_np.maximum, self.array, self.index, _np.asarray(value)))
 
 
 class _At:
@@ -55,7 +105,10 @@ class JArray(_np.ndarray):
         return _At(self)
 
     def __getitem__(self, index):
-        return _wrap(_np.ndarray.__getitem__(self, _unwrap_index(index)))
+        index = _unwrap_index(index)
+        if isinstance(index, (tuple, _np.ndarray)):
+            index = _clamped(index, self.shape)
+        return _wrap(_np.ndarray.__getitem__(self, index))
 
 
 def _wrap(value):

@@ -94,3 +94,31 @@ def test_dt_limiter_sensor_step(case, label):
     assert close(rmin, g[f"step_{label}_rho_min"], 1e-9)
     for k in g["block_names"]:
         assert close(res[k], g[f"step_{label}_{k}"], 1e-9)
+
+
+MOOD_CASES = ["box_p2", "box_p3", "mixed_p2"]
+
+
+@pytest.mark.parametrize("case", MOOD_CASES)
+def test_mood_recompute_and_step(case):
+    from oracle.subcell import MOODLimiter, SubcellFV
+    g, mesh, op, bc = build(case)
+    s = {k: g[f"U_shocked_{k}"] for k in g["block_names"]}
+    dt = float(g["dt_shocked"])
+    inv = op.inviscid_rhs(s, bc)
+    vis = op.viscous_rhs(s, bc)
+    cand = {k: s[k] + dt * (inv[k] + vis[k]) for k in s}
+    pos = PositivityLimiter(op)
+    lim = MOODLimiter(op, positivity=pos)
+    tr = lim.troubled(cand)
+    for k in g["block_names"]:
+        np.testing.assert_array_equal(tr[k], g[f"mood_troubled_{k}"])
+    for recon in ("constant", "tvd", "weno"):
+        res = SubcellFV(op, reconstruction=recon).recompute(s, cand, dt, tr, bc, vis)
+        for k in g["block_names"]:
+            assert close(res[k], g[f"mood_{recon}_{k}"]), (recon, k)
+    integ = TimeIntegrator(op, cfl=0.3, limiter=lim)
+    res, valid, rmin, pmin = integ.checked_step(s, dt, bc)
+    assert valid == bool(g["mood_step_valid"])
+    for k in g["block_names"]:
+        assert close(res[k], g[f"mood_step_{k}"]), k
