@@ -204,6 +204,31 @@ int dgb_subcell_recompute(dgb_plan* plan, const dgb_state* base, const dgb_state
 enum { DGB_RHS_STAGES = 5 };
 int dgb_rhs_profile(dgb_plan* plan, const dgb_state* U, float* ms_out, void* stream);
 
+/* Allocation-free CFL time step for one element block.  No counterpart in the reference.
+ *
+ * For callers that may not allocate device memory when they ask for a time step: host
+ * codes or coupling frameworks that hand the library a fixed device-memory pool and
+ * forbid allocations behind their back, and time loops that must not call cudaMalloc
+ * (an allocation synchronises the device and can fail once the pool is reserved).
+ * It needs no plan: U is the block's device state (E, Np, nvars) float64, length the
+ * device array of per-element characteristic lengths (hybrid/time_integration.py:49-91),
+ * dt_out a device double; the result is the same clipped dt as dgb_stable_dt
+ * (hybrid/time_integration.py:93-169).  For a mesh of several blocks, call it per block
+ * and take the smallest dt.
+ *
+ * Scratch: a file-scope device array of 2^20 doubles (8 MiB) that every GPU which loads
+ * the library keeps until the process exits; at most 1048576 elements per call (larger
+ * blocks are rejected with DGB_ERR_ARGUMENT).  The first call on a device looks up that
+ * array's device address (cudaGetSymbolAddress) with the device current; make that first
+ * call before any stream capture.  All calls share the array: calls whose kernels overlap
+ * on the GPU (different streams or threads) race on it.  Errors are reported by
+ * dgb_noalloc_last_error(). */
+int dgb_stable_dt_noalloc(const double* U, const double* length, int num_elements, int num_nodes, int nvars,
+                          int degree, double gamma, double gas_constant, double dynamic_viscosity,
+                          double thermal_conductivity, double br2_penalty, double cfl, double* dt_out,
+                          void* stream);
+const char* dgb_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

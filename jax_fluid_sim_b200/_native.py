@@ -87,6 +87,10 @@ def lib():
             raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m jax_fluid_sim_b200.build`")
         L = ctypes.CDLL(str(LIB_PATH))
         L.dgb_last_error.restype = ctypes.c_char_p
+        L.dgb_noalloc_last_error.restype = ctypes.c_char_p
+        L.dgb_stable_dt_noalloc.argtypes = [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_double, c_double,
+                                            c_double, c_double, c_double, c_double, c_void_p, c_void_p]
+        L.dgb_stable_dt_noalloc.restype = c_int
         L.dgb_version.restype = c_int
         sigs = {
             "dgb_plan_create": [ctypes.POINTER(Params), ctypes.POINTER(c_void_p)],
