@@ -229,6 +229,63 @@ int dgb_stable_dt_noalloc(const double* U, const double* length, int num_element
                           void* stream);
 const char* dgb_noalloc_last_error(void);
 
+/* ---- Finite-rate chemistry (operator-split source), hybrid/chemistry/ ----------------
+ *
+ * A reaction mechanism as dense tables, filled from the mechanism's species and
+ * reactions (ReactionMechanism.__init__, hybrid/chemistry/mechanism.py:58-123; the
+ * Air-11 Park data of hybrid/chemistry/air11_park.py:20-311).  Host pointers; the
+ * library copies them.  Species count: 3 or 11 (the kernels are compiled for those);
+ * at most DGB_CHEM_MAX_REACTIONS reactions, each with at most 3 distinct reactant,
+ * 3 distinct product and 6 distinct net-stoichiometry species. */
+enum { DGB_CHEM_MAX_SPECIES = 11, DGB_CHEM_MAX_REACTIONS = 32 };
+typedef struct {
+  int num_species, num_reactions;
+  const double* molar_mass;        /* [ns] kg/mol */
+  const double* nu_forward;        /* [nr][ns] reactant stoichiometry nu' */
+  const double* nu_reverse;        /* [nr][ns] product stoichiometry nu'' */
+  const double* efficiency;        /* [nr][ns] third-body efficiencies alpha_M */
+  const double* arrhenius;         /* [nr][3] A, b, theta of kf = A T^b exp(-theta/T) (SI) */
+  const int* third_body;           /* [nr] 0/1 */
+  const int* forward_mode;         /* [nr] controlling temperature: 0 T, 1 sqrt(T Tv), 2 Tv */
+  const int* reverse_mode;         /* [nr] */
+  const double* nasa_range;        /* [ns][3] t_low, t_mid, t_high */
+  const double* nasa_coeffs;       /* [ns][2][7] low-range then high-range a0..a6 */
+} dgb_chem_mechanism;
+
+/* ReactingFlowCoupler.__init__ (hybrid/chemistry/coupling.py:26-71) without relaxation
+ * (single temperature, relaxation=None). */
+typedef struct {
+  int max_newton_iters;            /* default 12 */
+  int dimensionless;               /* 0/1 */
+  double reference_temperature;    /* K, default 300 */
+  double reference_pressure;       /* Pa, default 101325 */
+  double reference_length;         /* m, default 1 */
+  double gamma;                    /* default 1.4 */
+} dgb_chem_params;
+
+typedef struct dgb_chem dgb_chem;
+
+int dgb_chem_create(const dgb_chem_mechanism* mechanism, const dgb_chem_params* params, dgb_chem** out);
+int dgb_chem_destroy(dgb_chem* chem);
+
+/* ReactingFlowCoupler.react_block (hybrid/chemistry/coupling.py:179-197, per node
+ * _react_single_cell :116-177 with PointImplicitIntegrator.step,
+ * hybrid/chemistry/integrator.py:31-104): U and out are device arrays
+ * (num_elements, num_nodes, nvars) float64 with the species partial densities in
+ * columns 5 .. 5+ns-1; out may equal U.  Columns 0..4 are copied unchanged.  dt is the
+ * time step (dimensionless when the coupler is); dt_per_element, when not null, is a
+ * device array of num_elements steps that replaces dt (local time stepping).
+ * nvars < 5 + ns is DGB_ERR_ARGUMENT (the reference raises ValueError). */
+int dgb_react_block(dgb_chem* chem, const double* U, double* out, int64_t num_elements, int num_nodes,
+                    int nvars, double dt, const double* dt_per_element, void* stream);
+
+/* ReactionMechanism.net_production_rates (hybrid/chemistry/mechanism.py:159-220) at
+ * count independent samples, single temperature: rho (count, ns) and T (count) device
+ * arrays; omega (molar rates), wdot (mass rates after the mass-conserving correction) and
+ * jacobian (count, ns, ns) = d wdot / d rho are device outputs, each may be null. */
+int dgb_chem_rates(dgb_chem* chem, const double* rho, const double* T, int64_t count, double* omega,
+                   double* wdot, double* jacobian, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

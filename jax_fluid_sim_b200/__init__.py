@@ -7,6 +7,9 @@ state layout; the arithmetic runs in hand-written sm_100a CUDA kernels in
 """
 
 from .boundary import FarfieldWallBoundary
+from .air11 import AIR11_REACTIONS, AIR11_SPECIES
+from .chemistry import Air11ParkMechanism, ReactingFlowCoupler, ReactionMechanism
+from .mechanism import Reaction, Species, make_nasa7
 from .limiter import (HybridMOODSubcellLimiter, HybridPositivityLimiter, HybridSubcellFV,
                       HybridTroubledCellSensor)
 from .mesh import HybridMesh
@@ -16,6 +19,8 @@ from .solver import CompressibleStateLayout, HybridCompressibleSolver
 from .time_integration import HybridSSPRK3
 
 __all__ = [
+    "AIR11_REACTIONS", "AIR11_SPECIES", "Air11ParkMechanism", "ReactingFlowCoupler", "Reaction", "ReactionMechanism",
+    "Species", "make_nasa7",
     "CompressibleStateLayout", "FarfieldWallBoundary", "HybridCompressibleSolver", "HybridEulerOperator",
     "HybridMOODSubcellLimiter", "HybridMesh", "HybridNavierStokesOperator", "HybridPositivityLimiter",
     "HybridSSPRK3", "HybridSubcellFV", "HybridTroubledCellSensor", "MeshSource", "polynomial_br2_penalty",

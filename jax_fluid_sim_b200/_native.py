@@ -76,6 +76,18 @@ class Status(ctypes.Structure):
     _fields_ = [("valid", ctypes.c_int32), ("pad", ctypes.c_int32), ("rho_min", c_double), ("p_min", c_double)]
 
 
+class ChemMechanism(ctypes.Structure):
+    _fields_ = [("num_species", c_int), ("num_reactions", c_int), ("molar_mass", P_double),
+                ("nu_forward", P_double), ("nu_reverse", P_double), ("efficiency", P_double),
+                ("arrhenius", P_double), ("third_body", P_int32), ("forward_mode", P_int32),
+                ("reverse_mode", P_int32), ("nasa_range", P_double), ("nasa_coeffs", P_double)]
+
+
+class ChemParams(ctypes.Structure):
+    _fields_ = [("max_newton_iters", c_int), ("dimensionless", c_int), ("reference_temperature", c_double),
+                ("reference_pressure", c_double), ("reference_length", c_double), ("gamma", c_double)]
+
+
 _lib = None
 
 
@@ -111,6 +123,11 @@ def lib():
             "dgb_plan_set_subcells": [c_void_p, c_int, ctypes.POINTER(SubcellBlockDesc)],
             "dgb_plan_set_subcell_faces": [c_void_p, c_int, P_int32, P_int32],
             "dgb_plan_enable_mood": [c_void_p],
+            "dgb_chem_create": [ctypes.POINTER(ChemMechanism), ctypes.POINTER(ChemParams), ctypes.POINTER(c_void_p)],
+            "dgb_chem_destroy": [c_void_p],
+            "dgb_react_block": [c_void_p, c_void_p, c_void_p, ctypes.c_int64, c_int, c_int, c_double, c_void_p,
+                                c_void_p],
+            "dgb_chem_rates": [c_void_p, c_void_p, c_void_p, ctypes.c_int64, c_void_p, c_void_p, c_void_p, c_void_p],
             "dgb_subcell_recompute": [c_void_p, ctypes.POINTER(State), ctypes.POINTER(State), c_double,
                                       ctypes.POINTER(State), c_void_p, ctypes.POINTER(State), c_void_p],
         }

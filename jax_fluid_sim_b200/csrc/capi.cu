@@ -31,6 +31,11 @@ int fail(int code, const std::string& msg) {
 
 }  // namespace
 
+namespace dgb {
+// Error channel shared with the other translation units of the library (chemistry).
+int set_error(int code, const std::string& msg) { return fail(code, msg); }
+}  // namespace dgb
+
 struct dgb_plan {
   dgb_params prm;
   DevPlan dev;

@@ -6,8 +6,8 @@ Only the fixture generator in ``tests/golden/make_golden.py`` puts this on
 ``sys.path``.  Semantics covered: immutable-style ``.at[...]`` updates (copy
 then ``np.add.at``/``np.minimum.at``), ``jit``/``vmap``/``jacobian``,
 ``lax.cond/fori_loop/scan/while_loop``, ``tree.map``, ``config``.
-``jacobian`` is a central finite difference; the reference only uses it inside
-a Newton iteration whose converged root does not depend on it.
+``jacobian`` is forward-mode differentiation with dual numbers (``_dual.py``),
+following JAX's derivative conventions for ``maximum``/``minimum``/``clip``.
 """
 
 import types
@@ -83,20 +83,14 @@ def vmap(function, in_axes=0, out_axes=0):
 
 
 def jacobian(function):
+    """Forward-mode derivative with JAX's tie rule for max/min/clip (see _dual.py)."""
+    from ._dual import Dual
+
     def jac(x):
         x = _np.asarray(x, dtype=_np.float64)
-        f0 = _np.asarray(function(_wrap(x.copy())))
-        out = _np.zeros(f0.shape + x.shape)
-        flat = x.reshape(-1)
-        for j in range(flat.size):
-            h = 1.0e-6 * max(abs(flat[j]), 1.0e-12)
-            xp = flat.copy()
-            xm = flat.copy()
-            xp[j] += h
-            xm[j] -= h
-            fp = _np.asarray(function(_wrap(xp.reshape(x.shape))))
-            fm = _np.asarray(function(_wrap(xm.reshape(x.shape))))
-            out.reshape(f0.shape + (-1,))[..., j] = (fp - fm) / (2.0 * h)
-        return _wrap(out)
+        n = x.size
+        seed = Dual(x, _np.eye(n).reshape(x.shape + (n,)))
+        out = function(seed)
+        return _wrap(_np.asarray(out.d).reshape(out.v.shape + x.shape))
 
     return jac

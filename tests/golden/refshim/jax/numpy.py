@@ -112,6 +112,8 @@ class JArray(_np.ndarray):
 
 
 def _wrap(value):
+    if type(value).__name__ == "Dual":
+        return value
     if isinstance(value, _np.ndarray) and not isinstance(value, JArray):
         return value.view(JArray)
     if isinstance(value, (_np.floating, _np.integer, _np.bool_)):
@@ -126,6 +128,8 @@ def _wrap(value):
 def _plain(value):
     if isinstance(value, JArray):
         return _np.asarray(value)
+    if type(value).__name__ == "Dual":
+        return value
     if isinstance(value, (list, tuple)):
         return type(value)(_plain(v) for v in value)
     return value
@@ -149,6 +153,8 @@ def einsum(subscripts, *operands, **kwargs):
 
 
 def asarray(value, dtype=None):
+    if type(value).__name__ == "Dual":
+        return value
     if isinstance(value, (list, tuple)):
         value = [_np.asarray(v) if isinstance(v, JArray) else v for v in value]
     return _wrap(_np.asarray(value, dtype=dtype))
