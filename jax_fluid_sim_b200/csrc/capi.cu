@@ -199,6 +199,16 @@ int run_positivity_hex(dgb_plan* p, const StatePtrs& S, cudaStream_t st) {
   return DGB_OK;
 }
 
+template <int P, int NV>
+int run_troubled_hex(dgb_plan* p, const StatePtrs& S, double* sensor, uint8_t* flags, cudaStream_t st) {
+  const size_t sm = sizeof(double) * (size_t)hex_troubled_smem<P, NV>();
+  int rc;
+  if ((rc = prepare(k_hex_troubled<P, NV>, sm))) return rc;
+  k_hex_troubled<P, NV><<<p->dev.blk[0].E, kThreads, sm, st>>>(p->dev, S, 0, p->hex_tables, p->lim, sensor, flags);
+  CK(cudaGetLastError());
+  return DGB_OK;
+}
+
 template <int NV>
 int run_positivity(dgb_plan* p, const StatePtrs& S, cudaStream_t st) {
   int rc;
@@ -246,6 +256,15 @@ int run_stable_dt(dgb_plan* p, const StatePtrs& S, double cfl, double* dt_out, c
 template <int NV>
 int run_troubled(dgb_plan* p, const StatePtrs& S, double* const* sensor, uint8_t* const* flags, cudaStream_t st) {
   int rc;
+  if (p->hex) {
+    double* so = sensor ? sensor[0] : nullptr;
+    uint8_t* fo = flags ? flags[0] : nullptr;
+    switch (p->dev.degree) {
+      case 1: return run_troubled_hex<1, NV>(p, S, so, fo, st);
+      case 2: return run_troubled_hex<2, NV>(p, S, so, fo, st);
+      default: return run_troubled_hex<3, NV>(p, S, so, fo, st);
+    }
+  }
   for (int b = 0; b < p->dev.nblocks; ++b) {
     if ((rc = prepare(k_troubled<NV>, p->smem_troubled[b]))) return rc;
     k_troubled<NV><<<p->dev.blk[b].E, kThreads, p->smem_troubled[b], st>>>(

@@ -50,7 +50,10 @@ struct Tables {
   int ns, nr;
   double W[DGB_CHEM_MAX_SPECIES];             // molar mass
   double RW[DGB_CHEM_MAX_SPECIES];            // R_univ / W
+  double iW[DGB_CHEM_MAX_SPECIES];            // 1 / W
   double trange[DGB_CHEM_MAX_SPECIES][3];
+  double clamp_log[DGB_CHEM_MAX_SPECIES][2];  // ln t_low, ln t_high
+  double clamp_inv[DGB_CHEM_MAX_SPECIES][2];  // 1 / t_low, 1 / t_high
   double cp[DGB_CHEM_MAX_SPECIES][2][5];      // a0..a4
   double h[DGB_CHEM_MAX_SPECIES][2][6];       // a0, a1/2, a2/3, a3/4, a4/5, a5
   double s[DGB_CHEM_MAX_SPECIES][2][6];       // a0, a1, a2/2, a3/3, a4/4, a6
@@ -78,39 +81,53 @@ struct Slots {
   __device__ double& dC(int q) const { return base[(NS * (NS + 3) + q) * stride]; }
   __device__ double& g(int q) const { return base[(NS * (NS + 4) + q) * stride]; }
   __device__ double& om(int q) const { return base[(NS * (NS + 5) + q) * stride]; }
-  static constexpr int kDoubles = NS * (NS + 6);
+  __device__ double& r0(int q) const { return base[(NS * (NS + 6) + q) * stride]; }   // Newton's rho0
+  static constexpr int kDoubles = NS * (NS + 7);
 };
 
+// Temperature powers shared by every species at one temperature T: ln T and 1/T.  A species
+// whose fit range clamps T uses the host-computed ln and reciprocal of its range end.
+struct TPow {
+  double T, lnT, invT;
+};
+
+__device__ __forceinline__ TPow tpow(double T) { return TPow{T, log(T), 1.0 / T}; }
+
 // species q at T: T clamped to [t_low, t_high], coefficient set by T_c < t_mid
-__device__ __forceinline__ int nasa_range(const Tables& M, int q, double T, double& Tc) {
-  Tc = jclip(T, M.trange[q][0], M.trange[q][2]);
+__device__ __forceinline__ int nasa_range(const Tables& M, int q, const TPow& t, double& Tc, double& lnTc,
+                                          double& invTc) {
+  Tc = jclip(t.T, M.trange[q][0], M.trange[q][2]);
+  const bool lo = Tc == M.trange[q][0] && Tc != t.T;
+  const bool hi = Tc == M.trange[q][2] && Tc != t.T;
+  lnTc = lo ? M.clamp_log[q][0] : (hi ? M.clamp_log[q][1] : t.lnT);
+  invTc = lo ? M.clamp_inv[q][0] : (hi ? M.clamp_inv[q][1] : t.invT);
   return Tc < M.trange[q][1] ? 0 : 1;
 }
 
-__device__ __forceinline__ double h_RT(const Tables& M, int q, double T) {
-  double Tc;
-  const int r = nasa_range(M, q, T, Tc);
+__device__ __forceinline__ double h_RT(const Tables& M, int q, const TPow& t) {
+  double Tc, lnTc, invTc;
+  const int r = nasa_range(M, q, t, Tc, lnTc, invTc);
   const double* a = M.h[q][r];
   const double T2 = Tc * Tc;
-  return a[0] + a[1] * Tc + a[2] * T2 + a[3] * (T2 * Tc) + a[4] * (T2 * T2) + a[5] / Tc;
+  return a[0] + a[1] * Tc + a[2] * T2 + a[3] * (T2 * Tc) + a[4] * (T2 * T2) + a[5] * invTc;
 }
 
-__device__ __forceinline__ double cp_R(const Tables& M, int q, double T) {
-  double Tc;
-  const int r = nasa_range(M, q, T, Tc);
+__device__ __forceinline__ double cp_R(const Tables& M, int q, const TPow& t) {
+  double Tc, lnTc, invTc;
+  const int r = nasa_range(M, q, t, Tc, lnTc, invTc);
   const double* a = M.cp[q][r];
   const double T2 = Tc * Tc;
   return a[0] + a[1] * Tc + a[2] * T2 + a[3] * (T2 * Tc) + a[4] * (T2 * T2);
 }
 
-__device__ __forceinline__ double g_RT(const Tables& M, int q, double T) {
-  double Tc;
-  const int r = nasa_range(M, q, T, Tc);
+__device__ __forceinline__ double g_RT(const Tables& M, int q, const TPow& t) {
+  double Tc, lnTc, invTc;
+  const int r = nasa_range(M, q, t, Tc, lnTc, invTc);
   const double* a = M.h[q][r];
   const double* c = M.s[q][r];
   const double T2 = Tc * Tc;
-  const double h = a[0] + a[1] * Tc + a[2] * T2 + a[3] * (T2 * Tc) + a[4] * (T2 * T2) + a[5] / Tc;
-  const double s = c[0] * log(Tc) + c[1] * Tc + c[2] * T2 + c[3] * (T2 * Tc) + c[4] * (T2 * T2) + c[5];
+  const double h = a[0] + a[1] * Tc + a[2] * T2 + a[3] * (T2 * Tc) + a[4] * (T2 * T2) + a[5] * invTc;
+  const double s = c[0] * lnTc + c[1] * Tc + c[2] * T2 + c[3] * (T2 * Tc) + c[4] * (T2 * T2) + c[5];
   return h - s;
 }
 
@@ -127,9 +144,10 @@ __device__ double internal_energy(const Tables& M, const double (&rho)[NS], doub
 #pragma unroll
   for (int q = 0; q < NS; ++q) S += rho[q];
   S = jmax(S, 1.0e-14);
+  const TPow t{T, 0.0, 1.0 / T};     // the energy fits need no logarithm
   double e = 0.0;
 #pragma unroll
-  for (int q = 0; q < NS; ++q) e += (jmax(rho[q], 0.0) / S) * ((h_RT(M, q, T) - 1.0) * (T * M.RW[q]));
+  for (int q = 0; q < NS; ++q) e += (jmax(rho[q], 0.0) / S) * ((h_RT(M, q, t) - 1.0) * (T * M.RW[q]));
   return e;
 }
 
@@ -145,11 +163,13 @@ __device__ double recover_T(const Tables& M, const double (&rho)[NS], double tar
   for (int q = 0; q < NS; ++q) Y[q] = jmax(rho[q], 0.0) / S;
   for (int it = 0; it < iters; ++it) {
     const double Ts = jclip(T, 50.0, 50000.0);
+    // 1/Ts is the only temperature power the energy fits need (no logarithm)
+    const TPow t{Ts, 0.0, 1.0 / Ts};
     double e = 0.0, cv = 0.0;
 #pragma unroll
     for (int q = 0; q < NS; ++q) {
-      e += Y[q] * ((h_RT(M, q, Ts) - 1.0) * (Ts * M.RW[q]));
-      cv += Y[q] * ((cp_R(M, q, Ts) - 1.0) * M.RW[q]);
+      e += Y[q] * ((h_RT(M, q, t) - 1.0) * (Ts * M.RW[q]));
+      cv += Y[q] * ((cp_R(M, q, t) - 1.0) * M.RW[q]);
     }
     const double dT = -(e - target) / jmax(cv, 1.0e-5);
     T = jclip(T + jclip(dT, -0.5 * T, 0.5 * T), 100.0, 50000.0);
@@ -161,21 +181,22 @@ __device__ double recover_T(const Tables& M, const double (&rho)[NS], double tar
 // into sl.A(s, j) (d w/d rho before the molar-mass scaling and the mass correction).
 template <int NS>
 __device__ void rates(const Tables& M, const Slots<NS>& sl, const double (&rho)[NS], double T, bool jac) {
-  double C[NS];
 #pragma unroll
   for (int q = 0; q < NS; ++q) {
-    const double craw = rho[q] / M.W[q];
-    C[q] = jmax(craw, 0.0);
-    const double dc = dmax_tie(craw, 0.0) / M.W[q];
-    const double cc = jmax(C[q], kMinC);
+    const double craw = rho[q] * M.iW[q];
+    const double c = jmax(craw, 0.0);
+    const double dc = dmax_tie(craw, 0.0) * M.iW[q];
+    const double cc = jmax(c, kMinC);
     sl.logC(q) = log(cc);
-    sl.dlog(q) = dmax_tie(C[q], kMinC) * dc / cc;
+    sl.dlog(q) = dmax_tie(c, kMinC) * dc / cc;
     sl.dC(q) = dc;
     sl.om(q) = 0.0;
   }
   const double Tg = jmax(T, 10.0);
+  const TPow tg = tpow(Tg);
+  const double base_g = kPStd / (kRUniv * Tg);
 #pragma unroll
-  for (int q = 0; q < NS; ++q) sl.g(q) = g_RT(M, q, Tg);
+  for (int q = 0; q < NS; ++q) sl.g(q) = g_RT(M, q, tg);
   if (jac) {
 #pragma unroll
     for (int i = 0; i < NS; ++i)
@@ -184,16 +205,19 @@ __device__ void rates(const Tables& M, const Slots<NS>& sl, const double (&rho)[
   }
   for (int r = 0; r < M.nr; ++r) {
     const Reaction& R = M.rx[r];
+    // kf = A T^b exp(-theta/T) as A exp(b ln T - theta/T); ln T and 1/T are shared
     const double Tf = jmax(select_T(R.fmode, T, T), 10.0);
-    const double kf = R.A * pow(Tf, R.b) * exp(-R.theta / Tf);
+    const TPow tf = Tf == Tg ? tg : tpow(Tf);
+    const double kf = R.A * exp(R.b * tf.lnT - R.theta * tf.invT);
     const double Tr = jmax(select_T(R.rmode, T, T), 10.0);
     double dG = 0.0;
     if (Tr == Tg) {
       for (int k = 0; k < R.nd; ++k) dG += R.d_nu[k] * sl.g(R.d_sp[k]);
     } else {
-      for (int k = 0; k < R.nd; ++k) dG += R.d_nu[k] * g_RT(M, R.d_sp[k], Tr);
+      const TPow tr = tpow(Tr);
+      for (int k = 0; k < R.nd; ++k) dG += R.d_nu[k] * g_RT(M, R.d_sp[k], tr);
     }
-    const double base = kPStd / (kRUniv * Tr);
+    const double base = Tr == Tg ? base_g : kPStd / (kRUniv * Tr);
     const double conv = R.dn == 0.0 ? 1.0 : (R.dn == 1.0 ? base : (R.dn == -1.0 ? 1.0 / base : pow(base, R.dn)));
     const double Kc = exp(-jclip(dG, -kClipExp, kClipExp)) * conv;
     const double kr = kf / jmax(Kc, kMinKc);
@@ -206,7 +230,7 @@ __device__ void rates(const Tables& M, const Slots<NS>& sl, const double (&rho)[
     if (R.third) {
       coll = 0.0;
 #pragma unroll
-      for (int q = 0; q < NS; ++q) coll += M.alpha[r][q] * C[q];
+      for (int q = 0; q < NS; ++q) coll += M.alpha[r][q] * jmax(rho[q] * M.iW[q], 0.0);
     }
     const double qf = kf * fwd * coll, qr = kr * rev * coll;
     const double qn = qf - qr;
@@ -236,26 +260,26 @@ __device__ void rates(const Tables& M, const Slots<NS>& sl, const double (&rho)[
   }
 }
 
-// Mass-conserving correction (mechanism.py:214-218): w = W omega - Y sum(W omega), and its
-// Jacobian J = dwd - dY sum(wd) - Y colsum(dwd).  newton: sl.A becomes [I - dt J | -res]
-// with res = rho - rho0 - dt w; otherwise sl.A holds J.  wfix receives w.
+// Mass-conserving correction (mechanism.py:214-218): w = W omega - Y sum(W omega) replaces
+// omega in sl.om, and its Jacobian J = dwd - dY sum(wd) - Y colsum(dwd) replaces sl.A
+// (newton: sl.A becomes [I - dt J | -res] with res = rho - rho0 - dt w).
 template <int NS>
-__device__ void finish(const Tables& M, const Slots<NS>& sl, const double (&rho)[NS], const double (&rho0)[NS],
-                       double dt, bool jac, bool newton, double (&wfix)[NS]) {
+__device__ void finish(const Tables& M, const Slots<NS>& sl, const double (&rho)[NS], double dt, bool jac,
+                       bool newton) {
   double Sraw = 0.0;
 #pragma unroll
   for (int q = 0; q < NS; ++q) Sraw += rho[q];
   const double S = jmax(Sraw, 1.0e-14);
   const double dS = dmax_tie(Sraw, 1.0e-14);
-  double wd[NS], Y[NS], sw = 0.0;
+  double sw = 0.0;
 #pragma unroll
   for (int q = 0; q < NS; ++q) {
-    wd[q] = sl.om(q) * M.W[q];
-    sw += wd[q];
-    Y[q] = jmax(rho[q], 0.0) / S;
+    const double wd = sl.om(q) * M.W[q];
+    sl.om(q) = wd;
+    sw += wd;
   }
 #pragma unroll
-  for (int q = 0; q < NS; ++q) wfix[q] = wd[q] - Y[q] * sw;
+  for (int q = 0; q < NS; ++q) sl.om(q) = sl.om(q) - (jmax(rho[q], 0.0) / S) * sw;
   if (!jac) return;
 #pragma unroll
   for (int j = 0; j < NS; ++j) {
@@ -268,14 +292,15 @@ __device__ void finish(const Tables& M, const Slots<NS>& sl, const double (&rho)
     }
 #pragma unroll
     for (int i = 0; i < NS; ++i) {
+      const double Yi = jmax(rho[i], 0.0) / S;
       const double dY = (i == j ? dmax_tie(rho[i], 0.0) / S : 0.0) - (jmax(rho[i], 0.0) / (S * S)) * dS;
-      const double J = sl.A(i, j) - dY * sw - Y[i] * col;
+      const double J = sl.A(i, j) - dY * sw - Yi * col;
       sl.A(i, j) = newton ? (i == j ? 1.0 : 0.0) - dt * J : J;
     }
   }
   if (newton) {
 #pragma unroll
-    for (int i = 0; i < NS; ++i) sl.A(i, NS) = -(rho[i] - rho0[i] - dt * wfix[i]);
+    for (int i = 0; i < NS; ++i) sl.A(i, NS) = -(rho[i] - sl.r0(i) - dt * sl.om(i));
   }
 }
 
@@ -361,19 +386,19 @@ __global__ void __launch_bounds__(kThreads) k_react(const __grid_constant__ Tabl
   }
 
   // PointImplicitIntegrator.step, constant_temperature=False
-  double rho0[NS], rho[NS], total = 0.0;
+  double rho[NS], total = 0.0;
 #pragma unroll
   for (int q = 0; q < NS; ++q) {
-    rho0[q] = jmax(rp[q], 1.0e-20);
-    rho[q] = rho0[q];
-    total += rho0[q];
+    rho[q] = jmax(rp[q], 1.0e-20);
+    sl.r0(q) = rho[q];
+    total += rho[q];
   }
-  const double e_init = internal_energy<NS>(M, rho0, T0);
+  const double e_init = internal_energy<NS>(M, rho, T0);
   double Tk = T0;
   for (int it = 0; it < M.iters; ++it) {
-    double w[NS], d[NS];
+    double d[NS];
     rates<NS>(M, sl, rho, Tk, true);
-    finish<NS>(M, sl, rho, rho0, dtp, true, true, w);
+    finish<NS>(M, sl, rho, dtp, true, true);
     lu_solve<NS>(sl, d);
 #pragma unroll
     for (int q = 0; q < NS; ++q) rho[q] = jmax(rho[q] + d[q], 0.0);
@@ -411,7 +436,7 @@ __global__ void __launch_bounds__(kThreads) k_rates(const __grid_constant__ Tabl
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= count) return;
   const Slots<NS> sl{smem + threadIdx.x, (int)blockDim.x};
-  double rho[NS], w[NS];
+  double rho[NS];
 #pragma unroll
   for (int q = 0; q < NS; ++q) rho[q] = rho_in[n * NS + q];
   const bool want = jac != nullptr;
@@ -419,10 +444,10 @@ __global__ void __launch_bounds__(kThreads) k_rates(const __grid_constant__ Tabl
 #pragma unroll
   for (int q = 0; q < NS; ++q)
     if (omega) omega[n * NS + q] = sl.om(q);
-  finish<NS>(M, sl, rho, rho, 0.0, want, false, w);
+  finish<NS>(M, sl, rho, 0.0, want, false);
 #pragma unroll
   for (int q = 0; q < NS; ++q)
-    if (wdot) wdot[n * NS + q] = w[q];
+    if (wdot) wdot[n * NS + q] = sl.om(q);
   if (want) {
 #pragma unroll
     for (int i = 0; i < NS; ++i)
@@ -490,7 +515,16 @@ int dgb_chem_create(const dgb_chem_mechanism* m, const dgb_chem_params* prm, dgb
   for (int q = 0; q < ns; ++q) {
     M.W[q] = m->molar_mass[q];
     M.RW[q] = kRUniv / m->molar_mass[q];
+    M.iW[q] = 1.0 / m->molar_mass[q];
     for (int k = 0; k < 3; ++k) M.trange[q][k] = m->nasa_range[q * 3 + k];
+    if (!(M.trange[q][0] > 0.0) || !(M.trange[q][2] > M.trange[q][0])) {
+      delete c;
+      return fail(DGB_ERR_ARGUMENT, "NASA-7 ranges must satisfy 0 < t_low < t_high");
+    }
+    M.clamp_log[q][0] = log(M.trange[q][0]);
+    M.clamp_log[q][1] = log(M.trange[q][2]);
+    M.clamp_inv[q][0] = 1.0 / M.trange[q][0];
+    M.clamp_inv[q][1] = 1.0 / M.trange[q][2];
     for (int r = 0; r < 2; ++r) {
       const double* a = m->nasa_coeffs + (q * 2 + r) * 7;
       for (int k = 0; k < 5; ++k) M.cp[q][r][k] = a[k];

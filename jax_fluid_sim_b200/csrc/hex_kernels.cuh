@@ -636,6 +636,42 @@ __global__ void __launch_bounds__(kThreads) k_hex_finalize(const DevPlan P_, con
 // by sum factorisation: nodes, volume points (tensor Gauss grid) and the Gauss grids of the six
 // faces -- for a hexahedron mesh these are exactly the distinct face points the reference
 // collects from its face groups.
+// Limiter / detector samples of one element (hybrid/limiter.py:29-67): the state at the nodes,
+// at the volume quadrature points and at the face quadrature points of the six faces, in that
+// order -> Smp[v][NS]; U receives the element state in lexicographic order and vq the
+// volume-point values [NV][Q3].  Ends without a barrier: callers synchronise before reading.
+template <int P, int NV>
+__device__ void hex_samples(const HexTables* tb, const double* Ug, double* U, double* Smp, double* t1, double* t2,
+                            double* slab, double* vq) {
+  using D = HexDims<P>;
+  constexpr int N = D::N, Q = D::Q, QF = D::QF, N3 = D::N3, Q3 = D::Q3, QF2 = D::QF2;
+  constexpr int NS = N3 + Q3 + 6 * QF2;
+  for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
+    const int v = idx / N3, l = idx % N3;
+    const double x = Ug[tb->lex2node[l] * NV + v];
+    U[idx] = x;
+    Smp[v * NS + l] = x;
+  }
+  __syncthreads();
+  tensor3<NV, N, N, N, Q, Q, Q, false>(U, vq, t1, t2, tb->bq, tb->bq, tb->bq);
+  for (int idx = threadIdx.x; idx < NV * Q3; idx += blockDim.x) {
+    const int v = idx / Q3, q = idx % Q3;
+    Smp[v * NS + N3 + q] = vq[idx];
+  }
+  for (int lf = 0; lf < 6; ++lf) {
+    int a0, end, a1, a2;
+    hex_face_axes(lf, a0, end, a1, a2);
+    __syncthreads();
+    face_slab<NV, N>(U, slab, a0, end, a1, a2);
+    __syncthreads();
+    tensor2<NV, N, N, QF, QF>(slab, t2, t1, tb->bf, tb->bf);
+    for (int idx = threadIdx.x; idx < NV * QF2; idx += blockDim.x) {
+      const int v = idx / QF2, q = idx % QF2;
+      Smp[v * NS + N3 + Q3 + lf * QF2 + q] = t2[idx];
+    }
+  }
+}
+
 template <int P, int NV>
 __global__ void __launch_bounds__(kThreads) k_hex_positivity(const DevPlan P_, const StatePtrs S, int b,
                                                             const HexTables tables, const LimiterConst Lc) {
@@ -657,33 +693,9 @@ __global__ void __launch_bounds__(kThreads) k_hex_positivity(const DevPlan P_, c
   const int e = blockIdx.x;
   load_tables<P>(tables, tb);
   double* Ug = S.b[b] + (size_t)e * N3 * NV;
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
-    const int v = idx / N3, l = idx % N3;
-    const double x = Ug[tb->lex2node[l] * NV + v];
-    U[idx] = x;
-    Smp[v * NS + l] = x;
-  }
-  __syncthreads();
-  // volume points -> Smp[v][N3 + q]  (written through a [NV][Q3] staging in t2's tail region)
   double* vq = slab + NV * N * N;                   // [NV][Q3]
-  tensor3<NV, N, N, N, Q, Q, Q, false>(U, vq, t1, t2, tb->bq, tb->bq, tb->bq);
-  for (int idx = threadIdx.x; idx < NV * Q3; idx += blockDim.x) {
-    const int v = idx / Q3, q = idx % Q3;
-    Smp[v * NS + N3 + q] = vq[idx];
-  }
-  for (int lf = 0; lf < 6; ++lf) {
-    int a0, end, a1, a2;
-    hex_face_axes(lf, a0, end, a1, a2);
-    __syncthreads();
-    face_slab<NV, N>(U, slab, a0, end, a1, a2);
-    __syncthreads();
-    tensor2<NV, N, N, QF, QF>(slab, t2, t1, tb->bf, tb->bf);
-    for (int idx = threadIdx.x; idx < NV * QF2; idx += blockDim.x) {
-      const int v = idx / QF2, q = idx % QF2;
-      Smp[v * NS + N3 + Q3 + lf * QF2 + q] = t2[idx];
-    }
-  }
+  __syncthreads();
+  hex_samples<P, NV>(tb, Ug, U, Smp, t1, t2, slab, vq);
   if (threadIdx.x == 0) red_nan = 0;
   __syncthreads();
   // cell mean from the volume samples
@@ -750,12 +762,124 @@ __global__ void __launch_bounds__(kThreads) k_hex_positivity(const DevPlan P_, c
   }
 }
 
+// Troubled-cell detector on the sum-factorised samples (hybrid/limiter.py:165-185 sensor on
+// (rho, p) at the nodes with the P1 projector; MOOD admissibility of every sample and the
+// cell mean, hybrid/limiter.py:285-300).  Same outputs as k_troubled.
+template <int P, int NV>
+__global__ void __launch_bounds__(kThreads) k_hex_troubled(const DevPlan P_, const StatePtrs S, int b,
+                                                          const HexTables tables, const LimiterConst Lc,
+                                                          double* sensor_out, uint8_t* flag_out) {
+  using D = HexDims<P>;
+  constexpr int N = D::N, Q = D::Q, N3 = D::N3, Q3 = D::Q3, QF2 = D::QF2;
+  constexpr int NS = N3 + Q3 + 6 * QF2;
+  extern __shared__ double smem[];
+  HexTables* tb = reinterpret_cast<HexTables*>(smem);
+  double* U = smem + HexSmem<P, NV>::T;
+  double* Smp = U + NV * N3;
+  double* t1 = Smp + NV * NS;
+  double* t2 = t1 + NV * N * N * Q;
+  double* slab = t2 + NV * N * Q * Q;
+  double* vq = slab + NV * N * N;
+  double* Mon = vq + NV * Q3;                       // [N3][2] (rho, p) in element node order
+  __shared__ double mean[NV];
+  __shared__ double red[4][kThreads / 32];
+  const BlockDev& B = P_.blk[b];
+  const int e = blockIdx.x;
+  load_tables<P>(tables, tb);
+  const double* Ug = S.b[b] + (size_t)e * N3 * NV;
+  __syncthreads();
+  hex_samples<P, NV>(tb, Ug, U, Smp, t1, t2, slab, vq);
+  for (int l = threadIdx.x; l < N3; l += blockDim.x) {
+    double u[NV], W[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) u[v] = U[v * N3 + l];
+    primitive<NV>(P_.ph, u, W);
+    const int node = tb->lex2node[l];
+    Mon[node * 2 + 0] = W[0];
+    Mon[node * 2 + 1] = W[4];
+  }
+  __syncthreads();
+  const double* wdet = B.wdet + (size_t)e * Q3;
+  for (int v = threadIdx.x; v < NV; v += blockDim.x) {
+    double s = 0.0, w = 0.0;
+    for (int q = 0; q < Q3; ++q) {
+      s += vq[v * Q3 + q] * wdet[q];
+      w += wdet[q];
+    }
+    mean[v] = s / w;
+  }
+  double hi0 = 0.0, hi1 = 0.0, sc0 = 0.0, sc1 = 0.0;
+  if (P >= 2) {
+    for (int i = threadIdx.x; i < N3; i += blockDim.x) {
+      const double* row = B.p1proj + (size_t)i * N3;
+      double l0 = 0.0, l1 = 0.0;
+      for (int j = 0; j < N3; ++j) {
+        const double pj = __ldg(row + j);
+        l0 += pj * Mon[j * 2 + 0];
+        l1 += pj * Mon[j * 2 + 1];
+      }
+      const double m0 = Mon[i * 2 + 0], m1 = Mon[i * 2 + 1];
+      const double d0 = m0 - l0, d1 = m1 - l1;
+      hi0 += d0 * d0;
+      hi1 += d1 * d1;
+      sc0 += m0 * m0;
+      sc1 += m1 * m1;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    hi0 += __shfl_xor_sync(0xffffffff, hi0, o);
+    hi1 += __shfl_xor_sync(0xffffffff, hi1, o);
+    sc0 += __shfl_xor_sync(0xffffffff, sc0, o);
+    sc1 += __shfl_xor_sync(0xffffffff, sc1, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = hi0;
+    red[1][threadIdx.x >> 5] = hi1;
+    red[2][threadIdx.x >> 5] = sc0;
+    red[3][threadIdx.x >> 5] = sc1;
+  }
+  __syncthreads();
+  bool bad = false;
+  for (int r = threadIdx.x; r <= NS; r += blockDim.x) {
+    double s[NV], W[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) s[v] = r < NS ? Smp[v * NS + r] : mean[v];
+    primitive<NV>(P_.ph, s, W);
+    bool finite = true;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) finite &= isfinite(W[v]);
+    bad |= !finite || (W[0] < Lc.density_floor) || (W[4] < Lc.pressure_floor);
+  }
+  const bool any_bad = __syncthreads_or(bad);
+  if (threadIdx.x == 0) {
+    double h0 = 0, h1 = 0, s0 = 0, s1 = 0;
+    for (int k = 0; k < kThreads / 32; ++k) {
+      h0 += red[0][k];
+      h1 += red[1][k];
+      s0 += red[2][k];
+      s1 += red[3][k];
+    }
+    double value = 0.0;
+    if (P >= 2) {
+      const double r0 = h0 / fmax(s0, 1.0e-12), r1 = h1 / fmax(s1, 1.0e-12);
+      value = (isnan(r0) || isnan(r1)) ? NAN : fmax(r0, r1);
+    }
+    if (sensor_out) sensor_out[e] = value;
+    if (flag_out) flag_out[e] = (uint8_t)((value > Lc.sensor_threshold) || any_bad);
+  }
+}
+
 template <int P, int NV>
 constexpr int hex_positivity_smem() {
   using D = HexDims<P>;
   constexpr int NS = D::N3 + D::Q3 + 6 * D::QF2;
   return HexSmem<P, NV>::T + NV * D::N3 + NV * NS + NV * D::N * D::N * D::Q + NV * D::N * D::Q * D::Q +
          NV * D::N2 + NV * D::Q3;
+}
+
+template <int P, int NV>
+constexpr int hex_troubled_smem() {
+  return hex_positivity_smem<P, NV>() + 2 * HexDims<P>::N3;
 }
 
 }  // namespace dgb

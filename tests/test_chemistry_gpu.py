@@ -116,29 +116,28 @@ def test_coupler_dimensionless_matches_reference():
     assert np.max(np.abs(out - GOLDEN["dimless_out"])[..., 5:] / U[..., :1]) < 2e-5
 
 
-def _random_reacting_block(E, Np, seed):
+def _air_block(E, Np, seed):
+    """Dimensionless (T_ref 220 K) frozen air between 3000 and 7000 K at Mach 0-8: the
+    state a Mach-8 shock layer hands to the coupler."""
     rng = np.random.default_rng(seed)
     U = np.zeros((E, Np, 16))
     rho = 0.5 + 3.0 * rng.random((E, Np))
     vel = 8.0 * np.sqrt(1.4) * rng.random((E, Np))
-    p = 1.0 + 120.0 * rng.random((E, Np))
-    Y = np.zeros((E, Np, 11))
-    Y[..., 9], Y[..., 10] = 0.767, 0.233
-    Y[..., 6:9] += 0.05 * rng.random((E, Np, 3))
-    Y /= Y.sum(-1, keepdims=True)
+    T = 3000.0 + 4000.0 * rng.random((E, Np))
     U[..., 0], U[..., 1] = rho, rho * vel
-    U[..., 4] = p / 0.4 + 0.5 * rho * vel ** 2
-    U[..., 5:] = rho[..., None] * Y
+    U[..., 4] = rho * T / 220.0 / 0.4 + 0.5 * rho * vel ** 2
+    U[..., 5 + 9], U[..., 5 + 10] = 0.767 * rho, 0.233 * rho
     return U
 
 
 def test_coupler_matches_oracle_per_element_dt_and_in_place():
-    """A sampled Mach-8 block with per-element (local time stepping) dt, updated in place,
-    against the oracle node by node (coupling.py:179-197 with an (E,) dt)."""
+    """A sampled block with per-element (local time stepping) dt, updated in place, against
+    the oracle node by node (coupling.py:179-197 with an (E,) dt).  The steps are chosen so
+    that every node's 12 Newton iterations converge (scaled residual below 5e-12)."""
     from jax_fluid_sim_b200 import ReactingFlowCoupler
     E, Np = 6, 9
-    U = _random_reacting_block(E, Np, 11)
-    dts = 1e-3 * (1.0 + np.arange(E))
+    U = _air_block(E, Np, 11)
+    dts = 3e-4 * (1.0 + np.arange(E))
     c = ReactingFlowCoupler(dimensionless=True, reference_temperature=220.0, reference_pressure=500.0,
                             reference_length=0.1)
     Ud = _cuda(U)
@@ -148,7 +147,8 @@ def test_coupler_matches_oracle_per_element_dt_and_in_place():
     ref = Coupler(12, True, 220.0, 500.0, 0.1)
     exp = np.stack([ref.react_block(U[e:e + 1], float(dts[e]))[0] for e in range(E)])
     _invariants(U, out)
-    assert np.max(np.abs(out - exp)[..., 5:] / U[..., :1]) < 2e-5
+    assert np.max(np.abs(out - U)[..., 5:]) > 1e-3          # the step does react
+    assert np.max(np.abs(out - exp)[..., 5:] / U[..., :1]) < 1e-8
 
 
 def test_coupler_argument_errors():
