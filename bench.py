@@ -5,11 +5,18 @@ Workload (the headline configuration): Mach-3 viscous flow past a sphere of radi
 (64 nodes per element), perfect gas gamma=1.4, Re_D=1e5, T_inf=220 K, no-slip
 isothermal wall T_w=300 K (non-dimensional as the reference driver does:
 rho=p=1, U=3*sqrt(1.4), mu=U/Re, T_w=300/220).  One step = one checked SSP-RK3
-step (three stages of inviscid HLLC + BR2 viscous residual, blend, Zhang-Shu
-positivity limiter and admissibility check), float64.  Synthetic seeded mesh
-(numpy generator); the state starts as the uniform free stream.
+step (three stages of inviscid HLLC + BR2 viscous residual, then per stage the MOOD
+troubled-cell check, subcell finite-volume recompute of troubled elements, Zhang-Shu
+positivity limiter, blend and admissibility check).  Synthetic seeded mesh (numpy
+generator); the state starts as the uniform free stream.
+
+By default the step is timed twice from the same state and dt: plain float64, then the
+mixed-precision path (float32 arithmetic in the BR2-lift and volume kernels; state, face
+fluxes, limiters and reductions float64).  The mixed step is the headline value; the
+plain one and the relative density L2 difference between the two rides along.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision both|mixed|float64] [--limiter mood|positivity]
 
 Metric: DOF-updates/s = sum_b E_b*Np_b * steps / seconds (Np = element nodes).
 --impl reference times the CPU oracle (a float64 numpy restatement of the
@@ -113,16 +120,34 @@ def rhs_bytes(op, nv, sizeof=8):
     return total
 
 
-def volume_kernel_bytes(op, nv, viscous, sizeof=8):
-    """Algorithmic bytes of k_volume: U, metrics, M^-1 (viscous lift), jumps in, lifts and residuals out."""
-    total = 0
+STAGES = ["traces", "face_flux", "lift", "volume", "face_visc", "finalize"]
+
+
+def stage_bytes(op, nv, split, sizeof=8):
+    """Algorithmic HBM bytes per launch of each RHS stage of the sum-factorised hex path
+    (every input read once, every output written once; the device buffers are float64 in both
+    precision modes)."""
+    out = dict.fromkeys(STAGES, 0)
+    visc = op.viscous
     for bp in op.plan.blocks:
-        per = nv * bp.Np + 10 * bp.Nq + nv * bp.Np
-        if viscous:
-            nq = max(fp.nq for fp in op.plan.faces.values())
-            per += bp.Np * bp.Np + bp.nlf * nq * 12 * 2 + nv * bp.Np
-        total += sizeof * bp.E * per
-    return total
+        E, Np, Nq, nlf = bp.E, bp.Np, bp.Nq, bp.nlf
+        nqf = max(fp.nq for fp in op.plan.faces.values())
+        out["traces"] += sizeof * E * (nv * Np + nlf * nqf * (nv + (16 if visc else 0)))
+        if visc:
+            out["lift"] += sizeof * E * (Np * Np + 2 * nlf * nqf * 12 + 12 * Np)
+        out["volume"] += sizeof * E * (nv * Np + 10 * Nq + (12 * Np if visc else 0) + (2 if split else 1) * nv * Np)
+        out["finalize"] += sizeof * E * (Np * Np + (2 if split else 1) * nv * Np + nlf * nqf * 2 * nv + 3 * nv * Np)
+    for fp in op.plan.faces.values():
+        out["face_flux"] += fp.F * (sizeof * fp.nq * (2 * nv + 4 + nv) + 8)
+        if visc:
+            out["face_visc"] += fp.F * sizeof * fp.nq * (2 * 4 + 2 * 12 + 2 * 12 + 4 + nv)
+    return out
+
+
+def build_integrator(jfs, op, args, wall_T):
+    pos = jfs.HybridPositivityLimiter(op)
+    limiter = jfs.HybridMOODSubcellLimiter(op, positivity=pos) if args.limiter == "mood" else pos
+    return limiter, jfs.HybridSSPRK3(op, cfl=0.3, limiter=limiter)
 
 
 def run_ours(args):
@@ -145,65 +170,85 @@ def run_ours(args):
     src = workload(args.scale)
     u, mu, farfield = freestream(3)
     solver = jfs.HybridCompressibleSolver(jfs.HybridMesh(src), polynomial_degree=args.degree, dynamic_viscosity=mu)
-    op = jfs.HybridNavierStokesOperator(solver)
+    modes = {"both": ["float64", "mixed"], "float64": ["float64"], "mixed": ["mixed"]}[args.precision]
+    base = jfs.HybridNavierStokesOperator(solver, precision=modes[0])
+    ops = {modes[0]: base}
+    for m in modes[1:]:
+        ops[m] = base.with_precision(m)
     bc = jfs.FarfieldWallBoundary(solver, farfield, wall_temperature=T_WALL / T_INF)
-    pos = jfs.HybridPositivityLimiter(op)
-    limiter = jfs.HybridMOODSubcellLimiter(op, positivity=pos) if args.limiter == "mood" else pos
-    integ = jfs.HybridSSPRK3(op, cfl=0.3, limiter=limiter)
+    runs = {m: build_integrator(jfs, ops[m], args, T_WALL / T_INF) for m in modes}
     U0 = solver.uniform_state_blocks(1.0, [u, 0.0, 0.0], 1.0)
-    U = {k: v.clone() for k, v in U0.items()}
-    dofs = sum(bp.E * bp.Np for bp in op.plan.blocks)
+    dofs = sum(bp.E * bp.Np for bp in base.plan.blocks)
     nv = solver.layout.number_of_variables
     setup_s = time.time() - t_setup
-    dt = integ.stable_dt(U, bc)
+    dt = runs[modes[0]][1].stable_dt(U0, bc)      # one fixed dt for every mode (same trajectory)
     torch.cuda.synchronize()
-    for _ in range(args.warmup):
-        integ.checked_step_inplace(U, dt, bc)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
+    results = {}
+    for m in modes:
+        limiter, integ = runs[m]
+        Uw = {k: v.clone() for k, v in U0.items()}
+        for _ in range(args.warmup):
+            integ.checked_step_inplace(Uw, dt, bc)
+        del Uw
+        U = {k: v.clone() for k, v in U0.items()}
         torch.cuda.synchronize()
-        start.record()
-        for _ in range(args.steps):
-            status = integ.checked_step_inplace(U, dt, bc)
-        stop.record()
-        torch.cuda.synchronize()
-    ms = start.elapsed_time(stop)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    valid, rmin, pmin = integ._status_tuple()
-    value = dofs * args.steps * world / (ms / 1e3)
-    troubled = None
-    if args.limiter == "mood":
-        flags = limiter.troubled(U)
-        troubled = int(sum(int(v.sum().item()) for v in flags.values()))
+        if world > 1:
+            dist.barrier()
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clocks:
+            torch.cuda.synchronize()
+            start.record()
+            for _ in range(args.steps):
+                integ.checked_step_inplace(U, dt, bc)
+            stop.record()
+            torch.cuda.synchronize()
+        ms = start.elapsed_time(stop)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        valid, rmin, pmin = integ._status_tuple()
+        troubled = None
+        if args.limiter == "mood":
+            flags = limiter.troubled(U)
+            troubled = int(sum(int(v.sum().item()) for v in flags.values()))
+        results[m] = dict(ms=ms, U=U, clocks=clocks.summary(), valid=valid, rho_min=rmin, p_min=pmin,
+                          troubled=troubled, value=dofs * args.steps * world / (ms / 1e3))
+    head = "mixed" if "mixed" in results else "float64"
+    op, (limiter, integ) = ops[head], runs[head]
+    R = results[head]
+    accuracy = None
+    if len(results) == 2:
+        a, b = results["mixed"]["U"], results["float64"]["U"]
+        num = sum(float(((a[k][..., 0] - b[k][..., 0]) ** 2).sum()) for k in a)
+        den = sum(float((b[k][..., 0] ** 2).sum()) for k in b)
+        accuracy = {"density_l2_rel_vs_plain": (num / den) ** 0.5, "after_steps": args.steps,
+                    "gate": 1e-6}
 
     # per-stage kernel durations of one RHS (CUDA events on the launching stream)
-    stage_ms = (ctypes.c_float * 5)()
-    st = op.native.state(op._blocks(U))
+    stage_ms = (ctypes.c_float * len(STAGES))()
+    st = op.native.state(op._blocks(R["U"]))
     for _ in range(3):
         N.check(N.lib().dgb_rhs_profile(op.native.handle, ctypes.byref(st), stage_ms, _stream_ptr()))
-    stages = dict(zip(["traces", "face_flux", "volume_lift", "face_visc", "finalize"], list(stage_ms)))
+    stages = dict(zip(STAGES, [float(x) for x in stage_ms]))
+    sbytes = stage_bytes(op, nv, split=True)
     dominant = max(stages, key=stages.get)
     pk, pk_kind = peaks()
     hbm = float(pk["hbm_gbs"])
-    vol_bytes = volume_kernel_bytes(op, nv, op.viscous)
-    achieved = vol_bytes / (stages["volume_lift"] / 1e3) / 1e9
+    achieved = sbytes[dominant] / (stages[dominant] / 1e3) / 1e9
     traffic = None
     tfile = ROOT / "profiles" / "traffic.json"
     if tfile.exists():
         try:
-            traffic = json.loads(tfile.read_text()).get("volume_lift_bytes_per_launch")
+            per_elem = json.loads(tfile.read_text()).get(dominant, {}).get("dram_bytes_per_element")
+            if per_elem:
+                traffic = per_elem * sum(bp.E for bp in op.plan.blocks)
         except Exception:
             traffic = None
 
     # end to end through the public API with host buffers: H2D state, step, D2H state
     host_in = {k: v.cpu().pin_memory() for k, v in U0.items()}
-    host_out = {k: torch.empty_like(v) .pin_memory() for k, v in host_in.items()}
+    host_out = {k: torch.empty_like(v).pin_memory() for k, v in host_in.items()}
     dev = {k: torch.empty_like(v) for k, v in U0.items()}
     e_steps = max(1, min(args.steps, 5))
     torch.cuda.synchronize()
@@ -223,39 +268,49 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.cpu_seconds)
-    # launches per checked step: per stage the five RHS stages (per block / face type),
-    # positivity and admissibility per block, one final admissibility reduction
+    # launches per checked step: per stage the RHS kernels (per block / face type), then the
+    # limiter and admissibility kernels
     nb, nf = len(op.plan.blocks), len(op.plan.faces)
-    # RHS: traces, lift (hex viscous), volume, finalize per block; face flux (+ viscous) per face type
     per_stage = nb * (4 if (op.native.sum_factorised and op.viscous) else 3) + nf * (2 if op.viscous else 1)
     if args.limiter == "mood":
         # troubled, subcell fv/update, positivity x2, blend per block; subcell faces per type; adm + final
         per_stage += nb * 6 + nf + nb + 1
     else:
         per_stage += nb * 2 + 1
+    E = int(sum(bp.E for bp in op.plan.blocks))
+    lim = "MOOD subcell FV (CWENO-Z) + positivity" if args.limiter == "mood" else "positivity limiter"
+    prec = ("mixed: float32 BR2-lift and volume arithmetic, float64 state, fluxes, limiters and reductions"
+            if head == "mixed" else "plain float64")
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"Mach-3 viscous sphere, O/H hex grid, {sum(bp.E for bp in op.plan.blocks)} "
-                               f"elements, P{args.degree} ({dofs} DOF), plain float64 SSP-RK3, "
-                               f"{'MOOD subcell FV (CWENO-Z) + positivity' if args.limiter == 'mood' else 'positivity limiter'}",
-                   "elements": int(sum(bp.E for bp in op.plan.blocks)), "degree": args.degree, "dofs": int(dofs),
+        "metric": METRIC, "value": R["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": R["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64" if head == "mixed" else "f64", "data": "synthetic",
+        "config": {"workload": f"Mach-3 viscous sphere, O/H hex grid, {E} elements, P{args.degree} ({dofs} DOF), "
+                               f"checked SSP-RK3 with {lim}, {prec}",
+                   "elements": E, "degree": args.degree, "dofs": int(dofs), "precision": head,
                    "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "inputs larger than L2 (state 0.5 GB, inverse mass 6.5 GB per pass)",
-                   "limiter": args.limiter, "troubled_elements_after": troubled, "setup_s": round(setup_s, 1)},
+                   "l2": "inputs larger than L2 (state 0.5 GB, inverse mass 6.6 GB per pass)",
+                   "limiter": args.limiter, "troubled_elements_after": R["troubled"], "setup_s": round(setup_s, 1)},
         "gpu_launches": per_stage * 3 * args.steps,
-        "step_status": {"valid": valid, "rho_min": rmin, "p_min": pmin, "dt": dt},
+        "step_status": {"valid": R["valid"], "rho_min": R["rho_min"], "p_min": R["p_min"], "dt": dt},
         "stage_ms": stages,
-        "roofline": {"bound": "hbm", "kernel": "volume_lift", "achieved": achieved, "peak": hbm,
+        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": hbm,
                      "unit": "GB/s", "frac": achieved / hbm, "peak_kind": pk_kind, "traffic": traffic,
-                     "dominant_stage": dominant, "algorithmic_bytes": vol_bytes,
+                     "algorithmic_bytes": sbytes[dominant],
+                     "stage_achieved_gbs": {k: sbytes[k] / (stages[k] / 1e3) / 1e9 if stages[k] > 0 else None
+                                            for k in STAGES},
                      "rhs_algorithmic_bytes": rhs_bytes(op, nv),
                      "rhs_achieved_gbs": rhs_bytes(op, nv) / (sum(stages.values()) / 1e3) / 1e9},
-        "clocks": clocks.summary(),
+        "clocks": R["clocks"],
         "e2e": {"value": dofs / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": state_bytes,
                 "d2h_bytes_per_step": state_bytes},
     }
+    if "float64" in results and head != "float64":
+        P = results["float64"]
+        line["plain"] = {"value": P["value"], "ms_per_step": P["ms"] / args.steps, "dtype": "f64",
+                         "clocks": P["clocks"], "valid": P["valid"]}
+    if accuracy:
+        line["accuracy"] = accuracy
     if cpu:
         line["cpu_baseline"] = cpu
     if rank == 0:
@@ -339,6 +394,10 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--limiter", default="mood", choices=["mood", "positivity"])
+    ap.add_argument("--precision", default="both", choices=["both", "mixed", "float64"],
+                    help="both: time the plain float64 step and the mixed step from the same state and dt; "
+                         "the mixed one is the headline value, the plain one and their density L2 "
+                         "difference ride along")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

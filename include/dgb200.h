@@ -61,6 +61,10 @@ typedef struct {
   double sensor_threshold;
   int limiter;                /* stage limiter of dgb_ssprk3_step: 0 none, 1 positivity, 2 MOOD */
   int reconstruction;         /* MOOD subcell faces: 0 constant, 1 tvd, 2 weno (CWENO-Z) */
+  int precision;              /* 0 float64 throughout; 1 mixed: float32 arithmetic and shared-memory
+                                 staging in the hexahedron lift and volume kernels (state, face
+                                 fluxes, limiters, reductions and the stage update stay float64);
+                                 needs the sum-factorised single-hexahedron-block path */
 } dgb_params;
 
 /* One element block (hybrid/geometry.py:139-203 metrics, precomputed by the host). */
@@ -200,8 +204,9 @@ int dgb_subcell_recompute(dgb_plan* plan, const dgb_state* base, const dgb_state
 /* Tracing (no reference counterpart; the reference only prints wall-clock progress,
  * run_hybrid_sphere.py:366-390): runs one dgb_rhs with CUDA events around each kernel
  * stage and writes the stage durations in milliseconds to host ms_out[DGB_RHS_STAGES]
- * (traces, face flux, volume+lift, viscous face flux, finalize).  Synchronises the stream. */
-enum { DGB_RHS_STAGES = 5 };
+ * (traces, face flux, BR2 lift, volume, viscous face flux, finalize; on the dense path the
+ * lift is part of the volume stage and its entry is 0).  Synchronises the stream. */
+enum { DGB_RHS_STAGES = 6 };
 int dgb_rhs_profile(dgb_plan* plan, const dgb_state* U, float* ms_out, void* stream);
 
 /* Allocation-free CFL time step for one element block.  No counterpart in the reference.
@@ -278,6 +283,37 @@ int dgb_chem_destroy(dgb_chem* chem);
  * nvars < 5 + ns is DGB_ERR_ARGUMENT (the reference raises ValueError). */
 int dgb_react_block(dgb_chem* chem, const double* U, double* out, int64_t num_elements, int num_nodes,
                     int nvars, double dt, const double* dt_per_element, void* stream);
+
+/* ---- Learned troubled-cell predictor (no reference counterpart) -----------------------
+ *
+ * A small MLP (8 features -> 64 -> 64 -> 64 -> 1, ReLU, sigmoid) that predicts from a stage's
+ * base state which elements the MOOD a-posteriori test (hybrid/limiter.py:285-300) will flag,
+ * so that they go to the subcell scheme without the failed high-order attempt.  The test
+ * stays the fallback and the judge.  Parameters are DGB_MLP_PARAMS floats in the order
+ * W1[8][64], b1[64], W2[64][64], b2[64], W3[64][64], b3[64], w4[64], b4; norm is the
+ * features' mean[8] then 1/std[8].  All arrays are device arrays. */
+enum { DGB_MLP_FEATURES = 8, DGB_MLP_PARAMS = 8961 };
+
+/* Features of every element of U, (sum of E, 8) float32 in block order. */
+int dgb_mlp_features(dgb_plan* plan, const dgb_state* U, float* features, void* stream);
+/* Inference with float16 weights and float32 accumulation: prob[n] and/or flag[n] = prob > threshold. */
+int dgb_mlp_infer(const void* weights_f16, const float* norm, const float* features, int64_t n, float threshold,
+                  float* prob, uint8_t* flag, void* stream);
+/* One Adam step (step >= 1) on the float32 weights over the samples features[index[0..batch)],
+ * labels 0/1, binary cross-entropy with positive samples weighted by pos_weight.  grad
+ * (DGB_MLP_PARAMS, zero on entry) is cleared again; weights_f16 (optional) receives the updated
+ * weights; loss (optional, device float) accumulates the batch loss. */
+int dgb_mlp_train_step(float* weights, float* grad, float* adam_m, float* adam_v, void* weights_f16,
+                       const float* norm, const float* features, const uint8_t* labels, const int* index,
+                       int batch, float pos_weight, float lr, int step, float* loss, void* stream);
+/* Use the predictor inside dgb_ssprk3_step's MOOD stages: mode 0 off, 1 learned (predicted
+ * elements skip the a-posteriori test and go to the subcell scheme), 2 evaluate (every element
+ * is tested and the step is the plain one; the prediction is only counted).  The weight and
+ * norm arrays must outlive their use. */
+int dgb_plan_set_predictor(dgb_plan* plan, const void* weights_f16, const float* norm, float threshold, int mode);
+/* Host int64[5]: [0] unused (0), [1] predicted, [2] missed (tested troubled but not predicted),
+ * [3] false positives and [4] hits (both counted in mode 2 only); reset clears them. */
+int dgb_plan_predictor_counts(dgb_plan* plan, int64_t* counts, int reset);
 
 /* ReactionMechanism.net_production_rates (hybrid/chemistry/mechanism.py:159-220) at
  * count independent samples, single temperature: rho (count, ns) and T (count) device

@@ -35,6 +35,7 @@ class Params(ctypes.Structure):
         ("sensor_threshold", c_double),
         ("limiter", c_int),
         ("reconstruction", c_int),
+        ("precision", c_int),
     ]
 
 

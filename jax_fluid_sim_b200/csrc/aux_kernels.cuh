@@ -142,14 +142,44 @@ __global__ void __launch_bounds__(kThreads) k_positivity(const DevPlan P, const 
   }
 }
 
+// Learned-predictor hooks of the troubled-cell kernels.  mode 1 (learned): an element whose
+// predicted flag is set goes to the subcell scheme without the a-posteriori test; mode 2
+// (evaluate): every element is tested and the flag is the test's, the prediction is only
+// counted.  counts: [1] predicted, [2] missed (tested troubled, not predicted),
+// [3] false positive and [4] hit (mode 2 only).
+struct PredictArgs {
+  const uint8_t* pred;
+  int mode;
+  unsigned long long* counts;
+};
+
+__device__ __forceinline__ bool predicted_skip(const PredictArgs& pa, int e, uint8_t* flag_out) {
+  if (pa.mode != 1 || !pa.pred || !pa.pred[e]) return false;
+  if (threadIdx.x == 0) {
+    if (flag_out) flag_out[e] = 1;
+    if (pa.counts) atomicAdd(pa.counts + 1, 1ULL);
+  }
+  return true;
+}
+
+__device__ __forceinline__ void count_prediction(const PredictArgs& pa, int e, bool detected) {
+  if (!pa.counts || !pa.pred || pa.mode == 0) return;
+  const bool pr = pa.pred[e] != 0;
+  if (pa.mode == 2 && pr) atomicAdd(pa.counts + 1, 1ULL);
+  if (detected && !pr) atomicAdd(pa.counts + 2, 1ULL);
+  if (pa.mode == 2 && pr && !detected) atomicAdd(pa.counts + 3, 1ULL);
+  if (pa.mode == 2 && pr && detected) atomicAdd(pa.counts + 4, 1ULL);
+}
+
 template <int NV>
 __global__ void __launch_bounds__(kThreads) k_troubled(const DevPlan P, const StatePtrs S, int b, const LimiterConst L,
-                                                      double* sensor_out, uint8_t* flag_out) {
+                                                      double* sensor_out, uint8_t* flag_out, const PredictArgs pa) {
   extern __shared__ double smem[];
   __shared__ double mean[NV];
   __shared__ double red[4][kThreads / 32];
   const BlockDev& B = P.blk[b];
   const int e = blockIdx.x;
+  if (predicted_skip(pa, e, flag_out)) return;
   const int Np = B.Np, Nq = B.Nq;
   const int Nt = Np + Nq + B.Ns;
   double* U = smem;
@@ -218,8 +248,10 @@ __global__ void __launch_bounds__(kThreads) k_troubled(const DevPlan P, const St
       const double r0 = h0 / fmax(s0, 1.0e-12), r1 = h1 / fmax(s1, 1.0e-12);
       value = (isnan(r0) || isnan(r1)) ? NAN : fmax(r0, r1);
     }
+    const bool detected = (value > L.sensor_threshold) || any_bad;
     if (sensor_out) sensor_out[e] = value;
-    if (flag_out) flag_out[e] = (uint8_t)((value > L.sensor_threshold) || any_bad);
+    if (flag_out) flag_out[e] = (uint8_t)detected;
+    count_prediction(pa, e, detected);
   }
 }
 

@@ -9,6 +9,7 @@
 
 #include "aux_kernels.cuh"
 #include "hex_kernels.cuh"
+#include "mlp_kernels.cuh"
 #include "mood_kernels.cuh"
 
 using namespace dgb;
@@ -65,6 +66,16 @@ struct dgb_plan {
   bool sub_face_set[2] = {false, false};
   bool mood_ready = false;
   uint8_t* flags[DGB_MAX_BLOCKS] = {nullptr, nullptr, nullptr};
+  // learned troubled-cell predictor (dgb_plan_set_predictor)
+  int pred_mode = 0;
+  const __half* pred_w16 = nullptr;
+  const float* pred_norm = nullptr;
+  float pred_threshold = 0.5f;
+  float* pred_stats[DGB_MAX_BLOCKS] = {nullptr, nullptr, nullptr};
+  float** pred_stats_dev = nullptr;
+  float* pred_feat = nullptr;
+  uint8_t* pred_flags[DGB_MAX_BLOCKS] = {nullptr, nullptr, nullptr};
+  unsigned long long* pred_counts = nullptr;
   double* unl[DGB_MAX_BLOCKS] = {nullptr, nullptr, nullptr};
   double* eul[DGB_MAX_BLOCKS] = {nullptr, nullptr, nullptr};
   double* vis[DGB_MAX_BLOCKS] = {nullptr, nullptr, nullptr};
@@ -113,13 +124,14 @@ int prepare(K kernel, size_t smem) {
 int blocks_for(long n, int per) { return (int)((n + per - 1) / per); }
 
 // ------------------------------------------------------------------ RHS pipeline
-template <int P, int NV, bool SPLIT>
+template <int P, int NV, bool SPLIT, typename R>
 int run_rhs_hex(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStream_t st, cudaEvent_t* ev) {
   using L = HexSmem<P, NV>;
+  using LR = HexSmem<P, NV, R>;
   const DevPlan& D = p->dev;
   const int E = D.blk[0].E;
-  const size_t sm_tr = sizeof(double) * (size_t)L::TRACES, sm_li = sizeof(double) * (size_t)L::LIFT;
-  const size_t sm_vo = sizeof(double) * (size_t)L::template VOLUME<SPLIT>, sm_fi = sizeof(double) * (size_t)L::FINAL;
+  const size_t sm_tr = sizeof(double) * (size_t)L::TRACES, sm_li = sizeof(R) * (size_t)LR::LIFT;
+  const size_t sm_vo = sizeof(R) * (size_t)LR::template VOLUME<SPLIT>, sm_fi = sizeof(double) * (size_t)L::FINAL;
   int rc;
   if (ev) CK(cudaEventRecord(ev[0], st));
   if ((rc = prepare(k_hex_traces<P, NV>, sm_tr))) return rc;
@@ -128,29 +140,36 @@ int run_rhs_hex(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStre
   k_face_flux<NV><<<blocks_for((long)D.face[1].F * D.face[1].nq, kThreads), kThreads, 0, st>>>(D, S, 1);
   if (ev) CK(cudaEventRecord(ev[2], st));
   if (D.viscous) {
-    if ((rc = prepare(k_hex_lift<P, NV>, sm_li))) return rc;
-    k_hex_lift<P, NV><<<E, kThreads, sm_li, st>>>(D, 0, p->hex_tables, p->hex_codes, p->hex_lift);
+    if ((rc = prepare(k_hex_lift<P, NV, R>, sm_li))) return rc;
+    k_hex_lift<P, NV, R><<<E, kThreads, sm_li, st>>>(D, 0, p->hex_tables, p->hex_codes, p->hex_lift);
   }
-  if ((rc = prepare(k_hex_volume<P, NV, SPLIT>, sm_vo))) return rc;
-  k_hex_volume<P, NV, SPLIT><<<E, kThreads, sm_vo, st>>>(D, S, 0, p->hex_tables, p->hex_lift);
   if (ev) CK(cudaEventRecord(ev[3], st));
+  if ((rc = prepare(k_hex_volume<P, NV, SPLIT, R>, sm_vo))) return rc;
+  k_hex_volume<P, NV, SPLIT, R><<<E, kThreads, sm_vo, st>>>(D, S, 0, p->hex_tables, p->hex_lift);
+  if (ev) CK(cudaEventRecord(ev[4], st));
   if (D.viscous)
     k_face_visc<NV><<<blocks_for((long)D.face[1].F * D.face[1].nq, kThreads), kThreads, 0, st>>>(D, 1);
-  if (ev) CK(cudaEventRecord(ev[4], st));
+  if (ev) CK(cudaEventRecord(ev[5], st));
   if ((rc = prepare(k_hex_finalize<P, NV, SPLIT>, sm_fi))) return rc;
   k_hex_finalize<P, NV, SPLIT><<<E, kThreads, sm_fi, st>>>(D, S, 0, p->hex_tables, p->hex_codes, A);
-  if (ev) CK(cudaEventRecord(ev[5], st));
+  if (ev) CK(cudaEventRecord(ev[6], st));
   CK(cudaGetLastError());
   return DGB_OK;
 }
 
-template <int NV, bool SPLIT>
+template <int NV, bool SPLIT, typename R>
 int run_rhs_hex_deg(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStream_t st, cudaEvent_t* ev) {
   switch (p->dev.degree) {
-    case 1: return run_rhs_hex<1, NV, SPLIT>(p, S, A, st, ev);
-    case 2: return run_rhs_hex<2, NV, SPLIT>(p, S, A, st, ev);
-    default: return run_rhs_hex<3, NV, SPLIT>(p, S, A, st, ev);
+    case 1: return run_rhs_hex<1, NV, SPLIT, R>(p, S, A, st, ev);
+    case 2: return run_rhs_hex<2, NV, SPLIT, R>(p, S, A, st, ev);
+    default: return run_rhs_hex<3, NV, SPLIT, R>(p, S, A, st, ev);
   }
+}
+
+template <int NV, bool SPLIT>
+int run_rhs_hex_prec(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStream_t st, cudaEvent_t* ev) {
+  return p->prm.precision == 1 ? run_rhs_hex_deg<NV, SPLIT, float>(p, S, A, st, ev)
+                               : run_rhs_hex_deg<NV, SPLIT, double>(p, S, A, st, ev);
 }
 
 // events: optional array of DGB_RHS_STAGES + 1 events recorded around the stages
@@ -159,7 +178,7 @@ int run_rhs(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStream_t
   const DevPlan& P = p->dev;
   int rc;
   const bool split = !A.stage || A.out_vis[0] != nullptr;
-  if (p->hex) return split ? run_rhs_hex_deg<NV, true>(p, S, A, st, ev) : run_rhs_hex_deg<NV, false>(p, S, A, st, ev);
+  if (p->hex) return split ? run_rhs_hex_prec<NV, true>(p, S, A, st, ev) : run_rhs_hex_prec<NV, false>(p, S, A, st, ev);
   if (ev) CK(cudaEventRecord(ev[0], st));
   for (int b = 0; b < P.nblocks; ++b) {
     if ((rc = prepare(k_traces<NV>, p->smem_traces[b]))) return rc;
@@ -170,21 +189,22 @@ int run_rhs(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStream_t
     if (p->face_present[ft])
       k_face_flux<NV><<<blocks_for((long)P.face[ft].F * P.face[ft].nq, kThreads), kThreads, 0, st>>>(P, S, ft);
   if (ev) CK(cudaEventRecord(ev[2], st));
+  if (ev) CK(cudaEventRecord(ev[3], st));     // the dense k_volume does the BR2 lift itself
   for (int b = 0; b < P.nblocks; ++b) {
     if ((rc = prepare(k_volume<NV>, p->smem_volume[b]))) return rc;
     k_volume<NV><<<P.blk[b].E, kThreads, p->smem_volume[b], st>>>(P, S, b);
   }
-  if (ev) CK(cudaEventRecord(ev[3], st));
+  if (ev) CK(cudaEventRecord(ev[4], st));
   if (P.viscous)
     for (int ft = 0; ft < 2; ++ft)
       if (p->face_present[ft])
         k_face_visc<NV><<<blocks_for((long)P.face[ft].F * P.face[ft].nq, kThreads), kThreads, 0, st>>>(P, ft);
-  if (ev) CK(cudaEventRecord(ev[4], st));
+  if (ev) CK(cudaEventRecord(ev[5], st));
   for (int b = 0; b < P.nblocks; ++b) {
     if ((rc = prepare(k_finalize<NV>, p->smem_final[b]))) return rc;
     k_finalize<NV><<<P.blk[b].E, kThreads, p->smem_final[b], st>>>(P, S, b, A);
   }
-  if (ev) CK(cudaEventRecord(ev[5], st));
+  if (ev) CK(cudaEventRecord(ev[6], st));
   CK(cudaGetLastError());
   return DGB_OK;
 }
@@ -200,11 +220,13 @@ int run_positivity_hex(dgb_plan* p, const StatePtrs& S, cudaStream_t st) {
 }
 
 template <int P, int NV>
-int run_troubled_hex(dgb_plan* p, const StatePtrs& S, double* sensor, uint8_t* flags, cudaStream_t st) {
+int run_troubled_hex(dgb_plan* p, const StatePtrs& S, double* sensor, uint8_t* flags, const PredictArgs& pa,
+                     cudaStream_t st) {
   const size_t sm = sizeof(double) * (size_t)hex_troubled_smem<P, NV>();
   int rc;
   if ((rc = prepare(k_hex_troubled<P, NV>, sm))) return rc;
-  k_hex_troubled<P, NV><<<p->dev.blk[0].E, kThreads, sm, st>>>(p->dev, S, 0, p->hex_tables, p->lim, sensor, flags);
+  k_hex_troubled<P, NV><<<p->dev.blk[0].E, kThreads, sm, st>>>(p->dev, S, 0, p->hex_tables, p->lim, sensor, flags,
+                                                               pa);
   CK(cudaGetLastError());
   return DGB_OK;
 }
@@ -254,21 +276,27 @@ int run_stable_dt(dgb_plan* p, const StatePtrs& S, double cfl, double* dt_out, c
 }
 
 template <int NV>
-int run_troubled(dgb_plan* p, const StatePtrs& S, double* const* sensor, uint8_t* const* flags, cudaStream_t st) {
+int run_troubled(dgb_plan* p, const StatePtrs& S, double* const* sensor, uint8_t* const* flags, cudaStream_t st,
+                 bool predicted = false) {
   int rc;
+  auto pargs = [&](int b) {
+    PredictArgs pa{nullptr, 0, nullptr};
+    if (predicted && p->pred_mode) pa = PredictArgs{p->pred_flags[b], p->pred_mode, p->pred_counts};
+    return pa;
+  };
   if (p->hex) {
     double* so = sensor ? sensor[0] : nullptr;
     uint8_t* fo = flags ? flags[0] : nullptr;
     switch (p->dev.degree) {
-      case 1: return run_troubled_hex<1, NV>(p, S, so, fo, st);
-      case 2: return run_troubled_hex<2, NV>(p, S, so, fo, st);
-      default: return run_troubled_hex<3, NV>(p, S, so, fo, st);
+      case 1: return run_troubled_hex<1, NV>(p, S, so, fo, pargs(0), st);
+      case 2: return run_troubled_hex<2, NV>(p, S, so, fo, pargs(0), st);
+      default: return run_troubled_hex<3, NV>(p, S, so, fo, pargs(0), st);
     }
   }
   for (int b = 0; b < p->dev.nblocks; ++b) {
     if ((rc = prepare(k_troubled<NV>, p->smem_troubled[b]))) return rc;
     k_troubled<NV><<<p->dev.blk[b].E, kThreads, p->smem_troubled[b], st>>>(
-        p->dev, S, b, p->lim, sensor ? sensor[b] : nullptr, flags ? flags[b] : nullptr);
+        p->dev, S, b, p->lim, sensor ? sensor[b] : nullptr, flags ? flags[b] : nullptr, pargs(b));
   }
   CK(cudaGetLastError());
   return DGB_OK;
@@ -311,9 +339,34 @@ int run_subcell(dgb_plan* p, const StatePtrs& cur, double* const* cand, double* 
 template <int NV>
 int run_positivity(dgb_plan* p, const StatePtrs& S, cudaStream_t st);
 template <int NV>
-int run_troubled(dgb_plan* p, const StatePtrs& S, double* const* sensor, uint8_t* const* flags, cudaStream_t st);
+int run_troubled(dgb_plan* p, const StatePtrs& S, double* const* sensor, uint8_t* const* flags, cudaStream_t st,
+                 bool predicted);
+template <int NV>
+int run_predict(dgb_plan* p, const StatePtrs& S, cudaStream_t st);
 template <int NV>
 int run_admissibility(dgb_plan* p, const StatePtrs& S, dgb_status* status, int combine, cudaStream_t st);
+
+// Features of the stage's base state and the predictor's flags (learned MOOD).
+template <int NV>
+int run_predict(dgb_plan* p, const StatePtrs& S, cudaStream_t st) {
+  const DevPlan& P = p->dev;
+  constexpr int per = kThreads / 32;                // elements per CTA (one warp each)
+  for (int b = 0; b < P.nblocks; ++b) {
+    const size_t sm = sizeof(double) * 2 * (size_t)P.blk[b].Np * per;
+    k_elem_stats<NV><<<blocks_for(P.blk[b].E, per), kThreads, sm, st>>>(P, S, b, p->pred_stats[b]);
+  }
+  long off = 0;
+  for (int b = 0; b < P.nblocks; ++b) {
+    float* feat = p->pred_feat + (size_t)off * kMlpIn;
+    k_mlp_features<<<blocks_for(P.blk[b].E, kThreads), kThreads, 0, st>>>(P, b, p->pred_stats_dev, feat);
+    if (p->pred_w16)
+      k_mlp_infer<<<blocks_for(P.blk[b].E, 128), 128, 0, st>>>(p->pred_w16, p->pred_norm, feat, P.blk[b].E,
+                                                               p->pred_threshold, nullptr, p->pred_flags[b]);
+    off += P.blk[b].E;
+  }
+  CK(cudaGetLastError());
+  return DGB_OK;
+}
 
 // MOOD branch of checked_step (hybrid/time_integration.py:450-554)
 template <int NV>
@@ -345,8 +398,10 @@ int run_step_mood(dgb_plan* p, const StatePtrs& U0, double dt, dgb_status* statu
       A.euler[b] = p->eul[b];
       A.out_vis[b] = p->vis[b];
     }
+    // the predictor reads the stage's base state: it decides before the high-order update
+    if (p->pred_mode && (rc = run_predict<NV>(p, *cur[s], st))) return rc;
     if ((rc = run_rhs<NV>(p, *cur[s], A, st))) return rc;
-    if ((rc = run_troubled<NV>(p, UNL, nullptr, p->flags, st))) return rc;
+    if ((rc = run_troubled<NV>(p, UNL, nullptr, p->flags, st, true))) return rc;
     if ((rc = run_subcell<NV>(p, *cur[s], p->eul, p->vis, dt, F, p->rec, st))) return rc;
     if ((rc = run_positivity<NV>(p, REC, st))) return rc;
     for (int b = 0; b < P.nblocks; ++b) {
@@ -388,6 +443,29 @@ int run_step(dgb_plan* p, const StatePtrs& U0, double dt, dgb_status* status, cu
     if (p->prm.limiter == 1 && (rc = run_positivity<NV>(p, *dst[s], st))) return rc;
     if ((rc = run_admissibility<NV>(p, *dst[s], status, s > 0, st))) return rc;
   }
+  return DGB_OK;
+}
+
+int ensure_predictor_buffers(dgb_plan* p) {
+  if (p->pred_feat) return DGB_OK;
+  long total = 0;
+  double* d;
+  int rc;
+  for (int b = 0; b < p->dev.nblocks; ++b) {
+    const int E = p->dev.blk[b].E;
+    if ((rc = alloc(p, ((size_t)E * kMlpStats + 1) / 2, &d))) return rc;
+    p->pred_stats[b] = reinterpret_cast<float*>(d);
+    if ((rc = alloc(p, ((size_t)E + 7) / 8, &d))) return rc;
+    p->pred_flags[b] = reinterpret_cast<uint8_t*>(d);
+    total += E;
+  }
+  if ((rc = alloc(p, ((size_t)total * kMlpIn + 1) / 2, &d))) return rc;
+  p->pred_feat = reinterpret_cast<float*>(d);
+  if ((rc = alloc(p, DGB_MAX_BLOCKS, &d))) return rc;
+  p->pred_stats_dev = reinterpret_cast<float**>(d);
+  CK(cudaMemcpy(p->pred_stats_dev, p->pred_stats, sizeof(p->pred_stats), cudaMemcpyHostToDevice));
+  if ((rc = alloc(p, 8, &d))) return rc;
+  p->pred_counts = reinterpret_cast<unsigned long long*>(d);
   return DGB_OK;
 }
 
@@ -462,6 +540,7 @@ int dgb_plan_create(const dgb_params* prm, dgb_plan** out) {
   if (prm->degree < 1 || prm->degree > 3) return fail(DGB_ERR_ARGUMENT, "Only P1, P2, and P3 are currently implemented");
   if (prm->nvars != 5 && prm->nvars != 16) return fail(DGB_ERR_UNSUPPORTED, "nvars must be 5 or 16");
   if (prm->num_blocks < 1 || prm->num_blocks > DGB_MAX_BLOCKS) return fail(DGB_ERR_ARGUMENT, "num_blocks out of range");
+  if (prm->precision != 0 && prm->precision != 1) return fail(DGB_ERR_ARGUMENT, "precision must be 0 or 1");
   if (prm->n_inlet > DGB_MAX_TAGS || prm->n_wall > DGB_MAX_TAGS || prm->n_no_slip > DGB_MAX_TAGS ||
       prm->n_slip > DGB_MAX_TAGS)
     return fail(DGB_ERR_ARGUMENT, "too many boundary tags");
@@ -479,8 +558,8 @@ int dgb_plan_create(const dgb_params* prm, dgb_plan** out) {
 int dgb_plan_update_params(dgb_plan* p, const dgb_params* prm) {
   if (!p || !prm) return fail(DGB_ERR_ARGUMENT, "null argument");
   if (prm->degree != p->dev.degree || prm->nvars != p->dev.nv || prm->num_blocks != p->dev.nblocks ||
-      prm->viscous != p->dev.viscous)
-    return fail(DGB_ERR_ARGUMENT, "degree, nvars, blocks and viscous flag are fixed for a plan");
+      prm->viscous != p->dev.viscous || prm->precision != p->prm.precision)
+    return fail(DGB_ERR_ARGUMENT, "degree, nvars, blocks, viscous flag and precision are fixed for a plan");
   if (prm->n_inlet > DGB_MAX_TAGS || prm->n_wall > DGB_MAX_TAGS || prm->n_no_slip > DGB_MAX_TAGS ||
       prm->n_slip > DGB_MAX_TAGS)
     return fail(DGB_ERR_ARGUMENT, "too many boundary tags");
@@ -617,6 +696,8 @@ int dgb_plan_finalize(dgb_plan* p) {
   if (!p) return fail(DGB_ERR_ARGUMENT, "null plan");
   const int NV = p->dev.nv;
   int rc;
+  if (p->prm.precision == 1 && !p->hex)
+    return fail(DGB_ERR_UNSUPPORTED, "mixed precision needs the sum-factorised single-hexahedron-block path");
   for (int b = 0; b < p->dev.nblocks; ++b)
     if (!p->block_set[b]) return fail(DGB_ERR_ARGUMENT, "block descriptor missing");
   for (int ft = 0; ft < 2; ++ft) {
@@ -786,6 +867,81 @@ int dgb_subcell_recompute(dgb_plan* p, const dgb_state* base, const dgb_state* c
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   return p->dev.nv == 5 ? run_subcell_api<5>(p, base, cand, dt, arhs, troubled, out, st)
                         : run_subcell_api<16>(p, base, cand, dt, arhs, troubled, out, st);
+}
+
+int dgb_mlp_features(dgb_plan* p, const dgb_state* U, float* features, void* stream) {
+  int rc;
+  if ((rc = check_ready(p)) || (rc = check_state(p, U, "U"))) return rc;
+  if (!features) return fail(DGB_ERR_ARGUMENT, "features is null");
+  if ((rc = ensure_predictor_buffers(p))) return rc;
+  const StatePtrs S = to_ptrs(U);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const __half* keep = p->pred_w16;
+  p->pred_w16 = nullptr;            // features only
+  rc = p->dev.nv == 5 ? run_predict<5>(p, S, st) : run_predict<16>(p, S, st);
+  p->pred_w16 = keep;
+  if (rc) return rc;
+  long total = 0;
+  for (int b = 0; b < p->dev.nblocks; ++b) total += p->dev.blk[b].E;
+  CK(cudaMemcpyAsync(features, p->pred_feat, sizeof(float) * (size_t)total * kMlpIn, cudaMemcpyDeviceToDevice, st));
+  return DGB_OK;
+}
+
+int dgb_mlp_infer(const void* w16, const float* norm, const float* features, int64_t n, float threshold, float* prob,
+                  uint8_t* flag, void* stream) {
+  if (!w16 || !norm || !features) return fail(DGB_ERR_ARGUMENT, "null argument");
+  if (n < 0) return fail(DGB_ERR_ARGUMENT, "negative count");
+  if (n == 0) return DGB_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  k_mlp_infer<<<blocks_for(n, 128), 128, 0, st>>>(static_cast<const __half*>(w16), norm, features, n, threshold, prob,
+                                                  flag);
+  CK(cudaGetLastError());
+  return DGB_OK;
+}
+
+int dgb_mlp_train_step(float* w, float* grad, float* m, float* v, void* w16, const float* norm, const float* features,
+                       const uint8_t* labels, const int* index, int batch, float pos_weight, float lr, int step,
+                       float* loss, void* stream) {
+  if (!w || !grad || !m || !v || !norm || !features || !labels || !index) return fail(DGB_ERR_ARGUMENT, "null argument");
+  if (batch < 1 || step < 1) return fail(DGB_ERR_ARGUMENT, "batch and step must be >= 1");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t sm = sizeof(float) * (size_t)kMlpTrainSmemFloats;
+  int rc;
+  if ((rc = prepare(k_mlp_train, sm))) return rc;
+  k_mlp_train<<<blocks_for(batch, kMlpChunk), kMlpTrainThreads, sm, st>>>(w, norm, features, labels, index, batch,
+                                                                         pos_weight, grad, loss);
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.f / (1.f - powf(b1, (float)step)), c2 = 1.f / (1.f - powf(b2, (float)step));
+  k_mlp_adam<<<blocks_for(kMlpParams, 256), 256, 0, st>>>(w, grad, m, v, static_cast<__half*>(w16), lr, b1, b2, 1e-8f,
+                                                          c1, c2);
+  CK(cudaGetLastError());
+  return DGB_OK;
+}
+
+int dgb_plan_set_predictor(dgb_plan* p, const void* w16, const float* norm, float threshold, int mode) {
+  int rc;
+  if ((rc = check_ready(p))) return rc;
+  if (mode < 0 || mode > 2) return fail(DGB_ERR_ARGUMENT, "mode must be 0 (off), 1 (learned) or 2 (evaluate)");
+  if (mode && (!w16 || !norm)) return fail(DGB_ERR_ARGUMENT, "weights and normalisation are needed");
+  if (mode && !p->mood_ready) return fail(DGB_ERR_ARGUMENT, "the predictor feeds MOOD: call dgb_plan_enable_mood first");
+  if (mode && (rc = ensure_predictor_buffers(p))) return rc;
+  p->pred_mode = mode;
+  p->pred_w16 = static_cast<const __half*>(w16);
+  p->pred_norm = norm;
+  p->pred_threshold = threshold;
+  return DGB_OK;
+}
+
+int dgb_plan_predictor_counts(dgb_plan* p, int64_t* out, int reset) {
+  int rc;
+  if ((rc = check_ready(p))) return rc;
+  if (!out) return fail(DGB_ERR_ARGUMENT, "out is null");
+  if ((rc = ensure_predictor_buffers(p))) return rc;
+  unsigned long long h[5];
+  CK(cudaMemcpy(h, p->pred_counts, sizeof(h), cudaMemcpyDeviceToHost));
+  for (int k = 0; k < 5; ++k) out[k] = (int64_t)h[k];
+  if (reset) CK(cudaMemset(p->pred_counts, 0, sizeof(h)));
+  return DGB_OK;
 }
 
 int dgb_rhs_profile(dgb_plan* p, const dgb_state* U, float* ms_out, void* stream) {

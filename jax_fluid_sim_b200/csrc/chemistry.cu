@@ -600,14 +600,15 @@ int dgb_chem_destroy(dgb_chem* chem) {
 
 int dgb_react_block(dgb_chem* chem, const double* U, double* out, int64_t num_elements, int num_nodes, int nvars,
                     double dt, const double* dt_per_element, void* stream) {
-  if (!chem || !U || !out) return fail(DGB_ERR_ARGUMENT, "null argument");
+  if (!chem) return fail(DGB_ERR_ARGUMENT, "null argument");
   const Tables& M = chem->tables;
   if (nvars < 5 + M.ns)
     return fail(DGB_ERR_ARGUMENT, "State has " + std::to_string(nvars) + " variables; expected at least " +
                                       std::to_string(5 + M.ns) + " for reacting mixture.");
   if (num_elements < 0 || num_nodes < 0) return fail(DGB_ERR_ARGUMENT, "negative block size");
   const long long nodes = (long long)num_elements * num_nodes;
-  if (nodes == 0) return DGB_OK;
+  if (nodes == 0) return DGB_OK;                    // an empty block needs no buffers
+  if (!U || !out) return fail(DGB_ERR_ARGUMENT, "null argument");
   if ((nodes + kThreads - 1) / kThreads > 0x7fffffffLL) return fail(DGB_ERR_ARGUMENT, "block too large");
   cudaStream_t st = (cudaStream_t)stream;
   return M.ns == 11 ? launch_react<11>(M, U, out, nodes, num_nodes, nvars, dt, dt_per_element, st)

@@ -16,19 +16,25 @@
 // through a per-trace-code permutation, so the face-point kernels and buffers are
 // shared with the generic path (dg_kernels.cuh).
 #pragma once
+#include "aux_kernels.cuh"
 #include "dg_kernels.cuh"
 
 namespace dgb {
 
-struct HexTables {
+template <typename R>
+struct HexTablesT {
   // volume Gauss points (Q) and face Gauss points (QF); nodes in 1-D order (0, 1, interior)
-  double bq[5 * 4], dq[5 * 4];     // [Q][N]
-  double bqT[4 * 5], dqT[4 * 5];   // [N][Q]
-  double bf[4 * 4], df[4 * 4];     // [QF][N]
-  double bfT[4 * 4];               // [N][QF]
-  double d0[4], d1[4];             // 1-D basis derivatives at xi = 0 and xi = 1
+  R bq[5 * 4], dq[5 * 4];          // [Q][N]
+  R bqT[4 * 5], dqT[4 * 5];        // [N][Q]
+  R bf[4 * 4], df[4 * 4];          // [QF][N]
+  R bfT[4 * 4];                    // [N][QF]
+  R d0[4], d1[4];                  // 1-D basis derivatives at xi = 0 and xi = 1
   int lex2node[64];                // lexicographic (x fastest) -> element node index
 };
+using HexTables = HexTablesT<double>;
+constexpr int kHexTableValues = 4 * 20 + 3 * 16 + 2 * 4;   // reals before lex2node
+static_assert(offsetof(HexTablesT<double>, lex2node) == kHexTableValues * sizeof(double), "table layout");
+static_assert(offsetof(HexTablesT<float>, lex2node) == kHexTableValues * sizeof(float), "table layout");
 
 struct HexCodes {
   const uint8_t* perm;   // [codes][QF*QF]: owner face-point order -> canonical face grid index
@@ -64,21 +70,21 @@ __device__ __forceinline__ int axis_stride(int a) { return a == 0 ? 1 : (a == 1 
 // at stride `stride` between consecutive entries) keeps its inputs and the (OUT x IN) matrix in
 // registers and produces the whole output line.  lines = number of lines; a line's first input
 // sits at in_base(line), its first output at out_base(line); outputs also at stride ostride.
-template <int IN, int OUT, bool ACC, typename InBase, typename OutBase>
-__device__ __forceinline__ void pencil(const double* in, double* out, const double* M, int lines, int istride,
-                                       int ostride, InBase in_base, OutBase out_base) {
-  double m[OUT * IN];
+template <int IN, int OUT, bool ACC, typename T, typename InBase, typename OutBase>
+__device__ __forceinline__ void pencil(const T* in, T* out, const T* M, int lines, int istride, int ostride,
+                                       InBase in_base, OutBase out_base) {
+  T m[OUT * IN];
 #pragma unroll
   for (int k = 0; k < OUT * IN; ++k) m[k] = M[k];
   for (int line = threadIdx.x; line < lines; line += blockDim.x) {
-    const double* src = in + in_base(line);
-    double x[IN];
+    const T* src = in + in_base(line);
+    T x[IN];
 #pragma unroll
     for (int i = 0; i < IN; ++i) x[i] = src[i * istride];
-    double* dst = out + out_base(line);
+    T* dst = out + out_base(line);
 #pragma unroll
     for (int o = 0; o < OUT; ++o) {
-      double s = 0.0;
+      T s = T(0);
 #pragma unroll
       for (int i = 0; i < IN; ++i) s += m[o * IN + i] * x[i];
       if (ACC) dst[o * ostride] += s; else dst[o * ostride] = s;
@@ -87,9 +93,8 @@ __device__ __forceinline__ void pencil(const double* in, double* out, const doub
 }
 
 // out[c][oz][oy][ox] (+)= sum Mz[oz][iz] My[oy][iy] Mx[ox][ix] in[c][iz][iy][ix]
-template <int C, int IX, int IY, int IZ, int OX, int OY, int OZ, bool ACC>
-__device__ __forceinline__ void tensor3(const double* in, double* out, double* t1, double* t2, const double* Mx,
-                                        const double* My, const double* Mz) {
+template <int C, int IX, int IY, int IZ, int OX, int OY, int OZ, bool ACC, typename T>
+__device__ __forceinline__ void tensor3(const T* in, T* out, T* t1, T* t2, const T* Mx, const T* My, const T* Mz) {
   // x: lines (c, iz, iy), contiguous inputs; t1[c][iz][iy][ox]
   pencil<IX, OX, false>(in, t1, Mx, C * IZ * IY, 1, 1, [](int l) { return l * IX; }, [](int l) { return l * OX; });
   __syncthreads();
@@ -106,8 +111,8 @@ __device__ __forceinline__ void tensor3(const double* in, double* out, double* t
 }
 
 // 2-D: out[c][k2][k1] = sum M2[k2][j2] M1[k1][j1] in[c][j2][j1]
-template <int C, int J1, int J2, int K1, int K2>
-__device__ __forceinline__ void tensor2(const double* in, double* out, double* t, const double* M1, const double* M2) {
+template <int C, int J1, int J2, int K1, int K2, typename T>
+__device__ __forceinline__ void tensor2(const T* in, T* out, T* t, const T* M1, const T* M2) {
   pencil<J1, K1, false>(in, t, M1, C * J2, 1, 1, [](int l) { return l * J1; }, [](int l) { return l * K1; });
   __syncthreads();
   pencil<J2, K2, false>(t, out, M2, C * K1, K1, K1,
@@ -117,8 +122,8 @@ __device__ __forceinline__ void tensor2(const double* in, double* out, double* t
 }
 
 // Gather the N^2 slab of face (a0, end) from lexicographic nodal data X[c][N^3] into slab[c][j2][j1].
-template <int C, int N>
-__device__ __forceinline__ void face_slab(const double* X, double* slab, int a0, int end, int a1, int a2) {
+template <int C, int N, typename T>
+__device__ __forceinline__ void face_slab(const T* X, T* slab, int a0, int end, int a1, int a2) {
   for (int idx = threadIdx.x; idx < C * N * N; idx += blockDim.x) {
     const int j1 = idx % N, j2 = (idx / N) % N, c = idx / (N * N);
     // 1-D node 0 sits at xi=0, node 1 at xi=1
@@ -131,11 +136,12 @@ __device__ __forceinline__ void face_slab(const double* X, double* slab, int a0,
 // Shared-memory layouts (doubles) of the hex element kernels; each kernel has its own.
 constexpr int cmax(int a, int b) { return a > b ? a : b; }
 
-template <int P, int NV>
+// Sizes are in units of the kernel's real type R (float64, or float32 in the mixed kernels).
+template <int P, int NV, typename R = double>
 struct HexSmem {
   using D = HexDims<P>;
   static constexpr int N = D::N, Q = D::Q, QF = D::QF, N2 = D::N2, N3 = D::N3, Q3 = D::Q3, QF2 = D::QF2;
-  static constexpr int T = (int)((sizeof(HexTables) + 7) / 8);
+  static constexpr int T = (int)((sizeof(HexTablesT<R>) + sizeof(R) - 1) / sizeof(R));
   static constexpr int MS = N3 + 1;                 // padded row stride of the staged M^-1 (transposed)
   // traces: U, v, then face scratch
   static constexpr int TR_U = T, TR_V = TR_U + NV * N3, TR_W = TR_V + 4 * N3;
@@ -162,6 +168,15 @@ __device__ __forceinline__ void load_tables(const HexTables& src, HexTables* dst
   const double* s = reinterpret_cast<const double*>(&src);
   double* d = reinterpret_cast<double*>(dst);
   for (int i = threadIdx.x; i < (int)(sizeof(HexTables) / sizeof(double)); i += blockDim.x) d[i] = s[i];
+}
+
+// float32 copy of the tables for the mixed-precision kernels
+template <int P>
+__device__ __forceinline__ void load_tables(const HexTables& src, HexTablesT<float>* dst) {
+  const double* s = reinterpret_cast<const double*>(&src);
+  float* d = reinterpret_cast<float*>(dst);
+  for (int i = threadIdx.x; i < kHexTableValues; i += blockDim.x) d[i] = (float)s[i];
+  for (int i = threadIdx.x; i < 64; i += blockDim.x) dst->lex2node[i] = src.lex2node[i];
 }
 
 // Stage M^-1 of one element transposed into shared memory, in lexicographic node order:
@@ -281,27 +296,28 @@ __global__ void __launch_bounds__(kThreads) k_hex_traces(const DevPlan P_, const
 //   lift = M^-1 sum_f b_f                      (= sum_f r_f, r_f = M^-1 b_f);
 //   B_f r_f = B_f M^-1[slab_f, slab_f] b_f     (b_f vanishes off its slab, B_f likewise).
 // Writes the nodal lift [12][N3] (lexicographic) and br2 * B_f r_f at each face's points.
-template <int P, int NV>
+template <int P, int NV, typename R = double>
 __global__ void __launch_bounds__(kThreads) k_hex_lift(const DevPlan P_, int b, const HexTables tables,
                                                       const HexCodes codes, double* lift_out) {
   using D = HexDims<P>;
-  using L = HexSmem<P, NV>;
+  using L = HexSmem<P, NV, R>;
   constexpr int N = D::N, QF = D::QF, N2 = D::N2, N3 = D::N3;
-  extern __shared__ double smem[];
-  HexTables* tb = reinterpret_cast<HexTables*>(smem);
-  double* bs = smem + L::LI_BS;         // [6][12][N2]
-  double* ball = smem + L::LI_B;        // [12][N3]
-  double* jc = smem + L::LI_W;          // [12][QF2]
-  double* tmp = jc + 12 * QF * QF;      // [12][QF][N]
-  double* rs = tmp + 12 * QF * N;       // [12][N2]
-  double* lq = rs + 12 * N2;            // [12][QF2]
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  R* smem = reinterpret_cast<R*>(dyn_smem);
+  HexTablesT<R>* tb = reinterpret_cast<HexTablesT<R>*>(smem);
+  R* bs = smem + L::LI_BS;              // [6][12][N2]
+  R* ball = smem + L::LI_B;             // [12][N3]
+  R* jc = smem + L::LI_W;               // [12][QF2]
+  R* tmp = jc + 12 * QF * QF;           // [12][QF][N]
+  R* rs = tmp + 12 * QF * N;            // [12][N2]
+  R* lq = rs + 12 * N2;                 // [12][QF2]
   __shared__ int node2lex[64];
   const BlockDev& B = P_.blk[b];
   const int e = blockIdx.x;
   load_tables<P>(tables, tb);
   __syncthreads();
   for (int l = threadIdx.x; l < N3; l += blockDim.x) node2lex[tb->lex2node[l]] = l;
-  for (int idx = threadIdx.x; idx < 12 * N3; idx += blockDim.x) ball[idx] = 0.0;
+  for (int idx = threadIdx.x; idx < 12 * N3; idx += blockDim.x) ball[idx] = R(0);
   // M^-T of this element in element node order: MT[j][i] = M^-1[i][j]
   const double* MT = B.minv + (size_t)e * N3 * N3;
   const FaceDev& fd = P_.face[1];
@@ -316,7 +332,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_lift(const DevPlan P_, int b, 
     __syncthreads();
     for (int idx = threadIdx.x; idx < QF * QF * 12; idx += blockDim.x) {
       const int q = idx / 12, c = idx % 12;
-      jc[c * QF * QF + perm[q]] = jw[idx];
+      jc[c * QF * QF + perm[q]] = (R)jw[idx];
     }
     __syncthreads();
     tensor2<12, QF, QF, N, N>(jc, bs + lf * 12 * N2, tmp, tb->bfT, tb->bfT);
@@ -339,17 +355,17 @@ __global__ void __launch_bounds__(kThreads) k_hex_lift(const DevPlan P_, int b, 
   double* lg = lift_out + (size_t)e * 12 * N3;
   for (int idx = threadIdx.x; idx < 2 * N3; idx += blockDim.x) {
     const int i = idx % N3, c0 = (idx / N3) * 6;
-    double s[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    R s[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
 #pragma unroll 4
     for (int j = 0; j < N3; ++j) {
-      const double m = __ldg(MT + (size_t)j * N3 + i);
+      const R m = (R)__ldg(MT + (size_t)j * N3 + i);
       const int lj = node2lex[j];
 #pragma unroll
       for (int k = 0; k < 6; ++k) s[k] += m * ball[(c0 + k) * N3 + lj];
     }
     const int li = node2lex[i];
 #pragma unroll
-    for (int k = 0; k < 6; ++k) lg[(c0 + k) * N3 + li] = s[k];
+    for (int k = 0; k < 6; ++k) lg[(c0 + k) * N3 + li] = (double)s[k];
   }
   // per face: r_f on its slab, then br2 * B_f r_f at the face points
   for (int lf = 0; lf < 6; ++lf) {
@@ -359,11 +375,11 @@ __global__ void __launch_bounds__(kThreads) k_hex_lift(const DevPlan P_, int b, 
     for (int idx = threadIdx.x; idx < 2 * N2; idx += blockDim.x) {
       const int s_i = idx % N2, c0 = (idx / N2) * 6;
       const int ni = tb->lex2node[end * st0 + (s_i % N) * st1 + (s_i / N) * st2];
-      double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+      R acc[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
 #pragma unroll
       for (int s_j = 0; s_j < N2; ++s_j) {
         const int nj = tb->lex2node[end * st0 + (s_j % N) * st1 + (s_j / N) * st2];
-        const double m = __ldg(MT + (size_t)nj * N3 + ni);
+        const R m = (R)__ldg(MT + (size_t)nj * N3 + ni);
 #pragma unroll
         for (int k = 0; k < 6; ++k) acc[k] += m * bs[(lf * 12 + c0 + k) * N2 + s_j];
       }
@@ -378,7 +394,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_lift(const DevPlan P_, int b, 
     const size_t slot = ((size_t)f * 2 + side) * (QF * QF);
     for (int idx = threadIdx.x; idx < QF * QF * 12; idx += blockDim.x) {
       const int q = idx / 12, c = idx % 12;
-      fd.liftF[(slot + q) * 12 + c] = P_.ph.br2 * lq[c * QF * QF + perm[q]];
+      fd.liftF[(slot + q) * 12 + c] = P_.ph.br2 * (double)lq[c * QF * QF + perm[q]];
     }
     __syncthreads();
   }
@@ -389,28 +405,34 @@ __global__ void __launch_bounds__(kThreads) k_hex_lift(const DevPlan P_, int b, 
 // points by sum factorisation; inviscid flux minus the anchor flux and the viscous flux,
 // contracted with w J^-T and the reference gradients (transposed sum factorisation).
 // SPLIT writes inviscid and viscous residuals separately, otherwise their sum into Rinv.
-template <int P, int NV, bool SPLIT>
+template <int P, int NV, bool SPLIT, typename R = double>
 __global__ void __launch_bounds__(kThreads) k_hex_volume(const DevPlan P_, const StatePtrs S, int b,
                                                         const HexTables tables, const double* lift_in) {
   using D = HexDims<P>;
-  using L = HexSmem<P, NV>;
+  using L = HexSmem<P, NV, R>;
   constexpr int N = D::N, Q = D::Q, N3 = D::N3, Q3 = D::Q3;
-  extern __shared__ double smem[];
-  HexTables* tb = reinterpret_cast<HexTables*>(smem);
-  double* U = smem + L::VO_U;        // [NV][N3] minus anchor
-  double* V = smem + L::VO_V;        // [4][N3]
-  double* Lf = smem + L::VO_L;       // [12][N3]
-  double* W = smem + L::VO_W;
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  R* smem = reinterpret_cast<R*>(dyn_smem);
+  HexTablesT<R>* tb = reinterpret_cast<HexTablesT<R>*>(smem);
+  R* U = smem + L::VO_U;             // [NV][N3] minus anchor
+  R* V = smem + L::VO_V;             // [4][N3]
+  R* Lf = smem + L::VO_L;            // [12][N3]
+  R* W = smem + L::VO_W;
   const BlockDev& B = P_.blk[b];
   const int e = blockIdx.x;
   load_tables<P>(tables, tb);
   const double* Ug = S.b[b] + (size_t)e * N3 * NV;
-  __shared__ double anchor[NV];
-  if (threadIdx.x < NV) anchor[threadIdx.x] = Ug[threadIdx.x];
+  __shared__ double anchor_d[NV];
+  __shared__ R anchor[NV];
+  if (threadIdx.x < NV) {
+    anchor_d[threadIdx.x] = Ug[threadIdx.x];
+    anchor[threadIdx.x] = (R)Ug[threadIdx.x];
+  }
   __syncthreads();
+  // differences to the anchor are formed in float64, then rounded to R
   for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
     const int v = idx / N3, l = idx % N3;
-    U[idx] = Ug[tb->lex2node[l] * NV + v] - anchor[v];
+    U[idx] = (R)(Ug[tb->lex2node[l] * NV + v] - anchor_d[v]);
   }
   const bool visc = P_.viscous;
   if (visc) {
@@ -421,16 +443,16 @@ __global__ void __launch_bounds__(kThreads) k_hex_volume(const DevPlan P_, const
       for (int v = 0; v < NV; ++v) u[v] = Ug[node * NV + v];
       viscous_vars<NV>(P_.ph, u, vv);
 #pragma unroll
-      for (int m = 0; m < 4; ++m) V[m * N3 + l] = vv[m];
+      for (int m = 0; m < 4; ++m) V[m * N3 + l] = (R)vv[m];
     }
     const double* lg = lift_in + (size_t)e * 12 * N3;
-    for (int idx = threadIdx.x; idx < 12 * N3; idx += blockDim.x) Lf[idx] = lg[idx];
+    for (int idx = threadIdx.x; idx < 12 * N3; idx += blockDim.x) Lf[idx] = (R)lg[idx];
   }
   __syncthreads();
-  double* uq = W;                      // [NV][Q3]   U - anchor at volume points
-  double* gq = uq + NV * Q3;           // [12][Q3]   gradients of v: reference (3 x 4), then physical + lift
-  double* t1 = gq + 12 * Q3;           // contraction scratch
-  double* t2 = t1 + L::C1 * N * N * Q;
+  R* uq = W;                           // [NV][Q3]   U - anchor at volume points
+  R* gq = uq + NV * Q3;                // [12][Q3]   gradients of v: reference (3 x 4), then physical + lift
+  R* t1 = gq + 12 * Q3;                // contraction scratch
+  R* t2 = t1 + L::C1 * N * N * Q;
   tensor3<NV, N, N, N, Q, Q, Q, false>(U, uq, t1, t2, tb->bq, tb->bq, tb->bq);
   const double* jinv = B.jinv + (size_t)e * Q3 * 9;
   const double* wdet = B.wdet + (size_t)e * Q3;
@@ -440,9 +462,9 @@ __global__ void __launch_bounds__(kThreads) k_hex_volume(const DevPlan P_, const
     tensor3<4, N, N, N, Q, Q, Q, false>(V, gq + 2 * 4 * Q3, t1, t2, tb->bq, tb->bq, tb->dq);
     // reference -> physical gradient, in place per point: g[m*3+d] = sum_r dv_m/dxi_r J^-1[r][d]
     for (int q = threadIdx.x; q < Q3; q += blockDim.x) {
-      double J[9], gr[12];
+      R J[9], gr[12];
 #pragma unroll
-      for (int k = 0; k < 9; ++k) J[k] = jinv[q * 9 + k];
+      for (int k = 0; k < 9; ++k) J[k] = (R)jinv[q * 9 + k];
 #pragma unroll
       for (int k = 0; k < 12; ++k) gr[k] = gq[k * Q3 + q];      // [r][m]
 #pragma unroll
@@ -455,34 +477,34 @@ __global__ void __launch_bounds__(kThreads) k_hex_volume(const DevPlan P_, const
     __syncthreads();
     tensor3<12, N, N, N, Q, Q, Q, true>(Lf, gq, t1, t2, tb->bq, tb->bq, tb->bq);   // + lift
   }
-  double* Gi = t1;                     // [3][NV][Q3]
-  double* Gv = Gi + 3 * NV * Q3;       // [3][NV][Q3] (SPLIT only)
-  double Fa[3][NV];
+  R* Gi = t1;                          // [3][NV][Q3]
+  R* Gv = Gi + 3 * NV * Q3;            // [3][NV][Q3] (SPLIT only)
+  R Fa[3][NV];
   {
-    const double ex[3] = {1.0, 0.0, 0.0}, ey[3] = {0.0, 1.0, 0.0}, ez[3] = {0.0, 0.0, 1.0};
+    const R ex[3] = {R(1), R(0), R(0)}, ey[3] = {R(0), R(1), R(0)}, ez[3] = {R(0), R(0), R(1)};
     normal_flux<NV>(P_.ph, anchor, ex, Fa[0]);
     normal_flux<NV>(P_.ph, anchor, ey, Fa[1]);
     normal_flux<NV>(P_.ph, anchor, ez, Fa[2]);
   }
   for (int q = threadIdx.x; q < Q3; q += blockDim.x) {
-    double J[9];
+    R J[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) J[k] = jinv[q * 9 + k];
-    const double wq = wdet[q];
-    double Uq[NV], F[3][NV];
+    for (int k = 0; k < 9; ++k) J[k] = (R)jinv[q * 9 + k];
+    const R wq = (R)wdet[q];
+    R Uq[NV], F[3][NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) Uq[v] = anchor[v] + uq[v * Q3 + q];
     {
-      const double ex[3] = {1.0, 0.0, 0.0}, ey[3] = {0.0, 1.0, 0.0}, ez[3] = {0.0, 0.0, 1.0};
+      const R ex[3] = {R(1), R(0), R(0)}, ey[3] = {R(0), R(1), R(0)}, ez[3] = {R(0), R(0), R(1)};
       normal_flux<NV>(P_.ph, Uq, ex, F[0]);
       normal_flux<NV>(P_.ph, Uq, ey, F[1]);
       normal_flux<NV>(P_.ph, Uq, ez, F[2]);
     }
-    double Fv[3 * NV];
+    R Fv[3 * NV];
 #pragma unroll
-    for (int k = 0; k < 3 * NV; ++k) Fv[k] = 0.0;
+    for (int k = 0; k < 3 * NV; ++k) Fv[k] = R(0);
     if (visc) {
-      double grad[12];
+      R grad[12];
 #pragma unroll
       for (int k = 0; k < 12; ++k) grad[k] = gq[k * Q3 + q];
       viscous_flux<NV>(P_.ph, Uq, grad, Fv);
@@ -491,10 +513,10 @@ __global__ void __launch_bounds__(kThreads) k_hex_volume(const DevPlan P_, const
     for (int r = 0; r < 3; ++r)
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
-        const double gi = (J[r * 3 + 0] * (F[0][v] - Fa[0][v]) + J[r * 3 + 1] * (F[1][v] - Fa[1][v]) +
-                           J[r * 3 + 2] * (F[2][v] - Fa[2][v])) * wq;
-        const double gv = -(J[r * 3 + 0] * Fv[0 * NV + v] + J[r * 3 + 1] * Fv[1 * NV + v] +
-                            J[r * 3 + 2] * Fv[2 * NV + v]) * wq;
+        const R gi = (J[r * 3 + 0] * (F[0][v] - Fa[0][v]) + J[r * 3 + 1] * (F[1][v] - Fa[1][v]) +
+                      J[r * 3 + 2] * (F[2][v] - Fa[2][v])) * wq;
+        const R gv = -(J[r * 3 + 0] * Fv[0 * NV + v] + J[r * 3 + 1] * Fv[1 * NV + v] +
+                       J[r * 3 + 2] * Fv[2 * NV + v]) * wq;
         if (SPLIT) {
           Gi[(r * NV + v) * Q3 + q] = gi;
           Gv[(r * NV + v) * Q3 + q] = gv;
@@ -504,10 +526,10 @@ __global__ void __launch_bounds__(kThreads) k_hex_volume(const DevPlan P_, const
       }
   }
   __syncthreads();
-  double* Ri = uq;                     // reuse: [NV][N3] (NV*N3 <= NV*Q3)
-  double* s1 = Gi + (SPLIT ? 6 : 3) * NV * Q3;
-  double* s2 = s1 + NV * Q * Q * N;
-  double* Rv = s2 + NV * Q * N * N;    // [NV][N3] (SPLIT only)
+  R* Ri = uq;                          // reuse: [NV][N3] (NV*N3 <= NV*Q3)
+  R* s1 = Gi + (SPLIT ? 6 : 3) * NV * Q3;
+  R* s2 = s1 + NV * Q * Q * N;
+  R* Rv = s2 + NV * Q * N * N;         // [NV][N3] (SPLIT only)
   tensor3<NV, Q, Q, Q, N, N, N, false>(Gi + 0 * NV * Q3, Ri, s1, s2, tb->dqT, tb->bqT, tb->bqT);
   tensor3<NV, Q, Q, Q, N, N, N, true>(Gi + 1 * NV * Q3, Ri, s1, s2, tb->bqT, tb->dqT, tb->bqT);
   tensor3<NV, Q, Q, Q, N, N, N, true>(Gi + 2 * NV * Q3, Ri, s1, s2, tb->bqT, tb->bqT, tb->dqT);
@@ -520,8 +542,8 @@ __global__ void __launch_bounds__(kThreads) k_hex_volume(const DevPlan P_, const
   double* Rig = B.Rinv + (size_t)e * N3 * NV;
   double* Rvg = B.Rvis + (size_t)e * N3 * NV;
   for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
-    Rig[idx] = Ri[idx];
-    if (SPLIT && visc) Rvg[idx] = Rv[idx];
+    Rig[idx] = (double)Ri[idx];
+    if (SPLIT && visc) Rvg[idx] = (double)Rv[idx];
   }
 }
 
@@ -768,7 +790,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_positivity(const DevPlan P_, c
 template <int P, int NV>
 __global__ void __launch_bounds__(kThreads) k_hex_troubled(const DevPlan P_, const StatePtrs S, int b,
                                                           const HexTables tables, const LimiterConst Lc,
-                                                          double* sensor_out, uint8_t* flag_out) {
+                                                          double* sensor_out, uint8_t* flag_out, const PredictArgs pa) {
   using D = HexDims<P>;
   constexpr int N = D::N, Q = D::Q, N3 = D::N3, Q3 = D::Q3, QF2 = D::QF2;
   constexpr int NS = N3 + Q3 + 6 * QF2;
@@ -785,6 +807,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_troubled(const DevPlan P_, con
   __shared__ double red[4][kThreads / 32];
   const BlockDev& B = P_.blk[b];
   const int e = blockIdx.x;
+  if (predicted_skip(pa, e, flag_out)) return;
   load_tables<P>(tables, tb);
   const double* Ug = S.b[b] + (size_t)e * N3 * NV;
   __syncthreads();
@@ -864,8 +887,10 @@ __global__ void __launch_bounds__(kThreads) k_hex_troubled(const DevPlan P_, con
       const double r0 = h0 / fmax(s0, 1.0e-12), r1 = h1 / fmax(s1, 1.0e-12);
       value = (isnan(r0) || isnan(r1)) ? NAN : fmax(r0, r1);
     }
+    const bool detected = (value > Lc.sensor_threshold) || any_bad;
     if (sensor_out) sensor_out[e] = value;
-    if (flag_out) flag_out[e] = (uint8_t)((value > Lc.sensor_threshold) || any_bad);
+    if (flag_out) flag_out[e] = (uint8_t)detected;
+    count_prediction(pa, e, detected);
   }
 }
 

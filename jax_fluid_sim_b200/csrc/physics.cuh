@@ -1,4 +1,5 @@
-// Pointwise compressible-flow physics shared by the DG kernels (float64).
+// Pointwise compressible-flow physics shared by the DG kernels, templated on the real type T
+// (float64 for the plain path; float32 inside the mixed-precision volume and lift kernels).
 //
 // Same arithmetic as the reference's hybrid/solver.py:
 //   conserved_to_primitive  :83-98   (density floored at 1e-14 in divisions only)
@@ -43,41 +44,44 @@ __device__ __forceinline__ bool tag_in(int tag, const int* set, int n) {
 __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
 
-template <int NV>
-__device__ __forceinline__ void primitive(const Physics& ph, const double* U, double* W) {
-  const double rho = U[0];
-  const double srho = fmax(rho, kRhoFloor);
+template <int NV, typename T>
+__device__ __forceinline__ void primitive(const Physics& ph, const T* U, T* W) {
+  const T rho = U[0];
+  const T srho = fmax(rho, T(kRhoFloor));
   W[0] = rho;
   W[1] = U[1] / srho;
   W[2] = U[2] / srho;
   W[3] = U[3] / srho;
-  const double m2 = add(add(mul(U[1], U[1]), mul(U[2], U[2])), mul(U[3], U[3]));
-  const double ke = mul(0.5, m2) / srho;
-  W[4] = mul(ph.gamma - 1.0, sub(U[4], ke));
+  const T m2 = add(add(mul(U[1], U[1]), mul(U[2], U[2])), mul(U[3], U[3]));
+  const T ke = mul(T(0.5), m2) / srho;
+  W[4] = mul(T(ph.gamma - 1.0), sub(U[4], ke));
 #pragma unroll
   for (int s = 5; s < NV; ++s) W[s] = U[s] / srho;
 }
 
-template <int NV>
-__device__ __forceinline__ void conserved(const Physics& ph, const double* W, double* U) {
-  const double rho = W[0];
+template <int NV, typename T>
+__device__ __forceinline__ void conserved(const Physics& ph, const T* W, T* U) {
+  const T rho = W[0];
   U[0] = rho;
   U[1] = mul(rho, W[1]);
   U[2] = mul(rho, W[2]);
   U[3] = mul(rho, W[3]);
-  const double v2 = add(add(mul(W[1], W[1]), mul(W[2], W[2])), mul(W[3], W[3]));
-  U[4] = add(W[4] / (ph.gamma - 1.0), mul(mul(0.5, rho), v2));
+  const T v2 = add(add(mul(W[1], W[1]), mul(W[2], W[2])), mul(W[3], W[3]));
+  U[4] = add(W[4] / T(ph.gamma - 1.0), mul(mul(T(0.5), rho), v2));
 #pragma unroll
   for (int s = 5; s < NV; ++s) U[s] = mul(rho, W[s]);
 }
 
-template <int NV>
-__device__ __forceinline__ void normal_flux(const Physics& ph, const double* U, const double* n, double* F) {
-  double W[NV];
+template <int NV, typename T>
+__device__ __forceinline__ void normal_flux(const Physics& ph, const T* U, const T* n, T* F) {
+  T W[NV];
   primitive<NV>(ph, U, W);
-  const double un = add(add(mul(W[1], n[0]), mul(W[2], n[1])), mul(W[3], n[2]));
-  const double ru = mul(W[0], un);
+  const T un = add(add(mul(W[1], n[0]), mul(W[2], n[1])), mul(W[3], n[2]));
+  const T ru = mul(W[0], un);
   F[0] = ru;
   F[1] = add(mul(mul(W[0], W[1]), un), mul(W[4], n[0]));
   F[2] = add(mul(mul(W[0], W[2]), un), mul(W[4], n[1]));
@@ -193,14 +197,14 @@ __device__ void ghost_state(const Physics& ph, const double* U, const double* n,
   conserved<NV>(ph, W, G);
 }
 
-template <int NV>
-__device__ __forceinline__ void viscous_vars(const Physics& ph, const double* U, double* out) {
-  double W[NV];
+template <int NV, typename T>
+__device__ __forceinline__ void viscous_vars(const Physics& ph, const T* U, T* out) {
+  T W[NV];
   primitive<NV>(ph, U, W);
   out[0] = W[1];
   out[1] = W[2];
   out[2] = W[3];
-  out[3] = W[4] / (fmax(W[0], kRhoFloor) * ph.R);
+  out[3] = W[4] / (fmax(W[0], T(kRhoFloor)) * T(ph.R));
 }
 
 // Ghost [u, v, w, T] for the viscous traces (boundary.py:74-102).
@@ -228,26 +232,27 @@ __device__ void viscous_ghost(const Physics& ph, const double* U, const double* 
 }
 
 // Cartesian viscous flux F[d][v]; grad[m][d] = d(u,v,w,T)_m / dx_d.
-template <int NV>
-__device__ void viscous_flux(const Physics& ph, const double* U, const double* grad, double* F) {
-  double W[NV];
+template <int NV, typename T>
+__device__ void viscous_flux(const Physics& ph, const T* U, const T* grad, T* F) {
+  T W[NV];
   primitive<NV>(ph, U, W);
-  const double div = grad[0 * 3 + 0] + grad[1 * 3 + 1] + grad[2 * 3 + 2];
-  double stress[3][3];
+  const T div = grad[0 * 3 + 0] + grad[1 * 3 + 1] + grad[2 * 3 + 2];
+  const T mu = T(ph.mu), two_thirds = T(2.0 / 3.0);
+  T stress[3][3];
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
     for (int d = 0; d < 3; ++d)
-      stress[i][d] = ph.mu * (grad[i * 3 + d] + grad[d * 3 + i] - (i == d ? (2.0 / 3.0) * div : 0.0));
+      stress[i][d] = mu * (grad[i * 3 + d] + grad[d * 3 + i] - (i == d ? two_thirds * div : T(0)));
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    F[d * NV + 0] = 0.0;
+    F[d * NV + 0] = T(0);
     F[d * NV + 1] = stress[0][d];
     F[d * NV + 2] = stress[1][d];
     F[d * NV + 3] = stress[2][d];
-    F[d * NV + 4] = W[1] * stress[0][d] + W[2] * stress[1][d] + W[3] * stress[2][d] + ph.kappa * grad[3 * 3 + d];
+    F[d * NV + 4] = W[1] * stress[0][d] + W[2] * stress[1][d] + W[3] * stress[2][d] + T(ph.kappa) * grad[3 * 3 + d];
 #pragma unroll
-    for (int v = 5; v < NV; ++v) F[d * NV + v] = 0.0;
+    for (int v = 5; v < NV; ++v) F[d * NV + v] = T(0);
   }
 }
 

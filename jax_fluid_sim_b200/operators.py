@@ -25,8 +25,13 @@ def _stream_ptr():
 class NativePlan:
     """Owns one ``dgb_plan``: uploads the host plan tables and keeps the parameter block."""
 
-    def __init__(self, plan: Plan, solver, viscous: bool, br2: float, sum_factorised=None):
+    PRECISIONS = {"float64": 0, "mixed": 1}
+
+    def __init__(self, plan: Plan, solver, viscous: bool, br2: float, sum_factorised=None, precision="float64"):
         L = N.lib()
+        if precision not in self.PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(self.PRECISIONS)}")
+        self.precision = precision
         self.plan = plan
         self.nblocks = len(plan.blocks)
         prm = N.Params()
@@ -43,6 +48,7 @@ class NativePlan:
         prm.adm_density_floor = prm.adm_pressure_floor = 1e-7
         prm.sensor_threshold = 5e-2
         prm.limiter = 0
+        prm.precision = self.PRECISIONS[precision]
         self.params = prm
         handle = ctypes.c_void_p()
         N.check(L.dgb_plan_create(ctypes.byref(prm), ctypes.byref(handle)))
@@ -51,6 +57,8 @@ class NativePlan:
         single_hex = len(plan.blocks) == 1 and plan.blocks[0].etype == "hexahedron"
         if sum_factorised is None:
             sum_factorised = single_hex
+        if precision == "mixed" and not sum_factorised:
+            raise NotImplementedError("precision='mixed' runs on the sum-factorised path: one hexahedron block")
         for b, bp in enumerate(plan.blocks):
             # the sum-factorised kernels stream M^-1 transposed (coalesced across nodes)
             minv = np.ascontiguousarray(np.swapaxes(bp.minv, 1, 2)) if sum_factorised else bp.minv
@@ -105,7 +113,10 @@ class NativePlan:
             raise ValueError("the subcell coupling of a plan is fixed once chosen")
         from .subcell import SubcellPlan
         L = N.lib()
-        sp = SubcellPlan(self.plan.mesh, self.plan.degree, coupling)
+        cache = self.plan.__dict__.setdefault("_subcell_plans", {})     # shared by plans of one mesh
+        if coupling not in cache:
+            cache[coupling] = SubcellPlan(self.plan.mesh, self.plan.degree, coupling)
+        sp = cache[coupling]
         keep = []
         for b, (bp, sb) in enumerate(zip(self.plan.blocks, sp.blocks)):
             rs = sp.refs[bp.etype]
@@ -171,7 +182,10 @@ class HybridEulerOperator:
 
     _viscous = False
 
-    def __init__(self, solver, br2_stabilization=None, sum_factorised=None):
+    def __init__(self, solver, br2_stabilization=None, sum_factorised=None, precision="float64"):
+        """``precision``: "float64" (the reference's arithmetic) or "mixed" (float32 arithmetic in
+        the hexahedron BR2-lift and volume kernels; the state, face fluxes, limiters, reductions
+        and the stage update stay float64)."""
         self.solver = solver
         self.mesh = solver.mesh
         P = solver.polynomial_degree
@@ -179,9 +193,20 @@ class HybridEulerOperator:
         self.plan = Plan(self.mesh, P)
         self.names = [b.element_type for b in self.mesh.element_blocks]
         viscous = self._viscous and solver.dynamic_viscosity > 0.0
-        self.native = NativePlan(self.plan, solver, viscous, self.br2_stabilization, sum_factorised)
+        self.native = NativePlan(self.plan, solver, viscous, self.br2_stabilization, sum_factorised, precision)
+        self.precision = precision
         self.viscous = viscous
         self.solution_node_coordinates = {bp.etype: bp.node_xyz for bp in self.plan.blocks}
+
+    def with_precision(self, precision):
+        """The same operator (mesh, host tables, parameters) on a second device plan that runs in
+        ``precision``; the host plan is shared, so this costs only the upload."""
+        other = object.__new__(type(self))
+        other.__dict__.update({k: v for k, v in self.__dict__.items() if k != "native"})
+        other.native = NativePlan(self.plan, self.solver, self.viscous, self.br2_stabilization,
+                                  self.native.sum_factorised, precision)
+        other.precision = precision
+        return other
 
     # -- state plumbing
     def to_device(self, states):
