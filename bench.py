@@ -10,13 +10,22 @@ troubled-cell check, subcell finite-volume recompute of troubled elements, Zhang
 positivity limiter, blend and admissibility check).  Synthetic seeded mesh (numpy
 generator); the state starts as the uniform free stream.
 
-By default the step is timed twice from the same state and dt: plain float64, then the
-mixed-precision path (float32 arithmetic in the BR2-lift and volume kernels; state, face
-fluxes, limiters and reductions float64).  The mixed step is the headline value; the
-plain one and the relative density L2 difference between the two rides along.
+Default flow (one state, one dt for every run):
+  1. start: the Mach-3 normal-shock state in the elements inside r < 0.65 around the sphere,
+     free stream in the others (the jump sharpens inside elements, so MOOD has work);
+  2. 20 plain steps, labelling every element by the a-posteriori detector on the first
+     SSP-RK stage; the troubled-cell predictor is trained on those samples;
+  3. from the state reached, three timed runs of K steps: plain float64, mixed precision
+     (float32 arithmetic in the traces, BR2-lift, volume and finalize kernels; state, face
+     fluxes, limiters and reductions float64), and learned + mixed (predicted elements go
+     straight to the subcell scheme; the detector still tests every other element);
+  4. learned + mixed is the headline value; the other runs, the density L2 difference to
+     the plain run, and the predictor's missed / false-positive rates (one step in evaluate
+     mode) ride along.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--precision both|mixed|float64] [--limiter mood|positivity]
+                    [--start shock|uniform] [--learned 0|1] [--train-steps S]
 
 Metric: DOF-updates/s = sum_b E_b*Np_b * steps / seconds (Np = element nodes).
 --impl reference times the CPU oracle (a float64 numpy restatement of the
@@ -132,13 +141,15 @@ def stage_bytes(op, nv, split, sizeof=8):
     for bp in op.plan.blocks:
         E, Np, Nq, nlf = bp.E, bp.Np, bp.Nq, bp.nlf
         nqf = max(fp.nq for fp in op.plan.faces.values())
-        out["traces"] += sizeof * E * (nv * Np + nlf * nqf * (nv + (16 if visc else 0)))
+        # U in; per face point: anchor-form U (+ v, gradients and the face inverse Jacobian) out / in
+        out["traces"] += sizeof * E * (nv * Np + nlf * nqf * (nv + (16 + 9 if visc else 0)))
         if visc:
             out["lift"] += sizeof * E * (Np * Np + 2 * nlf * nqf * 12 + 12 * Np)
         out["volume"] += sizeof * E * (nv * Np + 10 * Nq + (12 * Np if visc else 0) + (2 if split else 1) * nv * Np)
         out["finalize"] += sizeof * E * (Np * Np + (2 if split else 1) * nv * Np + nlf * nqf * 2 * nv + 3 * nv * Np)
     for fp in op.plan.faces.values():
-        out["face_flux"] += fp.F * (sizeof * fp.nq * (2 * nv + 4 + nv) + 8)
+        # traces of both sides, n and w in; both sides' fluxes out (+ v of both sides in, BR2 jumps out)
+        out["face_flux"] += fp.F * (sizeof * fp.nq * (2 * nv + 4 + 2 * nv + (8 + 12 if visc else 0)) + 8)
         if visc:
             out["face_visc"] += fp.F * sizeof * fp.nq * (2 * 4 + 2 * 12 + 2 * 12 + 4 + nv)
     return out
@@ -150,6 +161,33 @@ def build_integrator(jfs, op, args, wall_T):
     return limiter, jfs.HybridSSPRK3(op, cfl=0.3, limiter=limiter)
 
 
+def shock_layer(xyz):
+    """Per element (xyz: (E, Np, 3) node positions): True where the element's centroid lies
+    inside r < 0.65, the layer that starts in the post-shock state."""
+    return np.broadcast_to(np.linalg.norm(xyz.mean(axis=1), axis=-1)[:, None] < 0.65, xyz.shape[:-1])
+
+
+def bow_shock_state(solver, op, u):
+    """Synthetic start with a shock in it: the Mach-3 normal-shock (Rankine-Hugoniot) state in the
+    elements whose centroid lies inside r < 0.65 around the sphere of radius 0.5, the free stream
+    in the others.  Each element starts constant, so the jump sits on element faces (a jump
+    inside a P3 element would leave negative densities at its quadrature points); the first
+    steps sharpen it inside the elements next to it, which gives the MOOD detector work."""
+    g, M = GAMMA, MACH
+    rho2 = (g + 1) * M ** 2 / ((g - 1) * M ** 2 + 2)
+    p2 = 1 + 2 * g / (g + 1) * (M ** 2 - 1)
+
+    def prim(xyz):
+        inside = shock_layer(xyz)
+        W = np.zeros(xyz.shape[:-1] + (5,))
+        W[..., 0] = np.where(inside, rho2, 1.0)
+        W[..., 1] = np.where(inside, u / rho2, u)
+        W[..., 4] = np.where(inside, p2, 1.0)
+        return W
+
+    return solver.state_blocks_from_primitive_function(op, prim)
+
+
 def run_ours(args):
     import ctypes
 
@@ -159,6 +197,7 @@ def run_ours(args):
     import jax_fluid_sim_b200 as jfs
     from jax_fluid_sim_b200 import _native as N
     from jax_fluid_sim_b200.operators import _stream_ptr
+    from jax_fluid_sim_b200.predictor import TroubledCellPredictor
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -170,28 +209,53 @@ def run_ours(args):
     src = workload(args.scale)
     u, mu, farfield = freestream(3)
     solver = jfs.HybridCompressibleSolver(jfs.HybridMesh(src), polynomial_degree=args.degree, dynamic_viscosity=mu)
-    modes = {"both": ["float64", "mixed"], "float64": ["float64"], "mixed": ["mixed"]}[args.precision]
-    base = jfs.HybridNavierStokesOperator(solver, precision=modes[0])
-    ops = {modes[0]: base}
-    for m in modes[1:]:
+    precisions = {"both": ["float64", "mixed"], "float64": ["float64"], "mixed": ["mixed"]}[args.precision]
+    base = jfs.HybridNavierStokesOperator(solver, precision=precisions[0])
+    ops = {precisions[0]: base}
+    for m in precisions[1:]:
         ops[m] = base.with_precision(m)
     bc = jfs.FarfieldWallBoundary(solver, farfield, wall_temperature=T_WALL / T_INF)
-    runs = {m: build_integrator(jfs, ops[m], args, T_WALL / T_INF) for m in modes}
-    U0 = solver.uniform_state_blocks(1.0, [u, 0.0, 0.0], 1.0)
+    integs = {m: build_integrator(jfs, ops[m], args, T_WALL / T_INF) for m in precisions}
+    learned = args.limiter == "mood" and bool(args.learned)
+    head_prec = precisions[-1]
+    U0 = (bow_shock_state(solver, base, u) if args.start == "shock"
+          else solver.uniform_state_blocks(1.0, [u, 0.0, 0.0], 1.0))
     dofs = sum(bp.E * bp.Np for bp in base.plan.blocks)
+    E = int(sum(bp.E for bp in base.plan.blocks))
     nv = solver.layout.number_of_variables
     setup_s = time.time() - t_setup
-    dt = runs[modes[0]][1].stable_dt(U0, bc)      # one fixed dt for every mode (same trajectory)
-    torch.cuda.synchronize()
-    results = {}
-    for m in modes:
-        limiter, integ = runs[m]
-        Uw = {k: v.clone() for k, v in U0.items()}
+    lim0, integ0 = integs[precisions[0]]
+    dt = integ0.stable_dt(U0, bc)                   # one fixed dt for every run (same trajectory)
+
+    # training data: plain steps from the start, labelled by the a-posteriori detector
+    predictor, train = None, None
+    U_start = {k: v.clone() for k, v in U0.items()}
+    if learned:
+        t0 = time.time()
+        predictor = TroubledCellPredictor(ops[head_prec], threshold=args.threshold)
+        Xs, ys = [], []
+        for _ in range(args.train_steps):
+            X, y = predictor.labelled_samples(U_start, dt, bc, lim0)
+            Xs.append(X)
+            ys.append(y)
+            integ0.checked_step_inplace(U_start, dt, bc)
+        X, y = torch.cat(Xs), torch.cat(ys)
+        hist = predictor.fit(X, y, epochs=args.train_epochs, batch=8192)
+        torch.cuda.synchronize()
+        train = {"steps": args.train_steps, "samples": int(X.shape[0]), "positives": int(y.sum().item()),
+                 "epochs": args.train_epochs, "loss_first_last": [hist[0], hist[-1]],
+                 "seconds": round(time.time() - t0, 1)}
+        del Xs, ys, X, y
+
+    def timed(integ, pre=None):
+        Uw = {k: v.clone() for k, v in U_start.items()}
         for _ in range(args.warmup):
             integ.checked_step_inplace(Uw, dt, bc)
         del Uw
-        U = {k: v.clone() for k, v in U0.items()}
+        U = {k: v.clone() for k, v in U_start.items()}
         torch.cuda.synchronize()
+        if pre:
+            pre()
         if world > 1:
             dist.barrier()
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -208,22 +272,43 @@ def run_ours(args):
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms = float(t.item())
         valid, rmin, pmin = integ._status_tuple()
-        troubled = None
-        if args.limiter == "mood":
-            flags = limiter.troubled(U)
-            troubled = int(sum(int(v.sum().item()) for v in flags.values()))
-        results[m] = dict(ms=ms, U=U, clocks=clocks.summary(), valid=valid, rho_min=rmin, p_min=pmin,
-                          troubled=troubled, value=dofs * args.steps * world / (ms / 1e3))
-    head = "mixed" if "mixed" in results else "float64"
-    op, (limiter, integ) = ops[head], runs[head]
-    R = results[head]
+        return dict(ms=ms, U=U, clocks=clocks.summary(), valid=valid, rho_min=rmin, p_min=pmin,
+                    value=dofs * args.steps * world / (ms / 1e3))
+
+    runs = {}
+    for m in precisions:
+        runs[m] = timed(integs[m][1])
+    head = head_prec
+    if learned:
+        predictor.attach("learned")
+        runs["learned+" + head_prec] = timed(integs[head_prec][1], pre=lambda: predictor.counts(reset=True))
+        in_run = predictor.counts(reset=True)
+        # predictor quality on the same start: one step in evaluate mode (the plain step, every
+        # element tested, the prediction only counted)
+        predictor.attach("evaluate")
+        Ue = {k: v.clone() for k, v in U_start.items()}
+        integs[head_prec][1].checked_step_inplace(Ue, dt, bc)
+        ev = predictor.counts(reset=True)
+        predictor.attach("off")
+        tested_pos = ev["hit"] + ev["missed"]
+        train.update({
+            "missed_rate": ev["missed"] / max(tested_pos, 1),
+            "false_positive_rate": ev["false_positive"] / max(3 * E - tested_pos, 1),
+            "detector_flags_per_step": tested_pos, "predicted_per_step": ev["predicted"],
+            "timed_run": {"predicted": in_run["predicted"], "missed_caught_by_detector": in_run["missed"]}})
+        head = "learned+" + head_prec
+    R = runs[head]
+    op, (limiter, integ) = ops[head_prec], integs[head_prec]
+    troubled = None
+    if args.limiter == "mood":
+        flags = limiter.troubled(R["U"])
+        troubled = int(sum(int(v.sum().item()) for v in flags.values()))
     accuracy = None
-    if len(results) == 2:
-        a, b = results["mixed"]["U"], results["float64"]["U"]
+    if "float64" in runs and head != "float64":
+        a, b = R["U"], runs["float64"]["U"]
         num = sum(float(((a[k][..., 0] - b[k][..., 0]) ** 2).sum()) for k in a)
         den = sum(float((b[k][..., 0] ** 2).sum()) for k in b)
-        accuracy = {"density_l2_rel_vs_plain": (num / den) ** 0.5, "after_steps": args.steps,
-                    "gate": 1e-6}
+        accuracy = {"density_l2_rel_vs_plain": (num / den) ** 0.5, "after_steps": args.steps, "gate": 1e-6}
 
     # per-stage kernel durations of one RHS (CUDA events on the launching stream)
     stage_ms = (ctypes.c_float * len(STAGES))()
@@ -242,14 +327,16 @@ def run_ours(args):
         try:
             per_elem = json.loads(tfile.read_text()).get(dominant, {}).get("dram_bytes_per_element")
             if per_elem:
-                traffic = per_elem * sum(bp.E for bp in op.plan.blocks)
+                traffic = per_elem * E
         except Exception:
             traffic = None
 
     # end to end through the public API with host buffers: H2D state, step, D2H state
-    host_in = {k: v.cpu().pin_memory() for k, v in U0.items()}
+    if learned:
+        predictor.attach("learned")
+    host_in = {k: v.cpu().pin_memory() for k, v in U_start.items()}
     host_out = {k: torch.empty_like(v).pin_memory() for k, v in host_in.items()}
-    dev = {k: torch.empty_like(v) for k, v in U0.items()}
+    dev = {k: torch.empty_like(v) for k, v in U_start.items()}
     e_steps = max(1, min(args.steps, 5))
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -262,6 +349,8 @@ def run_ours(args):
             host_out[k].copy_(dev[k], non_blocking=True)
     e1.record()
     torch.cuda.synchronize()
+    if learned:
+        predictor.attach("off")
     e2e_ms = e0.elapsed_time(e1) / e_steps
     state_bytes = sum(v.numel() * 8 for v in host_in.values())
 
@@ -269,28 +358,31 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.cpu_seconds)
     # launches per checked step: per stage the RHS kernels (per block / face type), then the
-    # limiter and admissibility kernels
+    # limiter and admissibility kernels (and the predictor's three per block when learned)
     nb, nf = len(op.plan.blocks), len(op.plan.faces)
     per_stage = nb * (4 if (op.native.sum_factorised and op.viscous) else 3) + nf * (2 if op.viscous else 1)
     if args.limiter == "mood":
-        # troubled, subcell fv/update, positivity x2, blend per block; subcell faces per type; adm + final
         per_stage += nb * 6 + nf + nb + 1
+        if learned:
+            per_stage += 3 * nb
     else:
         per_stage += nb * 2 + 1
-    E = int(sum(bp.E for bp in op.plan.blocks))
     lim = "MOOD subcell FV (CWENO-Z) + positivity" if args.limiter == "mood" else "positivity limiter"
-    prec = ("mixed: float32 BR2-lift and volume arithmetic, float64 state, fluxes, limiters and reductions"
-            if head == "mixed" else "plain float64")
+    prec = ("mixed: float32 arithmetic in the traces, BR2-lift, volume and finalize kernels; float64 state, "
+            "face fluxes, limiters and reductions" if head_prec == "mixed" else "plain float64")
     line = {
         "metric": METRIC, "value": R["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": R["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32+f64" if head == "mixed" else "f64", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f32+f64" if head_prec == "mixed" else "f64", "data": "synthetic",
         "config": {"workload": f"Mach-3 viscous sphere, O/H hex grid, {E} elements, P{args.degree} ({dofs} DOF), "
-                               f"checked SSP-RK3 with {lim}, {prec}",
-                   "elements": E, "degree": args.degree, "dofs": int(dofs), "precision": head,
+                               f"checked SSP-RK3 with {lim}, {prec}"
+                               + (", learned troubled-cell predictor" if learned else ""),
+                   "elements": E, "degree": args.degree, "dofs": int(dofs), "mode": head,
+                   "start": ("Mach-3 normal-shock state in the elements inside r < 0.65, free stream outside"
+                             if args.start == "shock" else "uniform free stream"),
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": "inputs larger than L2 (state 0.5 GB, inverse mass 6.6 GB per pass)",
-                   "limiter": args.limiter, "troubled_elements_after": R["troubled"], "setup_s": round(setup_s, 1)},
+                   "limiter": args.limiter, "troubled_elements_after": troubled, "setup_s": round(setup_s, 1)},
         "gpu_launches": per_stage * 3 * args.steps,
         "step_status": {"valid": R["valid"], "rho_min": R["rho_min"], "p_min": R["p_min"], "dt": dt},
         "stage_ms": stages,
@@ -304,13 +396,14 @@ def run_ours(args):
         "clocks": R["clocks"],
         "e2e": {"value": dofs / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": state_bytes,
                 "d2h_bytes_per_step": state_bytes},
+        "runs": {k: {"value": v["value"], "ms_per_step": v["ms"] / args.steps, "valid": v["valid"],
+                     "clocks_sm_mhz": v["clocks"].get("sm_mhz"), "reasons": v["clocks"].get("reasons")}
+                 for k, v in runs.items()},
     }
-    if "float64" in results and head != "float64":
-        P = results["float64"]
-        line["plain"] = {"value": P["value"], "ms_per_step": P["ms"] / args.steps, "dtype": "f64",
-                         "clocks": P["clocks"], "valid": P["valid"]}
     if accuracy:
         line["accuracy"] = accuracy
+    if train:
+        line["predictor"] = train
     if cpu:
         line["cpu_baseline"] = cpu
     if rank == 0:
@@ -322,7 +415,8 @@ def run_ours(args):
 
 class CpuSample:
     """Oracle (numpy float64 restatement of the reference) on a bounded sample of the workload:
-    a coarse sphere O/H grid at P3, whole checked SSP-RK3 steps, all host threads for BLAS."""
+    a coarse sphere O/H grid at P3 from the same shocked start, whole checked SSP-RK3 steps with
+    MOOD, all host threads for BLAS."""
 
     def __init__(self):
         from oracle.dg import Operator, PositivityLimiter, TimeIntegrator
@@ -336,9 +430,21 @@ class CpuSample:
         self.bc = FarfieldWallBoundary(gas, mesh.physical_names, farfield, wall_temperature=T_WALL / T_INF)
         from oracle.subcell import MOODLimiter
         self.integ = TimeIntegrator(op, cfl=0.3, limiter=MOODLimiter(op, positivity=PositivityLimiter(op)))
-        U = gas.to_conserved(np.array([1.0, u, 0.0, 0.0, 1.0]))
-        self.states = {b.element_type: np.broadcast_to(U, (len(b.connectivity), 64, 5)).copy()
-                       for b in mesh.element_blocks}
+        from oracle.elements import RefElement
+        g, M = GAMMA, MACH
+        rho2 = (g + 1) * M ** 2 / ((g - 1) * M ** 2 + 2)
+        p2 = 1 + 2 * g / (g + 1) * (M ** 2 - 1)
+        self.states = {}
+        for b in mesh.element_blocks:
+            # the same shocked start as the GPU run (bow_shock_state), at first-order node positions
+            nodes = RefElement(b.element_type, 3).nodes
+            xyz = np.einsum("qi,eid->eqd", RefElement(b.element_type, 1).basis(nodes), mesh.points[b.connectivity])
+            inside = shock_layer(xyz)
+            W = np.zeros(xyz.shape[:-1] + (5,))
+            W[..., 0] = np.where(inside, rho2, 1.0)
+            W[..., 1] = np.where(inside, u / rho2, u)
+            W[..., 4] = np.where(inside, p2, 1.0)
+            self.states[b.element_type] = gas.to_conserved(W)
         self.dt = self.integ.stable_dt(self.states)
         self.elements = sum(len(b.connectivity) for b in mesh.element_blocks)
         self.dofs = self.elements * 64
@@ -394,6 +500,11 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--limiter", default="mood", choices=["mood", "positivity"])
+    ap.add_argument("--start", default="shock", choices=["shock", "uniform"])
+    ap.add_argument("--learned", type=int, default=1, help="train and use the troubled-cell predictor (MOOD)")
+    ap.add_argument("--train-steps", type=int, default=20)
+    ap.add_argument("--train-epochs", type=int, default=8)
+    ap.add_argument("--threshold", type=float, default=0.5)
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "float64"],
                     help="both: time the plain float64 step and the mixed step from the same state and dt; "
                          "the mixed one is the headline value, the plain one and their density L2 "

@@ -62,9 +62,10 @@ typedef struct {
   int limiter;                /* stage limiter of dgb_ssprk3_step: 0 none, 1 positivity, 2 MOOD */
   int reconstruction;         /* MOOD subcell faces: 0 constant, 1 tvd, 2 weno (CWENO-Z) */
   int precision;              /* 0 float64 throughout; 1 mixed: float32 arithmetic and shared-memory
-                                 staging in the hexahedron lift and volume kernels (state, face
-                                 fluxes, limiters, reductions and the stage update stay float64);
-                                 needs the sum-factorised single-hexahedron-block path */
+                                 staging in the hexahedron trace, BR2-lift, volume and finalize
+                                 kernels (state, face fluxes, limiters, reductions and the stage
+                                 update stay float64); needs the sum-factorised
+                                 single-hexahedron-block path */
 } dgb_params;
 
 /* One element block (hybrid/geometry.py:139-203 metrics, precomputed by the host). */

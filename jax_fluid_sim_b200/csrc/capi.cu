@@ -126,16 +126,15 @@ int blocks_for(long n, int per) { return (int)((n + per - 1) / per); }
 // ------------------------------------------------------------------ RHS pipeline
 template <int P, int NV, bool SPLIT, typename R>
 int run_rhs_hex(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStream_t st, cudaEvent_t* ev) {
-  using L = HexSmem<P, NV>;
   using LR = HexSmem<P, NV, R>;
   const DevPlan& D = p->dev;
   const int E = D.blk[0].E;
-  const size_t sm_tr = sizeof(double) * (size_t)L::TRACES, sm_li = sizeof(R) * (size_t)LR::LIFT;
-  const size_t sm_vo = sizeof(R) * (size_t)LR::template VOLUME<SPLIT>, sm_fi = sizeof(double) * (size_t)L::FINAL;
+  const size_t sm_tr = sizeof(R) * (size_t)LR::TRACES, sm_li = sizeof(R) * (size_t)LR::LIFT;
+  const size_t sm_vo = sizeof(R) * (size_t)LR::template VOLUME<SPLIT>, sm_fi = sizeof(R) * (size_t)LR::FINAL;
   int rc;
   if (ev) CK(cudaEventRecord(ev[0], st));
-  if ((rc = prepare(k_hex_traces<P, NV>, sm_tr))) return rc;
-  k_hex_traces<P, NV><<<E, kThreads, sm_tr, st>>>(D, S, 0, p->hex_tables, p->hex_codes);
+  if ((rc = prepare(k_hex_traces<P, NV, R>, sm_tr))) return rc;
+  k_hex_traces<P, NV, R><<<E, kThreads, sm_tr, st>>>(D, S, 0, p->hex_tables, p->hex_codes);
   if (ev) CK(cudaEventRecord(ev[1], st));
   k_face_flux<NV><<<blocks_for((long)D.face[1].F * D.face[1].nq, kThreads), kThreads, 0, st>>>(D, S, 1);
   if (ev) CK(cudaEventRecord(ev[2], st));
@@ -150,8 +149,8 @@ int run_rhs_hex(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStre
   if (D.viscous)
     k_face_visc<NV><<<blocks_for((long)D.face[1].F * D.face[1].nq, kThreads), kThreads, 0, st>>>(D, 1);
   if (ev) CK(cudaEventRecord(ev[5], st));
-  if ((rc = prepare(k_hex_finalize<P, NV, SPLIT>, sm_fi))) return rc;
-  k_hex_finalize<P, NV, SPLIT><<<E, kThreads, sm_fi, st>>>(D, S, 0, p->hex_tables, p->hex_codes, A);
+  if ((rc = prepare(k_hex_finalize<P, NV, SPLIT, R>, sm_fi))) return rc;
+  k_hex_finalize<P, NV, SPLIT, R><<<E, kThreads, sm_fi, st>>>(D, S, 0, p->hex_tables, p->hex_codes, A);
   if (ev) CK(cudaEventRecord(ev[6], st));
   CK(cudaGetLastError());
   return DGB_OK;

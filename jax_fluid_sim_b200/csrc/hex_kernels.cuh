@@ -143,9 +143,9 @@ struct HexSmem {
   static constexpr int N = D::N, Q = D::Q, QF = D::QF, N2 = D::N2, N3 = D::N3, Q3 = D::Q3, QF2 = D::QF2;
   static constexpr int T = (int)((sizeof(HexTablesT<R>) + sizeof(R) - 1) / sizeof(R));
   static constexpr int MS = N3 + 1;                 // padded row stride of the staged M^-1 (transposed)
-  // traces: U, v, then face scratch
+  // traces: U, v, then the six faces' slabs, contraction scratch, face values and tangential derivatives
   static constexpr int TR_U = T, TR_V = TR_U + NV * N3, TR_W = TR_V + 4 * N3;
-  static constexpr int TRACES = TR_W + (NV + 8) * N2 + (NV + 8) * N * QF + (NV + 16) * QF2;
+  static constexpr int TRACES = TR_W + 6 * (NV + 8) * (N2 + N * QF + QF2) + 2 * 24 * QF2;
   // lift: staged M^-T, b per face on its slab, b on all nodes, scratch
   static constexpr int LI_BS = T, LI_B = LI_BS + 6 * 12 * N2, LI_W = LI_B + 12 * N3;
   static constexpr int LIFT = LI_W + 12 * QF2 + 12 * QF * N + 12 * N2 + 12 * QF2;
@@ -160,7 +160,7 @@ struct HexSmem {
   static constexpr int VOLUME = VO_W + cmax(VOL1, VOL2<SPLIT>);
   // finalize: staged M^-T, residuals, face scratch
   static constexpr int FI_R = T, FI_W = FI_R + 2 * NV * N3;
-  static constexpr int FINAL = FI_W + 2 * NV * QF2 + 2 * NV * QF * N + 2 * NV * N2;
+  static constexpr int FINAL = FI_W + 6 * 2 * NV * (QF2 + QF * N) + cmax(6 * 2 * NV * N2, 4 * NV * N3);
 };
 
 template <int P>
@@ -192,101 +192,120 @@ __device__ __forceinline__ void stage_minv(const double* Mg, const int* lex2node
 // --------------------------------------------------------------------------------------------
 // Face traces of one hexahedron: anchor-form U, viscous variables, their raw physical
 // gradients, for each of the six faces, in the owner's face-point order.
-template <int P, int NV>
+template <int P, int NV, typename R = double>
 __global__ void __launch_bounds__(kThreads) k_hex_traces(const DevPlan P_, const StatePtrs S, int b,
                                                         const HexTables tables, const HexCodes codes) {
   using D = HexDims<P>;
-  using L = HexSmem<P, NV>;
-  constexpr int N = D::N, QF = D::QF;
-  extern __shared__ double smem[];
-  HexTables* tb = reinterpret_cast<HexTables*>(smem);
-  double* U = smem + L::TR_U;        // [NV][N3], minus anchor
-  double* V = smem + L::TR_V;        // [4][N3]
-  double* W = smem + L::TR_W;
+  using L = HexSmem<P, NV, R>;
+  constexpr int N = D::N, QF = D::QF, N2 = D::N2, N3 = D::N3, QF2 = D::QF2;
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  R* smem = reinterpret_cast<R*>(dyn_smem);
+  HexTablesT<R>* tb = reinterpret_cast<HexTablesT<R>*>(smem);
+  R* U = smem + L::TR_U;             // [NV][N3], minus anchor
+  R* V = smem + L::TR_V;             // [4][N3]
+  // all six faces at once, channel blocks [U: 6*NV][v: 6*4][dv/dn: 6*4], each of N2 (slabs)
+  // or QF2 (face points) values
+  constexpr int CH = 6 * (NV + 8);
+  R* slabs = smem + L::TR_W;
+  R* ftmp = slabs + CH * N2;         // tensor2 scratch [CH][N][QF]
+  R* fo = ftmp + CH * N * QF;        // [CH][QF2] values at the canonical face points
+  R* g1 = fo + CH * QF2;             // [6*4][QF2] derivative of v along a1
+  R* g2 = g1 + 24 * QF2;             // [6*4][QF2] derivative of v along a2
+  __shared__ int fslot[6], fperm[6];
   const BlockDev& B = P_.blk[b];
+  const FaceDev& fd = P_.face[1];
   const int e = blockIdx.x;
   load_tables<P>(tables, tb);
-  const double* Ug = S.b[b] + (size_t)e * D::N3 * NV;
+  const double* Ug = S.b[b] + (size_t)e * N3 * NV;
   __shared__ double anchor[NV];
   if (threadIdx.x < NV) anchor[threadIdx.x] = Ug[threadIdx.x];
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < NV * D::N3; idx += blockDim.x) {
-    const int v = idx / D::N3, l = idx % D::N3;
-    U[idx] = Ug[tb->lex2node[l] * NV + v] - anchor[v];
+  if (threadIdx.x < 6) {
+    int ft, f, side;
+    decode_face(B.elem_face[e * 6 + threadIdx.x], ft, f, side);
+    fslot[threadIdx.x] = (f * 2 + side) * QF2;
+    fperm[threadIdx.x] = (side == 0 ? fd.oc[f] : fd.nc[f]) * QF2;
   }
-  if (P_.viscous) {
-    for (int l = threadIdx.x; l < D::N3; l += blockDim.x) {
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
+    const int v = idx / N3, l = idx % N3;
+    U[idx] = (R)(Ug[tb->lex2node[l] * NV + v] - anchor[v]);
+  }
+  const bool visc = P_.viscous;
+  if (visc) {
+    for (int l = threadIdx.x; l < N3; l += blockDim.x) {
       const int node = tb->lex2node[l];
       double u[NV], vv[4];
 #pragma unroll
       for (int v = 0; v < NV; ++v) u[v] = Ug[node * NV + v];
       viscous_vars<NV>(P_.ph, u, vv);
 #pragma unroll
-      for (int m = 0; m < 4; ++m) V[m * D::N3 + l] = vv[m];
+      for (int m = 0; m < 4; ++m) V[m * N3 + l] = (R)vv[m];
     }
   }
   __syncthreads();
-  double* slab = W;                              // [NV+4+4][N][N]: U, v, dv/dn
-  double* tmp = slab + (NV + 8) * N * N;         // tensor2 scratch
-  double* fu = tmp + (NV + 8) * N * QF;          // [NV][QF2] U at canonical face points
-  double* fv = fu + NV * QF * QF;                // [4][QF2]
-  double* gn = fv + 4 * QF * QF;                 // [4][QF2] normal derivative
-  double* g1 = gn + 4 * QF * QF;                 // [4][QF2] derivative along a1
-  double* g2 = g1 + 4 * QF * QF;                 // [4][QF2] derivative along a2
-  const FaceDev& fd = P_.face[1];
-  for (int lf = 0; lf < 6; ++lf) {
-    int ft, f, side;
-    decode_face(B.elem_face[e * 6 + lf], ft, f, side);
+  const int nch = visc ? CH : 6 * NV;
+  for (int idx = threadIdx.x; idx < nch * N2; idx += blockDim.x) {
+    const int j1 = idx % N, j2 = (idx / N) % N, c = idx / N2;
+    int lf, m, kind;                   // kind 0: U, 1: v, 2: dv/dn
+    if (c < 6 * NV) {
+      lf = c / NV, m = c % NV, kind = 0;
+    } else if (c < 6 * NV + 24) {
+      lf = (c - 6 * NV) / 4, m = (c - 6 * NV) % 4, kind = 1;
+    } else {
+      lf = (c - 6 * NV - 24) / 4, m = (c - 6 * NV - 24) % 4, kind = 2;
+    }
     int a0, end, a1, a2;
     hex_face_axes(lf, a0, end, a1, a2);
-    face_slab<NV, N>(U, slab, a0, end, a1, a2);
-    if (P_.viscous) {
-      face_slab<4, N>(V, slab + NV * N * N, a0, end, a1, a2);
-      const double* dn = end ? tb->d1 : tb->d0;
-      for (int idx = threadIdx.x; idx < 4 * N * N; idx += blockDim.x) {
-        const int j1 = idx % N, j2 = (idx / N) % N, m = idx / (N * N);
-        double s = 0.0;
-#pragma unroll
-        for (int j0 = 0; j0 < N; ++j0) {
-          const int l = j0 * axis_stride<N>(a0) + j1 * axis_stride<N>(a1) + j2 * axis_stride<N>(a2);
-          s += dn[j0] * V[m * D::N3 + l];
-        }
-        slab[(NV + 4) * N * N + idx] = s;
-      }
-    }
-    __syncthreads();
-    if (P_.viscous) {
-      tensor2<NV + 8, N, N, QF, QF>(slab, fu, tmp, tb->bf, tb->bf);
-      tensor2<4, N, N, QF, QF>(slab + NV * N * N, g1, tmp, tb->df, tb->bf);
-      tensor2<4, N, N, QF, QF>(slab + NV * N * N, g2, tmp, tb->bf, tb->df);
+    const int st0 = axis_stride<N>(a0), off = j1 * axis_stride<N>(a1) + j2 * axis_stride<N>(a2);
+    R val;
+    if (kind == 0) {
+      val = U[m * N3 + end * st0 + off];
+    } else if (kind == 1) {
+      val = V[m * N3 + end * st0 + off];
     } else {
-      tensor2<NV, N, N, QF, QF>(slab, fu, tmp, tb->bf, tb->bf);
+      const R* dn = end ? tb->d1 : tb->d0;
+      val = R(0);
+#pragma unroll
+      for (int j0 = 0; j0 < N; ++j0) val += dn[j0] * V[m * N3 + j0 * st0 + off];
     }
-    const int tc = side == 0 ? fd.oc[f] : fd.nc[f];
-    const uint8_t* perm = codes.perm + tc * QF * QF;
-    const size_t slot = ((size_t)f * 2 + side) * (QF * QF);
-    for (int idx = threadIdx.x; idx < QF * QF * NV; idx += blockDim.x) {
-      const int q = idx / NV, v = idx % NV;
-      fd.trA[(slot + q) * NV + v] = anchor[v] + fu[v * QF * QF + perm[q]];
+    slabs[idx] = val;
+  }
+  __syncthreads();
+  if (visc) {
+    tensor2<CH, N, N, QF, QF>(slabs, fo, ftmp, tb->bf, tb->bf);
+    tensor2<24, N, N, QF, QF>(slabs + 6 * NV * N2, g1, ftmp, tb->df, tb->bf);
+    tensor2<24, N, N, QF, QF>(slabs + 6 * NV * N2, g2, ftmp, tb->bf, tb->df);
+  } else {
+    tensor2<6 * NV, N, N, QF, QF>(slabs, fo, ftmp, tb->bf, tb->bf);
+  }
+  for (int idx = threadIdx.x; idx < 6 * QF2 * NV; idx += blockDim.x) {
+    const int lf = idx / (QF2 * NV), q = (idx / NV) % QF2, v = idx % NV;
+    const int c = codes.perm[fperm[lf] + q];
+    fd.trA[((size_t)fslot[lf] + q) * NV + v] = anchor[v] + (double)fo[(lf * NV + v) * QF2 + c];
+  }
+  if (visc) {
+    const R* fv = fo + 6 * NV * QF2;          // [6][4][QF2]
+    const R* gn = fv + 24 * QF2;              // [6][4][QF2]
+    for (int idx = threadIdx.x; idx < 6 * QF2 * 4; idx += blockDim.x) {
+      const int lf = idx / (QF2 * 4), q = (idx / 4) % QF2, m = idx % 4;
+      const int c = codes.perm[fperm[lf] + q];
+      fd.trV[((size_t)fslot[lf] + q) * 4 + m] = (double)fv[(lf * 4 + m) * QF2 + c];
     }
-    if (P_.viscous) {
-      for (int idx = threadIdx.x; idx < QF * QF * 4; idx += blockDim.x) {
-        const int q = idx / 4, m = idx % 4;
-        fd.trV[(slot + q) * 4 + m] = fv[m * QF * QF + perm[q]];
-      }
-      for (int idx = threadIdx.x; idx < QF * QF * 12; idx += blockDim.x) {
-        const int q = idx / 12, m = (idx % 12) / 3, d = idx % 3;
-        const int c = perm[q];
-        const double gnv = gn[m * QF * QF + c], g1v = g1[m * QF * QF + c], g2v = g2[m * QF * QF + c];
-        // reference gradient component along axis r: normal (a0) or tangential (a1 < a2)
-        const double gx = a0 == 0 ? gnv : g1v;
-        const double gy = a0 == 1 ? gnv : (a0 == 0 ? g1v : g2v);
-        const double gz = a0 == 2 ? gnv : g2v;
-        const double* J = fd.jinv + (slot + q) * 9;
-        fd.trG[(slot + q) * 12 + m * 3 + d] = gx * J[0 * 3 + d] + gy * J[1 * 3 + d] + gz * J[2 * 3 + d];
-      }
+    for (int idx = threadIdx.x; idx < 6 * QF2 * 12; idx += blockDim.x) {
+      const int lf = idx / (QF2 * 12), q = (idx / 12) % QF2, m = (idx % 12) / 3, d = idx % 3;
+      int a0, end, a1, a2;
+      hex_face_axes(lf, a0, end, a1, a2);
+      const int c = codes.perm[fperm[lf] + q];
+      const int k = (lf * 4 + m) * QF2 + c;
+      const R gnv = gn[k], g1v = g1[k], g2v = g2[k];
+      // reference gradient component along axis r: normal (a0) or tangential (a1 < a2)
+      const R gx = a0 == 0 ? gnv : g1v;
+      const R gy = a0 == 1 ? gnv : (a0 == 0 ? g1v : g2v);
+      const R gz = a0 == 2 ? gnv : g2v;
+      const size_t pt = (size_t)fslot[lf] + q;
+      const double* J = fd.jinv + pt * 9;
+      fd.trG[pt * 12 + m * 3 + d] = (double)(gx * (R)J[0 * 3 + d] + gy * (R)J[1 * 3 + d] + gz * (R)J[2 * 3 + d]);
     }
-    __syncthreads();
   }
 }
 
@@ -551,122 +570,139 @@ __global__ void __launch_bounds__(kThreads) k_hex_volume(const DevPlan P_, const
 // Gather face contributions into the nodes (transposed face interpolation per face, in local
 // face order: deterministic), apply M^-1 (staged in shared memory), and write either the
 // right-hand sides or the fused SSP-RK stage.  Rinv holds the total volume residual when !SPLIT.
-template <int P, int NV, bool SPLIT>
+template <int P, int NV, bool SPLIT, typename R = double>
 __global__ void __launch_bounds__(kThreads) k_hex_finalize(const DevPlan P_, const StatePtrs S, int b,
                                                           const HexTables tables, const HexCodes codes,
                                                           const FinalizeArgs A) {
   using D = HexDims<P>;
-  using L = HexSmem<P, NV>;
-  constexpr int N = D::N, QF = D::QF, N3 = D::N3, MS = L::MS;
-  extern __shared__ double smem[];
-  HexTables* tb = reinterpret_cast<HexTables*>(smem);
-  double* Ri = smem + L::FI_R;                 // [NV][N3] lexicographic
-  double* Rv = Ri + NV * N3;
-  double* hc = smem + L::FI_W;                 // [2*NV][QF2] face flux at canonical points
-  double* tmp = hc + 2 * NV * QF * QF;         // [2*NV][QF][N]
-  double* hs = tmp + 2 * NV * QF * N;          // [2*NV][N][N]
+  using L = HexSmem<P, NV, R>;
+  constexpr int N = D::N, QF = D::QF, N2 = D::N2, N3 = D::N3, QF2 = D::QF2;
+  constexpr int C = SPLIT ? 2 * NV : NV;        // channels: inviscid (and viscous) residual
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  R* smem = reinterpret_cast<R*>(dyn_smem);
+  HexTablesT<R>* tb = reinterpret_cast<HexTablesT<R>*>(smem);
+  R* Rr = smem + L::FI_R;                       // [C][N3] lexicographic (Ri, then Rv)
+  R* hc = smem + L::FI_W;                       // [6][C][QF2] face flux at canonical points
+  R* tmp = hc + 6 * C * QF2;                    // [6][C][QF][N]
+  R* hs = tmp + 6 * C * QF * N;                 // [6][C][N2]; reused for the M^-1 partial sums
   __shared__ int node2lex[64];
+  __shared__ int fslot[6], fperm[6], fface[6];
   const BlockDev& B = P_.blk[b];
+  const FaceDev& fd = P_.face[1];
   const int e = blockIdx.x;
   load_tables<P>(tables, tb);
+  if (threadIdx.x < 6) {
+    int ft, f, side;
+    decode_face(B.elem_face[e * 6 + threadIdx.x], ft, f, side);
+    fslot[threadIdx.x] = (f * 2 + side) * QF2;
+    fperm[threadIdx.x] = (side == 0 ? fd.oc[f] : fd.nc[f]) * QF2;
+    fface[threadIdx.x] = (f << 1) | side;
+  }
   __syncthreads();
   for (int l = threadIdx.x; l < N3; l += blockDim.x) node2lex[tb->lex2node[l]] = l;
   const size_t base = (size_t)e * N3 * NV;
   const bool visc = P_.viscous;
-  for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
-    Ri[idx] = B.Rinv[base + idx];
-    Rv[idx] = (SPLIT && visc) ? B.Rvis[base + idx] : 0.0;
+  // the six faces' fluxes, signed for this side, at the canonical face points
+  for (int idx = threadIdx.x; idx < 6 * QF2 * NV; idx += blockDim.x) {
+    const int lf = idx / (QF2 * NV), q = (idx / NV) % QF2, v = idx % NV;
+    const int f = fface[lf] >> 1, side = fface[lf] & 1;
+    const double si = side == 0 ? -1.0 : 1.0;
+    const double hi = si * fd.fluxI[((size_t)fslot[lf] + q) * NV + v];
+    const double hv = visc ? -si * fd.fluxV[((size_t)f * QF2 + q) * NV + v] : 0.0;
+    const int c = codes.perm[fperm[lf] + q];
+    if (SPLIT) {
+      hc[(lf * C + v) * QF2 + c] = (R)hi;
+      hc[(lf * C + NV + v) * QF2 + c] = (R)hv;
+    } else {
+      hc[(lf * C + v) * QF2 + c] = (R)(hi + hv);
+    }
   }
   __syncthreads();
-  const double* MT = B.minv + (size_t)e * N3 * N3;   // M^-T in element node order
-  const FaceDev& fd = P_.face[1];
-  constexpr int C = SPLIT ? 2 * NV : NV;
-  for (int lf = 0; lf < 6; ++lf) {
-    int ft, f, side;
-    decode_face(B.elem_face[e * 6 + lf], ft, f, side);
-    int a0, end, a1, a2;
-    hex_face_axes(lf, a0, end, a1, a2);
-    const int tc = side == 0 ? fd.oc[f] : fd.nc[f];
-    const uint8_t* perm = codes.perm + tc * QF * QF;
-    const double* fi = fd.fluxI + ((size_t)f * 2 + side) * QF * QF * NV;
-    const double* fv = fd.fluxV + (size_t)f * QF * QF * NV;
-    const double si = side == 0 ? -1.0 : 1.0;
-    for (int idx = threadIdx.x; idx < QF * QF * NV; idx += blockDim.x) {
-      const int q = idx / NV, v = idx % NV;
-      const double hi = si * fi[idx];
-      const double hv = visc ? -si * fv[idx] : 0.0;
-      if (SPLIT) {
-        hc[v * QF * QF + perm[q]] = hi;
-        hc[(NV + v) * QF * QF + perm[q]] = hv;
-      } else {
-        hc[v * QF * QF + perm[q]] = hi + hv;
-      }
+  tensor2<6 * C, QF, QF, N, N>(hc, hs, tmp, tb->bfT, tb->bfT);
+  // residual plus the face terms of every face holding the node, faces in local order
+  for (int idx = threadIdx.x; idx < C * N3; idx += blockDim.x) {
+    const int c = idx / N3, l = idx % N3;
+    const int xyz[3] = {l % N, (l / N) % N, l / N2};
+    R acc = (R)(c < NV ? B.Rinv[base + c * N3 + l] : ((SPLIT && visc) ? B.Rvis[base + (c - NV) * N3 + l] : 0.0));
+#pragma unroll
+    for (int lf = 0; lf < 6; ++lf) {
+      int a0, end, a1, a2;
+      hex_face_axes(lf, a0, end, a1, a2);
+      if (xyz[a0] == end) acc += hs[(lf * C + c) * N2 + xyz[a2] * N + xyz[a1]];
     }
-    __syncthreads();
-    tensor2<C, QF, QF, N, N>(hc, hs, tmp, tb->bfT, tb->bfT);
-    for (int idx = threadIdx.x; idx < C * N * N; idx += blockDim.x) {
-      const int j1 = idx % N, j2 = (idx / N) % N, c = idx / (N * N);
-      const int l = end * axis_stride<N>(a0) + j1 * axis_stride<N>(a1) + j2 * axis_stride<N>(a2);
-      if (c < NV) Ri[c * N3 + l] += hs[idx];
-      else Rv[(c - NV) * N3 + l] += hs[idx];
-    }
-    __syncthreads();
+    Rr[idx] = acc;
   }
-  // M^-1: out[node(li)] = sum_lj Mt[lj][li] R[lj]; a thread owns node li and a group of
-  // up to VB variables, consecutive threads take consecutive li (conflict-free staged reads)
+  __syncthreads();
+  // M^-1: out[node(i)] = sum_j M^-T[j][i] R[lex(j)].  Work items (column half, variable group,
+  // node i); consecutive threads take consecutive i, so the M^-T rows are read coalesced.  The
+  // halves are added in a fixed order.
   constexpr int VB = NV < 8 ? NV : 8;
   constexpr int NG = (NV + VB - 1) / VB;
-  for (int idx = threadIdx.x; idx < NG * N3; idx += blockDim.x) {
-    const int i = idx % N3, v0 = (idx / N3) * VB;      // i: element node index
-    double ri[VB], rv[VB];
+  constexpr int HALVES = NG * N3 * 2 <= kThreads ? 2 : 1;
+  constexpr int JH = (N3 + HALVES - 1) / HALVES;      // N3 is odd at P2
+  const double* MT = B.minv + (size_t)e * N3 * N3;   // M^-T in element node order
+  R* part = hs;                                       // [HALVES][2][NV][N3]
+  for (int idx = threadIdx.x; idx < HALVES * NG * N3; idx += blockDim.x) {
+    const int i = idx % N3, g = (idx / N3) % NG, h = idx / (NG * N3);
+    const int v0 = g * VB;
+    R ri[VB], rv[VB];
 #pragma unroll
-    for (int k = 0; k < VB; ++k) ri[k] = rv[k] = 0.0;
+    for (int k = 0; k < VB; ++k) ri[k] = rv[k] = R(0);
+    const int j1 = (h + 1) * JH < N3 ? (h + 1) * JH : N3;
 #pragma unroll 4
-    for (int j = 0; j < N3; ++j) {
-      const double m = __ldg(MT + (size_t)j * N3 + i);
+    for (int j = h * JH; j < j1; ++j) {
+      const R m = (R)__ldg(MT + (size_t)j * N3 + i);
       const int lj = node2lex[j];
 #pragma unroll
       for (int k = 0; k < VB; ++k) {
         if (v0 + k < NV) {
-          ri[k] += m * Ri[(v0 + k) * N3 + lj];
-          if (SPLIT) rv[k] += m * Rv[(v0 + k) * N3 + lj];
+          ri[k] += m * Rr[(v0 + k) * N3 + lj];
+          if (SPLIT) rv[k] += m * Rr[(NV + v0 + k) * N3 + lj];
         }
       }
     }
-    const size_t ob = base + (size_t)i * NV;
 #pragma unroll
     for (int k = 0; k < VB; ++k) {
-      const int v = v0 + k;
-      if (v >= NV) continue;
-      const size_t o = ob + v;
-      if (!A.stage) {
-        if (A.out_inv[b]) A.out_inv[b][o] = ri[k];
-        if (SPLIT && A.out_vis[b]) A.out_vis[b][o] = rv[k];
-      } else {
-        const double total = SPLIT ? ri[k] + rv[k] : ri[k];
-        const double eul = S.b[b][o] + A.dt * total;
-        if (SPLIT && A.out_vis[b]) A.out_vis[b][o] = rv[k];
-        if (A.euler[b]) A.euler[b][o] = eul;
-        A.dst[b][o] = A.alpha * A.base[b][o] + A.beta * eul;
-      }
+      if (v0 + k >= NV) continue;
+      part[((h * 2 + 0) * NV + v0 + k) * N3 + i] = ri[k];
+      part[((h * 2 + 1) * NV + v0 + k) * N3 + i] = rv[k];
+    }
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
+    const int v = idx / N3, i = idx % N3;
+    R si = part[(0 * NV + v) * N3 + i], sv = part[(1 * NV + v) * N3 + i];
+    if (HALVES == 2) {
+      si += part[(2 * NV + v) * N3 + i];
+      sv += part[(3 * NV + v) * N3 + i];
+    }
+    const size_t o = base + (size_t)i * NV + v;
+    const double ri = (double)si, rv = (double)sv;
+    if (!A.stage) {
+      if (A.out_inv[b]) A.out_inv[b][o] = ri;
+      if (SPLIT && A.out_vis[b]) A.out_vis[b][o] = rv;
+    } else {
+      const double total = SPLIT ? ri + rv : ri;
+      const double eul = S.b[b][o] + A.dt * total;
+      if (SPLIT && A.out_vis[b]) A.out_vis[b][o] = rv;
+      if (A.euler[b]) A.euler[b][o] = eul;
+      A.dst[b][o] = A.alpha * A.base[b][o] + A.beta * eul;
     }
   }
 }
 
 // --------------------------------------------------------------------------------------------
-// Zhang-Shu positivity limiter for hexahedra (hybrid/limiter.py:69-147) with the samples built
-// by sum factorisation: nodes, volume points (tensor Gauss grid) and the Gauss grids of the six
-// faces -- for a hexahedron mesh these are exactly the distinct face points the reference
-// collects from its face groups.
 // Limiter / detector samples of one element (hybrid/limiter.py:29-67): the state at the nodes,
 // at the volume quadrature points and at the face quadrature points of the six faces, in that
 // order -> Smp[v][NS]; U receives the element state in lexicographic order and vq the
-// volume-point values [NV][Q3].  Ends without a barrier: callers synchronise before reading.
+// volume-point values [NV][Q3].  The six faces go through one 2-D contraction (their slabs
+// stacked as 6*NV channels) in fs, which holds 6*NV*(N2 + N*QF + QF2) values.  Ends without a
+// barrier: callers synchronise before reading.
 template <int P, int NV>
 __device__ void hex_samples(const HexTables* tb, const double* Ug, double* U, double* Smp, double* t1, double* t2,
-                            double* slab, double* vq) {
+                            double* vq, double* fs) {
   using D = HexDims<P>;
-  constexpr int N = D::N, Q = D::Q, QF = D::QF, N3 = D::N3, Q3 = D::Q3, QF2 = D::QF2;
+  constexpr int N = D::N, Q = D::Q, QF = D::QF, N2 = D::N2, N3 = D::N3, Q3 = D::Q3, QF2 = D::QF2;
   constexpr int NS = N3 + Q3 + 6 * QF2;
   for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
     const int v = idx / N3, l = idx % N3;
@@ -680,20 +716,27 @@ __device__ void hex_samples(const HexTables* tb, const double* Ug, double* U, do
     const int v = idx / Q3, q = idx % Q3;
     Smp[v * NS + N3 + q] = vq[idx];
   }
-  for (int lf = 0; lf < 6; ++lf) {
+  double* slabs = fs;                    // [6][NV][N2]
+  double* ftmp = slabs + 6 * NV * N2;    // [6][NV][N][QF]
+  double* fo = ftmp + 6 * NV * N * QF;   // [6][NV][QF2]
+  for (int idx = threadIdx.x; idx < 6 * NV * N2; idx += blockDim.x) {
+    const int j1 = idx % N, j2 = (idx / N) % N, c = idx / N2, lf = c / NV, v = c % NV;
     int a0, end, a1, a2;
     hex_face_axes(lf, a0, end, a1, a2);
-    __syncthreads();
-    face_slab<NV, N>(U, slab, a0, end, a1, a2);
-    __syncthreads();
-    tensor2<NV, N, N, QF, QF>(slab, t2, t1, tb->bf, tb->bf);
-    for (int idx = threadIdx.x; idx < NV * QF2; idx += blockDim.x) {
-      const int v = idx / QF2, q = idx % QF2;
-      Smp[v * NS + N3 + Q3 + lf * QF2 + q] = t2[idx];
-    }
+    slabs[idx] = U[v * N3 + end * axis_stride<N>(a0) + j1 * axis_stride<N>(a1) + j2 * axis_stride<N>(a2)];
+  }
+  __syncthreads();
+  tensor2<6 * NV, N, N, QF, QF>(slabs, fo, ftmp, tb->bf, tb->bf);
+  for (int idx = threadIdx.x; idx < 6 * NV * QF2; idx += blockDim.x) {
+    const int q = idx % QF2, c = idx / QF2, lf = c / NV, v = c % NV;
+    Smp[v * NS + N3 + Q3 + lf * QF2 + q] = fo[idx];
   }
 }
 
+// Zhang-Shu positivity limiter for hexahedra (hybrid/limiter.py:69-147) with the samples built
+// by sum factorisation: nodes, volume points (tensor Gauss grid) and the Gauss grids of the six
+// faces -- for a hexahedron mesh these are exactly the distinct face points the reference
+// collects from its face groups.
 template <int P, int NV>
 __global__ void __launch_bounds__(kThreads) k_hex_positivity(const DevPlan P_, const StatePtrs S, int b,
                                                             const HexTables tables, const LimiterConst Lc) {
@@ -706,7 +749,8 @@ __global__ void __launch_bounds__(kThreads) k_hex_positivity(const DevPlan P_, c
   double* Smp = U + NV * N3;                        // [NV][NS]
   double* t1 = Smp + NV * NS;                       // contraction scratch
   double* t2 = t1 + NV * N * N * Q;
-  double* slab = t2 + NV * N * Q * Q;               // [NV][N2]
+  double* vq = t2 + NV * N * Q * Q;                 // [NV][Q3]
+  double* fs = vq + NV * Q3;                        // face contraction scratch
   __shared__ double mean[NV];
   __shared__ double red[kThreads / 32];
   __shared__ int red_nan;
@@ -715,9 +759,8 @@ __global__ void __launch_bounds__(kThreads) k_hex_positivity(const DevPlan P_, c
   const int e = blockIdx.x;
   load_tables<P>(tables, tb);
   double* Ug = S.b[b] + (size_t)e * N3 * NV;
-  double* vq = slab + NV * N * N;                   // [NV][Q3]
   __syncthreads();
-  hex_samples<P, NV>(tb, Ug, U, Smp, t1, t2, slab, vq);
+  hex_samples<P, NV>(tb, Ug, U, Smp, t1, t2, vq, fs);
   if (threadIdx.x == 0) red_nan = 0;
   __syncthreads();
   // cell mean from the volume samples
@@ -800,9 +843,9 @@ __global__ void __launch_bounds__(kThreads) k_hex_troubled(const DevPlan P_, con
   double* Smp = U + NV * N3;
   double* t1 = Smp + NV * NS;
   double* t2 = t1 + NV * N * N * Q;
-  double* slab = t2 + NV * N * Q * Q;
-  double* vq = slab + NV * N * N;
-  double* Mon = vq + NV * Q3;                       // [N3][2] (rho, p) in element node order
+  double* vq = t2 + NV * N * Q * Q;
+  double* fs = vq + NV * Q3;
+  double* Mon = fs + 6 * NV * (D::N2 + N * D::QF + D::QF2);   // [N3][2] (rho, p) in element node order
   __shared__ double mean[NV];
   __shared__ double red[4][kThreads / 32];
   const BlockDev& B = P_.blk[b];
@@ -811,7 +854,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_troubled(const DevPlan P_, con
   load_tables<P>(tables, tb);
   const double* Ug = S.b[b] + (size_t)e * N3 * NV;
   __syncthreads();
-  hex_samples<P, NV>(tb, Ug, U, Smp, t1, t2, slab, vq);
+  hex_samples<P, NV>(tb, Ug, U, Smp, t1, t2, vq, fs);
   for (int l = threadIdx.x; l < N3; l += blockDim.x) {
     double u[NV], W[NV];
 #pragma unroll
@@ -899,7 +942,7 @@ constexpr int hex_positivity_smem() {
   using D = HexDims<P>;
   constexpr int NS = D::N3 + D::Q3 + 6 * D::QF2;
   return HexSmem<P, NV>::T + NV * D::N3 + NV * NS + NV * D::N * D::N * D::Q + NV * D::N * D::Q * D::Q +
-         NV * D::N2 + NV * D::Q3;
+         NV * D::Q3 + 6 * NV * (D::N2 + D::N * D::QF + D::QF2);
 }
 
 template <int P, int NV>

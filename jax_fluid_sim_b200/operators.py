@@ -184,8 +184,8 @@ class HybridEulerOperator:
 
     def __init__(self, solver, br2_stabilization=None, sum_factorised=None, precision="float64"):
         """``precision``: "float64" (the reference's arithmetic) or "mixed" (float32 arithmetic in
-        the hexahedron BR2-lift and volume kernels; the state, face fluxes, limiters, reductions
-        and the stage update stay float64)."""
+        the hexahedron trace, BR2-lift, volume and finalize kernels; the state, face fluxes,
+        limiters, reductions and the stage update stay float64)."""
         self.solver = solver
         self.mesh = solver.mesh
         P = solver.polynomial_degree
