@@ -123,14 +123,24 @@ int dgb_plan_set_trace(dgb_plan* plan, int element_type, int face_type, int num_
                        int num_nodes, const double* basis, const double* basis_grad);
 /* Optional sum-factorised path for a mesh of one hexahedron block (hexahedron bases are
  * tensor products of the 1-D Lagrange basis on the nodes 0, 1, interior: hybrid/elements.py:
- * 199-274, 325-456).  line_tables: 136 doubles, in order bq[5][4], dq[5][4] (1-D basis and
+ * 199-274, 325-456).  line_tables: 157 doubles, in order bq[5][4], dq[5][4] (1-D basis and
  * derivative at the volume Gauss points), bqT[4][5], dqT[4][5] (transposes), bf[4][4], df[4][4]
- * (at the face Gauss points), bfT[4][4], d0[4], d1[4] (derivatives at 0 and 1), each block
+ * (at the face Gauss points), bfT[4][4], d0[4], d1[4] (derivatives at 0 and 1), m1i[4][4] (the
+ * inverse of the 1-D mass matrix), w1[5] (1-D volume Gauss weights on [0, 1]), each block
  * using its leading (points x nodes) entries; lex2node: 64 ints mapping lexicographic
  * (x fastest) node positions to element node indices; perm: [codes][face_points] map from the
  * owner's face-point order to the side element's canonical face grid. */
 int dgb_plan_set_hex(dgb_plan* plan, const double* line_tables, const int32_t* lex2node, int num_codes,
                      int face_points, const uint8_t* perm);
+
+/* Optional, after dgb_plan_set_hex: elements whose map is affine (a parallelepiped; the
+ * inverse Jacobian is the same at every volume point).  For them the kernels use the constant
+ * inverse Jacobian jinv[E][9] and det J det[E] instead of the per-point metrics, and apply
+ * M^-1 = coef * (m1i (x) m1i (x) m1i) with coef[E] = sliver scale / det J by three 1-D passes
+ * instead of reading the element's dense M^-1 (hybrid/geometry.py:181-192 computes the same
+ * matrix by quadrature).  affine[E] is 1 for those elements, 0 for the others. */
+int dgb_plan_set_hex_affine(dgb_plan* plan, const uint8_t* affine, const double* coef, const double* jinv,
+                            const double* det);
 int dgb_plan_finalize(dgb_plan* plan);
 int dgb_plan_destroy(dgb_plan* plan);
 /* Replace the physics/boundary/limiter constants of a finalized plan (same mesh and degree);
@@ -167,6 +177,15 @@ int dgb_admissibility(dgb_plan* plan, const dgb_state* U, dgb_status* status, vo
  *   recompute -> positivity -> blend -> positivity -> admissibility; *status receives the
  *   last stage's admissibility, as the reference's MOOD branch returns. */
 int dgb_ssprk3_step(dgb_plan* plan, const dgb_state* U, double dt, dgb_status* status, void* stream);
+
+/* dgb_ssprk3_step as one CUDA graph: the first call (and any call whose state pointers, dt or
+ * status pointer differ from the previous one, or that follows a change of the plan's
+ * parameters, MOOD set-up or predictor) captures the step's kernels on a private stream and
+ * instantiates them; every call then launches the graph on `stream`.  Same results as
+ * dgb_ssprk3_step (the same kernels in the same order).  A replay is one launch instead of the
+ * step's several hundred, which matters when the step is short; keep dt and the state buffers
+ * fixed across steps to replay without capturing again. */
+int dgb_ssprk3_step_graph(dgb_plan* plan, const dgb_state* U, double dt, dgb_status* status, void* stream);
 
 /* MOOD subcell finite-volume tables of one element block (hybrid/subcell.py:216-396):
  * 64 subcells, NI internal and NB boundary subfaces of the reference subdivision. */

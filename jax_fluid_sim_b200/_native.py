@@ -112,6 +112,7 @@ def lib():
             "dgb_plan_set_trace": [c_void_p, c_int, c_int, c_int, c_int, c_int, P_double, P_double],
             "dgb_plan_finalize": [c_void_p],
             "dgb_plan_set_hex": [c_void_p, P_double, P_int32, c_int, c_int, ctypes.POINTER(ctypes.c_uint8)],
+            "dgb_plan_set_hex_affine": [c_void_p, ctypes.POINTER(ctypes.c_uint8), P_double, P_double, P_double],
             "dgb_plan_destroy": [c_void_p],
             "dgb_plan_update_params": [c_void_p, ctypes.POINTER(Params)],
             "dgb_rhs": [c_void_p, ctypes.POINTER(State), ctypes.POINTER(State), ctypes.POINTER(State), c_void_p],
@@ -120,6 +121,7 @@ def lib():
             "dgb_troubled": [c_void_p, ctypes.POINTER(State), c_void_p, c_void_p, c_void_p],
             "dgb_admissibility": [c_void_p, ctypes.POINTER(State), c_void_p, c_void_p],
             "dgb_ssprk3_step": [c_void_p, ctypes.POINTER(State), c_double, c_void_p, c_void_p],
+            "dgb_ssprk3_step_graph": [c_void_p, ctypes.POINTER(State), c_double, c_void_p, c_void_p],
             "dgb_rhs_profile": [c_void_p, ctypes.POINTER(State), ctypes.POINTER(ctypes.c_float), c_void_p],
             "dgb_plan_set_subcells": [c_void_p, c_int, ctypes.POINTER(SubcellBlockDesc)],
             "dgb_plan_set_subcell_faces": [c_void_p, c_int, P_int32, P_int32],

@@ -37,11 +37,26 @@ namespace dgb {
 int set_error(int code, const std::string& msg) { return fail(code, msg); }
 }  // namespace dgb
 
+// What a captured step depends on besides the plan's device buffers: the caller's pointers, dt
+// and the generation of the plan's parameters (bumped by every change that alters a kernel
+// argument).  Compared bytewise, so it is zero-filled before it is set.
+struct StepKey {
+  double* block[DGB_MAX_BLOCKS];
+  double dt;
+  dgb_status* status;
+  unsigned long long generation;
+};
+
 struct dgb_plan {
   dgb_params prm;
   DevPlan dev;
   LimiterConst lim;
   std::vector<void*> allocations;
+  // CUDA graph of one checked step (dgb_ssprk3_step_graph)
+  unsigned long long generation = 0;
+  cudaStream_t capture_stream = nullptr;
+  cudaGraphExec_t step_exec = nullptr;
+  StepKey step_key;
   bool block_set[DGB_MAX_BLOCKS] = {false, false, false};
   bool finalized = false;
   bool face_present[2] = {false, false};
@@ -555,6 +570,7 @@ int dgb_plan_create(const dgb_params* prm, dgb_plan** out) {
 }
 
 int dgb_plan_update_params(dgb_plan* p, const dgb_params* prm) {
+  if (p) ++p->generation;    // invalidates a captured step
   if (!p || !prm) return fail(DGB_ERR_ARGUMENT, "null argument");
   if (prm->degree != p->dev.degree || prm->nvars != p->dev.nv || prm->num_blocks != p->dev.nblocks ||
       prm->viscous != p->dev.viscous || prm->precision != p->prm.precision)
@@ -684,10 +700,26 @@ int dgb_plan_set_hex(dgb_plan* p, const double* line_tables, const int32_t* lex2
   memcpy(t.bfT, src, sizeof(t.bfT)); src += 16;
   memcpy(t.d0, src, sizeof(t.d0)); src += 4;
   memcpy(t.d1, src, sizeof(t.d1)); src += 4;
+  memcpy(t.m1i, src, sizeof(t.m1i)); src += 16;
+  memcpy(t.w1, src, sizeof(t.w1)); src += 5;
   for (int i = 0; i < 64; ++i) t.lex2node[i] = lex2node[i];
   int rc;
   if ((rc = upload(p, perm, (size_t)num_codes * face_points, &p->hex_codes.perm))) return rc;
   p->hex = true;
+  return DGB_OK;
+}
+
+int dgb_plan_set_hex_affine(dgb_plan* p, const uint8_t* affine, const double* coef, const double* jinv,
+                            const double* det) {
+  if (!p || !affine || !coef || !jinv || !det) return fail(DGB_ERR_ARGUMENT, "null argument");
+  if (p->finalized) return fail(DGB_ERR_ARGUMENT, "plan already finalized");
+  if (!p->hex) return fail(DGB_ERR_ARGUMENT, "call dgb_plan_set_hex first");
+  BlockDev& B = p->dev.blk[0];
+  int rc;
+  if ((rc = upload(p, affine, (size_t)B.E, &B.affine))) return rc;
+  if ((rc = upload(p, coef, (size_t)B.E, &B.acoef))) return rc;
+  if ((rc = upload(p, jinv, (size_t)B.E * 9, &B.ajinv))) return rc;
+  if ((rc = upload(p, det, (size_t)B.E, &B.adet))) return rc;
   return DGB_OK;
 }
 
@@ -758,6 +790,8 @@ int dgb_plan_finalize(dgb_plan* p) {
 
 int dgb_plan_destroy(dgb_plan* p) {
   if (!p) return DGB_OK;
+  if (p->step_exec) cudaGraphExecDestroy(p->step_exec);
+  if (p->capture_stream) cudaStreamDestroy(p->capture_stream);
   for (void* d : p->allocations) cudaFree(d);
   delete p;
   return DGB_OK;
@@ -818,6 +852,7 @@ int dgb_plan_set_subcell_faces(dgb_plan* p, int ft, const int32_t* osub, const i
 }
 
 int dgb_plan_enable_mood(dgb_plan* p) {
+  if (p) ++p->generation;    // invalidates a captured step
   if (!p || !p->finalized) return fail(DGB_ERR_ARGUMENT, "finalize the plan first");
   if (p->mood_ready) return DGB_OK;
   for (int b = 0; b < p->dev.nblocks; ++b)
@@ -918,6 +953,7 @@ int dgb_mlp_train_step(float* w, float* grad, float* m, float* v, void* w16, con
 }
 
 int dgb_plan_set_predictor(dgb_plan* p, const void* w16, const float* norm, float threshold, int mode) {
+  if (p) ++p->generation;    // invalidates a captured step
   int rc;
   if ((rc = check_ready(p))) return rc;
   if (mode < 0 || mode > 2) return fail(DGB_ERR_ARGUMENT, "mode must be 0 (off), 1 (learned) or 2 (evaluate)");
@@ -998,6 +1034,47 @@ int dgb_admissibility(dgb_plan* p, const dgb_state* U, dgb_status* status, void*
   const StatePtrs S = to_ptrs(U);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   return p->dev.nv == 5 ? run_admissibility<5>(p, S, status, 0, st) : run_admissibility<16>(p, S, status, 0, st);
+}
+
+int dgb_ssprk3_step_graph(dgb_plan* p, const dgb_state* U, double dt, dgb_status* status, void* stream) {
+  int rc;
+  if ((rc = check_ready(p)) || (rc = check_state(p, U, "U"))) return rc;
+  if (!status) return fail(DGB_ERR_ARGUMENT, "status is null");
+  if (p->prm.limiter == 2 && !p->mood_ready) return fail(DGB_ERR_ARGUMENT, "MOOD limiter needs dgb_plan_enable_mood");
+  StepKey key;
+  memset(&key, 0, sizeof(key));
+  for (int b = 0; b < DGB_MAX_BLOCKS; ++b) key.block[b] = U->block[b];
+  key.dt = dt;
+  key.status = status;
+  key.generation = p->generation;
+  if (!p->step_exec || memcmp(&key, &p->step_key, sizeof(key)) != 0) {
+    if (p->step_exec) {
+      CK(cudaGraphExecDestroy(p->step_exec));
+      p->step_exec = nullptr;
+    }
+    // the legacy default stream cannot be captured: capture on a private stream, replay on the caller's
+    if (!p->capture_stream) CK(cudaStreamCreateWithFlags(&p->capture_stream, cudaStreamNonBlocking));
+    CK(cudaStreamBeginCapture(p->capture_stream, cudaStreamCaptureModeRelaxed));
+    const StatePtrs S = to_ptrs(U);
+    rc = p->dev.nv == 5 ? run_step<5>(p, S, dt, status, p->capture_stream)
+                        : run_step<16>(p, S, dt, status, p->capture_stream);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t end = cudaStreamEndCapture(p->capture_stream, &graph);
+    if (rc || end != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      if (rc) return rc;
+      return fail(DGB_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(end));
+    }
+    const cudaError_t inst = cudaGraphInstantiate(&p->step_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (inst != cudaSuccess) {
+      p->step_exec = nullptr;
+      return fail(DGB_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(inst));
+    }
+    p->step_key = key;
+  }
+  CK(cudaGraphLaunch(p->step_exec, static_cast<cudaStream_t>(stream)));
+  return DGB_OK;
 }
 
 int dgb_ssprk3_step(dgb_plan* p, const dgb_state* U, double dt, dgb_status* status, void* stream) {

@@ -38,6 +38,11 @@ struct BlockDev {
   const double* trdB[2];  // per face type: [codes][nq][Np][3]
   double* Rinv;           // scratch [E][Np][NV]
   double* Rvis;
+  // affine hexahedra (sum-factorised path, optional): constant metrics, M^-1 = coef * (m1i)^(x)3
+  const uint8_t* affine;  // [E] 1 where the element map is affine
+  const double* acoef;    // [E] sliver scale / det J
+  const double* ajinv;    // [E][9] constant inverse Jacobian
+  const double* adet;     // [E] det J
 };
 
 struct FaceDev {

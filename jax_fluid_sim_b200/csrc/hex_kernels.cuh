@@ -29,10 +29,12 @@ struct HexTablesT {
   R bf[4 * 4], df[4 * 4];          // [QF][N]
   R bfT[4 * 4];                    // [N][QF]
   R d0[4], d1[4];                  // 1-D basis derivatives at xi = 0 and xi = 1
+  R m1i[4 * 4];                    // [N][N] inverse of the 1-D mass matrix (affine elements)
+  R w1[5];                         // 1-D volume Gauss weights on [0, 1]
   int lex2node[64];                // lexicographic (x fastest) -> element node index
 };
 using HexTables = HexTablesT<double>;
-constexpr int kHexTableValues = 4 * 20 + 3 * 16 + 2 * 4;   // reals before lex2node
+constexpr int kHexTableValues = 4 * 20 + 3 * 16 + 2 * 4 + 16 + 5;   // reals before lex2node
 static_assert(offsetof(HexTablesT<double>, lex2node) == kHexTableValues * sizeof(double), "table layout");
 static_assert(offsetof(HexTablesT<float>, lex2node) == kHexTableValues * sizeof(float), "table layout");
 
@@ -148,7 +150,8 @@ struct HexSmem {
   static constexpr int TRACES = TR_W + 6 * (NV + 8) * (N2 + N * QF + QF2) + 2 * 24 * QF2;
   // lift: staged M^-T, b per face on its slab, b on all nodes, scratch
   static constexpr int LI_BS = T, LI_B = LI_BS + 6 * 12 * N2, LI_W = LI_B + 12 * N3;
-  static constexpr int LIFT = LI_W + 12 * QF2 + 12 * QF * N + 12 * N2 + 12 * QF2;
+  static constexpr int LI_X = LI_W + 72 * QF2 + 72 * QF * N + 72 * N2 + 72 * QF2;   // affine scratch
+  static constexpr int LIFT = LI_X + 3 * 12 * N3;
   // volume: U, v, lift nodes, then U and gradients at the points and contraction scratch
   static constexpr int C1 = NV > 12 ? NV : 12;
   static constexpr int VO_U = T, VO_V = VO_U + NV * N3, VO_L = VO_V + 4 * N3, VO_W = VO_L + 12 * N3;
@@ -320,79 +323,94 @@ __global__ void __launch_bounds__(kThreads) k_hex_lift(const DevPlan P_, int b, 
                                                       const HexCodes codes, double* lift_out) {
   using D = HexDims<P>;
   using L = HexSmem<P, NV, R>;
-  constexpr int N = D::N, QF = D::QF, N2 = D::N2, N3 = D::N3;
+  constexpr int N = D::N, QF = D::QF, N2 = D::N2, N3 = D::N3, QF2 = D::QF2;
+  constexpr int CH = 6 * 12;                    // the six faces' 12 lift components
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   R* smem = reinterpret_cast<R*>(dyn_smem);
   HexTablesT<R>* tb = reinterpret_cast<HexTablesT<R>*>(smem);
-  R* bs = smem + L::LI_BS;              // [6][12][N2]
-  R* ball = smem + L::LI_B;             // [12][N3]
-  R* jc = smem + L::LI_W;               // [12][QF2]
-  R* tmp = jc + 12 * QF * QF;           // [12][QF][N]
-  R* rs = tmp + 12 * QF * N;            // [12][N2]
-  R* lq = rs + 12 * N2;                 // [12][QF2]
-  __shared__ int node2lex[64];
+  R* bs = smem + L::LI_BS;              // [6][12][N2] b_f on each face's slab
+  R* ball = smem + L::LI_B;             // [12][N3]    b on all nodes
+  R* jc = smem + L::LI_W;               // [6][12][QF2] jumps at the canonical face points
+  R* tmp = jc + CH * QF2;               // [6*12][QF][N] contraction scratch
+  R* rs = tmp + CH * QF * N;            // [6][12][N2] r_f on each face's slab
+  R* lq = rs + CH * N2;                 // [6][12][QF2] B_f r_f
+  __shared__ int node2lex[64], fslot[6], fperm[6], fjump[6];
   const BlockDev& B = P_.blk[b];
+  const FaceDev& fd = P_.face[1];
   const int e = blockIdx.x;
   load_tables<P>(tables, tb);
+  if (threadIdx.x < 6) {
+    int ft, f, side;
+    decode_face(B.elem_face[e * 6 + threadIdx.x], ft, f, side);
+    fslot[threadIdx.x] = (f * 2 + side) * QF2;
+    fperm[threadIdx.x] = (side == 0 ? fd.oc[f] : fd.nc[f]) * QF2;
+    fjump[threadIdx.x] = f;
+  }
   __syncthreads();
   for (int l = threadIdx.x; l < N3; l += blockDim.x) node2lex[tb->lex2node[l]] = l;
-  for (int idx = threadIdx.x; idx < 12 * N3; idx += blockDim.x) ball[idx] = R(0);
   // M^-T of this element in element node order: MT[j][i] = M^-1[i][j]
   const double* MT = B.minv + (size_t)e * N3 * N3;
-  const FaceDev& fd = P_.face[1];
-  int fcode[6];
-  for (int lf = 0; lf < 6; ++lf) {
-    int ft, f, side;
-    decode_face(B.elem_face[e * 6 + lf], ft, f, side);
-    fcode[lf] = (f << 1) | side;
-    const int tc = side == 0 ? fd.oc[f] : fd.nc[f];
-    const uint8_t* perm = codes.perm + tc * QF * QF;
-    const double* jw = fd.jumpW + (size_t)f * QF * QF * 12;
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < QF * QF * 12; idx += blockDim.x) {
-      const int q = idx / 12, c = idx % 12;
-      jc[c * QF * QF + perm[q]] = (R)jw[idx];
-    }
-    __syncthreads();
-    tensor2<12, QF, QF, N, N>(jc, bs + lf * 12 * N2, tmp, tb->bfT, tb->bfT);
-  }
-  // b on all nodes: faces scattered one after another in local-face order (deterministic;
-  // within one face every node appears once)
-  for (int lf = 0; lf < 6; ++lf) {
-    int a0, end, a1, a2;
-    hex_face_axes(lf, a0, end, a1, a2);
-    const int st0 = axis_stride<N>(a0), st1 = axis_stride<N>(a1), st2 = axis_stride<N>(a2);
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < 12 * N2; idx += blockDim.x) {
-      const int c = idx / N2, j1 = idx % N, j2 = (idx / N) % N;
-      ball[c * N3 + end * st0 + j1 * st1 + j2 * st2] += bs[(lf * 12 + c) * N2 + j2 * N + j1];
-    }
+  for (int idx = threadIdx.x; idx < 6 * QF2 * 12; idx += blockDim.x) {
+    const int lf = idx / (QF2 * 12), q = (idx / 12) % QF2, c = idx % 12;
+    jc[(lf * 12 + c) * QF2 + codes.perm[fperm[lf] + q]] = (R)fd.jumpW[((size_t)fjump[lf] * QF2 + q) * 12 + c];
   }
   __syncthreads();
-  // nodal lift = M^-1 b: a thread owns one element node i and half of the 12 components;
-  // MT rows are read coalesced across consecutive nodes
-  double* lg = lift_out + (size_t)e * 12 * N3;
-  for (int idx = threadIdx.x; idx < 2 * N3; idx += blockDim.x) {
-    const int i = idx % N3, c0 = (idx / N3) * 6;
-    R s[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
-#pragma unroll 4
-    for (int j = 0; j < N3; ++j) {
-      const R m = (R)__ldg(MT + (size_t)j * N3 + i);
-      const int lj = node2lex[j];
+  tensor2<CH, QF, QF, N, N>(jc, bs, tmp, tb->bfT, tb->bfT);
+  // b on all nodes: each node gathers the faces holding it, in local-face order (deterministic)
+  for (int idx = threadIdx.x; idx < 12 * N3; idx += blockDim.x) {
+    const int c = idx / N3, l = idx % N3;
+    const int xyz[3] = {l % N, (l / N) % N, l / N2};
+    R acc = R(0);
 #pragma unroll
-      for (int k = 0; k < 6; ++k) s[k] += m * ball[(c0 + k) * N3 + lj];
+    for (int lf = 0; lf < 6; ++lf) {
+      int a0, end, a1, a2;
+      hex_face_axes(lf, a0, end, a1, a2);
+      if (xyz[a0] == end) acc += bs[(lf * 12 + c) * N2 + xyz[a2] * N + xyz[a1]];
     }
-    const int li = node2lex[i];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) lg[(c0 + k) * N3 + li] = (double)s[k];
+    ball[idx] = acc;
   }
-  // per face: r_f on its slab, then br2 * B_f r_f at the face points
-  for (int lf = 0; lf < 6; ++lf) {
-    int a0, end, a1, a2;
-    hex_face_axes(lf, a0, end, a1, a2);
-    const int st0 = axis_stride<N>(a0), st1 = axis_stride<N>(a1), st2 = axis_stride<N>(a2);
-    for (int idx = threadIdx.x; idx < 2 * N2; idx += blockDim.x) {
-      const int s_i = idx % N2, c0 = (idx / N2) * 6;
+  __syncthreads();
+  // nodal lift = M^-1 b
+  double* lg = lift_out + (size_t)e * 12 * N3;
+  const bool aff = B.affine && B.affine[e];
+  if (aff) {
+    // affine: M^-1 = coef (m1i (x) m1i (x) m1i), three 1-D passes over the lexicographic b
+    R* ax = smem + L::LI_X;
+    R* at1 = ax + 12 * N3;
+    R* at2 = at1 + 12 * N3;
+    tensor3<12, N, N, N, N, N, N, false>(ball, ax, at1, at2, tb->m1i, tb->m1i, tb->m1i);
+    const R cf = (R)B.acoef[e];
+    for (int idx = threadIdx.x; idx < 12 * N3; idx += blockDim.x) lg[idx] = (double)(cf * ax[idx]);
+    // M^-1 restricted to each face's slab: coef m1i[end][end] (m1i (x) m1i) over the free axes
+    tensor2<CH, N, N, N, N>(bs, rs, tmp, tb->m1i, tb->m1i);
+    for (int idx = threadIdx.x; idx < CH * N2; idx += blockDim.x) {
+      int a0, end, a1, a2;
+      hex_face_axes(idx / (12 * N2), a0, end, a1, a2);
+      rs[idx] *= cf * tb->m1i[end * N + end];
+    }
+  } else {
+    // a thread owns one element node i and half of the 12 components; MT rows are read
+    // coalesced across consecutive nodes
+    for (int idx = threadIdx.x; idx < 2 * N3; idx += blockDim.x) {
+      const int i = idx % N3, c0 = (idx / N3) * 6;
+      R sacc[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
+#pragma unroll 4
+      for (int j = 0; j < N3; ++j) {
+        const R m = (R)__ldg(MT + (size_t)j * N3 + i);
+        const int lj = node2lex[j];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) sacc[k] += m * ball[(c0 + k) * N3 + lj];
+      }
+      const int li = node2lex[i];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) lg[(c0 + k) * N3 + li] = (double)sacc[k];
+    }
+    // r_f = M^-1[slab_f, slab_f] b_f for the six faces
+    for (int idx = threadIdx.x; idx < 6 * 2 * N2; idx += blockDim.x) {
+      const int lf = idx / (2 * N2), s_i = idx % N2, c0 = ((idx / N2) % 2) * 6;
+      int a0, end, a1, a2;
+      hex_face_axes(lf, a0, end, a1, a2);
+      const int st0 = axis_stride<N>(a0), st1 = axis_stride<N>(a1), st2 = axis_stride<N>(a2);
       const int ni = tb->lex2node[end * st0 + (s_i % N) * st1 + (s_i / N) * st2];
       R acc[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
 #pragma unroll
@@ -403,19 +421,16 @@ __global__ void __launch_bounds__(kThreads) k_hex_lift(const DevPlan P_, int b, 
         for (int k = 0; k < 6; ++k) acc[k] += m * bs[(lf * 12 + c0 + k) * N2 + s_j];
       }
 #pragma unroll
-      for (int k = 0; k < 6; ++k) rs[(c0 + k) * N2 + s_i] = acc[k];
+      for (int k = 0; k < 6; ++k) rs[(lf * 12 + c0 + k) * N2 + s_i] = acc[k];
     }
-    __syncthreads();
-    tensor2<12, N, N, QF, QF>(rs, lq, tmp, tb->bf, tb->bf);
-    const int f = fcode[lf] >> 1, side = fcode[lf] & 1;
-    const int tc = side == 0 ? fd.oc[f] : fd.nc[f];
-    const uint8_t* perm = codes.perm + tc * QF * QF;
-    const size_t slot = ((size_t)f * 2 + side) * (QF * QF);
-    for (int idx = threadIdx.x; idx < QF * QF * 12; idx += blockDim.x) {
-      const int q = idx / 12, c = idx % 12;
-      fd.liftF[(slot + q) * 12 + c] = P_.ph.br2 * (double)lq[c * QF * QF + perm[q]];
-    }
-    __syncthreads();
+  }
+  __syncthreads();
+  // br2 * B_f r_f at every face's points
+  tensor2<CH, N, N, QF, QF>(rs, lq, tmp, tb->bf, tb->bf);
+  for (int idx = threadIdx.x; idx < 6 * QF2 * 12; idx += blockDim.x) {
+    const int lf = idx / (QF2 * 12), q = (idx / 12) % QF2, c = idx % 12;
+    fd.liftF[((size_t)fslot[lf] + q) * 12 + c] =
+        P_.ph.br2 * (double)lq[(lf * 12 + c) * QF2 + codes.perm[fperm[lf] + q]];
   }
 }
 
@@ -475,6 +490,14 @@ __global__ void __launch_bounds__(kThreads) k_hex_volume(const DevPlan P_, const
   tensor3<NV, N, N, N, Q, Q, Q, false>(U, uq, t1, t2, tb->bq, tb->bq, tb->bq);
   const double* jinv = B.jinv + (size_t)e * Q3 * 9;
   const double* wdet = B.wdet + (size_t)e * Q3;
+  // affine element: one inverse Jacobian, w |J| = w1 w1 w1 det J (no per-point metrics read)
+  const bool aff = B.affine && B.affine[e];
+  R Ja[9], deta = R(0);
+  if (aff) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Ja[k] = (R)B.ajinv[(size_t)e * 9 + k];
+    deta = (R)B.adet[e];
+  }
   if (visc) {
     tensor3<4, N, N, N, Q, Q, Q, false>(V, gq + 0 * 4 * Q3, t1, t2, tb->dq, tb->bq, tb->bq);
     tensor3<4, N, N, N, Q, Q, Q, false>(V, gq + 1 * 4 * Q3, t1, t2, tb->bq, tb->dq, tb->bq);
@@ -483,7 +506,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_volume(const DevPlan P_, const
     for (int q = threadIdx.x; q < Q3; q += blockDim.x) {
       R J[9], gr[12];
 #pragma unroll
-      for (int k = 0; k < 9; ++k) J[k] = (R)jinv[q * 9 + k];
+      for (int k = 0; k < 9; ++k) J[k] = aff ? Ja[k] : (R)jinv[q * 9 + k];
 #pragma unroll
       for (int k = 0; k < 12; ++k) gr[k] = gq[k * Q3 + q];      // [r][m]
 #pragma unroll
@@ -508,8 +531,8 @@ __global__ void __launch_bounds__(kThreads) k_hex_volume(const DevPlan P_, const
   for (int q = threadIdx.x; q < Q3; q += blockDim.x) {
     R J[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) J[k] = (R)jinv[q * 9 + k];
-    const R wq = (R)wdet[q];
+    for (int k = 0; k < 9; ++k) J[k] = aff ? Ja[k] : (R)jinv[q * 9 + k];
+    const R wq = aff ? tb->w1[q / (Q * Q)] * tb->w1[(q / Q) % Q] * tb->w1[q % Q] * deta : (R)wdet[q];
     R Uq[NV], F[3][NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) Uq[v] = anchor[v] + uq[v * Q3 + q];
@@ -633,6 +656,31 @@ __global__ void __launch_bounds__(kThreads) k_hex_finalize(const DevPlan P_, con
     Rr[idx] = acc;
   }
   __syncthreads();
+  // the stage update (or right-hand-side output) of one value: node-order offset o
+  auto emit = [&](size_t o, double ri, double rv) {
+    if (!A.stage) {
+      if (A.out_inv[b]) A.out_inv[b][o] = ri;
+      if (SPLIT && A.out_vis[b]) A.out_vis[b][o] = rv;
+    } else {
+      const double total = SPLIT ? ri + rv : ri;
+      const double eul = S.b[b][o] + A.dt * total;
+      if (SPLIT && A.out_vis[b]) A.out_vis[b][o] = rv;
+      if (A.euler[b]) A.euler[b][o] = eul;
+      A.dst[b][o] = A.alpha * A.base[b][o] + A.beta * eul;
+    }
+  };
+  if (B.affine && B.affine[e]) {
+    // affine: M^-1 = coef (m1i (x) m1i (x) m1i), three 1-D passes over the lexicographic residual
+    tensor3<C, N, N, N, N, N, N, false>(Rr, hs, tmp, hc, tb->m1i, tb->m1i, tb->m1i);
+    const R cf = (R)B.acoef[e];
+    for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
+      const int v = idx / N3, l = idx % N3;
+      const double ri = (double)(cf * hs[v * N3 + l]);
+      const double rv = SPLIT ? (double)(cf * hs[(NV + v) * N3 + l]) : 0.0;
+      emit(base + (size_t)tb->lex2node[l] * NV + v, ri, rv);
+    }
+    return;
+  }
   // M^-1: out[node(i)] = sum_j M^-T[j][i] R[lex(j)].  Work items (column half, variable group,
   // node i); consecutive threads take consecutive i, so the M^-T rows are read coalesced.  The
   // halves are added in a fixed order.
@@ -676,18 +724,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_finalize(const DevPlan P_, con
       si += part[(2 * NV + v) * N3 + i];
       sv += part[(3 * NV + v) * N3 + i];
     }
-    const size_t o = base + (size_t)i * NV + v;
-    const double ri = (double)si, rv = (double)sv;
-    if (!A.stage) {
-      if (A.out_inv[b]) A.out_inv[b][o] = ri;
-      if (SPLIT && A.out_vis[b]) A.out_vis[b][o] = rv;
-    } else {
-      const double total = SPLIT ? ri + rv : ri;
-      const double eul = S.b[b][o] + A.dt * total;
-      if (SPLIT && A.out_vis[b]) A.out_vis[b][o] = rv;
-      if (A.euler[b]) A.euler[b][o] = eul;
-      A.dst[b][o] = A.alpha * A.base[b][o] + A.beta * eul;
-    }
+    emit(base + (size_t)i * NV + v, (double)si, (double)sv);
   }
 }
 

@@ -14,7 +14,7 @@ import numpy as np
 import torch
 
 from . import _native as N
-from .plan import Plan, hex_sumfact_tables
+from .plan import Plan, hex_affine_data, hex_sumfact_tables
 from .reference import FACE_TYPE_ID, TYPE_ID
 
 
@@ -27,7 +27,8 @@ class NativePlan:
 
     PRECISIONS = {"float64": 0, "mixed": 1}
 
-    def __init__(self, plan: Plan, solver, viscous: bool, br2: float, sum_factorised=None, precision="float64"):
+    def __init__(self, plan: Plan, solver, viscous: bool, br2: float, sum_factorised=None, precision="float64",
+                 affine=True):
         L = N.lib()
         if precision not in self.PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(self.PRECISIONS)}")
@@ -101,7 +102,16 @@ class NativePlan:
             keep += [tables, lex, perm]
             N.check(L.dgb_plan_set_hex(handle, N.dptr(tables), N.dptr(lex, ctypes.c_int32), perm.shape[0], nfq,
                                        N.dptr(perm, ctypes.c_uint8)))
+            if affine:
+                aff, coef, ajinv, det = hex_affine_data(plan)
+                aff, coef, ajinv, det = (np.ascontiguousarray(aff, np.uint8), N.as_f64(coef), N.as_f64(ajinv),
+                                         N.as_f64(det))
+                keep += [aff, coef, ajinv, det]
+                N.check(L.dgb_plan_set_hex_affine(handle, N.dptr(aff, ctypes.c_uint8), N.dptr(coef), N.dptr(ajinv),
+                                                  N.dptr(det)))
+                self.affine_fraction = float(aff.mean())
         self.sum_factorised = bool(sum_factorised)
+        self.affine = bool(sum_factorised and affine)
         N.check(L.dgb_plan_finalize(handle))
         self._pushed = self._snapshot()
 
@@ -182,10 +192,12 @@ class HybridEulerOperator:
 
     _viscous = False
 
-    def __init__(self, solver, br2_stabilization=None, sum_factorised=None, precision="float64"):
+    def __init__(self, solver, br2_stabilization=None, sum_factorised=None, precision="float64", affine=True):
         """``precision``: "float64" (the reference's arithmetic) or "mixed" (float32 arithmetic in
         the hexahedron trace, BR2-lift, volume and finalize kernels; the state, face fluxes,
-        limiters, reductions and the stage update stay float64)."""
+        limiters, reductions and the stage update stay float64).  ``affine``: on the sum-factorised
+        path, elements with an affine map use constant metrics and a tensor-product inverse mass
+        matrix (equal to the dense one to round-off) instead of reading per-element tables."""
         self.solver = solver
         self.mesh = solver.mesh
         P = solver.polynomial_degree
@@ -193,7 +205,8 @@ class HybridEulerOperator:
         self.plan = Plan(self.mesh, P)
         self.names = [b.element_type for b in self.mesh.element_blocks]
         viscous = self._viscous and solver.dynamic_viscosity > 0.0
-        self.native = NativePlan(self.plan, solver, viscous, self.br2_stabilization, sum_factorised, precision)
+        self.native = NativePlan(self.plan, solver, viscous, self.br2_stabilization, sum_factorised, precision,
+                                 affine)
         self.precision = precision
         self.viscous = viscous
         self.solution_node_coordinates = {bp.etype: bp.node_xyz for bp in self.plan.blocks}
@@ -204,7 +217,7 @@ class HybridEulerOperator:
         other = object.__new__(type(self))
         other.__dict__.update({k: v for k, v in self.__dict__.items() if k != "native"})
         other.native = NativePlan(self.plan, self.solver, self.viscous, self.br2_stabilization,
-                                  self.native.sum_factorised, precision)
+                                  self.native.sum_factorised, precision, self.native.affine)
         other.precision = precision
         return other
 

@@ -292,9 +292,14 @@ def hex_sumfact_tables(plan: Plan):
         out[:a.size] = a.ravel()
         return out
 
+    # 1-D mass matrix with the volume Gauss rule (exact: degree 2P <= 2Q - 1) and its inverse; the
+    # hexahedron mass matrix of an affine element is det J times its threefold tensor product
+    gpts, gw = gauss01(Q)
+    assert np.allclose(gpts, gq)
+    m1i = np.linalg.inv(np.einsum("q,qi,qj->ij", gw, bq, bq))
     tables = np.concatenate([packed(bq, 20), packed(dq, 20), packed(bq.T.copy(), 20), packed(dq.T.copy(), 20),
                              packed(bf, 16), packed(df, 16), packed(bf.T.copy(), 16),
-                             packed(d01[0], 4), packed(d01[1], 4)])
+                             packed(d01[0], 4), packed(d01[1], 4), packed(m1i, 16), packed(gw, 5)])
     lex = np.full(64, 0, np.int32)
     for iz in range(N):
         for iy in range(N):
@@ -315,3 +320,17 @@ def hex_sumfact_tables(plan: Plan):
         assert np.max(np.abs(gf[k1] - pts[:, a1])) < 1e-12 and np.max(np.abs(gf[k2] - pts[:, a2])) < 1e-12
         perm[c] = k2 * QF + k1
     return tables, lex, perm, QF * QF
+
+
+def hex_affine_data(plan: Plan, tol=1.0e-10):
+    """Elements of the (single) hexahedron block whose map is affine: the inverse Jacobian is the
+    same at every volume point to ``tol`` relative.  Returns (affine uint8[E], coef[E] = sliver
+    scale / det J, jinv[E][9], det[E]) in the layout of dgb_plan_set_hex_affine; for those
+    elements the inverse mass matrix is coef * (m1i (x) m1i (x) m1i)."""
+    bp = plan.blocks[0]
+    J = bp.jinv.reshape(bp.E, bp.Nq, 9)
+    dev = np.abs(J - J[:, :1]).max(axis=(1, 2)) / np.maximum(np.abs(J).max(axis=(1, 2)), 1e-300)
+    affine = (dev <= tol).astype(np.uint8)
+    det = bp.volume.astype(np.float64)              # the reference hexahedron [0, 1]^3 has volume 1
+    coef = np.minimum(1.0, bp.volume / 1.0e-4) / det
+    return affine, coef, np.ascontiguousarray(J.mean(axis=1)), det

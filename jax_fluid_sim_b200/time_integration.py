@@ -19,8 +19,11 @@ from .operators import _stream_ptr
 
 class HybridSSPRK3:
     def __init__(self, operator, cfl=0.15, limiter=None, density_floor=1.0e-7, pressure_floor=1.0e-7,
-                 maximum_rejections=16):
+                 maximum_rejections=16, graph=False):
+        """``graph=True`` runs every checked step as one CUDA graph (captured on the first step and
+        again whenever the state buffers, dt or the plan's parameters change)."""
         self.operator = operator
+        self.graph = bool(graph)
         self.solver = operator.solver
         self.cfl = float(cfl)
         self.limiter = limiter
@@ -83,8 +86,9 @@ class HybridSSPRK3:
         op = self.operator
         self._configure(boundary_state)
         st = op.native.state(op._blocks(states))
-        N.check(N.lib().dgb_ssprk3_step(op.native.handle, ctypes.byref(st), float(dt),
-                                        ctypes.c_void_p(self._status.data_ptr()), _stream_ptr()))
+        step = N.lib().dgb_ssprk3_step_graph if self.graph else N.lib().dgb_ssprk3_step
+        N.check(step(op.native.handle, ctypes.byref(st), float(dt), ctypes.c_void_p(self._status.data_ptr()),
+                     _stream_ptr()))
         return self._status
 
     def checked_step(self, states, dt, boundary_state=None):
