@@ -8,7 +8,7 @@ rho=p=1, U=3*sqrt(1.4), mu=U/Re, T_w=300/220).  One step = one checked SSP-RK3
 step (three stages of inviscid HLLC + BR2 viscous residual, then per stage the MOOD
 troubled-cell check, subcell finite-volume recompute of troubled elements, Zhang-Shu
 positivity limiter, blend and admissibility check).  Synthetic seeded mesh (numpy
-generator); the state starts as the uniform free stream.
+generator); the start is described below (--start uniform gives the uniform free stream).
 
 Default flow (one state, one dt for every run):
   1. start: the Mach-3 normal-shock state in the elements inside r < 0.65 around the sphere,
@@ -118,12 +118,16 @@ def freestream(degree):
 
 
 def rhs_bytes(op, nv, sizeof=8):
-    """Algorithmic HBM bytes of one RHS evaluation (each input read once, outputs written once)."""
+    """Algorithmic HBM bytes of one RHS evaluation (each input read once, outputs written once):
+    the whole-RHS formula with J^-1, w|J| and the inverse mass counted for the non-affine
+    elements only (affine hexahedra need 11 values)."""
     total = 0
-    for bp in op.plan.blocks:
+    for b, bp in enumerate(op.plan.blocks):
+        Ea = getattr(op.native, "affine_count", 0) if b == 0 else 0
         total += 2 * sizeof * nv * bp.E * bp.Np             # U in, R out
-        total += sizeof * 10 * bp.E * bp.Nq                 # J^-1 (9) + w|J| (1) per volume point
-        total += sizeof * bp.E * bp.Np * bp.Np              # dense inverse mass
+        total += sizeof * 10 * (bp.E - Ea) * bp.Nq          # J^-1 (9) + w|J| (1) per volume point
+        total += sizeof * (bp.E - Ea) * bp.Np * bp.Np       # dense inverse mass
+        total += sizeof * 11 * Ea
     for fp in op.plan.faces.values():
         total += fp.F * (sizeof * fp.nq * (2 * nv + 4 + nv) + 8)
     return total
@@ -138,15 +142,21 @@ def stage_bytes(op, nv, split, sizeof=8):
     precision modes)."""
     out = dict.fromkeys(STAGES, 0)
     visc = op.viscous
-    for bp in op.plan.blocks:
+    for b, bp in enumerate(op.plan.blocks):
         E, Np, Nq, nlf = bp.E, bp.Np, bp.Nq, bp.nlf
+        # affine hexahedra read 11 values (constant J^-1, det J, M^-1 factor) instead of the dense
+        # M^-1 and the per-point metrics
+        Ea = getattr(op.native, "affine_count", 0) if b == 0 else 0
+        Ed = E - Ea
         nqf = max(fp.nq for fp in op.plan.faces.values())
         # U in; per face point: anchor-form U (+ v, gradients and the face inverse Jacobian) out / in
         out["traces"] += sizeof * E * (nv * Np + nlf * nqf * (nv + (16 + 9 if visc else 0)))
         if visc:
-            out["lift"] += sizeof * E * (Np * Np + 2 * nlf * nqf * 12 + 12 * Np)
-        out["volume"] += sizeof * E * (nv * Np + 10 * Nq + (12 * Np if visc else 0) + (2 if split else 1) * nv * Np)
-        out["finalize"] += sizeof * E * (Np * Np + (2 if split else 1) * nv * Np + nlf * nqf * 2 * nv + 3 * nv * Np)
+            out["lift"] += sizeof * (Ed * Np * Np + Ea * 11 + E * (2 * nlf * nqf * 12 + 12 * Np))
+        out["volume"] += sizeof * (Ed * 10 * Nq + Ea * 11 + E * (nv * Np + (12 * Np if visc else 0)
+                                                                  + (2 if split else 1) * nv * Np))
+        out["finalize"] += sizeof * (Ed * Np * Np + Ea * 11 + E * ((2 if split else 1) * nv * Np + nlf * nqf * 2 * nv
+                                                                    + 3 * nv * Np))
     for fp in op.plan.faces.values():
         # traces of both sides, n and w in; both sides' fluxes out (+ v of both sides in, BR2 jumps out)
         out["face_flux"] += fp.F * (sizeof * fp.nq * (2 * nv + 4 + 2 * nv + (8 + 12 if visc else 0)) + 8)

@@ -123,11 +123,12 @@ int dgb_plan_set_trace(dgb_plan* plan, int element_type, int face_type, int num_
                        int num_nodes, const double* basis, const double* basis_grad);
 /* Optional sum-factorised path for a mesh of one hexahedron block (hexahedron bases are
  * tensor products of the 1-D Lagrange basis on the nodes 0, 1, interior: hybrid/elements.py:
- * 199-274, 325-456).  line_tables: 157 doubles, in order bq[5][4], dq[5][4] (1-D basis and
+ * 199-274, 325-456).  line_tables: 173 doubles, in order bq[5][4], dq[5][4] (1-D basis and
  * derivative at the volume Gauss points), bqT[4][5], dqT[4][5] (transposes), bf[4][4], df[4][4]
  * (at the face Gauss points), bfT[4][4], d0[4], d1[4] (derivatives at 0 and 1), m1i[4][4] (the
- * inverse of the 1-D mass matrix), w1[5] (1-D volume Gauss weights on [0, 1]), each block
- * using its leading (points x nodes) entries; lex2node: 64 ints mapping lexicographic
+ * inverse of the 1-D mass matrix), w1[5] (1-D volume Gauss weights on [0, 1]), p1d[4][4] (the
+ * nodal projector onto span{1, xi}, whose threefold tensor product is the sensor's P1
+ * projector), each block using its leading (points x nodes) entries; lex2node: 64 ints mapping lexicographic
  * (x fastest) node positions to element node indices; perm: [codes][face_points] map from the
  * owner's face-point order to the side element's canonical face grid. */
 int dgb_plan_set_hex(dgb_plan* plan, const double* line_tables, const int32_t* lex2node, int num_codes,

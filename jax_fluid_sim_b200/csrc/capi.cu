@@ -702,6 +702,7 @@ int dgb_plan_set_hex(dgb_plan* p, const double* line_tables, const int32_t* lex2
   memcpy(t.d1, src, sizeof(t.d1)); src += 4;
   memcpy(t.m1i, src, sizeof(t.m1i)); src += 16;
   memcpy(t.w1, src, sizeof(t.w1)); src += 5;
+  memcpy(t.p1d, src, sizeof(t.p1d)); src += 16;
   for (int i = 0; i < 64; ++i) t.lex2node[i] = lex2node[i];
   int rc;
   if ((rc = upload(p, perm, (size_t)num_codes * face_points, &p->hex_codes.perm))) return rc;

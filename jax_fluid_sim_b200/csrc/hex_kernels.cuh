@@ -31,10 +31,11 @@ struct HexTablesT {
   R d0[4], d1[4];                  // 1-D basis derivatives at xi = 0 and xi = 1
   R m1i[4 * 4];                    // [N][N] inverse of the 1-D mass matrix (affine elements)
   R w1[5];                         // 1-D volume Gauss weights on [0, 1]
+  R p1d[4 * 4];                    // [N][N] nodal projector onto span{1, xi} (sensor: P1 = p1d^(x)3)
   int lex2node[64];                // lexicographic (x fastest) -> element node index
 };
 using HexTables = HexTablesT<double>;
-constexpr int kHexTableValues = 4 * 20 + 3 * 16 + 2 * 4 + 16 + 5;   // reals before lex2node
+constexpr int kHexTableValues = 4 * 20 + 3 * 16 + 2 * 4 + 16 + 5 + 16;   // reals before lex2node
 static_assert(offsetof(HexTablesT<double>, lex2node) == kHexTableValues * sizeof(double), "table layout");
 static_assert(offsetof(HexTablesT<float>, lex2node) == kHexTableValues * sizeof(float), "table layout");
 
@@ -882,7 +883,8 @@ __global__ void __launch_bounds__(kThreads) k_hex_troubled(const DevPlan P_, con
   double* t2 = t1 + NV * N * N * Q;
   double* vq = t2 + NV * N * Q * Q;
   double* fs = vq + NV * Q3;
-  double* Mon = fs + 6 * NV * (D::N2 + N * D::QF + D::QF2);   // [N3][2] (rho, p) in element node order
+  double* Mon = fs + 6 * NV * (D::N2 + N * D::QF + D::QF2);   // [2][N3] (rho, p), lexicographic
+  double* Low = Mon + 2 * N3;                                   // [2][N3] their P1 projections
   __shared__ double mean[NV];
   __shared__ double red[4][kThreads / 32];
   const BlockDev& B = P_.blk[b];
@@ -897,11 +899,13 @@ __global__ void __launch_bounds__(kThreads) k_hex_troubled(const DevPlan P_, con
 #pragma unroll
     for (int v = 0; v < NV; ++v) u[v] = U[v * N3 + l];
     primitive<NV>(P_.ph, u, W);
-    const int node = tb->lex2node[l];
-    Mon[node * 2 + 0] = W[0];
-    Mon[node * 2 + 1] = W[4];
+    Mon[l] = W[0];
+    Mon[N3 + l] = W[4];
   }
   __syncthreads();
+  // P1 projection of (rho, p): the nodal projector onto the trilinear space is the threefold
+  // tensor product of the 1-D projector onto span{1, xi} (three passes of N x N)
+  if (P >= 2) tensor3<2, N, N, N, N, N, N, false>(Mon, Low, t1, t2, tb->p1d, tb->p1d, tb->p1d);
   const double* wdet = B.wdet + (size_t)e * Q3;
   for (int v = threadIdx.x; v < NV; v += blockDim.x) {
     double s = 0.0, w = 0.0;
@@ -914,15 +918,8 @@ __global__ void __launch_bounds__(kThreads) k_hex_troubled(const DevPlan P_, con
   double hi0 = 0.0, hi1 = 0.0, sc0 = 0.0, sc1 = 0.0;
   if (P >= 2) {
     for (int i = threadIdx.x; i < N3; i += blockDim.x) {
-      const double* row = B.p1proj + (size_t)i * N3;
-      double l0 = 0.0, l1 = 0.0;
-      for (int j = 0; j < N3; ++j) {
-        const double pj = __ldg(row + j);
-        l0 += pj * Mon[j * 2 + 0];
-        l1 += pj * Mon[j * 2 + 1];
-      }
-      const double m0 = Mon[i * 2 + 0], m1 = Mon[i * 2 + 1];
-      const double d0 = m0 - l0, d1 = m1 - l1;
+      const double m0 = Mon[i], m1 = Mon[N3 + i];
+      const double d0 = m0 - Low[i], d1 = m1 - Low[N3 + i];
       hi0 += d0 * d0;
       hi1 += d1 * d1;
       sc0 += m0 * m0;
@@ -984,7 +981,7 @@ constexpr int hex_positivity_smem() {
 
 template <int P, int NV>
 constexpr int hex_troubled_smem() {
-  return hex_positivity_smem<P, NV>() + 2 * HexDims<P>::N3;
+  return hex_positivity_smem<P, NV>() + 4 * HexDims<P>::N3;
 }
 
 }  // namespace dgb

@@ -110,6 +110,7 @@ class NativePlan:
                 N.check(L.dgb_plan_set_hex_affine(handle, N.dptr(aff, ctypes.c_uint8), N.dptr(coef), N.dptr(ajinv),
                                                   N.dptr(det)))
                 self.affine_fraction = float(aff.mean())
+                self.affine_count = int(aff.sum())
         self.sum_factorised = bool(sum_factorised)
         self.affine = bool(sum_factorised and affine)
         N.check(L.dgb_plan_finalize(handle))

@@ -297,9 +297,14 @@ def hex_sumfact_tables(plan: Plan):
     gpts, gw = gauss01(Q)
     assert np.allclose(gpts, gq)
     m1i = np.linalg.inv(np.einsum("q,qi,qj->ij", gw, bq, bq))
+    # nodal (Euclidean) projector onto span{1, xi}; on the tensor nodes the sensor's P1 projector
+    # (hybrid/limiter.py:158-163, the trilinear functions at the nodes times their pseudo-inverse)
+    # is its threefold tensor product
+    V1 = np.stack([np.ones(N), np.asarray(line)], axis=1)
+    p1d = V1 @ np.linalg.pinv(V1)
     tables = np.concatenate([packed(bq, 20), packed(dq, 20), packed(bq.T.copy(), 20), packed(dq.T.copy(), 20),
                              packed(bf, 16), packed(df, 16), packed(bf.T.copy(), 16),
-                             packed(d01[0], 4), packed(d01[1], 4), packed(m1i, 16), packed(gw, 5)])
+                             packed(d01[0], 4), packed(d01[1], 4), packed(m1i, 16), packed(gw, 5), packed(p1d, 16)])
     lex = np.full(64, 0, np.int32)
     for iz in range(N):
         for iy in range(N):
