@@ -229,6 +229,80 @@ def mixed_block(jitter=0.1, seed=0):
     return MeshSource(points, vol + bcells, phys + bphys, field)
 
 
+def hybrid_box(n=(8, 8, 8), lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), jitter=0.1, seed=0, fill=2.0 / 3.0):
+    """Fully periodic, conforming box of n cubes, each one hexahedron, two prisms or six tetrahedra.
+
+    The reference pairs faces by their vertex sets only (hybrid/mesh.py:391-405), so a quad
+    may only meet a quad and a triangle a triangle with the same diagonal.  Every triangulated
+    cube face here is cut along the diagonal through the cube's (0,0,0)-(1,1,1) corners, and a
+    cube's two faces normal to axis d are triangulated together or not at all, by a flag that
+    must then be the same along the whole line of cubes in d.  Three seeded 0/1 sequences a(i),
+    b(j), c(k), each with round(fill * n) ones, set the flags (x: b and c, y: a and c, z: a and b):
+    all three set gives six Kuhn tetrahedra round the main diagonal, one set gives two prisms
+    extruded along that axis, none a hexahedron.  fill = 2/3 puts roughly a third of the cubes in
+    each kind; the counts are in ``hybrid_box_fractions``.  Vertex columns are jittered by up to
+    jitter*h in x and y (seeded, periodic partners together), which keeps every face planar.
+    The lo/hi planes are identified in all three directions, so at least 3 cubes per direction
+    are needed for faces to be told apart by their vertex sets.
+    """
+    nx, ny, nz = n
+    if min(n) < 3:
+        raise ValueError("hybrid_box needs at least 3 cubes per direction")
+    lo, hi = np.asarray(lo, float), np.asarray(hi, float)
+    h = (hi - lo) / np.asarray(n, float)
+    K, J, I = (a.ravel() for a in np.indices((nz + 1, ny + 1, nx + 1)))
+    points = lo + np.stack([I, J, K], axis=1) * h
+
+    def pid(i, j, k):
+        return (k * (ny + 1) + j) * (nx + 1) + i
+
+    rng = np.random.default_rng(seed)
+
+    def flags(m):
+        f = np.zeros(m, bool)
+        f[:int(round(fill * m))] = True
+        return rng.permutation(f)
+
+    a, b, c = flags(nx), flags(ny), flags(nz)
+    if jitter > 0.0:
+        column = rng.uniform(-jitter, jitter, size=(ny + 1, nx + 1, 2))
+        column[-1, :] = column[0, :]
+        column[:, -1] = column[:, 0]
+        points[:, :2] += column[J, I] * h[:2]
+    canon = pid(np.where(I == nx, 0, I), np.where(J == ny, 0, J), np.where(K == nz, 0, K)).astype(np.int64)
+    hexes, wedges, tets = [], [], []
+    for k in range(nz):
+        for j in range(ny):
+            for i in range(nx):
+                q = {(x, y, z): pid(i + x, j + y, k + z) for x in (0, 1) for y in (0, 1) for z in (0, 1)}
+                tx, ty, tz = b[j] and c[k], a[i] and c[k], a[i] and b[j]
+                if tx and ty and tz:     # odd axis orders (1, 2, 5) are left-handed: swap two nodes
+                    tets.extend([t[0], t[2], t[1], t[3]] if r in (1, 2, 5) else t
+                                for r, t in enumerate(_kuhn_tets(q)))
+                elif tz:              # triangles in the z-faces, right-handed about +z
+                    wedges.append([q[0, 0, 0], q[1, 0, 0], q[1, 1, 0], q[0, 0, 1], q[1, 0, 1], q[1, 1, 1]])
+                    wedges.append([q[0, 0, 0], q[1, 1, 0], q[0, 1, 0], q[0, 0, 1], q[1, 1, 1], q[0, 1, 1]])
+                elif tx:              # about +x
+                    wedges.append([q[0, 0, 0], q[0, 1, 0], q[0, 1, 1], q[1, 0, 0], q[1, 1, 0], q[1, 1, 1]])
+                    wedges.append([q[0, 0, 0], q[0, 1, 1], q[0, 0, 1], q[1, 0, 0], q[1, 1, 1], q[1, 0, 1]])
+                elif ty:              # about +y
+                    wedges.append([q[0, 0, 0], q[0, 0, 1], q[1, 0, 1], q[0, 1, 0], q[0, 1, 1], q[1, 1, 1]])
+                    wedges.append([q[0, 0, 0], q[1, 0, 1], q[1, 0, 0], q[0, 1, 0], q[1, 1, 1], q[1, 1, 0]])
+                else:
+                    hexes.append([q[0, 0, 0], q[1, 0, 0], q[1, 1, 0], q[0, 1, 0],
+                                  q[0, 0, 1], q[1, 0, 1], q[1, 1, 1], q[0, 1, 1]])
+    vol = [(name, np.asarray(conn, np.int32)) for name, conn in
+           (("hexahedron", hexes), ("wedge", wedges), ("tetra", tets)) if conn]
+    return MeshSource(points, vol, [np.ones(len(v[1]), np.int32) for v in vol], {"fluid": (1, 3)}, canon)
+
+
+def hybrid_box_fractions(source):
+    """Fractions of cubes split into hexahedra, prism pairs and six tetrahedra."""
+    counts = {name: len(conn) for name, conn in source.cells}
+    cubes = np.array([counts.get("hexahedron", 0), counts.get("wedge", 0) / 2, counts.get("tetra", 0) / 6])
+    return dict(zip(("hexahedron", "wedge", "tetra"), cubes / cubes.sum()))
+
+
 def sphere_oh_grid(radius=0.5, box=((-4.0, 12.0), (-6.0, 6.0), (-6.0, 6.0)), cube=1.5, n=24, n_radial=20,
                    outer=((8, 32), (12, 12), (12, 12)), clustering=1.6):
     """Body-fitted O/H hex grid around a sphere centred at the origin.

@@ -1,0 +1,74 @@
+"""Host-side checks of the benchmark workloads: the periodic conforming hybrid box and the
+closed-form initial states (Taylor-Green and isentropic vortex)."""
+
+import numpy as np
+import pytest
+
+from jax_fluid_sim_b200 import meshgen, workloads
+from jax_fluid_sim_b200.mesh import HybridMesh
+from jax_fluid_sim_b200.plan import Plan, _p1_jacobian
+from oracle.mesh import Mesh, MeshSource
+
+
+@pytest.mark.parametrize("n,seed", [((4, 3, 4), 1), ((6, 5, 7), 4), ((8, 8, 8), 0)])
+def test_hybrid_box_is_conforming_and_periodic(n, seed):
+    src = meshgen.hybrid_box(n, jitter=0.1, seed=seed)
+    mesh = HybridMesh(src)
+    assert all(int(np.sum(fb.neighbor_block < 0)) == 0 for fb in mesh.face_blocks.values())
+    plan = Plan(mesh, 1)
+    assert sum(bp.volume.sum() for bp in plan.blocks) == pytest.approx(1.0, rel=1e-13)
+    for bp, block in zip(plan.blocks, mesh.element_blocks):
+        J = _p1_jacobian(bp.etype, mesh.points[block.connectivity][:, None], bp.ref.points[None])
+        assert np.all(np.linalg.det(J) > 0.0), bp.etype
+    frac = meshgen.hybrid_box_fractions(src)
+    assert set(frac) == {"hexahedron", "wedge", "tetra"} and all(0.1 < f < 0.6 for f in frac.values())
+
+
+def test_hybrid_box_faces_match_oracle_pairing():
+    """Face pairing, owners and orientations of the periodic box bit-exact against the oracle."""
+    src = meshgen.hybrid_box((4, 3, 4), jitter=0.1, seed=2)
+    ours = HybridMesh(src)
+    ref = Mesh(MeshSource(src.points, src.cells, src.physical, src.field_data, src.periodic_map))
+    assert [b.element_type for b in ours.element_blocks] == [b.element_type for b in ref.element_blocks]
+    for ftype, fb in ours.face_blocks.items():
+        rb = ref.face_blocks[ftype]
+        for key in ("nodes", "owner_block", "owner_local", "owner_face", "neighbor_block", "neighbor_local",
+                    "neighbor_face"):
+            np.testing.assert_array_equal(getattr(fb, key), getattr(rb, key), err_msg=key)
+        np.testing.assert_allclose(fb.normals, rb.normals, rtol=0, atol=1e-14)
+
+
+def test_hybrid_box_is_seeded_and_checks_size():
+    a, b = meshgen.hybrid_box((4, 4, 4), seed=3), meshgen.hybrid_box((4, 4, 4), seed=3)
+    np.testing.assert_array_equal(a.points, b.points)
+    for (na, ca), (nb, cb) in zip(a.cells, b.cells):
+        assert na == nb
+        np.testing.assert_array_equal(ca, cb)
+    with pytest.raises(ValueError):
+        meshgen.hybrid_box((2, 4, 4))
+
+
+def test_vortex_returns_after_one_period():
+    rng = np.random.default_rng(0)
+    x = rng.random((500, 3))
+    T = workloads.vortex_period()
+    np.testing.assert_allclose(workloads.vortex_primitive(x, T), workloads.vortex_primitive(x, 0.0), atol=1e-12)
+    W = workloads.vortex_primitive(x, 0.3 * T)
+    assert np.all(W[:, 0] > 0.0) and np.all(W[:, 4] > 0.0)
+    far = workloads.vortex_primitive(np.array([[0.0, 0.0, 0.5]]))[0]
+    np.testing.assert_allclose(far[1:4], workloads.vortex_velocity(), atol=1e-6)
+    # isentropic: p / rho^gamma is the free-stream value everywhere
+    np.testing.assert_allclose(W[:, 4] / W[:, 0] ** 1.4, 1.0, rtol=1e-12)
+
+
+def test_tgv_initial_state():
+    x = np.random.default_rng(1).random((200, 3)) * 2 * np.pi
+    W = workloads.tgv_primitive(x)
+    assert np.all(W[:, 0] == 1.0) and np.all(W[:, 3] == 0.0)
+    assert W[:, 4].min() >= 1.0 / (1.4 * 0.01) - 0.375 - 1e-12
+    # divergence-free velocity: du/dx + dv/dy = cos x cos y cos z - cos x cos y cos z
+    h = 1e-6
+    e = np.eye(3) * h
+    div = ((workloads.tgv_primitive(x + e[0])[:, 1] - workloads.tgv_primitive(x - e[0])[:, 1])
+           + (workloads.tgv_primitive(x + e[1])[:, 2] - workloads.tgv_primitive(x - e[1])[:, 2])) / (2 * h)
+    assert np.max(np.abs(div)) < 1e-8
