@@ -62,10 +62,9 @@ typedef struct {
   int limiter;                /* stage limiter of dgb_ssprk3_step: 0 none, 1 positivity, 2 MOOD */
   int reconstruction;         /* MOOD subcell faces: 0 constant, 1 tvd, 2 weno (CWENO-Z) */
   int precision;              /* 0 float64 throughout; 1 mixed: float32 arithmetic and shared-memory
-                                 staging in the hexahedron trace, BR2-lift, volume and finalize
-                                 kernels (state, face fluxes, limiters, reductions and the stage
-                                 update stay float64); needs the sum-factorised
-                                 single-hexahedron-block path */
+                                 staging in the trace, BR2-lift, volume and finalize kernels of
+                                 every element type (state, face fluxes, limiters, reductions and
+                                 the stage update stay float64) */
 } dgb_params;
 
 /* One element block (hybrid/geometry.py:139-203 metrics, precomputed by the host). */
@@ -142,6 +141,15 @@ int dgb_plan_set_hex(dgb_plan* plan, const double* line_tables, const int32_t* l
  * matrix by quadrature).  affine[E] is 1 for those elements, 0 for the others. */
 int dgb_plan_set_hex_affine(dgb_plan* plan, const uint8_t* affine, const double* coef, const double* jinv,
                             const double* det);
+/* Affine elements of a block on the dense (any element type) path: where affine[e] is 1 the
+ * kernels use the constant inverse Jacobian jinv[e][9], w_q |det J| = ref_weights[q] * det[e]
+ * and M^-1 = coef[e] * ref_inv_mass (coef = sliver scale / |det J|, ref_inv_mass the inverse of
+ * B^T diag(ref_weights) B, [Np][Np]) instead of the per-element tables; equal to them to
+ * round-off (hybrid/geometry.py:139-203 builds the per-element ones).  Not for the
+ * sum-factorised hexahedron path (dgb_plan_set_hex_affine). */
+int dgb_plan_set_block_affine(dgb_plan* plan, int block, const uint8_t* affine, const double* coef,
+                              const double* jinv, const double* det, const double* ref_weights,
+                              const double* ref_inv_mass);
 int dgb_plan_finalize(dgb_plan* plan);
 int dgb_plan_destroy(dgb_plan* plan);
 /* Replace the physics/boundary/limiter constants of a finalized plan (same mesh and degree);

@@ -113,6 +113,8 @@ def lib():
             "dgb_plan_finalize": [c_void_p],
             "dgb_plan_set_hex": [c_void_p, P_double, P_int32, c_int, c_int, ctypes.POINTER(ctypes.c_uint8)],
             "dgb_plan_set_hex_affine": [c_void_p, ctypes.POINTER(ctypes.c_uint8), P_double, P_double, P_double],
+            "dgb_plan_set_block_affine": [c_void_p, c_int, ctypes.POINTER(ctypes.c_uint8), P_double, P_double,
+                                          P_double, P_double, P_double],
             "dgb_plan_destroy": [c_void_p],
             "dgb_plan_update_params": [c_void_p, ctypes.POINTER(Params)],
             "dgb_rhs": [c_void_p, ctypes.POINTER(State), ctypes.POINTER(State), ctypes.POINTER(State), c_void_p],

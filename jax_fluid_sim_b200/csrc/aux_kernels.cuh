@@ -374,21 +374,39 @@ __global__ void __launch_bounds__(kThreads) k_adm(const DevPlan P, const StatePt
   }
 }
 
-// combine: first stage overwrites the status, later stages AND / min into it
-__global__ void k_adm_final(const Partial* partials, int n, double rho_floor, double p_floor, int combine,
-                            dgb_status* status) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// combine: first stage overwrites the status, later stages AND / min into it.  One CTA of
+// kAdmFinalThreads reduces the partials (a serial loop over thousands of them took 0.3 ms).
+constexpr int kAdmFinalThreads = 256;
+
+__global__ void __launch_bounds__(kAdmFinalThreads) k_adm_final(const Partial* partials, int n, double rho_floor,
+                                                               double p_floor, int combine, dgb_status* status) {
+  __shared__ double sr[kAdmFinalThreads], sp[kAdmFinalThreads];
   double rmin = INFINITY, pmin = INFINITY;
   int finite = 1, rnan = 0, pnan = 0;
-  for (int i = 0; i < n; ++i) {
-    rnan |= isnan(partials[i].a);
-    pnan |= isnan(partials[i].b);
-    rmin = fmin(rmin, partials[i].a);
-    pmin = fmin(pmin, partials[i].b);
-    finite &= partials[i].flag;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const Partial q = partials[i];
+    rnan |= isnan(q.a);
+    pnan |= isnan(q.b);
+    rmin = fmin(rmin, q.a);
+    pmin = fmin(pmin, q.b);
+    finite &= q.flag;
   }
-  if (rnan) rmin = NAN;
-  if (pnan) pmin = NAN;
+  finite = __syncthreads_and(finite);
+  rnan = __syncthreads_or(rnan);
+  pnan = __syncthreads_or(pnan);
+  sr[threadIdx.x] = rmin;
+  sp[threadIdx.x] = pmin;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) {
+      sr[threadIdx.x] = fmin(sr[threadIdx.x], sr[threadIdx.x + s]);
+      sp[threadIdx.x] = fmin(sp[threadIdx.x], sp[threadIdx.x + s]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  rmin = rnan ? NAN : sr[0];
+  pmin = pnan ? NAN : sp[0];
   const int valid = finite && (rmin >= rho_floor) && (pmin >= p_floor);
   if (combine) {
     status->valid = status->valid && valid;

@@ -5,6 +5,7 @@
 #include <string.h>
 
 #include <string>
+#include <algorithm>
 #include <vector>
 
 #include "aux_kernels.cuh"
@@ -68,7 +69,9 @@ struct dgb_plan {
   int adm_grid[DGB_MAX_BLOCKS] = {0, 0, 0};
   int npartials = 0;
   double* dt_scratch = nullptr;
-  size_t smem_traces[DGB_MAX_BLOCKS], smem_volume[DGB_MAX_BLOCKS], smem_final[DGB_MAX_BLOCKS];
+  // batched launches of the dense element kernels (all blocks in one grid) and their shared memory
+  ElemLaunch launch_tr, launch_vol, launch_fin, launch_tr64;
+  size_t smem_tr = 0, smem_vol = 0, smem_fin = 0, smem_tr64 = 0;
   size_t smem_pos[DGB_MAX_BLOCKS], smem_troubled[DGB_MAX_BLOCKS];
   // sum-factorised hexahedron path (single hexahedron block)
   bool hex = false;
@@ -138,6 +141,50 @@ int prepare(K kernel, size_t smem) {
 
 int blocks_for(long n, int per) { return (int)((n + per - 1) / per); }
 
+// ------------------------------------------------------------------ dense element launches
+enum DenseKind { traces_kind, volume_kind, finalize_kind };
+
+// Threads per element: a power of two covering the nodes, volume points and face points (the
+// face-point count bounded by local faces x the largest face rule), 16 to kThreads.
+int dense_width(const dgb_plan* p, const BlockDev& B) {
+  int nq = 0;
+  for (int ft = 0; ft < 2; ++ft)
+    if (p->face_present[ft] && p->dev.face[ft].nq > nq) nq = p->dev.face[ft].nq;
+  const int need = std::max(std::max(B.Np, B.Nq), B.nlf * nq);
+  int w = 16;
+  while (w < need && w < kThreads) w *= 2;
+  return w;
+}
+
+// Per-element shared-memory slots (bytes, 16-aligned) for one kernel kind and real size.
+void dense_slots(const dgb_plan* p, ElemLaunch& L, DenseKind kind, size_t rs) {
+  const int NV = p->dev.nv;
+  for (int b = 0; b < p->dev.nblocks; ++b) {
+    const BlockDev& B = p->dev.blk[b];
+    size_t vals = 0;
+    if (kind == traces_kind) vals = traces_slot(B.Np, NV);
+    else if (kind == volume_kind)
+      vals = VolumeSmem(B.Np, B.Nq, B.nlf, NV, p->dev.viscous, volume_chunks(B.Np, L.W[b])).total;
+    else vals = finalize_slot(B.Np, B.nlf, NV, p->dev.viscous);
+    L.slot[b] = (int)((vals * rs + 15) / 16 * 16);
+  }
+}
+
+// Fills the launch (block offsets, widths, slots) and returns its dynamic shared memory.
+size_t dense_smem(const dgb_plan* p, ElemLaunch& L, DenseKind kind, size_t rs) {
+  L.nblocks = p->dev.nblocks;
+  L.cta0[0] = 0;
+  for (int b = 0; b < p->dev.nblocks; ++b) {
+    L.W[b] = dense_width(p, p->dev.blk[b]);
+    L.cta0[b + 1] = L.cta0[b] + blocks_for(p->dev.blk[b].E, kThreads / L.W[b]);
+  }
+  dense_slots(p, L, kind, rs);
+  size_t most = 0;
+  for (int b = 0; b < p->dev.nblocks; ++b)
+    most = std::max(most, (size_t)(kThreads / L.W[b]) * (size_t)L.slot[b]);
+  return most;
+}
+
 // ------------------------------------------------------------------ RHS pipeline
 template <int P, int NV, bool SPLIT, typename R>
 int run_rhs_hex(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStream_t st, cudaEvent_t* ev) {
@@ -186,41 +233,40 @@ int run_rhs_hex_prec(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cud
                                : run_rhs_hex_deg<NV, SPLIT, double>(p, S, A, st, ev);
 }
 
-// events: optional array of DGB_RHS_STAGES + 1 events recorded around the stages
-template <int NV>
-int run_rhs(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStream_t st, cudaEvent_t* ev = nullptr) {
+template <int NV, typename R>
+int run_rhs_dense(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStream_t st, cudaEvent_t* ev) {
   const DevPlan& P = p->dev;
   int rc;
-  const bool split = !A.stage || A.out_vis[0] != nullptr;
-  if (p->hex) return split ? run_rhs_hex_prec<NV, true>(p, S, A, st, ev) : run_rhs_hex_prec<NV, false>(p, S, A, st, ev);
   if (ev) CK(cudaEventRecord(ev[0], st));
-  for (int b = 0; b < P.nblocks; ++b) {
-    if ((rc = prepare(k_traces<NV>, p->smem_traces[b]))) return rc;
-    k_traces<NV><<<P.blk[b].E, kThreads, p->smem_traces[b], st>>>(P, S, b);
-  }
+  if ((rc = prepare(k_traces<NV, R>, p->smem_tr))) return rc;
+  k_traces<NV, R><<<p->launch_tr.cta0[P.nblocks], kThreads, p->smem_tr, st>>>(P, S, p->launch_tr);
   if (ev) CK(cudaEventRecord(ev[1], st));
   for (int ft = 0; ft < 2; ++ft)
     if (p->face_present[ft])
       k_face_flux<NV><<<blocks_for((long)P.face[ft].F * P.face[ft].nq, kThreads), kThreads, 0, st>>>(P, S, ft);
   if (ev) CK(cudaEventRecord(ev[2], st));
   if (ev) CK(cudaEventRecord(ev[3], st));     // the dense k_volume does the BR2 lift itself
-  for (int b = 0; b < P.nblocks; ++b) {
-    if ((rc = prepare(k_volume<NV>, p->smem_volume[b]))) return rc;
-    k_volume<NV><<<P.blk[b].E, kThreads, p->smem_volume[b], st>>>(P, S, b);
-  }
+  if ((rc = prepare(k_volume<NV, R>, p->smem_vol))) return rc;
+  k_volume<NV, R><<<p->launch_vol.cta0[P.nblocks], kThreads, p->smem_vol, st>>>(P, S, p->launch_vol);
   if (ev) CK(cudaEventRecord(ev[4], st));
   if (P.viscous)
     for (int ft = 0; ft < 2; ++ft)
       if (p->face_present[ft])
         k_face_visc<NV><<<blocks_for((long)P.face[ft].F * P.face[ft].nq, kThreads), kThreads, 0, st>>>(P, ft);
   if (ev) CK(cudaEventRecord(ev[5], st));
-  for (int b = 0; b < P.nblocks; ++b) {
-    if ((rc = prepare(k_finalize<NV>, p->smem_final[b]))) return rc;
-    k_finalize<NV><<<P.blk[b].E, kThreads, p->smem_final[b], st>>>(P, S, b, A);
-  }
+  if ((rc = prepare(k_finalize<NV, R>, p->smem_fin))) return rc;
+  k_finalize<NV, R><<<p->launch_fin.cta0[P.nblocks], kThreads, p->smem_fin, st>>>(P, S, p->launch_fin, A);
   if (ev) CK(cudaEventRecord(ev[6], st));
   CK(cudaGetLastError());
   return DGB_OK;
+}
+
+// events: optional array of DGB_RHS_STAGES + 1 events recorded around the stages
+template <int NV>
+int run_rhs(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStream_t st, cudaEvent_t* ev = nullptr) {
+  const bool split = !A.stage || A.out_vis[0] != nullptr;
+  if (p->hex) return split ? run_rhs_hex_prec<NV, true>(p, S, A, st, ev) : run_rhs_hex_prec<NV, false>(p, S, A, st, ev);
+  return p->prm.precision == 1 ? run_rhs_dense<NV, float>(p, S, A, st, ev) : run_rhs_dense<NV, double>(p, S, A, st, ev);
 }
 
 template <int P, int NV>
@@ -270,7 +316,7 @@ int run_admissibility(dgb_plan* p, const StatePtrs& S, dgb_status* status, int c
     k_adm<NV><<<p->adm_grid[b], kThreads, 0, st>>>(p->dev, S, b, p->partials, off);
     off += p->adm_grid[b];
   }
-  k_adm_final<<<1, 32, 0, st>>>(p->partials, off, p->lim.adm_density_floor, p->lim.adm_pressure_floor, combine,
+  k_adm_final<<<1, kAdmFinalThreads, 0, st>>>(p->partials, off, p->lim.adm_density_floor, p->lim.adm_pressure_floor, combine,
                                 status);
   CK(cudaGetLastError());
   return DGB_OK;
@@ -527,10 +573,9 @@ int run_subcell_api(dgb_plan* p, const dgb_state* base, const dgb_state* cand, d
       }
     }
   } else {
-    for (int b = 0; b < P.nblocks; ++b) {
-      if ((rc = prepare(k_traces<NV>, p->smem_traces[b]))) return rc;
-      k_traces<NV><<<P.blk[b].E, kThreads, p->smem_traces[b], st>>>(P, S, b);
-    }
+    // the subcell scheme's DG face flux takes float64 traces in either precision mode
+    if ((rc = prepare(k_traces<NV, double>, p->smem_tr64))) return rc;
+    k_traces<NV, double><<<p->launch_tr64.cta0[P.nblocks], kThreads, p->smem_tr64, st>>>(P, S, p->launch_tr64);
   }
   double* candp[DGB_MAX_BLOCKS] = {cand->block[0], cand->block[1], cand->block[2]};
   double* visp[DGB_MAX_BLOCKS] = {arhs ? arhs->block[0] : nullptr, arhs ? arhs->block[1] : nullptr,
@@ -716,6 +761,7 @@ int dgb_plan_set_hex_affine(dgb_plan* p, const uint8_t* affine, const double* co
   if (p->finalized) return fail(DGB_ERR_ARGUMENT, "plan already finalized");
   if (!p->hex) return fail(DGB_ERR_ARGUMENT, "call dgb_plan_set_hex first");
   BlockDev& B = p->dev.blk[0];
+  if (B.wref) return fail(DGB_ERR_ARGUMENT, "block 0 already has dense affine data");
   int rc;
   if ((rc = upload(p, affine, (size_t)B.E, &B.affine))) return rc;
   if ((rc = upload(p, coef, (size_t)B.E, &B.acoef))) return rc;
@@ -724,12 +770,28 @@ int dgb_plan_set_hex_affine(dgb_plan* p, const uint8_t* affine, const double* co
   return DGB_OK;
 }
 
+int dgb_plan_set_block_affine(dgb_plan* p, int b, const uint8_t* affine, const double* coef, const double* jinv,
+                              const double* det, const double* ref_weights, const double* ref_inv_mass) {
+  if (!p || b < 0 || b >= p->dev.nblocks || !affine || !coef || !jinv || !det || !ref_weights || !ref_inv_mass)
+    return fail(DGB_ERR_ARGUMENT, "bad block-affine argument");
+  if (p->finalized) return fail(DGB_ERR_ARGUMENT, "plan already finalized");
+  if (!p->block_set[b]) return fail(DGB_ERR_ARGUMENT, "call dgb_plan_set_block first");
+  if (p->hex) return fail(DGB_ERR_ARGUMENT, "the sum-factorised path takes dgb_plan_set_hex_affine");
+  BlockDev& B = p->dev.blk[b];
+  int rc;
+  if ((rc = upload(p, affine, (size_t)B.E, &B.affine))) return rc;
+  if ((rc = upload(p, coef, (size_t)B.E, &B.acoef))) return rc;
+  if ((rc = upload(p, jinv, (size_t)B.E * 9, &B.ajinv))) return rc;
+  if ((rc = upload(p, det, (size_t)B.E, &B.adet))) return rc;
+  if ((rc = upload(p, ref_weights, (size_t)B.Nq, &B.wref))) return rc;
+  if ((rc = upload(p, ref_inv_mass, (size_t)B.Np * B.Np, &B.mref_inv))) return rc;
+  return DGB_OK;
+}
+
 int dgb_plan_finalize(dgb_plan* p) {
   if (!p) return fail(DGB_ERR_ARGUMENT, "null plan");
   const int NV = p->dev.nv;
   int rc;
-  if (p->prm.precision == 1 && !p->hex)
-    return fail(DGB_ERR_UNSUPPORTED, "mixed precision needs the sum-factorised single-hexahedron-block path");
   for (int b = 0; b < p->dev.nblocks; ++b)
     if (!p->block_set[b]) return fail(DGB_ERR_ARGUMENT, "block descriptor missing");
   for (int ft = 0; ft < 2; ++ft) {
@@ -739,8 +801,7 @@ int dgb_plan_finalize(dgb_plan* p) {
     if ((rc = alloc(p, n * 2 * nq * NV, &F.trA))) return rc;
     if ((rc = alloc(p, n * 2 * nq * NV, &F.fluxI))) return rc;
     if (p->dev.viscous) {
-      if (p->hex) F.trP = F.trA;   // the sum-factorised path uses the anchor-form trace for both
-      else if ((rc = alloc(p, n * 2 * nq * NV, &F.trP))) return rc;
+      F.trP = F.trA;   // the viscous terms take the anchor-form trace (equal to the plain one)
       if ((rc = alloc(p, n * 2 * nq * 4, &F.trV))) return rc;
       if ((rc = alloc(p, n * 2 * nq * 12, &F.trG))) return rc;
       if ((rc = alloc(p, n * nq * 12, &F.jumpW))) return rc;
@@ -764,16 +825,22 @@ int dgb_plan_finalize(dgb_plan* p) {
     for (int ft = 0; ft < 2; ++ft)
       if (p->face_present[ft] && p->dev.face[ft].nq > max_nq) max_nq = p->dev.face[ft].nq;
     (void)max_nq;
-    p->smem_traces[b] = sizeof(double) * (size_t)B.Np * (NV + 4);
-    p->smem_volume[b] = sizeof(double) * (size_t)VolumeSmem(B.Np, B.Nq, B.nlf, NV, p->dev.viscous).total;
-    p->smem_final[b] = sizeof(double) * (size_t)B.Np * NV * 2;
     p->smem_pos[b] = sizeof(double) * (size_t)(B.Np + B.Np + B.Nq + B.Ns) * NV;
     p->smem_troubled[b] = sizeof(double) * ((size_t)(B.Np + B.Np + B.Nq + B.Ns) * NV + 2 * B.Np);
     p->rate_grid[b] = blocks_for(B.E, kThreads / 32) < 2 * 148 * 8 ? blocks_for(B.E, kThreads / 32) : 2 * 148 * 8;
     const long nodes = (long)B.E * B.Np;
     p->adm_grid[b] = blocks_for(nodes, kThreads) < 148 * 8 ? blocks_for(nodes, kThreads) : 148 * 8;
     p->npartials += (p->rate_grid[b] > p->adm_grid[b] ? p->rate_grid[b] : p->adm_grid[b]);
-    if (p->smem_volume[b] > 227 * 1024 || p->smem_pos[b] > 227 * 1024)
+    if (p->smem_pos[b] > 227 * 1024)
+      return fail(DGB_ERR_UNSUPPORTED, "element too large for the shared-memory kernels");
+  }
+  if (!p->hex) {
+    const size_t rs = p->prm.precision == 1 ? sizeof(float) : sizeof(double);
+    p->smem_tr = dense_smem(p, p->launch_tr, traces_kind, rs);
+    p->smem_vol = dense_smem(p, p->launch_vol, volume_kind, rs);
+    p->smem_fin = dense_smem(p, p->launch_fin, finalize_kind, rs);
+    p->smem_tr64 = dense_smem(p, p->launch_tr64, traces_kind, sizeof(double));
+    if (p->smem_tr > 227 * 1024 || p->smem_vol > 227 * 1024 || p->smem_fin > 227 * 1024)
       return fail(DGB_ERR_UNSUPPORTED, "element too large for the shared-memory kernels");
   }
   {

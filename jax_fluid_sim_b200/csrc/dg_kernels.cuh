@@ -1,10 +1,10 @@
-// DG residual-and-update kernels (float64, any element type, P1-P3).
+// DG residual-and-update kernels for any element type (hexahedron, wedge, tetrahedron; P1-P3).
 //
 // Pipeline of one right-hand-side evaluation (reference: hybrid/spatial.py:137-249 and
 // hybrid/navier_stokes.py:27-347):
-//   k_traces      element-parallel: traces of U (anchor form and plain), of the viscous
-//                 variables and of their raw physical gradients at every face point of the
-//                 element's faces, written to face-side buffers.
+//   k_traces      element-parallel: anchor-form traces of U, traces of the viscous variables
+//                 and of their raw physical gradients at every face point of the element's
+//                 faces, written to face-side buffers.
 //   k_face_flux   face-point-parallel: HLLC flux (or boundary ghost) minus each side's anchor
 //                 flux, times w; BR2 jump 0.5*w*[v](x)n.
 //   k_volume      element-parallel: BR2 lifts r_f = M^-1 (B_f^T jump) per face, their face
@@ -13,7 +13,12 @@
 //   k_finalize    element-parallel: gathers the element's face contributions in local-face
 //                 order (no atomics: deterministic), applies M^-1, and either writes the
 //                 right-hand sides or the fused SSP-RK stage (current + dt*rhs, blended).
-// Every element kernel is one CTA per element; every face kernel one thread per face point.
+// The element kernels cover every block in one launch (ElemLaunch): a CTA of kThreads works on
+// G = kThreads / W elements of one block, W threads each (W a power of two >= the element's
+// nodes, volume points and face points, so P1 elements share a CTA and P2/P3 take one each).
+// They are templated on the arithmetic type R: double, or float for precision mode 1 (state,
+// anchors, face buffers and the stage update stay double).  Every face kernel is one thread per
+// face point.
 #pragma once
 #include <stdint.h>
 
@@ -38,11 +43,14 @@ struct BlockDev {
   const double* trdB[2];  // per face type: [codes][nq][Np][3]
   double* Rinv;           // scratch [E][Np][NV]
   double* Rvis;
-  // affine hexahedra (sum-factorised path, optional): constant metrics, M^-1 = coef * (m1i)^(x)3
+  // affine elements (optional): constant metrics; M^-1 = coef * (m1i)^(x)3 on the sum-factorised
+  // hexahedron path, coef * mref_inv on the dense path
   const uint8_t* affine;  // [E] 1 where the element map is affine
-  const double* acoef;    // [E] sliver scale / det J
+  const double* acoef;    // [E] sliver scale / |det J|
   const double* ajinv;    // [E][9] constant inverse Jacobian
-  const double* adet;     // [E] det J
+  const double* adet;     // [E] |det J|
+  const double* wref;     // [Nq] reference quadrature weights (dense path)
+  const double* mref_inv; // [Np][Np] inverse of the reference mass matrix B^T diag(wref) B (dense path)
 };
 
 struct FaceDev {
@@ -72,6 +80,23 @@ struct StatePtrs {
   double* b[DGB_MAX_BLOCKS];
 };
 
+// One launch over all blocks: CTAs [cta0[b], cta0[b+1]) work on block b, kThreads / W[b] elements
+// per CTA, slot[b] bytes of dynamic shared memory per element.
+struct ElemLaunch {
+  int nblocks;
+  int cta0[DGB_MAX_BLOCKS + 1];
+  int W[DGB_MAX_BLOCKS];
+  int slot[DGB_MAX_BLOCKS];
+};
+
+constexpr int kMaxGroups = kThreads / 16;   // W >= 16
+
+__device__ __forceinline__ int launch_block(const ElemLaunch& L) {
+  int b = 0;
+  while (b + 1 < L.nblocks && (int)blockIdx.x >= L.cta0[b + 1]) ++b;
+  return b;
+}
+
 __device__ __forceinline__ void decode_face(int32_t code, int& ft, int& f, int& side) {
   ft = (code >> 30) & 1;
   f = (code >> 1) & ((1 << 29) - 1);
@@ -79,60 +104,108 @@ __device__ __forceinline__ void decode_face(int32_t code, int& ft, int& f, int& 
 }
 
 // ---------------------------------------------------------------------------------------------
-template <int NV>
-__global__ void __launch_bounds__(kThreads) k_traces(const DevPlan P, const StatePtrs S, int b) {
-  extern __shared__ double smem[];
-  const BlockDev& B = P.blk[b];
-  const int e = blockIdx.x;
-  const int Np = B.Np;
-  double* U = smem;                 // [Np][NV]
-  double* V = U + Np * NV;          // [Np][4]
-  const double* Ug = S.b[b] + (size_t)e * Np * NV;
-  for (int i = threadIdx.x; i < Np * NV; i += blockDim.x) U[i] = Ug[i];
-  __syncthreads();
-  if (P.viscous) {
-    for (int i = threadIdx.x; i < Np; i += blockDim.x) viscous_vars<NV>(P.ph, U + i * NV, V + i * 4);
-    __syncthreads();
-  }
-  for (int lf = 0; lf < B.nlf; ++lf) {
+// Per-element face table of the element kernels: for local face lf its face type, face index,
+// side and trace code.
+struct ElemFaces {
+  int ft[6], f[6], side[6], code[6], nq[6];
+};
+
+__device__ __forceinline__ void load_faces(const DevPlan& P, const BlockDev& B, int e, int lane, ElemFaces& F) {
+  if (lane < B.nlf) {
     int ft, f, side;
-    decode_face(B.elem_face[e * B.nlf + lf], ft, f, side);
+    decode_face(B.elem_face[(size_t)e * B.nlf + lane], ft, f, side);
+    F.ft[lane] = ft;
+    F.f[lane] = f;
+    F.side[lane] = side;
+    F.code[lane] = side == 0 ? P.face[ft].oc[f] : P.face[ft].nc[f];
+    F.nq[lane] = P.face[ft].nq;
+  }
+}
+
+// Shared memory per element (in R values) of k_traces: U - anchor [Np][NV], v [Np][4].
+__host__ __device__ inline int traces_slot(int Np, int nv) { return Np * (nv + 4); }
+
+template <int NV, typename R>
+__global__ void __launch_bounds__(kThreads) k_traces(const DevPlan P, const StatePtrs S, const ElemLaunch L) {
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  __shared__ ElemFaces faces[kMaxGroups];
+  __shared__ double anchor[kMaxGroups][NV];
+  const int b = launch_block(L);
+  const BlockDev& B = P.blk[b];
+  const int W = L.W[b], g = threadIdx.x / W, lane = threadIdx.x % W;
+  const int e = (blockIdx.x - L.cta0[b]) * (kThreads / W) + g;
+  const bool live = e < B.E;
+  const int Np = B.Np, nlf = B.nlf;
+  R* U = reinterpret_cast<R*>(dyn_smem + (size_t)g * L.slot[b]);
+  R* V = U + Np * NV;
+  const double* Ug = S.b[b] + (size_t)(live ? e : 0) * Np * NV;
+  if (live) {
+    load_faces(P, B, e, lane, faces[g]);
+    if (lane < NV) anchor[g][lane] = Ug[lane];
+  }
+  __syncthreads();
+  if (live) {
+    for (int i = lane; i < Np * NV; i += W) U[i] = (R)(Ug[i] - anchor[g][i % NV]);
+    if (P.viscous)
+      for (int i = lane; i < Np; i += W) {
+        double u[NV], vv[4];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) u[v] = Ug[i * NV + v];
+        viscous_vars<NV>(P.ph, u, vv);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) V[i * 4 + m] = (R)vv[m];
+      }
+  }
+  __syncthreads();
+  if (!live) return;
+  const ElemFaces& Fc = faces[g];
+  int items = 0;
+  for (int lf = 0; lf < nlf; ++lf) items += Fc.nq[lf];
+  for (int t = lane; t < items; t += W) {
+    int lf = 0, q = t;
+    while (q >= Fc.nq[lf]) q -= Fc.nq[lf++];
+    const int ft = Fc.ft[lf], nq = Fc.nq[lf];
     const FaceDev& fd = P.face[ft];
-    const int nq = fd.nq;
-    const int tc = side == 0 ? fd.oc[f] : fd.nc[f];
-    const double* Bt = B.trB[ft] + (size_t)tc * nq * Np;
-    const size_t slot = ((size_t)f * 2 + side) * nq;
-    for (int idx = threadIdx.x; idx < nq * NV; idx += blockDim.x) {
-      const int q = idx / NV, v = idx % NV;
-      double s = 0.0;
-      for (int i = 0; i < Np; ++i) s += Bt[q * Np + i] * (U[i * NV + v] - U[v]);
-      fd.trA[(slot + q) * NV + v] = U[v] + s;
+    const double* Bt = B.trB[ft] + ((size_t)Fc.code[lf] * nq + q) * Np;
+    const size_t pt = ((size_t)Fc.f[lf] * 2 + Fc.side[lf]) * nq + q;
+    R acc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) acc[v] = (R)0;
+    for (int i = 0; i < Np; ++i) {
+      const R bt = (R)Bt[i];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) acc[v] += bt * U[i * NV + v];
     }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) fd.trA[pt * NV + v] = anchor[g][v] + (double)acc[v];
     if (P.viscous) {
-      const double* dBt = B.trdB[ft] + (size_t)tc * nq * Np * 3;
-      for (int idx = threadIdx.x; idx < nq * NV; idx += blockDim.x) {
-        const int q = idx / NV, v = idx % NV;
-        double s = 0.0;
-        for (int i = 0; i < Np; ++i) s += Bt[q * Np + i] * U[i * NV + v];
-        fd.trP[(slot + q) * NV + v] = s;
-      }
-      for (int idx = threadIdx.x; idx < nq * 4; idx += blockDim.x) {
-        const int q = idx / 4, m = idx % 4;
-        double s = 0.0;
-        for (int i = 0; i < Np; ++i) s += Bt[q * Np + i] * V[i * 4 + m];
-        fd.trV[(slot + q) * 4 + m] = s;
-      }
-      for (int idx = threadIdx.x; idx < nq * 12; idx += blockDim.x) {
-        const int q = idx / 12, m = (idx % 12) / 3, d = idx % 3;
-        const double* J = fd.jinv + (slot + q) * 9;
-        double s = 0.0;
-        for (int i = 0; i < Np; ++i) {
-          const double* g = dBt + ((size_t)q * Np + i) * 3;
-          const double gp = g[0] * J[0 * 3 + d] + g[1] * J[1 * 3 + d] + g[2] * J[2 * 3 + d];
-          s += V[i * 4 + m] * gp;
+      const double* dBt = B.trdB[ft] + ((size_t)Fc.code[lf] * nq + q) * Np * 3;
+      R J[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) J[k] = (R)fd.jinv[pt * 9 + k];
+      R tv[4], tg[12];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) tv[k] = (R)0;
+#pragma unroll
+      for (int k = 0; k < 12; ++k) tg[k] = (R)0;
+      for (int i = 0; i < Np; ++i) {
+        const R bt = (R)Bt[i];
+        const R g0 = (R)dBt[i * 3 + 0], g1 = (R)dBt[i * 3 + 1], g2 = (R)dBt[i * 3 + 2];
+        R gp[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) gp[d] = g0 * J[0 * 3 + d] + g1 * J[1 * 3 + d] + g2 * J[2 * 3 + d];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const R vm = V[i * 4 + m];
+          tv[m] += bt * vm;
+#pragma unroll
+          for (int d = 0; d < 3; ++d) tg[m * 3 + d] += vm * gp[d];
         }
-        fd.trG[(slot + q) * 12 + m * 3 + d] = s;
       }
+#pragma unroll
+      for (int m = 0; m < 4; ++m) fd.trV[pt * 4 + m] = (double)tv[m];
+#pragma unroll
+      for (int k = 0; k < 12; ++k) fd.trG[pt * 12 + k] = (double)tg[k];
     }
   }
 }
@@ -203,171 +276,232 @@ __global__ void __launch_bounds__(kThreads) k_face_flux(const DevPlan P, const S
 }
 
 // ---------------------------------------------------------------------------------------------
-// Shared-memory layout of k_volume, in doubles.
+// Shared-memory layout of k_volume per element, in R values.  The residual sum over volume points
+// is split into C chunks of points (C = W / Np threads per node) and the chunks' partial sums
+// are added in a second pass.
 struct VolumeSmem {
-  int U, V, lift, bf, rf, Gi, Gv, total;
-  __host__ __device__ VolumeSmem(int Np, int Nq, int nlf, int nv, int viscous) {
+  int U, V, lift, bf, rf, Gi, Gv, Rp, Rpv, total;
+  __host__ __device__ VolumeSmem(int Np, int Nq, int nlf, int nv, int viscous, int C) {
     U = 0;
     V = U + Np * nv;
-    lift = V + Np * 4;
+    lift = V + (viscous ? Np * 4 : 0);
     bf = lift + (viscous ? Np * 12 : 0);
     rf = bf + (viscous ? nlf * Np * 12 : 0);
     Gi = rf + (viscous ? nlf * Np * 12 : 0);
     Gv = Gi + Nq * 3 * nv;
-    total = Gv + (viscous ? Nq * 3 * nv : 0);
+    Rp = Gv + (viscous ? Nq * 3 * nv : 0);
+    Rpv = Rp + C * Np * nv;
+    total = Rpv + (viscous ? C * Np * nv : 0);
   }
 };
 
-template <int NV>
-__global__ void __launch_bounds__(kThreads) k_volume(const DevPlan P, const StatePtrs S, int b) {
-  extern __shared__ double smem[];
+__host__ __device__ inline int volume_chunks(int Np, int W) { return Np <= W ? W / Np : 1; }
+
+template <int NV, typename R>
+__global__ void __launch_bounds__(kThreads, NV <= 5 ? 4 : 1) k_volume(const DevPlan P, const StatePtrs S,
+                                                                    const ElemLaunch L) {
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  __shared__ ElemFaces faces[kMaxGroups];
+  __shared__ double anchor[kMaxGroups][NV];
+  const int b = launch_block(L);
   const BlockDev& B = P.blk[b];
-  const int e = blockIdx.x;
+  const int W = L.W[b], g = threadIdx.x / W, lane = threadIdx.x % W;
+  const int e = (blockIdx.x - L.cta0[b]) * (kThreads / W) + g;
+  const bool live = e < B.E;
   const int Np = B.Np, Nq = B.Nq, nlf = B.nlf;
-  const VolumeSmem L(Np, Nq, nlf, NV, P.viscous);
-  double* U = smem + L.U;
-  double* V = smem + L.V;
-  double* lift = smem + L.lift;
-  double* bf = smem + L.bf;
-  double* rf = smem + L.rf;
-  double* Gi = smem + L.Gi;
-  double* Gv = smem + L.Gv;
-  const double* Ug = S.b[b] + (size_t)e * Np * NV;
-  for (int i = threadIdx.x; i < Np * NV; i += blockDim.x) U[i] = Ug[i];
+  const int C = volume_chunks(Np, W);
+  const VolumeSmem Ls(Np, Nq, nlf, NV, P.viscous, C);
+  R* sm = reinterpret_cast<R*>(dyn_smem + (size_t)g * L.slot[b]);
+  R* U = sm + Ls.U;
+  R* V = sm + Ls.V;
+  R* lift = sm + Ls.lift;
+  R* bf = sm + Ls.bf;
+  R* rf = sm + Ls.rf;
+  R* Gi = sm + Ls.Gi;
+  R* Gv = sm + Ls.Gv;
+  R* Rp = sm + Ls.Rp;
+  R* Rpv = sm + Ls.Rpv;
+  const size_t ee = live ? e : 0;
+  const double* Ug = S.b[b] + ee * Np * NV;
+  if (live) {
+    load_faces(P, B, (int)ee, lane, faces[g]);
+    if (lane < NV) anchor[g][lane] = Ug[lane];
+  }
   __syncthreads();
-  const double* jinv = B.jinv + (size_t)e * Nq * 9;
-  const double* wdet = B.wdet + (size_t)e * Nq;
-  if (P.viscous) {
-    for (int i = threadIdx.x; i < Np; i += blockDim.x) viscous_vars<NV>(P.ph, U + i * NV, V + i * 4);
-    // b_f[i][c] = sum_q B_f(q,i) jumpW_f(q,c)
-    for (int idx = threadIdx.x; idx < nlf * Np * 12; idx += blockDim.x) {
-      const int lf = idx / (Np * 12), i = (idx / 12) % Np, c = idx % 12;
-      int ft, f, side;
-      decode_face(B.elem_face[e * nlf + lf], ft, f, side);
-      const FaceDev& fd = P.face[ft];
-      const int nq = fd.nq;
-      const int tc = side == 0 ? fd.oc[f] : fd.nc[f];
-      const double* Bt = B.trB[ft] + (size_t)tc * nq * Np;
-      const double* J = fd.jumpW + (size_t)f * nq * 12;
-      double s = 0.0;
-      for (int q = 0; q < nq; ++q) s += J[q * 12 + c] * Bt[q * Np + i];
-      bf[idx] = s;
+  // affine elements read one inverse Jacobian and |det J| instead of per-point tables
+  const bool aff = B.affine != nullptr && B.affine[ee];
+  const double* jinv = aff ? B.ajinv + ee * 9 : B.jinv + ee * Nq * 9;
+  const int jstride = aff ? 0 : 9;
+  const double* wdet = aff ? B.wref : B.wdet + ee * Nq;
+  const double wscale = aff ? B.adet[ee] : 1.0;
+  const double* Mi = aff ? B.mref_inv : B.minv + ee * Np * Np;
+  const R mscale = (R)(aff ? B.acoef[ee] : 1.0);
+  const ElemFaces& Fc = faces[g];
+  if (live) {
+    for (int i = lane; i < Np * NV; i += W) U[i] = (R)(Ug[i] - anchor[g][i % NV]);
+    if (P.viscous) {
+      for (int i = lane; i < Np; i += W) {
+        double u[NV], vv[4];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) u[v] = Ug[i * NV + v];
+        viscous_vars<NV>(P.ph, u, vv);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) V[i * 4 + m] = (R)vv[m];
+      }
+      // b_f[i][c] = sum_q B_f(q,i) jumpW_f(q,c)
+      for (int idx = lane; idx < nlf * Np * 12; idx += W) {
+        const int lf = idx / (Np * 12), i = (idx / 12) % Np, c = idx % 12;
+        const int nq = Fc.nq[lf];
+        const double* Bt = B.trB[Fc.ft[lf]] + (size_t)Fc.code[lf] * nq * Np;
+        const double* Jw = P.face[Fc.ft[lf]].jumpW + (size_t)Fc.f[lf] * nq * 12;
+        R acc = (R)0;
+        for (int q = 0; q < nq; ++q) acc += (R)Jw[q * 12 + c] * (R)Bt[q * Np + i];
+        bf[idx] = acc;
+      }
     }
-    __syncthreads();
+  }
+  __syncthreads();
+  if (live && P.viscous) {
     // r_f = M^-1 b_f
-    const double* Mi = B.minv + (size_t)e * Np * Np;
-    for (int idx = threadIdx.x; idx < nlf * Np * 12; idx += blockDim.x) {
+    for (int idx = lane; idx < nlf * Np * 12; idx += W) {
       const int lf = idx / (Np * 12), i = (idx / 12) % Np, c = idx % 12;
       const double* row = Mi + (size_t)i * Np;
-      const double* col = bf + (size_t)lf * Np * 12 + c;
-      double s = 0.0;
-      for (int j = 0; j < Np; ++j) s += row[j] * col[j * 12];
-      rf[idx] = s;
+      const R* col = bf + (size_t)lf * Np * 12 + c;
+      R acc = (R)0;
+      for (int j = 0; j < Np; ++j) acc += (R)row[j] * col[j * 12];
+      rf[idx] = mscale * acc;
     }
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < Np * 12; idx += blockDim.x) {
-      double s = 0.0;
-      for (int lf = 0; lf < nlf; ++lf) s += rf[lf * Np * 12 + idx];
-      lift[idx] = s;
+  }
+  __syncthreads();
+  if (live && P.viscous) {
+    for (int idx = lane; idx < Np * 12; idx += W) {
+      R acc = (R)0;
+      for (int lf = 0; lf < nlf; ++lf) acc += rf[lf * Np * 12 + idx];
+      lift[idx] = acc;
     }
     // face values of each face's own lift, scaled by the BR2 penalty
-    for (int lf = 0; lf < nlf; ++lf) {
-      int ft, f, side;
-      decode_face(B.elem_face[e * nlf + lf], ft, f, side);
-      const FaceDev& fd = P.face[ft];
-      const int nq = fd.nq;
-      const int tc = side == 0 ? fd.oc[f] : fd.nc[f];
-      const double* Bt = B.trB[ft] + (size_t)tc * nq * Np;
-      for (int idx = threadIdx.x; idx < nq * 12; idx += blockDim.x) {
-        const int q = idx / 12, c = idx % 12;
-        double s = 0.0;
-        for (int i = 0; i < Np; ++i) s += Bt[q * Np + i] * rf[(lf * Np + i) * 12 + c];
-        fd.liftF[(((size_t)f * 2 + side) * nq + q) * 12 + c] = P.ph.br2 * s;
-      }
+    int items = 0;
+    for (int lf = 0; lf < nlf; ++lf) items += Fc.nq[lf] * 12;
+    for (int t = lane; t < items; t += W) {
+      int lf = 0, r = t;
+      while (r >= Fc.nq[lf] * 12) r -= Fc.nq[lf++] * 12;
+      const int q = r / 12, c = r % 12, nq = Fc.nq[lf];
+      const double* Bt = B.trB[Fc.ft[lf]] + ((size_t)Fc.code[lf] * nq + q) * Np;
+      R acc = (R)0;
+      for (int i = 0; i < Np; ++i) acc += (R)Bt[i] * rf[(lf * Np + i) * 12 + c];
+      P.face[Fc.ft[lf]].liftF[(((size_t)Fc.f[lf] * 2 + Fc.side[lf]) * nq + q) * 12 + c] =
+          P.ph.br2 * (double)acc;
     }
-    __syncthreads();
   }
+  __syncthreads();
   // volume terms at each quadrature point
-  double Fa[3][NV];
-  {
-    const double ex[3] = {1.0, 0.0, 0.0}, ey[3] = {0.0, 1.0, 0.0}, ez[3] = {0.0, 0.0, 1.0};
-    normal_flux<NV>(P.ph, U, ex, Fa[0]);
-    normal_flux<NV>(P.ph, U, ey, Fa[1]);
-    normal_flux<NV>(P.ph, U, ez, Fa[2]);
-  }
-  for (int q = threadIdx.x; q < Nq; q += blockDim.x) {
-    const double* Bq = B.B + (size_t)q * Np;
-    const double* J = jinv + q * 9;
-    const double wq = wdet[q];
-    double Uq[NV], F[3][NV];
+  if (live) {
+    R a[NV], Fa[3][NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      double s = 0.0;
-      for (int i = 0; i < Np; ++i) s += Bq[i] * (U[i * NV + v] - U[v]);
-      Uq[v] = U[v] + s;
-    }
+    for (int v = 0; v < NV; ++v) a[v] = (R)anchor[g][v];
     {
-      const double ex[3] = {1.0, 0.0, 0.0}, ey[3] = {0.0, 1.0, 0.0}, ez[3] = {0.0, 0.0, 1.0};
-      normal_flux<NV>(P.ph, Uq, ex, F[0]);
-      normal_flux<NV>(P.ph, Uq, ey, F[1]);
-      normal_flux<NV>(P.ph, Uq, ez, F[2]);
+      const R ex[3] = {(R)1, (R)0, (R)0}, ey[3] = {(R)0, (R)1, (R)0}, ez[3] = {(R)0, (R)0, (R)1};
+      normal_flux<NV>(P.ph, a, ex, Fa[0]);
+      normal_flux<NV>(P.ph, a, ey, Fa[1]);
+      normal_flux<NV>(P.ph, a, ez, Fa[2]);
     }
+    for (int q = lane; q < Nq; q += W) {
+      const double* Bq = B.B + (size_t)q * Np;
+      const double* Jd = jinv + q * jstride;
+      R J[9];
 #pragma unroll
-    for (int r = 0; r < 3; ++r)
+      for (int k = 0; k < 9; ++k) J[k] = (R)Jd[k];
+      const R wq = (R)(wdet[q] * wscale);
+      R Uq[NV];
 #pragma unroll
-      for (int v = 0; v < NV; ++v)
-        Gi[(q * 3 + r) * NV + v] = (J[r * 3 + 0] * (F[0][v] - Fa[0][v]) + J[r * 3 + 1] * (F[1][v] - Fa[1][v]) +
-                                    J[r * 3 + 2] * (F[2][v] - Fa[2][v])) * wq;
-    if (P.viscous) {
-      double Up[NV], grad[12];
-#pragma unroll
-      for (int v = 0; v < NV; ++v) {
-        double s = 0.0;
-        for (int i = 0; i < Np; ++i) s += Bq[i] * U[i * NV + v];
-        Up[v] = s;
-      }
-#pragma unroll
-      for (int c = 0; c < 12; ++c) grad[c] = 0.0;
+      for (int v = 0; v < NV; ++v) Uq[v] = (R)0;
       for (int i = 0; i < Np; ++i) {
-        const double* g = B.dB + ((size_t)q * Np + i) * 3;
-        double gp[3];
+        const R bq = (R)Bq[i];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) gp[d] = g[0] * J[0 * 3 + d] + g[1] * J[1 * 3 + d] + g[2] * J[2 * 3 + d];
-#pragma unroll
-        for (int m = 0; m < 4; ++m)
-#pragma unroll
-          for (int d = 0; d < 3; ++d) grad[m * 3 + d] += V[i * 4 + m] * gp[d];
+        for (int v = 0; v < NV; ++v) Uq[v] += bq * U[i * NV + v];
       }
 #pragma unroll
-      for (int c = 0; c < 12; ++c) {
-        double s = 0.0;
-        for (int i = 0; i < Np; ++i) s += Bq[i] * lift[i * 12 + c];
-        grad[c] += s;
+      for (int v = 0; v < NV; ++v) Uq[v] = (R)(anchor[g][v] + (double)Uq[v]);
+      R F[3][NV];
+      {
+        const R ex[3] = {(R)1, (R)0, (R)0}, ey[3] = {(R)0, (R)1, (R)0}, ez[3] = {(R)0, (R)0, (R)1};
+        normal_flux<NV>(P.ph, Uq, ex, F[0]);
+        normal_flux<NV>(P.ph, Uq, ey, F[1]);
+        normal_flux<NV>(P.ph, Uq, ez, F[2]);
       }
-      double Fv[3 * NV];
-      viscous_flux<NV>(P.ph, Up, grad, Fv);
 #pragma unroll
       for (int r = 0; r < 3; ++r)
 #pragma unroll
         for (int v = 0; v < NV; ++v)
-          Gv[(q * 3 + r) * NV + v] =
-              -(J[r * 3 + 0] * Fv[0 * NV + v] + J[r * 3 + 1] * Fv[1 * NV + v] + J[r * 3 + 2] * Fv[2 * NV + v]) * wq;
+          Gi[(q * 3 + r) * NV + v] = (J[r * 3 + 0] * (F[0][v] - Fa[0][v]) + J[r * 3 + 1] * (F[1][v] - Fa[1][v]) +
+                                      J[r * 3 + 2] * (F[2][v] - Fa[2][v])) * wq;
+      if (P.viscous) {
+        R grad[12];
+#pragma unroll
+        for (int c = 0; c < 12; ++c) grad[c] = (R)0;
+        for (int i = 0; i < Np; ++i) {
+          const double* gd = B.dB + ((size_t)q * Np + i) * 3;
+          const R g0 = (R)gd[0], g1 = (R)gd[1], g2 = (R)gd[2], bq = (R)Bq[i];
+          R gp[3];
+#pragma unroll
+          for (int d = 0; d < 3; ++d) gp[d] = g0 * J[0 * 3 + d] + g1 * J[1 * 3 + d] + g2 * J[2 * 3 + d];
+#pragma unroll
+          for (int m = 0; m < 4; ++m)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) grad[m * 3 + d] += V[i * 4 + m] * gp[d] + bq * lift[i * 12 + m * 3 + d];
+        }
+        R Fv[3 * NV];
+        viscous_flux<NV>(P.ph, Uq, grad, Fv);
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int v = 0; v < NV; ++v)
+            Gv[(q * 3 + r) * NV + v] =
+                -(J[r * 3 + 0] * Fv[0 * NV + v] + J[r * 3 + 1] * Fv[1 * NV + v] + J[r * 3 + 2] * Fv[2 * NV + v]) * wq;
+      }
     }
   }
   __syncthreads();
-  double* Ri = B.Rinv + (size_t)e * Np * NV;
-  double* Rv = B.Rvis + (size_t)e * Np * NV;
-  for (int idx = threadIdx.x; idx < Np * NV; idx += blockDim.x) {
-    const int i = idx / NV, v = idx % NV;
-    double si = 0.0, sv = 0.0;
-    for (int q = 0; q < Nq; ++q) {
-      const double* g = B.dB + ((size_t)q * Np + i) * 3;
-      si += g[0] * Gi[(q * 3 + 0) * NV + v] + g[1] * Gi[(q * 3 + 1) * NV + v] + g[2] * Gi[(q * 3 + 2) * NV + v];
+  // residual: thread (node i, chunk c) sums its chunk of points, all variables at once
+  if (live) {
+    for (int t = lane; t < C * Np; t += W) {
+      const int i = t % Np, c = t / Np;
+      const int q0 = c * Nq / C, q1 = (c + 1) * Nq / C;
+      R si[NV], sv[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) si[v] = sv[v] = (R)0;
+      for (int q = q0; q < q1; ++q) {
+        const double* gd = B.dB + ((size_t)q * Np + i) * 3;
+        const R g0 = (R)gd[0], g1 = (R)gd[1], g2 = (R)gd[2];
+        const R* G = Gi + q * 3 * NV;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) si[v] += g0 * G[v] + g1 * G[NV + v] + g2 * G[2 * NV + v];
+        if (P.viscous) {
+          const R* H = Gv + q * 3 * NV;
+#pragma unroll
+          for (int v = 0; v < NV; ++v) sv[v] += g0 * H[v] + g1 * H[NV + v] + g2 * H[2 * NV + v];
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < NV; ++v) Rp[(c * Np + i) * NV + v] = si[v];
       if (P.viscous)
-        sv += g[0] * Gv[(q * 3 + 0) * NV + v] + g[1] * Gv[(q * 3 + 1) * NV + v] + g[2] * Gv[(q * 3 + 2) * NV + v];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Rpv[(c * Np + i) * NV + v] = sv[v];
     }
-    Ri[idx] = si;
-    if (P.viscous) Rv[idx] = sv;
+  }
+  __syncthreads();
+  if (live) {
+    double* Ri = B.Rinv + ee * Np * NV;
+    double* Rv = B.Rvis + ee * Np * NV;
+    for (int idx = lane; idx < Np * NV; idx += W) {
+      R si = (R)0, sv = (R)0;
+      for (int c = 0; c < C; ++c) {
+        si += Rp[c * Np * NV + idx];
+        if (P.viscous) sv += Rpv[c * Np * NV + idx];
+      }
+      Ri[idx] = (double)si;
+      if (P.viscous) Rv[idx] = (double)sv;
+    }
   }
 }
 
@@ -419,58 +553,101 @@ struct FinalizeArgs {
   double* euler[DGB_MAX_BLOCKS];     // may be null
 };
 
-template <int NV>
-__global__ void __launch_bounds__(kThreads) k_finalize(const DevPlan P, const StatePtrs S, int b,
+// Shared memory per element (in R values) of k_finalize: face partials [nlf][Np][NV] and the
+// totals [Np][NV], inviscid and (when viscous) viscous.
+__host__ __device__ inline int finalize_slot(int Np, int nlf, int nv, int viscous) {
+  return (viscous ? 2 : 1) * (nlf + 1) * Np * nv;
+}
+
+template <int NV, typename R>
+__global__ void __launch_bounds__(kThreads) k_finalize(const DevPlan P, const StatePtrs S, const ElemLaunch L,
                                                       const FinalizeArgs A) {
-  extern __shared__ double smem[];
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  __shared__ ElemFaces faces[kMaxGroups];
+  const int b = launch_block(L);
   const BlockDev& B = P.blk[b];
-  const int e = blockIdx.x;
+  const int W = L.W[b], g = threadIdx.x / W, lane = threadIdx.x % W;
+  const int e = (blockIdx.x - L.cta0[b]) * (kThreads / W) + g;
+  const bool live = e < B.E;
   const int Np = B.Np, nlf = B.nlf;
-  double* Ri = smem;
-  double* Rv = smem + Np * NV;
-  const size_t base = (size_t)e * Np * NV;
-  for (int idx = threadIdx.x; idx < Np * NV; idx += blockDim.x) {
-    const int i = idx / NV, v = idx % NV;
-    double si = B.Rinv[base + idx];
-    double sv = P.viscous ? B.Rvis[base + idx] : 0.0;
-    for (int lf = 0; lf < nlf; ++lf) {
-      int ft, f, side;
-      decode_face(B.elem_face[e * nlf + lf], ft, f, side);
-      const FaceDev& fd = P.face[ft];
-      const int nq = fd.nq;
-      const int tc = side == 0 ? fd.oc[f] : fd.nc[f];
-      const double* Bt = B.trB[ft] + (size_t)tc * nq * Np;
-      const double* fi = fd.fluxI + ((size_t)f * 2 + side) * nq * NV;
-      double s = 0.0;
-      for (int q = 0; q < nq; ++q) s += Bt[q * Np + i] * fi[q * NV + v];
-      si += side == 0 ? -s : s;
-      if (P.viscous) {
-        const double* fv = fd.fluxV + (size_t)f * nq * NV;
-        double t = 0.0;
-        for (int q = 0; q < nq; ++q) t += Bt[q * Np + i] * fv[q * NV + v];
-        sv += side == 0 ? t : -t;
+  const bool visc = P.viscous;
+  R* Fp = reinterpret_cast<R*>(dyn_smem + (size_t)g * L.slot[b]);   // [nlf][Np][NV]
+  R* Ft = Fp + nlf * Np * NV;                                         // [Np][NV]
+  R* Vp = Ft + Np * NV;                                               // viscous copies
+  R* Vt = Vp + nlf * Np * NV;
+  const size_t ee = live ? e : 0;
+  if (live) load_faces(P, B, (int)ee, lane, faces[g]);
+  __syncthreads();
+  const ElemFaces& Fc = faces[g];
+  if (live) {
+    // face contributions: thread (face, node) sums the face's points, all variables at once
+    for (int t = lane; t < nlf * Np; t += W) {
+      const int lf = t / Np, i = t % Np, nq = Fc.nq[lf];
+      const FaceDev& fd = P.face[Fc.ft[lf]];
+      const double* Bt = B.trB[Fc.ft[lf]] + (size_t)Fc.code[lf] * nq * Np + i;
+      const double* fi = fd.fluxI + ((size_t)Fc.f[lf] * 2 + Fc.side[lf]) * nq * NV;
+      const R sgn = Fc.side[lf] == 0 ? (R)-1 : (R)1;
+      R si[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) si[v] = (R)0;
+      for (int q = 0; q < nq; ++q) {
+        const R bt = (R)Bt[(size_t)q * Np];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) si[v] += bt * (R)fi[q * NV + v];
+      }
+#pragma unroll
+      for (int v = 0; v < NV; ++v) Fp[t * NV + v] = sgn * si[v];
+      if (visc) {
+        const double* fv = fd.fluxV + (size_t)Fc.f[lf] * nq * NV;
+        R sv[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) sv[v] = (R)0;
+        for (int q = 0; q < nq; ++q) {
+          const R bt = (R)Bt[(size_t)q * Np];
+#pragma unroll
+          for (int v = 0; v < NV; ++v) sv[v] += bt * (R)fv[q * NV + v];
+        }
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Vp[t * NV + v] = -sgn * sv[v];
       }
     }
-    Ri[idx] = si;
-    Rv[idx] = sv;
   }
   __syncthreads();
-  const double* Mi = B.minv + (size_t)e * Np * Np;
-  for (int idx = threadIdx.x; idx < Np * NV; idx += blockDim.x) {
+  const size_t base = ee * Np * NV;
+  if (live) {
+    for (int idx = lane; idx < Np * NV; idx += W) {
+      R si = (R)B.Rinv[base + idx];
+      for (int lf = 0; lf < nlf; ++lf) si += Fp[lf * Np * NV + idx];
+      Ft[idx] = si;
+      if (visc) {
+        R sv = (R)B.Rvis[base + idx];
+        for (int lf = 0; lf < nlf; ++lf) sv += Vp[lf * Np * NV + idx];
+        Vt[idx] = sv;
+      }
+    }
+  }
+  __syncthreads();
+  if (!live) return;
+  const bool aff = B.affine != nullptr && B.affine[ee];
+  const double* Mi = aff ? B.mref_inv : B.minv + ee * Np * Np;
+  const R mscale = (R)(aff ? B.acoef[ee] : 1.0);
+  for (int idx = lane; idx < Np * NV; idx += W) {
     const int i = idx / NV, v = idx % NV;
     const double* row = Mi + (size_t)i * Np;
-    double ri = 0.0, rv = 0.0;
+    R ri = (R)0, rv = (R)0;
     for (int j = 0; j < Np; ++j) {
-      ri += row[j] * Ri[j * NV + v];
-      rv += row[j] * Rv[j * NV + v];
+      const R m = (R)row[j];
+      ri += m * Ft[j * NV + v];
+      if (visc) rv += m * Vt[j * NV + v];
     }
+    const double rid = (double)(mscale * ri), rvd = visc ? (double)(mscale * rv) : 0.0;
     if (!A.stage) {
-      if (A.out_inv[b]) A.out_inv[b][base + idx] = ri;
-      if (A.out_vis[b]) A.out_vis[b][base + idx] = rv;
+      if (A.out_inv[b]) A.out_inv[b][base + idx] = rid;
+      if (A.out_vis[b]) A.out_vis[b][base + idx] = rvd;
     } else {
-      const double total = P.viscous ? ri + rv : ri;
+      const double total = visc ? rid + rvd : rid;
       const double eul = S.b[b][base + idx] + A.dt * total;
-      if (A.out_vis[b]) A.out_vis[b][base + idx] = rv;
+      if (A.out_vis[b]) A.out_vis[b][base + idx] = rvd;
       if (A.euler[b]) A.euler[b][base + idx] = eul;
       A.dst[b][base + idx] = A.alpha * A.base[b][base + idx] + A.beta * eul;
     }

@@ -14,7 +14,7 @@ import numpy as np
 import torch
 
 from . import _native as N
-from .plan import Plan, hex_affine_data, hex_sumfact_tables
+from .plan import Plan, block_affine_data, hex_affine_data, hex_sumfact_tables
 from .reference import FACE_TYPE_ID, TYPE_ID
 
 
@@ -55,11 +55,10 @@ class NativePlan:
         N.check(L.dgb_plan_create(ctypes.byref(prm), ctypes.byref(handle)))
         self.handle = handle
         keep = []
+        affine_counts = []
         single_hex = len(plan.blocks) == 1 and plan.blocks[0].etype == "hexahedron"
         if sum_factorised is None:
             sum_factorised = single_hex
-        if precision == "mixed" and not sum_factorised:
-            raise NotImplementedError("precision='mixed' runs on the sum-factorised path: one hexahedron block")
         for b, bp in enumerate(plan.blocks):
             # the sum-factorised kernels stream M^-1 transposed (coalesced across nodes)
             minv = np.ascontiguousarray(np.swapaxes(bp.minv, 1, 2)) if sum_factorised else bp.minv
@@ -75,6 +74,13 @@ class NativePlan:
             for k, a in arrays.items():
                 setattr(d, k, N.dptr(a))
             N.check(L.dgb_plan_set_block(handle, b, ctypes.byref(d)))
+            if affine and not sum_factorised:
+                aff, coef, ajinv, det, wref, mref_inv = block_affine_data(bp)
+                aff = np.ascontiguousarray(aff, np.uint8)
+                dbl = [N.as_f64(a) for a in (coef, ajinv, det, wref, mref_inv)]
+                keep += [aff] + dbl
+                N.check(L.dgb_plan_set_block_affine(handle, b, N.dptr(aff, ctypes.c_uint8), *[N.dptr(a) for a in dbl]))
+                affine_counts.append(int(aff.sum()))
         for ftype, fp in plan.faces.items():
             ints = {k: N.as_i32(v) for k, v in dict(owner_block=fp.owner_block, owner_local=fp.owner_local,
                                                       owner_code=fp.ocode, nbr_block=fp.nbr_block,
@@ -111,8 +117,12 @@ class NativePlan:
                                                   N.dptr(det)))
                 self.affine_fraction = float(aff.mean())
                 self.affine_count = int(aff.sum())
+        if affine_counts:
+            self.affine_count = sum(affine_counts)
+            self.affine_fraction = self.affine_count / sum(bp.E for bp in plan.blocks)
+            self.block_affine_counts = affine_counts
         self.sum_factorised = bool(sum_factorised)
-        self.affine = bool(sum_factorised and affine)
+        self.affine = bool(affine)
         N.check(L.dgb_plan_finalize(handle))
         self._pushed = self._snapshot()
 
@@ -195,8 +205,8 @@ class HybridEulerOperator:
 
     def __init__(self, solver, br2_stabilization=None, sum_factorised=None, precision="float64", affine=True):
         """``precision``: "float64" (the reference's arithmetic) or "mixed" (float32 arithmetic in
-        the hexahedron trace, BR2-lift, volume and finalize kernels; the state, face fluxes,
-        limiters, reductions and the stage update stay float64).  ``affine``: on the sum-factorised
+        the trace, BR2-lift, volume and finalize kernels of every element type; the state, face
+        fluxes, limiters, reductions and the stage update stay float64).  ``affine``: on the sum-factorised
         path, elements with an affine map use constant metrics and a tensor-product inverse mass
         matrix (equal to the dense one to round-off) instead of reading per-element tables."""
         self.solver = solver

@@ -339,3 +339,19 @@ def hex_affine_data(plan: Plan, tol=1.0e-10):
     det = bp.volume.astype(np.float64)              # the reference hexahedron [0, 1]^3 has volume 1
     coef = np.minimum(1.0, bp.volume / 1.0e-4) / det
     return affine, coef, np.ascontiguousarray(J.mean(axis=1)), det
+
+
+def block_affine_data(bp, tol=1.0e-10):
+    """Elements of one block whose map is affine (the inverse Jacobian is the same at every volume
+    point to ``tol`` relative) for the dense path: (affine uint8[E], coef[E] = sliver scale /
+    |det J|, jinv[E][9], |det J|[E], reference weights [Nq], inverse reference mass [Np][Np]) in
+    the layout of dgb_plan_set_block_affine.  For those elements w_q |det J| = w_q * det and the
+    inverse mass matrix (hybrid/geometry.py:181-192) is coef * inv(B^T diag(w) B)."""
+    J = bp.jinv.reshape(bp.E, bp.Nq, 9)
+    dev = np.abs(J - J[:, :1]).max(axis=(1, 2)) / np.maximum(np.abs(J).max(axis=(1, 2)), 1e-300)
+    affine = (dev <= tol).astype(np.uint8)
+    w = np.asarray(bp.ref.weights, np.float64)
+    det = bp.volume / w.sum()
+    coef = np.minimum(1.0, bp.volume / 1.0e-4) / det
+    mref = np.einsum("q,qi,qj->ij", w, bp.ref.B, bp.ref.B)
+    return affine, coef, np.ascontiguousarray(J.mean(axis=1)), det, w, np.linalg.inv(mref)

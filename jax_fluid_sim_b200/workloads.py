@@ -36,14 +36,15 @@ def vortex_period(mach=0.5, gamma=1.4, length=1.0):
     return length / vortex_velocity(mach, gamma)[0]
 
 
-def vortex_primitive(xyz, t=0.0, beta=5.0, radius=0.08, mach=0.5, gamma=1.4, center=(0.5, 0.5), length=1.0):
+def vortex_primitive(xyz, t=0.0, beta=5.0, radius=0.1, mach=0.5, gamma=1.4, center=(0.5, 0.5), length=1.0):
     """Isentropic vortex of strength beta (axis along z), advected by the free stream of
     ``vortex_velocity`` through the periodic box [0, length]^3; ``radius`` and ``center`` are in
     units of the box side.  u = U - beta/(2 pi) f y', v = V + beta/(2 pi) f x',
     T = 1 - (gamma-1) beta^2 / (8 gamma pi^2) f^2, rho = T^(1/(gamma-1)), p = rho T, with
     f = exp((1 - r^2)/2), (x', y') the nearest-image offsets from the moved centre in units of
-    the radius and r^2 = x'^2 + y'^2.  With radius 0.08 the vortex has f r < 1e-7 at the half-box
-    distance, so the nearest-image field is smooth across the periodic seams to that level."""
+    the radius and r^2 = x'^2 + y'^2.  Radius 0.1 is Shu's vortex (radius 1 in a box of side 10);
+    f r is 3e-5 at the half-box distance, the size of the nearest-image field's kink across the
+    periodic seams."""
     U = vortex_velocity(mach, gamma)
     cx = (center[0] + U[0] * t / length) % 1.0
     cy = (center[1] + U[1] * t / length) % 1.0
@@ -166,7 +167,8 @@ def _timed(fn):
     return out, start.elapsed_time(stop) * 1e-3
 
 
-def run_vortex(n, degree, precisions=("float64",), cfl=0.3, length=10.0, periods=1.0, graph=True, seed=0):
+def run_vortex(n, degree, precisions=("float64",), cfl=0.3, length=10.0, periods=1.0, graph=True, seed=0,
+               radius=0.1):
     """One size of the order study: the vortex through ``periods`` periods on the n^3 hybrid box
     of side ``length``, once per precision from the same start (one host plan).  Each result
     holds the density L2 error (divided by sqrt(box volume)), the step count and the
@@ -174,7 +176,7 @@ def run_vortex(n, degree, precisions=("float64",), cfl=0.3, length=10.0, periods
     captures the step graph)."""
     import torch
     from .time_integration import HybridSSPRK3
-    solver, op64, start = vortex_case(n, degree, seed=seed, length=length)
+    solver, op64, start = vortex_case(n, degree, seed=seed, length=length, radius=radius)
     t_end = periods * vortex_period(length=length)
     steps, dt = equal_steps(t_end, convective_dt(op64, start, cfl))
     out = []
@@ -184,8 +186,10 @@ def run_vortex(n, degree, precisions=("float64",), cfl=0.3, length=10.0, periods
         integ = HybridSSPRK3(op, cfl=cfl, graph=graph)
         first = integ.checked_step_inplace(states, dt).view(torch.int32)[0] != 0     # the graph capture
         ok, seconds = _timed(lambda: advance(integ, states, steps - 1, dt))
-        err = l2_density_error(op, states, lambda x: vortex_primitive(x, t_end, length=length)) / length ** 1.5
-        out.append(dict(n=n, degree=degree, precision=precision, elements={bp.etype: bp.E for bp in op.plan.blocks},
+        err = l2_density_error(op, states, lambda x: vortex_primitive(x, t_end, radius=radius, length=length))
+        err /= length ** 1.5
+        out.append(dict(n=n, degree=degree, precision=precision, cfl=cfl, radius=radius,
+                        elements={bp.etype: bp.E for bp in op.plan.blocks},
                         dofs=dof_count(op), steps=steps, dt=dt, admissible=ok and bool(first.item()),
                         l2_density=err, seconds=seconds, dof_updates_per_s=dof_count(op) * (steps - 1) / seconds))
         del states, integ
@@ -229,6 +233,7 @@ def main(argv=None):
     ap.add_argument("--precision", default="float64,mixed")
     ap.add_argument("--cfl", type=float, default=0.3)
     ap.add_argument("--periods", type=float, default=1.0)
+    ap.add_argument("--radius", type=float, default=0.1)
     ap.add_argument("--n", type=int, default=16)
     ap.add_argument("--degree", type=int, default=2)
     ap.add_argument("--steps", type=int, default=10)
@@ -242,7 +247,7 @@ def main(argv=None):
     for degree in (int(d) for d in args.degrees.split(",")):
         errors = {}
         for n in sizes:
-            for r in run_vortex(n, degree, precisions, args.cfl, periods=args.periods):
+            for r in run_vortex(n, degree, precisions, args.cfl, periods=args.periods, radius=args.radius):
                 prev = errors.get(r["precision"])
                 if prev is not None:
                     r["order"] = float(np.log(prev[1] / r["l2_density"]) / np.log(n / prev[0]))

@@ -121,12 +121,13 @@ def test_mood_recompute_and_step(case):
         close(res[k], g[f"mood_step_{k}"])
 
 
-@pytest.mark.parametrize("case", ["box_p2", "box_p3"])
+@pytest.mark.parametrize("case", ["box_p2", "box_p3", "mixed_p2", "smoke_p1", "smoke_p3", "box_p2:dense"])
 @pytest.mark.parametrize("label", ["smooth", "shocked"])
 def test_mixed_precision_against_reference(case, label):
-    """precision='mixed' (float32 lift and volume arithmetic) against the reference's float64
-    residuals: within 2e-5 of each field's largest magnitude, and one checked step within the
-    1e-6 relative density L2 gate of the float64 step."""
+    """precision='mixed' (float32 trace, lift, volume and finalize arithmetic, on the
+    sum-factorised hexahedron path and on the dense path of hexahedra, prisms and tetrahedra)
+    against the reference's float64 residuals: within 2e-5 of each field's largest magnitude, and
+    one checked step within the 1e-6 relative density L2 gate of the float64 step."""
     from jax_fluid_sim_b200 import HybridPositivityLimiter, HybridSSPRK3
     g, solver, op, bc = setup(case)
     mixed = op.with_precision("mixed")
@@ -141,9 +142,3 @@ def test_mixed_precision_against_reference(case, label):
     num = sum(float(((step[k][..., 0] - plain[k][..., 0]) ** 2).sum()) for k in plain)
     den = sum(float((plain[k][..., 0] ** 2).sum()) for k in plain)
     assert (num / den) ** 0.5 <= 1e-6
-
-
-def test_mixed_precision_needs_the_hex_path():
-    g, solver, op, bc = setup("mixed_p2")
-    with pytest.raises(NotImplementedError):
-        op.with_precision("mixed")

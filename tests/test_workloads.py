@@ -72,3 +72,24 @@ def test_tgv_initial_state():
     div = ((workloads.tgv_primitive(x + e[0])[:, 1] - workloads.tgv_primitive(x - e[0])[:, 1])
            + (workloads.tgv_primitive(x + e[1])[:, 2] - workloads.tgv_primitive(x - e[1])[:, 2])) / (2 * h)
     assert np.max(np.abs(div)) < 1e-8
+
+
+def test_block_affine_data_equals_dense_tables():
+    """Affine elements of the dense path: coef * inv(B^T diag(w) B) equals the per-element
+    sliver-scaled inverse mass matrix, w * det equals w |J| and the constant J^-1 equals every
+    point's, on the jittered hybrid box (tetrahedra and z-prisms are affine there)."""
+    from jax_fluid_sim_b200.plan import block_affine_data
+    plan = Plan(HybridMesh(meshgen.hybrid_box((4, 3, 4), jitter=0.1, seed=1)), 2)
+    seen = 0
+    for bp in plan.blocks:
+        aff, coef, jinv, det, w, mref_inv = block_affine_data(bp)
+        idx = np.flatnonzero(aff)
+        if bp.etype == "tetra":
+            assert len(idx) == bp.E
+        seen += len(idx)
+        for e in idx:
+            np.testing.assert_allclose(coef[e] * mref_inv, bp.minv[e], rtol=1e-11, atol=1e-11 * np.abs(bp.minv[e]).max())
+            np.testing.assert_allclose(w * det[e], bp.wdet[e], rtol=1e-12)
+            np.testing.assert_allclose(np.broadcast_to(jinv[e], (bp.Nq, 9)), bp.jinv[e].reshape(bp.Nq, 9),
+                                       rtol=0, atol=1e-12 * np.abs(jinv[e]).max())
+    assert seen > 0
