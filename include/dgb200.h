@@ -150,6 +150,14 @@ int dgb_plan_set_hex_affine(dgb_plan* plan, const uint8_t* affine, const double*
 int dgb_plan_set_block_affine(dgb_plan* plan, int block, const uint8_t* affine, const double* coef,
                               const double* jinv, const double* det, const double* ref_weights,
                               const double* ref_inv_mass);
+/* Ensembles of independent cases in one plan (the mesh is the disjoint union of the cases'
+ * meshes; no face joins two cases).  cases is [num_cases][3 + nvars]: dynamic viscosity,
+ * thermal conductivity, wall temperature (used where the plan's parameters ask for an
+ * isothermal wall) and the far-field primitive state; element_case[b] gives the case of each
+ * element of block b.  These replace the plan-wide values of dgb_params in the viscous flux,
+ * the boundary ghosts and the stable time step; everything else (gamma, gas constant, BR2
+ * penalty, boundary tags, limiter settings) stays shared.  One dt serves all cases. */
+int dgb_plan_set_cases(dgb_plan* plan, int num_cases, const double* cases, const int32_t* const* element_case);
 int dgb_plan_finalize(dgb_plan* plan);
 int dgb_plan_destroy(dgb_plan* plan);
 /* Replace the physics/boundary/limiter constants of a finalized plan (same mesh and degree);
@@ -161,6 +169,13 @@ int dgb_plan_update_params(dgb_plan* plan, const dgb_params* params);
  * Either output may be NULL (not computed / not written). */
 int dgb_rhs(dgb_plan* plan, const dgb_state* U, const dgb_state* inviscid_out,
             const dgb_state* viscous_out, void* stream);
+/* Autotuner of the dense (any element type) kernels: times the trace, volume and finalize
+ * launches on state U for each block's threads-per-element width in {16, 32, 64, 128} (best of
+ * `reps` runs, one coordinate sweep) and keeps the fastest in the plan.  widths (optional,
+ * [3][DGB_MAX_BLOCKS]) receives the choice per kernel (trace, volume, finalize) and block; all
+ * zeros on the sum-factorised hexahedron path, whose launches are fixed.  Synchronises the
+ * stream. */
+int dgb_plan_autotune(dgb_plan* plan, const dgb_state* U, int reps, int* widths, void* stream);
 
 /* HybridSSPRK3.stable_dt (hybrid/time_integration.py:93-169): writes the clipped dt
  * to the device double *dt_out. */

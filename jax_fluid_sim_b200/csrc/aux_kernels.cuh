@@ -294,7 +294,8 @@ __global__ void __launch_bounds__(kThreads) k_rate(const DevPlan P, const StateP
     double rate = en ? NAN : df * smax / h;
     if (P.viscous) {
       const double rmin = fmax(rsum / B.Np, 0.1);
-      const double diff = fmax((4.0 / 3.0) * P.ph.mu / rmin, P.ph.kappa / (rmin * cp));
+      const CaseView cv = case_view(P.ph, B.ecase, e);
+      const double diff = fmax((4.0 / 3.0) * cv.mu / rmin, cv.kappa / (rmin * cp));
       const double vl = fmax(h, 0.01);
       rate = rate + 2.0 * P.ph.br2 * df * df * diff / (vl * vl);
     }

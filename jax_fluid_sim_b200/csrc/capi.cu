@@ -70,6 +70,7 @@ struct dgb_plan {
   int npartials = 0;
   double* dt_scratch = nullptr;
   // batched launches of the dense element kernels (all blocks in one grid) and their shared memory
+  int num_cases = 0;   // dgb_plan_set_cases
   ElemLaunch launch_tr, launch_vol, launch_fin, launch_tr64;
   size_t smem_tr = 0, smem_vol = 0, smem_fin = 0, smem_tr64 = 0;
   size_t smem_pos[DGB_MAX_BLOCKS], smem_troubled[DGB_MAX_BLOCKS];
@@ -171,18 +172,23 @@ void dense_slots(const dgb_plan* p, ElemLaunch& L, DenseKind kind, size_t rs) {
 }
 
 // Fills the launch (block offsets, widths, slots) and returns its dynamic shared memory.
-size_t dense_smem(const dgb_plan* p, ElemLaunch& L, DenseKind kind, size_t rs) {
+// Lays the launch out for the widths in L.W (block offsets, slots) and returns its dynamic
+// shared memory.
+size_t dense_layout(const dgb_plan* p, ElemLaunch& L, DenseKind kind, size_t rs) {
   L.nblocks = p->dev.nblocks;
   L.cta0[0] = 0;
-  for (int b = 0; b < p->dev.nblocks; ++b) {
-    L.W[b] = dense_width(p, p->dev.blk[b]);
+  for (int b = 0; b < p->dev.nblocks; ++b)
     L.cta0[b + 1] = L.cta0[b] + blocks_for(p->dev.blk[b].E, kThreads / L.W[b]);
-  }
   dense_slots(p, L, kind, rs);
   size_t most = 0;
   for (int b = 0; b < p->dev.nblocks; ++b)
     most = std::max(most, (size_t)(kThreads / L.W[b]) * (size_t)L.slot[b]);
   return most;
+}
+
+size_t dense_smem(const dgb_plan* p, ElemLaunch& L, DenseKind kind, size_t rs) {
+  for (int b = 0; b < p->dev.nblocks; ++b) L.W[b] = dense_width(p, p->dev.blk[b]);
+  return dense_layout(p, L, kind, rs);
 }
 
 // ------------------------------------------------------------------ RHS pipeline
@@ -258,6 +264,77 @@ int run_rhs_dense(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaSt
   k_finalize<NV, R><<<p->launch_fin.cta0[P.nblocks], kThreads, p->smem_fin, st>>>(P, S, p->launch_fin, A);
   if (ev) CK(cudaEventRecord(ev[6], st));
   CK(cudaGetLastError());
+  return DGB_OK;
+}
+
+// Autotuner of the dense element kernels: for each kernel and block, the threads per element W
+// in {16, 32, 64, 128} that gives the shortest launch (best of `reps` CUDA-event timings with
+// the other blocks' widths fixed, one coordinate sweep), on the plan's own buffers filled by one
+// right-hand-side evaluation of U.  The choice is kept in the plan's launches.
+template <int NV, typename R>
+int autotune_dense(dgb_plan* p, const StatePtrs& S, int reps, cudaStream_t st, int* widths) {
+  const DevPlan& P = p->dev;
+  FinalizeArgs A;
+  memset(&A, 0, sizeof(A));
+  int rc;
+  if ((rc = run_rhs_dense<NV, R>(p, S, A, st, nullptr))) return rc;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const size_t rs = sizeof(R);
+  ElemLaunch* launches[3] = {&p->launch_tr, &p->launch_vol, &p->launch_fin};
+  size_t* smems[3] = {&p->smem_tr, &p->smem_vol, &p->smem_fin};
+  const DenseKind kinds[3] = {traces_kind, volume_kind, finalize_kind};
+  auto launch = [&](int k, const ElemLaunch& L, size_t sm) -> int {
+    int r;
+    if (k == 0) {
+      if ((r = prepare(k_traces<NV, R>, sm))) return r;
+      k_traces<NV, R><<<L.cta0[P.nblocks], kThreads, sm, st>>>(P, S, L);
+    } else if (k == 1) {
+      if ((r = prepare(k_volume<NV, R>, sm))) return r;
+      k_volume<NV, R><<<L.cta0[P.nblocks], kThreads, sm, st>>>(P, S, L);
+    } else {
+      if ((r = prepare(k_finalize<NV, R>, sm))) return r;
+      k_finalize<NV, R><<<L.cta0[P.nblocks], kThreads, sm, st>>>(P, S, L, A);
+    }
+    CK(cudaGetLastError());
+    return DGB_OK;
+  };
+  for (int k = 0; k < 3; ++k) {
+    for (int b = 0; b < P.nblocks; ++b) {
+      ElemLaunch best = *launches[k];
+      size_t best_sm = *smems[k];
+      float best_ms = 3.4e38f;
+      for (int W = 16; W <= kThreads; W *= 2) {
+        ElemLaunch L = best;
+        L.W[b] = W;
+        const size_t sm = dense_layout(p, L, kinds[k], rs);
+        if (sm > 227 * 1024) continue;
+        float t = 3.4e38f;
+        for (int r = 0; r < reps; ++r) {
+          CK(cudaEventRecord(e0, st));
+          if ((rc = launch(k, L, sm))) return rc;
+          CK(cudaEventRecord(e1, st));
+          CK(cudaEventSynchronize(e1));
+          float ms = 0.0f;
+          CK(cudaEventElapsedTime(&ms, e0, e1));
+          t = std::min(t, ms);
+        }
+        if (t < best_ms) {
+          best_ms = t;
+          best = L;
+          best_sm = sm;
+        }
+      }
+      *launches[k] = best;
+      *smems[k] = best_sm;
+    }
+    if (widths)
+      for (int b = 0; b < DGB_MAX_BLOCKS; ++b) widths[k * DGB_MAX_BLOCKS + b] = b < P.nblocks ? launches[k]->W[b] : 0;
+  }
+  CK(cudaEventDestroy(e0));
+  CK(cudaEventDestroy(e1));
+  ++p->generation;
   return DGB_OK;
 }
 
@@ -788,6 +865,31 @@ int dgb_plan_set_block_affine(dgb_plan* p, int b, const uint8_t* affine, const d
   return DGB_OK;
 }
 
+int dgb_plan_set_cases(dgb_plan* p, int num_cases, const double* cases, const int32_t* const* element_case) {
+  if (!p || num_cases < 1 || !cases || !element_case) return fail(DGB_ERR_ARGUMENT, "bad case argument");
+  const int stride = 3 + p->dev.nv;
+  for (int b = 0; b < p->dev.nblocks; ++b) {
+    if (!p->block_set[b]) return fail(DGB_ERR_ARGUMENT, "call dgb_plan_set_block first");
+    if (!element_case[b] && p->dev.blk[b].E > 0) return fail(DGB_ERR_ARGUMENT, "null element case array");
+    for (int e = 0; e < p->dev.blk[b].E; ++e)
+      if (element_case[b][e] < 0 || element_case[b][e] >= num_cases)
+        return fail(DGB_ERR_ARGUMENT, "element case id out of range");
+  }
+  for (int c = 0; c < num_cases; ++c)
+    if (!(cases[(size_t)c * stride] >= 0.0) || !(cases[(size_t)c * stride + 1] >= 0.0))
+      return fail(DGB_ERR_ARGUMENT, "case viscosity and conductivity must be >= 0");
+  int rc;
+  const double* table = nullptr;
+  if ((rc = upload(p, cases, (size_t)num_cases * stride, &table))) return rc;
+  for (int b = 0; b < p->dev.nblocks; ++b)
+    if ((rc = upload(p, element_case[b], (size_t)p->dev.blk[b].E, &p->dev.blk[b].ecase))) return rc;
+  p->dev.ph.cases = table;
+  p->dev.ph.case_stride = stride;
+  p->num_cases = num_cases;
+  ++p->generation;
+  return DGB_OK;
+}
+
 int dgb_plan_finalize(dgb_plan* p) {
   if (!p) return fail(DGB_ERR_ARGUMENT, "null plan");
   const int NV = p->dev.nv;
@@ -877,6 +979,24 @@ int dgb_rhs(dgb_plan* p, const dgb_state* U, const dgb_state* inv_out, const dgb
   const StatePtrs S = to_ptrs(U);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   return p->dev.nv == 5 ? run_rhs<5>(p, S, A, st) : run_rhs<16>(p, S, A, st);
+}
+
+int dgb_plan_autotune(dgb_plan* p, const dgb_state* U, int reps, int* widths, void* stream) {
+  int rc;
+  if ((rc = check_ready(p)) || (rc = check_state(p, U, "U"))) return rc;
+  if (reps < 1) return fail(DGB_ERR_ARGUMENT, "reps must be >= 1");
+  if (p->hex) {   // the sum-factorised kernels have fixed per-degree launches
+    if (widths)
+      for (int k = 0; k < 3 * DGB_MAX_BLOCKS; ++k) widths[k] = 0;
+    return DGB_OK;
+  }
+  const StatePtrs S = to_ptrs(U);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (p->prm.precision == 1)
+    return p->dev.nv == 5 ? autotune_dense<5, float>(p, S, reps, st, widths)
+                          : autotune_dense<16, float>(p, S, reps, st, widths);
+  return p->dev.nv == 5 ? autotune_dense<5, double>(p, S, reps, st, widths)
+                        : autotune_dense<16, double>(p, S, reps, st, widths);
 }
 
 int dgb_plan_set_subcells(dgb_plan* p, int b, const dgb_subcell_block_desc* d) {

@@ -51,6 +51,7 @@ struct BlockDev {
   const double* adet;     // [E] |det J|
   const double* wref;     // [Nq] reference quadrature weights (dense path)
   const double* mref_inv; // [Np][Np] inverse of the reference mass matrix B^T diag(wref) B (dense path)
+  const int32_t* ecase;   // [E] case of each element (ensembles; null for one case)
 };
 
 struct FaceDev {
@@ -229,7 +230,7 @@ __global__ void __launch_bounds__(kThreads) k_face_flux(const DevPlan P, const S
 #pragma unroll
     for (int v = 0; v < NV; ++v) UR[v] = fd.trA[sn * NV + v];
   } else if (P.ph.has_boundary) {
-    ghost_state<NV>(P.ph, UL, n, fd.tag[f], UR);
+    ghost_state<NV>(P.ph, case_view(P.ph, P.blk[ob].ecase, fd.ol[f]).far, UL, n, fd.tag[f], UR);
   } else {
 #pragma unroll
     for (int v = 0; v < NV; ++v) UR[v] = UL[v];
@@ -264,7 +265,10 @@ __global__ void __launch_bounds__(kThreads) k_face_flux(const DevPlan P, const S
       double Up[NV];
 #pragma unroll
       for (int v = 0; v < NV; ++v) Up[v] = fd.trP[so * NV + v];
-      if (P.ph.has_boundary) viscous_ghost<NV>(P.ph, Up, n, fd.tag[f], vn);
+      if (P.ph.has_boundary) {
+        const CaseView cv = case_view(P.ph, P.blk[ob].ecase, fd.ol[f]);
+        viscous_ghost<NV>(P.ph, cv.far, cv.wall_T, Up, n, fd.tag[f], vn);
+      }
       else viscous_vars<NV>(P.ph, Up, vn);
     }
     double* out = fd.jumpW + ((size_t)f * nq + q) * 12;
@@ -336,6 +340,7 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 4 : 1) k_volume(const DevP
   const double wscale = aff ? B.adet[ee] : 1.0;
   const double* Mi = aff ? B.mref_inv : B.minv + ee * Np * Np;
   const R mscale = (R)(aff ? B.acoef[ee] : 1.0);
+  const CaseView cv = case_view(P.ph, B.ecase, ee);
   const ElemFaces& Fc = faces[g];
   if (live) {
     for (int i = lane; i < Np * NV; i += W) U[i] = (R)(Ug[i] - anchor[g][i % NV]);
@@ -451,7 +456,7 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 4 : 1) k_volume(const DevP
             for (int d = 0; d < 3; ++d) grad[m * 3 + d] += V[i * 4 + m] * gp[d] + bq * lift[i * 12 + m * 3 + d];
         }
         R Fv[3 * NV];
-        viscous_flux<NV>(P.ph, Uq, grad, Fv);
+        viscous_flux<NV>(P.ph, cv.mu, cv.kappa, Uq, grad, Fv);
 #pragma unroll
         for (int r = 0; r < 3; ++r)
 #pragma unroll
@@ -517,19 +522,21 @@ __global__ void __launch_bounds__(kThreads) k_face_visc(const DevPlan P, int ft)
   const double* n = fd.n + ((size_t)f * nq + q) * 3;
   const double w = fd.w[(size_t)f * nq + q];
   const size_t so = ((size_t)f * 2 + 0) * nq + q, sn = ((size_t)f * 2 + 1) * nq + q;
+  // the two sides of a face always belong to one case
+  const CaseView cv = case_view(P.ph, P.blk[fd.ob[f]].ecase, fd.ol[f]);
   double U[NV], g[12], Fo[3 * NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) U[v] = fd.trP[so * NV + v];
 #pragma unroll
   for (int c = 0; c < 12; ++c) g[c] = fd.trG[so * 12 + c] + fd.liftF[so * 12 + c];
-  viscous_flux<NV>(P.ph, U, g, Fo);
+  viscous_flux<NV>(P.ph, cv.mu, cv.kappa, U, g, Fo);
   if (nb >= 0) {
     double Fn[3 * NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) U[v] = fd.trP[sn * NV + v];
 #pragma unroll
     for (int c = 0; c < 12; ++c) g[c] = fd.trG[sn * 12 + c] + fd.liftF[sn * 12 + c];
-    viscous_flux<NV>(P.ph, U, g, Fn);
+    viscous_flux<NV>(P.ph, cv.mu, cv.kappa, U, g, Fn);
 #pragma unroll
     for (int k = 0; k < 3 * NV; ++k) Fo[k] = 0.5 * (Fo[k] + Fn[k]);
   }

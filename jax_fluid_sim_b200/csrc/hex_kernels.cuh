@@ -455,6 +455,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_volume(const DevPlan P_, const
   R* W = smem + L::VO_W;
   const BlockDev& B = P_.blk[b];
   const int e = blockIdx.x;
+  const CaseView cv = case_view(P_.ph, B.ecase, e);
   load_tables<P>(tables, tb);
   const double* Ug = S.b[b] + (size_t)e * N3 * NV;
   __shared__ double anchor_d[NV];
@@ -550,7 +551,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_volume(const DevPlan P_, const
       R grad[12];
 #pragma unroll
       for (int k = 0; k < 12; ++k) grad[k] = gq[k * Q3 + q];
-      viscous_flux<NV>(P_.ph, Uq, grad, Fv);
+      viscous_flux<NV>(P_.ph, cv.mu, cv.kappa, Uq, grad, Fv);
     }
 #pragma unroll
     for (int r = 0; r < 3; ++r)

@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(kThreads) k_mood_faces(const DevPlan P, const 
         dg_at_subface<NV>(S.b[nb] + (size_t)nl * Bn.Np * NV, Cn.bbasis + (size_t)ns * Bn.Np, Bn.Np, UR);
       }
     } else if (P.ph.has_boundary) {
-      ghost_state<NV>(P.ph, UL, n, fd.tag[f], UR);
+      ghost_state<NV>(P.ph, case_view(P.ph, P.blk[ob].ecase, ol).far, UL, n, fd.tag[f], UR);
     } else {
 #pragma unroll
       for (int v = 0; v < NV; ++v) UR[v] = UL[v];
@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(kThreads) k_mood_faces(const DevPlan P, const 
 #pragma unroll
         for (int v = 0; v < NV; ++v) UR[v] = fd.trA[sn * NV + v];
       } else if (P.ph.has_boundary) {
-        ghost_state<NV>(P.ph, UL, n, fd.tag[f], UR);
+        ghost_state<NV>(P.ph, case_view(P.ph, P.blk[ob].ecase, ol).far, UL, n, fd.tag[f], UR);
       } else {
 #pragma unroll
         for (int v = 0; v < NV; ++v) UR[v] = UL[v];

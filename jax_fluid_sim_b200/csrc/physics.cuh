@@ -8,10 +8,11 @@
 //   hllc_wave_speeds/_star  :163-243 (_safe_signed :154-161)
 //   hllc_flux               :245-300 (Rusanov fallback, identical-state shortcut)
 //   viscous_variables       :307-315
-//   viscous_physical_flux   :357-406 (constant mu, kappa; WALE off)
+//   viscous_physical_flux   :357-406 (constant mu, kappa per case; WALE off)
 // and hybrid/boundary.py:54-102 for the ghost states.
 #pragma once
 #include <math.h>
+#include <stdint.h>
 
 #include "../../include/dgb200.h"
 
@@ -29,7 +30,23 @@ struct Physics {
   int slip[DGB_MAX_TAGS], n_slip;
   int has_wall_T;
   double wall_T;
+  // ensembles of independent cases in one plan (optional): per case [mu, kappa, T_wall,
+  // far-field primitive (nvars)], case_stride = 3 + nvars; elements carry their case id
+  const double* cases;
+  int case_stride;
 };
+
+// The transport coefficients, wall temperature and far-field state that apply to one element.
+struct CaseView {
+  double mu, kappa, wall_T;
+  const double* far;
+};
+
+__device__ __forceinline__ CaseView case_view(const Physics& ph, const int32_t* element_case, size_t e) {
+  if (ph.cases == nullptr || element_case == nullptr) return CaseView{ph.mu, ph.kappa, ph.wall_T, ph.farfield_W};
+  const double* c = ph.cases + (size_t)element_case[e] * ph.case_stride;
+  return CaseView{c[0], c[1], c[2], c + 3};
+}
 
 __device__ __forceinline__ bool tag_in(int tag, const int* set, int n) {
   bool hit = false;
@@ -181,7 +198,8 @@ __device__ void hllc(const Physics& ph, const double* UL, const double* UR, cons
 
 // Inviscid ghost state: slip reflection on walls, far-field on inlets, copy elsewhere.
 template <int NV>
-__device__ void ghost_state(const Physics& ph, const double* U, const double* n, int tag, double* G) {
+__device__ void ghost_state(const Physics& ph, const double* far, const double* U, const double* n, int tag,
+                            double* G) {
   double W[NV];
   primitive<NV>(ph, U, W);
   if (tag_in(tag, ph.wall, ph.n_wall)) {
@@ -192,7 +210,7 @@ __device__ void ghost_state(const Physics& ph, const double* U, const double* n,
   }
   if (tag_in(tag, ph.inlet, ph.n_inlet)) {
 #pragma unroll
-    for (int v = 0; v < NV; ++v) W[v] = ph.farfield_W[v];
+    for (int v = 0; v < NV; ++v) W[v] = far[v];
   }
   conserved<NV>(ph, W, G);
 }
@@ -209,13 +227,14 @@ __device__ __forceinline__ void viscous_vars(const Physics& ph, const T* U, T* o
 
 // Ghost [u, v, w, T] for the viscous traces (boundary.py:74-102).
 template <int NV>
-__device__ void viscous_ghost(const Physics& ph, const double* U, const double* n, int tag, double* g) {
+__device__ void viscous_ghost(const Physics& ph, const double* far, double wall_T, const double* U, const double* n,
+                              int tag, double* g) {
   double v[4];
   viscous_vars<NV>(ph, U, v);
   g[0] = v[0]; g[1] = v[1]; g[2] = v[2]; g[3] = v[3];
   if (tag_in(tag, ph.no_slip, ph.n_no_slip)) {
     g[0] = -v[0]; g[1] = -v[1]; g[2] = -v[2];
-    g[3] = ph.has_wall_T ? 2.0 * ph.wall_T - v[3] : v[3];
+    g[3] = ph.has_wall_T ? 2.0 * wall_T - v[3] : v[3];
   }
   if (tag_in(tag, ph.slip, ph.n_slip)) {
     const double un = v[0] * n[0] + v[1] * n[1] + v[2] * n[2];
@@ -226,18 +245,18 @@ __device__ void viscous_ghost(const Physics& ph, const double* U, const double* 
   }
   if (tag_in(tag, ph.inlet, ph.n_inlet)) {
     double Uf[NV];
-    conserved<NV>(ph, ph.farfield_W, Uf);
+    conserved<NV>(ph, far, Uf);
     viscous_vars<NV>(ph, Uf, g);
   }
 }
 
 // Cartesian viscous flux F[d][v]; grad[m][d] = d(u,v,w,T)_m / dx_d.
 template <int NV, typename T>
-__device__ void viscous_flux(const Physics& ph, const T* U, const T* grad, T* F) {
+__device__ void viscous_flux(const Physics& ph, double mu_, double kappa, const T* U, const T* grad, T* F) {
   T W[NV];
   primitive<NV>(ph, U, W);
   const T div = grad[0 * 3 + 0] + grad[1 * 3 + 1] + grad[2 * 3 + 2];
-  const T mu = T(ph.mu), two_thirds = T(2.0 / 3.0);
+  const T mu = T(mu_), two_thirds = T(2.0 / 3.0);
   T stress[3][3];
 #pragma unroll
   for (int i = 0; i < 3; ++i)
@@ -250,7 +269,7 @@ __device__ void viscous_flux(const Physics& ph, const T* U, const T* grad, T* F)
     F[d * NV + 1] = stress[0][d];
     F[d * NV + 2] = stress[1][d];
     F[d * NV + 3] = stress[2][d];
-    F[d * NV + 4] = W[1] * stress[0][d] + W[2] * stress[1][d] + W[3] * stress[2][d] + T(ph.kappa) * grad[3 * 3 + d];
+    F[d * NV + 4] = W[1] * stress[0][d] + W[2] * stress[1][d] + W[3] * stress[2][d] + T(kappa) * grad[3 * 3 + d];
 #pragma unroll
     for (int v = 5; v < NV; ++v) F[d * NV + v] = T(0);
   }

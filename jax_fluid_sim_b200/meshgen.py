@@ -393,6 +393,70 @@ def sphere_oh_grid(radius=0.5, box=((-4.0, 12.0), (-6.0, 6.0), (-6.0, 6.0)), cub
     return MeshSource(points, vol + bcells, [np.ones(len(hexes), np.int32)] + bphys, field)
 
 
+def cylinder_o_grid(n_theta=96, n_radial=48, radius=0.5, outer_radius=15.0, span=1.0, growth=None):
+    """Extruded O-grid around a cylinder of the given radius (axis z), one element deep.
+
+    n_theta cells around, n_radial cells out to ``outer_radius`` with radii in geometric
+    progression (ratio ``growth``, by default the one that keeps the wall cells square).
+    Tags: cylinder_wall (no-slip body), inlet (outer faces whose centre has x < 0: far-field
+    state), outlet (outer faces with x >= 0: copy), symmetry (the two span planes, slip).  With
+    one element in the span a z-periodic pair of planes would make every side face's vertex set
+    degenerate for the reference's vertex-key face pairing (hybrid/mesh.py:391-405); slip planes
+    give the same residual for the span-invariant flow (w = 0, no z-gradients).
+    """
+    if growth is None:
+        growth = (outer_radius / radius) ** (1.0 / n_radial)
+    r = radius * growth ** np.arange(n_radial + 1)
+    r = radius + (r - radius) * (outer_radius - radius) / (r[-1] - radius)
+    th = 2.0 * np.pi * np.arange(n_theta) / n_theta
+    K, J, I = (a.ravel() for a in np.indices((2, n_radial + 1, n_theta)))
+    points = np.stack([r[J] * np.cos(th[I]), r[J] * np.sin(th[I]), span * K], axis=1)
+
+    def pid(i, j, k):
+        return (k * (n_radial + 1) + j) * n_theta + (i % n_theta)
+
+    i, j = (a.ravel() for a in np.meshgrid(np.arange(n_theta), np.arange(n_radial), indexing="ij"))
+    # counter-clockwise about +z: (i, j) -> (i, j+1) -> (i+1, j+1) -> (i+1, j)
+    bottom = [pid(i, j, 0), pid(i, j + 1, 0), pid(i + 1, j + 1, 0), pid(i + 1, j, 0)]
+    hexes = np.stack(bottom + [b + n_theta * (n_radial + 1) for b in bottom], axis=1).astype(np.int32)
+    it = np.arange(n_theta)
+    wall = np.stack([pid(it, 0, 0), pid(it + 1, 0, 0), pid(it + 1, 0, 1), pid(it, 0, 1)], axis=1)
+    outer = np.stack([pid(it, n_radial, 0), pid(it, n_radial, 1), pid(it + 1, n_radial, 1),
+                      pid(it + 1, n_radial, 0)], axis=1)
+    ends = np.concatenate([hexes[:, :4], hexes[:, 4:]])
+    xc = points[outer].mean(axis=1)[:, 0]
+    field = {"fluid": (1, 3), "inlet": (10, 2), "outlet": (11, 2), "symmetry": (12, 2), "cylinder_wall": (13, 2)}
+    quads = np.concatenate([wall, outer, ends]).astype(np.int32)
+    tags = np.concatenate([np.full(n_theta, 13), np.where(xc < 0.0, 10, 11), np.full(len(ends), 12)]).astype(np.int32)
+    return MeshSource(points, [("hexahedron", hexes), ("quad", quads)], [np.ones(len(hexes), np.int32), tags], field)
+
+
+def union(sources):
+    """Disjoint union of meshes with the same physical names: (MeshSource, counts) where
+    counts[c][type] is the number of volume cells of each type that case c contributes; within
+    each volume type the union lists case 0's cells first, then case 1's, and so on."""
+    points, pmaps, offset = [], [], 0
+    by_type, phys_by_type, counts = {}, {}, []
+    field = dict(sources[0].field_data)
+    for src in sources:
+        if dict(src.field_data) != field:
+            raise ValueError("union needs the same physical names and tags in every mesh")
+        points.append(src.points)
+        pmaps.append((np.arange(len(src.points)) if src.periodic_map is None else np.asarray(src.periodic_map))
+                     + offset)
+        count = {}
+        for (ctype, conn), phys in zip(src.cells, src.physical):
+            by_type.setdefault(ctype, []).append(np.asarray(conn) + offset)
+            phys_by_type.setdefault(ctype, []).append(np.asarray(phys))
+            count[ctype] = count.get(ctype, 0) + len(conn)
+        counts.append(count)
+        offset += len(src.points)
+    cells = [(t, np.concatenate(c).astype(np.int32)) for t, c in by_type.items()]
+    phys = [np.concatenate(phys_by_type[t]).astype(np.int32) for t in by_type]
+    periodic = any(s.periodic_map is not None for s in sources)
+    return MeshSource(np.concatenate(points), cells, phys, field, np.concatenate(pmaps) if periodic else None), counts
+
+
 def _boundary_cells_fast(volume_cells, points, tagger):
     """Vectorised unpaired-face search for large hex meshes (same result as _boundary_cells)."""
     ctype, conn = volume_cells[0]

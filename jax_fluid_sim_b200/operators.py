@@ -268,6 +268,23 @@ class HybridEulerOperator:
         inv, _ = self._run_rhs(states, boundary_state, True, False)
         return inv
 
+    def autotune(self, states, boundary_state=None, reps=3):
+        """Pick the threads-per-element width of the dense kernels by timing them on ``states``
+        (dgb_plan_autotune); returns {kernel: {element_type: width}} (empty on the
+        sum-factorised hexahedron path, whose launches are fixed)."""
+        U = self.to_device(states)
+        self.native.set_boundary(boundary_state)
+        widths = np.zeros(3 * N.MAX_BLOCKS, np.int32)
+        N.check(N.lib().dgb_plan_autotune(self.native.handle, ctypes.byref(self.native.state(self._blocks(U))),
+                                          int(reps), N.dptr(widths, ctypes.c_int32), _stream_ptr()))
+        out = {}
+        for k, kernel in enumerate(("traces", "volume", "finalize")):
+            row = {name: int(widths[k * N.MAX_BLOCKS + b]) for b, name in enumerate(self.names)
+                   if widths[k * N.MAX_BLOCKS + b]}
+            if row:
+                out[kernel] = row
+        return out
+
 
 class HybridNavierStokesOperator(HybridEulerOperator):
     """BR2 viscous operator on top of the Euler residual (hybrid/navier_stokes.py:9-352)."""

@@ -183,6 +183,7 @@ def run_vortex(n, degree, precisions=("float64",), cfl=0.3, length=10.0, periods
     for precision in precisions:
         op = op64 if precision == "float64" else op64.with_precision(precision)
         states = {k: v.clone() for k, v in start.items()}
+        widths = op.autotune(states)
         integ = HybridSSPRK3(op, cfl=cfl, graph=graph)
         first = integ.checked_step_inplace(states, dt).view(torch.int32)[0] != 0     # the graph capture
         ok, seconds = _timed(lambda: advance(integ, states, steps - 1, dt))
@@ -191,7 +192,8 @@ def run_vortex(n, degree, precisions=("float64",), cfl=0.3, length=10.0, periods
         out.append(dict(n=n, degree=degree, precision=precision, cfl=cfl, radius=radius,
                         elements={bp.etype: bp.E for bp in op.plan.blocks},
                         dofs=dof_count(op), steps=steps, dt=dt, admissible=ok and bool(first.item()),
-                        l2_density=err, seconds=seconds, dof_updates_per_s=dof_count(op) * (steps - 1) / seconds))
+                        l2_density=err, seconds=seconds, dof_updates_per_s=dof_count(op) * (steps - 1) / seconds,
+                        widths=widths))
         del states, integ
     return out
 
@@ -222,12 +224,16 @@ def run_tgv(n=16, degree=2, steps=10, cfl=0.3, precision="float64", graph=False)
 
 def main(argv=None):
     """python -m jax_fluid_sim_b200.workloads vortex [--sizes 8,16,32] [--degrees 1,2,3]
-    [--precision float64,mixed] | tgv [--n 16] [--degree 2] [--steps 10]: one JSON line per run,
-    and for the vortex the observed orders between consecutive sizes."""
+    [--precision float64,mixed] | tgv [--n 16] [--degree 2] [--steps 10] | reacting [--scale full]
+    [--degree 2] [--steps 10] | ensemble [--cases 64] [--elements 5000,60000] [--steps 10]: one
+    JSON line per run, and for the vortex the observed orders between consecutive sizes."""
     import argparse
     import json
     ap = argparse.ArgumentParser(prog="python -m jax_fluid_sim_b200.workloads")
-    ap.add_argument("case", choices=["vortex", "tgv"])
+    ap.add_argument("case", choices=["vortex", "tgv", "reacting", "ensemble"])
+    ap.add_argument("--cases", type=int, default=64)
+    ap.add_argument("--elements", default="5000,60000")
+    ap.add_argument("--scale", default="full")
     ap.add_argument("--sizes", default="8,16,32")
     ap.add_argument("--degrees", default="1,2,3")
     ap.add_argument("--precision", default="float64,mixed")
@@ -239,6 +245,17 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=10)
     args = ap.parse_args(argv)
     precisions = args.precision.split(",")
+    if args.case == "ensemble":
+        lo, hi = (float(x) for x in args.elements.split(","))
+        groups, total = run_ensemble(args.cases, (lo, hi), args.steps, precision=precisions[0], cfl=args.cfl)
+        for g in groups:
+            print(json.dumps(g), flush=True)
+        print(json.dumps(total), flush=True)
+        return
+    if args.case == "reacting":
+        for r in run_reacting(args.scale, args.degree, args.steps, precisions=precisions, cfl=args.cfl):
+            print(json.dumps(r), flush=True)
+        return
     if args.case == "tgv":
         for prec in precisions:
             print(json.dumps(run_tgv(args.n, args.degree, args.steps, args.cfl, prec)), flush=True)
@@ -257,3 +274,208 @@ def main(argv=None):
 
 if __name__ == "__main__":
     main()
+
+
+# --------------------------------------------------------------------------- reacting sphere
+REACTING_MACH, REACTING_T_INF, REACTING_P_INF, REACTING_T_WALL = 8.0, 220.0, 500.0, 300.0
+AIR_MASS_FRACTIONS = {"N2": 0.767, "O2": 0.233}
+
+
+def reacting_farfield(mach=REACTING_MACH, gamma=1.4):
+    """Free stream [rho, u, v, w, p, Y(e-, N+, O+, NO+, N2+, O2+, N, O, NO, N2, O2)] in the
+    reference driver's units (rho = p = 1, gas constant 1, u = M sqrt(gamma);
+    run_hybrid_sphere.py:79-91,107-108)."""
+    W = np.zeros(16)
+    W[0], W[1], W[4] = 1.0, mach * np.sqrt(gamma), 1.0
+    W[5 + 9], W[5 + 10] = AIR_MASS_FRACTIONS["N2"], AIR_MASS_FRACTIONS["O2"]
+    return W
+
+
+def reacting_mesh(scale="full"):
+    """O/H sphere grids of radius 0.5 (0.1 m): "full" about 150k hexahedra."""
+    if scale == "full":
+        return meshgen.sphere_oh_grid(n=22, n_radial=18, outer=((7, 28), (10, 10), (10, 10)))
+    if scale == "small":
+        return meshgen.sphere_oh_grid(n=8, n_radial=6, outer=((3, 10), (4, 4), (4, 4)))
+    return meshgen.sphere_oh_grid(n=4, n_radial=2, outer=((1, 3), (1, 1), (1, 1)))
+
+
+def reacting_case(scale="full", degree=2, reynolds=2.6e5, precision="float64", mach=REACTING_MACH, gamma=1.4):
+    """Mach-8 viscous flow past the sphere with the 11 Air-11 species carried as conserved
+    variables: solver, Navier-Stokes operator, boundary (isothermal 300 K wall), coupler and the
+    shocked start (the normal-shock state in the elements whose centroid lies inside r < 0.65,
+    the free stream elsewhere; species at the free-stream fractions).  Re_D = 2.6e5 is the
+    Reynolds number of 500 Pa, 220 K air past a 0.2 m sphere at Mach 8; the coupler's length
+    unit is 0.2 m (the grid's sphere diameter is 1)."""
+    from .air11 import AIR11_SPECIES
+    from .boundary import FarfieldWallBoundary
+    from .chemistry import ReactingFlowCoupler
+    from .mesh import HybridMesh
+    from .operators import HybridNavierStokesOperator
+    from .solver import HybridCompressibleSolver
+    far = reacting_farfield(mach, gamma)
+    mu = far[1] / reynolds
+    solver = HybridCompressibleSolver(HybridMesh(reacting_mesh(scale)), species_names=tuple(s.name for s in AIR11_SPECIES),
+                                      gamma=gamma, polynomial_degree=degree, dynamic_viscosity=mu)
+    op = HybridNavierStokesOperator(solver, precision=precision)
+    bc = FarfieldWallBoundary(solver, far, wall_temperature=REACTING_T_WALL / REACTING_T_INF)
+    coupler = ReactingFlowCoupler(dimensionless=True, reference_temperature=REACTING_T_INF,
+                                  reference_pressure=REACTING_P_INF, reference_length=0.2, gamma=gamma)
+    rho2 = (gamma + 1) * mach ** 2 / ((gamma - 1) * mach ** 2 + 2)
+    p2 = 1 + 2 * gamma / (gamma + 1) * (mach ** 2 - 1)
+
+    def prim(xyz):
+        inside = np.broadcast_to(np.linalg.norm(xyz.mean(axis=1), axis=-1)[:, None] < 0.65, xyz.shape[:-1])
+        W = np.broadcast_to(far, xyz.shape[:-1] + (16,)).copy()
+        W[..., 0] = np.where(inside, rho2, 1.0)
+        W[..., 1] = np.where(inside, far[1] / rho2, far[1])
+        W[..., 4] = np.where(inside, p2, 1.0)
+        return W
+
+    return solver, op, bc, coupler, solver.state_blocks_from_primitive_function(op, prim)
+
+
+def species_closure(states):
+    """max over nodes of |sum_s rho_s - rho| / rho: the species densities' sum against the mixture
+    density (both conserved; the flux and the coupler keep them equal to round-off)."""
+    worst = 0.0
+    for U in states.values():
+        rho = U[..., 0]
+        worst = max(worst, float(((U[..., 5:].sum(-1) - rho).abs() / rho).max()))
+    return worst
+
+
+def run_reacting(scale="full", degree=2, steps=10, warmup=3, precisions=("float64", "mixed"), cfl=0.3):
+    """The reacting-sphere configuration: each step is one checked SSP-RK3 step with the MOOD
+    limiter (replayed as a CUDA graph) followed by the operator-split Air-11 source on every
+    block (run_hybrid_sphere.py:292-312).  From the shocked start, ``warmup`` steps, then
+    ``steps`` timed steps per precision from the same state and dt; returns DOF-updates/s,
+    the flow and chemistry shares, the species closure and the density L2 difference of each
+    run to the float64 run."""
+    import torch
+    from .limiter import HybridMOODSubcellLimiter, HybridPositivityLimiter
+    from .time_integration import HybridSSPRK3
+    solver, op64, bc, coupler, start = reacting_case(scale, degree)
+
+    def integrator(op):
+        lim = HybridMOODSubcellLimiter(op, positivity=HybridPositivityLimiter(op))
+        return HybridSSPRK3(op, cfl=cfl, limiter=lim, graph=True)
+
+    integ = integrator(op64)
+    dt = integ.stable_dt(start, bc)
+    for _ in range(warmup):
+        integ.checked_step_inplace(start, dt, bc)
+        for k in start:
+            coupler.react_block(start[k], dt, out=start[k])
+    torch.cuda.synchronize()
+    out, plain = [], None
+    for precision in precisions:
+        op = op64 if precision == "float64" else op64.with_precision(precision)
+        it = integ if precision == "float64" else integrator(op)
+        U = {k: v.clone() for k, v in start.items()}
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * steps + 1)]
+        ok = torch.ones((), dtype=torch.bool, device="cuda")
+        torch.cuda.synchronize()
+        ev[0].record()
+        for s in range(steps):
+            ok &= it.checked_step_inplace(U, dt, bc).view(torch.int32)[0] != 0
+            ev[2 * s + 1].record()
+            for k in U:
+                coupler.react_block(U[k], dt, out=U[k])
+            ev[2 * s + 2].record()
+        torch.cuda.synchronize()
+        total = ev[0].elapsed_time(ev[-1]) * 1e-3
+        chem = sum(ev[2 * s + 1].elapsed_time(ev[2 * s + 2]) for s in range(steps)) * 1e-3
+        r = dict(precision=precision, elements=sum(bp.E for bp in op.plan.blocks), dofs=dof_count(op), steps=steps,
+                 dt=dt, admissible=bool(ok.item()), seconds=total, chemistry_seconds=chem,
+                 dof_updates_per_s=dof_count(op) * steps / total, species_closure=species_closure(U))
+        if plain is None:
+            plain = U
+        else:
+            num = sum(float(((U[k][..., 0] - plain[k][..., 0]) ** 2).sum()) for k in U)
+            den = sum(float((plain[k][..., 0] ** 2).sum()) for k in U)
+            r["density_l2_vs_float64"] = (num / den) ** 0.5
+        out.append(r)
+    return out
+
+
+# --------------------------------------------------------------------------- cylinder ensembles
+def ensemble_cases(num_cases=64, elements=(5000, 60000), seed=0, degrees=(2, 3)):
+    """Seeded cases of extruded cylinder O-grids: element count uniform in ``elements``
+    (n_theta ~ 3 n_radial), free-stream Mach uniform in [0.3, 4], Re_D log-uniform in
+    [1e2, 1e5], degree drawn from ``degrees``."""
+    rng = np.random.default_rng(seed)
+    E = rng.uniform(*elements, size=num_cases)
+    mach = rng.uniform(0.3, 4.0, num_cases)
+    re = 10.0 ** rng.uniform(2.0, 5.0, num_cases)
+    deg = rng.choice(np.asarray(degrees), num_cases)
+    out = []
+    for c in range(num_cases):
+        n_radial = max(4, int(round(np.sqrt(E[c] / 3.0))))
+        n_theta = max(8, int(round(E[c] / n_radial / 4.0)) * 4)
+        out.append(dict(n_theta=n_theta, n_radial=n_radial, mach=float(mach[c]), reynolds=float(re[c]),
+                        degree=int(deg[c])))
+    return out
+
+
+def _cylinder_case(case, gamma=1.4):
+    far = np.array([1.0, case["mach"] * np.sqrt(gamma), 0.0, 0.0, 1.0])
+    return meshgen.cylinder_o_grid(case["n_theta"], case["n_radial"]), far, far[1] / case["reynolds"]
+
+
+def run_ensemble(num_cases=64, elements=(5000, 60000), steps=10, warmup=2, seed=0, precision="float64", cfl=0.3):
+    """The ensemble configuration: the cases of ``ensemble_cases`` grouped by degree, each group
+    one HybridEnsemble (one launch per kernel per RK stage for all its cases, the step replayed
+    as a CUDA graph), against the same cases solved one after another on their own plans, at the
+    same dt and step count (MOOD limiter, checked SSP-RK3).  Returns per group and in total
+    the DOF-updates/s of both, timed with CUDA events after ``warmup`` untimed steps."""
+    import torch
+    from .ensemble import HybridEnsemble
+    from .limiter import HybridMOODSubcellLimiter, HybridPositivityLimiter
+    from .time_integration import HybridSSPRK3
+    from .boundary import FarfieldWallBoundary
+    from .mesh import HybridMesh
+    from .operators import HybridNavierStokesOperator
+    from .solver import HybridCompressibleSolver
+
+    def integrator(op):
+        return HybridSSPRK3(op, cfl=cfl, limiter=HybridMOODSubcellLimiter(op, positivity=HybridPositivityLimiter(op)),
+                            graph=True)
+
+    def timed_steps(it, U, dt, bc):
+        for _ in range(warmup):
+            it.checked_step_inplace(U, dt, bc)
+        return _timed(lambda: [it.checked_step_inplace(U, dt, bc) for _ in range(steps)])[1]
+
+    cases = ensemble_cases(num_cases, elements, seed)
+    groups, total = [], dict(dofs=0, ensemble_seconds=0.0, sequential_seconds=0.0)
+    for degree in sorted({c["degree"] for c in cases}):
+        members = [c for c in cases if c["degree"] == degree]
+        built = [_cylinder_case(c) for c in members]
+        ens = HybridEnsemble([b[0] for b in built], [b[1] for b in built], [b[2] for b in built],
+                             polynomial_degree=degree, precision=precision)
+        U = ens.freestream_states()
+        it = integrator(ens.operator)
+        dt = it.stable_dt(U, ens.boundary)
+        t_ens = timed_steps(it, U, dt, ens.boundary)
+        t_seq, ok = 0.0, True
+        for src, far, mu in built:
+            solver = HybridCompressibleSolver(HybridMesh(src), polynomial_degree=degree, dynamic_viscosity=mu)
+            op = HybridNavierStokesOperator(solver, precision=precision)
+            bc = FarfieldWallBoundary(solver, far)
+            Uc = solver.uniform_state_blocks(far[0], far[1:4], far[4])
+            t_seq += timed_steps(integrator(op), Uc, dt, bc)
+            del solver, op, Uc
+        dofs = ens.dofs
+        groups.append(dict(degree=degree, cases=len(members), elements=sum(bp.E for bp in ens.operator.plan.blocks),
+                           dofs=dofs, dt=dt, ensemble_dof_updates_per_s=dofs * steps / t_ens,
+                           sequential_dof_updates_per_s=dofs * steps / t_seq, speedup=t_seq / t_ens))
+        total["dofs"] += dofs
+        total["ensemble_seconds"] += t_ens
+        total["sequential_seconds"] += t_seq
+        del ens, U, it
+        torch.cuda.empty_cache()
+    total.update(steps=steps, ensemble_dof_updates_per_s=total["dofs"] * steps / total["ensemble_seconds"],
+                 sequential_dof_updates_per_s=total["dofs"] * steps / total["sequential_seconds"],
+                 speedup=total["sequential_seconds"] / total["ensemble_seconds"])
+    return groups, total

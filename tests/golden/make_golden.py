@@ -63,13 +63,13 @@ def shocked_primitive(xyz, x_shock):
     return W
 
 
-def run_case(name, source, degree, mu, farfield, wall_temperature, x_shock, mood=False, step=True):
+def run_case(name, source, degree, mu, farfield, wall_temperature, x_shock, mood=False, step=True, species=()):
     out = {}
     with tempfile.TemporaryDirectory() as tmp:
         path = os.path.join(tmp, "mesh.msh")
         meshio.write_gmsh22(path, source.points, source.cells, source.physical, source.field_data)
         solver = HybridCompressibleSolver(path, polynomial_degree=degree, dynamic_viscosity=mu,
-                                          gamma=1.4, gas_constant=1.0)
+                                          gamma=1.4, gas_constant=1.0, species_names=tuple(species))
     op = HybridNavierStokesOperator(solver)
     bc = FarfieldWallBoundary(solver, jnp.asarray(farfield), wall_temperature=wall_temperature)
     geo = op.geometry
@@ -149,6 +149,8 @@ def run_case(name, source, degree, mu, farfield, wall_temperature, x_shock, mood
         out["mood_step_rho_min"] = np.asarray(rmin)
         for k in names:
             out[f"mood_step_{k}"] = np.asarray(res[k])
+    if species:
+        out["species"] = np.asarray(species)
     out["degree"] = np.asarray(degree)
     out["mu"] = np.asarray(mu)
     out["farfield"] = np.asarray(farfield, float)

@@ -29,7 +29,7 @@ def build(case):
     src = MeshSource(g["source"].points, g["source"].cells, g["source"].physical, g["source"].field_data,
                      g["source"].periodic_map)
     mesh = Mesh(src)
-    gas = Gas(dynamic_viscosity=float(g["mu"]))
+    gas = Gas(dynamic_viscosity=float(g["mu"]), n_species=len(g["species"]) if "species" in g else 0)
     op = Operator(mesh, gas, int(g["degree"]))
     wt = float(g["wall_temperature"])
     bc = FarfieldWallBoundary(gas, mesh.physical_names, g["farfield"], wall_temperature=None if np.isnan(wt) else wt)
@@ -96,7 +96,7 @@ def test_dt_limiter_sensor_step(case, label):
         assert close(res[k], g[f"step_{label}_{k}"], 1e-9)
 
 
-MOOD_CASES = ["box_p2", "box_p3", "mixed_p2"]
+MOOD_CASES = ["box_p2", "box_p3", "mixed_p2", "species_p2"]
 
 
 @pytest.mark.parametrize("case", MOOD_CASES)

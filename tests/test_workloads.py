@@ -93,3 +93,34 @@ def test_block_affine_data_equals_dense_tables():
             np.testing.assert_allclose(np.broadcast_to(jinv[e], (bp.Nq, 9)), bp.jinv[e].reshape(bp.Nq, 9),
                                        rtol=0, atol=1e-12 * np.abs(jinv[e]).max())
     assert seen > 0
+
+
+def test_cylinder_grid_and_union():
+    """The extruded O-grid is valid (positive Jacobians, tagged boundary faces only on the wall,
+    the outer ring and the span planes); the union keeps every case's cells in case order."""
+    a, b = meshgen.cylinder_o_grid(16, 6), meshgen.cylinder_o_grid(20, 5, outer_radius=8.0)
+    mesh = HybridMesh(a)
+    quads = mesh.face_blocks["quad"]
+    tags = quads.boundary_tags[quads.neighbor_block < 0]
+    names = {v: k for k, v in mesh.physical_names.items()}
+    assert sorted({names[t] for t in tags}) == ["cylinder_wall", "inlet", "outlet", "symmetry"]
+    assert int(np.sum(tags == mesh.physical_names["cylinder_wall"])) == 16
+    assert int(np.sum(tags == mesh.physical_names["symmetry"])) == 2 * 16 * 6
+    plan = Plan(mesh, 1)
+    J = _p1_jacobian("hexahedron", mesh.points[mesh.element_blocks[0].connectivity][:, None],
+                     plan.blocks[0].ref.points[None])
+    assert np.all(np.linalg.det(J) > 0.0)
+    u, counts = meshgen.union([a, b])
+    assert counts == [{"hexahedron": 96, "quad": 16 + 16 + 2 * 96}, {"hexahedron": 100, "quad": 20 + 20 + 2 * 100}]
+    merged = HybridMesh(u)
+    conn = merged.element_blocks[0].connectivity
+    np.testing.assert_array_equal(conn[:96], a.cells[0][1])
+    np.testing.assert_array_equal(conn[96:], b.cells[0][1] + len(a.points))
+
+
+def test_ensemble_cases_are_seeded_and_in_range():
+    c1, c2 = workloads.ensemble_cases(16, seed=3), workloads.ensemble_cases(16, seed=3)
+    assert c1 == c2
+    for c in c1:
+        assert 0.3 <= c["mach"] <= 4.0 and 1e2 <= c["reynolds"] <= 1e5 and c["degree"] in (2, 3)
+        assert 0.6 * 5000 <= c["n_theta"] * c["n_radial"] <= 1.3 * 60000
