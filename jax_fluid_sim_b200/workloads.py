@@ -199,11 +199,16 @@ def run_vortex(n, degree, precisions=("float64",), cfl=0.3, length=10.0, periods
 
 
 def run_tgv(n=16, degree=2, steps=10, cfl=0.3, precision="float64", graph=False):
-    """The Taylor-Green configuration: ``steps`` checked steps at the stable dt of each step."""
+    """The Taylor-Green configuration: ``steps`` checked steps at the stable dt of each step, timed
+    with CUDA events after two untimed steps on a copy of the start."""
     import torch
     from .time_integration import HybridSSPRK3
     solver, op, states = tgv_case(n, degree, precision=precision)
     integ = HybridSSPRK3(op, cfl=cfl, graph=graph)
+    spare = {k: v.clone() for k, v in states.items()}
+    for _ in range(2):                       # untimed: module load and first launches
+        integ.checked_step_inplace(spare, float(integ.stable_dt_device(spare).item()))
+    del spare
 
     def run():
         ok = torch.ones((), dtype=torch.bool, device="cuda")
@@ -271,9 +276,6 @@ def main(argv=None):
                 errors[r["precision"]] = (n, r["l2_density"])
                 print(json.dumps(r), flush=True)
 
-
-if __name__ == "__main__":
-    main()
 
 
 # --------------------------------------------------------------------------- reacting sphere
@@ -479,3 +481,7 @@ def run_ensemble(num_cases=64, elements=(5000, 60000), steps=10, warmup=2, seed=
                  sequential_dof_updates_per_s=total["dofs"] * steps / total["sequential_seconds"],
                  speedup=total["sequential_seconds"] / total["ensemble_seconds"])
     return groups, total
+
+
+if __name__ == "__main__":
+    main()

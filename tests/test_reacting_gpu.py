@@ -5,8 +5,9 @@ with the MOOD limiter, then the operator-split chemistry source with the dimensi
 
 Tolerance: the step to 1e-9 of each field's largest magnitude (float64, different summation
 order); the reacted species to 1e-5 of the node density (the Newton matrix I - dt J is stiff
-here, as in the coupler fixture test); the species densities sum to the mixture density to
-1e-12 relative after the step and after the source."""
+here, as in the coupler fixture test); the species densities sum to the mixture density as
+closely as the oracle's after the step (the CWENO-Z subcell reconstruction is per species) and to
+1e-12 relative after the source, which renormalises them."""
 
 import numpy as np
 import pytest
@@ -42,7 +43,12 @@ def test_reacting_step_against_oracle():
         scale = np.maximum(np.abs(ref[k]).max(axis=(0, 1)), 1e-300)
         err = np.abs(got[k].cpu().numpy() - ref[k]).max(axis=(0, 1)) / scale
         assert err.max() <= 1e-9, err
-    assert workloads.species_closure(got) <= 1e-12
+    # the subcell scheme reconstructs every species with its own CWENO-Z weights, so the sum of
+    # the species densities drifts from the mixture density by the weights' nonlinearity; the
+    # drift must match the oracle's, and the coupler's renormalisation removes it
+    drift = max(float(np.max(np.abs(ref[k][..., 5:].sum(-1) - ref[k][..., 0]) / ref[k][..., 0])) for k in ref)
+    assert drift < 1e-6
+    assert workloads.species_closure(got) <= 2.0 * drift + 1e-13
     oc = Coupler(16, True, 220.0, 500.0, 0.2)
     for k in ref:
         reacted = coupler.react_block(got[k], dt).cpu().numpy()
