@@ -169,6 +169,17 @@ int dgb_plan_update_params(dgb_plan* plan, const dgb_params* params);
  * Either output may be NULL (not computed / not written). */
 int dgb_rhs(dgb_plan* plan, const dgb_state* U, const dgb_state* inviscid_out,
             const dgb_state* viscous_out, void* stream);
+/* Physical coordinates of every face point, [F][nq][3] for one face type (the moment arms of
+ * dgb_wall_forces). */
+int dgb_plan_set_face_points(dgb_plan* plan, int face_type, const double* points);
+/* Surface forces on the boundary faces whose tag is in wall_tags (hybrid/aerodynamics.py:149-250):
+ * evaluates the right-hand side of U (for the face traces, gradients and BR2 lifts; boundary
+ * descriptor as set by dgb_plan_update_params) and writes to the DEVICE array out[12]: pressure
+ * force sum p n dA (3), its moment about moment_center (3), viscous force -sum (tau . n) dA
+ * (3) and its moment (3); n is the face normal out of the fluid.  Deterministic (fixed-order
+ * reductions). */
+int dgb_wall_forces(dgb_plan* plan, const dgb_state* U, const int32_t* wall_tags, int n_wall_tags,
+                    const double* moment_center, double* out, void* stream);
 /* Autotuner of the dense (any element type) kernels: times the trace, volume and finalize
  * launches on state U for each block's threads-per-element width in {16, 32, 64, 128} (best of
  * `reps` runs, one coordinate sweep) and keeps the fastest in the plan.  widths (optional,

@@ -113,6 +113,8 @@ def lib():
             "dgb_plan_finalize": [c_void_p],
             "dgb_plan_set_hex": [c_void_p, P_double, P_int32, c_int, c_int, ctypes.POINTER(ctypes.c_uint8)],
             "dgb_plan_set_hex_affine": [c_void_p, ctypes.POINTER(ctypes.c_uint8), P_double, P_double, P_double],
+            "dgb_plan_set_face_points": [c_void_p, c_int, P_double],
+            "dgb_wall_forces": [c_void_p, ctypes.POINTER(State), P_int32, c_int, P_double, c_void_p, c_void_p],
             "dgb_plan_autotune": [c_void_p, ctypes.POINTER(State), c_int, P_int32, c_void_p],
             "dgb_plan_set_cases": [c_void_p, c_int, P_double, ctypes.POINTER(ctypes.c_void_p)],
             "dgb_plan_set_block_affine": [c_void_p, c_int, ctypes.POINTER(ctypes.c_uint8), P_double, P_double,

@@ -71,6 +71,9 @@ struct dgb_plan {
   double* dt_scratch = nullptr;
   // batched launches of the dense element kernels (all blocks in one grid) and their shared memory
   int num_cases = 0;   // dgb_plan_set_cases
+  const double* face_points[2] = {nullptr, nullptr};   // dgb_plan_set_face_points
+  double* force_partials = nullptr;                    // dgb_wall_forces scratch
+  size_t force_partials_n = 0;
   ElemLaunch launch_tr, launch_vol, launch_fin, launch_tr64;
   size_t smem_tr = 0, smem_vol = 0, smem_fin = 0, smem_tr64 = 0;
   size_t smem_pos[DGB_MAX_BLOCKS], smem_troubled[DGB_MAX_BLOCKS];
@@ -192,6 +195,14 @@ size_t dense_smem(const dgb_plan* p, ElemLaunch& L, DenseKind kind, size_t rs) {
 }
 
 // ------------------------------------------------------------------ RHS pipeline
+template <int NV>
+int launch_face_flux(dgb_plan* p, const StatePtrs& S, int ft, cudaStream_t st) {
+  const FaceDev& F = p->dev.face[ft];
+  if (F.F == 0) return DGB_OK;
+  k_face_flux<NV><<<blocks_for((long)F.F * F.nq, kThreads), kThreads, 0, st>>>(p->dev, S, ft);
+  return DGB_OK;
+}
+
 template <int P, int NV, bool SPLIT, typename R>
 int run_rhs_hex(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStream_t st, cudaEvent_t* ev) {
   using LR = HexSmem<P, NV, R>;
@@ -204,7 +215,7 @@ int run_rhs_hex(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStre
   if ((rc = prepare(k_hex_traces<P, NV, R>, sm_tr))) return rc;
   k_hex_traces<P, NV, R><<<E, kThreads, sm_tr, st>>>(D, S, 0, p->hex_tables, p->hex_codes);
   if (ev) CK(cudaEventRecord(ev[1], st));
-  k_face_flux<NV><<<blocks_for((long)D.face[1].F * D.face[1].nq, kThreads), kThreads, 0, st>>>(D, S, 1);
+  if ((rc = launch_face_flux<NV>(p, S, 1, st))) return rc;
   if (ev) CK(cudaEventRecord(ev[2], st));
   if (D.viscous) {
     if ((rc = prepare(k_hex_lift<P, NV, R>, sm_li))) return rc;
@@ -249,7 +260,7 @@ int run_rhs_dense(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaSt
   if (ev) CK(cudaEventRecord(ev[1], st));
   for (int ft = 0; ft < 2; ++ft)
     if (p->face_present[ft])
-      k_face_flux<NV><<<blocks_for((long)P.face[ft].F * P.face[ft].nq, kThreads), kThreads, 0, st>>>(P, S, ft);
+      if ((rc = launch_face_flux<NV>(p, S, ft, st))) return rc;
   if (ev) CK(cudaEventRecord(ev[2], st));
   if (ev) CK(cudaEventRecord(ev[3], st));     // the dense k_volume does the BR2 lift itself
   if ((rc = prepare(k_volume<NV, R>, p->smem_vol))) return rc;
@@ -752,6 +763,21 @@ int dgb_plan_set_block(dgb_plan* p, int b, const dgb_block_desc* d) {
   int rc;
   if ((rc = upload(p, d->basis, Nq * Np, &B.B))) return rc;
   if ((rc = upload(p, d->basis_grad, Nq * Np * 3, &B.dB))) return rc;
+  if (d->basis && d->basis_grad) {
+    std::vector<double> bt(Nq * Np), dq(Nq * Np * 3), di(Nq * Np * 3);
+    for (size_t q = 0; q < Nq; ++q)
+      for (size_t i = 0; i < Np; ++i) {
+        bt[i * Nq + q] = d->basis[q * Np + i];
+        for (size_t r = 0; r < 3; ++r) {
+          const double g = d->basis_grad[(q * Np + i) * 3 + r];
+          dq[(i * 3 + r) * Nq + q] = g;
+          di[(q * 3 + r) * Np + i] = g;
+        }
+      }
+    if ((rc = upload(p, bt.data(), bt.size(), &B.Bt))) return rc;
+    if ((rc = upload(p, dq.data(), dq.size(), &B.dBq))) return rc;
+    if ((rc = upload(p, di.data(), di.size(), &B.dBi))) return rc;
+  }
   if ((rc = upload(p, d->inv_jacobian, E * Nq * 9, &B.jinv))) return rc;
   if ((rc = upload(p, d->wdet, E * Nq, &B.wdet))) return rc;
   if ((rc = upload(p, d->inv_mass, E * Np * Np, &B.minv))) return rc;
@@ -796,6 +822,17 @@ int dgb_plan_set_trace(dgb_plan* p, int etype, int ftype, int ncodes, int nq, in
     int rc;
     if ((rc = upload(p, B, (size_t)ncodes * nq * np, &blk.trB[ftype]))) return rc;
     if ((rc = upload(p, dB, (size_t)ncodes * nq * np * 3, &blk.trdB[ftype]))) return rc;
+    if (B && dB) {
+      std::vector<double> bt((size_t)ncodes * nq * np), dt((size_t)ncodes * nq * np * 3);
+      for (size_t c = 0; c < (size_t)ncodes; ++c)
+        for (size_t q = 0; q < (size_t)nq; ++q)
+          for (size_t i = 0; i < (size_t)np; ++i) {
+            bt[(c * np + i) * nq + q] = B[(c * nq + q) * np + i];
+            for (size_t r = 0; r < 3; ++r) dt[((c * np + i) * 3 + r) * nq + q] = dB[((c * nq + q) * np + i) * 3 + r];
+          }
+      if ((rc = upload(p, bt.data(), bt.size(), &blk.trBt[ftype]))) return rc;
+      if ((rc = upload(p, dt.data(), dt.size(), &blk.trdBt[ftype]))) return rc;
+    }
     found = 1;
   }
   if (!found) return fail(DGB_ERR_ARGUMENT, "trace table for an element type without a block");
@@ -902,6 +939,7 @@ int dgb_plan_finalize(dgb_plan* p) {
     const size_t n = F.F, nq = F.nq;
     if ((rc = alloc(p, n * 2 * nq * NV, &F.trA))) return rc;
     if ((rc = alloc(p, n * 2 * nq * NV, &F.fluxI))) return rc;
+    if ((rc = alloc(p, n * 2 * NV, &F.anc))) return rc;
     if (p->dev.viscous) {
       F.trP = F.trA;   // the viscous terms take the anchor-form trace (equal to the plain one)
       if ((rc = alloc(p, n * 2 * nq * 4, &F.trV))) return rc;
@@ -997,6 +1035,55 @@ int dgb_plan_autotune(dgb_plan* p, const dgb_state* U, int reps, int* widths, vo
                           : autotune_dense<16, float>(p, S, reps, st, widths);
   return p->dev.nv == 5 ? autotune_dense<5, double>(p, S, reps, st, widths)
                         : autotune_dense<16, double>(p, S, reps, st, widths);
+}
+
+int dgb_plan_set_face_points(dgb_plan* p, int face_type, const double* points) {
+  if (!p || face_type < 0 || face_type > 1 || !points) return fail(DGB_ERR_ARGUMENT, "bad face point argument");
+  if (!p->face_present[face_type]) return fail(DGB_ERR_ARGUMENT, "no faces of that type");
+  const FaceDev& F = p->dev.face[face_type];
+  return upload(p, points, (size_t)F.F * F.nq * 3, &p->face_points[face_type]);
+}
+
+int dgb_wall_forces(dgb_plan* p, const dgb_state* U, const int32_t* wall_tags, int n_wall_tags,
+                    const double* moment_center, double* out, void* stream) {
+  int rc;
+  if ((rc = check_ready(p)) || (rc = check_state(p, U, "U"))) return rc;
+  if (!out || !moment_center || n_wall_tags < 0 || n_wall_tags > DGB_MAX_TAGS || (n_wall_tags && !wall_tags))
+    return fail(DGB_ERR_ARGUMENT, "bad wall-force argument");
+  WallSet walls;
+  walls.n = n_wall_tags;
+  for (int k = 0; k < DGB_MAX_TAGS; ++k) walls.tags[k] = k < n_wall_tags ? wall_tags[k] : -1;
+  for (int d = 0; d < 3; ++d) walls.center[d] = moment_center[d];
+  size_t blocks[2] = {0, 0}, total = 0;
+  for (int ft = 0; ft < 2; ++ft)
+    if (p->face_present[ft]) {
+      if (!p->face_points[ft]) return fail(DGB_ERR_ARGUMENT, "call dgb_plan_set_face_points first");
+      blocks[ft] = (size_t)blocks_for((long)p->dev.face[ft].F * p->dev.face[ft].nq, kThreads);
+      total += blocks[ft];
+    }
+  if (total > p->force_partials_n) {
+    if ((rc = alloc(p, total * kForceValues, &p->force_partials))) return rc;
+    p->force_partials_n = total;
+  }
+  // the face buffers of one right-hand-side evaluation (traces, gradients, BR2 lifts)
+  FinalizeArgs A;
+  memset(&A, 0, sizeof(A));
+  const StatePtrs S = to_ptrs(U);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if ((rc = p->dev.nv == 5 ? run_rhs<5>(p, S, A, st) : run_rhs<16>(p, S, A, st))) return rc;
+  size_t off = 0;
+  for (int ft = 0; ft < 2; ++ft) {
+    if (!blocks[ft]) continue;
+    double* part = p->force_partials + off * kForceValues;
+    if (p->dev.nv == 5)
+      k_wall_forces<5><<<(unsigned)blocks[ft], kThreads, 0, st>>>(p->dev, ft, p->face_points[ft], walls, part);
+    else
+      k_wall_forces<16><<<(unsigned)blocks[ft], kThreads, 0, st>>>(p->dev, ft, p->face_points[ft], walls, part);
+    off += blocks[ft];
+  }
+  k_wall_forces_final<<<1, 32, 0, st>>>(p->force_partials, (int)total, out);
+  CK(cudaGetLastError());
+  return DGB_OK;
 }
 
 int dgb_plan_set_subcells(dgb_plan* p, int b, const dgb_subcell_block_desc* d) {

@@ -41,6 +41,12 @@ struct BlockDev {
   const int32_t* elem_face;  // [E][nlf]
   const double* trB[2];   // per face type: [codes][nq][Np]
   const double* trdB[2];  // per face type: [codes][nq][Np][3]
+  // the same tables laid out so that the thread index runs along the fastest axis (coalesced):
+  const double* Bt;       // [Np][Nq]            (thread per volume point)
+  const double* dBq;      // [Np][3][Nq]         (thread per volume point)
+  const double* dBi;      // [Nq][3][Np]         (thread per node)
+  const double* trBt[2];  // [codes][Np][nq]     (thread per face point)
+  const double* trdBt[2]; // [codes][Np][3][nq]  (thread per face point)
   double* Rinv;           // scratch [E][Np][NV]
   double* Rvis;
   // affine elements (optional): constant metrics; M^-1 = coef * (m1i)^(x)3 on the sum-factorised
@@ -61,6 +67,7 @@ struct FaceDev {
   const double* w;        // [F][nq]
   const double* jinv;     // [F][2][nq][9]
   double* trA;            // [F][2][nq][NV] anchor-form U traces
+  double* anc;            // [F][2][NV] anchor state (node 0) of each side's element
   double* trP;            // [F][2][nq][NV] plain U traces
   double* trV;            // [F][2][nq][4]
   double* trG;            // [F][2][nq][12] raw gradients of the viscous variables
@@ -167,20 +174,23 @@ __global__ void __launch_bounds__(kThreads) k_traces(const DevPlan P, const Stat
     while (q >= Fc.nq[lf]) q -= Fc.nq[lf++];
     const int ft = Fc.ft[lf], nq = Fc.nq[lf];
     const FaceDev& fd = P.face[ft];
-    const double* Bt = B.trB[ft] + ((size_t)Fc.code[lf] * nq + q) * Np;
+    const double* Bt = B.trBt[ft] + (size_t)Fc.code[lf] * Np * nq + q;    // [i][q]: stride nq
     const size_t pt = ((size_t)Fc.f[lf] * 2 + Fc.side[lf]) * nq + q;
     R acc[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) acc[v] = (R)0;
     for (int i = 0; i < Np; ++i) {
-      const R bt = (R)Bt[i];
+      const R bt = (R)Bt[(size_t)i * nq];
 #pragma unroll
       for (int v = 0; v < NV; ++v) acc[v] += bt * U[i * NV + v];
     }
 #pragma unroll
     for (int v = 0; v < NV; ++v) fd.trA[pt * NV + v] = anchor[g][v] + (double)acc[v];
+    if (q == 0)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) fd.anc[((size_t)Fc.f[lf] * 2 + Fc.side[lf]) * NV + v] = anchor[g][v];
     if (P.viscous) {
-      const double* dBt = B.trdB[ft] + ((size_t)Fc.code[lf] * nq + q) * Np * 3;
+      const double* dBt = B.trdBt[ft] + (size_t)Fc.code[lf] * Np * 3 * nq + q;   // [i][r][q]
       R J[9];
 #pragma unroll
       for (int k = 0; k < 9; ++k) J[k] = (R)fd.jinv[pt * 9 + k];
@@ -190,8 +200,9 @@ __global__ void __launch_bounds__(kThreads) k_traces(const DevPlan P, const Stat
 #pragma unroll
       for (int k = 0; k < 12; ++k) tg[k] = (R)0;
       for (int i = 0; i < Np; ++i) {
-        const R bt = (R)Bt[i];
-        const R g0 = (R)dBt[i * 3 + 0], g1 = (R)dBt[i * 3 + 1], g2 = (R)dBt[i * 3 + 2];
+        const R bt = (R)Bt[(size_t)i * nq];
+        const double* gi = dBt + (size_t)i * 3 * nq;
+        const R g0 = (R)gi[0], g1 = (R)gi[nq], g2 = (R)gi[2 * nq];
         R gp[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) gp[d] = g0 * J[0 * 3 + d] + g1 * J[1 * 3 + d] + g2 * J[2 * 3 + d];
@@ -212,14 +223,17 @@ __global__ void __launch_bounds__(kThreads) k_traces(const DevPlan P, const Stat
 }
 
 // ---------------------------------------------------------------------------------------------
+// k_face_flux: one thread per face point.  Every input is independent of the others (traces,
+// normal, weight, and each side's anchor state, which the trace kernels write per face side), so
+// a thread issues all its loads at once instead of chasing face -> element -> state.
 template <int NV>
-__global__ void __launch_bounds__(kThreads) k_face_flux(const DevPlan P, const StatePtrs S, int ft) {
+__global__ void __launch_bounds__(kThreads, NV <= 5 ? 6 : 1) k_face_flux(const DevPlan P, const StatePtrs S, int ft) {
   const FaceDev& fd = P.face[ft];
   const int nq = fd.nq;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= fd.F * nq) return;
   const int f = t / nq, q = t % nq;
-  const int ob = fd.ob[f], nb = fd.nb[f];
+  const int nb = fd.nb[f];
   const double* n = fd.n + ((size_t)f * nq + q) * 3;
   const double w = fd.w[(size_t)f * nq + q];
   const size_t so = ((size_t)f * 2 + 0) * nq + q, sn = ((size_t)f * 2 + 1) * nq + q;
@@ -230,26 +244,24 @@ __global__ void __launch_bounds__(kThreads) k_face_flux(const DevPlan P, const S
 #pragma unroll
     for (int v = 0; v < NV; ++v) UR[v] = fd.trA[sn * NV + v];
   } else if (P.ph.has_boundary) {
-    ghost_state<NV>(P.ph, case_view(P.ph, P.blk[ob].ecase, fd.ol[f]).far, UL, n, fd.tag[f], UR);
+    ghost_state<NV>(P.ph, case_view(P.ph, P.blk[fd.ob[f]].ecase, fd.ol[f]).far, UL, n, fd.tag[f], UR);
   } else {
 #pragma unroll
     for (int v = 0; v < NV; ++v) UR[v] = UL[v];
   }
   hllc<NV>(P.ph, UL, UR, n, Fh);
   {
-    const double* ao = S.b[ob] + (size_t)fd.ol[f] * P.blk[ob].Np * NV;
     double a[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) a[v] = ao[v];
+    for (int v = 0; v < NV; ++v) a[v] = fd.anc[((size_t)f * 2 + 0) * NV + v];
     normal_flux<NV>(P.ph, a, n, Fa);
 #pragma unroll
     for (int v = 0; v < NV; ++v) fd.fluxI[so * NV + v] = (Fh[v] - Fa[v]) * w;
   }
   if (nb >= 0) {
-    const double* an = S.b[nb] + (size_t)fd.nl[f] * P.blk[nb].Np * NV;
     double a[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) a[v] = an[v];
+    for (int v = 0; v < NV; ++v) a[v] = fd.anc[((size_t)f * 2 + 1) * NV + v];
     normal_flux<NV>(P.ph, a, n, Fa);
 #pragma unroll
     for (int v = 0; v < NV; ++v) fd.fluxI[sn * NV + v] = (Fh[v] - Fa[v]) * w;
@@ -261,15 +273,11 @@ __global__ void __launch_bounds__(kThreads) k_face_flux(const DevPlan P, const S
     if (nb >= 0) {
 #pragma unroll
       for (int m = 0; m < 4; ++m) vn[m] = fd.trV[sn * 4 + m];
+    } else if (P.ph.has_boundary) {
+      const CaseView cv = case_view(P.ph, P.blk[fd.ob[f]].ecase, fd.ol[f]);
+      viscous_ghost<NV>(P.ph, cv.far, cv.wall_T, UL, n, fd.tag[f], vn);
     } else {
-      double Up[NV];
-#pragma unroll
-      for (int v = 0; v < NV; ++v) Up[v] = fd.trP[so * NV + v];
-      if (P.ph.has_boundary) {
-        const CaseView cv = case_view(P.ph, P.blk[ob].ecase, fd.ol[f]);
-        viscous_ghost<NV>(P.ph, cv.far, cv.wall_T, Up, n, fd.tag[f], vn);
-      }
-      else viscous_vars<NV>(P.ph, Up, vn);
+      viscous_vars<NV>(P.ph, UL, vn);
     }
     double* out = fd.jumpW + ((size_t)f * nq + q) * 12;
 #pragma unroll
@@ -411,7 +419,7 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 4 : 1) k_volume(const DevP
       normal_flux<NV>(P.ph, a, ez, Fa[2]);
     }
     for (int q = lane; q < Nq; q += W) {
-      const double* Bq = B.B + (size_t)q * Np;
+      const double* Bq = B.Bt + q;                    // [i][q]: stride Nq
       const double* Jd = jinv + q * jstride;
       R J[9];
 #pragma unroll
@@ -421,7 +429,7 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 4 : 1) k_volume(const DevP
 #pragma unroll
       for (int v = 0; v < NV; ++v) Uq[v] = (R)0;
       for (int i = 0; i < Np; ++i) {
-        const R bq = (R)Bq[i];
+        const R bq = (R)Bq[(size_t)i * Nq];
 #pragma unroll
         for (int v = 0; v < NV; ++v) Uq[v] += bq * U[i * NV + v];
       }
@@ -445,8 +453,8 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 4 : 1) k_volume(const DevP
 #pragma unroll
         for (int c = 0; c < 12; ++c) grad[c] = (R)0;
         for (int i = 0; i < Np; ++i) {
-          const double* gd = B.dB + ((size_t)q * Np + i) * 3;
-          const R g0 = (R)gd[0], g1 = (R)gd[1], g2 = (R)gd[2], bq = (R)Bq[i];
+          const double* gd = B.dBq + (size_t)i * 3 * Nq + q;   // [i][r][q]
+          const R g0 = (R)gd[0], g1 = (R)gd[Nq], g2 = (R)gd[2 * Nq], bq = (R)Bq[(size_t)i * Nq];
           R gp[3];
 #pragma unroll
           for (int d = 0; d < 3; ++d) gp[d] = g0 * J[0 * 3 + d] + g1 * J[1 * 3 + d] + g2 * J[2 * 3 + d];
@@ -476,8 +484,8 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 4 : 1) k_volume(const DevP
 #pragma unroll
       for (int v = 0; v < NV; ++v) si[v] = sv[v] = (R)0;
       for (int q = q0; q < q1; ++q) {
-        const double* gd = B.dB + ((size_t)q * Np + i) * 3;
-        const R g0 = (R)gd[0], g1 = (R)gd[1], g2 = (R)gd[2];
+        const double* gd = B.dBi + (size_t)q * 3 * Np + i;     // [q][r][i]
+        const R g0 = (R)gd[0], g1 = (R)gd[Np], g2 = (R)gd[2 * Np];
         const R* G = Gi + q * 3 * NV;
 #pragma unroll
         for (int v = 0; v < NV; ++v) si[v] += g0 * G[v] + g1 * G[NV + v] + g2 * G[2 * NV + v];
@@ -546,6 +554,89 @@ __global__ void __launch_bounds__(kThreads) k_face_visc(const DevPlan P, int ft)
   if (nb < 0 && P.ph.has_boundary && tag_in(fd.tag[f], P.ph.wall, P.ph.n_wall)) out[4] = 0.0;
 #pragma unroll
   for (int v = 0; v < NV; ++v) fd.fluxV[((size_t)f * nq + q) * NV + v] = out[v] * w;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Surface forces on the wall faces (hybrid/aerodynamics.py:149-250), from the face buffers of a
+// right-hand-side evaluation: pressure traction p n dA and viscous traction -(tau . n) dA of the
+// owner side at every face point, and their moments about a centre.  One thread per face point;
+// each CTA reduces its 12 sums in a fixed order into partials[blockIdx.x].
+struct WallSet {
+  int tags[DGB_MAX_TAGS];
+  int n;
+  double center[3];
+};
+
+constexpr int kForceValues = 12;   // F_pressure (3), M_pressure (3), F_viscous (3), M_viscous (3)
+
+template <int NV>
+__global__ void __launch_bounds__(kThreads) k_wall_forces(const DevPlan P, int ft, const double* __restrict__ points,
+                                                         const WallSet walls, double* __restrict__ partials) {
+  __shared__ double red[kForceValues][kThreads];
+  const FaceDev& fd = P.face[ft];
+  const int nq = fd.nq;
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  double c[kForceValues];
+#pragma unroll
+  for (int k = 0; k < kForceValues; ++k) c[k] = 0.0;
+  if (t < (long)fd.F * nq) {
+    const int f = (int)(t / nq), q = (int)(t % nq);
+    if (fd.nb[f] < 0 && tag_in(fd.tag[f], walls.tags, walls.n)) {
+      const size_t so = ((size_t)f * 2 + 0) * nq + q;
+      const double* n = fd.n + ((size_t)f * nq + q) * 3;
+      const double w = fd.w[(size_t)f * nq + q];
+      const double* x = points + ((size_t)f * nq + q) * 3;
+      const double r[3] = {x[0] - walls.center[0], x[1] - walls.center[1], x[2] - walls.center[2]};
+      double U[NV], W[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) U[v] = fd.trA[so * NV + v];
+      primitive<NV>(P.ph, U, W);
+      double F[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) F[d] = W[4] * n[d] * w;
+      c[0] = F[0];
+      c[1] = F[1];
+      c[2] = F[2];
+      c[3] = r[1] * F[2] - r[2] * F[1];
+      c[4] = r[2] * F[0] - r[0] * F[2];
+      c[5] = r[0] * F[1] - r[1] * F[0];
+      if (P.viscous) {
+        double g[12], Fv[3 * NV];
+#pragma unroll
+        for (int k = 0; k < 12; ++k) g[k] = fd.trG[so * 12 + k] + fd.liftF[so * 12 + k];
+        const CaseView cv = case_view(P.ph, P.blk[fd.ob[f]].ecase, fd.ol[f]);
+        viscous_flux<NV>(P.ph, cv.mu, cv.kappa, U, g, Fv);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+          F[i] = -(Fv[0 * NV + 1 + i] * n[0] + Fv[1 * NV + 1 + i] * n[1] + Fv[2 * NV + 1 + i] * n[2]) * w;
+        c[6] = F[0];
+        c[7] = F[1];
+        c[8] = F[2];
+        c[9] = r[1] * F[2] - r[2] * F[1];
+        c[10] = r[2] * F[0] - r[0] * F[2];
+        c[11] = r[0] * F[1] - r[1] * F[0];
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kForceValues; ++k) red[k][threadIdx.x] = c[k];
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s)
+#pragma unroll
+      for (int k = 0; k < kForceValues; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x < kForceValues) partials[(size_t)blockIdx.x * kForceValues + threadIdx.x] = red[threadIdx.x][0];
+}
+
+// Sums the CTAs' partials in order (one thread per component).
+__global__ void k_wall_forces_final(const double* __restrict__ partials, int n, double* __restrict__ out) {
+  const int k = threadIdx.x;
+  if (k >= kForceValues) return;
+  double s = 0.0;
+  for (int i = 0; i < n; ++i) s += partials[(size_t)i * kForceValues + k];
+  out[k] = s;
 }
 
 // ---------------------------------------------------------------------------------------------

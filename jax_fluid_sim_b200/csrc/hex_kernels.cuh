@@ -287,6 +287,9 @@ __global__ void __launch_bounds__(kThreads) k_hex_traces(const DevPlan P_, const
     const int c = codes.perm[fperm[lf] + q];
     fd.trA[((size_t)fslot[lf] + q) * NV + v] = anchor[v] + (double)fo[(lf * NV + v) * QF2 + c];
   }
+  // the anchor state per face side, for the face kernel's anchor flux
+  for (int idx = threadIdx.x; idx < 6 * NV; idx += blockDim.x)
+    fd.anc[(size_t)(fslot[idx / NV] / QF2) * NV + idx % NV] = anchor[idx % NV];
   if (visc) {
     const R* fv = fo + 6 * NV * QF2;          // [6][4][QF2]
     const R* gn = fv + 24 * QF2;              // [6][4][QF2]

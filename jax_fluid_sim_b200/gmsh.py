@@ -1,0 +1,171 @@
+"""Gmsh mesh files (MSH 2.2 and 4.1, ASCII) into a ``MeshSource``.
+
+The reference reads its meshes with meshio (hybrid/mesh.py:182-236, mesh_loader.py).  This
+reader keeps what the hybrid path uses: node coordinates, the physical names and, per cell
+block, the cells and their physical tags.  Element types follow the reference's aliases
+(hybrid/mesh.py:11-20): tetrahedra, wedges and hexahedra of first order, and the serendipity
+hexahedron20 / wedge15, whose corner nodes come first; boundary triangles and quadrilaterals
+(and their second-order forms) keep their corners.  The complete second-order cells tetra10,
+wedge18 and hexahedron27 carry curved geometry, which the reference maps isoparametrically
+(hybrid/geometry.py:104-150) and the CUDA path does not: reading one raises NotImplementedError.
+"""
+
+from pathlib import Path
+
+import numpy as np
+
+from .meshgen import MeshSource
+
+# Gmsh element type -> (cell type name, corner count, total node count)
+_TYPES = {
+    2: ("triangle", 3, 3), 3: ("quad", 4, 4), 4: ("tetra", 4, 4), 5: ("hexahedron", 8, 8), 6: ("wedge", 6, 6),
+    9: ("triangle", 3, 6), 10: ("quad", 4, 9), 16: ("quad", 4, 8), 17: ("hexahedron", 8, 20),
+    18: ("wedge", 6, 15), 1: (None, 2, 2), 8: (None, 2, 3), 15: (None, 1, 1),
+}
+_CURVED = {11: "tetra10", 12: "hexahedron27", 13: "wedge18"}
+_ORDER = ("hexahedron", "wedge", "tetra", "quad", "triangle")
+
+
+def _sections(lines):
+    out, i = {}, 0
+    while i < len(lines):
+        line = lines[i].strip()
+        if line.startswith("$") and not line.startswith("$End"):
+            name = line[1:]
+            j = i + 1
+            while not lines[j].strip().startswith("$End" + name):
+                j += 1
+            out[name] = lines[i + 1:j]
+            i = j
+        i += 1
+    return out
+
+
+def _physical_names(sec):
+    names = {}
+    for line in sec[1:1 + int(sec[0])] if sec else []:
+        parts = line.split(maxsplit=2)
+        names[parts[2].strip().strip('"')] = (int(parts[1]), int(parts[0]))
+    return names
+
+
+def _assemble(points, node_index, records):
+    """records: list of (gmsh type, physical tag, node tags array (n, k))."""
+    grouped = {}
+    for etype, phys, nodes in records:
+        if etype in _CURVED:
+            raise NotImplementedError(f"{_CURVED[etype]} cells carry curved geometry; the CUDA path maps every "
+                                      "element by its corners (straight-sided)")
+        if etype not in _TYPES:
+            raise ValueError(f"unsupported Gmsh element type {etype}")
+        name, corners, _ = _TYPES[etype]
+        if name is None:
+            continue
+        conn = node_index[nodes[:, :corners]]
+        grouped.setdefault(name, ([], []))
+        grouped[name][0].append(conn)
+        grouped[name][1].append(np.broadcast_to(np.asarray(phys, np.int32), (len(conn),)))
+    if not any(t in grouped for t in ("hexahedron", "wedge", "tetra")):
+        raise ValueError("Mesh contains no tetrahedron, wedge, or hexahedron")
+    cells = [(t, np.concatenate(grouped[t][0]).astype(np.int32)) for t in _ORDER if t in grouped]
+    phys = [np.concatenate(grouped[t][1]).astype(np.int32) for t in _ORDER if t in grouped]
+    return cells, phys
+
+
+def _read_v2(sec, field):
+    nodes = np.array([line.split() for line in sec["Nodes"][1:1 + int(sec["Nodes"][0])]], dtype=np.float64)
+    ids = nodes[:, 0].astype(np.int64)
+    index = np.full(ids.max() + 1, -1, np.int64)
+    index[ids] = np.arange(len(ids))
+    by_shape = {}
+    for line in sec["Elements"][1:1 + int(sec["Elements"][0])]:
+        v = [int(x) for x in line.split()]
+        etype, ntags = v[1], v[2]
+        phys = v[3] if ntags > 0 else 0
+        by_shape.setdefault((etype, phys), []).append(v[3 + ntags:])
+    records = [(t, p, np.asarray(n, np.int64)) for (t, p), n in by_shape.items()]
+    return nodes[:, 1:4], index, records
+
+
+def _read_v4(sec, field):
+    # $Entities: physical tags of each (dim, entity)
+    phys_of = {}
+    ent = sec.get("Entities")
+    if ent:
+        counts = [int(x) for x in ent[0].split()]
+        row = 1
+        for dim, count in enumerate(counts):
+            for _ in range(count):
+                v = ent[row].split()
+                row += 1
+                tag = int(v[0])
+                nfix = 4 if dim == 0 else 7              # point: tag x y z; others: tag + bounding box
+                nphys = int(v[nfix])
+                phys_of[(dim, tag)] = int(v[nfix + 1]) if nphys > 0 else 0
+    head = [int(x) for x in sec["Nodes"][0].split()]
+    nblocks, row = head[0], 1
+    tags_all, xyz_all = [], []
+    for _ in range(nblocks):
+        _, _, parametric, count = (int(x) for x in sec["Nodes"][row].split())
+        row += 1
+        tags_all.append(np.asarray([int(sec["Nodes"][row + k]) for k in range(count)], np.int64))
+        row += count
+        xyz = np.array([sec["Nodes"][row + k].split() for k in range(count)], dtype=np.float64).reshape(count, -1)
+        xyz_all.append(xyz[:, :3])
+        row += count
+    ids = np.concatenate(tags_all)
+    index = np.full(ids.max() + 1, -1, np.int64)
+    index[ids] = np.arange(len(ids))
+    head = [int(x) for x in sec["Elements"][0].split()]
+    nblocks, row = head[0], 1
+    by_shape = {}
+    for _ in range(nblocks):
+        dim, tag, etype, count = (int(x) for x in sec["Elements"][row].split())
+        row += 1
+        data = np.array([sec["Elements"][row + k].split() for k in range(count)], dtype=np.int64)
+        row += count
+        by_shape.setdefault((etype, phys_of.get((dim, tag), 0)), []).append(data[:, 1:])
+    records = [(t, p, np.concatenate(n)) for (t, p), n in by_shape.items()]
+    return np.concatenate(xyz_all), index, records
+
+
+def read_msh(path, periodic_map=None):
+    """Read a Gmsh MSH 2.2 or 4.1 ASCII file into a ``MeshSource`` (optionally with a periodic
+    point map for ``HybridMesh``)."""
+    lines = Path(path).read_text().splitlines()
+    sec = _sections(lines)
+    if "MeshFormat" not in sec:
+        raise ValueError(f"{path} is not a Gmsh mesh")
+    version, binary = sec["MeshFormat"][0].split()[:2]
+    if int(binary) != 0:
+        raise NotImplementedError("binary MSH files are not supported; save as ASCII")
+    field = _physical_names(sec.get("PhysicalNames"))
+    if version.startswith("2"):
+        points, index, records = _read_v2(sec, field)
+    elif version.startswith("4"):
+        points, index, records = _read_v4(sec, field)
+    else:
+        raise NotImplementedError(f"MSH version {version}")
+    cells, phys = _assemble(points, index, records)
+    return MeshSource(points, cells, phys, field, periodic_map)
+
+
+def write_msh22(path, source):
+    """Write a ``MeshSource`` as an MSH 2.2 ASCII file (first-order cells)."""
+    codes = {"triangle": 2, "quad": 3, "tetra": 4, "hexahedron": 5, "wedge": 6}
+    out = ["$MeshFormat", "2.2 0 8", "$EndMeshFormat", "$PhysicalNames", str(len(source.field_data))]
+    for name, (tag, dim) in source.field_data.items():
+        out.append(f'{dim} {tag} "{name}"')
+    out += ["$EndPhysicalNames", "$Nodes", str(len(source.points))]
+    out += [f"{i + 1} {x!r} {y!r} {z!r}" for i, (x, y, z) in enumerate(np.asarray(source.points, float).tolist())]
+    out += ["$EndNodes", "$Elements", str(sum(len(c) for _, c in source.cells))]
+    k = 1
+    for (ctype, conn), phys in zip(source.cells, source.physical):
+        for cell, p in zip(np.asarray(conn), np.asarray(phys)):
+            out.append(f"{k} {codes[ctype]} 2 {int(p)} {int(p)} " + " ".join(str(int(v) + 1) for v in cell))
+            k += 1
+    out.append("$EndElements")
+    Path(path).write_text("\n".join(out) + "\n")
+
+
+read_gmsh = read_msh     # the name HybridMesh(path) uses

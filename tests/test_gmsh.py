@@ -1,0 +1,123 @@
+"""Gmsh MSH 2.2 / 4.1 ASCII reading: a written file reads back to the same mesh (points, cells,
+physical tags and names, hence the same face tables), hand-written 4.1 and second-order files
+parse, and curved cells are refused."""
+
+import numpy as np
+import pytest
+
+from jax_fluid_sim_b200 import gmsh, meshgen
+from jax_fluid_sim_b200.mesh import HybridMesh
+
+
+def _same_faces(a, b):
+    ma, mb = HybridMesh(a), HybridMesh(b)
+    assert [x.element_type for x in ma.element_blocks] == [x.element_type for x in mb.element_blocks]
+    for ftype, fa in ma.face_blocks.items():
+        fb = mb.face_blocks[ftype]
+        for key in ("nodes", "owner_block", "owner_local", "neighbor_block", "neighbor_local", "boundary_tags"):
+            np.testing.assert_array_equal(getattr(fa, key), getattr(fb, key))
+
+
+@pytest.mark.parametrize("source", [meshgen.mixed_block(jitter=0.1, seed=3), meshgen.smoke_mesh()])
+def test_msh22_round_trip(tmp_path, source):
+    path = tmp_path / "m.msh"
+    gmsh.write_msh22(path, source)
+    back = gmsh.read_msh(path)
+    np.testing.assert_array_equal(back.points, source.points)
+    assert back.field_data == source.field_data
+    _same_faces(source, back)
+
+
+def test_reference_shim_writer_reads_back(tmp_path):
+    """The MSH 2.2 writer the golden fixtures use (tests/golden/refshim/meshio.py) reads back."""
+    import importlib.util
+    from pathlib import Path
+    spec = importlib.util.spec_from_file_location("shim_meshio", Path(__file__).parent / "golden" / "refshim" / "meshio.py")
+    shim = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(shim)
+    src = meshgen.box_hex((3, 3, 2), lo=(0, 0, 0), hi=(1.5, 1.5, 1.0), jitter=0.15, seed=7)
+    path = tmp_path / "b.msh"
+    shim.write_gmsh22(str(path), src.points, src.cells, src.physical, src.field_data)
+    _same_faces(src, gmsh.read_msh(path))
+
+
+MSH41 = """$MeshFormat
+4.1 0 8
+$EndMeshFormat
+$PhysicalNames
+2
+2 7 "walls"
+3 1 "fluid"
+$EndPhysicalNames
+$Entities
+0 0 1 1
+3 0 0 0 1 1 1 1 7 0
+5 0 0 0 1 1 1 1 1 0
+$EndEntities
+$Nodes
+1 8 1 8
+3 5 0 8
+1
+2
+3
+4
+5
+6
+7
+8
+0 0 0
+1 0 0
+1 1 0
+0 1 0
+0 0 1
+1 0 1
+1 1 1
+0 1 1
+$EndNodes
+$Elements
+2 2 1 2
+2 3 3 1
+1 1 2 3 4
+3 5 5 1
+2 1 2 3 4 5 6 7 8
+$EndElements
+"""
+
+
+def test_msh41_entities_and_blocks(tmp_path):
+    path = tmp_path / "c.msh"
+    path.write_text(MSH41)
+    src = gmsh.read_msh(path)
+    assert src.field_data == {"walls": (7, 2), "fluid": (1, 3)}
+    assert [c[0] for c in src.cells] == ["hexahedron", "quad"]
+    np.testing.assert_array_equal(src.cells[0][1], [[0, 1, 2, 3, 4, 5, 6, 7]])
+    assert src.physical[0].tolist() == [1] and src.physical[1].tolist() == [7]
+
+
+def test_second_order_cells(tmp_path):
+    """Serendipity hexahedron20 keeps its corners; a complete hexahedron27 is refused."""
+    pts = "\n".join(f"{i + 1} {x} {y} {z}" for i, (x, y, z) in enumerate(
+        [(a, b, c) for c in (0, 1, 2) for b in (0, 1, 2) for a in (0, 1, 2)]))
+    corners = [1, 3, 9, 7, 19, 21, 27, 25]
+    hex20 = corners + list(range(2, 14))
+    body = f"$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n27\n{pts}\n$EndNodes\n$Elements\n1\n1 17 2 1 1 " + \
+           " ".join(map(str, hex20)) + "\n$EndElements\n"
+    path = tmp_path / "h20.msh"
+    path.write_text(body)
+    src = gmsh.read_msh(path)
+    np.testing.assert_array_equal(src.cells[0][1][0], np.asarray(corners) - 1)
+    path.write_text(body.replace(" 17 2 1 1 ", " 12 2 1 1 ").replace(" ".join(map(str, hex20)),
+                                                                     " ".join(map(str, range(1, 28)))))
+    with pytest.raises(NotImplementedError):
+        gmsh.read_msh(path)
+
+
+def test_hybrid_mesh_and_solver_take_a_path(tmp_path):
+    """HybridMesh(path) and HybridCompressibleSolver(path) read the file, as the reference's do."""
+    from jax_fluid_sim_b200 import HybridCompressibleSolver
+    src = meshgen.mixed_block(jitter=0.1, seed=3)
+    path = tmp_path / "mixed.msh"
+    gmsh.write_msh22(path, src)
+    _same_faces(src, HybridMesh(str(path)).source)
+    solver = HybridCompressibleSolver(str(path), polynomial_degree=2)
+    assert [b.element_type for b in solver.mesh.element_blocks] == ["hexahedron", "wedge", "tetra"]
