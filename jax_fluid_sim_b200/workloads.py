@@ -168,7 +168,7 @@ def _timed(fn):
 
 
 def run_vortex(n, degree, precisions=("float64",), cfl=0.3, length=10.0, periods=1.0, graph=True, seed=0,
-               radius=0.1):
+               radius=0.1, autotune=True):
     """One size of the order study: the vortex through ``periods`` periods on the n^3 hybrid box
     of side ``length``, once per precision from the same start (one host plan).  Each result
     holds the density L2 error (divided by sqrt(box volume)), the step count and the
@@ -183,7 +183,7 @@ def run_vortex(n, degree, precisions=("float64",), cfl=0.3, length=10.0, periods
     for precision in precisions:
         op = op64 if precision == "float64" else op64.with_precision(precision)
         states = {k: v.clone() for k, v in start.items()}
-        widths = op.autotune(states)
+        widths = op.autotune(states) if autotune else None
         integ = HybridSSPRK3(op, cfl=cfl, graph=graph)
         first = integ.checked_step_inplace(states, dt).view(torch.int32)[0] != 0     # the graph capture
         ok, seconds = _timed(lambda: advance(integ, states, steps - 1, dt))
@@ -245,6 +245,7 @@ def main(argv=None):
     ap.add_argument("--cfl", type=float, default=0.3)
     ap.add_argument("--periods", type=float, default=1.0)
     ap.add_argument("--radius", type=float, default=0.1)
+    ap.add_argument("--autotune", type=int, default=1, help="time the dense kernels' launch shapes first")
     ap.add_argument("--n", type=int, default=16)
     ap.add_argument("--degree", type=int, default=2)
     ap.add_argument("--steps", type=int, default=10)
@@ -269,7 +270,8 @@ def main(argv=None):
     for degree in (int(d) for d in args.degrees.split(",")):
         errors = {}
         for n in sizes:
-            for r in run_vortex(n, degree, precisions, args.cfl, periods=args.periods, radius=args.radius):
+            for r in run_vortex(n, degree, precisions, args.cfl, periods=args.periods, radius=args.radius,
+                                autotune=bool(args.autotune)):
                 prev = errors.get(r["precision"])
                 if prev is not None:
                     r["order"] = float(np.log(prev[1] / r["l2_density"]) / np.log(n / prev[0]))
