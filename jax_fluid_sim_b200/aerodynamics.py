@@ -14,7 +14,7 @@ import numpy as np
 import torch
 
 from . import _native as N
-from .reference import FACE_TYPE_ID, RefElement
+from .reference import FACE_TYPE_ID
 
 
 @dataclass
@@ -57,7 +57,7 @@ class AerodynamicResult:
 
 def face_points(plan):
     """Physical coordinates of every face point, {face type: (F, nq, 3)}, by the owner element's
-    first-order map (the reference's face_metrics.physical_points)."""
+    geometry map (the reference's face_metrics.physical_points)."""
     out = {}
     for ftype, fp in plan.faces.items():
         pts = np.empty((fp.F, fp.nq, 3))
@@ -65,8 +65,9 @@ def face_points(plan):
             sel = np.flatnonzero(fp.owner_block == b)
             if not len(sel):
                 continue
-            xyz = plan.mesh.points[block.connectivity[fp.owner_local[sel]]]            # (f, nc, 3)
-            N1 = RefElement(block.element_type, 1).basis(fp.own_pts[sel].reshape(-1, 3))
+            geo, xyz_b = plan.mesh.geometry(block)
+            xyz = xyz_b[fp.owner_local[sel]]                                             # (f, n, 3)
+            N1 = geo.basis(fp.own_pts[sel].reshape(-1, 3))
             pts[sel] = np.einsum("fqk,fkd->fqd", N1.reshape(len(sel), fp.nq, -1), xyz)
         out[ftype] = pts
     return out

@@ -6,8 +6,9 @@ block, the cells and their physical tags.  Element types follow the reference's 
 (hybrid/mesh.py:11-20): tetrahedra, wedges and hexahedra of first order, and the serendipity
 hexahedron20 / wedge15, whose corner nodes come first; boundary triangles and quadrilaterals
 (and their second-order forms) keep their corners.  The complete second-order cells tetra10,
-wedge18 and hexahedron27 carry curved geometry, which the reference maps isoparametrically
-(hybrid/geometry.py:104-150) and the CUDA path does not: reading one raises NotImplementedError.
+wedge18 and hexahedron27 carry curved geometry, which the mesh takes in meshio's node order
+(``MeshSource`` cells of those names); this reader does not convert Gmsh's node order of those
+cells to meshio's, so it refuses them with NotImplementedError.
 """
 
 from pathlib import Path
@@ -54,8 +55,8 @@ def _assemble(points, node_index, records):
     grouped = {}
     for etype, phys, nodes in records:
         if etype in _CURVED:
-            raise NotImplementedError(f"{_CURVED[etype]} cells carry curved geometry; the CUDA path maps every "
-                                      "element by its corners (straight-sided)")
+            raise NotImplementedError(f"{_CURVED[etype]} cells: pass them as MeshSource cells in meshio's node "
+                                      "order (this reader does not reorder Gmsh's second-order nodes)")
         if etype not in _TYPES:
             raise ValueError(f"unsupported Gmsh element type {etype}")
         name, corners, _ = _TYPES[etype]

@@ -26,6 +26,18 @@ TET_SPLITS = {
     "hexahedron": ((0, 1, 2, 6), (0, 2, 3, 6), (0, 3, 7, 6), (0, 7, 4, 6), (0, 4, 5, 6), (0, 5, 1, 6)),
 }
 CORNER_COUNT = {"tetra": 4, "wedge": 6, "hexahedron": 8}
+# Source cell types (meshio names) -> (element type, corner count); hybrid/mesh.py:11-20
+ALIASES = {"tetra": ("tetra", 4), "tetra10": ("tetra", 4), "wedge": ("wedge", 6), "wedge15": ("wedge", 6),
+           "wedge18": ("wedge", 6), "hexahedron": ("hexahedron", 8), "hexahedron20": ("hexahedron", 8),
+           "hexahedron27": ("hexahedron", 8)}
+# Complete second-order cells carry curved geometry: their nodes in meshio/VTK order go to the
+# second-order reference element's node order (hybrid/mesh.py:22-35).
+P2_PERMUTATIONS = {
+    "tetra10": np.asarray([0, 1, 2, 3, 4, 6, 7, 5, 8, 9], np.int32),
+    "wedge18": np.asarray([0, 1, 2, 6, 9, 7, 3, 4, 5, 12, 14, 13, 8, 10, 11, 15, 17, 16], np.int32),
+    "hexahedron27": np.asarray([0, 1, 8, 3, 2, 10, 11, 9, 24, 4, 5, 12, 7, 6, 14, 15, 13, 25,
+                                16, 17, 22, 19, 18, 23, 20, 21, 26], np.int32),
+}
 
 
 @dataclass
@@ -35,6 +47,12 @@ class ElementBlock:
     centers: np.ndarray
     volumes: np.ndarray
     global_ids: np.ndarray
+    source_cell_type: str = ""
+    geometry_connectivity: np.ndarray | None = None   # second-order geometry nodes (curved cells)
+
+    @property
+    def geometry_degree(self):
+        return 1 if self.geometry_connectivity is None else 2
 
 
 @dataclass
@@ -88,20 +106,38 @@ class HybridMesh:
         self._validate()
 
     def _blocks(self, source):
+        """hybrid/mesh.py:238-286; one source cell type per element type (the reference would
+        make two blocks of one element type, which the type-keyed state dicts cannot hold)."""
         grouped = {}
         for ctype, data in source.cells:
-            if ctype in CORNER_COUNT:
-                grouped.setdefault(ctype, []).append(np.asarray(data)[:, :CORNER_COUNT[ctype]])
+            if ctype in ALIASES:
+                etype = ALIASES[ctype][0]
+                if etype in grouped and grouped[etype][0] != ctype:
+                    raise NotImplementedError(f"{etype} cells of two source types ({grouped[etype][0]}, {ctype})")
+                grouped.setdefault(etype, (ctype, []))[1].append(np.asarray(data))
         if not grouped:
             raise ValueError("Mesh contains no tetrahedron, wedge, or hexahedron")
         blocks, start = [], 0
         for etype in ("hexahedron", "wedge", "tetra"):
             if etype in grouped:
-                conn = np.concatenate(grouped[etype]).astype(np.int32)
+                ctype, arrays = grouped[etype]
+                geometry = np.concatenate(arrays).astype(np.int32)
+                conn = np.ascontiguousarray(geometry[:, :ALIASES[ctype][1]])
                 c, v = _cell_geometry(self.points, etype, conn)
-                blocks.append(ElementBlock(etype, conn, c, v, np.arange(start, start + len(conn), dtype=np.int32)))
+                gconn = (np.ascontiguousarray(geometry[:, P2_PERMUTATIONS[ctype]])
+                         if ctype in P2_PERMUTATIONS else None)
+                blocks.append(ElementBlock(etype, conn, c, v, np.arange(start, start + len(conn), dtype=np.int32),
+                                           ctype, gconn))
                 start += len(conn)
         return blocks
+
+    def geometry(self, block):
+        """(geometry reference element, node coordinates (E, n, 3)) of a block: the second-order
+        map of curved cells, the first-order map otherwise (hybrid/geometry.py:102-110)."""
+        from .reference import RefElement
+        if block.geometry_connectivity is not None:
+            return RefElement(block.element_type, 2), self.points[block.geometry_connectivity]
+        return RefElement(block.element_type, 1), self.points[block.connectivity]
 
     def _boundary_tags(self, source):
         keys, tags = [], []

@@ -393,6 +393,55 @@ def sphere_oh_grid(radius=0.5, box=((-4.0, 12.0), (-6.0, 6.0), (-6.0, 6.0)), cub
     return MeshSource(points, vol + bcells, [np.ones(len(hexes), np.int32)] + bphys, field)
 
 
+def curved_box(n=(3, 3, 2), lo=(0.0, 0.0, 0.0), hi=(1.5, 1.5, 1.0), amplitude=0.05,
+               plane_tags=(("inlet", "outlet"), ("walls", "walls"), ("sphere_wall", "sphere_wall"))):
+    """Box of curved triquadratic hexahedra ("hexahedron27" cells, node order as meshio gives
+    it, which the mesh maps to the second-order reference element's order).
+
+    The nodes of a (2n+1)^3 grid at half spacing are displaced by amplitude * h * S(x) along
+    (1, 1, 1), S = prod_d sin(pi (x_d - lo_d) / L_d), which vanishes on the box faces: interior
+    faces and cells curve while the boundary stays on the box planes.  Boundary quadrilaterals
+    are tagged per plane as in ``box_hex``."""
+    from .reference import RefElement
+    from .mesh import P2_PERMUTATIONS
+    nx, ny, nz = n
+    lo, hi = np.asarray(lo, float), np.asarray(hi, float)
+    L = hi - lo
+    h = L / np.asarray(n, float)
+    axes = [np.linspace(lo[d], hi[d], 2 * n[d] + 1) for d in range(3)]
+    Z, Y, X = np.meshgrid(axes[2], axes[1], axes[0], indexing="ij")
+    points = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
+    bump = np.prod(np.sin(np.pi * (points - lo) / L), axis=1)
+    points = points + amplitude * np.min(h) * bump[:, None] * np.ones(3)
+
+    def gid(i, j, k):
+        return (k * (2 * ny + 1) + j) * (2 * nx + 1) + i
+
+    offsets = np.rint(2.0 * RefElement("hexahedron", 2).nodes).astype(int)     # internal order, (27, 3)
+    perm = P2_PERMUTATIONS["hexahedron27"]
+    cells27, corners = [], []
+    for k in range(nz):
+        for j in range(ny):
+            for i in range(nx):
+                internal = [gid(2 * i + a, 2 * j + b, 2 * k + c) for a, b, c in offsets]
+                meshio_order = np.empty(27, np.int64)
+                meshio_order[perm] = internal
+                cells27.append(meshio_order)
+                corners.append(meshio_order[:8])
+    cells27 = np.asarray(cells27, np.int32)
+    corners = np.asarray(corners, np.int32)
+    names = sorted({nm for pair in plane_tags for nm in pair})
+    field = {"fluid": (1, 3)}
+    for t, name in enumerate(names):
+        field[name] = (10 + t, 2)
+    tag_of = {name: field[name][0] for name in names}
+    tagger = _box_tagger(points, lo, hi, [(tag_of[a], tag_of[b]) for a, b in plane_tags] + [0])
+    bcells, bphys = _boundary_cells([("hexahedron", corners)], np.arange(len(points)), tagger)
+    used = {int(t) for p in bphys for t in p}
+    field = {k: v for k, v in field.items() if k == "fluid" or v[0] in used}
+    return MeshSource(points, [("hexahedron27", cells27)] + bcells, [np.ones(len(cells27), np.int32)] + bphys, field)
+
+
 def cylinder_o_grid(n_theta=96, n_radial=48, radius=0.5, outer_radius=15.0, span=1.0, growth=None):
     """Extruded O-grid around a cylinder of the given radius (axis z), one element deep.
 

@@ -25,6 +25,11 @@ def _p1_jacobian(etype, xyz, points):
     return np.einsum("...kd,...kr->...dr", xyz, g)
 
 
+def _geo_jacobian(geo, xyz, points):
+    """J[..., d, r] = sum_k x_k[d] dN_k/dxi_r with the block's geometry basis (first or second order)."""
+    return np.einsum("...kd,...kr->...dr", xyz, geo.basis_gradients(points))
+
+
 class ElementPlan:
     pass
 
@@ -52,8 +57,8 @@ class Plan:
     # ------------------------------------------------------------ elements
     def _element_plan(self, block, k):
         ref = RefElement(block.element_type, self.degree)
-        xyz = self.mesh.points[block.connectivity]               # (E, nc, 3)
-        J = _p1_jacobian(block.element_type, xyz[:, None, :, :], ref.points[None])    # (E, Nq, 3, 3)
+        geo, xyz = self.mesh.geometry(block)                     # (E, n_geometry_nodes, 3)
+        J = _geo_jacobian(geo, xyz[:, None, :, :], ref.points[None])                # (E, Nq, 3, 3)
         det = np.linalg.det(J)
         jinv = np.linalg.inv(J)                                   # [r][d] = dxi_r/dx_d
         wdet = ref.weights[None, :] * np.abs(det)
@@ -65,7 +70,7 @@ class Plan:
         p.E, p.Np, p.Nq = len(block.connectivity), ref.np, ref.nq
         p.nlf = len(LOCAL_FACES[block.element_type])
         p.jinv, p.wdet, p.minv, p.volume = jinv, wdet, minv, vol
-        p.node_xyz = np.einsum("qi,eid->eqd", RefElement(block.element_type, 1).basis(ref.nodes), xyz)
+        p.node_xyz = np.einsum("qi,eid->eqd", geo.basis(ref.nodes), xyz)
         p.affine = bool(np.all(np.ptp(det, axis=1) <= 1e-13 * np.abs(det).max(axis=1)))
         return p
 
@@ -140,9 +145,10 @@ class Plan:
         measure = 0.5 if ftype == "triangle" else 1.0
         for b, block in enumerate(mesh.element_blocks):
             sel = np.flatnonzero(fb.owner_block == b)
+            geo, xyz_b = mesh.geometry(block)
             if len(sel):
-                xyz = mesh.points[block.connectivity[fb.owner_local[sel]]]
-                J = _p1_jacobian(block.element_type, xyz[:, None], own_pts[sel])
+                xyz = xyz_b[fb.owner_local[sel]]
+                J = _geo_jacobian(geo, xyz[:, None], own_pts[sel])
                 tu = np.einsum("fqdr,fqr->fqd", J, tu_ref[sel])
                 tv = np.einsum("fqdr,fqr->fqd", J, tv_ref[sel])
                 area = np.cross(tu, tv)
@@ -154,8 +160,8 @@ class Plan:
                 jinv_side[sel, 0] = np.linalg.inv(J)
             seln = np.flatnonzero(fb.neighbor_block == b)
             if len(seln):
-                xyz = mesh.points[block.connectivity[fb.neighbor_local[seln]]]
-                J = _p1_jacobian(block.element_type, xyz[:, None], nbr_pts[seln])
+                xyz = xyz_b[fb.neighbor_local[seln]]
+                J = _geo_jacobian(geo, xyz[:, None], nbr_pts[seln])
                 jinv_side[seln, 1] = np.linalg.inv(J)
         fp.normals, fp.weights, fp.jinv_side = normals, weights, jinv_side
         return fp

@@ -147,8 +147,7 @@ class SubcellBlockPlan:
     def __init__(self, mesh, block, degree, rs, chunk=4096):
         etype = block.element_type
         ref = RefElement(etype, degree)
-        geo1 = RefElement(etype, 1)
-        xyz_all = mesh.points[block.connectivity]
+        geo1, xyz_all = mesh.geometry(block)          # subcell.py:282-288: the block's geometry map
         mp, rw = _subcell_rule(rs)
         flat = mp.reshape(-1, 3)
         sb = ref.basis(flat).reshape(rs.count, mp.shape[1], -1)

@@ -65,11 +65,10 @@ def vortex_primitive(xyz, t=0.0, beta=5.0, radius=0.1, mach=0.5, gamma=1.4, cent
 
 def quadrature_points(plan):
     """Physical quadrature points (E, Nq, 3) and weights w_q |J| (E, Nq) of every element block."""
-    from .reference import RefElement
     out = []
     for bp, block in zip(plan.blocks, plan.mesh.element_blocks):
-        xyz = plan.mesh.points[block.connectivity]
-        xq = np.einsum("qi,eid->eqd", RefElement(bp.etype, 1).basis(bp.ref.points), xyz)
+        geo, xyz = plan.mesh.geometry(block)
+        xq = np.einsum("qi,eid->eqd", geo.basis(bp.ref.points), xyz)
         out.append((xq, bp.wdet))
     return out
 

@@ -9,8 +9,8 @@ Oracle restatement of ``hybrid/geometry.py``:
   mapped by the owner Jacobian, area vector oriented like the mesh normal,
   weights = normalised rule x reference measure x |area vector|
   (``:205-362``).
-Only straight-sided (P1-geometry) cells are handled; the meshes used here are
-linear.
+Blocks of complete second-order cells use the second-order reference element as
+the geometry basis on their geometry nodes (``:102-110``); all others the first-order one.
 """
 
 import numpy as np
@@ -33,17 +33,22 @@ class Geometry:
         self.degree = degree
         types = {b.element_type for b in mesh.element_blocks}
         self.ref = {t: RefElement(t, degree) for t in types}
-        self.geo_ref = {t: RefElement(t, 1) for t in types}
+        self.geo_ref = {b.element_type: RefElement(b.element_type, 1 if b.geometry_connectivity is None else 2)
+                        for b in mesh.element_blocks}
         self.element = [self._element_metrics(b) for b in mesh.element_blocks]
         self.node_xyz = {}
         for b in mesh.element_blocks:
             gb = self.geo_ref[b.element_type].basis(self.ref[b.element_type].nodes)
-            self.node_xyz[b.element_type] = np.einsum("qi,eid->eqd", gb, mesh.points[b.connectivity])
+            self.node_xyz[b.element_type] = np.einsum("qi,eid->eqd", gb, self.geometry_nodes(b))
         self.face = {ft: self._face_metrics(ft, fb) for ft, fb in mesh.face_blocks.items()}
+
+    def geometry_nodes(self, block):
+        return self.mesh.points[block.connectivity if block.geometry_connectivity is None
+                                else block.geometry_connectivity]
 
     def _element_metrics(self, block):
         ref, gref = self.ref[block.element_type], self.geo_ref[block.element_type]
-        xyz = self.mesh.points[block.connectivity]
+        xyz = self.geometry_nodes(block)
         gb = gref.basis(ref.volume_points)
         gg = gref.basis_gradients(ref.volume_points)
         m = ElementMetrics()
@@ -103,7 +108,7 @@ class Geometry:
             idx = np.flatnonzero(fb.owner_block == ob)
             block = self.mesh.element_blocks[int(ob)]
             gref = self.geo_ref[block.element_type]
-            xyz = self.mesh.points[block.connectivity[fb.owner_local[idx]]]
+            xyz = self.geometry_nodes(block)[fb.owner_local[idx]]
             gb = gref.basis(own_pts[idx])
             gg = gref.basis_gradients(own_pts[idx])
             mapped = np.einsum("fqi,fid->fqd", gb, xyz)
@@ -126,6 +131,6 @@ class Geometry:
         """navier_stokes.py:112-136: grad phi at arbitrary reference points, J inverted per point."""
         block = self.mesh.element_blocks[block_id]
         ref, gref = self.ref[block.element_type], self.geo_ref[block.element_type]
-        xyz = self.mesh.points[block.connectivity[cells]]
+        xyz = self.geometry_nodes(block)[cells]
         jac = np.einsum("fid,fqir->fqdr", xyz, gref.basis_gradients(points))
         return np.einsum("fqir,fqrd->fqid", ref.basis_gradients(points), np.linalg.inv(jac))

@@ -1,8 +1,9 @@
 """Type-blocked mesh topology: element blocks and face pairing.
 
 Oracle restatement of ``hybrid/mesh.py``:
-* element blocks in hex -> wedge -> tet order, first-order corners only
-  (``hybrid/mesh.py:240-286``);
+* element blocks in hex -> wedge -> tet order; corners for the topology, and for the complete
+  second-order cells (tetra10, wedge18, hexahedron27) their geometry nodes permuted from
+  meshio order to the reference element's node order (``hybrid/mesh.py:11-35,240-286``);
 * cell centres/volumes from a fixed tetrahedral decomposition (``:61-76,207-238``);
 * face pairing by sorted corner ids in visiting order, owner = first visitor,
   unpaired faces tagged from boundary cells (``:343-359,378-405``);
@@ -20,7 +21,15 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-ALIASES = {"tetra": ("tetra", 4), "wedge": ("wedge", 6), "hexahedron": ("hexahedron", 8)}
+ALIASES = {"tetra": ("tetra", 4), "tetra10": ("tetra", 4), "wedge": ("wedge", 6), "wedge15": ("wedge", 6),
+           "wedge18": ("wedge", 6), "hexahedron": ("hexahedron", 8), "hexahedron20": ("hexahedron", 8),
+           "hexahedron27": ("hexahedron", 8)}
+P2_PERMUTATIONS = {
+    "tetra10": [0, 1, 2, 3, 4, 6, 7, 5, 8, 9],
+    "wedge18": [0, 1, 2, 6, 9, 7, 3, 4, 5, 12, 14, 13, 8, 10, 11, 15, 17, 16],
+    "hexahedron27": [0, 1, 8, 3, 2, 10, 11, 9, 24, 4, 5, 12, 7, 6, 14, 15, 13, 25, 16, 17, 22, 19, 18, 23, 20, 21,
+                     26],
+}
 LOCAL_FACES = {
     "tetra": ((0, 2, 1), (0, 1, 3), (1, 2, 3), (2, 0, 3)),
     "wedge": ((0, 2, 1), (3, 4, 5), (0, 1, 4, 3), (1, 2, 5, 4), (2, 0, 3, 5)),
@@ -49,6 +58,7 @@ class Block:
     connectivity: np.ndarray
     centers: np.ndarray
     volumes: np.ndarray
+    geometry_connectivity: np.ndarray | None = None
 
 
 @dataclass
@@ -91,14 +101,17 @@ class Mesh:
         grouped = {}
         for (ctype, data) in source.cells:
             if ctype in ALIASES:
-                grouped.setdefault(ctype, []).append(np.asarray(data, np.int64))
+                grouped.setdefault(ALIASES[ctype][0], []).append((ctype, np.asarray(data, np.int64)))
         if not grouped:
             raise ValueError("Mesh contains no tetrahedron, wedge, or hexahedron")
         blocks = []
         for etype in ("hexahedron", "wedge", "tetra"):
             if etype not in grouped:
                 continue
-            conn = np.concatenate(grouped[etype]).astype(np.int32)
+            ctype = grouped[etype][0][0]
+            geometry = np.concatenate([a for _, a in grouped[etype]]).astype(np.int32)
+            conn = geometry[:, :ALIASES[ctype][1]]
+            gconn = geometry[:, P2_PERMUTATIONS[ctype]] if ctype in P2_PERMUTATIONS else None
             centers, volumes = [], []
             for cell in conn:
                 v = self.points[cell]
@@ -107,7 +120,7 @@ class Mesh:
                 total = float(np.sum(vols))
                 centers.append(np.sum([vol * p.mean(axis=0) for vol, p in zip(vols, pieces)], axis=0) / total)
                 volumes.append(total)
-            blocks.append(Block(etype, conn, np.asarray(centers), np.asarray(volumes)))
+            blocks.append(Block(etype, conn, np.asarray(centers), np.asarray(volumes), gconn))
         return blocks
 
     def _boundary_tags(self, source):

@@ -145,14 +145,15 @@ class SubcellProjection:
         mesh, geo = op.mesh, op.geo
         block = mesh.element_blocks[block_id]
         etype = block.element_type
-        xyz = mesh.points[block.connectivity]
-        pv = np.einsum("vi,eid->evd", _basis(etype, 1, rs.vertices), xyz)
+        gdeg = 1 if block.geometry_connectivity is None else 2          # subcell.py:282-288
+        xyz = geo.geometry_nodes(block)
+        pv = np.einsum("vi,eid->evd", _basis(etype, gdeg, rs.vertices), xyz)
         cells_xyz = pv[:, rs.cells]
         self.centers = cells_xyz.mean(axis=2)
         mp, rw = _mapped_quadrature(rs)
         flat = mp.reshape(-1, 3)
         sb = _basis(etype, op.degree, flat).reshape(rs.count, mp.shape[1], -1)
-        gg = _basis_grad(etype, 1, flat).reshape(rs.count, mp.shape[1], -1, 3)
+        gg = _basis_grad(etype, gdeg, flat).reshape(rs.count, mp.shape[1], -1, 3)
         jac = np.einsum("eir,sqij->esqrj", xyz, gg)
         pw = np.abs(np.linalg.det(jac)) * rw[None]
         self.volumes = pw.sum(axis=-1)

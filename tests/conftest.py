@@ -11,7 +11,7 @@ if str(ROOT) not in sys.path:
 from jax_fluid_sim_b200.meshgen import MeshSource  # noqa: E402
 
 GOLDEN = ROOT / "tests" / "golden"
-GOLDEN_CASES = ["smoke_p1", "smoke_p2", "smoke_p3", "box_p2", "box_p3", "mixed_p2", "species_p2"]
+GOLDEN_CASES = ["smoke_p1", "smoke_p2", "smoke_p3", "box_p2", "box_p3", "mixed_p2", "species_p2", "curved_p2"]
 
 
 def pytest_configure(config):

@@ -167,6 +167,7 @@ def main():
     for p in (2, 3):
         run_case(f"box_p{p}", box, p, 0.01, ff, 1.2, 0.6, mood=True)
     run_case("mixed_p2", meshgen.mixed_block(jitter=0.1, seed=3), 2, 0.01, ff, 1.1, 1.0, mood=True)
+    run_case("curved_p2", meshgen.curved_box(amplitude=0.05), 2, 0.01, ff, 1.2, 0.6, mood=True)
 
 
 if __name__ == "__main__":

@@ -3,8 +3,8 @@
 Returns the fields the reference's ``hybrid/mesh.py:186-205,343-359`` reads:
 ``points``, ``cells`` (blocks with ``type``/``data``), ``field_data`` and
 ``cell_data["gmsh:physical"]``.  Consecutive elements of one type form one
-block, as meshio does.  Only first-order cell types are handled; those need no
-node reordering between Gmsh and meshio.
+block, as meshio does.  First-order cell types need no node reordering between Gmsh
+and meshio; second-order cells are passed through in the order they were written.
 """
 
 from dataclasses import dataclass
@@ -12,7 +12,10 @@ from dataclasses import dataclass
 import numpy as np
 
 _GMSH_TYPES = {1: ("line", 2), 2: ("triangle", 3), 3: ("quad", 4), 4: ("tetra", 4),
-               5: ("hexahedron", 8), 6: ("wedge", 6), 15: ("vertex", 1)}
+               5: ("hexahedron", 8), 6: ("wedge", 6), 15: ("vertex", 1),
+               # complete second-order cells, kept in the node order they were written in (the
+               # fixture generators write meshio's order, so nothing is reordered here)
+               11: ("tetra10", 10), 12: ("hexahedron27", 27), 13: ("wedge18", 18)}
 _TYPE_IDS = {name: (tid, n) for tid, (name, n) in _GMSH_TYPES.items()}
 
 

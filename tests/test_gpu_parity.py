@@ -39,7 +39,7 @@ def setup(case):
     return g, solver, op, bc
 
 
-CASES = GOLDEN_CASES + ["box_p2:dense", "box_p3:dense", "species_p2:dense"]
+CASES = GOLDEN_CASES + ["box_p2:dense", "box_p3:dense", "species_p2:dense", "curved_p2:dense"]
 
 
 @pytest.mark.parametrize("case", CASES)
@@ -91,7 +91,8 @@ def test_uniform_state_is_steady():
     assert torch.count_nonzero(r["hexahedron"]).item() == 0
 
 
-MOOD_CASES = ["box_p2", "box_p3", "mixed_p2", "box_p2:dense", "species_p2", "species_p2:dense"]
+MOOD_CASES = ["box_p2", "box_p3", "mixed_p2", "box_p2:dense", "species_p2", "species_p2:dense", "curved_p2",
+              "curved_p2:dense"]
 
 
 @pytest.mark.parametrize("case", MOOD_CASES)
@@ -122,7 +123,8 @@ def test_mood_recompute_and_step(case):
         close(res[k], g[f"mood_step_{k}"])
 
 
-@pytest.mark.parametrize("case", ["box_p2", "box_p3", "mixed_p2", "smoke_p1", "smoke_p3", "box_p2:dense", "species_p2"])
+@pytest.mark.parametrize("case", ["box_p2", "box_p3", "mixed_p2", "smoke_p1", "smoke_p3", "box_p2:dense", "species_p2",
+                                  "curved_p2"])
 @pytest.mark.parametrize("label", ["smooth", "shocked"])
 def test_mixed_precision_against_reference(case, label):
     """precision='mixed' (float32 trace, lift, volume and finalize arithmetic, on the

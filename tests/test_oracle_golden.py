@@ -96,7 +96,7 @@ def test_dt_limiter_sensor_step(case, label):
         assert close(res[k], g[f"step_{label}_{k}"], 1e-9)
 
 
-MOOD_CASES = ["box_p2", "box_p3", "mixed_p2", "species_p2"]
+MOOD_CASES = ["box_p2", "box_p3", "mixed_p2", "species_p2", "curved_p2"]
 
 
 @pytest.mark.parametrize("case", MOOD_CASES)
