@@ -377,6 +377,29 @@ int dgb_plan_predictor_counts(dgb_plan* plan, int64_t* counts, int reset);
 int dgb_chem_rates(dgb_chem* chem, const double* rho, const double* T, int64_t count, double* omega,
                    double* wdot, double* jacobian, void* stream);
 
+/* ---------------------------------------------------------------- midplane rasteriser
+ * (hybrid/gui/gpu_rasterizer.py:18-344) into a headless RGBA buffer.  The host locates each
+ * pixel on the cut plane: pixel_block[p] (-1 outside the mesh), pixel_element[p] and the
+ * solution-basis weights pixel_weights[p][max_nodes] (float32) of that element at the pixel.
+ * Device arrays throughout. */
+typedef struct {
+  int nx, ny, max_nodes;
+  int block_nodes[DGB_MAX_BLOCKS];   /* nodes per element of each block */
+  const int32_t* pixel_block;
+  const int32_t* pixel_element;
+  const float* pixel_weights;
+  const uint8_t* body_mask;          /* 1: paint the background colour (the body) */
+  const uint8_t* grad_mask;          /* 1: no schlieren gradient (next to the body) */
+  const uint8_t* luts;               /* [2][256][4]: the field palette, the temperature palette */
+  uint8_t background[4];
+  double dx, dy;                     /* pixel spacing */
+} dgb_raster_desc;
+
+/* Renders mode 0 schlieren, 1 density, 2 pressure, 3 Mach, 4 temperature of U into rgba
+ * [ny][nx][4] (row 0 at the top); grid is scratch [ny][nx][5] float64 (rho, u, v, w, p). */
+int dgb_raster_render(const dgb_raster_desc* desc, const dgb_state* U, int nvars, double gamma, int mode,
+                      double vmin, double vmax, double* grid, uint8_t* rgba, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

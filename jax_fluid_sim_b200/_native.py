@@ -114,6 +114,8 @@ def lib():
             "dgb_plan_set_hex": [c_void_p, P_double, P_int32, c_int, c_int, ctypes.POINTER(ctypes.c_uint8)],
             "dgb_plan_set_hex_affine": [c_void_p, ctypes.POINTER(ctypes.c_uint8), P_double, P_double, P_double],
             "dgb_plan_set_face_points": [c_void_p, c_int, P_double],
+            "dgb_raster_render": [ctypes.POINTER(RasterDesc), ctypes.POINTER(State), c_int, ctypes.c_double, c_int,
+                                  ctypes.c_double, ctypes.c_double, c_void_p, c_void_p, c_void_p],
             "dgb_wall_forces": [c_void_p, ctypes.POINTER(State), P_int32, c_int, P_double, c_void_p, c_void_p],
             "dgb_plan_autotune": [c_void_p, ctypes.POINTER(State), c_int, P_int32, c_void_p],
             "dgb_plan_set_cases": [c_void_p, c_int, P_double, ctypes.POINTER(ctypes.c_void_p)],
@@ -156,6 +158,13 @@ def check(rc):
         if rc == -3:
             raise NotImplementedError(msg)
         raise RuntimeError(f"dgb200 error {rc}: {msg}")
+
+
+class RasterDesc(ctypes.Structure):
+    _fields_ = [("nx", c_int), ("ny", c_int), ("max_nodes", c_int), ("block_nodes", c_int * MAX_BLOCKS),
+                ("pixel_block", c_void_p), ("pixel_element", c_void_p), ("pixel_weights", c_void_p),
+                ("body_mask", c_void_p), ("grad_mask", c_void_p), ("luts", c_void_p),
+                ("background", ctypes.c_uint8 * 4), ("dx", ctypes.c_double), ("dy", ctypes.c_double)]
 
 
 def dptr(a, ctype=ctypes.c_double):

@@ -14,7 +14,8 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 LIB = PKG / "libdgb200.so"
-SOURCES = [PKG / "csrc" / "capi.cu", PKG / "csrc" / "noalloc.cu", PKG / "csrc" / "chemistry.cu"]
+SOURCES = [PKG / "csrc" / "capi.cu", PKG / "csrc" / "noalloc.cu", PKG / "csrc" / "chemistry.cu",
+           PKG / "csrc" / "raster.cu"]
 DEPENDS = sorted((PKG / "csrc").glob("*.cu*")) + [ROOT / "include" / "dgb200.h"]
 
 
