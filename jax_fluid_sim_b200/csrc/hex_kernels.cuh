@@ -740,6 +740,39 @@ __global__ void __launch_bounds__(kThreads) k_hex_finalize(const DevPlan P_, con
 // volume-point values [NV][Q3].  The six faces go through one 2-D contraction (their slabs
 // stacked as 6*NV channels) in fs, which holds 6*NV*(N2 + N*QF + QF2) values.  Ends without a
 // barrier: callers synchronise before reading.
+// Cell mean sum_q u_q w_q |J_q| / sum_q w_q |J_q| of NV fields at the Q3 volume points, worked by
+// all threads: each strides over the points, a warp combines its lanes by shuffles and thread 0
+// adds the warps in order (deterministic).  Ends with the block synchronised and mean[] set.
+template <int NV>
+__device__ void hex_cell_mean(const double* vq, const double* __restrict__ wdet, int Q3, double* mean,
+                              double (*part)[NV + 1]) {
+  double s[NV + 1];
+#pragma unroll
+  for (int v = 0; v <= NV; ++v) s[v] = 0.0;
+  for (int q = threadIdx.x; q < Q3; q += blockDim.x) {
+    const double w = wdet[q];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) s[v] += vq[v * Q3 + q] * w;
+    s[NV] += w;
+  }
+#pragma unroll
+  for (int v = 0; v <= NV; ++v)
+    for (int o = 16; o > 0; o >>= 1) s[v] += __shfl_xor_sync(0xffffffff, s[v], o);
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int v = 0; v <= NV; ++v) part[threadIdx.x >> 5][v] = s[v];
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double a = 0.0, w = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+      a += part[k][threadIdx.x];
+      w += part[k][NV];
+    }
+    mean[threadIdx.x] = a / w;
+  }
+  __syncthreads();
+}
+
 template <int P, int NV>
 __device__ void hex_samples(const HexTables* tb, const double* Ug, double* U, double* Smp, double* t1, double* t2,
                             double* vq, double* fs) {
@@ -806,16 +839,8 @@ __global__ void __launch_bounds__(kThreads) k_hex_positivity(const DevPlan P_, c
   if (threadIdx.x == 0) red_nan = 0;
   __syncthreads();
   // cell mean from the volume samples
-  const double* wdet = B.wdet + (size_t)e * Q3;
-  for (int v = threadIdx.x; v < NV; v += blockDim.x) {
-    double s = 0.0, w = 0.0;
-    for (int q = 0; q < Q3; ++q) {
-      s += vq[v * Q3 + q] * wdet[q];
-      w += wdet[q];
-    }
-    mean[v] = s / w;
-  }
-  __syncthreads();
+  __shared__ double part[kThreads / 32][NV + 1];
+  hex_cell_mean<NV>(vq, B.wdet + (size_t)e * Q3, Q3, mean, part);
   double Wm[NV];
   primitive<NV>(P_.ph, mean, Wm);
   const double rfloor = fmax(Lc.density_floor, Lc.relative_floor * Wm[0]);
@@ -910,15 +935,8 @@ __global__ void __launch_bounds__(kThreads) k_hex_troubled(const DevPlan P_, con
   // P1 projection of (rho, p): the nodal projector onto the trilinear space is the threefold
   // tensor product of the 1-D projector onto span{1, xi} (three passes of N x N)
   if (P >= 2) tensor3<2, N, N, N, N, N, N, false>(Mon, Low, t1, t2, tb->p1d, tb->p1d, tb->p1d);
-  const double* wdet = B.wdet + (size_t)e * Q3;
-  for (int v = threadIdx.x; v < NV; v += blockDim.x) {
-    double s = 0.0, w = 0.0;
-    for (int q = 0; q < Q3; ++q) {
-      s += vq[v * Q3 + q] * wdet[q];
-      w += wdet[q];
-    }
-    mean[v] = s / w;
-  }
+  __shared__ double part[kThreads / 32][NV + 1];
+  hex_cell_mean<NV>(vq, B.wdet + (size_t)e * Q3, Q3, mean, part);
   double hi0 = 0.0, hi1 = 0.0, sc0 = 0.0, sc1 = 0.0;
   if (P >= 2) {
     for (int i = threadIdx.x; i < N3; i += blockDim.x) {
