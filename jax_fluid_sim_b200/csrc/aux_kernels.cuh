@@ -47,18 +47,38 @@ __device__ void build_samples(const BlockDev& B, const double* U, double* S) {
   }
 }
 
-// Cell mean: sum_q wdet (B U) / sum_q wdet, from the volume samples.
+// Cell mean: sum_q wdet (B U) / sum_q wdet, from the volume samples [q][v], worked by all threads
+// (a strided sum per thread, shuffles per warp, the warps added in order by thread 0); ends with
+// the block synchronised and mean[] set.
 template <int NV>
 __device__ void cell_mean(const BlockDev& B, int e, const double* Svol, double* mean) {
+  __shared__ double part[kThreads / 32][NV + 1];
   const double* wdet = B.wdet + (size_t)e * B.Nq;
-  for (int v = threadIdx.x; v < NV; v += blockDim.x) {
-    double s = 0.0, wsum = 0.0;
-    for (int q = 0; q < B.Nq; ++q) {
-      s += Svol[q * NV + v] * wdet[q];
-      wsum += wdet[q];
-    }
-    mean[v] = s / wsum;
+  double s[NV + 1];
+#pragma unroll
+  for (int v = 0; v <= NV; ++v) s[v] = 0.0;
+  for (int q = threadIdx.x; q < B.Nq; q += blockDim.x) {
+    const double w = wdet[q];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) s[v] += Svol[q * NV + v] * w;
+    s[NV] += w;
   }
+#pragma unroll
+  for (int v = 0; v <= NV; ++v)
+    for (int o = 16; o > 0; o >>= 1) s[v] += __shfl_xor_sync(0xffffffff, s[v], o);
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int v = 0; v <= NV; ++v) part[threadIdx.x >> 5][v] = s[v];
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double a = 0.0, w = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+      a += part[k][threadIdx.x];
+      w += part[k][NV];
+    }
+    mean[threadIdx.x] = a / w;
+  }
+  __syncthreads();
 }
 
 template <int NV>
