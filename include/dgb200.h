@@ -76,7 +76,8 @@ typedef struct {
   const double* inv_jacobian; /* [E][Nq][3][3] dxi_r/dx_d                       */
   const double* wdet;         /* [E][Nq]       w |det J|                        */
   const double* inv_mass;     /* [E][Np][Np]   sliver-scaled inverse mass; stored transposed
-                                 ([E][j][i] = M^-1[i][j]) when dgb_plan_set_hex is used */
+                                 ([E][j][i] = M^-1[i][j]) when dgb_plan_set_hex is used; may be
+                                 NULL, then dgb_plan_build_inverse_mass forms it on the device */
   const int32_t* elem_face;   /* [E][nlf]      (face type<<30)|(face<<1)|side   */
   const double* length;       /* [E]           characteristic length (CFL)      */
   int num_face_samples;
@@ -120,6 +121,33 @@ int dgb_plan_set_faces(dgb_plan* plan, const dgb_face_desc* desc);
  * at each code's reference face points. */
 int dgb_plan_set_trace(dgb_plan* plan, int element_type, int face_type, int num_codes, int num_qp,
                        int num_nodes, const double* basis, const double* basis_grad);
+/* Forms the sliver-scaled inverse mass matrices of block b on the device from the block's basis
+ * and w|det J| tables, for a block whose descriptor gave inv_mass = NULL (hybrid/geometry.py:
+ * 181-192 forms M = B^T diag(w|J|) B and inverts it on the host; the scale is
+ * min(1, volume[e] / 1e-4)).  volume: host [E], the element volumes sum_q w|det J|.
+ * transposed: store [E][j][i] (the layout of the sum-factorised path).  Synchronous (set-up);
+ * fails on an element whose mass matrix is not positive definite. */
+int dgb_plan_build_inverse_mass(dgb_plan* plan, int block, const double* volume, int transposed);
+/* Set-up helper: inverts count symmetric positive definite n x n matrices (device memory,
+ * [count][n][n], n <= 160) in place, one per CTA, by Gauss-Jordan elimination without pivoting;
+ * *status (a device int) is set to 0, or to 1 + the index of a matrix found not positive
+ * definite, which is then left partly reduced.  Asynchronous on stream.  Used for the
+ * least-squares Gram matrices of the MOOD subcell reconstruction (hybrid/subcell.py:324-334
+ * inverts them with a dense inverse). */
+int dgb_spd_inverse(double* matrices, int n, int count, int* status, void* stream);
+/* Host-side geometry metrics for plan set-up (no GPU needed; hybrid/geometry.py:139-203,
+ * 299-353 form the same with dense einsums).  For count elements, element i taking the
+ * geometry nodes nodes[index ? index[i] : i] ([n][3] each), at num_points reference points
+ * with geometry-basis gradients grad[num_points][n][3]: jacobian [count][Q][3][3]
+ * (J[d][r] = dx_d/dxi_r), det [count][Q], inv_jacobian [count][Q][3][3], wdet [count][Q]
+ * = weights[q] |det J|; with tangents [Q][2][3] (reference face tangents t_u, t_v) and
+ * orientation [count][3] (a direction the normal must not oppose): normals [count][Q][3]
+ * (unit J t_u x J t_v) and area_weights [count][Q] = weights[q] |J t_u x J t_v|.  Any output
+ * may be NULL.  Runs on the host cores in threads. */
+int dgb_map_metrics(const double* nodes, const int32_t* index, int count, int num_nodes, const double* grad,
+                    int num_points, const double* weights, const double* tangents, const double* orientation,
+                    double* jacobian, double* det, double* inv_jacobian, double* wdet, double* normals,
+                    double* area_weights);
 /* Optional sum-factorised path for a mesh of one hexahedron block (hexahedron bases are
  * tensor products of the 1-D Lagrange basis on the nodes 0, 1, interior: hybrid/elements.py:
  * 199-274, 325-456).  line_tables: 173 doubles, in order bq[5][4], dq[5][4] (1-D basis and

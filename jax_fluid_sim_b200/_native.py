@@ -121,6 +121,10 @@ def lib():
             "dgb_plan_set_cases": [c_void_p, c_int, P_double, ctypes.POINTER(ctypes.c_void_p)],
             "dgb_plan_set_block_affine": [c_void_p, c_int, ctypes.POINTER(ctypes.c_uint8), P_double, P_double,
                                           P_double, P_double, P_double],
+            "dgb_plan_build_inverse_mass": [c_void_p, c_int, P_double, c_int],
+            "dgb_spd_inverse": [c_void_p, c_int, c_int, c_void_p, c_void_p],
+            "dgb_map_metrics": [P_double, P_int32, c_int, c_int, P_double, c_int, P_double, P_double, P_double,
+                                P_double, P_double, P_double, P_double, P_double, P_double],
             "dgb_plan_destroy": [c_void_p],
             "dgb_plan_update_params": [c_void_p, ctypes.POINTER(Params)],
             "dgb_rhs": [c_void_p, ctypes.POINTER(State), ctypes.POINTER(State), ctypes.POINTER(State), c_void_p],
@@ -179,3 +183,28 @@ def as_f64(a):
 
 def as_i32(a):
     return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def map_metrics(nodes, grad, index=None, weights=None, tangents=None, orientation=None,
+                outputs=("det", "inv_jacobian")):
+    """Geometry metrics on the host cores (``dgb_map_metrics``): element i of the result maps
+    by nodes[index[i]] (all of ``nodes`` when ``index`` is None) at the points of ``grad``
+    (Q, n, 3).  ``outputs`` names the arrays to return, in that order, from jacobian (count, Q,
+    3, 3), det (count, Q), inv_jacobian (count, Q, 3, 3), wdet (count, Q), normals (count, Q, 3)
+    and area_weights (count, Q)."""
+    nodes = as_f64(nodes)
+    grad = as_f64(grad)
+    idx = None if index is None else as_i32(index)
+    count = len(nodes) if idx is None else len(idx)
+    Q, n = grad.shape[0], grad.shape[1]
+    if nodes.shape[1:] != (n, 3):
+        raise ValueError(f"nodes have shape {nodes.shape}; the geometry basis has {n} nodes")
+    shapes = dict(jacobian=(count, Q, 3, 3), det=(count, Q), inv_jacobian=(count, Q, 3, 3), wdet=(count, Q),
+                  normals=(count, Q, 3), area_weights=(count, Q))
+    out = {k: np.empty(shapes[k]) for k in outputs}
+    keep = [None if a is None else as_f64(a) for a in (weights, tangents, orientation)]
+    args = [None if a is None else dptr(a) for a in keep]
+    check(lib().dgb_map_metrics(dptr(nodes), None if idx is None else dptr(idx, ctypes.c_int32), count, n,
+                                dptr(grad), Q, *args,
+                                *[dptr(out[k]) if k in out else None for k in shapes]))
+    return tuple(out[k] for k in outputs)

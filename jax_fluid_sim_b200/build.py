@@ -15,8 +15,8 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 LIB = PKG / "libdgb200.so"
 SOURCES = [PKG / "csrc" / "capi.cu", PKG / "csrc" / "noalloc.cu", PKG / "csrc" / "chemistry.cu",
-           PKG / "csrc" / "raster.cu"]
-DEPENDS = sorted((PKG / "csrc").glob("*.cu*")) + [ROOT / "include" / "dgb200.h"]
+           PKG / "csrc" / "raster.cu", PKG / "csrc" / "setup.cpp"]
+DEPENDS = sorted((PKG / "csrc").glob("*.c*")) + [ROOT / "include" / "dgb200.h"]
 
 
 def nvcc():

@@ -15,6 +15,10 @@
 
 using namespace dgb;
 
+namespace dgb {
+int set_error(int code, const char* msg);
+}
+
 namespace {
 
 thread_local std::string g_error;
@@ -780,7 +784,9 @@ int dgb_plan_set_block(dgb_plan* p, int b, const dgb_block_desc* d) {
   }
   if ((rc = upload(p, d->inv_jacobian, E * Nq * 9, &B.jinv))) return rc;
   if ((rc = upload(p, d->wdet, E * Nq, &B.wdet))) return rc;
-  if ((rc = upload(p, d->inv_mass, E * Np * Np, &B.minv))) return rc;
+  // the inverse mass matrices may instead be built on the device (dgb_plan_build_inverse_mass)
+  B.minv = nullptr;
+  if (d->inv_mass && (rc = upload(p, d->inv_mass, E * Np * Np, &B.minv))) return rc;
   if ((rc = upload(p, d->length, E, &B.length))) return rc;
   if ((rc = upload(p, d->face_sample_basis, (size_t)B.Ns * Np, &B.fsB))) return rc;
   if ((rc = upload(p, d->p1_projector, Np * Np, &B.p1proj))) return rc;
@@ -884,6 +890,131 @@ int dgb_plan_set_hex_affine(dgb_plan* p, const uint8_t* affine, const double* co
   return DGB_OK;
 }
 
+// In-place inverse of the symmetric positive definite n x n matrix A in shared memory by
+// Gauss-Jordan elimination without pivoting (every pivot of an SPD matrix is positive), worked by
+// the whole block; rk, ck: n doubles of shared scratch.  Returns false, uniformly across the
+// block, at a pivot that is not positive and finite.  Ends with the block synchronised.
+__device__ bool gauss_jordan_spd(double* A, int n, double* rk, double* ck) {
+  for (int k = 0; k < n; ++k) {
+    __syncthreads();
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+      rk[t] = A[k * n + t];
+      ck[t] = A[t * n + k];
+    }
+    __syncthreads();
+    const double piv = rk[k];
+    if (!(piv > 0.0) || !isfinite(piv)) return false;   // every thread read the same pivot
+    const double r = 1.0 / piv;
+    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+      const int i = idx / n, j = idx % n;
+      if (i == k)
+        A[idx] = j == k ? r : rk[j] * r;
+      else if (j == k)
+        A[idx] = -ck[i] * r;
+      else
+        A[idx] -= ck[i] * rk[j] * r;
+    }
+  }
+  __syncthreads();
+  return true;
+}
+
+// Inverse mass matrices, one element per CTA (plan set-up; hybrid/geometry.py:181-192):
+// M_e = B^T diag(w|J|) B is formed in shared memory, each entry summed over the volume points in
+// order and mirrored so that M_e is exactly symmetric, inverted in place (gauss_jordan_spd; a
+// matrix that is not positive definite marks the element in *bad) and scaled by the sliver
+// factor min(1, V/1e-4).  Shared memory: (Np^2 + Nq + 2 Np) doubles.
+__global__ void __launch_bounds__(256) k_inverse_mass(const double* __restrict__ B, const double* __restrict__ wdet,
+                                                      const double* __restrict__ volume, int Np, int Nq,
+                                                      int transposed, double* __restrict__ minv, int* bad) {
+  extern __shared__ double sm[];
+  double* A = sm;
+  double* w = A + Np * Np;
+  double* rk = w + Nq;
+  double* ck = rk + Np;
+  const size_t e = blockIdx.x;
+  for (int q = threadIdx.x; q < Nq; q += blockDim.x) w[q] = wdet[e * Nq + q];
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < Np * Np; idx += blockDim.x) {
+    const int i = idx / Np, j = idx % Np;
+    if (i > j) continue;
+    double s = 0.0;
+    for (int q = 0; q < Nq; ++q) s += w[q] * B[q * Np + i] * B[q * Np + j];
+    A[i * Np + j] = s;
+    A[j * Np + i] = s;
+  }
+  if (!gauss_jordan_spd(A, Np, rk, ck)) {
+    if (threadIdx.x == 0) *bad = (int)e + 1;
+    return;
+  }
+  const double scale = fmin(1.0, volume[e] / 1.0e-4);
+  double* out = minv + e * Np * Np;
+  for (int idx = threadIdx.x; idx < Np * Np; idx += blockDim.x) {
+    const int i = idx / Np, j = idx % Np;
+    out[transposed ? j * Np + i : idx] = scale * A[idx];
+  }
+}
+
+// In-place inverses of a batch of SPD matrices, one per CTA (set-up).
+__global__ void __launch_bounds__(256) k_spd_inverse(double* __restrict__ mats, int n, int* bad) {
+  extern __shared__ double sm[];
+  double* A = sm;
+  double* rk = A + n * n;
+  double* ck = rk + n;
+  double* m = mats + (size_t)blockIdx.x * n * n;
+  for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) A[idx] = m[idx];
+  if (!gauss_jordan_spd(A, n, rk, ck)) {
+    if (threadIdx.x == 0) *bad = (int)blockIdx.x + 1;
+    return;
+  }
+  for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) m[idx] = A[idx];
+}
+
+int dgb_spd_inverse(double* matrices, int n, int count, int* status, void* stream) {
+  if (!matrices || !status || n < 1 || count < 0) return fail(DGB_ERR_ARGUMENT, "bad SPD-inverse argument");
+  const size_t smem = sizeof(double) * ((size_t)n * n + 2 * n);
+  if (smem > 200 * 1024) return fail(DGB_ERR_ARGUMENT, "matrix too large for the SPD-inverse kernel");
+  if (count == 0) return DGB_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CK(cudaFuncSetAttribute(k_spd_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(cudaMemsetAsync(status, 0, sizeof(int), st));
+  k_spd_inverse<<<count, 256, smem, st>>>(matrices, n, status);
+  CK(cudaGetLastError());
+  return DGB_OK;
+}
+
+int dgb_plan_build_inverse_mass(dgb_plan* p, int b, const double* volume, int transposed) {
+  if (!p || b < 0 || b >= p->dev.nblocks || !volume) return fail(DGB_ERR_ARGUMENT, "bad inverse-mass argument");
+  if (p->finalized) return fail(DGB_ERR_ARGUMENT, "plan already finalized");
+  if (!p->block_set[b]) return fail(DGB_ERR_ARGUMENT, "call dgb_plan_set_block first");
+  BlockDev& B = p->dev.blk[b];
+  if (B.minv) return fail(DGB_ERR_ARGUMENT, "block already has inverse mass matrices");
+  if (B.E == 0) return DGB_OK;
+  if (!B.B || !B.wdet) return fail(DGB_ERR_ARGUMENT, "block needs its basis and w|J| tables");
+  const size_t smem = sizeof(double) * ((size_t)B.Np * B.Np + B.Nq + 2 * B.Np);
+  if (smem > 200 * 1024) return fail(DGB_ERR_ARGUMENT, "element too large for the inverse-mass kernel");
+  int rc;
+  const double* vol = nullptr;
+  if ((rc = upload(p, volume, (size_t)B.E, &vol))) return rc;
+  double* out = nullptr;
+  if ((rc = alloc(p, (size_t)B.E * B.Np * B.Np, &out))) return rc;
+  int* bad = nullptr;
+  CK(cudaMalloc(&bad, sizeof(int)));
+  int h_bad = 0;
+  cudaError_t err = cudaMemset(bad, 0, sizeof(int));
+  if (err == cudaSuccess) err = cudaFuncSetAttribute(k_inverse_mass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err == cudaSuccess) {
+    k_inverse_mass<<<B.E, 256, smem>>>(B.B, B.wdet, vol, B.Np, B.Nq, transposed, out, bad);
+    err = cudaGetLastError();
+  }
+  if (err == cudaSuccess) err = cudaMemcpy(&h_bad, bad, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(bad);
+  if (err != cudaSuccess) return fail(DGB_ERR_CUDA, cudaGetErrorString(err));
+  if (h_bad) return fail(DGB_ERR_ARGUMENT, "degenerate element: its mass matrix is not positive definite");
+  B.minv = out;
+  return DGB_OK;
+}
+
 int dgb_plan_set_block_affine(dgb_plan* p, int b, const uint8_t* affine, const double* coef, const double* jinv,
                               const double* det, const double* ref_weights, const double* ref_inv_mass) {
   if (!p || b < 0 || b >= p->dev.nblocks || !affine || !coef || !jinv || !det || !ref_weights || !ref_inv_mass)
@@ -931,8 +1062,12 @@ int dgb_plan_finalize(dgb_plan* p) {
   if (!p) return fail(DGB_ERR_ARGUMENT, "null plan");
   const int NV = p->dev.nv;
   int rc;
-  for (int b = 0; b < p->dev.nblocks; ++b)
+  for (int b = 0; b < p->dev.nblocks; ++b) {
     if (!p->block_set[b]) return fail(DGB_ERR_ARGUMENT, "block descriptor missing");
+    if (!p->dev.blk[b].minv && p->dev.blk[b].E > 0)
+      return fail(DGB_ERR_ARGUMENT, "block without inverse mass matrices: pass inv_mass or call "
+                                    "dgb_plan_build_inverse_mass");
+  }
   for (int ft = 0; ft < 2; ++ft) {
     FaceDev& F = p->dev.face[ft];
     if (!p->face_present[ft]) continue;
@@ -1363,3 +1498,8 @@ int dgb_ssprk3_step(dgb_plan* p, const dgb_state* U, double dt, dgb_status* stat
 }
 
 }  // extern "C"
+
+namespace dgb {
+// error reporting for the host-only set-up routines compiled in other translation units
+int set_error(int code, const char* msg) { return fail(code, msg); }
+}  // namespace dgb

@@ -6,11 +6,12 @@ block, the cells and their physical tags.  Element types follow the reference's 
 (hybrid/mesh.py:11-20): tetrahedra, wedges and hexahedra of first order, and the serendipity
 hexahedron20 / wedge15, whose corner nodes come first; boundary triangles and quadrilaterals
 (and their second-order forms) keep their corners.  The complete second-order cells tetra10,
-wedge18 and hexahedron27 carry curved geometry, which the mesh takes in meshio's node order
-(``MeshSource`` cells of those names); this reader does not convert Gmsh's node order of those
-cells to meshio's, so it refuses them with NotImplementedError.
+wedge18 and hexahedron27 carry curved geometry: their nodes are reordered from Gmsh's numbering
+to meshio's (the order ``HybridMesh`` and the reference's P2 permutations take).  The
+reordering is not a stored table: each node is placed at its reference coordinates under both
+numberings (Gmsh's from its documented edge, face and centre nodes; meshio's from the
+second-order reference element's nodes and the P2 permutations) and matched by position.
 """
-
 from pathlib import Path
 
 import numpy as np
@@ -24,7 +25,49 @@ _TYPES = {
     18: ("wedge", 6, 15), 1: (None, 2, 2), 8: (None, 2, 3), 15: (None, 1, 1),
 }
 _CURVED = {11: "tetra10", 12: "hexahedron27", 13: "wedge18"}
-_ORDER = ("hexahedron", "wedge", "tetra", "quad", "triangle")
+# Gmsh's complete second-order cells: the corner nodes of the first-order cell, then one node at
+# the midpoint of each listed edge, at the centre of each listed quadrilateral face and, for the
+# hexahedron, at the cell centre (Gmsh reference manual, node ordering of the reference elements).
+_GMSH_P2 = {
+    "tetra10": ("tetra", ((0, 1), (1, 2), (2, 0), (3, 0), (3, 2), (3, 1)), (), False),
+    "wedge18": ("wedge", ((0, 1), (0, 2), (0, 3), (1, 2), (1, 4), (2, 5), (3, 4), (3, 5), (4, 5)),
+                ((0, 1, 4, 3), (0, 2, 5, 3), (1, 2, 5, 4)), False),
+    "hexahedron27": ("hexahedron", ((0, 1), (0, 3), (0, 4), (1, 2), (1, 5), (2, 3), (2, 6), (3, 7), (4, 5),
+                                    (4, 7), (5, 6), (6, 7)),
+                     ((0, 1, 2, 3), (0, 1, 5, 4), (0, 3, 7, 4), (1, 2, 6, 5), (2, 3, 7, 6), (4, 5, 6, 7)), True),
+}
+
+
+def _gmsh_p2_points(ctype):
+    from .reference import CORNERS
+    etype, edges, faces, centre = _GMSH_P2[ctype]
+    c = CORNERS[etype]
+    pts = list(c) + [0.5 * (c[a] + c[b]) for a, b in edges] + [c[list(f)].mean(axis=0) for f in faces]
+    if centre:
+        pts.append(c.mean(axis=0))
+    return np.asarray(pts)
+
+
+def _meshio_p2_points(ctype):
+    from .mesh import P2_PERMUTATIONS
+    from .reference import RefElement
+    etype = _GMSH_P2[ctype][0]
+    nodes = RefElement(etype, 2).nodes                 # reference node r is meshio node perm[r]
+    out = np.empty_like(nodes)
+    out[P2_PERMUTATIONS[ctype]] = nodes
+    return out
+
+
+def gmsh_to_meshio(ctype):
+    """Column order taking a complete second-order cell's Gmsh node list to meshio's:
+    meshio_cells = gmsh_cells[:, gmsh_to_meshio(ctype)]."""
+    g, m = _gmsh_p2_points(ctype), _meshio_p2_points(ctype)
+    d = np.linalg.norm(m[:, None, :] - g[None, :, :], axis=-1)
+    order = np.argmin(d, axis=1)
+    if len(g) != len(m) or not np.array_equal(np.sort(order), np.arange(len(g))) or d.min(axis=1).max() > 1e-12:
+        raise AssertionError(f"{ctype}: Gmsh and meshio node positions do not match one to one")
+    return order.astype(np.int64)
+_ORDER = ("hexahedron", "hexahedron27", "wedge", "wedge18", "tetra", "tetra10", "quad", "triangle")
 
 
 def _sections(lines):
@@ -55,18 +98,19 @@ def _assemble(points, node_index, records):
     grouped = {}
     for etype, phys, nodes in records:
         if etype in _CURVED:
-            raise NotImplementedError(f"{_CURVED[etype]} cells: pass them as MeshSource cells in meshio's node "
-                                      "order (this reader does not reorder Gmsh's second-order nodes)")
-        if etype not in _TYPES:
+            name = _CURVED[etype]
+            conn = node_index[nodes[:, gmsh_to_meshio(name)]]
+        elif etype in _TYPES:
+            name, corners, _ = _TYPES[etype]
+            if name is None:
+                continue
+            conn = node_index[nodes[:, :corners]]
+        else:
             raise ValueError(f"unsupported Gmsh element type {etype}")
-        name, corners, _ = _TYPES[etype]
-        if name is None:
-            continue
-        conn = node_index[nodes[:, :corners]]
         grouped.setdefault(name, ([], []))
         grouped[name][0].append(conn)
         grouped[name][1].append(np.broadcast_to(np.asarray(phys, np.int32), (len(conn),)))
-    if not any(t in grouped for t in ("hexahedron", "wedge", "tetra")):
+    if not any(t in grouped for t in ("hexahedron", "wedge", "tetra", "hexahedron27", "wedge18", "tetra10")):
         raise ValueError("Mesh contains no tetrahedron, wedge, or hexahedron")
     cells = [(t, np.concatenate(grouped[t][0]).astype(np.int32)) for t in _ORDER if t in grouped]
     phys = [np.concatenate(grouped[t][1]).astype(np.int32) for t in _ORDER if t in grouped]
@@ -152,8 +196,10 @@ def read_msh(path, periodic_map=None):
 
 
 def write_msh22(path, source):
-    """Write a ``MeshSource`` as an MSH 2.2 ASCII file (first-order cells)."""
-    codes = {"triangle": 2, "quad": 3, "tetra": 4, "hexahedron": 5, "wedge": 6}
+    """Write a ``MeshSource`` as an MSH 2.2 ASCII file (first-order cells, and complete
+    second-order cells given in meshio's node order, written in Gmsh's)."""
+    codes = {"triangle": 2, "quad": 3, "tetra": 4, "hexahedron": 5, "wedge": 6,
+             "tetra10": 11, "hexahedron27": 12, "wedge18": 13}
     out = ["$MeshFormat", "2.2 0 8", "$EndMeshFormat", "$PhysicalNames", str(len(source.field_data))]
     for name, (tag, dim) in source.field_data.items():
         out.append(f'{dim} {tag} "{name}"')
@@ -162,7 +208,12 @@ def write_msh22(path, source):
     out += ["$EndNodes", "$Elements", str(sum(len(c) for _, c in source.cells))]
     k = 1
     for (ctype, conn), phys in zip(source.cells, source.physical):
-        for cell, p in zip(np.asarray(conn), np.asarray(phys)):
+        conn = np.asarray(conn)
+        if ctype in _GMSH_P2:
+            to_gmsh = np.empty(conn.shape[1], np.int64)
+            to_gmsh[gmsh_to_meshio(ctype)] = np.arange(conn.shape[1])
+            conn = conn[:, to_gmsh]
+        for cell, p in zip(conn, np.asarray(phys)):
             out.append(f"{k} {codes[ctype]} 2 {int(p)} {int(p)} " + " ".join(str(int(v) + 1) for v in cell))
             k += 1
     out.append("$EndElements")

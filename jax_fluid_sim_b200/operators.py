@@ -28,7 +28,12 @@ class NativePlan:
     PRECISIONS = {"float64": 0, "mixed": 1}
 
     def __init__(self, plan: Plan, solver, viscous: bool, br2: float, sum_factorised=None, precision="float64",
-                 affine=True):
+                 affine=True, inverse_mass="device"):
+        """``inverse_mass``: "device" builds the inverse mass matrices on the GPU from w|det J|
+        (``dgb_plan_build_inverse_mass``); "host" uploads the host plan's copy (numpy), the
+        set-up the device build is tested against."""
+        if inverse_mass not in ("device", "host"):
+            raise ValueError('inverse_mass must be "device" or "host"')
         L = N.lib()
         if precision not in self.PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(self.PRECISIONS)}")
@@ -60,12 +65,13 @@ class NativePlan:
         if sum_factorised is None:
             sum_factorised = single_hex
         for b, bp in enumerate(plan.blocks):
-            # the sum-factorised kernels stream M^-1 transposed (coalesced across nodes)
-            minv = np.ascontiguousarray(np.swapaxes(bp.minv, 1, 2)) if sum_factorised else bp.minv
             arrays = dict(basis=N.as_f64(bp.ref.B), basis_grad=N.as_f64(bp.ref.dB),
-                          inv_jacobian=N.as_f64(bp.jinv), wdet=N.as_f64(bp.wdet), inv_mass=N.as_f64(minv),
+                          inv_jacobian=N.as_f64(bp.jinv), wdet=N.as_f64(bp.wdet),
                           length=N.as_f64(bp.length), face_sample_basis=N.as_f64(bp.face_sample_B),
                           p1_projector=N.as_f64(bp.p1_projector))
+            if inverse_mass == "host":
+                # the sum-factorised kernels stream M^-1 transposed (coalesced across nodes)
+                arrays["inv_mass"] = N.as_f64(np.swapaxes(bp.minv, 1, 2) if sum_factorised else bp.minv)
             ef = N.as_i32(bp.elem_face)
             keep += list(arrays.values()) + [ef]
             d = N.BlockDesc(element_type=TYPE_ID[bp.etype], num_elements=bp.E, num_nodes=bp.Np, num_qp=bp.Nq,
@@ -74,6 +80,9 @@ class NativePlan:
             for k, a in arrays.items():
                 setattr(d, k, N.dptr(a))
             N.check(L.dgb_plan_set_block(handle, b, ctypes.byref(d)))
+            if inverse_mass == "device":
+                volume = N.as_f64(bp.volume)
+                N.check(L.dgb_plan_build_inverse_mass(handle, b, N.dptr(volume), int(bool(sum_factorised))))
             if affine and not sum_factorised:
                 aff, coef, ajinv, det, wref, mref_inv = block_affine_data(bp)
                 aff = np.ascontiguousarray(aff, np.uint8)

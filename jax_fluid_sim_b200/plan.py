@@ -1,18 +1,23 @@
 """Host-side construction of the device plan (all tables the kernels read).
 
-Geometry follows the reference's isoparametric, first-order mapping
-(``hybrid/geometry.py:139-362``): per element and volume point the inverse
-Jacobian and w|det J|; per element the dense inverse mass matrix with the
-sliver scale ``min(1, V/1e-4)``; per face and face point the unit normal and
-w*dA from the owner mapping; per face side the reference points (owner:
+Geometry follows the reference's isoparametric mapping (``hybrid/geometry.py:139-362``;
+first order, or second order for curved cells): per element and volume point the inverse
+Jacobian and w|det J|; per element the dense inverse mass matrix with the sliver scale
+``min(1, V/1e-4)``; per face and face point the unit normal and w*dA from the owner mapping; per face side the reference points (owner:
 its local-face corners, neighbour: corners matched by node id), from which a
 small set of distinct "trace codes" per element type is built.  Each code owns
 a trace matrix (basis at the side's face points) and its reference-gradient
 counterpart.  Faces are stored per face type (triangle, quad).
+
+The per-point metrics are computed by ``dgb_map_metrics`` on the host cores in threads, one
+geometry-basis table per point set (a face group's points are shared by all its faces).  The
+inverse mass matrices are not formed here: the operator builds them on the device from w|det J|
+(``dgb_plan_build_inverse_mass``); ``ElementPlan.minv`` forms a host copy only when read.
 """
 
 import numpy as np
 
+from . import _native as N
 from .mesh import HybridMesh
 from .reference import CORNERS, FACE_TYPE_ID, LOCAL_FACES, TYPE_ID, RefElement, face_quadrature, gauss01
 
@@ -25,13 +30,18 @@ def _p1_jacobian(etype, xyz, points):
     return np.einsum("...kd,...kr->...dr", xyz, g)
 
 
-def _geo_jacobian(geo, xyz, points):
-    """J[..., d, r] = sum_k x_k[d] dN_k/dxi_r with the block's geometry basis (first or second order)."""
-    return np.einsum("...kd,...kr->...dr", xyz, geo.basis_gradients(points))
-
-
 class ElementPlan:
-    pass
+    """Arrays of one element block.  ``minv`` (the dense inverse mass matrices, E * Np^2 values)
+    is formed on the host only when read: the device plan builds its own copy from ``wdet``
+    (``dgb_plan_build_inverse_mass``)."""
+
+    @property
+    def minv(self):
+        if getattr(self, "_minv", None) is None:
+            m = _inverse_mass(self.wdet, self.ref.B)
+            m *= np.minimum(1.0, self.volume / 1.0e-4)[:, None, None]
+            self._minv = m
+        return self._minv
 
 
 class FacePlan:
@@ -58,18 +68,15 @@ class Plan:
     def _element_plan(self, block, k):
         ref = RefElement(block.element_type, self.degree)
         geo, xyz = self.mesh.geometry(block)                     # (E, n_geometry_nodes, 3)
-        J = _geo_jacobian(geo, xyz[:, None, :, :], ref.points[None])                # (E, Nq, 3, 3)
-        det = np.linalg.det(J)
-        jinv = np.linalg.inv(J)                                   # [r][d] = dxi_r/dx_d
-        wdet = ref.weights[None, :] * np.abs(det)
+        # jinv[r][d] = dxi_r/dx_d, wdet = w |det J| at the volume points (host threads)
+        det, jinv, wdet = N.map_metrics(xyz, geo.basis_gradients(ref.points), weights=ref.weights,
+                                        outputs=("det", "inv_jacobian", "wdet"))
         vol = wdet.sum(axis=1)
-        minv = _inverse_mass(wdet, ref.B)
-        minv *= np.minimum(1.0, vol / 1.0e-4)[:, None, None]
         p = ElementPlan()
         p.etype, p.type_id, p.ref = block.element_type, TYPE_ID[block.element_type], ref
         p.E, p.Np, p.Nq = len(block.connectivity), ref.np, ref.nq
         p.nlf = len(LOCAL_FACES[block.element_type])
-        p.jinv, p.wdet, p.minv, p.volume = jinv, wdet, minv, vol
+        p.jinv, p.wdet, p.volume = jinv, wdet, vol
         p.node_xyz = np.einsum("qi,eid->eqd", geo.basis(ref.nodes), xyz)
         p.affine = bool(np.all(np.ptp(det, axis=1) <= 1e-13 * np.abs(det).max(axis=1)))
         return p
@@ -97,10 +104,14 @@ class Plan:
         nbr_pts = np.full((F, nq, 3), np.nan)
         ocode = np.empty(F, np.int32)
         ncode = np.full(F, -1, np.int32)
-        tu_ref = np.empty((F, nq, 3))
-        tv_ref = np.empty((F, nq, 3))
-        # owner side: one point set per (owner type, local face)
+        normals = np.empty((F, nq, 3))
+        weights = np.empty((F, nq))
+        jinv_side = np.zeros((F, 2, nq, 3, 3))
+        measure = 0.5 if ftype == "triangle" else 1.0
+        # Owner side: one point set per (owner type, local face).  The metrics come from the owner
+        # mapping (geometry.py:299-353), with the geometry basis evaluated once per point set.
         for b, block in enumerate(mesh.element_blocks):
+            geo, xyz_b = mesh.geometry(block)
             for lf, loc in enumerate(LOCAL_FACES[block.element_type]):
                 sel = np.flatnonzero((fb.owner_block == b) & (fb.owner_face == lf))
                 if not len(sel):
@@ -118,7 +129,12 @@ class Plan:
                     c0, c1, c2, c3 = corners
                     tu = -(1 - v)[:, None] * c0 + (1 - v)[:, None] * c1 + v[:, None] * c2 - v[:, None] * c3
                     tv = -(1 - u)[:, None] * c0 - u[:, None] * c1 + u[:, None] * c2 + (1 - u)[:, None] * c3
-                tu_ref[sel], tv_ref[sel] = tu, tv
+                # unit normals and w dA from the owner map's tangents J t_u x J t_v, oriented like
+                # the face's corner normal (host threads)
+                normals[sel], weights[sel], jinv_side[sel, 0] = N.map_metrics(
+                    xyz_b, geo.basis_gradients(pts), index=fb.owner_local[sel], weights=nweights * measure,
+                    tangents=np.stack([tu, tv], axis=1), orientation=fb.normals[sel],
+                    outputs=("normals", "area_weights", "inv_jacobian"))
         # neighbour side: corners matched by canonical node id (geometry.py:205-224)
         internal = np.flatnonzero(fb.neighbor_block >= 0)
         if len(internal):
@@ -131,38 +147,17 @@ class Plan:
             uniq, inverse = np.unique(keys, axis=0, return_inverse=True)
             inverse = inverse.ravel()
             for u, (b, lf, *pm) in enumerate(uniq.tolist()):
-                etype = mesh.element_blocks[b].element_type
+                block = mesh.element_blocks[b]
+                etype = block.element_type
                 corners = CORNERS[etype][list(LOCAL_FACES[etype][lf])][list(pm)]
                 pts = shapes @ corners
                 faces = internal[inverse == u]
                 nbr_pts[faces] = pts
                 ncode[faces] = self._code(etype, ftype, pts)
+                geo, xyz_b = mesh.geometry(block)
+                jinv_side[faces, 1] = N.map_metrics(xyz_b, geo.basis_gradients(pts), index=fb.neighbor_local[faces],
+                                                    outputs=("inv_jacobian",))[0]
         fp.own_pts, fp.nbr_pts, fp.ocode, fp.ncode = own_pts, nbr_pts, ocode, ncode
-        # metrics from the owner mapping (geometry.py:299-353)
-        normals = np.empty((F, nq, 3))
-        weights = np.empty((F, nq))
-        jinv_side = np.zeros((F, 2, nq, 3, 3))
-        measure = 0.5 if ftype == "triangle" else 1.0
-        for b, block in enumerate(mesh.element_blocks):
-            sel = np.flatnonzero(fb.owner_block == b)
-            geo, xyz_b = mesh.geometry(block)
-            if len(sel):
-                xyz = xyz_b[fb.owner_local[sel]]
-                J = _geo_jacobian(geo, xyz[:, None], own_pts[sel])
-                tu = np.einsum("fqdr,fqr->fqd", J, tu_ref[sel])
-                tv = np.einsum("fqdr,fqr->fqd", J, tv_ref[sel])
-                area = np.cross(tu, tv)
-                sign = np.where(np.sum(area * fb.normals[sel][:, None, :], axis=-1) >= 0, 1.0, -1.0)
-                area = area * sign[..., None]
-                mag = np.linalg.norm(area, axis=-1)
-                normals[sel] = area / mag[..., None]
-                weights[sel] = nweights[None, :] * measure * mag
-                jinv_side[sel, 0] = np.linalg.inv(J)
-            seln = np.flatnonzero(fb.neighbor_block == b)
-            if len(seln):
-                xyz = xyz_b[fb.neighbor_local[seln]]
-                J = _geo_jacobian(geo, xyz[:, None], nbr_pts[seln])
-                jinv_side[seln, 1] = np.linalg.inv(J)
         fp.normals, fp.weights, fp.jinv_side = normals, weights, jinv_side
         return fp
 
@@ -224,24 +219,10 @@ class Plan:
 
 
 def _inverse_mass(wdet, B, chunk=8192):
-    """Per-element inverse of M_e = B^T diag(w|J|) B (hybrid/geometry.py:181-188).
-
-    Float64 throughout; large meshes are inverted in chunks on the GPU (torch.linalg,
-    set-up only) when one is present, else with numpy."""
+    """Per-element inverse of M_e = B^T diag(w|J|) B (hybrid/geometry.py:181-188), float64, on the
+    host.  The operators build the device copy with ``dgb_plan_build_inverse_mass`` instead."""
     E = wdet.shape[0]
     out = np.empty((E, B.shape[1], B.shape[1]))
-    try:
-        import torch
-        use_gpu = torch.cuda.is_available() and E > 4096
-    except Exception:
-        use_gpu = False
-    if use_gpu:
-        Bt = torch.as_tensor(B, device="cuda")
-        for s in range(0, E, chunk):
-            w = torch.as_tensor(wdet[s:s + chunk], device="cuda")
-            M = torch.einsum("eq,qi,qj->eij", w, Bt, Bt)
-            out[s:s + chunk] = torch.linalg.inv(M).cpu().numpy()
-        return out
     for s in range(0, E, chunk):
         M = np.einsum("eq,qi,qj->eij", wdet[s:s + chunk], B, B, optimize=True)
         out[s:s + chunk] = np.linalg.inv(M)

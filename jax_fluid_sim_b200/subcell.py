@@ -16,8 +16,11 @@ written.  ``coupling="reference"`` reproduces that; ``coupling="subcell"``
 uses the subcell owning each subface.
 """
 
+import ctypes
+
 import numpy as np
 
+from . import _native as N
 from .reference import LOCAL_FACES, RefElement, volume_quadrature
 
 DIVISIONS = 4
@@ -151,7 +154,6 @@ class SubcellBlockPlan:
         mp, rw = _subcell_rule(rs)
         flat = mp.reshape(-1, 3)
         sb = ref.basis(flat).reshape(rs.count, mp.shape[1], -1)
-        gg = geo1.basis_gradients(flat).reshape(rs.count, mp.shape[1], -1, 3)
         vb = geo1.basis(rs.vertices)
         E = len(block.connectivity)
         S, Np = rs.count, ref.np
@@ -165,32 +167,25 @@ class SubcellBlockPlan:
         self.boundary_normals = np.empty((E, NB, 3))
         self.boundary_areas = np.empty((E, NB))
         self.boundary_centers = np.empty((E, NB, 3))
-        try:
-            import torch
-            dev = "cuda" if torch.cuda.is_available() and E > 2048 else None
-        except Exception:
-            dev = None
+        gflat = geo1.basis_gradients(flat)                 # (S * Qs, n, 3)
+        Qs = mp.shape[1]
         for s0 in range(0, E, chunk):
             xyz = xyz_all[s0:s0 + chunk]
+            e = len(xyz)
             pv = np.einsum("vi,eid->evd", vb, xyz)
             cen = pv[:, rs.cells].mean(axis=2)
-            if dev is None:
-                jac = np.einsum("eir,sqij->esqrj", xyz, gg)
-                pw = np.abs(np.linalg.det(jac)) * rw[None]
-                vol = pw.sum(axis=-1)
-                proj = np.einsum("esq,sqi->esi", pw, sb) / vol[..., None]
-                gram = np.einsum("esi,es,esj->eij", proj, vol, proj)
-                rec = np.einsum("eij,esj,es->eis", np.linalg.inv(gram), proj, vol)
-            else:   # same float64 arithmetic on the GPU (set-up only)
-                t = lambda a: torch.as_tensor(a, device=dev)
-                jac = torch.einsum("eir,sqij->esqrj", t(xyz), t(gg))
-                pw = torch.abs(torch.linalg.det(jac)) * t(rw)[None]
-                volt = pw.sum(dim=-1)
-                projt = torch.einsum("esq,sqi->esi", pw, t(sb)) / volt[..., None]
-                gram = torch.einsum("esi,es,esj->eij", projt, volt, projt)
-                rect = torch.einsum("eij,esj,es->eis", torch.linalg.inv(gram), projt, volt)
-                vol, proj, rec = volt.cpu().numpy(), projt.cpu().numpy(), rect.cpu().numpy()
-            sl = slice(s0, s0 + len(xyz))
+            # subcell.py:308-323: |det J| at the mapped subcell points (host threads), subcell
+            # volumes and the metric-weighted projection; matrix products per subcell / element
+            det = N.map_metrics(xyz, gflat, outputs=("det",))[0]
+            pw = np.abs(det).reshape(e, S, Qs) * rw[None]
+            vol = pw.sum(axis=-1)
+            # (contiguous operands, so that each product of the stack goes to BLAS)
+            proj = np.matmul(np.ascontiguousarray(pw.transpose(1, 0, 2)), sb).transpose(1, 0, 2) / vol[..., None]
+            # subcell.py:324-334: volume-weighted least-squares left inverse
+            wpT = np.ascontiguousarray((proj * vol[..., None]).transpose(0, 2, 1))     # (e, Np, S)
+            gram = np.matmul(wpT, proj)
+            rec = np.matmul(_spd_inverse(gram), wpT)
+            sl = slice(s0, s0 + e)
             self.projection[sl], self.reconstruction[sl], self.volumes[sl], self.centers[sl] = proj, rec, vol, cen
             n, a, _ = _face_metrics(pv, cen, rs.internal_faces, rs.internal_owner, rs.internal_neighbor)
             self.internal_normals[sl], self.internal_areas[sl] = n, a
@@ -199,17 +194,39 @@ class SubcellBlockPlan:
         self.boundary_basis = ref.basis(rs.boundary_reference_centers)    # [NB][Np]
 
 
+def _spd_inverse(gram):
+    """Inverses of a stack of SPD matrices: on the GPU (``dgb_spd_inverse``) when one is present,
+    else with numpy (set-up only)."""
+    import torch
+    if not torch.cuda.is_available() or len(gram) < 256:
+        return np.linalg.inv(gram)
+    t = torch.as_tensor(np.ascontiguousarray(gram), device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    N.check(N.lib().dgb_spd_inverse(ctypes.c_void_p(t.data_ptr()), gram.shape[1], len(gram),
+                                    ctypes.c_void_p(status.data_ptr()),
+                                    ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    if int(status.item()):
+        raise ValueError(f"subcell Gram matrix {int(status.item()) - 1} of the chunk is not positive definite")
+    return t.cpu().numpy()
+
+
 def _face_metrics(pv, cen, faces, owners, neighbors):
-    """Area vectors of subcell faces oriented owner -> neighbour (or outward), unit normals."""
-    av, fc = [], []
-    for face in faces:
-        p = pv[:, np.asarray(face)]
-        a = 0.5 * np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0])
-        if len(face) == 4:
-            a = a + 0.5 * np.cross(p[:, 2] - p[:, 0], p[:, 3] - p[:, 0])
-        av.append(a)
-        fc.append(p.mean(axis=1))
-    av, fc = np.stack(av, axis=1), np.stack(fc, axis=1)
+    """Area vectors of subcell faces oriented owner -> neighbour (or outward), unit normals
+    (subcell.py:336-360); triangles a = (p1 - p0) x (p2 - p0) / 2, quadrilaterals as two triangles
+    about p0.  Faces of one vertex count are handled together."""
+    nf = len(faces)
+    av = np.empty((pv.shape[0], nf, 3))
+    fc = np.empty((pv.shape[0], nf, 3))
+    for k in (3, 4):
+        sel = [i for i, f in enumerate(faces) if len(f) == k]
+        if not sel:
+            continue
+        p = pv[:, np.asarray([faces[i] for i in sel])]                 # (e, m, k, 3)
+        a = 0.5 * np.cross(p[:, :, 1] - p[:, :, 0], p[:, :, 2] - p[:, :, 0])
+        if k == 4:
+            a = a + 0.5 * np.cross(p[:, :, 2] - p[:, :, 0], p[:, :, 3] - p[:, :, 0])
+        av[:, sel] = a
+        fc[:, sel] = p.mean(axis=2)
     oc = cen[:, owners]
     d = fc - oc if neighbors is None else cen[:, neighbors] - oc
     av = av * np.where(np.sum(av * d, axis=-1) >= 0.0, 1.0, -1.0)[..., None]

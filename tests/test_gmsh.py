@@ -1,6 +1,6 @@
 """Gmsh MSH 2.2 / 4.1 ASCII reading: a written file reads back to the same mesh (points, cells,
 physical tags and names, hence the same face tables), hand-written 4.1 and second-order files
-parse, and curved cells are refused."""
+parse, and complete second-order cells come back in meshio's node order."""
 
 import numpy as np
 import pytest
@@ -95,7 +95,7 @@ def test_msh41_entities_and_blocks(tmp_path):
 
 
 def test_second_order_cells(tmp_path):
-    """Serendipity hexahedron20 keeps its corners; a complete hexahedron27 is refused."""
+    """Serendipity hexahedron20 keeps its corners."""
     pts = "\n".join(f"{i + 1} {x} {y} {z}" for i, (x, y, z) in enumerate(
         [(a, b, c) for c in (0, 1, 2) for b in (0, 1, 2) for a in (0, 1, 2)]))
     corners = [1, 3, 9, 7, 19, 21, 27, 25]
@@ -106,10 +106,69 @@ def test_second_order_cells(tmp_path):
     path.write_text(body)
     src = gmsh.read_msh(path)
     np.testing.assert_array_equal(src.cells[0][1][0], np.asarray(corners) - 1)
-    path.write_text(body.replace(" 17 2 1 1 ", " 12 2 1 1 ").replace(" ".join(map(str, hex20)),
-                                                                     " ".join(map(str, range(1, 28)))))
-    with pytest.raises(NotImplementedError):
-        gmsh.read_msh(path)
+
+
+def _p2_node_deviation(points, meshio_cells):
+    """Largest distance, relative to the cell's bounding-box diagonal, between a hexahedron27's
+    nodes (taken to the reference element's order by the P2 permutation) and the trilinear map of
+    its corners at the reference nodes: small for any cell of a mildly curved mesh, about half the
+    cell when the node order is wrong."""
+    from jax_fluid_sim_b200.mesh import P2_PERMUTATIONS
+    from jax_fluid_sim_b200.reference import RefElement
+    ref1, ref2 = RefElement("hexahedron", 1), RefElement("hexahedron", 2)
+    xyz = points[meshio_cells[:, P2_PERMUTATIONS["hexahedron27"]]]
+    corners = points[meshio_cells[:, :8]]
+    linear = np.einsum("ri,eid->erd", ref1.basis(ref2.nodes), corners)
+    size = np.linalg.norm(corners.max(axis=1) - corners.min(axis=1), axis=-1)
+    return float((np.linalg.norm(xyz - linear, axis=-1).max(axis=1) / size).max())
+
+
+@pytest.mark.parametrize("name", ["cylinder", "sphere"])
+def test_gmsh_hexahedron27_node_order(name):
+    """Hexahedron27 cells written by Gmsh (extracted from the reference's own meshes by
+    tests/golden/make_gmsh_p2.py) read into meshio's order: every node then sits where the
+    reference element puts it (within the cell's curvature), the Jacobian is positive, and the
+    unconverted Gmsh order fails the same check."""
+    from pathlib import Path
+    from jax_fluid_sim_b200.mesh import P2_PERMUTATIONS
+    from jax_fluid_sim_b200.reference import RefElement
+    path = Path(__file__).parent / "golden" / f"gmsh_hex27_{name}.msh"
+    src = gmsh.read_msh(path)
+    (ctype, cells), = src.cells
+    assert ctype == "hexahedron27" and cells.shape == (24, 27)
+    assert _p2_node_deviation(src.points, cells) < 0.01
+    ref2 = RefElement("hexahedron", 2)
+    J = np.einsum("eid,qir->eqdr", src.points[cells[:, P2_PERMUTATIONS["hexahedron27"]]],
+                  ref2.basis_gradients(ref2.points))
+    assert np.linalg.det(J).min() > 0.0
+    raw = np.empty_like(cells)
+    raw[:, gmsh.gmsh_to_meshio("hexahedron27")] = cells       # undo the reordering
+    assert _p2_node_deviation(src.points, raw) > 0.3
+
+
+def test_gmsh_second_order_orders_are_permutations():
+    """The Gmsh -> meshio column orders are permutations that keep the corners in place; the
+    wedge18 order is the identity (the reference's P2 table takes wedge18 in Gmsh's numbering)."""
+    for ctype, n in (("tetra10", 10), ("wedge18", 18), ("hexahedron27", 27)):
+        order = gmsh.gmsh_to_meshio(ctype)
+        np.testing.assert_array_equal(np.sort(order), np.arange(n))
+        corners = {"tetra10": 4, "wedge18": 6, "hexahedron27": 8}[ctype]
+        np.testing.assert_array_equal(order[:corners], np.arange(corners))
+    np.testing.assert_array_equal(gmsh.gmsh_to_meshio("wedge18"), np.arange(18))
+
+
+def test_curved_round_trip_and_geometry(tmp_path):
+    """A curved hexahedron27 box written as MSH 2.2 (Gmsh order) reads back to the same cells in
+    meshio order, and the mesh built from the file has the same element geometry."""
+    src = meshgen.curved_box()
+    path = tmp_path / "curved.msh"
+    gmsh.write_msh22(path, src)
+    back = gmsh.read_msh(path)
+    volume = lambda m: [np.asarray(c) for t, c in m.cells if t == "hexahedron27"]
+    np.testing.assert_array_equal(volume(back)[0], volume(src)[0])
+    ma, mb = HybridMesh(src), HybridMesh(back)
+    np.testing.assert_array_equal(ma.geometry(ma.element_blocks[0])[1], mb.geometry(mb.element_blocks[0])[1])
+    _same_faces(src, back)
 
 
 def test_hybrid_mesh_and_solver_take_a_path(tmp_path):
