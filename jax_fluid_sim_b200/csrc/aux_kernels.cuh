@@ -18,6 +18,7 @@ struct LimiterConst {
   double density_floor, pressure_floor, relative_floor;   // positivity limiter
   double adm_density_floor, adm_pressure_floor;           // integrator admissibility
   double sensor_threshold;
+  double lebesgue;   // max over the limiter's sample points of sum_i |B_i(x)|; 0: no nodal certificate
 };
 
 template <int NV>
@@ -25,6 +26,82 @@ __device__ __forceinline__ double pressure_of(const Physics& ph, const double* U
   const double srho = fmax(U[0], kRhoFloor);
   const double ke = 0.5 * (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / srho;
   return (ph.gamma - 1.0) * (U[4] - ke);
+}
+
+// Certificate, from the nodal values alone, that density and pressure are admissible at every
+// limiter sample of the element and at its cell mean.  A sample u(x) = sum_i B_i(x) U_i, with
+// sum_i B_i = 1, obeys |u(x) - c| <= L h, for c and h the midpoint and half-range of the nodal
+// values and L the largest sum_i |B_i| over the sample points (their Lebesgue constant).  Intervals of
+// rho, m and E then bound rho and p = (gamma - 1)(E - |m|^2 / 2 rho) from below at every sample.
+// The cell mean is a positive combination of samples, so its rho lies in the same interval and
+// its p is at least the smallest sample p (p is concave in the conserved variables).  The margins
+// tol_r and tol_p cover the rounding of the computed samples many times over.  True when
+//   rho_lo - tol_r >= max(rho_floor, rel (rho_hi + tol_r)),
+//   p_lo - tol_p >= max(p_floor, rel pmean_hi + tol_p),
+// with rho_lo >= 1e-3 rho_hi, so that the relative rounding of |m|^2 / rho stays small.
+// A non-finite nodal value gives false.  Every thread returns the same value.
+template <int NV>
+__device__ bool nodal_certificate(const double* __restrict__ Ug, int Np, const Physics& ph, double L,
+                                  double rho_floor, double p_floor, double rel) {
+  __shared__ double red[10][kThreads / 32];
+  double lo[5], hi[5];
+#pragma unroll
+  for (int v = 0; v < 5; ++v) {
+    lo[v] = INFINITY;
+    hi[v] = -INFINITY;
+  }
+  bool fin = true;
+  for (int l = threadIdx.x; l < Np; l += blockDim.x) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      const double x = Ug[l * NV + v];
+      fin &= isfinite(x);
+      if (v < 5) {
+        lo[v] = fmin(lo[v], x);
+        hi[v] = fmax(hi[v], x);
+      }
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < 5; ++v)
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[v] = fmin(lo[v], __shfl_xor_sync(0xffffffff, lo[v], o));
+      hi[v] = fmax(hi[v], __shfl_xor_sync(0xffffffff, hi[v], o));
+    }
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      red[v][threadIdx.x >> 5] = lo[v];
+      red[5 + v][threadIdx.x >> 5] = hi[v];
+    }
+  const bool all_finite = __syncthreads_and(fin);
+  if (!all_finite || !(L >= 1.0)) return false;
+  double a[5], b[5];
+#pragma unroll
+  for (int v = 0; v < 5; ++v) {
+    double mn = red[v][0], mx = red[5 + v][0];
+    for (int k = 1; k < kThreads / 32; ++k) {
+      mn = fmin(mn, red[v][k]);
+      mx = fmax(mx, red[5 + v][k]);
+    }
+    const double c = 0.5 * (mn + mx), h = 0.5 * (mx - mn);
+    a[v] = c - L * h;
+    b[v] = c + L * h;
+  }
+  const double tol_r = 1.0e-12 * L * fmax(fabs(a[0]), fabs(b[0]));
+  if (!(a[0] - tol_r > 0.0) || !(a[0] >= 1.0e-3 * b[0])) return false;
+  double m2hi = 0.0, m2lo = 0.0;
+#pragma unroll
+  for (int d = 1; d <= 3; ++d) {
+    m2hi += fmax(a[d] * a[d], b[d] * b[d]);
+    m2lo += (a[d] <= 0.0 && b[d] >= 0.0) ? 0.0 : fmin(a[d] * a[d], b[d] * b[d]);
+  }
+  const double g1 = ph.gamma - 1.0;
+  const double ke_hi = 0.5 * m2hi / a[0], ke_lo = 0.5 * m2lo / b[0];
+  const double p_lo = g1 * (a[4] - ke_hi), pmean_hi = g1 * (b[4] - ke_lo);
+  const double tol_p = 1.0e-6 * g1 * (L * fmax(fabs(a[4]), fabs(b[4])) + ke_hi);
+  return (a[0] - tol_r >= fmax(rho_floor, rel * (b[0] + tol_r))) &&
+         (p_lo - tol_p >= fmax(p_floor, rel * pmean_hi + tol_p));
 }
 
 // samples = [U at nodes; B U at volume points; Bfs U at face points]  -> S[Ns_total][NV]
@@ -94,6 +171,8 @@ __global__ void __launch_bounds__(kThreads) k_positivity(const DevPlan P, const 
   double* U = smem;
   double* Smp = U + Np * NV;
   double* Ug = S.b[b] + (size_t)e * Np * NV;
+  // nodal certificate of theta = 1: the state stays as it is (mean + 1 * (U - mean) is U to rounding)
+  if (nodal_certificate<NV>(Ug, Np, P.ph, B.lebesgue, L.density_floor, L.pressure_floor, L.relative_floor)) return;
   for (int i = threadIdx.x; i < Np * NV; i += blockDim.x) U[i] = Ug[i];
   __syncthreads();
   build_samples<NV>(B, U, Smp);
@@ -206,9 +285,11 @@ __global__ void __launch_bounds__(kThreads) k_troubled(const DevPlan P, const St
   double* Smp = U + Np * NV;
   double* Mon = Smp + Nt * NV;   // [Np][2] monitored (rho, p)
   const double* Ug = S.b[b] + (size_t)e * Np * NV;
+  // nodal certificate of admissible samples and mean: then only the sensor needs computing
+  const bool certified = nodal_certificate<NV>(Ug, Np, P.ph, B.lebesgue, L.density_floor, L.pressure_floor, 0.0);
   for (int i = threadIdx.x; i < Np * NV; i += blockDim.x) U[i] = Ug[i];
   __syncthreads();
-  build_samples<NV>(B, U, Smp);
+  if (!certified) build_samples<NV>(B, U, Smp);
   for (int i = threadIdx.x; i < Np; i += blockDim.x) {
     double W[NV];
     primitive<NV>(P.ph, U + i * NV, W);
@@ -216,7 +297,7 @@ __global__ void __launch_bounds__(kThreads) k_troubled(const DevPlan P, const St
     Mon[i * 2 + 1] = W[4];
   }
   __syncthreads();
-  cell_mean<NV>(B, e, Smp + Np * NV, mean);
+  if (!certified) cell_mean<NV>(B, e, Smp + Np * NV, mean);
   // sensor: sum_i (m - Pi m)^2 / max(sum_i m^2, 1e-12), max over (rho, p)
   double hi0 = 0.0, hi1 = 0.0, sc0 = 0.0, sc1 = 0.0;
   if (P.degree >= 2) {
@@ -248,7 +329,7 @@ __global__ void __launch_bounds__(kThreads) k_troubled(const DevPlan P, const St
   __syncthreads();
   // invalid samples (including the cell mean)
   bool bad = false;
-  for (int r = threadIdx.x; r <= Nt; r += blockDim.x) {
+  for (int r = threadIdx.x; r <= (certified ? -1 : Nt); r += blockDim.x) {
     const double* s = r < Nt ? Smp + r * NV : mean;
     double W[NV];
     primitive<NV>(P.ph, s, W);

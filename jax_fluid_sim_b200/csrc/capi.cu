@@ -782,6 +782,18 @@ int dgb_plan_set_block(dgb_plan* p, int b, const dgb_block_desc* d) {
     if ((rc = upload(p, dq.data(), dq.size(), &B.dBq))) return rc;
     if ((rc = upload(p, di.data(), di.size(), &B.dBi))) return rc;
   }
+  // Lebesgue constant of the limiter's sample set (nodes, volume points, face samples)
+  B.lebesgue = 1.0;
+  for (int tbl = 0; tbl < 2; ++tbl) {
+    const double* rows = tbl == 0 ? d->basis : d->face_sample_basis;
+    const size_t nrows = tbl == 0 ? Nq : (size_t)B.Ns;
+    if (!rows) continue;
+    for (size_t r = 0; r < nrows; ++r) {
+      double a = 0.0;
+      for (size_t i = 0; i < Np; ++i) a += fabs(rows[r * Np + i]);
+      B.lebesgue = fmax(B.lebesgue, a);
+    }
+  }
   if ((rc = upload(p, d->inv_jacobian, E * Nq * 9, &B.jinv))) return rc;
   if ((rc = upload(p, d->wdet, E * Nq, &B.wdet))) return rc;
   // the inverse mass matrices may instead be built on the device (dgb_plan_build_inverse_mass)
@@ -869,6 +881,23 @@ int dgb_plan_set_hex(dgb_plan* p, const double* line_tables, const int32_t* lex2
   memcpy(t.w1, src, sizeof(t.w1)); src += 5;
   memcpy(t.p1d, src, sizeof(t.p1d)); src += 16;
   for (int i = 0; i < 64; ++i) t.lex2node[i] = lex2node[i];
+  // Lebesgue constant of the limiter's samples: a volume point is a product of three 1-D rows of
+  // bq, a face point of two rows of bf (its third coordinate is a node), a node gives 1
+  {
+    const int N = p->dev.degree + 1, Q = p->dev.degree == 1 ? 2 : (p->dev.degree == 2 ? 3 : 5);
+    double lq = 0.0, lf = 0.0;
+    for (int q = 0; q < Q; ++q) {
+      double a = 0.0;
+      for (int j = 0; j < N; ++j) a += fabs(t.bq[q * N + j]);   // [Q][N], packed
+      lq = fmax(lq, a);
+    }
+    for (int q = 0; q < qf; ++q) {
+      double a = 0.0;
+      for (int j = 0; j < N; ++j) a += fabs(t.bf[q * N + j]);   // [QF][N], packed
+      lf = fmax(lf, a);
+    }
+    p->lim.lebesgue = fmax(1.0, fmax(lq * lq * lq, lf * lf));
+  }
   int rc;
   if ((rc = upload(p, perm, (size_t)num_codes * face_points, &p->hex_codes.perm))) return rc;
   p->hex = true;

@@ -35,6 +35,7 @@ struct BlockDev {
   const double* jinv;     // [E][Nq][9]
   const double* wdet;     // [E][Nq]
   const double* minv;     // [E][Np][Np]
+  double lebesgue;        // max over the limiter samples (nodes, volume, face) of sum_i |B_i|
   const double* length;   // [E]
   const double* fsB;      // [Ns][Np]
   const double* p1proj;   // [Np][Np]

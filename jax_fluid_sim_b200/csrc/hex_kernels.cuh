@@ -832,8 +832,13 @@ __global__ void __launch_bounds__(kThreads) k_hex_positivity(const DevPlan P_, c
   __shared__ double sh_upper;
   const BlockDev& B = P_.blk[b];
   const int e = blockIdx.x;
-  load_tables<P>(tables, tb);
   double* Ug = S.b[b] + (size_t)e * N3 * NV;
+  // An element whose nodal values certify admissible samples at theta = 1 keeps its state: the
+  // reference's mean + 1 * (U - mean) equals U to rounding, so nothing is written.
+  if (nodal_certificate<NV>(Ug, N3, P_.ph, Lc.lebesgue, Lc.density_floor, Lc.pressure_floor,
+                                    Lc.relative_floor))
+    return;
+  load_tables<P>(tables, tb);
   __syncthreads();
   hex_samples<P, NV>(tb, Ug, U, Smp, t1, t2, vq, fs);
   if (threadIdx.x == 0) red_nan = 0;
@@ -919,10 +924,21 @@ __global__ void __launch_bounds__(kThreads) k_hex_troubled(const DevPlan P_, con
   const BlockDev& B = P_.blk[b];
   const int e = blockIdx.x;
   if (predicted_skip(pa, e, flag_out)) return;
-  load_tables<P>(tables, tb);
   const double* Ug = S.b[b] + (size_t)e * N3 * NV;
+  // nodal certificate of admissible samples and mean: then only the sensor needs computing
+  const bool certified = nodal_certificate<NV>(Ug, N3, P_.ph, Lc.lebesgue, Lc.density_floor,
+                                                       Lc.pressure_floor, 0.0);
+  load_tables<P>(tables, tb);
   __syncthreads();
-  hex_samples<P, NV>(tb, Ug, U, Smp, t1, t2, vq, fs);
+  if (certified) {
+    for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
+      const int v = idx / N3, l = idx % N3;
+      U[idx] = Ug[tb->lex2node[l] * NV + v];
+    }
+    __syncthreads();
+  } else {
+    hex_samples<P, NV>(tb, Ug, U, Smp, t1, t2, vq, fs);
+  }
   for (int l = threadIdx.x; l < N3; l += blockDim.x) {
     double u[NV], W[NV];
 #pragma unroll
@@ -936,7 +952,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_troubled(const DevPlan P_, con
   // tensor product of the 1-D projector onto span{1, xi} (three passes of N x N)
   if (P >= 2) tensor3<2, N, N, N, N, N, N, false>(Mon, Low, t1, t2, tb->p1d, tb->p1d, tb->p1d);
   __shared__ double part[kThreads / 32][NV + 1];
-  hex_cell_mean<NV>(vq, B.wdet + (size_t)e * Q3, Q3, mean, part);
+  if (!certified) hex_cell_mean<NV>(vq, B.wdet + (size_t)e * Q3, Q3, mean, part);
   double hi0 = 0.0, hi1 = 0.0, sc0 = 0.0, sc1 = 0.0;
   if (P >= 2) {
     for (int i = threadIdx.x; i < N3; i += blockDim.x) {
@@ -962,7 +978,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_troubled(const DevPlan P_, con
   }
   __syncthreads();
   bool bad = false;
-  for (int r = threadIdx.x; r <= NS; r += blockDim.x) {
+  for (int r = threadIdx.x; r <= (certified ? -1 : NS); r += blockDim.x) {
     double s[NV], W[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) s[v] = r < NS ? Smp[v * NS + r] : mean[v];

@@ -196,9 +196,10 @@ class SubcellBlockPlan:
 
 def _spd_inverse(gram):
     """Inverses of a stack of SPD matrices: on the GPU (``dgb_spd_inverse``) when one is present,
-    else with numpy (set-up only)."""
+    else with numpy (set-up only).  The choice does not depend on the stack's size, so an element
+    gets the same matrix whichever mesh or chunk it is part of."""
     import torch
-    if not torch.cuda.is_available() or len(gram) < 256:
+    if not torch.cuda.is_available() or len(gram) == 0:
         return np.linalg.inv(gram)
     t = torch.as_tensor(np.ascontiguousarray(gram), device="cuda")
     status = torch.zeros(1, dtype=torch.int32, device="cuda")

@@ -108,7 +108,7 @@ def test_device_inverse_mass_matches_host(case):
                                   "float64", affine=False, inverse_mass=where)
         out.append(other.rhs(states, bc))
     for k in g["block_names"]:
-        close(out[0][k], out[1][k], 1e-12)
+        close(out[0][k], out[1][k].cpu().numpy(), 1e-12)
 
 
 def test_degenerate_element_is_refused_by_the_device_inverse_mass():
