@@ -40,51 +40,15 @@ __device__ __forceinline__ double pressure_of(const Physics& ph, const double* U
 //   p_lo - tol_p >= max(p_floor, rel pmean_hi + tol_p),
 // with rho_lo >= 1e-3 rho_hi, so that the relative rounding of |m|^2 / rho stays small.
 // A non-finite nodal value gives false.  Every thread returns the same value.
-template <int NV>
-__device__ bool nodal_certificate(const double* __restrict__ Ug, int Np, const Physics& ph, double L,
-                                  double rho_floor, double p_floor, double rel) {
-  __shared__ double red[10][kThreads / 32];
-  double lo[5], hi[5];
-#pragma unroll
-  for (int v = 0; v < 5; ++v) {
-    lo[v] = INFINITY;
-    hi[v] = -INFINITY;
-  }
-  bool fin = true;
-  for (int l = threadIdx.x; l < Np; l += blockDim.x) {
-#pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      const double x = Ug[l * NV + v];
-      fin &= isfinite(x);
-      if (v < 5) {
-        lo[v] = fmin(lo[v], x);
-        hi[v] = fmax(hi[v], x);
-      }
-    }
-  }
-#pragma unroll
-  for (int v = 0; v < 5; ++v)
-    for (int o = 16; o > 0; o >>= 1) {
-      lo[v] = fmin(lo[v], __shfl_xor_sync(0xffffffff, lo[v], o));
-      hi[v] = fmax(hi[v], __shfl_xor_sync(0xffffffff, hi[v], o));
-    }
-  if ((threadIdx.x & 31) == 0)
-#pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      red[v][threadIdx.x >> 5] = lo[v];
-      red[5 + v][threadIdx.x >> 5] = hi[v];
-    }
-  const bool all_finite = __syncthreads_and(fin);
-  if (!all_finite || !(L >= 1.0)) return false;
+// The bound check of the certificate, from the smallest and largest nodal value of rho, m and E.
+__device__ __forceinline__ bool certificate_from_range(const double (&mn)[5], const double (&mx)[5],
+                                                       const Physics& ph, double L, double rho_floor,
+                                                       double p_floor, double rel) {
+  if (!(L >= 1.0)) return false;
   double a[5], b[5];
 #pragma unroll
   for (int v = 0; v < 5; ++v) {
-    double mn = red[v][0], mx = red[5 + v][0];
-    for (int k = 1; k < kThreads / 32; ++k) {
-      mn = fmin(mn, red[v][k]);
-      mx = fmax(mx, red[5 + v][k]);
-    }
-    const double c = 0.5 * (mn + mx), h = 0.5 * (mx - mn);
+    const double c = 0.5 * (mn[v] + mx[v]), h = 0.5 * (mx[v] - mn[v]);
     a[v] = c - L * h;
     b[v] = c + L * h;
   }
@@ -102,6 +66,81 @@ __device__ bool nodal_certificate(const double* __restrict__ Ug, int Np, const P
   const double tol_p = 1.0e-6 * g1 * (L * fmax(fabs(a[4]), fabs(b[4])) + ke_hi);
   return (a[0] - tol_r >= fmax(rho_floor, rel * (b[0] + tol_r))) &&
          (p_lo - tol_p >= fmax(p_floor, rel * pmean_hi + tol_p));
+}
+
+// Warp-level range of the nodal rho, m, E of one element ([Np][NV] at Ug, read as one contiguous
+// run so that the warp's loads coalesce) and whether every nodal value is finite.  Every lane
+// returns the same range.
+template <int NV>
+__device__ __forceinline__ bool warp_nodal_range(const double* __restrict__ Ug, int Np, double (&mn)[5],
+                                                 double (&mx)[5]) {
+#pragma unroll
+  for (int v = 0; v < 5; ++v) {
+    mn[v] = INFINITY;
+    mx[v] = -INFINITY;
+  }
+  bool fin = true;
+  for (int i = (threadIdx.x & 31); i < Np * NV; i += 32) {
+    const double x = Ug[i];
+    const int v = i % NV;
+    fin &= isfinite(x);
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+      if (v == k) {
+        mn[k] = fmin(mn[k], x);
+        mx[k] = fmax(mx[k], x);
+      }
+  }
+#pragma unroll
+  for (int v = 0; v < 5; ++v)
+    for (int o = 16; o > 0; o >>= 1) {
+      mn[v] = fmin(mn[v], __shfl_xor_sync(0xffffffff, mn[v], o));
+      mx[v] = fmax(mx[v], __shfl_xor_sync(0xffffffff, mx[v], o));
+    }
+  return __all_sync(0xffffffff, fin);
+}
+
+// The certificate worked by a whole block for one element.  Every thread returns the same value.
+template <int NV>
+__device__ bool nodal_certificate(const double* __restrict__ Ug, int Np, const Physics& ph, double L,
+                                  double rho_floor, double p_floor, double rel) {
+  __shared__ double range[10];
+  __shared__ int all_finite;
+  double mn[5], mx[5];
+  if ((threadIdx.x >> 5) == 0) {   // warp 0 reads the element's nodal values
+    const bool fin = warp_nodal_range<NV>(Ug, Np, mn, mx);
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        range[v] = mn[v];
+        range[5 + v] = mx[v];
+      }
+      all_finite = fin;
+    }
+  }
+  __syncthreads();
+  if (!all_finite) return false;
+#pragma unroll
+  for (int v = 0; v < 5; ++v) {
+    mn[v] = range[v];
+    mx[v] = range[5 + v];
+  }
+  return certificate_from_range(mn, mx, ph, L, rho_floor, p_floor, rel);
+}
+
+// Certificate pre-pass, one warp per element: elements of block U that the certificate does not
+// clear are appended to list (in no fixed order; each is then processed on its own, so results do
+// not depend on it).  *count must be zero before the launch.
+template <int NV>
+__global__ void __launch_bounds__(kThreads) k_certify(const double* __restrict__ U, int E, int Np, const Physics ph,
+                                                     double L, double rho_floor, double p_floor, double rel,
+                                                     int* __restrict__ list, int* __restrict__ count) {
+  const long long e = (long long)blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
+  if (e >= E) return;
+  double mn[5], mx[5];
+  const bool fin = warp_nodal_range<NV>(U + e * Np * NV, Np, mn, mx);
+  if ((threadIdx.x & 31) == 0 && !(fin && certificate_from_range(mn, mx, ph, L, rho_floor, p_floor, rel)))
+    list[atomicAdd(count, 1)] = (int)e;
 }
 
 // samples = [U at nodes; B U at volume points; Bfs U at face points]  -> S[Ns_total][NV]

@@ -84,6 +84,11 @@ struct dgb_plan {
   // sum-factorised hexahedron path (single hexahedron block)
   bool hex = false;
   HexTables hex_tables;
+  // hexahedron positivity: elements the certificate pre-pass did not clear, and the grid that
+  // works through them (resident CTAs of k_hex_positivity)
+  int* cert_list = nullptr;
+  int* cert_count = nullptr;
+  int pos_grid = 0;
   HexCodes hex_codes = {nullptr, nullptr};
   double* hex_lift = nullptr;     // [E][12][N3] nodal BR2 lift scratch
   // MOOD subcell fallback
@@ -361,12 +366,34 @@ int run_rhs(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStream_t
   return p->prm.precision == 1 ? run_rhs_dense<NV, float>(p, S, A, st, ev) : run_rhs_dense<NV, double>(p, S, A, st, ev);
 }
 
+// Resident CTAs of k_hex_positivity over the whole GPU (set-up; at most one per element).
 template <int P, int NV>
-int run_positivity_hex(dgb_plan* p, const StatePtrs& S, cudaStream_t st) {
+int hex_positivity_grid(dgb_plan* p) {
   const size_t sm = sizeof(double) * (size_t)hex_positivity_smem<P, NV>();
   int rc;
   if ((rc = prepare(k_hex_positivity<P, NV>, sm))) return rc;
-  k_hex_positivity<P, NV><<<p->dev.blk[0].E, kThreads, sm, st>>>(p->dev, S, 0, p->hex_tables, p->lim);
+  int dev = 0, sms = 0, per_sm = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hex_positivity<P, NV>, kThreads, sm));
+  const long long grid = (long long)std::max(per_sm, 1) * std::max(sms, 1);
+  p->pos_grid = (int)std::min<long long>(grid, std::max(p->dev.blk[0].E, 1));
+  return DGB_OK;
+}
+
+// Positivity on the sum-factorised path: the certificate pre-pass (one warp per element) lists the
+// elements it cannot clear, and k_hex_positivity limits only those.
+template <int P, int NV>
+int run_positivity_hex(dgb_plan* p, const StatePtrs& S, cudaStream_t st) {
+  const size_t sm = sizeof(double) * (size_t)hex_positivity_smem<P, NV>();
+  const BlockDev& B = p->dev.blk[0];
+  if (B.E == 0) return DGB_OK;
+  CK(cudaMemsetAsync(p->cert_count, 0, sizeof(int), st));
+  k_certify<NV><<<blocks_for(B.E, kThreads / 32), kThreads, 0, st>>>(
+      S.b[0], B.E, B.Np, p->dev.ph, p->lim.lebesgue, p->lim.density_floor, p->lim.pressure_floor,
+      p->lim.relative_floor, p->cert_list, p->cert_count);
+  k_hex_positivity<P, NV><<<p->pos_grid, kThreads, sm, st>>>(p->dev, S, 0, p->hex_tables, p->lim, p->cert_list,
+                                                             p->cert_count);
   CK(cudaGetLastError());
   return DGB_OK;
 }
@@ -1112,6 +1139,18 @@ int dgb_plan_finalize(dgb_plan* p) {
       if ((rc = alloc(p, n * 2 * nq * 12, &F.liftF))) return rc;
       if ((rc = alloc(p, n * nq * NV, &F.fluxV))) return rc;
     }
+  }
+  if (p->hex && p->dev.blk[0].E > 0) {
+    CK(cudaMalloc(&p->cert_list, sizeof(int) * (size_t)p->dev.blk[0].E));
+    p->allocations.push_back(p->cert_list);
+    CK(cudaMalloc(&p->cert_count, sizeof(int)));
+    p->allocations.push_back(p->cert_count);
+    const int deg = p->dev.degree;
+    rc = NV == 5 ? (deg == 1 ? hex_positivity_grid<1, 5>(p) : deg == 2 ? hex_positivity_grid<2, 5>(p)
+                                                              : hex_positivity_grid<3, 5>(p))
+                 : (deg == 1 ? hex_positivity_grid<1, 16>(p) : deg == 2 ? hex_positivity_grid<2, 16>(p)
+                                                               : hex_positivity_grid<3, 16>(p));
+    if (rc) return rc;
   }
   p->npartials = 0;
   for (int b = 0; b < p->dev.nblocks; ++b) {

@@ -814,7 +814,9 @@ __device__ void hex_samples(const HexTables* tb, const double* Ug, double* U, do
 // collects from its face groups.
 template <int P, int NV>
 __global__ void __launch_bounds__(kThreads) k_hex_positivity(const DevPlan P_, const StatePtrs S, int b,
-                                                            const HexTables tables, const LimiterConst Lc) {
+                                                            const HexTables tables, const LimiterConst Lc,
+                                                            const int* __restrict__ list,
+                                                            const int* __restrict__ count) {
   using D = HexDims<P>;
   constexpr int N = D::N, Q = D::Q, QF = D::QF, N3 = D::N3, Q3 = D::Q3, QF2 = D::QF2;
   constexpr int NS = N3 + Q3 + 6 * QF2;             // samples per element
@@ -831,71 +833,74 @@ __global__ void __launch_bounds__(kThreads) k_hex_positivity(const DevPlan P_, c
   __shared__ int red_nan;
   __shared__ double sh_upper;
   const BlockDev& B = P_.blk[b];
-  const int e = blockIdx.x;
-  double* Ug = S.b[b] + (size_t)e * N3 * NV;
-  // An element whose nodal values certify admissible samples at theta = 1 keeps its state: the
-  // reference's mean + 1 * (U - mean) equals U to rounding, so nothing is written.
-  if (nodal_certificate<NV>(Ug, N3, P_.ph, Lc.lebesgue, Lc.density_floor, Lc.pressure_floor,
-                                    Lc.relative_floor))
-    return;
+  // The elements are those of list[0, *count): the ones the certificate pre-pass (k_certify) did not
+  // clear.  A cleared element keeps its state: its theta is 1, and the reference's
+  // mean + 1 * (U - mean) equals U to rounding.  Each CTA loads the tables once and takes the
+  // listed elements in a grid stride.
   load_tables<P>(tables, tb);
   __syncthreads();
-  hex_samples<P, NV>(tb, Ug, U, Smp, t1, t2, vq, fs);
-  if (threadIdx.x == 0) red_nan = 0;
-  __syncthreads();
-  // cell mean from the volume samples
-  __shared__ double part[kThreads / 32][NV + 1];
-  hex_cell_mean<NV>(vq, B.wdet + (size_t)e * Q3, Q3, mean, part);
-  double Wm[NV];
-  primitive<NV>(P_.ph, mean, Wm);
-  const double rfloor = fmax(Lc.density_floor, Lc.relative_floor * Wm[0]);
-  const double pfloor = fmax(Lc.pressure_floor, Lc.relative_floor * Wm[4]);
-  double rmin = INFINITY;
-  bool nan_seen = false;
-  for (int r = threadIdx.x; r < NS; r += blockDim.x) {
-    const double d = Smp[r];
-    nan_seen |= isnan(d);
-    rmin = fmin(rmin, d);
-  }
-  for (int o = 16; o > 0; o >>= 1) rmin = fmin(rmin, __shfl_xor_sync(0xffffffff, rmin, o));
-  if (nan_seen) atomicOr(&red_nan, 1);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = rmin;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double m = red[0];
-    for (int k = 1; k < kThreads / 32; ++k) m = fmin(m, red[k]);
-    if (red_nan) m = NAN;
-    const double th = (m < rfloor) ? (mean[0] - rfloor) / fmax(mean[0] - m, 1.0e-30) : 1.0;
-    sh_upper = isnan(th) ? th : fmin(fmax(th, 0.0), 1.0);
-  }
-  __syncthreads();
-  const double upper = sh_upper;
-  auto pressure_ok = [&](double theta) -> bool {
-    bool ok = true;
+  const int n = *count;
+  for (int item = blockIdx.x; item < n; item += gridDim.x) {
+    const int e = list[item];
+    double* Ug = S.b[b] + (size_t)e * N3 * NV;
+    hex_samples<P, NV>(tb, Ug, U, Smp, t1, t2, vq, fs);
+    if (threadIdx.x == 0) red_nan = 0;
+    __syncthreads();
+    // cell mean from the volume samples
+    __shared__ double part[kThreads / 32][NV + 1];
+    hex_cell_mean<NV>(vq, B.wdet + (size_t)e * Q3, Q3, mean, part);
+    double Wm[NV];
+    primitive<NV>(P_.ph, mean, Wm);
+    const double rfloor = fmax(Lc.density_floor, Lc.relative_floor * Wm[0]);
+    const double pfloor = fmax(Lc.pressure_floor, Lc.relative_floor * Wm[4]);
+    double rmin = INFINITY;
+    bool nan_seen = false;
     for (int r = threadIdx.x; r < NS; r += blockDim.x) {
-      double s[NV];
-#pragma unroll
-      for (int v = 0; v < NV; ++v) s[v] = mean[v] + theta * (Smp[v * NS + r] - mean[v]);
-      ok &= (pressure_of<NV>(P_.ph, s) >= pfloor);
+      const double d = Smp[r];
+      nan_seen |= isnan(d);
+      rmin = fmin(rmin, d);
     }
-    return __syncthreads_and(ok);
-  };
-  // theta = upper when the pressure is admissible there; only otherwise is the reference's
-  // 30-step bisection result used, so it is computed only in that case (same theta)
-  double theta = upper;
-  if (!pressure_ok(upper)) {
-    double lo = 0.0, hi = upper;
-    for (int it = 0; it < 30; ++it) {
-      const double mid = 0.5 * (lo + hi);
-      const bool ok = pressure_ok(mid);
-      lo = ok ? mid : lo;
-      hi = ok ? hi : mid;
+    for (int o = 16; o > 0; o >>= 1) rmin = fmin(rmin, __shfl_xor_sync(0xffffffff, rmin, o));
+    if (nan_seen) atomicOr(&red_nan, 1);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = rmin;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double m = red[0];
+      for (int k = 1; k < kThreads / 32; ++k) m = fmin(m, red[k]);
+      if (red_nan) m = NAN;
+      const double th = (m < rfloor) ? (mean[0] - rfloor) / fmax(mean[0] - m, 1.0e-30) : 1.0;
+      sh_upper = isnan(th) ? th : fmin(fmax(th, 0.0), 1.0);
     }
-    theta = lo;
-  }
-  for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
-    const int v = idx / N3, l = idx % N3;
-    Ug[tb->lex2node[l] * NV + v] = mean[v] + theta * (U[idx] - mean[v]);
+    __syncthreads();
+    const double upper = sh_upper;
+    auto pressure_ok = [&](double theta) -> bool {
+      bool ok = true;
+      for (int r = threadIdx.x; r < NS; r += blockDim.x) {
+        double s[NV];
+  #pragma unroll
+        for (int v = 0; v < NV; ++v) s[v] = mean[v] + theta * (Smp[v * NS + r] - mean[v]);
+        ok &= (pressure_of<NV>(P_.ph, s) >= pfloor);
+      }
+      return __syncthreads_and(ok);
+    };
+    // theta = upper when the pressure is admissible there; only otherwise is the reference's
+    // 30-step bisection result used, so it is computed only in that case (same theta)
+    double theta = upper;
+    if (!pressure_ok(upper)) {
+      double lo = 0.0, hi = upper;
+      for (int it = 0; it < 30; ++it) {
+        const double mid = 0.5 * (lo + hi);
+        const bool ok = pressure_ok(mid);
+        lo = ok ? mid : lo;
+        hi = ok ? hi : mid;
+      }
+      theta = lo;
+    }
+    for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
+      const int v = idx / N3, l = idx % N3;
+      Ug[tb->lex2node[l] * NV + v] = mean[v] + theta * (U[idx] - mean[v]);
+    }
+    __syncthreads();   // the next element reuses the shared buffers and scalars
   }
 }
 
