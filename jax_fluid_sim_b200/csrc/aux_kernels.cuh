@@ -68,28 +68,31 @@ __device__ __forceinline__ bool certificate_from_range(const double (&mn)[5], co
          (p_lo - tol_p >= fmax(p_floor, rel * pmean_hi + tol_p));
 }
 
-// Warp-level range of the nodal rho, m, E of one element ([Np][NV] at Ug, read as one contiguous
-// run so that the warp's loads coalesce) and whether every nodal value is finite.  Every lane
+// Warp-level range of the nodal rho, m, E of one element ([NP][NV] at Ug, read as one contiguous
+// run, NP * NV / 32 independent loads a lane) and whether every nodal value is finite.  Every lane
 // returns the same range.
-template <int NV>
-__device__ __forceinline__ bool warp_nodal_range(const double* __restrict__ Ug, int Np, double (&mn)[5],
-                                                 double (&mx)[5]) {
+template <int NV, int NP>
+__device__ __forceinline__ bool warp_nodal_range(const double* __restrict__ Ug, double (&mn)[5], double (&mx)[5]) {
 #pragma unroll
   for (int v = 0; v < 5; ++v) {
     mn[v] = INFINITY;
     mx[v] = -INFINITY;
   }
   bool fin = true;
-  for (int i = (threadIdx.x & 31); i < Np * NV; i += 32) {
-    const double x = Ug[i];
-    const int v = i % NV;
-    fin &= isfinite(x);
 #pragma unroll
-    for (int k = 0; k < 5; ++k)
-      if (v == k) {
-        mn[k] = fmin(mn[k], x);
-        mx[k] = fmax(mx[k], x);
-      }
+  for (int i0 = 0; i0 < NP * NV; i0 += 32) {
+    const int i = i0 + (threadIdx.x & 31);
+    if (i < NP * NV) {
+      const double x = Ug[i];
+      const int v = i % NV;
+      fin &= isfinite(x);
+#pragma unroll
+      for (int k = 0; k < 5; ++k)
+        if (v == k) {
+          mn[k] = fmin(mn[k], x);
+          mx[k] = fmax(mx[k], x);
+        }
+    }
   }
 #pragma unroll
   for (int v = 0; v < 5; ++v)
@@ -100,45 +103,68 @@ __device__ __forceinline__ bool warp_nodal_range(const double* __restrict__ Ug, 
   return __all_sync(0xffffffff, fin);
 }
 
-// The certificate worked by a whole block for one element.  Every thread returns the same value.
+// The certificate worked by a whole block for one element: each thread takes nodes in a stride,
+// warps combine by shuffles and every thread combines the warps.  Every thread returns the same
+// value.
 template <int NV>
 __device__ bool nodal_certificate(const double* __restrict__ Ug, int Np, const Physics& ph, double L,
                                   double rho_floor, double p_floor, double rel) {
-  __shared__ double range[10];
-  __shared__ int all_finite;
+  __shared__ double red[10][kThreads / 32];
   double mn[5], mx[5];
-  if ((threadIdx.x >> 5) == 0) {   // warp 0 reads the element's nodal values
-    const bool fin = warp_nodal_range<NV>(Ug, Np, mn, mx);
-    if (threadIdx.x == 0) {
 #pragma unroll
-      for (int v = 0; v < 5; ++v) {
-        range[v] = mn[v];
-        range[5 + v] = mx[v];
+  for (int v = 0; v < 5; ++v) {
+    mn[v] = INFINITY;
+    mx[v] = -INFINITY;
+  }
+  bool fin = true;
+  for (int l = threadIdx.x; l < Np; l += blockDim.x) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      const double x = Ug[l * NV + v];
+      fin &= isfinite(x);
+      if (v < 5) {
+        mn[v] = fmin(mn[v], x);
+        mx[v] = fmax(mx[v], x);
       }
-      all_finite = fin;
     }
   }
-  __syncthreads();
+#pragma unroll
+  for (int v = 0; v < 5; ++v)
+    for (int o = 16; o > 0; o >>= 1) {
+      mn[v] = fmin(mn[v], __shfl_xor_sync(0xffffffff, mn[v], o));
+      mx[v] = fmax(mx[v], __shfl_xor_sync(0xffffffff, mx[v], o));
+    }
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      red[v][threadIdx.x >> 5] = mn[v];
+      red[5 + v][threadIdx.x >> 5] = mx[v];
+    }
+  const bool all_finite = __syncthreads_and(fin);
   if (!all_finite) return false;
 #pragma unroll
   for (int v = 0; v < 5; ++v) {
-    mn[v] = range[v];
-    mx[v] = range[5 + v];
+    mn[v] = red[v][0];
+    mx[v] = red[5 + v][0];
+    for (int k = 1; k < kThreads / 32; ++k) {
+      mn[v] = fmin(mn[v], red[v][k]);
+      mx[v] = fmax(mx[v], red[5 + v][k]);
+    }
   }
   return certificate_from_range(mn, mx, ph, L, rho_floor, p_floor, rel);
 }
 
-// Certificate pre-pass, one warp per element: elements of block U that the certificate does not
-// clear are appended to list (in no fixed order; each is then processed on its own, so results do
-// not depend on it).  *count must be zero before the launch.
-template <int NV>
-__global__ void __launch_bounds__(kThreads) k_certify(const double* __restrict__ U, int E, int Np, const Physics ph,
-                                                     double L, double rho_floor, double p_floor, double rel,
+// Certificate pre-pass, one warp per element of NP nodes: elements of block U that the
+// certificate does not clear are appended to list (in no fixed order; each is then processed on
+// its own, so results do not depend on it).  *count must be zero before the launch.
+template <int NV, int NP>
+__global__ void __launch_bounds__(kThreads) k_certify(const double* __restrict__ U, int E, const Physics ph, double L,
+                                                     double rho_floor, double p_floor, double rel,
                                                      int* __restrict__ list, int* __restrict__ count) {
   const long long e = (long long)blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
   if (e >= E) return;
   double mn[5], mx[5];
-  const bool fin = warp_nodal_range<NV>(U + e * Np * NV, Np, mn, mx);
+  const bool fin = warp_nodal_range<NV, NP>(U + e * NP * NV, mn, mx);
   if ((threadIdx.x & 31) == 0 && !(fin && certificate_from_range(mn, mx, ph, L, rho_floor, p_floor, rel)))
     list[atomicAdd(count, 1)] = (int)e;
 }

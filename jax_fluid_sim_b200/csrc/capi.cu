@@ -389,8 +389,8 @@ int run_positivity_hex(dgb_plan* p, const StatePtrs& S, cudaStream_t st) {
   const BlockDev& B = p->dev.blk[0];
   if (B.E == 0) return DGB_OK;
   CK(cudaMemsetAsync(p->cert_count, 0, sizeof(int), st));
-  k_certify<NV><<<blocks_for(B.E, kThreads / 32), kThreads, 0, st>>>(
-      S.b[0], B.E, B.Np, p->dev.ph, p->lim.lebesgue, p->lim.density_floor, p->lim.pressure_floor,
+  k_certify<NV, HexDims<P>::N3><<<blocks_for(B.E, kThreads / 32), kThreads, 0, st>>>(
+      S.b[0], B.E, p->dev.ph, p->lim.lebesgue, p->lim.density_floor, p->lim.pressure_floor,
       p->lim.relative_floor, p->cert_list, p->cert_count);
   k_hex_positivity<P, NV><<<p->pos_grid, kThreads, sm, st>>>(p->dev, S, 0, p->hex_tables, p->lim, p->cert_list,
                                                              p->cert_count);
