@@ -68,9 +68,9 @@ __device__ __forceinline__ bool certificate_from_range(const double (&mn)[5], co
          (p_lo - tol_p >= fmax(p_floor, rel * pmean_hi + tol_p));
 }
 
-// Warp-level range of the nodal rho, m, E of one element ([NP][NV] at Ug, read as one contiguous
-// run, NP * NV / 32 independent loads a lane) and whether every nodal value is finite.  Every lane
-// returns the same range.
+// Warp-level range of the nodal rho, m, E of one element ([NP][NV] at Ug; lane l takes nodes l,
+// l + 32, ..., so each variable goes straight to its own minimum and maximum) and whether every
+// nodal value is finite.  Every lane returns the same range.
 template <int NV, int NP>
 __device__ __forceinline__ bool warp_nodal_range(const double* __restrict__ Ug, double (&mn)[5], double (&mx)[5]) {
 #pragma unroll
@@ -80,18 +80,18 @@ __device__ __forceinline__ bool warp_nodal_range(const double* __restrict__ Ug, 
   }
   bool fin = true;
 #pragma unroll
-  for (int i0 = 0; i0 < NP * NV; i0 += 32) {
-    const int i = i0 + (threadIdx.x & 31);
-    if (i < NP * NV) {
-      const double x = Ug[i];
-      const int v = i % NV;
-      fin &= isfinite(x);
+  for (int l0 = 0; l0 < NP; l0 += 32) {
+    const int l = l0 + (threadIdx.x & 31);
+    if (l < NP) {
 #pragma unroll
-      for (int k = 0; k < 5; ++k)
-        if (v == k) {
-          mn[k] = fmin(mn[k], x);
-          mx[k] = fmax(mx[k], x);
+      for (int v = 0; v < NV; ++v) {
+        const double x = Ug[l * NV + v];
+        fin &= isfinite(x);
+        if (v < 5) {
+          mn[v] = fmin(mn[v], x);
+          mx[v] = fmax(mx[v], x);
         }
+      }
     }
   }
 #pragma unroll
