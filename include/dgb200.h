@@ -148,6 +148,18 @@ int dgb_map_metrics(const double* nodes, const int32_t* index, int count, int nu
                     int num_points, const double* weights, const double* tangents, const double* orientation,
                     double* jacobian, double* det, double* inv_jacobian, double* wdet, double* normals,
                     double* area_weights);
+/* Host-side subcell face metrics for the MOOD subcell plan (no GPU; hybrid/subcell.py:336-360).
+ * For count elements with the physical subcell vertices vertices[count][num_vertices][3] and subcell
+ * centres centers[count][num_subcells][3]: each face f of faces[num_faces][4] (face_sizes[f] = 3 or
+ * 4 vertex ids) gets its area vector (a triangle p0 p1 p2: (p1 - p0) x (p2 - p0) / 2; a
+ * quadrilateral adds (p2 - p0) x (p3 - p0) / 2), turned toward centre[neighbors[f]] -
+ * centre[owners[f]] (or, with neighbors NULL, toward the face centre), as normals
+ * [count][num_faces][3] (unit), areas [count][num_faces] and, when not NULL, face_centers
+ * [count][num_faces][3] (the mean of the face's vertices).  Runs on the host cores in threads. */
+int dgb_subcell_face_metrics(const double* vertices, int count, int num_vertices, const int32_t* faces,
+                             const int32_t* face_sizes, int num_faces, const double* centers, int num_subcells,
+                             const int32_t* owners, const int32_t* neighbors, double* normals, double* areas,
+                             double* face_centers);
 /* Optional sum-factorised path for a mesh of one hexahedron block (hexahedron bases are
  * tensor products of the 1-D Lagrange basis on the nodes 0, 1, interior: hybrid/elements.py:
  * 199-274, 325-456).  line_tables: 173 doubles, in order bq[5][4], dq[5][4] (1-D basis and

@@ -123,6 +123,8 @@ def lib():
                                           P_double, P_double, P_double],
             "dgb_plan_build_inverse_mass": [c_void_p, c_int, P_double, c_int],
             "dgb_spd_inverse": [c_void_p, c_int, c_int, c_void_p, c_void_p],
+            "dgb_subcell_face_metrics": [P_double, c_int, c_int, P_int32, P_int32, c_int, P_double, c_int, P_int32,
+                                         P_int32, P_double, P_double, P_double],
             "dgb_map_metrics": [P_double, P_int32, c_int, c_int, P_double, c_int, P_double, P_double, P_double,
                                 P_double, P_double, P_double, P_double, P_double, P_double],
             "dgb_plan_destroy": [c_void_p],
@@ -208,3 +210,25 @@ def map_metrics(nodes, grad, index=None, weights=None, tangents=None, orientatio
                                 dptr(grad), Q, *args,
                                 *[dptr(out[k]) if k in out else None for k in shapes]))
     return tuple(out[k] for k in outputs)
+
+
+def subcell_face_metrics(vertices, centers, faces, owners, neighbors=None):
+    """Subcell face metrics on the host cores (``dgb_subcell_face_metrics``): vertices (E, V, 3),
+    centers (E, S, 3), faces a list of 3- or 4-vertex id sequences; returns unit normals (E, F, 3),
+    areas (E, F) and face centres (E, F, 3)."""
+    vertices, centers = as_f64(vertices), as_f64(centers)
+    E, V, _ = vertices.shape
+    F = len(faces)
+    table = np.zeros((max(F, 1), 4), np.int32)
+    sizes = np.zeros(max(F, 1), np.int32)
+    for f, face in enumerate(faces):
+        table[f, :len(face)] = face
+        sizes[f] = len(face)
+    own = as_i32(owners)
+    nbr = None if neighbors is None else as_i32(neighbors)
+    normals, areas, fc = np.empty((E, F, 3)), np.empty((E, F)), np.empty((E, F, 3))
+    check(lib().dgb_subcell_face_metrics(dptr(vertices), E, V, dptr(table, ctypes.c_int32), dptr(sizes, ctypes.c_int32),
+                                         F, dptr(centers), centers.shape[1], dptr(own, ctypes.c_int32),
+                                         None if nbr is None else dptr(nbr, ctypes.c_int32), dptr(normals), dptr(areas),
+                                         dptr(fc)))
+    return normals, areas, fc

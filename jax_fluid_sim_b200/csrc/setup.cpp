@@ -104,3 +104,69 @@ extern "C" int dgb_map_metrics(const double* nodes, const int32_t* index, int co
   });
   return DGB_OK;
 }
+
+// Subcell face metrics of the MOOD subcell plan (hybrid/subcell.py:336-360), per element: the area
+// vector of each subcell face (a triangle p0 p1 p2 gives (p1 - p0) x (p2 - p0) / 2, a quadrilateral
+// adds (p2 - p0) x (p3 - p0) / 2), turned to point from the owner subcell's centre toward the
+// neighbour's (or, without a neighbour, toward the face centre), its length and unit vector, and
+// the face centre (the mean of its vertices).
+extern "C" int dgb_subcell_face_metrics(const double* vertices, int count, int num_vertices, const int32_t* faces,
+                                        const int32_t* face_sizes, int num_faces, const double* centers,
+                                        int num_subcells, const int32_t* owners, const int32_t* neighbors,
+                                        double* normals, double* areas, double* face_centers) {
+  if (count < 0 || num_vertices < 1 || num_faces < 0 || num_subcells < 1 || !vertices || !faces || !face_sizes ||
+      !centers || !owners || !normals || !areas)
+    return dgb::set_error(DGB_ERR_ARGUMENT, "bad subcell face-metrics argument");
+  for (int f = 0; f < num_faces; ++f) {
+    if (face_sizes[f] != 3 && face_sizes[f] != 4) return dgb::set_error(DGB_ERR_ARGUMENT, "faces have 3 or 4 vertices");
+    for (int k = 0; k < face_sizes[f]; ++k)
+      if (faces[f * 4 + k] < 0 || faces[f * 4 + k] >= num_vertices)
+        return dgb::set_error(DGB_ERR_ARGUMENT, "face vertex out of range");
+    if (owners[f] < 0 || owners[f] >= num_subcells || (neighbors && (neighbors[f] < 0 || neighbors[f] >= num_subcells)))
+      return dgb::set_error(DGB_ERR_ARGUMENT, "face subcell out of range");
+  }
+  const int V = num_vertices, F = num_faces, S = num_subcells;
+  parallel_ranges(count, [=](int lo, int hi) {
+    for (int e = lo; e < hi; ++e) {
+      const double* pv = vertices + (size_t)e * V * 3;
+      const double* cen = centers + (size_t)e * S * 3;
+      for (int f = 0; f < F; ++f) {
+        const int n = face_sizes[f];
+        const double* p[4];
+        for (int k = 0; k < n; ++k) p[k] = pv + faces[f * 4 + k] * 3;
+        double u[3], w[3], a[3], fc[3];
+        for (int d = 0; d < 3; ++d) {
+          u[d] = p[1][d] - p[0][d];
+          w[d] = p[2][d] - p[0][d];
+        }
+        a[0] = 0.5 * (u[1] * w[2] - u[2] * w[1]);
+        a[1] = 0.5 * (u[2] * w[0] - u[0] * w[2]);
+        a[2] = 0.5 * (u[0] * w[1] - u[1] * w[0]);
+        if (n == 4) {
+          double z[3];
+          for (int d = 0; d < 3; ++d) z[d] = p[3][d] - p[0][d];
+          a[0] = a[0] + 0.5 * (w[1] * z[2] - w[2] * z[1]);
+          a[1] = a[1] + 0.5 * (w[2] * z[0] - w[0] * z[2]);
+          a[2] = a[2] + 0.5 * (w[0] * z[1] - w[1] * z[0]);
+        }
+        for (int d = 0; d < 3; ++d) {
+          double s = p[0][d] + p[1][d];
+          for (int k = 2; k < n; ++k) s += p[k][d];
+          fc[d] = s / n;
+        }
+        const double* oc = cen + owners[f] * 3;
+        double dir[3];
+        for (int d = 0; d < 3; ++d) dir[d] = neighbors ? cen[neighbors[f] * 3 + d] - oc[d] : fc[d] - oc[d];
+        const double sgn = (a[0] * dir[0] + a[1] * dir[1] + a[2] * dir[2]) >= 0.0 ? 1.0 : -1.0;
+        for (double& v : a) v *= sgn;
+        const double mag = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+        const size_t o = (size_t)e * F + f;
+        for (int d = 0; d < 3; ++d) normals[o * 3 + d] = a[d] / mag;
+        areas[o] = mag;
+        if (face_centers)
+          for (int d = 0; d < 3; ++d) face_centers[o * 3 + d] = fc[d];
+      }
+    }
+  });
+  return DGB_OK;
+}

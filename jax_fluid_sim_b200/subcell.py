@@ -212,27 +212,9 @@ def _spd_inverse(gram):
 
 
 def _face_metrics(pv, cen, faces, owners, neighbors):
-    """Area vectors of subcell faces oriented owner -> neighbour (or outward), unit normals
-    (subcell.py:336-360); triangles a = (p1 - p0) x (p2 - p0) / 2, quadrilaterals as two triangles
-    about p0.  Faces of one vertex count are handled together."""
-    nf = len(faces)
-    av = np.empty((pv.shape[0], nf, 3))
-    fc = np.empty((pv.shape[0], nf, 3))
-    for k in (3, 4):
-        sel = [i for i, f in enumerate(faces) if len(f) == k]
-        if not sel:
-            continue
-        p = pv[:, np.asarray([faces[i] for i in sel])]                 # (e, m, k, 3)
-        a = 0.5 * np.cross(p[:, :, 1] - p[:, :, 0], p[:, :, 2] - p[:, :, 0])
-        if k == 4:
-            a = a + 0.5 * np.cross(p[:, :, 2] - p[:, :, 0], p[:, :, 3] - p[:, :, 0])
-        av[:, sel] = a
-        fc[:, sel] = p.mean(axis=2)
-    oc = cen[:, owners]
-    d = fc - oc if neighbors is None else cen[:, neighbors] - oc
-    av = av * np.where(np.sum(av * d, axis=-1) >= 0.0, 1.0, -1.0)[..., None]
-    area = np.linalg.norm(av, axis=-1)
-    return av / area[..., None], area, fc
+    """Unit normals, areas and centres of subcell faces, area vectors oriented owner -> neighbour
+    (or outward) (subcell.py:336-360), on the host cores (``dgb_subcell_face_metrics``)."""
+    return N.subcell_face_metrics(pv, cen, faces, owners, neighbors)
 
 
 class SubcellPlan:

@@ -1,7 +1,8 @@
 """Host-side geometry metrics of plan set-up (``dgb_map_metrics``, csrc/setup.cpp, host threads,
 no GPU) against plain numpy: Jacobians, determinants, inverses and w|det J| of curved and
 straight elements at shared reference points, with and without an element gather index, and the
-face normals and area weights from the mapped tangents (hybrid/geometry.py:139-203, 299-353)."""
+face normals and area weights from the mapped tangents (hybrid/geometry.py:139-203, 299-353); and
+the subcell face metrics of the MOOD plan (``dgb_subcell_face_metrics``, hybrid/subcell.py:336-360)."""
 
 import numpy as np
 import pytest
@@ -59,3 +60,49 @@ def test_bad_arguments_are_errors():
         N.map_metrics(np.zeros((2, 8, 3)), g, outputs=("wdet",))          # wdet needs weights
     with pytest.raises(ValueError):
         N.map_metrics(np.zeros((2, 8, 3)), g, weights=np.ones(1), outputs=("normals",))   # needs tangents
+
+
+def _subcell_face_metrics_numpy(pv, cen, faces, owners, neighbors):
+    """hybrid/subcell.py:336-360 restated with numpy, one face at a time."""
+    av, fc = [], []
+    for face in faces:
+        p = pv[:, np.asarray(face)]
+        a = 0.5 * np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0])
+        if len(face) == 4:
+            a = a + 0.5 * np.cross(p[:, 2] - p[:, 0], p[:, 3] - p[:, 0])
+        av.append(a)
+        fc.append(p.mean(axis=1))
+    av, fc = np.stack(av, axis=1), np.stack(fc, axis=1)
+    oc = cen[:, owners]
+    d = fc - oc if neighbors is None else cen[:, neighbors] - oc
+    av = av * np.where(np.sum(av * d, axis=-1) >= 0.0, 1.0, -1.0)[..., None]
+    area = np.linalg.norm(av, axis=-1)
+    return av / area[..., None], area, fc
+
+
+@pytest.mark.parametrize("source", ["hybrid", "curved"])
+def test_subcell_face_metrics_match_numpy(source):
+    """dgb_subcell_face_metrics (host threads) against the numpy restatement, on the internal and
+    boundary subfaces of every element type of a hybrid box and of a curved hexahedron box."""
+    from jax_fluid_sim_b200.subcell import ReferenceSubcells
+    src = meshgen.hybrid_box((3, 3, 3), seed=4) if source == "hybrid" else meshgen.curved_box()
+    mesh = HybridMesh(src)
+    for block in mesh.element_blocks:
+        rs = ReferenceSubcells(block.element_type)
+        geo, xyz = mesh.geometry(block)
+        pv = np.einsum("vi,eid->evd", geo.basis(rs.vertices), xyz)
+        cen = pv[:, rs.cells].mean(axis=2)
+        for faces, own, nbr in ((rs.internal_faces, rs.internal_owner, rs.internal_neighbor),
+                                (rs.boundary_faces, rs.boundary_owner, None)):
+            got = N.subcell_face_metrics(pv, cen, faces, own, nbr)
+            want = _subcell_face_metrics_numpy(pv, cen, faces, own, nbr)
+            for g, w in zip(got, want):
+                np.testing.assert_allclose(g, w, rtol=1e-13, atol=1e-15)
+
+
+def test_subcell_face_metrics_reject_bad_faces():
+    pv, cen = np.zeros((1, 4, 3)), np.zeros((1, 1, 3))
+    with pytest.raises(ValueError):
+        N.subcell_face_metrics(pv, cen, [(0, 1)], np.zeros(1, np.int32))          # two vertices
+    with pytest.raises(ValueError):
+        N.subcell_face_metrics(pv, cen, [(0, 1, 7)], np.zeros(1, np.int32))       # vertex out of range
