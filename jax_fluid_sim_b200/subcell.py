@@ -17,6 +17,8 @@ uses the subcell owning each subface.
 """
 
 import ctypes
+import os
+import threading
 
 import numpy as np
 
@@ -169,7 +171,13 @@ class SubcellBlockPlan:
         self.boundary_centers = np.empty((E, NB, 3))
         gflat = geo1.basis_gradients(flat)                 # (S * Qs, n, 3)
         Qs = mp.shape[1]
-        for s0 in range(0, E, chunk):
+        import torch
+        device = torch.cuda.current_device() if torch.cuda.is_available() else None
+
+        # Chunks of elements are independent and write disjoint rows, so they run in host threads
+        # (numpy and the native routines release the interpreter lock); each chunk's arithmetic is
+        # the same whichever thread takes it.
+        def work(s0):
             xyz = xyz_all[s0:s0 + chunk]
             e = len(xyz)
             pv = np.einsum("vi,eid->evd", vb, xyz)
@@ -184,23 +192,42 @@ class SubcellBlockPlan:
             # subcell.py:324-334: volume-weighted least-squares left inverse
             wpT = np.ascontiguousarray((proj * vol[..., None]).transpose(0, 2, 1))     # (e, Np, S)
             gram = np.matmul(wpT, proj)
-            rec = np.matmul(_spd_inverse(gram), wpT)
+            rec = np.matmul(_spd_inverse(gram, device), wpT)
             sl = slice(s0, s0 + e)
             self.projection[sl], self.reconstruction[sl], self.volumes[sl], self.centers[sl] = proj, rec, vol, cen
             n, a, _ = _face_metrics(pv, cen, rs.internal_faces, rs.internal_owner, rs.internal_neighbor)
             self.internal_normals[sl], self.internal_areas[sl] = n, a
             n, a, c = _face_metrics(pv, cen, rs.boundary_faces, rs.boundary_owner, None)
             self.boundary_normals[sl], self.boundary_areas[sl], self.boundary_centers[sl] = n, a, c
+
+        starts = range(0, E, chunk)
+        if len(starts) > 1:
+            from concurrent.futures import ThreadPoolExecutor
+            with ThreadPoolExecutor(max_workers=min(len(starts), os.cpu_count() or 1, 8)) as pool:
+                list(pool.map(work, starts))
+        else:
+            for s0 in starts:
+                work(s0)
         self.boundary_basis = ref.basis(rs.boundary_reference_centers)    # [NB][Np]
 
 
-def _spd_inverse(gram):
-    """Inverses of a stack of SPD matrices: on the GPU (``dgb_spd_inverse``) when one is present,
-    else with numpy (set-up only).  The choice does not depend on the stack's size, so an element
-    gets the same matrix whichever mesh or chunk it is part of."""
-    import torch
-    if not torch.cuda.is_available() or len(gram) == 0:
+_GPU_LOCK = threading.Lock()
+
+
+def _spd_inverse(gram, device):
+    """Inverses of a stack of SPD matrices: on GPU ``device`` (``dgb_spd_inverse``) when one is
+    given, else with numpy (set-up only).  The choice does not depend on the stack's size, so an
+    element gets the same matrix whichever mesh or chunk it is part of.  Host threads take the GPU
+    one at a time, each first making ``device`` its current device (that setting is per thread)."""
+    if device is None or len(gram) == 0:
         return np.linalg.inv(gram)
+    import torch
+    with _GPU_LOCK:
+        torch.cuda.set_device(device)
+        return _spd_inverse_gpu(torch, gram)
+
+
+def _spd_inverse_gpu(torch, gram):
     t = torch.as_tensor(np.ascontiguousarray(gram), device="cuda")
     status = torch.zeros(1, dtype=torch.int32, device="cuda")
     N.check(N.lib().dgb_spd_inverse(ctypes.c_void_p(t.data_ptr()), gram.shape[1], len(gram),
