@@ -388,8 +388,9 @@ def run_ours(args):
     else:
         per_stage += nb * 2 + 1
     if op.native.sum_factorised:
-        # the certificate pre-pass before each positivity pass (two per stage with MOOD)
-        per_stage += 2 if args.limiter == "mood" else 1
+        # the certificate pre-pass before each positivity pass (two per stage with MOOD) and the
+        # sensor pre-pass before the troubled-cell test (MOOD)
+        per_stage += 3 if args.limiter == "mood" else 1
     lim = "MOOD subcell FV (CWENO-Z) + positivity" if args.limiter == "mood" else "positivity limiter"
     prec = ("mixed: float32 arithmetic in the traces, BR2-lift, volume and finalize kernels; float64 state, "
             "face fluxes, limiters and reductions" if head_prec == "mixed" else "plain float64")

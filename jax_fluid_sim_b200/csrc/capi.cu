@@ -89,6 +89,7 @@ struct dgb_plan {
   int* cert_list = nullptr;
   int* cert_count = nullptr;
   int pos_grid = 0;
+  int trb_grid = 0;   // the same for k_hex_troubled, which shares the list
   HexCodes hex_codes = {nullptr, nullptr};
   double* hex_lift = nullptr;     // [E][12][N3] nodal BR2 lift scratch
   // MOOD subcell fallback
@@ -398,14 +399,35 @@ int run_positivity_hex(dgb_plan* p, const StatePtrs& S, cudaStream_t st) {
   return DGB_OK;
 }
 
+// Resident CTAs of k_hex_troubled over the whole GPU (set-up; at most one per element).
+template <int P, int NV>
+int hex_troubled_grid(dgb_plan* p) {
+  const size_t sm = sizeof(double) * (size_t)hex_troubled_smem<P, NV>();
+  int rc;
+  if ((rc = prepare(k_hex_troubled<P, NV>, sm))) return rc;
+  int dev = 0, sms = 0, per_sm = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hex_troubled<P, NV>, kThreads, sm));
+  const long long grid = (long long)std::max(per_sm, 1) * std::max(sms, 1);
+  p->trb_grid = (int)std::min<long long>(grid, std::max(p->dev.blk[0].E, 1));
+  return DGB_OK;
+}
+
+// Troubled-cell detection on the sum-factorised path: the warp pre-pass (k_hex_sensor) settles the
+// predicted and the certified elements and lists the rest, which k_hex_troubled tests in full.
 template <int P, int NV>
 int run_troubled_hex(dgb_plan* p, const StatePtrs& S, double* sensor, uint8_t* flags, const PredictArgs& pa,
                      cudaStream_t st) {
   const size_t sm = sizeof(double) * (size_t)hex_troubled_smem<P, NV>();
-  int rc;
-  if ((rc = prepare(k_hex_troubled<P, NV>, sm))) return rc;
-  k_hex_troubled<P, NV><<<p->dev.blk[0].E, kThreads, sm, st>>>(p->dev, S, 0, p->hex_tables, p->lim, sensor, flags,
-                                                               pa);
+  const BlockDev& B = p->dev.blk[0];
+  if (B.E == 0) return DGB_OK;
+  CK(cudaMemsetAsync(p->cert_count, 0, sizeof(int), st));
+  k_hex_sensor<P, NV><<<blocks_for(B.E, kThreads / 32), kThreads, 0, st>>>(p->dev, S, 0, p->hex_tables, p->lim,
+                                                                          sensor, flags, pa, p->cert_list,
+                                                                          p->cert_count);
+  k_hex_troubled<P, NV><<<p->trb_grid, kThreads, sm, st>>>(p->dev, S, 0, p->hex_tables, p->lim, sensor, flags, pa,
+                                                           p->cert_list, p->cert_count);
   CK(cudaGetLastError());
   return DGB_OK;
 }
@@ -1150,6 +1172,11 @@ int dgb_plan_finalize(dgb_plan* p) {
                                                               : hex_positivity_grid<3, 5>(p))
                  : (deg == 1 ? hex_positivity_grid<1, 16>(p) : deg == 2 ? hex_positivity_grid<2, 16>(p)
                                                                : hex_positivity_grid<3, 16>(p));
+    if (rc) return rc;
+    rc = NV == 5 ? (deg == 1 ? hex_troubled_grid<1, 5>(p) : deg == 2 ? hex_troubled_grid<2, 5>(p)
+                                                             : hex_troubled_grid<3, 5>(p))
+                 : (deg == 1 ? hex_troubled_grid<1, 16>(p) : deg == 2 ? hex_troubled_grid<2, 16>(p)
+                                                              : hex_troubled_grid<3, 16>(p));
     if (rc) return rc;
   }
   p->npartials = 0;

@@ -73,13 +73,19 @@ __device__ __forceinline__ int axis_stride(int a) { return a == 0 ? 1 : (a == 1 
 // at stride `stride` between consecutive entries) keeps its inputs and the (OUT x IN) matrix in
 // registers and produces the whole output line.  lines = number of lines; a line's first input
 // sits at in_base(line), its first output at out_base(line); outputs also at stride ostride.
+// The lines are shared among the block's threads, or, with first/step = lane/32, among one warp's
+// lanes; a line's arithmetic does not depend on which thread takes it.
 template <int IN, int OUT, bool ACC, typename T, typename InBase, typename OutBase>
 __device__ __forceinline__ void pencil(const T* in, T* out, const T* M, int lines, int istride, int ostride,
-                                       InBase in_base, OutBase out_base) {
+                                       InBase in_base, OutBase out_base, int first = -1, int step = 0) {
   T m[OUT * IN];
 #pragma unroll
   for (int k = 0; k < OUT * IN; ++k) m[k] = M[k];
-  for (int line = threadIdx.x; line < lines; line += blockDim.x) {
+  if (first < 0) {
+    first = threadIdx.x;
+    step = blockDim.x;
+  }
+  for (int line = first; line < lines; line += step) {
     const T* src = in + in_base(line);
     T x[IN];
 #pragma unroll
@@ -111,6 +117,22 @@ __device__ __forceinline__ void tensor3(const T* in, T* out, T* t1, T* t2, const
                       [](int l) { return (l / (OX * OY)) * IZ * OX * OY + l % (OX * OY); },
                       [](int l) { return (l / (OX * OY)) * OZ * OX * OY + l % (OX * OY); });
   __syncthreads();
+}
+
+// tensor3 with one N x N matrix on all three axes, worked by one warp (same arithmetic per output).
+template <int C, int N, typename T>
+__device__ __forceinline__ void warp_tensor3(const T* in, T* out, T* t1, T* t2, const T* M) {
+  const int lane = threadIdx.x & 31;
+  pencil<N, N, false>(in, t1, M, C * N * N, 1, 1, [](int l) { return l * N; }, [](int l) { return l * N; }, lane, 32);
+  __syncwarp();
+  pencil<N, N, false>(t1, t2, M, C * N * N, N, N,
+                      [](int l) { return (l / N) * N * N + l % N; },
+                      [](int l) { return (l / N) * N * N + l % N; }, lane, 32);
+  __syncwarp();
+  pencil<N, N, false>(t2, out, M, C * N * N, N * N, N * N,
+                      [](int l) { return (l / (N * N)) * N * N * N + l % (N * N); },
+                      [](int l) { return (l / (N * N)) * N * N * N + l % (N * N); }, lane, 32);
+  __syncwarp();
 }
 
 // 2-D: out[c][k2][k1] = sum M2[k2][j2] M1[k1][j1] in[c][j2][j1]
@@ -910,7 +932,9 @@ __global__ void __launch_bounds__(kThreads) k_hex_positivity(const DevPlan P_, c
 template <int P, int NV>
 __global__ void __launch_bounds__(kThreads) k_hex_troubled(const DevPlan P_, const StatePtrs S, int b,
                                                           const HexTables tables, const LimiterConst Lc,
-                                                          double* sensor_out, uint8_t* flag_out, const PredictArgs pa) {
+                                                          double* sensor_out, uint8_t* flag_out, const PredictArgs pa,
+                                                          const int* __restrict__ list,
+                                                          const int* __restrict__ count) {
   using D = HexDims<P>;
   constexpr int N = D::N, Q = D::Q, N3 = D::N3, Q3 = D::Q3, QF2 = D::QF2;
   constexpr int NS = N3 + Q3 + 6 * QF2;
@@ -927,23 +951,15 @@ __global__ void __launch_bounds__(kThreads) k_hex_troubled(const DevPlan P_, con
   __shared__ double mean[NV];
   __shared__ double red[4][kThreads / 32];
   const BlockDev& B = P_.blk[b];
-  const int e = blockIdx.x;
-  if (predicted_skip(pa, e, flag_out)) return;
-  const double* Ug = S.b[b] + (size_t)e * N3 * NV;
-  // nodal certificate of admissible samples and mean: then only the sensor needs computing
-  const bool certified = nodal_certificate<NV>(Ug, N3, P_.ph, Lc.lebesgue, Lc.density_floor,
-                                                       Lc.pressure_floor, 0.0);
+  // The elements are those of list[0, *count): the ones k_hex_sensor neither skipped (predicted)
+  // nor certified.  Each CTA loads the tables once and takes the listed elements in a grid stride.
   load_tables<P>(tables, tb);
   __syncthreads();
-  if (certified) {
-    for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
-      const int v = idx / N3, l = idx % N3;
-      U[idx] = Ug[tb->lex2node[l] * NV + v];
-    }
-    __syncthreads();
-  } else {
-    hex_samples<P, NV>(tb, Ug, U, Smp, t1, t2, vq, fs);
-  }
+  const int n = *count;
+  for (int item = blockIdx.x; item < n; item += gridDim.x) {
+  const int e = list[item];
+  const double* Ug = S.b[b] + (size_t)e * N3 * NV;
+  hex_samples<P, NV>(tb, Ug, U, Smp, t1, t2, vq, fs);
   for (int l = threadIdx.x; l < N3; l += blockDim.x) {
     double u[NV], W[NV];
 #pragma unroll
@@ -957,7 +973,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_troubled(const DevPlan P_, con
   // tensor product of the 1-D projector onto span{1, xi} (three passes of N x N)
   if (P >= 2) tensor3<2, N, N, N, N, N, N, false>(Mon, Low, t1, t2, tb->p1d, tb->p1d, tb->p1d);
   __shared__ double part[kThreads / 32][NV + 1];
-  if (!certified) hex_cell_mean<NV>(vq, B.wdet + (size_t)e * Q3, Q3, mean, part);
+  hex_cell_mean<NV>(vq, B.wdet + (size_t)e * Q3, Q3, mean, part);
   double hi0 = 0.0, hi1 = 0.0, sc0 = 0.0, sc1 = 0.0;
   if (P >= 2) {
     for (int i = threadIdx.x; i < N3; i += blockDim.x) {
@@ -983,7 +999,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_troubled(const DevPlan P_, con
   }
   __syncthreads();
   bool bad = false;
-  for (int r = threadIdx.x; r <= (certified ? -1 : NS); r += blockDim.x) {
+  for (int r = threadIdx.x; r <= NS; r += blockDim.x) {
     double s[NV], W[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) s[v] = r < NS ? Smp[v * NS + r] : mean[v];
@@ -1008,6 +1024,87 @@ __global__ void __launch_bounds__(kThreads) k_hex_troubled(const DevPlan P_, con
       value = (isnan(r0) || isnan(r1)) ? NAN : fmax(r0, r1);
     }
     const bool detected = (value > Lc.sensor_threshold) || any_bad;
+    if (sensor_out) sensor_out[e] = value;
+    if (flag_out) flag_out[e] = (uint8_t)detected;
+    count_prediction(pa, e, detected);
+  }
+  __syncthreads();   // the next element reuses the shared buffers
+  }
+}
+
+// Troubled-cell pre-pass, one warp per element: predicted elements are flagged and skipped (as in
+// predicted_skip); an element whose nodal values certify admissible samples and mean
+// (certificate_from_range with the absolute floors) gets its sensor here (the same arithmetic and
+// summation order as k_hex_troubled: the P1 projection by the same pencils, the squares summed
+// per 32 nodes by the same shuffle tree) and its flag; every other element is appended to list
+// for k_hex_troubled.  *count must be zero before the launch.
+template <int P, int NV>
+__global__ void __launch_bounds__(kThreads) k_hex_sensor(const DevPlan P_, const StatePtrs S, int b,
+                                                        const HexTables tables, const LimiterConst Lc,
+                                                        double* sensor_out, uint8_t* flag_out, const PredictArgs pa,
+                                                        int* __restrict__ list, int* __restrict__ count) {
+  using D = HexDims<P>;
+  constexpr int N = D::N, N3 = D::N3;
+  __shared__ double work[kThreads / 32][4 * 2 * N3];   // per warp: Mon, Low, t1, t2
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int E = P_.blk[b].E;
+  const int e = blockIdx.x * (kThreads / 32) + warp;
+  if (e >= E) return;
+  if (pa.mode == 1 && pa.pred && pa.pred[e]) {
+    if (lane == 0) {
+      if (flag_out) flag_out[e] = 1;
+      if (pa.counts) atomicAdd(pa.counts + 1, 1ULL);
+    }
+    return;
+  }
+  const double* Ug = S.b[b] + (size_t)e * N3 * NV;
+  double mn[5], mx[5];
+  const bool fin = warp_nodal_range<NV, N3>(Ug, mn, mx);
+  if (!(fin && certificate_from_range(mn, mx, P_.ph, Lc.lebesgue, Lc.density_floor, Lc.pressure_floor, 0.0))) {
+    if (lane == 0) list[atomicAdd(count, 1)] = e;
+    return;
+  }
+  double* Mon = work[warp];
+  double* Low = Mon + 2 * N3;
+  double* t1 = Low + 2 * N3;
+  double* t2 = t1 + 2 * N3;
+  for (int l = lane; l < N3; l += 32) {
+    double u[NV], W[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) u[v] = Ug[tables.lex2node[l] * NV + v];
+    primitive<NV>(P_.ph, u, W);
+    Mon[l] = W[0];
+    Mon[N3 + l] = W[4];
+  }
+  __syncwarp();
+  double value = 0.0;
+  if (P >= 2) {
+    warp_tensor3<2, N>(Mon, Low, t1, t2, tables.p1d);
+    // squares of the nodes lane and lane + 32, each set reduced by the block kernel's tree
+    double h[2][4] = {};
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+      const int i = lane + 32 * half;
+      if (i < N3) {
+        const double m0 = Mon[i], m1 = Mon[N3 + i];
+        const double d0 = m0 - Low[i], d1 = m1 - Low[N3 + i];
+        h[half][0] += d0 * d0;
+        h[half][1] += d1 * d1;
+        h[half][2] += m0 * m0;
+        h[half][3] += m1 * m1;
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        for (int o = 16; o > 0; o >>= 1) h[half][k] += __shfl_xor_sync(0xffffffff, h[half][k], o);
+    }
+    double t[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) t[k] = ((0.0 + h[0][k]) + h[1][k]);
+    const double r0 = t[0] / fmax(t[2], 1.0e-12), r1 = t[1] / fmax(t[3], 1.0e-12);
+    value = (isnan(r0) || isnan(r1)) ? NAN : fmax(r0, r1);
+  }
+  if (lane == 0) {
+    const bool detected = value > Lc.sensor_threshold;
     if (sensor_out) sensor_out[e] = value;
     if (flag_out) flag_out[e] = (uint8_t)detected;
     count_prediction(pa, e, detected);
