@@ -384,7 +384,7 @@ int dgb_react_block(dgb_chem* chem, const double* U, double* out, int64_t num_el
  * A small MLP (8 features -> 64 -> 64 -> 64 -> 1, ReLU, sigmoid) that predicts from a stage's
  * base state which elements the MOOD a-posteriori test (hybrid/limiter.py:285-300) will flag,
  * so that they go to the subcell scheme without the failed high-order attempt.  The test
- * stays the fallback and the judge.  Parameters are DGB_MLP_PARAMS floats in the order
+ * stays the fallback and the arbiter.  Parameters are DGB_MLP_PARAMS floats in the order
  * W1[8][64], b1[64], W2[64][64], b2[64], W3[64][64], b3[64], w4[64], b4; norm is the
  * features' mean[8] then 1/std[8].  All arrays are device arrays. */
 enum { DGB_MLP_FEATURES = 8, DGB_MLP_PARAMS = 8961 };

@@ -1,6 +1,6 @@
 // Learned troubled-cell predictor: element features, inference and training (no reference
 // counterpart; the reference only has the a-posteriori MOOD detector, hybrid/limiter.py:150-185,
-// 285-300, which stays the judge).
+// 285-300, which stays the arbiter).
 //
 // Features (8 per element, from the stage's base state, before the high-order update):
 //   0, 1  log10 of the Persson high-mode fraction of rho and of p (the detector's sensor:

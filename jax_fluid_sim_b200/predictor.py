@@ -5,7 +5,7 @@ No reference counterpart: the reference only has the a-posteriori detector
 flags the elements that the detector is expected to reject; inside
 ``HybridSSPRK3.checked_step`` those go to the subcell finite-volume scheme without the
 failed high-order attempt, while every other element is still tested a posteriori, so
-the detector stays the fallback and the judge.
+the detector stays the fallback and the arbiter.
 
 Everything runs in hand-written kernels (``csrc/mlp_kernels.cuh``): features
 (``dgb_mlp_features``), training (``dgb_mlp_train_step``: forward, backward, Adam on float32
