@@ -82,3 +82,29 @@ def test_certificate_refuses_non_finite_values():
     assert certificate(U, 1.0, 1e-10, 1e-10, 0.05)
     U[3, 2] = np.nan
     assert not certificate(U, 1.0, 1e-10, 1e-10, 0.05)
+
+
+@pytest.mark.parametrize("etype", ["wedge", "tetra", "hexahedron"])
+def test_certificate_is_sound_on_the_dense_sample_rows(etype):
+    """The dense kernels take L as the largest row sum of [I; B; B_face] (dgb_plan_set_block): the
+    certificate is sound with that L for every element type's sample rows."""
+    src = meshgen.hybrid_box((3, 3, 3), seed=5)
+    plan = Plan(HybridMesh(src), 2)
+    bp = next(b for b in plan.blocks if b.etype == etype) if etype != "hexahedron" else \
+        Plan(HybridMesh(meshgen.box_hex((3, 3, 3))), 2).blocks[0]
+    rows = np.concatenate([np.eye(bp.Np), bp.ref.B, bp.face_sample_B])
+    L = max(1.0, np.abs(np.concatenate([bp.ref.B, bp.face_sample_B])).sum(axis=1).max())
+    rng = np.random.default_rng(7)
+    base = np.array([1.0, 0.5, -0.3, 0.2, 2.5 + 0.5 * (0.25 + 0.09 + 0.04)])
+    passed = 0
+    for trial in range(400):
+        amp = 10.0 ** rng.uniform(-4, 0.3)
+        U = base[None, :] * (1.0 + amp * rng.standard_normal((bp.Np, 5)))
+        S = rows @ U
+        w = bp.ref.weights * rng.uniform(0.5, 2.0, bp.Nq)
+        mean = w @ (bp.ref.B @ U) / w.sum()
+        if certificate(U, L, 1e-10, 1e-10, 0.05):
+            passed += 1
+            assert S[:, 0].min() >= 0.05 * mean[0]
+            assert pressure(S).min() >= 0.05 * pressure(mean)
+    assert passed > 50
