@@ -957,78 +957,78 @@ __global__ void __launch_bounds__(kThreads) k_hex_troubled(const DevPlan P_, con
   __syncthreads();
   const int n = *count;
   for (int item = blockIdx.x; item < n; item += gridDim.x) {
-  const int e = list[item];
-  const double* Ug = S.b[b] + (size_t)e * N3 * NV;
-  hex_samples<P, NV>(tb, Ug, U, Smp, t1, t2, vq, fs);
-  for (int l = threadIdx.x; l < N3; l += blockDim.x) {
-    double u[NV], W[NV];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) u[v] = U[v * N3 + l];
-    primitive<NV>(P_.ph, u, W);
-    Mon[l] = W[0];
-    Mon[N3 + l] = W[4];
-  }
-  __syncthreads();
-  // P1 projection of (rho, p): the nodal projector onto the trilinear space is the threefold
-  // tensor product of the 1-D projector onto span{1, xi} (three passes of N x N)
-  if (P >= 2) tensor3<2, N, N, N, N, N, N, false>(Mon, Low, t1, t2, tb->p1d, tb->p1d, tb->p1d);
-  __shared__ double part[kThreads / 32][NV + 1];
-  hex_cell_mean<NV>(vq, B.wdet + (size_t)e * Q3, Q3, mean, part);
-  double hi0 = 0.0, hi1 = 0.0, sc0 = 0.0, sc1 = 0.0;
-  if (P >= 2) {
-    for (int i = threadIdx.x; i < N3; i += blockDim.x) {
-      const double m0 = Mon[i], m1 = Mon[N3 + i];
-      const double d0 = m0 - Low[i], d1 = m1 - Low[N3 + i];
-      hi0 += d0 * d0;
-      hi1 += d1 * d1;
-      sc0 += m0 * m0;
-      sc1 += m1 * m1;
+    const int e = list[item];
+    const double* Ug = S.b[b] + (size_t)e * N3 * NV;
+    hex_samples<P, NV>(tb, Ug, U, Smp, t1, t2, vq, fs);
+    for (int l = threadIdx.x; l < N3; l += blockDim.x) {
+      double u[NV], W[NV];
+  #pragma unroll
+      for (int v = 0; v < NV; ++v) u[v] = U[v * N3 + l];
+      primitive<NV>(P_.ph, u, W);
+      Mon[l] = W[0];
+      Mon[N3 + l] = W[4];
     }
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    hi0 += __shfl_xor_sync(0xffffffff, hi0, o);
-    hi1 += __shfl_xor_sync(0xffffffff, hi1, o);
-    sc0 += __shfl_xor_sync(0xffffffff, sc0, o);
-    sc1 += __shfl_xor_sync(0xffffffff, sc1, o);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    red[0][threadIdx.x >> 5] = hi0;
-    red[1][threadIdx.x >> 5] = hi1;
-    red[2][threadIdx.x >> 5] = sc0;
-    red[3][threadIdx.x >> 5] = sc1;
-  }
-  __syncthreads();
-  bool bad = false;
-  for (int r = threadIdx.x; r <= NS; r += blockDim.x) {
-    double s[NV], W[NV];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) s[v] = r < NS ? Smp[v * NS + r] : mean[v];
-    primitive<NV>(P_.ph, s, W);
-    bool finite = true;
-#pragma unroll
-    for (int v = 0; v < NV; ++v) finite &= isfinite(W[v]);
-    bad |= !finite || (W[0] < Lc.density_floor) || (W[4] < Lc.pressure_floor);
-  }
-  const bool any_bad = __syncthreads_or(bad);
-  if (threadIdx.x == 0) {
-    double h0 = 0, h1 = 0, s0 = 0, s1 = 0;
-    for (int k = 0; k < kThreads / 32; ++k) {
-      h0 += red[0][k];
-      h1 += red[1][k];
-      s0 += red[2][k];
-      s1 += red[3][k];
-    }
-    double value = 0.0;
+    __syncthreads();
+    // P1 projection of (rho, p): the nodal projector onto the trilinear space is the threefold
+    // tensor product of the 1-D projector onto span{1, xi} (three passes of N x N)
+    if (P >= 2) tensor3<2, N, N, N, N, N, N, false>(Mon, Low, t1, t2, tb->p1d, tb->p1d, tb->p1d);
+    __shared__ double part[kThreads / 32][NV + 1];
+    hex_cell_mean<NV>(vq, B.wdet + (size_t)e * Q3, Q3, mean, part);
+    double hi0 = 0.0, hi1 = 0.0, sc0 = 0.0, sc1 = 0.0;
     if (P >= 2) {
-      const double r0 = h0 / fmax(s0, 1.0e-12), r1 = h1 / fmax(s1, 1.0e-12);
-      value = (isnan(r0) || isnan(r1)) ? NAN : fmax(r0, r1);
+      for (int i = threadIdx.x; i < N3; i += blockDim.x) {
+        const double m0 = Mon[i], m1 = Mon[N3 + i];
+        const double d0 = m0 - Low[i], d1 = m1 - Low[N3 + i];
+        hi0 += d0 * d0;
+        hi1 += d1 * d1;
+        sc0 += m0 * m0;
+        sc1 += m1 * m1;
+      }
     }
-    const bool detected = (value > Lc.sensor_threshold) || any_bad;
-    if (sensor_out) sensor_out[e] = value;
-    if (flag_out) flag_out[e] = (uint8_t)detected;
-    count_prediction(pa, e, detected);
-  }
-  __syncthreads();   // the next element reuses the shared buffers
+    for (int o = 16; o > 0; o >>= 1) {
+      hi0 += __shfl_xor_sync(0xffffffff, hi0, o);
+      hi1 += __shfl_xor_sync(0xffffffff, hi1, o);
+      sc0 += __shfl_xor_sync(0xffffffff, sc0, o);
+      sc1 += __shfl_xor_sync(0xffffffff, sc1, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      red[0][threadIdx.x >> 5] = hi0;
+      red[1][threadIdx.x >> 5] = hi1;
+      red[2][threadIdx.x >> 5] = sc0;
+      red[3][threadIdx.x >> 5] = sc1;
+    }
+    __syncthreads();
+    bool bad = false;
+    for (int r = threadIdx.x; r <= NS; r += blockDim.x) {
+      double s[NV], W[NV];
+  #pragma unroll
+      for (int v = 0; v < NV; ++v) s[v] = r < NS ? Smp[v * NS + r] : mean[v];
+      primitive<NV>(P_.ph, s, W);
+      bool finite = true;
+  #pragma unroll
+      for (int v = 0; v < NV; ++v) finite &= isfinite(W[v]);
+      bad |= !finite || (W[0] < Lc.density_floor) || (W[4] < Lc.pressure_floor);
+    }
+    const bool any_bad = __syncthreads_or(bad);
+    if (threadIdx.x == 0) {
+      double h0 = 0, h1 = 0, s0 = 0, s1 = 0;
+      for (int k = 0; k < kThreads / 32; ++k) {
+        h0 += red[0][k];
+        h1 += red[1][k];
+        s0 += red[2][k];
+        s1 += red[3][k];
+      }
+      double value = 0.0;
+      if (P >= 2) {
+        const double r0 = h0 / fmax(s0, 1.0e-12), r1 = h1 / fmax(s1, 1.0e-12);
+        value = (isnan(r0) || isnan(r1)) ? NAN : fmax(r0, r1);
+      }
+      const bool detected = (value > Lc.sensor_threshold) || any_bad;
+      if (sensor_out) sensor_out[e] = value;
+      if (flag_out) flag_out[e] = (uint8_t)detected;
+      count_prediction(pa, e, detected);
+    }
+    __syncthreads();   // the next element reuses the shared buffers
   }
 }
 
