@@ -43,3 +43,14 @@ def pytest_collection_modifyitems(config, items):
     for item in items:
         if "gpu" in item.keywords:
             item.add_marker(skip)
+
+
+@pytest.fixture(scope="session", autouse=True)
+def native_library():
+    """Plan set-up calls the host routines of libdgb200.so (no GPU needed): build the library once
+    when it is missing (nvcc cross-compiles for sm_100a without a GPU).  An existing library is
+    used as it is."""
+    from jax_fluid_sim_b200 import build
+    if not build.LIB.exists():
+        build.build()
+    yield
