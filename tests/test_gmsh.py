@@ -180,3 +180,31 @@ def test_hybrid_mesh_and_solver_take_a_path(tmp_path):
     _same_faces(src, HybridMesh(str(path)).source)
     solver = HybridCompressibleSolver(str(path), polynomial_degree=2)
     assert [b.element_type for b in solver.mesh.element_blocks] == ["hexahedron", "wedge", "tetra"]
+
+
+def test_msh41_hexahedron27_reads_like_msh22(tmp_path):
+    """The same Gmsh-written hexahedron27 cells, written again as MSH 4.1 (one entity, one node
+    block, one element block), read to the same meshio-ordered cells as the MSH 2.2 fixture."""
+    from pathlib import Path
+    src22 = gmsh.read_msh(Path(__file__).parent / "golden" / "gmsh_hex27_cylinder.msh")
+    raw = Path(__file__).parent / "golden" / "gmsh_hex27_cylinder.msh"
+    lines = raw.read_text().splitlines()
+    nodes = lines[lines.index("$Nodes") + 2:lines.index("$EndNodes")]
+    elems = lines[lines.index("$Elements") + 2:lines.index("$EndElements")]
+    n = len(nodes)
+    out = ["$MeshFormat", "4.1 0 8", "$EndMeshFormat", "$PhysicalNames", "1", '3 1 "fluid"', "$EndPhysicalNames",
+           "$Entities", "0 0 0 1", "1 -9 -9 -9 9 9 9 1 1 0", "$EndEntities",
+           "$Nodes", f"1 {n} 1 {n}", f"3 1 0 {n}"]
+    out += [ln.split()[0] for ln in nodes]
+    out += [" ".join(ln.split()[1:]) for ln in nodes]
+    out += ["$EndNodes", "$Elements", f"1 {len(elems)} 1 {len(elems)}", f"3 1 12 {len(elems)}"]
+    out += [" ".join([ln.split()[0]] + ln.split()[5:]) for ln in elems]
+    out.append("$EndElements")
+    path = tmp_path / "hex27_v41.msh"
+    path.write_text("\n".join(out) + "\n")
+    src41 = gmsh.read_msh(path)
+    np.testing.assert_array_equal(src41.points, src22.points)
+    (c41, a41), = src41.cells
+    (c22, a22), = src22.cells
+    assert c41 == c22 == "hexahedron27"
+    np.testing.assert_array_equal(a41, a22)
