@@ -101,6 +101,18 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+def max_over_ranks(value, world, device="cuda"):
+    """The largest of every rank's value: a time measured on several GPUs is the slowest rank's.
+    Every rank takes part and gets the result."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def workload(scale="full"):
     from jax_fluid_sim_b200 import meshgen
     if scale == "full":
@@ -276,11 +288,7 @@ def run_ours(args):
                 integ.checked_step_inplace(U, dt, bc)
             stop.record()
             torch.cuda.synchronize()
-        ms = start.elapsed_time(stop)
-        if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(start.elapsed_time(stop), world)
         valid, rmin, pmin = integ._status_tuple()
         return dict(ms=ms, U=U, clocks=clocks.summary(), valid=valid, rho_min=rmin, p_min=pmin,
                     value=dofs * args.steps * world / (ms / 1e3))
