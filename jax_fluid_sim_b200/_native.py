@@ -197,6 +197,8 @@ def map_metrics(nodes, grad, index=None, weights=None, tangents=None, orientatio
     nodes = as_f64(nodes)
     grad = as_f64(grad)
     idx = None if index is None else as_i32(index)
+    if idx is not None and len(idx) and (idx.min() < 0 or idx.max() >= len(nodes)):
+        raise ValueError(f"element index out of range for {len(nodes)} node sets")
     count = len(nodes) if idx is None else len(idx)
     Q, n = grad.shape[0], grad.shape[1]
     if nodes.shape[1:] != (n, 3):

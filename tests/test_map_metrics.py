@@ -60,6 +60,8 @@ def test_bad_arguments_are_errors():
         N.map_metrics(np.zeros((2, 8, 3)), g, outputs=("wdet",))          # wdet needs weights
     with pytest.raises(ValueError):
         N.map_metrics(np.zeros((2, 8, 3)), g, weights=np.ones(1), outputs=("normals",))   # needs tangents
+    with pytest.raises(ValueError):
+        N.map_metrics(np.zeros((2, 8, 3)), g, index=[0, 2], outputs=("det",))          # index past the nodes
 
 
 def _subcell_face_metrics_numpy(pv, cen, faces, owners, neighbors):
