@@ -318,10 +318,15 @@ int dgb_rhs_profile(dgb_plan* plan, const dgb_state* U, float* ms_out, void* str
  *
  * Scratch: a file-scope device array of 2^20 doubles (8 MiB) that every GPU which loads
  * the library keeps until the process exits; at most 1048576 elements per call (larger
- * blocks are rejected with DGB_ERR_ARGUMENT).  The first call on a device looks up that
- * array's device address (cudaGetSymbolAddress) with the device current; make that first
- * call before any stream capture.  All calls share the array: calls whose kernels overlap
- * on the GPU (different streams or threads) race on it.  Errors are reported by
+ * blocks are rejected with DGB_ERR_ARGUMENT, and so is a negative degree).  The first call
+ * on a device looks up that array's device address (cudaGetSymbolAddress) with the device
+ * current; make that first call before any stream capture.  Under CUDA's default lazy
+ * module loading that first call is also when the driver loads this code's module on the
+ * device and with it the 8 MiB array: that one time the driver itself takes device
+ * memory.  A caller that reserves its whole pool up front should make the first call
+ * before reserving it (or run with CUDA_MODULE_LOADING=EAGER, which loads the module, and
+ * the array, when the library is loaded).  All calls share the array: calls whose kernels
+ * overlap on the GPU (different streams or threads) race on it.  Errors are reported by
  * dgb_noalloc_last_error(). */
 int dgb_stable_dt_noalloc(const double* U, const double* length, int num_elements, int num_nodes, int nvars,
                           int degree, double gamma, double gas_constant, double dynamic_viscosity,

@@ -4,19 +4,25 @@
 
 The library is a plain C-ABI shared object (see ``include/dgb200.h``) loaded by
 ctypes; it is built in the package directory so that it travels with the tree.
+Each translation unit is compiled to its own object in parallel (``_build/``), and
+only the units whose sources changed are recompiled; then nvcc links the library.
 """
 
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 LIB = PKG / "libdgb200.so"
-SOURCES = [PKG / "csrc" / "capi.cu", PKG / "csrc" / "noalloc.cu", PKG / "csrc" / "chemistry.cu",
-           PKG / "csrc" / "raster.cu", PKG / "csrc" / "setup.cpp"]
-DEPENDS = sorted((PKG / "csrc").glob("*.c*")) + [ROOT / "include" / "dgb200.h"]
+OBJ = PKG / "_build"
+SOURCES = [PKG / "csrc" / "capi.cu",
+           PKG / "csrc" / "noalloc.cu", PKG / "csrc" / "chemistry.cu", PKG / "csrc" / "raster.cu",
+           PKG / "csrc" / "setup.cpp"]
+HEADERS = sorted((PKG / "csrc").glob("*.cuh")) + sorted((PKG / "csrc").glob("*.h")) + [ROOT / "include" / "dgb200.h"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
 def nvcc():
@@ -26,29 +32,54 @@ def nvcc():
     raise RuntimeError("nvcc not found")
 
 
+def _object(src):
+    return OBJ / (src.name + ".o")
+
+
+def _stale(src, newest_header):
+    obj = _object(src)
+    if not obj.exists():
+        return True
+    t = obj.stat().st_mtime
+    return src.stat().st_mtime > t or newest_header > t
+
+
 def up_to_date():
     if not LIB.exists():
         return False
     t = LIB.stat().st_mtime
-    return all(p.stat().st_mtime <= t for p in DEPENDS)
+    return all(p.stat().st_mtime <= t for p in SOURCES + HEADERS)
+
+
+def _compile(src, verbose):
+    cmd = [nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-I", str(ROOT / "include"),
+           "-c", str(src), "-o", str(_object(src))]
+    if verbose:
+        cmd += ["-Xptxas", "-v"]
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    if proc.returncode != 0:
+        raise RuntimeError(f"nvcc failed on {src.name}:\n" + proc.stdout + proc.stderr)
+    return proc.stderr
 
 
 def build(force=False, verbose=False):
     if not force and up_to_date():
         return LIB
-    cmd = [nvcc(), "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
-           "-shared", "-Xcompiler", "-fPIC", "-I", str(ROOT / "include"), "-o", str(LIB)]
+    OBJ.mkdir(exist_ok=True)
+    newest_header = max(p.stat().st_mtime for p in HEADERS)
+    todo = [s for s in SOURCES if force or _stale(s, newest_header)]
+    with ThreadPoolExecutor(max_workers=max(1, min(len(todo), os.cpu_count() or 1))) as pool:
+        logs = list(pool.map(lambda s: _compile(s, verbose), todo))
     if verbose:
-        cmd += ["-Xptxas", "-v"]
-    cmd += [str(s) for s in SOURCES]
+        for text in logs:
+            sys.stderr.write(text)
+    cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB)] + [str(_object(s)) for s in SOURCES]
     proc = subprocess.run(cmd, capture_output=True, text=True)
     if proc.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + proc.stdout + proc.stderr)
-    if verbose:
-        sys.stderr.write(proc.stderr)
+        raise RuntimeError("nvcc link failed:\n" + proc.stdout + proc.stderr)
     return LIB
 
 
 if __name__ == "__main__":
-    build(force=True, verbose="--verbose" in sys.argv)
+    build(force="--force" in sys.argv or "--verbose" in sys.argv, verbose="--verbose" in sys.argv)
     print(LIB)

@@ -48,7 +48,8 @@ def load_restart(path, element_types=None, into=None, device="cuda"):
     ``element_types``: the blocks to read (default: every ``U_*`` array in the file); a missing
     block raises ``KeyError`` as the reference's loader does.  ``into``: existing tensors
     {element_type: tensor} to fill in place (shapes must match); the copies are asynchronous on
-    the current stream from pinned staging buffers, which are kept alive until they finish.
+    the current stream from pinned staging buffers, which are kept alive until one synchronisation
+    of the stream after the last block.
     """
     with np.load(Path(path)) as restart:
         names = element_types if element_types is not None else [k[2:] for k in restart.files if k.startswith("U_")]
@@ -59,16 +60,20 @@ def load_restart(path, element_types=None, into=None, device="cuda"):
         if into is not None and name in into and tuple(into[name].shape) != a.shape:
             raise ValueError(f"U_{name} has shape {a.shape}; the buffer has {tuple(into[name].shape)}")
     states = {}
+    staging = []
     for name, a in arrays.items():
         if into is not None and name in into:
             dst = into[name]
             if dst.device.type == "cuda":
-                staging = torch.from_numpy(a).pin_memory()
-                dst.copy_(staging, non_blocking=True)
-                torch.cuda.current_stream().synchronize()
+                pinned = torch.from_numpy(a).pin_memory()
+                dst.copy_(pinned, non_blocking=True)
+                staging.append(pinned)
             else:
                 dst.copy_(torch.from_numpy(a))
             states[name] = dst
         else:
             states[name] = torch.as_tensor(a, device=device)
+    if staging:
+        # one wait for all blocks' copies; the pinned buffers live until then
+        torch.cuda.current_stream().synchronize()
     return states, current_time, step

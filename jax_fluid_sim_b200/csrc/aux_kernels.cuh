@@ -445,9 +445,11 @@ __global__ void __launch_bounds__(kThreads) k_rate(const DevPlan P, const StateP
     for (int i = lane; i < B.Np; i += 32) {
       double W[NV];
       primitive<NV>(P.ph, U + i * NV, W);
+      // jnp.maximum propagates NaN where fmax drops it: a NaN density or pressure makes the
+      // reference's rate NaN (then 1e7), so it is flagged before the floors
       const double rho = fmax(W[0], 1.0e-14), p = fmax(W[4], 1.0e-14);
       const double sp = sqrt(W[1] * W[1] + W[2] * W[2] + W[3] * W[3]) + sqrt(P.ph.gamma * p / rho);
-      en |= isnan(sp);
+      en |= isnan(W[0]) || isnan(W[4]) || isnan(sp);
       smax = fmax(smax, sp);
       rsum += rho;
     }

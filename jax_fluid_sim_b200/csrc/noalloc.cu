@@ -46,9 +46,11 @@ __global__ void k_rates_noalloc(const double* U, const double* length, int E, in
       const double vx = u[1] / srho, vy = u[2] / srho, vz = u[3] / srho;
       const double m2 = __dadd_rn(__dadd_rn(__dmul_rn(u[1], u[1]), __dmul_rn(u[2], u[2])), __dmul_rn(u[3], u[3]));
       const double p = __dmul_rn(gamma - 1.0, __dsub_rn(u[4], __dmul_rn(0.5, m2) / srho));
+      // a NaN density or pressure makes the reference's rate NaN (jnp.maximum keeps NaN,
+      // fmax would drop it), which it then maps to 1e7
       const double r = fmax(rho, 1.0e-14), pf = fmax(p, 1.0e-14);
       const double sp = sqrt(vx * vx + vy * vy + vz * vz) + sqrt(gamma * pf / r);
-      nan_seen |= isnan(sp);
+      nan_seen |= isnan(rho) || isnan(p) || isnan(sp);
       smax = fmax(smax, sp);
       rsum += r;
     }
@@ -102,6 +104,7 @@ int dgb_stable_dt_noalloc(const double* U, const double* length, int num_element
                           void* stream) {
   if (!U || !length || !dt_out) return noalloc_fail("null pointer argument");
   if (num_elements < 1 || num_nodes < 1 || nvars < 5) return noalloc_fail("empty or malformed state");
+  if (degree < 0) return noalloc_fail("polynomial degree must be non-negative");
   if (num_elements > kMaxElements)
     return noalloc_fail("dgb_stable_dt_noalloc handles at most 1048576 elements per call (" +
                         std::to_string(num_elements) + " given); use dgb_stable_dt or split the block");

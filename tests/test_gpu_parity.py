@@ -79,6 +79,27 @@ def test_dt_limiter_flags_step(case, label):
         close(res[k], g[f"step_{label}_{k}"], 1e-9)
 
 
+@pytest.mark.parametrize("case", ["smoke_p2", "box_p2", "box_p3:dense"])
+@pytest.mark.parametrize("poison", [0, 4, 1])
+def test_dt_of_nan_state_matches_reference(case, poison):
+    """A NaN in one node's density, energy or momentum makes the reference's rate NaN, which
+    stable_dt maps to 1e7 (jnp.maximum keeps NaN through the 1e-14 floors,
+    hybrid/time_integration.py:107-108,167).  With cfl = 5 the result 5e-7 lies inside the clip
+    range, so a kernel that dropped the NaN at a floor (a huge finite rate, clipped to 1e-7)
+    fails."""
+    from jax_fluid_sim_b200 import HybridSSPRK3
+    from oracle.dg import TimeIntegrator
+
+    from .test_oracle_golden import build as oracle_build
+    g, solver, op, bc = setup(case)
+    states = {k: np.array(g[f"U_smooth_{k}"]) for k in g["block_names"]}
+    first = g["block_names"][0]
+    states[first][1, 0, poison] = np.nan
+    expected = TimeIntegrator(oracle_build(case.partition(":")[0])[2], cfl=5.0).stable_dt(states)
+    assert abs(expected - 5e-7) <= 1e-18, expected
+    close(HybridSSPRK3(op, cfl=5.0).stable_dt(states, bc), expected, 1e-12)
+
+
 def test_uniform_state_is_steady():
     """A uniform state with no boundary ghost has an exactly zero inviscid residual (anchor form)."""
     from jax_fluid_sim_b200 import HybridCompressibleSolver, HybridMesh, HybridNavierStokesOperator

@@ -112,3 +112,38 @@ def test_shocked_mood_step_against_oracle(sphere):
     assert rmin == pytest.approx(ref_rmin, rel=1e-9) and pmin == pytest.approx(ref_pmin, rel=1e-9)
     for k in ref:
         _close(got[k], ref[k], 1e-9)
+
+
+def test_shocked_mood_flags_bit_exact(sphere):
+    """The MOOD troubled-cell flags on the benchmark's grid bit for bit against the oracle
+    (hybrid/limiter.py:285-300): on the shocked start and on the first stage's DG candidate
+    U + dt R(U), the state the detector judges inside the checked step."""
+    jfs, gas, mesh, u = sphere["jfs"], sphere["gas"], sphere["mesh"], sphere["u"]
+    from oracle.dg import PositivityLimiter, TimeIntegrator, TroubledCellSensor, mood_troubled
+    g, M = GAMMA, MACH
+    rho2 = (g + 1) * M ** 2 / ((g - 1) * M ** 2 + 2)
+    p2 = 1 + 2 * g / (g + 1) * (M ** 2 - 1)
+    states = {}
+    for b in mesh.element_blocks:
+        x = _node_xyz(mesh, b)
+        inside = np.broadcast_to(np.linalg.norm(x.mean(axis=1), axis=-1)[:, None] < 0.65, x.shape[:-1])
+        W = np.zeros(x.shape[:-1] + (5,))
+        W[..., 0] = np.where(inside, rho2, 1.0)
+        W[..., 1] = np.where(inside, u / rho2, u)
+        W[..., 4] = np.where(inside, p2, 1.0)
+        states[b.element_type] = gas.to_conserved(W)
+    oop, obc = sphere["oop"], sphere["obc"]
+    opos = PositivityLimiter(oop)
+    dt = TimeIntegrator(oop, cfl=0.3, limiter=opos).stable_dt(states)
+    rhs = oop.rhs(states, obc)
+    candidate = {k: states[k] + dt * rhs[k] for k in states}
+    op = sphere["op"]
+    lim = jfs.HybridMOODSubcellLimiter(op, positivity=jfs.HybridPositivityLimiter(op))
+    seen = 0
+    for s in (states, candidate):
+        ref = mood_troubled(oop, opos, TroubledCellSensor(oop), s)
+        got = lim.troubled(s)
+        for k in ref:
+            np.testing.assert_array_equal(got[k].cpu().numpy(), ref[k])
+            seen += int(ref[k].sum())
+    assert seen > 0, "the shocked start should flag some elements"

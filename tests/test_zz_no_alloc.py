@@ -34,10 +34,13 @@ def test_noalloc_dt_matches_planned_dt_twice():
     from jax_fluid_sim_b200 import HybridSSPRK3
     from jax_fluid_sim_b200 import _native as N
     L = N.lib()
-    for n, degree, mu, seed, cfl in (((4, 3, 3), 3, 0.01, 1, 0.3), ((6, 5, 2), 2, 0.0, 2, 0.15)):
+    # a viscous P3 case, then an inviscid P2 one on another mesh; both cfl values put the
+    # expected dt well inside the clip range (1e-7, 1e-3), so the rates are really compared
+    for n, degree, mu, seed, cfl in (((4, 3, 3), 3, 0.01, 1, 0.3), ((6, 5, 2), 2, 0.0, 2, 0.05)):
         solver, op, U = _case(n, degree, mu, seed)
         integ = HybridSSPRK3(op, cfl=cfl)
         expected = integ.stable_dt(U)
+        assert 2e-7 < expected < 0.9e-3, expected
         Ud = op.to_device(U)["hexahedron"]
         length = torch.as_tensor(op.plan.blocks[0].length, device="cuda")
         dt = torch.full((1,), -1.0, dtype=torch.float64, device="cuda")
@@ -51,6 +54,27 @@ def test_noalloc_dt_matches_planned_dt_twice():
         assert abs(got - expected) <= 1e-12 * abs(expected), (got, expected)
 
 
+def test_noalloc_nan_state_gives_reference_rate():
+    """A NaN density in one node: the reference maps that element's NaN rate to 1e7, so with
+    cfl = 5 the step is 5e-7, the same as the planned entry point's."""
+    from jax_fluid_sim_b200 import HybridSSPRK3
+    from jax_fluid_sim_b200 import _native as N
+    L = N.lib()
+    solver, op, U = _case((4, 3, 3), 2, 0.01, 3)
+    U["hexahedron"][2, 5, 0] = np.nan
+    expected = HybridSSPRK3(op, cfl=5.0).stable_dt(U)
+    assert abs(expected - 5e-7) <= 1e-18, expected
+    Ud = op.to_device(U)["hexahedron"]
+    length = torch.as_tensor(op.plan.blocks[0].length, device="cuda")
+    dt = torch.full((1,), -1.0, dtype=torch.float64, device="cuda")
+    E, Np, nv = Ud.shape
+    rc = L.dgb_stable_dt_noalloc(Ud.data_ptr(), length.data_ptr(), E, Np, nv, 2, solver.gamma, solver.gas_constant,
+                                 solver.dynamic_viscosity, solver.thermal_conductivity, op.br2_stabilization, 5.0,
+                                 dt.data_ptr(), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert rc == 0, L.dgb_noalloc_last_error()
+    assert abs(float(dt.item()) - expected) <= 1e-12 * expected
+
+
 def test_noalloc_rejects_oversized_blocks():
     from jax_fluid_sim_b200 import _native as N
     L = N.lib()
@@ -59,3 +83,7 @@ def test_noalloc_rejects_oversized_blocks():
                                  3.0, 0.3, dummy.data_ptr(), None)
     assert rc == -1
     assert b"at most 1048576 elements" in L.dgb_noalloc_last_error()
+    rc = L.dgb_stable_dt_noalloc(dummy.data_ptr(), dummy.data_ptr(), 1, 8, 5, -1, 1.4, 1.0, 0.0, 0.0,
+                                 3.0, 0.3, dummy.data_ptr(), None)
+    assert rc == -1
+    assert b"degree" in L.dgb_noalloc_last_error()
