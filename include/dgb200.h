@@ -227,6 +227,20 @@ int dgb_wall_forces(dgb_plan* plan, const dgb_state* U, const int32_t* wall_tags
  * zeros on the sum-factorised hexahedron path, whose launches are fixed.  Synchronises the
  * stream. */
 int dgb_plan_autotune(dgb_plan* plan, const dgb_state* U, int reps, int* widths, void* stream);
+/* Inviscid volume integrals of the dense blocks on the tensor cores (replaces the einsum
+ * contractions of HybridEulerOperator._volume_terms, hybrid/spatial.py:47-72, for those blocks):
+ * a tcgen05 kernel with three-term TF32 products (about float32 accuracy) and bulk-copied
+ * element tiles.  It applies to plans in precision mode 1 (mixed) without viscous terms, to
+ * blocks with an even node count of at most 40 and at most 128 volume points, 5 variables
+ * (prisms and tetrahedra up to P3); other blocks keep the CUDA-core kernel.  enable = 0 turns it
+ * off.  blocks_out (optional) receives how many blocks use it.  Packs the block's constant
+ * operands on the device the first time (synchronises the device). */
+int dgb_plan_set_tensor_cores(dgb_plan* plan, int enable, int* blocks_out);
+/* Error bits that kernels with bounded waits record on the device (1: a wait on the tensor
+ * cores or the bulk-copy engine ran out of time; the kernel released its tensor memory and
+ * returned without writing that tile).  Copies the word to host *out; reset = 1 clears it.
+ * Synchronises the device. */
+int dgb_plan_device_errors(dgb_plan* plan, int* out, int reset);
 
 /* HybridSSPRK3.stable_dt (hybrid/time_integration.py:93-169): writes the clipped dt
  * to the device double *dt_out. */

@@ -18,7 +18,7 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 LIB = PKG / "libdgb200.so"
 OBJ = PKG / "_build"
-SOURCES = [PKG / "csrc" / "capi.cu",
+SOURCES = [PKG / "csrc" / "capi.cu", PKG / "csrc" / "tc_volume.cu",
            PKG / "csrc" / "noalloc.cu", PKG / "csrc" / "chemistry.cu", PKG / "csrc" / "raster.cu",
            PKG / "csrc" / "setup.cpp"]
 HEADERS = sorted((PKG / "csrc").glob("*.cuh")) + sorted((PKG / "csrc").glob("*.h")) + [ROOT / "include" / "dgb200.h"]

@@ -12,6 +12,7 @@
 #include "hex_kernels.cuh"
 #include "mlp_kernels.cuh"
 #include "mood_kernels.cuh"
+#include "tc_volume.h"
 
 using namespace dgb;
 
@@ -112,6 +113,12 @@ struct dgb_plan {
   double* eul[DGB_MAX_BLOCKS] = {nullptr, nullptr, nullptr};
   double* vis[DGB_MAX_BLOCKS] = {nullptr, nullptr, nullptr};
   double* rec[DGB_MAX_BLOCKS] = {nullptr, nullptr, nullptr};
+  // tensor-core (tcgen05) inviscid volume kernel of the dense blocks (dgb_plan_set_tensor_cores)
+  TcShape tc[DGB_MAX_BLOCKS];
+  float* tc_image[DGB_MAX_BLOCKS] = {nullptr, nullptr, nullptr};
+  bool tc_on[DGB_MAX_BLOCKS] = {false, false, false};
+  int sm_count = 0;
+  int* dev_err = nullptr;   // DGB_DEVICE_* bits recorded by kernels with bounded waits
 };
 
 namespace {
@@ -138,6 +145,25 @@ int alloc(dgb_plan* p, size_t count, double** out) {
   p->allocations.push_back(d);
   CK(cudaMemset(d, 0, count * sizeof(double)));
   *out = static_cast<double*>(d);
+  return DGB_OK;
+}
+
+__global__ void k_to_float32(const double* __restrict__ src, float* __restrict__ dst, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = (float)src[i];
+}
+
+// A float32 copy of n device doubles, owned by the plan (null source: null copy).
+int to_float32(dgb_plan* p, const double* src, size_t n, float** out) {
+  *out = nullptr;
+  if (!src || n == 0) return DGB_OK;
+  void* d = nullptr;
+  CK(cudaMalloc(&d, n * sizeof(float)));
+  p->allocations.push_back(d);
+  k_to_float32<<<(unsigned)std::min<size_t>((n + 255) / 256, 148 * 16), 256>>>(src, static_cast<float*>(d), n);
+  CK(cudaGetLastError());
+  CK(cudaDeviceSynchronize());
+  *out = static_cast<float*>(d);
   return DGB_OK;
 }
 
@@ -274,7 +300,21 @@ int run_rhs_dense(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaSt
   if (ev) CK(cudaEventRecord(ev[2], st));
   if (ev) CK(cudaEventRecord(ev[3], st));     // the dense k_volume does the BR2 lift itself
   if ((rc = prepare(k_volume<NV, R>, p->smem_vol))) return rc;
-  k_volume<NV, R><<<p->launch_vol.cta0[P.nblocks], kThreads, p->smem_vol, st>>>(P, S, p->launch_vol);
+  if (sizeof(R) == sizeof(float) && NV == 5 && !P.viscous && (p->tc_on[0] || p->tc_on[1] || p->tc_on[2])) {
+    // tensor-core blocks first, then one launch of k_volume over the remaining blocks' CTA ranges
+    ElemLaunch rest = p->launch_vol;
+    rest.cta0[0] = 0;
+    for (int b = 0; b < P.nblocks; ++b) {
+      const int n = p->tc_on[b] ? 0 : p->launch_vol.cta0[b + 1] - p->launch_vol.cta0[b];
+      rest.cta0[b + 1] = rest.cta0[b] + n;
+      if (p->tc_on[b] && tc_volume(P, S, b, p->tc[b], p->tc_image[b], p->dev_err, p->sm_count, st))
+        return fail(DGB_ERR_CUDA, "tensor-core volume launch failed");
+    }
+    if (rest.cta0[P.nblocks] > 0)
+      k_volume<NV, R><<<rest.cta0[P.nblocks], kThreads, p->smem_vol, st>>>(P, S, rest);
+  } else {
+    k_volume<NV, R><<<p->launch_vol.cta0[P.nblocks], kThreads, p->smem_vol, st>>>(P, S, p->launch_vol);
+  }
   if (ev) CK(cudaEventRecord(ev[4], st));
   if (P.viscous)
     for (int ft = 0; ft < 2; ++ft)
@@ -1220,9 +1260,66 @@ int dgb_plan_finalize(dgb_plan* p) {
     p->partials = static_cast<Partial*>(d);
   }
   if ((rc = alloc(p, 1, &p->dt_scratch))) return rc;
+  {
+    double* d;
+    if ((rc = alloc(p, 1, &d))) return rc;
+    p->dev_err = reinterpret_cast<int*>(d);
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&p->sm_count, cudaDevAttrMultiProcessorCount, dev));
+  }
   if (p->hex && p->dev.viscous)
     if ((rc = alloc(p, (size_t)p->dev.blk[0].E * 12 * p->dev.blk[0].Np, &p->hex_lift))) return rc;
+  if (p->hex && p->prm.precision == 1) {
+    // float32 copies of the inverse mass matrices and the per-point inverse Jacobians that the
+    // mixed-precision hexahedron kernels read (half the bytes of the float64 tables)
+    BlockDev& B = p->dev.blk[0];
+    float* f;
+    if ((rc = to_float32(p, B.minv, (size_t)B.E * B.Np * B.Np, &f))) return rc;
+    B.minv32 = f;
+    if ((rc = to_float32(p, B.jinv, (size_t)B.E * B.Nq * 9, &f))) return rc;
+    B.jinv32 = f;
+    FaceDev& F = p->dev.face[1];
+    if (p->face_present[1]) {
+      if ((rc = to_float32(p, F.jinv, (size_t)F.F * 2 * F.nq * 9, &f))) return rc;
+      F.jinv32 = f;
+    }
+  }
   p->finalized = true;
+  return DGB_OK;
+}
+
+int dgb_plan_set_tensor_cores(dgb_plan* p, int enable, int* blocks_out) {
+  if (!p || !p->finalized) return fail(DGB_ERR_ARGUMENT, "plan not finalized");
+  int n = 0;
+  const bool allowed = enable && !p->hex && p->prm.precision == 1 && !p->dev.viscous && p->dev.nv == 5;
+  for (int b = 0; b < p->dev.nblocks; ++b) {
+    const BlockDev& B = p->dev.blk[b];
+    p->tc_on[b] = false;
+    if (!allowed || B.E == 0) continue;
+    const TcShape s = tc_shape(B.Np, B.Nq, p->dev.nv);
+    if (!s.eligible) continue;
+    if (!p->tc_image[b]) {
+      double* d;
+      int rc;
+      if ((rc = alloc(p, ((size_t)s.image_floats + 1) / 2, &d))) return rc;
+      p->tc_image[b] = reinterpret_cast<float*>(d);
+      if (tc_pack(B, s, p->tc_image[b], nullptr)) return fail(DGB_ERR_CUDA, "tensor-core operand packing failed");
+      CK(cudaDeviceSynchronize());
+    }
+    p->tc[b] = s;
+    p->tc_on[b] = true;
+    ++n;
+  }
+  p->generation++;
+  if (blocks_out) *blocks_out = n;
+  return DGB_OK;
+}
+
+int dgb_plan_device_errors(dgb_plan* p, int* out, int reset) {
+  if (!p || !out || !p->dev_err) return fail(DGB_ERR_ARGUMENT, "plan not finalized or null output");
+  CK(cudaMemcpy(out, p->dev_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (reset) CK(cudaMemset(p->dev_err, 0, sizeof(int)));
   return DGB_OK;
 }
 

@@ -59,6 +59,9 @@ struct BlockDev {
   const double* wref;     // [Nq] reference quadrature weights (dense path)
   const double* mref_inv; // [Np][Np] inverse of the reference mass matrix B^T diag(wref) B (dense path)
   const int32_t* ecase;   // [E] case of each element (ensembles; null for one case)
+  // float32 copies read by the mixed-precision hexahedron kernels (null in float64 plans)
+  const float* minv32;    // [E][Np][Np], same layout as minv
+  const float* jinv32;    // [E][Nq][9]
 };
 
 struct FaceDev {
@@ -76,6 +79,7 @@ struct FaceDev {
   double* jumpW;          // [F][nq][12]    0.5 w [v] (x) n
   double* liftF;          // [F][2][nq][12] br2 * B_f r_f per side
   double* fluxV;          // [F][nq][NV]    viscous normal flux times w
+  const float* jinv32;    // float32 copy of jinv (mixed-precision plans; else null)
 };
 
 struct DevPlan {
@@ -632,7 +636,7 @@ __global__ void __launch_bounds__(kThreads) k_wall_forces(const DevPlan P, int f
 }
 
 // Sums the CTAs' partials in order (one thread per component).
-__global__ void k_wall_forces_final(const double* __restrict__ partials, int n, double* __restrict__ out) {
+static __global__ void k_wall_forces_final(const double* __restrict__ partials, int n, double* __restrict__ out) {
   const int k = threadIdx.x;
   if (k >= kForceValues) return;
   double s = 0.0;

@@ -332,8 +332,15 @@ __global__ void __launch_bounds__(kThreads) k_hex_traces(const DevPlan P_, const
       const R gy = a0 == 1 ? gnv : (a0 == 0 ? g1v : g2v);
       const R gz = a0 == 2 ? gnv : g2v;
       const size_t pt = (size_t)fslot[lf] + q;
-      const double* J = fd.jinv + pt * 9;
-      fd.trG[pt * 12 + m * 3 + d] = (double)(gx * (R)J[0 * 3 + d] + gy * (R)J[1 * 3 + d] + gz * (R)J[2 * 3 + d]);
+      R J0, J1, J2;
+      if (sizeof(R) == sizeof(float) && fd.jinv32) {
+        const float* J = fd.jinv32 + pt * 9;
+        J0 = (R)J[0 * 3 + d], J1 = (R)J[1 * 3 + d], J2 = (R)J[2 * 3 + d];
+      } else {
+        const double* J = fd.jinv + pt * 9;
+        J0 = (R)J[0 * 3 + d], J1 = (R)J[1 * 3 + d], J2 = (R)J[2 * 3 + d];
+      }
+      fd.trG[pt * 12 + m * 3 + d] = (double)(gx * J0 + gy * J1 + gz * J2);
     }
   }
 }
@@ -374,8 +381,10 @@ __global__ void __launch_bounds__(kThreads) k_hex_lift(const DevPlan P_, int b, 
   }
   __syncthreads();
   for (int l = threadIdx.x; l < N3; l += blockDim.x) node2lex[tb->lex2node[l]] = l;
-  // M^-T of this element in element node order: MT[j][i] = M^-1[i][j]
+  // M^-T of this element in element node order: MT[j][i] = M^-1[i][j] (float32 copy in
+  // mixed-precision plans)
   const double* MT = B.minv + (size_t)e * N3 * N3;
+  const float* MT32 = (sizeof(R) == sizeof(float) && B.minv32) ? B.minv32 + (size_t)e * N3 * N3 : nullptr;
   for (int idx = threadIdx.x; idx < 6 * QF2 * 12; idx += blockDim.x) {
     const int lf = idx / (QF2 * 12), q = (idx / 12) % QF2, c = idx % 12;
     jc[(lf * 12 + c) * QF2 + codes.perm[fperm[lf] + q]] = (R)fd.jumpW[((size_t)fjump[lf] * QF2 + q) * 12 + c];
@@ -415,40 +424,43 @@ __global__ void __launch_bounds__(kThreads) k_hex_lift(const DevPlan P_, int b, 
       rs[idx] *= cf * tb->m1i[end * N + end];
     }
   } else {
-    // a thread owns one element node i and half of the 12 components; MT rows are read
-    // coalesced across consecutive nodes
-    for (int idx = threadIdx.x; idx < 2 * N3; idx += blockDim.x) {
-      const int i = idx % N3, c0 = (idx / N3) * 6;
-      R sacc[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
+    auto dense_lift = [&](const auto* M) {
+      // a thread owns one element node i and half of the 12 components; M rows are read
+      // coalesced across consecutive nodes
+      for (int idx = threadIdx.x; idx < 2 * N3; idx += blockDim.x) {
+        const int i = idx % N3, c0 = (idx / N3) * 6;
+        R sacc[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
 #pragma unroll 4
-      for (int j = 0; j < N3; ++j) {
-        const R m = (R)__ldg(MT + (size_t)j * N3 + i);
-        const int lj = node2lex[j];
+        for (int j = 0; j < N3; ++j) {
+          const R m = (R)__ldg(M + (size_t)j * N3 + i);
+          const int lj = node2lex[j];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) sacc[k] += m * ball[(c0 + k) * N3 + lj];
+          for (int k = 0; k < 6; ++k) sacc[k] += m * ball[(c0 + k) * N3 + lj];
+        }
+        const int li = node2lex[i];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) lg[(c0 + k) * N3 + li] = (double)sacc[k];
       }
-      const int li = node2lex[i];
+      // r_f = M^-1[slab_f, slab_f] b_f for the six faces
+      for (int idx = threadIdx.x; idx < 6 * 2 * N2; idx += blockDim.x) {
+        const int lf = idx / (2 * N2), s_i = idx % N2, c0 = ((idx / N2) % 2) * 6;
+        int a0, end, a1, a2;
+        hex_face_axes(lf, a0, end, a1, a2);
+        const int st0 = axis_stride<N>(a0), st1 = axis_stride<N>(a1), st2 = axis_stride<N>(a2);
+        const int ni = tb->lex2node[end * st0 + (s_i % N) * st1 + (s_i / N) * st2];
+        R acc[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
 #pragma unroll
-      for (int k = 0; k < 6; ++k) lg[(c0 + k) * N3 + li] = (double)sacc[k];
-    }
-    // r_f = M^-1[slab_f, slab_f] b_f for the six faces
-    for (int idx = threadIdx.x; idx < 6 * 2 * N2; idx += blockDim.x) {
-      const int lf = idx / (2 * N2), s_i = idx % N2, c0 = ((idx / N2) % 2) * 6;
-      int a0, end, a1, a2;
-      hex_face_axes(lf, a0, end, a1, a2);
-      const int st0 = axis_stride<N>(a0), st1 = axis_stride<N>(a1), st2 = axis_stride<N>(a2);
-      const int ni = tb->lex2node[end * st0 + (s_i % N) * st1 + (s_i / N) * st2];
-      R acc[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
+        for (int s_j = 0; s_j < N2; ++s_j) {
+          const int nj = tb->lex2node[end * st0 + (s_j % N) * st1 + (s_j / N) * st2];
+          const R m = (R)__ldg(M + (size_t)nj * N3 + ni);
 #pragma unroll
-      for (int s_j = 0; s_j < N2; ++s_j) {
-        const int nj = tb->lex2node[end * st0 + (s_j % N) * st1 + (s_j / N) * st2];
-        const R m = (R)__ldg(MT + (size_t)nj * N3 + ni);
+          for (int k = 0; k < 6; ++k) acc[k] += m * bs[(lf * 12 + c0 + k) * N2 + s_j];
+        }
 #pragma unroll
-        for (int k = 0; k < 6; ++k) acc[k] += m * bs[(lf * 12 + c0 + k) * N2 + s_j];
+        for (int k = 0; k < 6; ++k) rs[(lf * 12 + c0 + k) * N2 + s_i] = acc[k];
       }
-#pragma unroll
-      for (int k = 0; k < 6; ++k) rs[(lf * 12 + c0 + k) * N2 + s_i] = acc[k];
-    }
+    };
+    if (MT32) dense_lift(MT32); else dense_lift(MT);
   }
   __syncthreads();
   // br2 * B_f r_f at every face's points
@@ -516,6 +528,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_volume(const DevPlan P_, const
   R* t2 = t1 + L::C1 * N * N * Q;
   tensor3<NV, N, N, N, Q, Q, Q, false>(U, uq, t1, t2, tb->bq, tb->bq, tb->bq);
   const double* jinv = B.jinv + (size_t)e * Q3 * 9;
+  const float* jinv32 = (sizeof(R) == sizeof(float) && B.jinv32) ? B.jinv32 + (size_t)e * Q3 * 9 : nullptr;
   const double* wdet = B.wdet + (size_t)e * Q3;
   // affine element: one inverse Jacobian, w |J| = w1 w1 w1 det J (no per-point metrics read)
   const bool aff = B.affine && B.affine[e];
@@ -533,7 +546,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_volume(const DevPlan P_, const
     for (int q = threadIdx.x; q < Q3; q += blockDim.x) {
       R J[9], gr[12];
 #pragma unroll
-      for (int k = 0; k < 9; ++k) J[k] = aff ? Ja[k] : (R)jinv[q * 9 + k];
+      for (int k = 0; k < 9; ++k) J[k] = aff ? Ja[k] : (jinv32 ? (R)jinv32[q * 9 + k] : (R)jinv[q * 9 + k]);
 #pragma unroll
       for (int k = 0; k < 12; ++k) gr[k] = gq[k * Q3 + q];      // [r][m]
 #pragma unroll
@@ -558,7 +571,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_volume(const DevPlan P_, const
   for (int q = threadIdx.x; q < Q3; q += blockDim.x) {
     R J[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) J[k] = aff ? Ja[k] : (R)jinv[q * 9 + k];
+    for (int k = 0; k < 9; ++k) J[k] = aff ? Ja[k] : (jinv32 ? (R)jinv32[q * 9 + k] : (R)jinv[q * 9 + k]);
     const R wq = aff ? tb->w1[q / (Q * Q)] * tb->w1[(q / Q) % Q] * tb->w1[q % Q] * deta : (R)wdet[q];
     R Uq[NV], F[3][NV];
 #pragma unroll
@@ -716,33 +729,37 @@ __global__ void __launch_bounds__(kThreads) k_hex_finalize(const DevPlan P_, con
   constexpr int HALVES = NG * N3 * 2 <= kThreads ? 2 : 1;
   constexpr int JH = (N3 + HALVES - 1) / HALVES;      // N3 is odd at P2
   const double* MT = B.minv + (size_t)e * N3 * N3;   // M^-T in element node order
+  const float* MT32 = (sizeof(R) == sizeof(float) && B.minv32) ? B.minv32 + (size_t)e * N3 * N3 : nullptr;
   R* part = hs;                                       // [HALVES][2][NV][N3]
-  for (int idx = threadIdx.x; idx < HALVES * NG * N3; idx += blockDim.x) {
-    const int i = idx % N3, g = (idx / N3) % NG, h = idx / (NG * N3);
-    const int v0 = g * VB;
-    R ri[VB], rv[VB];
+  auto apply = [&](const auto* M) {
+    for (int idx = threadIdx.x; idx < HALVES * NG * N3; idx += blockDim.x) {
+      const int i = idx % N3, g = (idx / N3) % NG, h = idx / (NG * N3);
+      const int v0 = g * VB;
+      R ri[VB], rv[VB];
 #pragma unroll
-    for (int k = 0; k < VB; ++k) ri[k] = rv[k] = R(0);
-    const int j1 = (h + 1) * JH < N3 ? (h + 1) * JH : N3;
+      for (int k = 0; k < VB; ++k) ri[k] = rv[k] = R(0);
+      const int j1 = (h + 1) * JH < N3 ? (h + 1) * JH : N3;
 #pragma unroll 4
-    for (int j = h * JH; j < j1; ++j) {
-      const R m = (R)__ldg(MT + (size_t)j * N3 + i);
-      const int lj = node2lex[j];
+      for (int j = h * JH; j < j1; ++j) {
+        const R m = (R)__ldg(M + (size_t)j * N3 + i);
+        const int lj = node2lex[j];
 #pragma unroll
-      for (int k = 0; k < VB; ++k) {
-        if (v0 + k < NV) {
-          ri[k] += m * Rr[(v0 + k) * N3 + lj];
-          if (SPLIT) rv[k] += m * Rr[(NV + v0 + k) * N3 + lj];
+        for (int k = 0; k < VB; ++k) {
+          if (v0 + k < NV) {
+            ri[k] += m * Rr[(v0 + k) * N3 + lj];
+            if (SPLIT) rv[k] += m * Rr[(NV + v0 + k) * N3 + lj];
+          }
         }
       }
-    }
 #pragma unroll
-    for (int k = 0; k < VB; ++k) {
-      if (v0 + k >= NV) continue;
-      part[((h * 2 + 0) * NV + v0 + k) * N3 + i] = ri[k];
-      part[((h * 2 + 1) * NV + v0 + k) * N3 + i] = rv[k];
+      for (int k = 0; k < VB; ++k) {
+        if (v0 + k >= NV) continue;
+        part[((h * 2 + 0) * NV + v0 + k) * N3 + i] = ri[k];
+        part[((h * 2 + 1) * NV + v0 + k) * N3 + i] = rv[k];
+      }
     }
-  }
+  };
+  if (MT32) apply(MT32); else apply(MT);
   __syncthreads();
   for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
     const int v = idx / N3, i = idx % N3;

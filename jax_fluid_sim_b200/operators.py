@@ -176,6 +176,21 @@ class NativePlan:
         self.mood_coupling = coupling
         self.subcell_plan = sp
 
+    def set_tensor_cores(self, enable=True):
+        """Run the inviscid volume integrals of the eligible dense blocks (prisms, tetrahedra up to
+        P3) on the tensor cores (``dgb_plan_set_tensor_cores``); applies to mixed-precision plans
+        without viscous terms.  Returns the number of blocks that use them."""
+        n = ctypes.c_int(0)
+        N.check(N.lib().dgb_plan_set_tensor_cores(self.handle, int(bool(enable)), ctypes.byref(n)))
+        self.tensor_core_blocks = n.value
+        return n.value
+
+    def device_errors(self, reset=True):
+        """Error bits recorded on the device by kernels with bounded waits (0: none)."""
+        out = ctypes.c_int(0)
+        N.check(N.lib().dgb_plan_device_errors(self.handle, ctypes.byref(out), int(bool(reset))))
+        return out.value
+
     def _snapshot(self):
         return bytes(self.params)
 
