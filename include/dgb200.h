@@ -227,6 +227,13 @@ int dgb_wall_forces(dgb_plan* plan, const dgb_state* U, const int32_t* wall_tags
  * zeros on the sum-factorised hexahedron path, whose launches are fixed.  Synchronises the
  * stream. */
 int dgb_plan_autotune(dgb_plan* plan, const dgb_state* U, int reps, int* widths, void* stream);
+/* Execution form of the sum-factorised hexahedron right-hand side (no reference counterpart; the
+ * results agree to round-off): enable = 1 (the default) runs it as three launches, the traces,
+ * one face kernel (HLLC, BR2 jumps, both sides' local lifts and the viscous face flux) and one
+ * element kernel (nodal lift, volume terms, face terms, M^-1 and the stage update, with the lift
+ * and the residuals kept on chip); enable = 0 runs the six-launch form (traces, face flux, lift,
+ * volume, viscous face flux, finalize). */
+int dgb_plan_set_fused(dgb_plan* plan, int enable);
 /* Inviscid volume integrals of the dense blocks on the tensor cores (replaces the einsum
  * contractions of HybridEulerOperator._volume_terms, hybrid/spatial.py:47-72, for those blocks):
  * a tcgen05 kernel with three-term TF32 products (about float32 accuracy) and bulk-copied

@@ -119,6 +119,7 @@ def lib():
             "dgb_wall_forces": [c_void_p, ctypes.POINTER(State), P_int32, c_int, P_double, c_void_p, c_void_p],
             "dgb_plan_autotune": [c_void_p, ctypes.POINTER(State), c_int, P_int32, c_void_p],
             "dgb_plan_set_tensor_cores": [c_void_p, c_int, ctypes.POINTER(c_int)],
+            "dgb_plan_set_fused": [c_void_p, c_int],
             "dgb_plan_device_errors": [c_void_p, ctypes.POINTER(c_int), c_int],
             "dgb_plan_set_cases": [c_void_p, c_int, P_double, ctypes.POINTER(ctypes.c_void_p)],
             "dgb_plan_set_block_affine": [c_void_p, c_int, ctypes.POINTER(ctypes.c_uint8), P_double, P_double,

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "aux_kernels.cuh"
+#include "hex_fused.cuh"
 #include "hex_kernels.cuh"
 #include "mlp_kernels.cuh"
 #include "mood_kernels.cuh"
@@ -93,6 +94,9 @@ struct dgb_plan {
   int trb_grid = 0;   // the same for k_hex_troubled, which shares the list
   HexCodes hex_codes = {nullptr, nullptr};
   double* hex_lift = nullptr;     // [E][12][N3] nodal BR2 lift scratch
+  // fused right-hand side (hex_fused.cuh): on by default, dgb_plan_set_fused
+  bool fused = true;
+  HexFaceArgs hex_face = {nullptr, nullptr, nullptr};
   // MOOD subcell fallback
   MoodDev mood;
   bool sub_block_set[DGB_MAX_BLOCKS] = {false, false, false};
@@ -180,6 +184,53 @@ int prepare(K kernel, size_t smem) {
 }
 
 int blocks_for(long n, int per) { return (int)((n + per - 1) / per); }
+
+template <int P>
+void launch_hex_lop(dgb_plan* p, const int* elems, int count, double* lop) {
+  k_hex_lop<P, double><<<count * 6, 128>>>(p->dev, p->hex_tables, elems, count, lop);
+}
+
+// Tables of the fused face kernel (set-up): the local face of every face side, and the local-lift
+// operators of the elements whose map is not affine (all elements when the plan has no affine
+// data), indexed through lop_index.
+int build_hex_face_tables(dgb_plan* p) {
+  const BlockDev& B = p->dev.blk[0];
+  const FaceDev& F = p->dev.face[1];
+  const int E = B.E, QF2 = F.nq;
+  void* d = nullptr;
+  CK(cudaMalloc(&d, sizeof(int8_t) * (size_t)F.F * 2));
+  p->allocations.push_back(d);
+  CK(cudaMemset(d, 0, sizeof(int8_t) * (size_t)F.F * 2));
+  int8_t* face_lf = static_cast<int8_t*>(d);
+  k_hex_face_lf<<<blocks_for((long)E * 6, 256), 256>>>(p->dev, face_lf);
+  CK(cudaGetLastError());
+  std::vector<uint8_t> aff(E, 0);
+  if (B.affine) CK(cudaMemcpy(aff.data(), B.affine, E, cudaMemcpyDeviceToHost));
+  std::vector<int> index(E, -1), elems;
+  for (int e = 0; e < E; ++e)
+    if (!aff[e]) {
+      index[e] = (int)elems.size();
+      elems.push_back(e);
+    }
+  const int* dindex = nullptr;
+  int rc;
+  if ((rc = upload(p, index.data(), index.size(), &dindex))) return rc;
+  double* lop = nullptr;
+  if (!elems.empty()) {
+    const int* delems = nullptr;
+    if ((rc = upload(p, elems.data(), elems.size(), &delems))) return rc;
+    if ((rc = alloc(p, elems.size() * 6 * (size_t)QF2 * QF2, &lop))) return rc;
+    switch (p->dev.degree) {
+      case 1: launch_hex_lop<1>(p, delems, (int)elems.size(), lop); break;
+      case 2: launch_hex_lop<2>(p, delems, (int)elems.size(), lop); break;
+      default: launch_hex_lop<3>(p, delems, (int)elems.size(), lop); break;
+    }
+    CK(cudaGetLastError());
+  }
+  CK(cudaDeviceSynchronize());
+  p->hex_face = HexFaceArgs{face_lf, dindex, lop};
+  return DGB_OK;
+}
 
 // ------------------------------------------------------------------ dense element launches
 enum DenseKind { traces_kind, volume_kind, finalize_kind };
@@ -271,8 +322,48 @@ int run_rhs_hex(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStre
   return DGB_OK;
 }
 
+// The fused form: traces, one face kernel, one element kernel (hex_fused.cuh).  Stage events as
+// in run_rhs_hex, the lift, viscous-face and finalize stages being part of the face and element
+// kernels (zero-length).
+template <int P, int NV, bool SPLIT, typename R>
+int run_rhs_hex_fused(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStream_t st, cudaEvent_t* ev) {
+  using LR = HexSmem<P, NV, R>;
+  using LE = HexElemSmem<P, NV, SPLIT, R>;
+  const DevPlan& D = p->dev;
+  const int E = D.blk[0].E;
+  const size_t sm_tr = sizeof(R) * (size_t)LR::TRACES, sm_el = sizeof(R) * (size_t)LE::TOTAL;
+  int rc;
+  if (ev) CK(cudaEventRecord(ev[0], st));
+  if ((rc = prepare(k_hex_traces<P, NV, R>, sm_tr))) return rc;
+  k_hex_traces<P, NV, R><<<E, kThreads, sm_tr, st>>>(D, S, 0, p->hex_tables, p->hex_codes);
+  if (ev) CK(cudaEventRecord(ev[1], st));
+  constexpr int FPC = kThreads / HexDims<P>::QF2;
+  if (D.face[1].F > 0)
+    k_hex_face<P, NV><<<blocks_for(D.face[1].F, FPC), kThreads, 0, st>>>(D, p->hex_tables, p->hex_codes, p->hex_face);
+  if (ev) {
+    CK(cudaEventRecord(ev[2], st));
+    CK(cudaEventRecord(ev[3], st));
+  }
+  if ((rc = prepare(k_hex_element<P, NV, SPLIT, R>, sm_el))) return rc;
+  k_hex_element<P, NV, SPLIT, R><<<E, kThreads, sm_el, st>>>(D, S, p->hex_tables, p->hex_codes, A);
+  if (ev) {
+    CK(cudaEventRecord(ev[4], st));
+    CK(cudaEventRecord(ev[5], st));
+    CK(cudaEventRecord(ev[6], st));
+  }
+  CK(cudaGetLastError());
+  return DGB_OK;
+}
+
 template <int NV, bool SPLIT, typename R>
 int run_rhs_hex_deg(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStream_t st, cudaEvent_t* ev) {
+  if (p->fused) {
+    switch (p->dev.degree) {
+      case 1: return run_rhs_hex_fused<1, NV, SPLIT, R>(p, S, A, st, ev);
+      case 2: return run_rhs_hex_fused<2, NV, SPLIT, R>(p, S, A, st, ev);
+      default: return run_rhs_hex_fused<3, NV, SPLIT, R>(p, S, A, st, ev);
+    }
+  }
   switch (p->dev.degree) {
     case 1: return run_rhs_hex<1, NV, SPLIT, R>(p, S, A, st, ev);
     case 2: return run_rhs_hex<2, NV, SPLIT, R>(p, S, A, st, ev);
@@ -1270,6 +1361,9 @@ int dgb_plan_finalize(dgb_plan* p) {
   }
   if (p->hex && p->dev.viscous)
     if ((rc = alloc(p, (size_t)p->dev.blk[0].E * 12 * p->dev.blk[0].Np, &p->hex_lift))) return rc;
+  if (p->hex && p->dev.viscous && p->dev.blk[0].E > 0 && p->face_present[1]) {
+    if ((rc = build_hex_face_tables(p))) return rc;
+  }
   if (p->hex && p->prm.precision == 1) {
     // float32 copies of the inverse mass matrices and the per-point inverse Jacobians that the
     // mixed-precision hexahedron kernels read (half the bytes of the float64 tables)
@@ -1286,6 +1380,15 @@ int dgb_plan_finalize(dgb_plan* p) {
     }
   }
   p->finalized = true;
+  return DGB_OK;
+}
+
+int dgb_plan_set_fused(dgb_plan* p, int enable) {
+  if (!p) return fail(DGB_ERR_ARGUMENT, "null plan");
+  if (enable && p->finalized && p->hex && p->dev.viscous && !p->hex_face.face_lf && p->face_present[1])
+    return fail(DGB_ERR_ARGUMENT, "fused tables missing");
+  p->fused = enable != 0;
+  p->generation++;
   return DGB_OK;
 }
 

@@ -1,0 +1,570 @@
+// Fused right-hand side of the sum-factorised hexahedron path: three launches per evaluation
+// instead of six.
+//
+//   k_hex_traces   (hex_kernels.cuh, unchanged): face traces of U, of the viscous variables and of
+//                  their raw gradients, per face side.
+//   k_hex_face     one thread per face point, the points of a face in consecutive threads:
+//                  HLLC (or the boundary ghost) minus each side's anchor flux, the BR2 jump,
+//                  then each side's local lift at the face points, r_f = M^-1[slab_f] B_f^T jump
+//                  seen through B_f (hybrid/navier_stokes.py:138-188), and the averaged viscous
+//                  normal flux (hybrid/navier_stokes.py:210-324).  The local lift is a fixed linear
+//                  map of the face's jumps: for an affine element br2 coef m1i[end][end] (K (x) K)
+//                  with K = bf m1i bf^T, otherwise a QF^2 x QF^2 operator per element face built
+//                  once from M^-1 (k_hex_lop).  This replaces k_face_flux, the per-face part of
+//                  k_hex_lift and k_face_visc, and the traces are read once.
+//   k_hex_element  one CTA per element: the nodal lift M^-1 sum_f B_f^T jump_f, the volume terms
+//                  (U, grad v and lift at the volume points; inviscid and viscous fluxes), the face
+//                  terms and M^-1 with the stage update.  The lift and the residuals stay in shared
+//                  memory (no nodal-lift or residual buffers in HBM); M^-1 is read by the lift and
+//                  by the final product.
+// Arithmetic and summation order inside each phase are those of the unfused kernels; the local
+// lift is summed as one operator instead of three factors, which moves results by round-off.
+#pragma once
+#include "hex_kernels.cuh"
+
+namespace dgb {
+
+// Local face of each face side of the hexahedron block: face_lf[f * 2 + side] (set-up).
+__global__ void k_hex_face_lf(const DevPlan P_, int8_t* face_lf) {
+  const BlockDev& B = P_.blk[0];
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= B.E * 6) return;
+  int ft, f, side;
+  decode_face(B.elem_face[t], ft, f, side);
+  face_lf[(size_t)f * 2 + side] = (int8_t)(t % 6);
+}
+
+// Local-lift operator of every face of the non-affine elements (set-up), in the canonical face-point
+// order of that face: L[c][c'] = sum_{i,j in slab} BF[c][i] M^-1[node i][node j] BF[c'][j], BF the
+// face interpolation bf (x) bf.  One CTA per (listed element, local face).  Mt is M^-1 transposed
+// in element node order (the hexahedron path's layout).
+template <int P, typename T>
+__global__ void k_hex_lop(const DevPlan P_, const HexTables tables, const int* __restrict__ elems, int count,
+                          T* __restrict__ lop) {
+  using D = HexDims<P>;
+  constexpr int N = D::N, QF = D::QF, N2 = D::N2, N3 = D::N3, QF2 = D::QF2;
+  __shared__ double ms[N2][N2];
+  __shared__ double t1[N2][QF2];     // Mslab BF^T
+  const int item = blockIdx.x;
+  if (item >= count * 6) return;
+  const int e = elems[item / 6], lf = item % 6;
+  int a0, end, a1, a2;
+  hex_face_axes(lf, a0, end, a1, a2);
+  const int st0 = axis_stride<N>(a0), st1 = axis_stride<N>(a1), st2 = axis_stride<N>(a2);
+  const double* Mt = P_.blk[0].minv + (size_t)e * N3 * N3;
+  for (int idx = threadIdx.x; idx < N2 * N2; idx += blockDim.x) {
+    const int si = idx / N2, sj = idx % N2;
+    const int ni = tables.lex2node[end * st0 + (si % N) * st1 + (si / N) * st2];
+    const int nj = tables.lex2node[end * st0 + (sj % N) * st1 + (sj / N) * st2];
+    ms[si][sj] = Mt[(size_t)nj * N3 + ni];
+  }
+  __syncthreads();
+  // BF[c][s] = bf[c % QF][s % N] bf[c / QF][s / N] (canonical face point c, slab node s)
+  for (int idx = threadIdx.x; idx < N2 * QF2; idx += blockDim.x) {
+    const int si = idx / QF2, c = idx % QF2;
+    double acc = 0.0;
+    for (int sj = 0; sj < N2; ++sj)
+      acc += ms[si][sj] * tables.bf[(c % QF) * N + sj % N] * tables.bf[(c / QF) * N + sj / N];
+    t1[si][c] = acc;
+  }
+  __syncthreads();
+  T* out = lop + ((size_t)(item / 6) * 6 + lf) * QF2 * QF2;
+  for (int idx = threadIdx.x; idx < QF2 * QF2; idx += blockDim.x) {
+    const int c = idx / QF2, cp = idx % QF2;
+    double acc = 0.0;
+    for (int si = 0; si < N2; ++si)
+      acc += tables.bf[(c % QF) * N + si % N] * tables.bf[(c / QF) * N + si / N] * t1[si][cp];
+    out[idx] = (T)acc;
+  }
+}
+
+// Inputs of the fused face kernel beyond the plan: the local face of each face side, the lift
+// operators of the non-affine elements (lop_index[e] >= 0 selects one) and its precision.
+struct HexFaceArgs {
+  const int8_t* face_lf;      // [F][2]
+  const int* lop_index;       // [E], -1 for affine elements
+  const double* lop;          // [count][6][QF2][QF2]
+};
+
+template <int P, int NV>
+__global__ void __launch_bounds__(kThreads) k_hex_face(const DevPlan P_, const HexTables tables, const HexCodes codes,
+                                                      const HexFaceArgs A) {
+  using D = HexDims<P>;
+  constexpr int N = D::N, QF = D::QF, QF2 = D::QF2;
+  constexpr int FPC = kThreads / QF2;                // faces per CTA
+  __shared__ double jmp[FPC * QF2][12];
+  __shared__ double K[QF][QF];                       // bf m1i bf^T
+  const FaceDev& fd = P_.face[1];
+  const int slot = threadIdx.x / QF2, q = threadIdx.x % QF2;
+  const int f = blockIdx.x * FPC + slot;
+  const bool live = slot < FPC && f < fd.F;
+  if (threadIdx.x < QF * QF) {
+    const int a = threadIdx.x / QF, c = threadIdx.x % QF;
+    double acc = 0.0;
+    for (int j = 0; j < N; ++j)
+      for (int k = 0; k < N; ++k) acc += tables.bf[a * N + j] * tables.m1i[j * N + k] * tables.bf[c * N + k];
+    K[a][c] = acc;
+  }
+  int nb = -1;
+  double n[3] = {0.0, 0.0, 0.0}, w = 0.0;
+  size_t so = 0, sn = 0;
+  double UL[NV];
+  if (live) {
+    nb = fd.nb[f];
+    const double* np_ = fd.n + ((size_t)f * QF2 + q) * 3;
+    n[0] = np_[0], n[1] = np_[1], n[2] = np_[2];
+    w = fd.w[(size_t)f * QF2 + q];
+    so = ((size_t)f * 2 + 0) * QF2 + q;
+    sn = ((size_t)f * 2 + 1) * QF2 + q;
+    double UR[NV], Fh[NV], Fa[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) UL[v] = fd.trA[so * NV + v];
+    if (nb >= 0) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) UR[v] = fd.trA[sn * NV + v];
+    } else if (P_.ph.has_boundary) {
+      ghost_state<NV>(P_.ph, case_view(P_.ph, P_.blk[0].ecase, fd.ol[f]).far, UL, n, fd.tag[f], UR);
+    } else {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) UR[v] = UL[v];
+    }
+    hllc<NV>(P_.ph, UL, UR, n, Fh);
+    {
+      double a[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) a[v] = fd.anc[((size_t)f * 2 + 0) * NV + v];
+      normal_flux<NV>(P_.ph, a, n, Fa);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) fd.fluxI[so * NV + v] = (Fh[v] - Fa[v]) * w;
+    }
+    if (nb >= 0) {
+      double a[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) a[v] = fd.anc[((size_t)f * 2 + 1) * NV + v];
+      normal_flux<NV>(P_.ph, a, n, Fa);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) fd.fluxI[sn * NV + v] = (Fh[v] - Fa[v]) * w;
+    }
+  }
+  if (!P_.viscous) return;
+  double vo[4], vn[4];
+  if (live) {
+#pragma unroll
+    for (int m = 0; m < 4; ++m) vo[m] = fd.trV[so * 4 + m];
+    if (nb >= 0) {
+#pragma unroll
+      for (int m = 0; m < 4; ++m) vn[m] = fd.trV[sn * 4 + m];
+    } else if (P_.ph.has_boundary) {
+      const CaseView cv = case_view(P_.ph, P_.blk[0].ecase, fd.ol[f]);
+      viscous_ghost<NV>(P_.ph, cv.far, cv.wall_T, UL, n, fd.tag[f], vn);
+    } else {
+      viscous_vars<NV>(P_.ph, UL, vn);
+    }
+    double* out = fd.jumpW + ((size_t)f * QF2 + q) * 12;
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const double j = 0.5 * w * (vn[m] - vo[m]) * n[d];
+        out[m * 3 + d] = j;
+        jmp[threadIdx.x][m * 3 + d] = j;
+      }
+  }
+  __syncthreads();
+  if (!live) return;
+  const BlockDev& B = P_.blk[0];
+  const CaseView cv = case_view(P_.ph, B.ecase, fd.ol[f]);
+  const double* jf = &jmp[slot * QF2][0];
+  double Fo[3 * NV];
+  const int nsides = nb >= 0 ? 2 : 1;
+  for (int s = 0; s < nsides; ++s) {
+    const int e = s == 0 ? fd.ol[f] : fd.nl[f];
+    const int code = s == 0 ? fd.oc[f] : fd.nc[f];
+    const uint8_t* perm = codes.perm + (size_t)code * QF2;
+    const int lf = A.face_lf[(size_t)f * 2 + s];
+    const int cq = perm[q];
+    double lift[12];
+#pragma unroll
+    for (int c = 0; c < 12; ++c) lift[c] = 0.0;
+    const int li = A.lop_index ? A.lop_index[e] : -1;
+    if (li < 0) {
+      // affine: br2 coef m1i[end][end] (K (x) K) in this side's canonical order
+      int a0, end, a1, a2;
+      hex_face_axes(lf, a0, end, a1, a2);
+      const double scale = P_.ph.br2 * B.acoef[e] * tables.m1i[end * N + end];
+      const int c1 = cq % QF, c2 = cq / QF;
+      for (int qp = 0; qp < QF2; ++qp) {
+        const int cp = perm[qp];
+        const double kk = K[c1][cp % QF] * K[c2][cp / QF];
+#pragma unroll
+        for (int c = 0; c < 12; ++c) lift[c] += kk * jf[qp * 12 + c];
+      }
+#pragma unroll
+      for (int c = 0; c < 12; ++c) lift[c] *= scale;
+    } else {
+      const double* L = A.lop + ((size_t)li * 6 + lf) * QF2 * QF2 + (size_t)cq * QF2;
+      for (int qp = 0; qp < QF2; ++qp) {
+        const double kk = __ldg(L + perm[qp]);
+#pragma unroll
+        for (int c = 0; c < 12; ++c) lift[c] += kk * jf[qp * 12 + c];
+      }
+#pragma unroll
+      for (int c = 0; c < 12; ++c) lift[c] *= P_.ph.br2;
+    }
+    const size_t ss = s == 0 ? so : sn;
+    double U[NV], g[12];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) U[v] = fd.trP[ss * NV + v];
+#pragma unroll
+    for (int c = 0; c < 12; ++c) g[c] = fd.trG[ss * 12 + c] + lift[c];
+    if (s == 0) {
+      viscous_flux<NV>(P_.ph, cv.mu, cv.kappa, U, g, Fo);
+    } else {
+      double Fn[3 * NV];
+      viscous_flux<NV>(P_.ph, cv.mu, cv.kappa, U, g, Fn);
+#pragma unroll
+      for (int k = 0; k < 3 * NV; ++k) Fo[k] = 0.5 * (Fo[k] + Fn[k]);
+    }
+  }
+  double out[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) out[v] = Fo[0 * NV + v] * n[0] + Fo[1 * NV + v] * n[1] + Fo[2 * NV + v] * n[2];
+  if (nb < 0 && P_.ph.has_boundary && tag_in(fd.tag[f], P_.ph.wall, P_.ph.n_wall)) out[4] = 0.0;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) fd.fluxV[((size_t)f * QF2 + q) * NV + v] = out[v] * w;
+}
+
+// Shared-memory layout of k_hex_element, in units of R.
+template <int P, int NV, bool SPLIT, typename R>
+struct HexElemSmem {
+  using D = HexDims<P>;
+  static constexpr int N = D::N, Q = D::Q, QF = D::QF, N2 = D::N2, N3 = D::N3, Q3 = D::Q3, QF2 = D::QF2;
+  static constexpr int T = (int)((sizeof(HexTablesT<R>) + sizeof(R) - 1) / sizeof(R));
+  static constexpr int C = SPLIT ? 2 * NV : NV;          // residual channels
+  static constexpr int U = T, V = U + NV * N3, LF = V + 4 * N3, RR = LF + 12 * N3, W = RR + C * N3;
+  // phase scratch (aliased)
+  static constexpr int LIFT = 72 * QF2 + 72 * QF * N + 72 * N2 + 12 * N3 + 3 * 12 * N3;
+  static constexpr int C1 = NV > 12 ? NV : 12;
+  static constexpr int VOL1 = NV * Q3 + 12 * Q3 + C1 * N * N * Q + C1 * N * Q * Q;
+  static constexpr int VOL2 = NV * Q3 + 12 * Q3 + (SPLIT ? 6 : 3) * NV * Q3 + NV * Q * Q * N + NV * Q * N * N;
+  static constexpr int FIN = 6 * C * (QF2 + QF * N) + cmax(6 * C * N2, 4 * NV * N3);
+  static constexpr int TOTAL = W + cmax(cmax(LIFT, VOL1), cmax(VOL2, FIN));
+};
+
+// Lift + volume + finalize of one hexahedron (see the file comment).  SPLIT keeps the inviscid
+// and viscous residuals apart (right-hand-side outputs, the MOOD step's viscous residual).
+template <int P, int NV, bool SPLIT, typename R = double>
+__global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) k_hex_element(const DevPlan P_, const StatePtrs S, const HexTables tables,
+                                                         const HexCodes codes, const FinalizeArgs A) {
+  using D = HexDims<P>;
+  using L = HexElemSmem<P, NV, SPLIT, R>;
+  constexpr int N = D::N, Q = D::Q, QF = D::QF, N2 = D::N2, N3 = D::N3, Q3 = D::Q3, QF2 = D::QF2;
+  constexpr int C = L::C;
+  constexpr int b = 0;
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  R* smem = reinterpret_cast<R*>(dyn_smem);
+  HexTablesT<R>* tb = reinterpret_cast<HexTablesT<R>*>(smem);
+  R* U = smem + L::U;            // [NV][N3] minus anchor
+  R* V = smem + L::V;            // [4][N3]
+  R* Lf = smem + L::LF;          // [12][N3] nodal lift
+  R* Rr = smem + L::RR;          // [C][N3] residuals (inviscid, then viscous)
+  R* W = smem + L::W;
+  __shared__ int node2lex[64], fslot[6], fperm[6], fface[6];
+  __shared__ double anchor_d[NV];
+  __shared__ R anchor[NV];
+  const BlockDev& B = P_.blk[b];
+  const FaceDev& fd = P_.face[1];
+  const int e = blockIdx.x;
+  const CaseView cv = case_view(P_.ph, B.ecase, e);
+  load_tables<P>(tables, tb);
+  const double* Ug = S.b[b] + (size_t)e * N3 * NV;
+  if (threadIdx.x < NV) {
+    anchor_d[threadIdx.x] = Ug[threadIdx.x];
+    anchor[threadIdx.x] = (R)Ug[threadIdx.x];
+  }
+  if (threadIdx.x < 6) {
+    int ft, f, side;
+    decode_face(B.elem_face[e * 6 + threadIdx.x], ft, f, side);
+    fslot[threadIdx.x] = (f * 2 + side) * QF2;
+    fperm[threadIdx.x] = (side == 0 ? fd.oc[f] : fd.nc[f]) * QF2;
+    fface[threadIdx.x] = (f << 1) | side;
+  }
+  __syncthreads();
+  for (int l = threadIdx.x; l < N3; l += blockDim.x) node2lex[tb->lex2node[l]] = l;
+  for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
+    const int v = idx / N3, l = idx % N3;
+    U[idx] = (R)(Ug[tb->lex2node[l] * NV + v] - anchor_d[v]);
+  }
+  const bool visc = P_.viscous;
+  const bool aff = B.affine && B.affine[e];
+  const double* MT = B.minv + (size_t)e * N3 * N3;
+  const float* MT32 = (sizeof(R) == sizeof(float) && B.minv32) ? B.minv32 + (size_t)e * N3 * N3 : nullptr;
+  if (visc) {
+    for (int l = threadIdx.x; l < N3; l += blockDim.x) {
+      const int node = tb->lex2node[l];
+      double u[NV], vv[4];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) u[v] = Ug[node * NV + v];
+      viscous_vars<NV>(P_.ph, u, vv);
+#pragma unroll
+      for (int m = 0; m < 4; ++m) V[m * N3 + l] = (R)vv[m];
+    }
+    // ---- phase B: nodal lift M^-1 sum_f B_f^T jump_f
+    constexpr int CH = 72;
+    R* jc = W;                        // [6][12][QF2] jumps at the canonical face points
+    R* tmp = jc + CH * QF2;           // [72][QF][N]
+    R* bs = tmp + CH * QF * N;        // [6][12][N2]
+    R* ball = bs + CH * N2;           // [12][N3]
+    R* ax = ball + 12 * N3;           // affine scratch [3][12][N3]
+    for (int idx = threadIdx.x; idx < 6 * QF2 * 12; idx += blockDim.x) {
+      const int lf = idx / (QF2 * 12), q = (idx / 12) % QF2, c = idx % 12;
+      jc[(lf * 12 + c) * QF2 + codes.perm[fperm[lf] + q]] =
+          (R)fd.jumpW[((size_t)(fface[lf] >> 1) * QF2 + q) * 12 + c];
+    }
+    __syncthreads();
+    tensor2<CH, QF, QF, N, N>(jc, bs, tmp, tb->bfT, tb->bfT);
+    for (int idx = threadIdx.x; idx < 12 * N3; idx += blockDim.x) {
+      const int c = idx / N3, l = idx % N3;
+      const int xyz[3] = {l % N, (l / N) % N, l / N2};
+      R acc = R(0);
+#pragma unroll
+      for (int lf = 0; lf < 6; ++lf) {
+        int a0, end, a1, a2;
+        hex_face_axes(lf, a0, end, a1, a2);
+        if (xyz[a0] == end) acc += bs[(lf * 12 + c) * N2 + xyz[a2] * N + xyz[a1]];
+      }
+      ball[idx] = acc;
+    }
+    __syncthreads();
+    if (aff) {
+      tensor3<12, N, N, N, N, N, N, false>(ball, Lf, ax, ax + 12 * N3, tb->m1i, tb->m1i, tb->m1i);
+      const R cf = (R)B.acoef[e];
+      for (int idx = threadIdx.x; idx < 12 * N3; idx += blockDim.x) Lf[idx] *= cf;
+    } else {
+      auto dense_lift = [&](const auto* M) {
+        for (int idx = threadIdx.x; idx < 2 * N3; idx += blockDim.x) {
+          const int i = idx % N3, c0 = (idx / N3) * 6;
+          R sacc[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
+#pragma unroll 4
+          for (int j = 0; j < N3; ++j) {
+            const R m = (R)__ldg(M + (size_t)j * N3 + i);
+            const int lj = node2lex[j];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) sacc[k] += m * ball[(c0 + k) * N3 + lj];
+          }
+          const int li = node2lex[i];
+#pragma unroll
+          for (int k = 0; k < 6; ++k) Lf[(c0 + k) * N3 + li] = sacc[k];
+        }
+      };
+      if (MT32) dense_lift(MT32); else dense_lift(MT);
+    }
+  }
+  __syncthreads();
+  // ---- phase C: volume terms (k_hex_volume with the lift from shared memory)
+  {
+    R* uq = W;                           // [NV][Q3]   U - anchor at volume points
+    R* gq = uq + NV * Q3;                // [12][Q3]   gradients of v: reference (3 x 4), then physical + lift
+    R* t1 = gq + 12 * Q3;                // contraction scratch
+    R* t2 = t1 + L::C1 * N * N * Q;
+    tensor3<NV, N, N, N, Q, Q, Q, false>(U, uq, t1, t2, tb->bq, tb->bq, tb->bq);
+    const double* jinv = B.jinv + (size_t)e * Q3 * 9;
+    const float* jinv32 = (sizeof(R) == sizeof(float) && B.jinv32) ? B.jinv32 + (size_t)e * Q3 * 9 : nullptr;
+    const double* wdet = B.wdet + (size_t)e * Q3;
+    R Ja[9], deta = R(0);
+    if (aff) {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) Ja[k] = (R)B.ajinv[(size_t)e * 9 + k];
+      deta = (R)B.adet[e];
+    }
+    if (visc) {
+      tensor3<4, N, N, N, Q, Q, Q, false>(V, gq + 0 * 4 * Q3, t1, t2, tb->dq, tb->bq, tb->bq);
+      tensor3<4, N, N, N, Q, Q, Q, false>(V, gq + 1 * 4 * Q3, t1, t2, tb->bq, tb->dq, tb->bq);
+      tensor3<4, N, N, N, Q, Q, Q, false>(V, gq + 2 * 4 * Q3, t1, t2, tb->bq, tb->bq, tb->dq);
+      for (int q = threadIdx.x; q < Q3; q += blockDim.x) {
+        R J[9], gr[12];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) J[k] = aff ? Ja[k] : (jinv32 ? (R)jinv32[q * 9 + k] : (R)jinv[q * 9 + k]);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) gr[k] = gq[k * Q3 + q];
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
+#pragma unroll
+          for (int d = 0; d < 3; ++d)
+            gq[(m * 3 + d) * Q3 + q] = gr[0 * 4 + m] * J[0 * 3 + d] + gr[1 * 4 + m] * J[1 * 3 + d] +
+                                       gr[2 * 4 + m] * J[2 * 3 + d];
+      }
+      __syncthreads();
+      tensor3<12, N, N, N, Q, Q, Q, true>(Lf, gq, t1, t2, tb->bq, tb->bq, tb->bq);
+    }
+    R* Gi = t1;                          // [3][NV][Q3]
+    R* Gv = Gi + 3 * NV * Q3;            // [3][NV][Q3] (SPLIT only)
+    R Fa[3][NV];
+    {
+      const R ex[3] = {R(1), R(0), R(0)}, ey[3] = {R(0), R(1), R(0)}, ez[3] = {R(0), R(0), R(1)};
+      normal_flux<NV>(P_.ph, anchor, ex, Fa[0]);
+      normal_flux<NV>(P_.ph, anchor, ey, Fa[1]);
+      normal_flux<NV>(P_.ph, anchor, ez, Fa[2]);
+    }
+    for (int q = threadIdx.x; q < Q3; q += blockDim.x) {
+      R J[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) J[k] = aff ? Ja[k] : (jinv32 ? (R)jinv32[q * 9 + k] : (R)jinv[q * 9 + k]);
+      const R wq = aff ? tb->w1[q / (Q * Q)] * tb->w1[(q / Q) % Q] * tb->w1[q % Q] * deta : (R)wdet[q];
+      R Uq[NV], F[3][NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) Uq[v] = anchor[v] + uq[v * Q3 + q];
+      {
+        const R ex[3] = {R(1), R(0), R(0)}, ey[3] = {R(0), R(1), R(0)}, ez[3] = {R(0), R(0), R(1)};
+        normal_flux<NV>(P_.ph, Uq, ex, F[0]);
+        normal_flux<NV>(P_.ph, Uq, ey, F[1]);
+        normal_flux<NV>(P_.ph, Uq, ez, F[2]);
+      }
+      R Fv[3 * NV];
+#pragma unroll
+      for (int k = 0; k < 3 * NV; ++k) Fv[k] = R(0);
+      if (visc) {
+        R grad[12];
+#pragma unroll
+        for (int k = 0; k < 12; ++k) grad[k] = gq[k * Q3 + q];
+        viscous_flux<NV>(P_.ph, cv.mu, cv.kappa, Uq, grad, Fv);
+      }
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          const R gi = (J[r * 3 + 0] * (F[0][v] - Fa[0][v]) + J[r * 3 + 1] * (F[1][v] - Fa[1][v]) +
+                        J[r * 3 + 2] * (F[2][v] - Fa[2][v])) * wq;
+          const R gv = -(J[r * 3 + 0] * Fv[0 * NV + v] + J[r * 3 + 1] * Fv[1 * NV + v] +
+                         J[r * 3 + 2] * Fv[2 * NV + v]) * wq;
+          if (SPLIT) {
+            Gi[(r * NV + v) * Q3 + q] = gi;
+            Gv[(r * NV + v) * Q3 + q] = gv;
+          } else {
+            Gi[(r * NV + v) * Q3 + q] = gi + gv;
+          }
+        }
+    }
+    __syncthreads();
+    R* s1 = Gi + (SPLIT ? 6 : 3) * NV * Q3;
+    R* s2 = s1 + NV * Q * Q * N;
+    R* Ri = Rr;
+    R* Rv = Rr + NV * N3;
+    tensor3<NV, Q, Q, Q, N, N, N, false>(Gi + 0 * NV * Q3, Ri, s1, s2, tb->dqT, tb->bqT, tb->bqT);
+    tensor3<NV, Q, Q, Q, N, N, N, true>(Gi + 1 * NV * Q3, Ri, s1, s2, tb->bqT, tb->dqT, tb->bqT);
+    tensor3<NV, Q, Q, Q, N, N, N, true>(Gi + 2 * NV * Q3, Ri, s1, s2, tb->bqT, tb->bqT, tb->dqT);
+    if (SPLIT) {
+      if (visc) {
+        tensor3<NV, Q, Q, Q, N, N, N, false>(Gv + 0 * NV * Q3, Rv, s1, s2, tb->dqT, tb->bqT, tb->bqT);
+        tensor3<NV, Q, Q, Q, N, N, N, true>(Gv + 1 * NV * Q3, Rv, s1, s2, tb->bqT, tb->dqT, tb->bqT);
+        tensor3<NV, Q, Q, Q, N, N, N, true>(Gv + 2 * NV * Q3, Rv, s1, s2, tb->bqT, tb->bqT, tb->dqT);
+      } else {
+        for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) Rv[idx] = R(0);
+        __syncthreads();
+      }
+    }
+  }
+  // ---- phase D: face terms, M^-1, stage update (k_hex_finalize with the residuals in shared memory)
+  R* hc = W;                                    // [6][C][QF2] face flux at canonical points
+  R* tmp = hc + 6 * C * QF2;                    // [6][C][QF][N]
+  R* hs = tmp + 6 * C * QF * N;                 // [6][C][N2]; reused for the M^-1 partial sums
+  const size_t base = (size_t)e * N3 * NV;
+  for (int idx = threadIdx.x; idx < 6 * QF2 * NV; idx += blockDim.x) {
+    const int lf = idx / (QF2 * NV), q = (idx / NV) % QF2, v = idx % NV;
+    const int f = fface[lf] >> 1, side = fface[lf] & 1;
+    const double si = side == 0 ? -1.0 : 1.0;
+    const double hi = si * fd.fluxI[((size_t)fslot[lf] + q) * NV + v];
+    const double hv = visc ? -si * fd.fluxV[((size_t)f * QF2 + q) * NV + v] : 0.0;
+    const int c = codes.perm[fperm[lf] + q];
+    if (SPLIT) {
+      hc[(lf * C + v) * QF2 + c] = (R)hi;
+      hc[(lf * C + NV + v) * QF2 + c] = (R)hv;
+    } else {
+      hc[(lf * C + v) * QF2 + c] = (R)(hi + hv);
+    }
+  }
+  __syncthreads();
+  tensor2<6 * C, QF, QF, N, N>(hc, hs, tmp, tb->bfT, tb->bfT);
+  for (int idx = threadIdx.x; idx < C * N3; idx += blockDim.x) {
+    const int c = idx / N3, l = idx % N3;
+    const int xyz[3] = {l % N, (l / N) % N, l / N2};
+    R acc = Rr[idx];
+#pragma unroll
+    for (int lf = 0; lf < 6; ++lf) {
+      int a0, end, a1, a2;
+      hex_face_axes(lf, a0, end, a1, a2);
+      if (xyz[a0] == end) acc += hs[(lf * C + c) * N2 + xyz[a2] * N + xyz[a1]];
+    }
+    Rr[idx] = acc;
+  }
+  __syncthreads();
+  auto emit = [&](size_t o, double ri, double rv) {
+    if (!A.stage) {
+      if (A.out_inv[b]) A.out_inv[b][o] = ri;
+      if (SPLIT && A.out_vis[b]) A.out_vis[b][o] = rv;
+    } else {
+      const double total = SPLIT ? ri + rv : ri;
+      const double eul = S.b[b][o] + A.dt * total;
+      if (SPLIT && A.out_vis[b]) A.out_vis[b][o] = rv;
+      if (A.euler[b]) A.euler[b][o] = eul;
+      A.dst[b][o] = A.alpha * A.base[b][o] + A.beta * eul;
+    }
+  };
+  if (aff) {
+    tensor3<C, N, N, N, N, N, N, false>(Rr, hs, tmp, hc, tb->m1i, tb->m1i, tb->m1i);
+    const R cf = (R)B.acoef[e];
+    for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
+      const int v = idx / N3, l = idx % N3;
+      const double ri = (double)(cf * hs[v * N3 + l]);
+      const double rv = SPLIT ? (double)(cf * hs[(NV + v) * N3 + l]) : 0.0;
+      emit(base + (size_t)tb->lex2node[l] * NV + v, ri, rv);
+    }
+    return;
+  }
+  constexpr int VB = NV < 8 ? NV : 8;
+  constexpr int NG = (NV + VB - 1) / VB;
+  constexpr int HALVES = NG * N3 * 2 <= kThreads ? 2 : 1;
+  constexpr int JH = (N3 + HALVES - 1) / HALVES;
+  R* part = hs;                                       // [HALVES][2][NV][N3]
+  auto apply = [&](const auto* M) {
+    for (int idx = threadIdx.x; idx < HALVES * NG * N3; idx += blockDim.x) {
+      const int i = idx % N3, g = (idx / N3) % NG, h = idx / (NG * N3);
+      const int v0 = g * VB;
+      R ri[VB], rv[VB];
+#pragma unroll
+      for (int k = 0; k < VB; ++k) ri[k] = rv[k] = R(0);
+      const int j1 = (h + 1) * JH < N3 ? (h + 1) * JH : N3;
+#pragma unroll 4
+      for (int j = h * JH; j < j1; ++j) {
+        const R m = (R)__ldg(M + (size_t)j * N3 + i);
+        const int lj = node2lex[j];
+#pragma unroll
+        for (int k = 0; k < VB; ++k) {
+          if (v0 + k < NV) {
+            ri[k] += m * Rr[(v0 + k) * N3 + lj];
+            if (SPLIT) rv[k] += m * Rr[(NV + v0 + k) * N3 + lj];
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < VB; ++k) {
+        if (v0 + k >= NV) continue;
+        part[((h * 2 + 0) * NV + v0 + k) * N3 + i] = ri[k];
+        part[((h * 2 + 1) * NV + v0 + k) * N3 + i] = rv[k];
+      }
+    }
+  };
+  if (MT32) apply(MT32); else apply(MT);
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
+    const int v = idx / N3, i = idx % N3;
+    R si = part[(0 * NV + v) * N3 + i], sv = part[(1 * NV + v) * N3 + i];
+    if (HALVES == 2) {
+      si += part[(2 * NV + v) * N3 + i];
+      sv += part[(3 * NV + v) * N3 + i];
+    }
+    emit(base + (size_t)i * NV + v, (double)si, (double)sv);
+  }
+}
+
+}  // namespace dgb

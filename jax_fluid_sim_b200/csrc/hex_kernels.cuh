@@ -478,7 +478,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_lift(const DevPlan P_, int b, 
 // contracted with w J^-T and the reference gradients (transposed sum factorisation).
 // SPLIT writes inviscid and viscous residuals separately, otherwise their sum into Rinv.
 template <int P, int NV, bool SPLIT, typename R = double>
-__global__ void __launch_bounds__(kThreads) k_hex_volume(const DevPlan P_, const StatePtrs S, int b,
+__global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) k_hex_volume(const DevPlan P_, const StatePtrs S, int b,
                                                         const HexTables tables, const double* lift_in) {
   using D = HexDims<P>;
   using L = HexSmem<P, NV, R>;

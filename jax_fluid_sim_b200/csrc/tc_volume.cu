@@ -465,7 +465,11 @@ int tc_volume(const DevPlan& P, const StatePtrs& S, int b, const TcShape& s, con
   if (E == 0) return 0;
   const int ntiles = (E + kTcTe - 1) / kTcTe;
   const int grid = ntiles < sm_count ? ntiles : sm_count;
-  k_tc_volume<<<grid, kTcThreads, s.smem, st>>>(P, S, b, s, image, err);
+  // at least 60 KB of shared memory per CTA keeps at most three CTAs on an SM, so their tensor
+  // memory (at most 128 columns each) always fits in the SM's 512 columns: no CTA waits in
+  // tcgen05.alloc
+  const size_t smem = s.smem > 60 * 1024 ? s.smem : 60 * 1024;
+  k_tc_volume<<<grid, kTcThreads, smem, st>>>(P, S, b, s, image, err);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

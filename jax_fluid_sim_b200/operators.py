@@ -185,6 +185,12 @@ class NativePlan:
         self.tensor_core_blocks = n.value
         return n.value
 
+    def set_fused(self, enable=True):
+        """Choose the three-launch (fused, the default) or the six-launch form of the
+        sum-factorised hexahedron right-hand side (``dgb_plan_set_fused``)."""
+        N.check(N.lib().dgb_plan_set_fused(self.handle, int(bool(enable))))
+        self.fused = bool(enable)
+
     def device_errors(self, reset=True):
         """Error bits recorded on the device by kernels with bounded waits (0: none)."""
         out = ctypes.c_int(0)
