@@ -177,6 +177,30 @@ def stage_bytes(op, nv, split, sizeof=8):
     return out
 
 
+def stage_bytes_fused(op, nv, split, sizeof=8):
+    """Algorithmic HBM bytes per launch of the fused sum-factorised hex right-hand side (traces,
+    face kernel, element kernel; every input read once, every output written once).  The face
+    kernel is reported as the "face_flux" stage and the element kernel (nodal lift, volume terms,
+    face terms, M^-1 and the outputs) as the "volume" stage.  Mixed-precision plans read float32
+    copies of M^-1 and of the per-point inverse Jacobians."""
+    out = dict.fromkeys(STAGES, 0)
+    visc = op.viscous
+    msz = 4 if op.precision == "mixed" else sizeof
+    bp = op.plan.blocks[0]
+    E, Np, Nq, nlf = bp.E, bp.Np, bp.Nq, bp.nlf
+    Ea = getattr(op.native, "affine_count", 0)
+    Ed = E - Ea
+    fp = op.plan.faces["quad"]
+    nqf = fp.nq
+    out["traces"] = sizeof * E * (nv * Np + nlf * nqf * (nv + (16 if visc else 0))) + (msz * E * nlf * nqf * 9 if visc else 0)
+    per_point = 2 * nv + 4 + 2 * nv + ((2 * 4 + 2 * 12 + 12 + nv) if visc else 0)
+    out["face_flux"] = fp.F * (sizeof * nqf * per_point + 8) + (sizeof * Ed * nlf * nqf * nqf if visc else 0)
+    outputs = (2 if split else 1) * nv * Np
+    out["volume"] = (sizeof * E * (nv * Np + outputs + nlf * nqf * ((12 + 2 * nv) if visc else nv))
+                     + msz * Ed * (10 * Nq + Np * Np) + sizeof * 11 * Ea)
+    return out
+
+
 def build_integrator(jfs, op, args, wall_T):
     pos = jfs.HybridPositivityLimiter(op)
     limiter = jfs.HybridMOODSubcellLimiter(op, positivity=pos) if args.limiter == "mood" else pos
@@ -343,7 +367,8 @@ def run_ours(args):
     for _ in range(3):
         N.check(N.lib().dgb_rhs_profile(op.native.handle, ctypes.byref(st), stage_ms, _stream_ptr()))
     stages = dict(zip(STAGES, [float(x) for x in stage_ms]))
-    sbytes = stage_bytes(op, nv, split=True)
+    fused = bool(getattr(op.native, "fused", True)) and op.native.sum_factorised
+    sbytes = stage_bytes_fused(op, nv, split=True) if fused else stage_bytes(op, nv, split=True)
     dominant = max(stages, key=stages.get)
     pk, pk_kind = peaks()
     hbm = float(pk["hbm_gbs"])
@@ -388,7 +413,10 @@ def run_ours(args):
     # launches per checked step: per stage the RHS kernels (per block / face type), then the
     # limiter and admissibility kernels (and the predictor's three per block when learned)
     nb, nf = len(op.plan.blocks), len(op.plan.faces)
-    per_stage = nb * (4 if (op.native.sum_factorised and op.viscous) else 3) + nf * (2 if op.viscous else 1)
+    if fused:
+        per_stage = 2 * nb + nf                    # traces, face kernel, element kernel
+    else:
+        per_stage = nb * (4 if (op.native.sum_factorised and op.viscous) else 3) + nf * (2 if op.viscous else 1)
     if args.limiter == "mood":
         per_stage += nb * 6 + nf + nb + 1
         if learned_head:

@@ -730,8 +730,10 @@ int run_step_mood(dgb_plan* p, const StatePtrs& U0, double dt, dgb_status* statu
       A.euler[b] = p->eul[b];
       A.out_vis[b] = p->vis[b];
     }
-    // the predictor reads the stage's base state: it decides before the high-order update
+    // the predictor reads the stage's base state: it decides before the high-order update, and
+    // in learned mode its elements skip the inviscid part of that update (fused hexahedron path)
     if (p->pred_mode && (rc = run_predict<NV>(p, *cur[s], st))) return rc;
+    if (p->pred_mode == 1 && p->hex && p->fused) A.skip_inviscid = p->pred_flags[0];
     if ((rc = run_rhs<NV>(p, *cur[s], A, st))) return rc;
     if ((rc = run_troubled<NV>(p, UNL, nullptr, p->flags, st, true))) return rc;
     if ((rc = run_subcell<NV>(p, *cur[s], p->eul, p->vis, dt, F, p->rec, st))) return rc;

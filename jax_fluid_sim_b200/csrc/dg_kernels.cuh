@@ -654,6 +654,10 @@ struct FinalizeArgs {
   const double* base[DGB_MAX_BLOCKS];
   double* dst[DGB_MAX_BLOCKS];
   double* euler[DGB_MAX_BLOCKS];     // may be null
+  // elements whose high-order inviscid update is not needed (the learned predictor sent them to
+  // the subcell scheme, which uses only their viscous residual); null: none.  Read by the fused
+  // hexahedron element kernel.
+  const uint8_t* skip_inviscid;
 };
 
 // Shared memory per element (in R values) of k_finalize: face partials [nlf][Np][NV] and the

@@ -297,6 +297,9 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
   }
   const bool visc = P_.viscous;
   const bool aff = B.affine && B.affine[e];
+  // a predicted troubled element: only its viscous residual is used (the subcell scheme replaces
+  // its update), so the inviscid volume and face terms are not formed
+  const bool skip_inv = SPLIT && A.skip_inviscid && A.skip_inviscid[e];
   const double* MT = B.minv + (size_t)e * N3 * N3;
   const float* MT32 = (sizeof(R) == sizeof(float) && B.minv32) ? B.minv32 + (size_t)e * N3 * N3 : nullptr;
   if (visc) {
@@ -414,7 +417,12 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
       R Uq[NV], F[3][NV];
 #pragma unroll
       for (int v = 0; v < NV; ++v) Uq[v] = anchor[v] + uq[v * Q3 + q];
-      {
+      if (skip_inv) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+#pragma unroll
+          for (int v = 0; v < NV; ++v) F[d][v] = Fa[d][v];
+      } else {
         const R ex[3] = {R(1), R(0), R(0)}, ey[3] = {R(0), R(1), R(0)}, ez[3] = {R(0), R(0), R(1)};
         normal_flux<NV>(P_.ph, Uq, ex, F[0]);
         normal_flux<NV>(P_.ph, Uq, ey, F[1]);
@@ -450,9 +458,14 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
     R* s2 = s1 + NV * Q * Q * N;
     R* Ri = Rr;
     R* Rv = Rr + NV * N3;
-    tensor3<NV, Q, Q, Q, N, N, N, false>(Gi + 0 * NV * Q3, Ri, s1, s2, tb->dqT, tb->bqT, tb->bqT);
-    tensor3<NV, Q, Q, Q, N, N, N, true>(Gi + 1 * NV * Q3, Ri, s1, s2, tb->bqT, tb->dqT, tb->bqT);
-    tensor3<NV, Q, Q, Q, N, N, N, true>(Gi + 2 * NV * Q3, Ri, s1, s2, tb->bqT, tb->bqT, tb->dqT);
+    if (skip_inv) {
+      for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) Ri[idx] = R(0);
+      __syncthreads();
+    } else {
+      tensor3<NV, Q, Q, Q, N, N, N, false>(Gi + 0 * NV * Q3, Ri, s1, s2, tb->dqT, tb->bqT, tb->bqT);
+      tensor3<NV, Q, Q, Q, N, N, N, true>(Gi + 1 * NV * Q3, Ri, s1, s2, tb->bqT, tb->dqT, tb->bqT);
+      tensor3<NV, Q, Q, Q, N, N, N, true>(Gi + 2 * NV * Q3, Ri, s1, s2, tb->bqT, tb->bqT, tb->dqT);
+    }
     if (SPLIT) {
       if (visc) {
         tensor3<NV, Q, Q, Q, N, N, N, false>(Gv + 0 * NV * Q3, Rv, s1, s2, tb->dqT, tb->bqT, tb->bqT);
@@ -473,7 +486,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
     const int lf = idx / (QF2 * NV), q = (idx / NV) % QF2, v = idx % NV;
     const int f = fface[lf] >> 1, side = fface[lf] & 1;
     const double si = side == 0 ? -1.0 : 1.0;
-    const double hi = si * fd.fluxI[((size_t)fslot[lf] + q) * NV + v];
+    const double hi = skip_inv ? 0.0 : si * fd.fluxI[((size_t)fslot[lf] + q) * NV + v];
     const double hv = visc ? -si * fd.fluxV[((size_t)f * QF2 + q) * NV + v] : 0.0;
     const int c = codes.perm[fperm[lf] + q];
     if (SPLIT) {

@@ -133,6 +133,7 @@ class NativePlan:
         self.sum_factorised = bool(sum_factorised)
         self.affine = bool(affine)
         N.check(L.dgb_plan_finalize(handle))
+        self.fused = True          # the plan's default form of the hexahedron right-hand side
         self._pushed = self._snapshot()
 
     def enable_mood(self, coupling="reference"):
