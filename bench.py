@@ -114,14 +114,8 @@ def max_over_ranks(value, world, device="cuda"):
 
 
 def workload(scale="full"):
-    from jax_fluid_sim_b200 import meshgen
-    if scale == "full":
-        return meshgen.sphere_oh_grid()
-    if scale == "medium":
-        return meshgen.sphere_oh_grid(n=16, n_radial=10, outer=((4, 16), (6, 6), (6, 6)))
-    if scale == "small":
-        return meshgen.sphere_oh_grid(n=8, n_radial=6, outer=((3, 10), (4, 4), (4, 4)))
-    return meshgen.sphere_oh_grid(n=4, n_radial=2, outer=((1, 3), (1, 1), (1, 1)))
+    from jax_fluid_sim_b200 import workloads
+    return workloads.sphere_mesh(scale)
 
 
 def freestream(degree):
@@ -216,22 +210,12 @@ def shock_layer(xyz):
 def bow_shock_state(solver, op, u):
     """Synthetic start with a shock in it: the Mach-3 normal-shock (Rankine-Hugoniot) state in the
     elements whose centroid lies inside r < 0.65 around the sphere of radius 0.5, the free stream
-    in the others.  Each element starts constant, so the jump sits on element faces (a jump
-    inside a P3 element would leave negative densities at its quadrature points); the first
-    steps sharpen it inside the elements next to it, which gives the MOOD detector work."""
-    g, M = GAMMA, MACH
-    rho2 = (g + 1) * M ** 2 / ((g - 1) * M ** 2 + 2)
-    p2 = 1 + 2 * g / (g + 1) * (M ** 2 - 1)
-
-    def prim(xyz):
-        inside = shock_layer(xyz)
-        W = np.zeros(xyz.shape[:-1] + (5,))
-        W[..., 0] = np.where(inside, rho2, 1.0)
-        W[..., 1] = np.where(inside, u / rho2, u)
-        W[..., 4] = np.where(inside, p2, 1.0)
-        return W
-
-    return solver.state_blocks_from_primitive_function(op, prim)
+    in the others (workloads.sphere_shock_state).  Each element starts constant, so the jump sits
+    on element faces (a jump inside a P3 element would leave negative densities at its quadrature
+    points); the first steps sharpen it inside the elements next to it, which gives the MOOD
+    detector work."""
+    from jax_fluid_sim_b200 import workloads
+    return workloads.sphere_shock_state(solver, op, u, GAMMA, MACH)
 
 
 def run_ours(args):

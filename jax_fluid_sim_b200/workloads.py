@@ -3,6 +3,8 @@ vortex (periodic hexahedron box) and the isentropic vortex on hybrid meshes (ord
 accuracy).  Non-dimensional with rho_inf = p_inf = 1 and gas constant 1 (c_inf = sqrt(gamma)).
 """
 
+import time
+
 import numpy as np
 
 from . import meshgen
@@ -167,7 +169,7 @@ def _timed(fn):
 
 
 def run_vortex(n, degree, precisions=("float64",), cfl=0.3, length=10.0, periods=1.0, graph=True, seed=0,
-               radius=0.1, autotune=True):
+               radius=0.1, autotune=True, tensor_cores=False):
     """One size of the order study: the vortex through ``periods`` periods on the n^3 hybrid box
     of side ``length``, once per precision from the same start (one host plan).  Each result
     holds the density L2 error (divided by sqrt(box volume)), the step count and the
@@ -181,6 +183,7 @@ def run_vortex(n, degree, precisions=("float64",), cfl=0.3, length=10.0, periods
     out = []
     for precision in precisions:
         op = op64 if precision == "float64" else op64.with_precision(precision)
+        tc_blocks = op.native.set_tensor_cores(True) if tensor_cores and precision == "mixed" else 0
         states = {k: v.clone() for k, v in start.items()}
         widths = op.autotune(states) if autotune else None
         integ = HybridSSPRK3(op, cfl=cfl, graph=graph)
@@ -192,7 +195,7 @@ def run_vortex(n, degree, precisions=("float64",), cfl=0.3, length=10.0, periods
                         elements={bp.etype: bp.E for bp in op.plan.blocks},
                         dofs=dof_count(op), steps=steps, dt=dt, admissible=ok and bool(first.item()),
                         l2_density=err, seconds=seconds, dof_updates_per_s=dof_count(op) * (steps - 1) / seconds,
-                        widths=widths))
+                        widths=widths, tensor_core_blocks=tc_blocks))
         del states, integ
     return out
 
@@ -234,7 +237,11 @@ def main(argv=None):
     import argparse
     import json
     ap = argparse.ArgumentParser(prog="python -m jax_fluid_sim_b200.workloads")
-    ap.add_argument("case", choices=["vortex", "tgv", "reacting", "ensemble"])
+    ap.add_argument("case", choices=["vortex", "tgv", "reacting", "ensemble", "learned"])
+    ap.add_argument("--train-steps", type=int, default=2000)
+    ap.add_argument("--eval-steps", type=int, default=2000)
+    ap.add_argument("--threshold", type=float, default=0.5)
+    ap.add_argument("--tensor-cores", type=int, default=0, help="vortex: mixed runs on the tensor-core volume kernel")
     ap.add_argument("--cases", type=int, default=64)
     ap.add_argument("--elements", default="5000,60000")
     ap.add_argument("--scale", default="full")
@@ -250,6 +257,10 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=10)
     args = ap.parse_args(argv)
     precisions = args.precision.split(",")
+    if args.case == "learned":
+        print(json.dumps(run_learned(args.scale, args.train_steps, args.eval_steps, threshold=args.threshold,
+                                     precision=precisions[-1])), flush=True)
+        return
     if args.case == "ensemble":
         lo, hi = (float(x) for x in args.elements.split(","))
         groups, total = run_ensemble(args.cases, (lo, hi), args.steps, precision=precisions[0], cfl=args.cfl)
@@ -270,13 +281,160 @@ def main(argv=None):
         errors = {}
         for n in sizes:
             for r in run_vortex(n, degree, precisions, args.cfl, periods=args.periods, radius=args.radius,
-                                autotune=bool(args.autotune)):
+                                autotune=bool(args.autotune), tensor_cores=bool(args.tensor_cores)):
                 prev = errors.get(r["precision"])
                 if prev is not None:
                     r["order"] = float(np.log(prev[1] / r["l2_density"]) / np.log(n / prev[0]))
                 errors[r["precision"]] = (n, r["l2_density"])
                 print(json.dumps(r), flush=True)
 
+
+
+# --------------------------------------------------------------------------- Mach-3 sphere
+SPHERE_GAMMA, SPHERE_MACH, SPHERE_RE, SPHERE_T_INF, SPHERE_T_WALL = 1.4, 3.0, 1.0e5, 220.0, 300.0
+
+
+def sphere_mesh(scale="full"):
+    """O/H sphere grids of the Mach-3 configuration: "full" 202,752 hexahedra, "medium" 39,488,
+    "small" and "tiny" for tests."""
+    if scale == "full":
+        return meshgen.sphere_oh_grid()
+    if scale == "medium":
+        return meshgen.sphere_oh_grid(n=16, n_radial=10, outer=((4, 16), (6, 6), (6, 6)))
+    if scale == "small":
+        return meshgen.sphere_oh_grid(n=8, n_radial=6, outer=((3, 10), (4, 4), (4, 4)))
+    return meshgen.sphere_oh_grid(n=4, n_radial=2, outer=((1, 3), (1, 1), (1, 1)))
+
+
+def sphere_shock_state(solver, op, u, gamma=SPHERE_GAMMA, mach=SPHERE_MACH, radius=0.65):
+    """The Mach-3 normal-shock (Rankine-Hugoniot) state in the elements whose centroid lies inside
+    r < radius, the free stream (rho = p = 1, velocity u along x) in the others; each element
+    starts constant, so the jump sits on element faces."""
+    g, M = gamma, mach
+    rho2 = (g + 1) * M ** 2 / ((g - 1) * M ** 2 + 2)
+    p2 = 1 + 2 * g / (g + 1) * (M ** 2 - 1)
+
+    def prim(xyz):
+        inside = np.broadcast_to(np.linalg.norm(xyz.mean(axis=1), axis=-1)[:, None] < radius, xyz.shape[:-1])
+        W = np.zeros(xyz.shape[:-1] + (5,))
+        W[..., 0] = np.where(inside, rho2, 1.0)
+        W[..., 1] = np.where(inside, u / rho2, u)
+        W[..., 4] = np.where(inside, p2, 1.0)
+        return W
+
+    return solver.state_blocks_from_primitive_function(op, prim)
+
+
+def sphere_case(scale="full", degree=3, precision="mixed"):
+    """Solver, Navier-Stokes operator, boundary descriptor and shocked start of the Mach-3 viscous
+    sphere (Re_D = 1e5, isothermal wall 300 K / 220 K), non-dimensional as the reference driver
+    (rho = p = 1, U = 3 sqrt(gamma), mu = U / Re)."""
+    from .boundary import FarfieldWallBoundary
+    from .mesh import HybridMesh
+    from .operators import HybridNavierStokesOperator
+    from .solver import HybridCompressibleSolver
+    u = SPHERE_MACH * np.sqrt(SPHERE_GAMMA)
+    solver = HybridCompressibleSolver(HybridMesh(sphere_mesh(scale)), polynomial_degree=degree,
+                                      dynamic_viscosity=u / SPHERE_RE)
+    op = HybridNavierStokesOperator(solver, precision=precision)
+    bc = FarfieldWallBoundary(solver, np.array([1.0, u, 0.0, 0.0, 1.0]),
+                              wall_temperature=SPHERE_T_WALL / SPHERE_T_INF)
+    return solver, op, bc, sphere_shock_state(solver, op, u)
+
+
+def run_learned(scale="full", train_steps=2000, eval_steps=2000, negative_fraction=0.02, threshold=0.5,
+                epochs=20, precision="mixed", seed=0, evaluate_every=100):
+    """The learned troubled-cell protocol on the Mach-3 sphere at P3 with MOOD: ``train_steps``
+    plain steps from the shocked start, each labelling every element by the a-posteriori detector
+    on the first SSP-RK stage (all positives and a seeded ``negative_fraction`` of the negatives
+    are kept); the predictor is trained on them; then, from the state reached, ``eval_steps``
+    plain steps and ``eval_steps`` learned steps (one dt for all), each run replayed as a CUDA graph
+    and timed with CUDA events.  The predictor's missed-cell and false-positive rates are measured
+    in evaluate mode (the plain step, every element tested, predictions only counted) on every
+    ``evaluate_every``-th step of the plain run.  Returns one dict."""
+    import torch
+    from .limiter import HybridMOODSubcellLimiter, HybridPositivityLimiter
+    from .predictor import TroubledCellPredictor
+    from .time_integration import HybridSSPRK3
+    solver, op, bc, U = sphere_case(scale, 3, precision)
+    limiter = HybridMOODSubcellLimiter(op, positivity=HybridPositivityLimiter(op))
+    integ = HybridSSPRK3(op, cfl=0.3, limiter=limiter, graph=True)
+    dt = integ.stable_dt(U, bc)
+    E = sum(bp.E for bp in op.plan.blocks)
+    predictor = TroubledCellPredictor(op, threshold=threshold, seed=seed)
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    Xs, ys, flagged = [], [], []
+    t0 = time.time()
+    for _ in range(train_steps):
+        X, y = predictor.labelled_samples(U, dt, bc, limiter)
+        keep = y.bool() | (torch.rand(y.shape, generator=gen, device="cuda") < negative_fraction)
+        Xs.append(X[keep])
+        ys.append(y[keep])
+        flagged.append(y.sum())
+        integ.checked_step_inplace(U, dt, bc)
+    flagged = torch.stack(flagged).double().cpu().numpy() / E
+    X, y = torch.cat(Xs), torch.cat(ys)
+    del Xs, ys
+    history = predictor.fit(X, y, epochs=epochs, batch=8192)
+    train_s = time.time() - t0
+    start = {k: v.clone() for k, v in U.items()}
+
+    def run(mode):
+        predictor.attach(mode)
+        predictor.counts(reset=True)
+        cur = {k: v.clone() for k, v in start.items()}
+        ok = torch.ones((), dtype=torch.bool, device="cuda")
+        evals = []
+        ok &= integ.checked_step_inplace(cur, dt, bc).view(torch.int32)[0] != 0     # graph capture
+        t_start, t_stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t_start.record()
+        for k in range(1, eval_steps):
+            ok &= integ.checked_step_inplace(cur, dt, bc).view(torch.int32)[0] != 0
+        t_stop.record()
+        torch.cuda.synchronize()
+        counts = predictor.counts(reset=True)
+        predictor.attach("off")
+        return cur, bool(ok.item()), t_start.elapsed_time(t_stop) / 1e3, counts, evals
+
+    plain, plain_ok, plain_s, _, _ = run("off")
+    learned, learned_ok, learned_s, learned_counts, _ = run("learned")
+    # predictor quality: evaluate mode on every evaluate_every-th step of a plain run
+    predictor.attach("evaluate")
+    predictor.counts(reset=True)
+    cur = {k: v.clone() for k, v in start.items()}
+    integ_eval = HybridSSPRK3(op, cfl=0.3, limiter=limiter, graph=False)
+    hit = missed = fp = predicted = steps_eval = 0
+    for k in range(eval_steps):
+        if k % evaluate_every == 0:
+            predictor.attach("evaluate")
+            integ_eval.checked_step_inplace(cur, dt, bc)
+            c = predictor.counts(reset=True)
+            hit, missed, fp, predicted = hit + c["hit"], missed + c["missed"], fp + c["false_positive"], \
+                predicted + c["predicted"]
+            steps_eval += 1
+            predictor.attach("off")
+        else:
+            integ.checked_step_inplace(cur, dt, bc)
+    num = sum(float(((learned[k][..., 0] - plain[k][..., 0]) ** 2).sum()) for k in plain)
+    den = sum(float((plain[k][..., 0] ** 2).sum()) for k in plain)
+    dofs = dof_count(op)
+    positives = hit + missed
+    return dict(case="learned", scale=scale, elements=E, dofs=dofs, precision=precision, dt=dt,
+                train_steps=train_steps, eval_steps=eval_steps, samples=int(X.shape[0]),
+                positives_in_samples=int(y.sum().item()), negative_fraction=negative_fraction,
+                threshold=threshold, epochs=epochs, loss_first_last=[history[0], history[-1]],
+                train_seconds=round(train_s, 1),
+                flagged_fraction_per_stage={"mean": float(flagged.mean()), "min": float(flagged.min()),
+                                            "max": float(flagged.max())},
+                plain={"dof_updates_per_s": dofs * (eval_steps - 1) / plain_s, "admissible": plain_ok},
+                learned={"dof_updates_per_s": dofs * (eval_steps - 1) / learned_s, "admissible": learned_ok,
+                         "predicted_per_stage": learned_counts["predicted"] / max(3 * (eval_steps), 1),
+                         "missed_caught_by_detector_per_stage": learned_counts["missed"] / max(3 * eval_steps, 1)},
+                evaluate={"steps": steps_eval, "missed_rate": missed / max(positives, 1),
+                          "false_positive_rate": fp / max(3 * steps_eval * E - positives, 1),
+                          "detector_flags_per_stage": positives / max(3 * steps_eval, 1),
+                          "predicted_per_stage": predicted / max(3 * steps_eval, 1)},
+                density_l2_rel_learned_vs_plain=(num / den) ** 0.5)
 
 
 # --------------------------------------------------------------------------- reacting sphere
