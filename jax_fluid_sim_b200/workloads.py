@@ -238,6 +238,7 @@ def main(argv=None):
     import json
     ap = argparse.ArgumentParser(prog="python -m jax_fluid_sim_b200.workloads")
     ap.add_argument("case", choices=["vortex", "tgv", "reacting", "ensemble", "learned"])
+    ap.add_argument("--limiter", default="mood", choices=["mood", "positivity"])
     ap.add_argument("--train-steps", type=int, default=2000)
     ap.add_argument("--eval-steps", type=int, default=2000)
     ap.add_argument("--threshold", type=float, default=0.5)
@@ -263,7 +264,8 @@ def main(argv=None):
         return
     if args.case == "ensemble":
         lo, hi = (float(x) for x in args.elements.split(","))
-        groups, total = run_ensemble(args.cases, (lo, hi), args.steps, precision=precisions[0], cfl=args.cfl)
+        groups, total = run_ensemble(args.cases, (lo, hi), args.steps, precision=precisions[0], cfl=args.cfl,
+                                     limiter=args.limiter)
         for g in groups:
             print(json.dumps(g), flush=True)
         print(json.dumps(total), flush=True)
@@ -584,11 +586,13 @@ def _cylinder_case(case, gamma=1.4):
     return meshgen.cylinder_o_grid(case["n_theta"], case["n_radial"]), far, far[1] / case["reynolds"]
 
 
-def run_ensemble(num_cases=64, elements=(5000, 60000), steps=10, warmup=2, seed=0, precision="float64", cfl=0.3):
+def run_ensemble(num_cases=64, elements=(5000, 60000), steps=10, warmup=2, seed=0, precision="float64", cfl=0.3,
+                 limiter="mood"):
     """The ensemble configuration: the cases of ``ensemble_cases`` grouped by degree, each group
     one HybridEnsemble (one launch per kernel per RK stage for all its cases, the step replayed
     as a CUDA graph), against the same cases solved one after another on their own plans, at the
-    same dt and step count (MOOD limiter, checked SSP-RK3).  Returns per group and in total
+    same dt and step count (checked SSP-RK3 with the MOOD limiter, or with ``limiter="positivity"``
+    the positivity limiter alone, which needs no subcell tables).  Returns per group and in total
     the DOF-updates/s of both, timed with CUDA events after ``warmup`` untimed steps."""
     import torch
     from .ensemble import HybridEnsemble
@@ -600,8 +604,9 @@ def run_ensemble(num_cases=64, elements=(5000, 60000), steps=10, warmup=2, seed=
     from .solver import HybridCompressibleSolver
 
     def integrator(op):
-        return HybridSSPRK3(op, cfl=cfl, limiter=HybridMOODSubcellLimiter(op, positivity=HybridPositivityLimiter(op)),
-                            graph=True)
+        pos = HybridPositivityLimiter(op)
+        lim = HybridMOODSubcellLimiter(op, positivity=pos) if limiter == "mood" else pos
+        return HybridSSPRK3(op, cfl=cfl, limiter=lim, graph=True)
 
     def timed_steps(it, U, dt, bc):
         for _ in range(warmup):
@@ -628,7 +633,8 @@ def run_ensemble(num_cases=64, elements=(5000, 60000), steps=10, warmup=2, seed=
             t_seq += timed_steps(integrator(op), Uc, dt, bc)
             del solver, op, Uc
         dofs = ens.dofs
-        groups.append(dict(degree=degree, cases=len(members), elements=sum(bp.E for bp in ens.operator.plan.blocks),
+        groups.append(dict(degree=degree, cases=len(members), limiter=limiter, precision=precision,
+                           elements=sum(bp.E for bp in ens.operator.plan.blocks),
                            dofs=dofs, dt=dt, ensemble_dof_updates_per_s=dofs * steps / t_ens,
                            sequential_dof_updates_per_s=dofs * steps / t_seq, speedup=t_seq / t_ens))
         total["dofs"] += dofs
