@@ -398,8 +398,11 @@ int run_rhs_dense(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaSt
     for (int b = 0; b < P.nblocks; ++b) {
       const int n = p->tc_on[b] ? 0 : p->launch_vol.cta0[b + 1] - p->launch_vol.cta0[b];
       rest.cta0[b + 1] = rest.cta0[b] + n;
-      if (p->tc_on[b] && tc_volume(P, S, b, p->tc[b], p->tc_image[b], p->dev_err, p->sm_count, st))
-        return fail(DGB_ERR_CUDA, "tensor-core volume launch failed");
+      if (p->tc_on[b]) {
+        const cudaError_t e = tc_volume(P, S, b, p->tc[b], p->tc_image[b], p->dev_err, p->sm_count, st);
+        if (e != cudaSuccess)
+          return fail(DGB_ERR_CUDA, std::string("tensor-core volume launch: ") + cudaGetErrorString(e));
+      }
     }
     if (rest.cta0[P.nblocks] > 0)
       k_volume<NV, R><<<rest.cta0[P.nblocks], kThreads, p->smem_vol, st>>>(P, S, rest);

@@ -87,7 +87,7 @@ struct HexFaceArgs {
 };
 
 template <int P, int NV>
-__global__ void __launch_bounds__(kThreads) k_hex_face(const DevPlan P_, const HexTables tables, const HexCodes codes,
+__global__ void __launch_bounds__(kThreads, NV <= 5 ? 5 : 1) k_hex_face(const DevPlan P_, const HexTables tables, const HexCodes codes,
                                                       const HexFaceArgs A) {
   using D = HexDims<P>;
   constexpr int N = D::N, QF = D::QF, QF2 = D::QF2;
@@ -212,6 +212,11 @@ __global__ void __launch_bounds__(kThreads) k_hex_face(const DevPlan P_, const H
       for (int c = 0; c < 12; ++c) lift[c] *= P_.ph.br2;
     }
     const size_t ss = s == 0 ? so : sn;
+    // the owner's lift at boundary faces stays in the face buffers for the wall-force integral
+    // (dgb_wall_forces reads the viscous traction there)
+    if (nb < 0)
+#pragma unroll
+      for (int c = 0; c < 12; ++c) fd.liftF[ss * 12 + c] = lift[c];
     double U[NV], g[12];
 #pragma unroll
     for (int v = 0; v < NV; ++v) U[v] = fd.trP[ss * NV + v];

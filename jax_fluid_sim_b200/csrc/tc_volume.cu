@@ -453,24 +453,21 @@ int tc_pack(const BlockDev& B, const TcShape& s, float* image, cudaStream_t st) 
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
-int tc_volume(const DevPlan& P, const StatePtrs& S, int b, const TcShape& s, const float* image, int* err,
-              int sm_count, cudaStream_t st) {
-  static bool configured = false;
-  if (!configured) {
-    if (cudaFuncSetAttribute(k_tc_volume, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess)
-      return -1;
-    configured = true;
-  }
+cudaError_t tc_volume(const DevPlan& P, const StatePtrs& S, int b, const TcShape& s, const float* image, int* err,
+                      int sm_count, cudaStream_t st) {
   const int E = P.blk[b].E;
-  if (E == 0) return 0;
+  if (E == 0) return cudaSuccess;
   const int ntiles = (E + kTcTe - 1) / kTcTe;
   const int grid = ntiles < sm_count ? ntiles : sm_count;
   // at least 60 KB of shared memory per CTA keeps at most three CTAs on an SM, so their tensor
   // memory (at most 128 columns each) always fits in the SM's 512 columns: no CTA waits in
-  // tcgen05.alloc
+  // tcgen05.alloc.  The attribute is the dynamic size of this launch (static shared memory comes
+  // on top of it within the 227 KB limit).
   const size_t smem = s.smem > 60 * 1024 ? s.smem : 60 * 1024;
+  cudaError_t e = cudaFuncSetAttribute(k_tc_volume, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
   k_tc_volume<<<grid, kTcThreads, smem, st>>>(P, S, b, s, image, err);
-  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+  return cudaGetLastError();
 }
 
 }  // namespace dgb

@@ -30,7 +30,7 @@ TcShape tc_shape(int Np, int Nq, int nv);
 // Packs the constant operands of block B into `image` (s.image_floats floats, device memory).
 int tc_pack(const BlockDev& B, const TcShape& s, float* image, cudaStream_t st);
 // Inviscid volume residuals of block b into B.Rinv; err: device word for DGB_DEVICE_TIMEOUT.
-int tc_volume(const DevPlan& P, const StatePtrs& S, int b, const TcShape& s, const float* image, int* err,
-              int sm_count, cudaStream_t st);
+cudaError_t tc_volume(const DevPlan& P, const StatePtrs& S, int b, const TcShape& s, const float* image, int* err,
+                      int sm_count, cudaStream_t st);
 
 }  // namespace dgb

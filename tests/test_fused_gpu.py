@@ -5,8 +5,11 @@ The fused form computes each face side's local BR2 lift in the face kernel as on
 of the face's jumps (for affine elements br2 coef m1i[end][end] (K (x) K), K = bf m1i bf^T; for the
 others an operator built once from M^-1) and keeps the nodal lift and the residuals in shared
 memory.  It sums in a different order than the six-launch form, so the two agree to round-off:
-1e-12 of each field's largest magnitude in float64, 1e-6 in mixed precision (float32 sums).
-Against the golden fixtures of the reference the float64 bar stays 1e-9."""
+1e-12 of each field's largest magnitude in float64.  In mixed precision the six-launch form
+forms the local lifts in float32 and the fused face kernel in float64, so the two differ by the
+float32 rounding of the lift (observed 1.3e-6); the bar there is 1e-5 between the forms and the
+mixed-precision bar of 2e-5 against the reference's float64 fixtures.  In float64 the bar
+against the fixtures stays 1e-9."""
 
 import numpy as np
 import pytest
@@ -36,7 +39,7 @@ def test_fused_matches_six_launch_form(case, precision, affine):
     assert op.native.sum_factorised
     wt = float(g["wall_temperature"])
     bc = FarfieldWallBoundary(solver, g["farfield"], wall_temperature=None if np.isnan(wt) else wt)
-    tol = 1e-12 if precision == "float64" else 1e-6
+    tol = 1e-12 if precision == "float64" else 1e-5
     for label in ("smooth", "shocked"):
         states = {k: g[f"U_{label}_{k}"] for k in g["block_names"]}
         op.native.set_fused(True)
@@ -48,9 +51,9 @@ def test_fused_matches_six_launch_form(case, precision, affine):
             assert _rel(fi[k], si[k]) <= tol, (k, _rel(fi[k], si[k]))
             assert _rel(fv[k], sv[k]) <= tol, (k, _rel(fv[k], sv[k]))
             assert _rel(ft[k], st[k]) <= tol, (k, _rel(ft[k], st[k]))
-            if precision == "float64":
-                assert _rel(fi[k], g[f"rhs_inviscid_{label}_{k}"]) <= 1e-9
-                assert _rel(fv[k], g[f"rhs_viscous_{label}_{k}"]) <= 1e-9
+            ref_tol = 1e-9 if precision == "float64" else 2e-5
+            assert _rel(fi[k], g[f"rhs_inviscid_{label}_{k}"]) <= ref_tol
+            assert _rel(fv[k], g[f"rhs_viscous_{label}_{k}"]) <= ref_tol
 
 
 @pytest.mark.parametrize("precision", ["float64", "mixed"])
@@ -75,6 +78,6 @@ def test_fused_mood_step_matches_six_launch_form(precision):
     op.native.set_fused(False)
     b = integ.checked_step(states, dt, bc)[0]
     op.native.set_fused(True)
-    tol = 1e-12 if precision == "float64" else 1e-6
+    tol = 1e-12 if precision == "float64" else 1e-5
     for k in a:
         assert _rel(a[k], b[k]) <= tol

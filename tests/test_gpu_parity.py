@@ -94,7 +94,7 @@ def test_dt_of_nan_state_matches_reference(case, poison):
     g, solver, op, bc = setup(case)
     states = {k: np.array(g[f"U_smooth_{k}"]) for k in g["block_names"]}
     first = g["block_names"][0]
-    states[first][1, 0, poison] = np.nan
+    states[first][0, 0, poison] = np.nan
     expected = TimeIntegrator(oracle_build(case.partition(":")[0])[2], cfl=5.0).stable_dt(states)
     assert abs(expected - 5e-7) <= 1e-18, expected
     close(HybridSSPRK3(op, cfl=5.0).stable_dt(states, bc), expected, 1e-12)
