@@ -256,6 +256,9 @@ def run_ours(args):
     setup_s = time.time() - t_setup
     lim0, integ0 = integs[precisions[0]]
     dt = integ0.stable_dt(U0, bc)                   # one fixed dt for every run (same trajectory)
+    # execution form of the hexahedron right-hand side per precision (fused three-launch or
+    # six-launch), the faster on the start state
+    forms = {m: ops[m].autotune_form(U0, bc) for m in precisions}
 
     # training data: plain steps from the start, labelled by the a-posteriori detector
     predictor, train = None, None
@@ -427,7 +430,9 @@ def run_ours(args):
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": "inputs larger than L2 (state 0.5 GB, inverse mass 6.6 GB per pass)",
                    "limiter": args.limiter, "troubled_elements_after": troubled, "setup_s": round(setup_s, 1),
-                   "cuda_graph_step": bool(args.graph)},
+                   "cuda_graph_step": bool(args.graph),
+                   "rhs_form": {m: f.get("chosen") for m, f in forms.items()},
+                   "rhs_form_ms": {m: {k: v for k, v in f.items() if k != "chosen"} for m, f in forms.items()}},
         "gpu_launches": per_stage * 3 * args.steps,
         "step_status": {"valid": R["valid"], "rho_min": R["rho_min"], "p_min": R["p_min"], "dt": dt},
         "stage_ms": stages,

@@ -687,6 +687,15 @@ int run_predict(dgb_plan* p, const StatePtrs& S, cudaStream_t st) {
   const DevPlan& P = p->dev;
   constexpr int per = kThreads / 32;                // elements per CTA (one warp each)
   for (int b = 0; b < P.nblocks; ++b) {
+    if (p->hex) {
+      const int g = blocks_for(P.blk[0].E, per);
+      switch (P.degree) {
+        case 1: k_hex_elem_stats<1, NV><<<g, kThreads, 0, st>>>(P, S, p->hex_tables, p->pred_stats[0]); break;
+        case 2: k_hex_elem_stats<2, NV><<<g, kThreads, 0, st>>>(P, S, p->hex_tables, p->pred_stats[0]); break;
+        default: k_hex_elem_stats<3, NV><<<g, kThreads, 0, st>>>(P, S, p->hex_tables, p->pred_stats[0]); break;
+      }
+      continue;
+    }
     const size_t sm = sizeof(double) * 2 * (size_t)P.blk[b].Np * per;
     k_elem_stats<NV><<<blocks_for(P.blk[b].E, per), kThreads, sm, st>>>(P, S, b, p->pred_stats[b]);
   }

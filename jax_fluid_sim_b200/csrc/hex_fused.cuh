@@ -21,6 +21,7 @@
 // lift is summed as one operator instead of three factors, which moves results by round-off.
 #pragma once
 #include "hex_kernels.cuh"
+#include "mlp_kernels.cuh"
 
 namespace dgb {
 
@@ -582,6 +583,75 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
       sv += part[(3 * NV + v) * N3 + i];
     }
     emit(base + (size_t)i * NV + v, (double)si, (double)sv);
+  }
+}
+
+// Predictor statistics of the hexahedron block (the layout of k_elem_stats), one warp per element:
+// the Persson fractions use the tensor-product P1 projector (three N x N pencil passes, as the
+// troubled-cell sensor) instead of the dense Np x Np projector, whose rows every warp would
+// stream from L2 for every element.
+template <int P, int NV>
+__global__ void __launch_bounds__(kThreads) k_hex_elem_stats(const DevPlan P_, const StatePtrs S,
+                                                            const HexTables tables, float* __restrict__ stats) {
+  using D = HexDims<P>;
+  constexpr int N = D::N, N3 = D::N3;
+  __shared__ double work[kThreads / 32][4 * 2 * N3];   // per warp: Mon, Low, t1, t2
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int e = blockIdx.x * (kThreads / 32) + warp;
+  if (e >= P_.blk[0].E) return;
+  const double* Ug = S.b[0] + (size_t)e * N3 * NV;
+  double* Mon = work[warp];
+  double* Low = Mon + 2 * N3;
+  double* t1 = Low + 2 * N3;
+  double* t2 = t1 + 2 * N3;
+  double srho = 0, sp = 0, rmin = INFINITY, rmax = -INFINITY, pmin = INFINITY, pmax = -INFINITY;
+  for (int l = lane; l < N3; l += 32) {
+    double u[NV], W[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) u[v] = Ug[tables.lex2node[l] * NV + v];
+    primitive<NV>(P_.ph, u, W);
+    Mon[l] = W[0];
+    Mon[N3 + l] = W[4];
+    srho += W[0];
+    sp += W[4];
+    rmin = fmin(rmin, W[0]);
+    rmax = fmax(rmax, W[0]);
+    pmin = fmin(pmin, W[4]);
+    pmax = fmax(pmax, W[4]);
+  }
+  __syncwarp();
+  double h0 = 0, h1 = 0, s0 = 0, s1 = 0;
+  if (P >= 2) {
+    warp_tensor3<2, N>(Mon, Low, t1, t2, tables.p1d);
+    for (int i = lane; i < N3; i += 32) {
+      const double m0 = Mon[i], m1 = Mon[N3 + i];
+      const double d0 = m0 - Low[i], d1 = m1 - Low[N3 + i];
+      h0 += d0 * d0;
+      h1 += d1 * d1;
+      s0 += m0 * m0;
+      s1 += m1 * m1;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    srho += __shfl_xor_sync(0xffffffff, srho, o);
+    sp += __shfl_xor_sync(0xffffffff, sp, o);
+    rmin = fmin(rmin, __shfl_xor_sync(0xffffffff, rmin, o));
+    rmax = fmax(rmax, __shfl_xor_sync(0xffffffff, rmax, o));
+    pmin = fmin(pmin, __shfl_xor_sync(0xffffffff, pmin, o));
+    pmax = fmax(pmax, __shfl_xor_sync(0xffffffff, pmax, o));
+    h0 += __shfl_xor_sync(0xffffffff, h0, o);
+    h1 += __shfl_xor_sync(0xffffffff, h1, o);
+    s0 += __shfl_xor_sync(0xffffffff, s0, o);
+    s1 += __shfl_xor_sync(0xffffffff, s1, o);
+  }
+  if (lane == 0) {
+    float* st = stats + (size_t)e * kMlpStats;
+    st[0] = (float)(srho / N3);
+    st[1] = (float)(sp / N3);
+    st[2] = (float)(rmin / fmax(fabs(rmax), 1e-30));
+    st[3] = (float)(pmin / fmax(fabs(pmax), 1e-30));
+    st[4] = (float)(h0 / fmax(s0, 1e-12));
+    st[5] = (float)(h1 / fmax(s1, 1e-12));
   }
 }
 

@@ -316,6 +316,29 @@ class HybridEulerOperator:
                 out[kernel] = row
         return out
 
+    def autotune_form(self, states, boundary_state=None, reps=3):
+        """Sum-factorised hexahedron path: time one right-hand side in the step's split form
+        (dgb_rhs_profile, CUDA events around each launch) in the fused (three-launch) and in the
+        six-launch form on ``states``, best of ``reps``, and keep the faster form in the plan.
+        Returns {"fused": ms, "six_launch": ms, "chosen": form}; an empty dict elsewhere."""
+        if not self.native.sum_factorised:
+            return {}
+        U = self.to_device(states)
+        self.native.set_boundary(boundary_state)
+        st = self.native.state(self._blocks(U))
+        ms = (ctypes.c_float * 6)()
+        out = {}
+        for name, fused in (("fused", True), ("six_launch", False)):
+            self.native.set_fused(fused)
+            best = float("inf")
+            for _ in range(int(reps) + 1):       # the first run loads the kernels
+                N.check(N.lib().dgb_rhs_profile(self.native.handle, ctypes.byref(st), ms, _stream_ptr()))
+                best = min(best, float(sum(ms)))
+            out[name] = best
+        out["chosen"] = "fused" if out["fused"] <= out["six_launch"] else "six_launch"
+        self.native.set_fused(out["chosen"] == "fused")
+        return out
+
 
 class HybridNavierStokesOperator(HybridEulerOperator):
     """BR2 viscous operator on top of the Euler residual (hybrid/navier_stokes.py:9-352)."""
