@@ -93,7 +93,10 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 5 : 1) k_hex_face(const De
   using D = HexDims<P>;
   constexpr int N = D::N, QF = D::QF, QF2 = D::QF2;
   constexpr int FPC = kThreads / QF2;                // faces per CTA
-  __shared__ double jmp[FPC * QF2][12];
+  // jumps of each face's points, [face][point][12]; the face stride is padded by two doubles so
+  // that the faces sharing a warp read different banks
+  constexpr int JS = QF2 * 12 + 2;
+  __shared__ double jmp[FPC * JS];
   __shared__ double K[QF][QF];                       // bf m1i bf^T
   const FaceDev& fd = P_.face[1];
   const int slot = threadIdx.x / QF2, q = threadIdx.x % QF2;
@@ -168,14 +171,14 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 5 : 1) k_hex_face(const De
       for (int d = 0; d < 3; ++d) {
         const double j = 0.5 * w * (vn[m] - vo[m]) * n[d];
         out[m * 3 + d] = j;
-        jmp[threadIdx.x][m * 3 + d] = j;
+        jmp[slot * JS + q * 12 + m * 3 + d] = j;
       }
   }
   __syncthreads();
   if (!live) return;
   const BlockDev& B = P_.blk[0];
   const CaseView cv = case_view(P_.ph, B.ecase, fd.ol[f]);
-  const double* jf = &jmp[slot * QF2][0];
+  const double* jf = &jmp[slot * JS];
   double Fo[3 * NV];
   const int nsides = nb >= 0 ? 2 : 1;
   for (int s = 0; s < nsides; ++s) {
