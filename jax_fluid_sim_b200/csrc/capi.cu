@@ -339,7 +339,8 @@ int run_rhs_hex_fused(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cu
   if (ev) CK(cudaEventRecord(ev[1], st));
   constexpr int FPC = kThreads / HexDims<P>::QF2;
   if (D.face[1].F > 0)
-    k_hex_face<P, NV><<<blocks_for(D.face[1].F, FPC), kThreads, 0, st>>>(D, p->hex_tables, p->hex_codes, p->hex_face);
+    k_hex_face<P, NV, R><<<blocks_for(D.face[1].F, FPC), kThreads, 0, st>>>(D, p->hex_tables, p->hex_codes,
+                                                                             p->hex_face);
   if (ev) {
     CK(cudaEventRecord(ev[2], st));
     CK(cudaEventRecord(ev[3], st));

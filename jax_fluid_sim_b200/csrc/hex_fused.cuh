@@ -87,17 +87,19 @@ struct HexFaceArgs {
   const double* lop;          // [count][6][QF2][QF2]
 };
 
-template <int P, int NV>
-__global__ void __launch_bounds__(kThreads, NV <= 5 ? 5 : 1) k_hex_face(const DevPlan P_, const HexTables tables, const HexCodes codes,
-                                                      const HexFaceArgs A) {
+// R: arithmetic of the local lifts and the viscous face flux (float in precision mode 1; HLLC and
+// the jumps are float64 in both modes).
+template <int P, int NV, typename R = double>
+__global__ void __launch_bounds__(kThreads, NV <= 5 ? 5 : 1) k_hex_face(const DevPlan P_, const HexTables tables,
+                                                                       const HexCodes codes, const HexFaceArgs A) {
   using D = HexDims<P>;
   constexpr int N = D::N, QF = D::QF, QF2 = D::QF2;
   constexpr int FPC = kThreads / QF2;                // faces per CTA
   // jumps of each face's points, [face][point][12]; the face stride is padded by two doubles so
   // that the faces sharing a warp read different banks
   constexpr int JS = QF2 * 12 + 2;
-  __shared__ double jmp[FPC * JS];
-  __shared__ double K[QF][QF];                       // bf m1i bf^T
+  __shared__ R jmp[FPC * JS];
+  __shared__ R K[QF][QF];                            // bf m1i bf^T
   const FaceDev& fd = P_.face[1];
   const int slot = threadIdx.x / QF2, q = threadIdx.x % QF2;
   const int f = blockIdx.x * FPC + slot;
@@ -107,7 +109,7 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 5 : 1) k_hex_face(const De
     double acc = 0.0;
     for (int j = 0; j < N; ++j)
       for (int k = 0; k < N; ++k) acc += tables.bf[a * N + j] * tables.m1i[j * N + k] * tables.bf[c * N + k];
-    K[a][c] = acc;
+    K[a][c] = (R)acc;
   }
   int nb = -1;
   double n[3] = {0.0, 0.0, 0.0}, w = 0.0;
@@ -171,15 +173,15 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 5 : 1) k_hex_face(const De
       for (int d = 0; d < 3; ++d) {
         const double j = 0.5 * w * (vn[m] - vo[m]) * n[d];
         out[m * 3 + d] = j;
-        jmp[slot * JS + q * 12 + m * 3 + d] = j;
+        jmp[slot * JS + q * 12 + m * 3 + d] = (R)j;
       }
   }
   __syncthreads();
   if (!live) return;
   const BlockDev& B = P_.blk[0];
   const CaseView cv = case_view(P_.ph, B.ecase, fd.ol[f]);
-  const double* jf = &jmp[slot * JS];
-  double Fo[3 * NV];
+  const R* jf = &jmp[slot * JS];
+  R Fo[3 * NV];
   const int nsides = nb >= 0 ? 2 : 1;
   for (int s = 0; s < nsides; ++s) {
     const int e = s == 0 ? fd.ol[f] : fd.nl[f];
@@ -187,19 +189,19 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 5 : 1) k_hex_face(const De
     const uint8_t* perm = codes.perm + (size_t)code * QF2;
     const int lf = A.face_lf[(size_t)f * 2 + s];
     const int cq = perm[q];
-    double lift[12];
+    R lift[12];
 #pragma unroll
-    for (int c = 0; c < 12; ++c) lift[c] = 0.0;
+    for (int c = 0; c < 12; ++c) lift[c] = R(0);
     const int li = A.lop_index ? A.lop_index[e] : -1;
     if (li < 0) {
       // affine: br2 coef m1i[end][end] (K (x) K) in this side's canonical order
       int a0, end, a1, a2;
       hex_face_axes(lf, a0, end, a1, a2);
-      const double scale = P_.ph.br2 * B.acoef[e] * tables.m1i[end * N + end];
+      const R scale = (R)(P_.ph.br2 * B.acoef[e] * tables.m1i[end * N + end]);
       const int c1 = cq % QF, c2 = cq / QF;
       for (int qp = 0; qp < QF2; ++qp) {
         const int cp = perm[qp];
-        const double kk = K[c1][cp % QF] * K[c2][cp / QF];
+        const R kk = K[c1][cp % QF] * K[c2][cp / QF];
 #pragma unroll
         for (int c = 0; c < 12; ++c) lift[c] += kk * jf[qp * 12 + c];
       }
@@ -208,39 +210,40 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 5 : 1) k_hex_face(const De
     } else {
       const double* L = A.lop + ((size_t)li * 6 + lf) * QF2 * QF2 + (size_t)cq * QF2;
       for (int qp = 0; qp < QF2; ++qp) {
-        const double kk = __ldg(L + perm[qp]);
+        const R kk = (R)__ldg(L + perm[qp]);
 #pragma unroll
         for (int c = 0; c < 12; ++c) lift[c] += kk * jf[qp * 12 + c];
       }
 #pragma unroll
-      for (int c = 0; c < 12; ++c) lift[c] *= P_.ph.br2;
+      for (int c = 0; c < 12; ++c) lift[c] *= (R)P_.ph.br2;
     }
     const size_t ss = s == 0 ? so : sn;
     // the owner's lift at boundary faces stays in the face buffers for the wall-force integral
     // (dgb_wall_forces reads the viscous traction there)
     if (nb < 0)
 #pragma unroll
-      for (int c = 0; c < 12; ++c) fd.liftF[ss * 12 + c] = lift[c];
-    double U[NV], g[12];
+      for (int c = 0; c < 12; ++c) fd.liftF[ss * 12 + c] = (double)lift[c];
+    R U[NV], g[12];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) U[v] = fd.trP[ss * NV + v];
+    for (int v = 0; v < NV; ++v) U[v] = (R)fd.trP[ss * NV + v];
 #pragma unroll
-    for (int c = 0; c < 12; ++c) g[c] = fd.trG[ss * 12 + c] + lift[c];
+    for (int c = 0; c < 12; ++c) g[c] = (R)fd.trG[ss * 12 + c] + lift[c];
     if (s == 0) {
       viscous_flux<NV>(P_.ph, cv.mu, cv.kappa, U, g, Fo);
     } else {
-      double Fn[3 * NV];
+      R Fn[3 * NV];
       viscous_flux<NV>(P_.ph, cv.mu, cv.kappa, U, g, Fn);
 #pragma unroll
-      for (int k = 0; k < 3 * NV; ++k) Fo[k] = 0.5 * (Fo[k] + Fn[k]);
+      for (int k = 0; k < 3 * NV; ++k) Fo[k] = R(0.5) * (Fo[k] + Fn[k]);
     }
   }
-  double out[NV];
+  R out[NV];
 #pragma unroll
-  for (int v = 0; v < NV; ++v) out[v] = Fo[0 * NV + v] * n[0] + Fo[1 * NV + v] * n[1] + Fo[2 * NV + v] * n[2];
-  if (nb < 0 && P_.ph.has_boundary && tag_in(fd.tag[f], P_.ph.wall, P_.ph.n_wall)) out[4] = 0.0;
+  for (int v = 0; v < NV; ++v)
+    out[v] = Fo[0 * NV + v] * (R)n[0] + Fo[1 * NV + v] * (R)n[1] + Fo[2 * NV + v] * (R)n[2];
+  if (nb < 0 && P_.ph.has_boundary && tag_in(fd.tag[f], P_.ph.wall, P_.ph.n_wall)) out[4] = R(0);
 #pragma unroll
-  for (int v = 0; v < NV; ++v) fd.fluxV[((size_t)f * QF2 + q) * NV + v] = out[v] * w;
+  for (int v = 0; v < NV; ++v) fd.fluxV[((size_t)f * QF2 + q) * NV + v] = (double)(out[v] * (R)w);
 }
 
 // Shared-memory layout of k_hex_element, in units of R.
