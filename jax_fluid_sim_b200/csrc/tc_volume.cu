@@ -24,8 +24,9 @@
 // Shared-memory operand layouts (canonical, no swizzle):
 //   A (K-major): core matrices of 8 rows x 4 values (128 B), [k/4][row/8][row%8][k%4];
 //                LBO = stride between k/4 blocks, SBO = 128 B between row groups.
-//   B (MN-major): core matrices of 8 k x 4 columns, [k/8][col/4][k%8][col%4];
-//                LBO = stride between k/8 blocks, SBO = 128 B between column groups.
+//   B (K-major as well): core matrices of 8 columns x 4 k, [k/4][col/8][col%8][k%4];
+//                LBO = stride between k/4 blocks, SBO = 128 B between column groups.
+// (An MN-major B with no swizzle read as zeros on this hardware; both operands are K-major.)
 // A2 holds only the ceil(Np/8) real row groups of each k/4 block; the MMA's rows beyond them read
 // the next block's data (in bounds: the B region follows A2) and land in TMEM lanes that are
 // never read.
@@ -93,7 +94,7 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
          ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
 }
 
-// D[tmem] (+)= A . B, kind::tf32, M = 128, A K-major, B MN-major, f32 accumulate
+// D[tmem] (+)= A . B, kind::tf32, M = 128, A and B K-major, f32 accumulate
 __device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
@@ -220,10 +221,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_volume(const DevPlan P, co
   tc_fence_after();
   const uint32_t tbase = tmem_base;
   const uint32_t d1 = tbase, d2 = tbase + ncols / 2;
-  // instruction descriptor: f32 accumulate, tf32 A and B, A K-major, B MN-major, N = N1, M = 128
-  const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | (1u << 16) | ((uint32_t)(N1 >> 3) << 17) |
+  // instruction descriptor: f32 accumulate, tf32 A and B, both K-major, N = N1, M = 128
+  const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N1 >> 3) << 17) |
                          ((uint32_t)(128 >> 4) << 24);
-  const uint32_t a1_lbo = 16 * 128, a2_lbo = (uint32_t)s.G8 * 128, b_lbo = (uint32_t)(N1 / 4) * 128;
+  const uint32_t a1_lbo = 16 * 128, a2_lbo = (uint32_t)s.G8 * 128, b_lbo = (uint32_t)(N1 / 8) * 128;
   uint32_t tma_phase = 0, mma_phase = 0;
   if (tid == 0) {
     mbar_expect_tx(&bar_tma, (uint32_t)(sizeof(float) * s.image_floats));
@@ -274,23 +275,24 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_volume(const DevPlan P, co
     ok = mbar_wait(&bar_tma, tma_phase);
     tma_phase ^= 1;
     __syncthreads();
-    // X = U - anchor (float64 difference, then float32) into B1 hi/lo, MN-major; column n = v*Te + e
+    // X = U - anchor (float64 difference, then float32) into B1 hi/lo, K-major; column n = v*Te + e
     {
       float* B1h = Bm;
       float* B1l = Bm + N1 * s.Kp1;
-      const int quads = N1 / 4;
-      for (int t = tid; t < quads * s.Kp1; t += kTcThreads) {
-        const int k = t / quads, nb = t % quads;   // node k, columns 4nb..4nb+3
+      const int kquads = s.Kp1 / 4;
+      for (int t = tid; t < kquads * N1; t += kTcThreads) {
+        const int n = t % N1, kb = t / N1;          // column n, nodes 4kb..4kb+3
+        const int v = n / Te, e = n % Te;
         float hp[4], lp[4];
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-          const int n = nb * 4 + c, v = n / Te, e = n % Te;
+          const int k = kb * 4 + c;
           float x = 0.f;
           if (v < NV && e < ne && k < Np) x = (float)(stage[((size_t)e * Np + k) * NV + v] - anchor[e][v]);
           hp[c] = tf32_hi(x);
           lp[c] = x - hp[c];
         }
-        const int off = (k / 8) * (N1 / 4) * 32 + nb * 32 + (k % 8) * 4;
+        const int off = (kb * (N1 / 8) + n / 8) * 32 + (n % 8) * 4;
         *reinterpret_cast<float4*>(B1h + off) = make_float4(hp[0], hp[1], hp[2], hp[3]);
         *reinterpret_cast<float4*>(B1l + off) = make_float4(lp[0], lp[1], lp[2], lp[3]);
       }
@@ -302,7 +304,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_volume(const DevPlan P, co
       const uint32_t a1h = smem_u32(A1), a1l = a1h + sizeof(float) * s.a1_floats;
       const uint32_t b1h = smem_u32(Bm), b1l = b1h + sizeof(float) * N1 * s.Kp1;
       for (int ks = 0; ks < s.Kp1 / 8; ++ks) {
-        const uint32_t ao = ks * 2 * a1_lbo, bo = ks * b_lbo;
+        const uint32_t ao = ks * 2 * a1_lbo, bo = ks * 2 * b_lbo;
         mma_tf32(d1, smem_desc(a1h + ao, a1_lbo, 128), smem_desc(b1h + bo, b_lbo, 128), idesc, ks > 0);
         mma_tf32(d1, smem_desc(a1h + ao, a1_lbo, 128), smem_desc(b1l + bo, b_lbo, 128), idesc, 1);
         mma_tf32(d1, smem_desc(a1l + ao, a1_lbo, 128), smem_desc(b1h + bo, b_lbo, 128), idesc, 1);
@@ -366,26 +368,23 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_volume(const DevPlan P, co
         mma_phase ^= 1;
       }
       if (q < Kq) {
+        // K-major: element (n, k = q) at ((q/4) * N1/8 + n/8) * 32 + (n%8) * 4 + q%4
         float* B2h = Bm;
         float* B2l = Bm + N1 * Kq;
-        const int kb = (q / 8) * (N1 / 4) * 32 + (q % 8) * 4;
+        const int kb = (q / 4) * (N1 / 8) * 32 + q % 4;
 #pragma unroll
-        for (int v = 0; v < NV; ++v) {
-          float hp[HALF], lp[HALF];
+        for (int v = 0; v < NV; ++v)
 #pragma unroll
           for (int j = 0; j < HALF; ++j) {
-            hp[j] = tf32_hi(G[r][j][v]);
-            lp[j] = G[r][j][v] - hp[j];
+            const int n = v * Te + half * HALF + j;
+            const float hi = tf32_hi(G[r][j][v]);
+            B2h[kb + (n / 8) * 32 + (n % 8) * 4] = hi;
+            B2l[kb + (n / 8) * 32 + (n % 8) * 4] = G[r][j][v] - hi;
           }
-          const int nb = (v * Te + half * HALF) / 4;
-          *reinterpret_cast<float4*>(B2h + kb + nb * 32) = make_float4(hp[0], hp[1], hp[2], hp[3]);
-          *reinterpret_cast<float4*>(B2l + kb + nb * 32) = make_float4(lp[0], lp[1], lp[2], lp[3]);
-        }
         if (half == 0)
-          for (int nb = (NV * Te) / 4; nb < N1 / 4; ++nb) {
-            const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-            *reinterpret_cast<float4*>(B2h + kb + nb * 32) = z;
-            *reinterpret_cast<float4*>(B2l + kb + nb * 32) = z;
+          for (int n = NV * Te; n < N1; ++n) {
+            B2h[kb + (n / 8) * 32 + (n % 8) * 4] = 0.f;
+            B2l[kb + (n / 8) * 32 + (n % 8) * 4] = 0.f;
           }
       }
       fence_async_smem();
@@ -396,7 +395,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_volume(const DevPlan P, co
         const uint32_t a2l = a2h + (uint32_t)(sizeof(float) * s.a2_floats);
         const uint32_t b2h = smem_u32(Bm), b2l = b2h + (uint32_t)(sizeof(float) * N1 * Kq);
         for (int ks = 0; ks < Kq / 8; ++ks) {
-          const uint32_t ao = ks * 2 * a2_lbo, bo = ks * b_lbo;
+          const uint32_t ao = ks * 2 * a2_lbo, bo = ks * 2 * b_lbo;
           mma_tf32(d2, smem_desc(a2h + ao, a2_lbo, 128), smem_desc(b2h + bo, b_lbo, 128), idesc, (r > 0 || ks > 0));
           mma_tf32(d2, smem_desc(a2h + ao, a2_lbo, 128), smem_desc(b2l + bo, b_lbo, 128), idesc, 1);
           mma_tf32(d2, smem_desc(a2l + ao, a2_lbo, 128), smem_desc(b2h + bo, b_lbo, 128), idesc, 1);
