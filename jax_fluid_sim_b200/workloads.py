@@ -344,8 +344,8 @@ def sphere_case(scale="full", degree=3, precision="mixed"):
     return solver, op, bc, sphere_shock_state(solver, op, u)
 
 
-def run_learned(scale="full", train_steps=2000, eval_steps=2000, negative_fraction=0.02, threshold=0.5,
-                epochs=20, precision="mixed", seed=0, evaluate_every=100):
+def run_learned(scale="full", train_steps=2000, eval_steps=2000, negative_fraction=0.01, threshold=0.5,
+                epochs=4, precision="mixed", seed=0, evaluate_every=100):
     """The learned troubled-cell protocol on the Mach-3 sphere at P3 with MOOD: ``train_steps``
     plain steps from the shocked start, each labelling every element by the a-posteriori detector
     on the first SSP-RK stage (all positives and a seeded ``negative_fraction`` of the negatives
@@ -386,7 +386,6 @@ def run_learned(scale="full", train_steps=2000, eval_steps=2000, negative_fracti
         predictor.counts(reset=True)
         cur = {k: v.clone() for k, v in start.items()}
         ok = torch.ones((), dtype=torch.bool, device="cuda")
-        evals = []
         ok &= integ.checked_step_inplace(cur, dt, bc).view(torch.int32)[0] != 0     # graph capture
         t_start, t_stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         t_start.record()
@@ -396,10 +395,10 @@ def run_learned(scale="full", train_steps=2000, eval_steps=2000, negative_fracti
         torch.cuda.synchronize()
         counts = predictor.counts(reset=True)
         predictor.attach("off")
-        return cur, bool(ok.item()), t_start.elapsed_time(t_stop) / 1e3, counts, evals
+        return cur, bool(ok.item()), t_start.elapsed_time(t_stop) / 1e3, counts
 
-    plain, plain_ok, plain_s, _, _ = run("off")
-    learned, learned_ok, learned_s, learned_counts, _ = run("learned")
+    plain, plain_ok, plain_s, _ = run("off")
+    learned, learned_ok, learned_s, learned_counts = run("learned")
     # predictor quality: evaluate mode on every evaluate_every-th step of a plain run
     predictor.attach("evaluate")
     predictor.counts(reset=True)
