@@ -11,9 +11,9 @@
 //   the flux at each point is evaluated from D1 (TMEM lane q = point q) on the CUDA cores and
 //   contracted with the metrics into G_r (r = 0, 1, 2);
 //   GEMM 2: D2 (Np nodes x Te*NV) += A2_r (Np x 128 points) . G_r (128 points x Te*NV).
-// Every operand is split hi + lo (hi = the value with its 13 low mantissa bits cleared, lo = the
-// exact float32 remainder) and each product is summed as hi.hi + hi.lo + lo.hi in float32, which
-// gives about 2^-21 relative error per product (3xTF32).
+// Every operand is split hi + lo (hi = the value rounded to tf32, lo = the remainder rounded to tf32)
+// and each product is summed as hi.hi + hi.lo + lo.hi in float32, which gives about 2^-21 relative
+// error per product (3xTF32), against 2^-24 for float32 arithmetic.
 //
 // Data movement: the constant A1/A2 images (packed once per plan by k_tc_pack) and each tile's
 // element states (Te consecutive elements are one contiguous run of the state) are copied into
@@ -122,7 +122,17 @@ __device__ __forceinline__ void tmem_ld4(uint32_t taddr, float* v) {
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-__device__ __forceinline__ float tf32_hi(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
+// x rounded to the nearest tf32 value (10 explicit mantissa bits; ties away from zero): add half
+// of the dropped unit, then clear the 13 low bits
+__device__ __forceinline__ float tf32_round(float x) {
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+}
+// the two tf32 terms of x: hi = round(x), lo = round(x - hi) (x - hi is exact in float32); hi + lo
+// represents x to about 2^-22 relative
+__device__ __forceinline__ void tf32_split(float x, float& hi, float& lo) {
+  hi = tf32_round(x);
+  lo = tf32_round(x - hi);
+}
 
 __host__ __device__ inline int round_up(int a, int b) { return (a + b - 1) / b * b; }
 
@@ -166,8 +176,9 @@ __global__ void k_tc_pack(const double* __restrict__ B, const double* __restrict
       const int kb = core / 16, g = core % 16;
       const int m = g * 8 + in / 4, k = kb * 4 + in % 4;
       const float x = (m < s.Nq && k < s.Np) ? (float)B[(size_t)m * s.Np + k] : 0.0f;
-      const float hi = tf32_hi(x);
-      image[t] = part == 0 ? hi : x - hi;
+      float hi, lo;
+      tf32_split(x, hi, lo);
+      image[t] = part == 0 ? hi : lo;
     } else {
       const int u = t - 2 * s.a1_floats;
       const int buf = u / s.a2_floats;  // r * 2 + (0 hi, 1 lo)
@@ -179,8 +190,9 @@ __global__ void k_tc_pack(const double* __restrict__ B, const double* __restrict
       const int kb = core / s.G8, g = core % s.G8;
       const int m = g * 8 + in / 4, k = kb * 4 + in % 4;
       const float x = (m < s.Np && k < s.Nq) ? (float)dB[((size_t)k * s.Np + m) * 3 + r] : 0.0f;
-      const float hi = tf32_hi(x);
-      image[t] = part == 0 ? hi : x - hi;
+      float hi, lo;
+      tf32_split(x, hi, lo);
+      image[t] = part == 0 ? hi : lo;
     }
   }
 }
@@ -289,8 +301,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_volume(const DevPlan P, co
           const int k = kb * 4 + c;
           float x = 0.f;
           if (v < NV && e < ne && k < Np) x = (float)(stage[((size_t)e * Np + k) * NV + v] - anchor[e][v]);
-          hp[c] = tf32_hi(x);
-          lp[c] = x - hp[c];
+          tf32_split(x, hp[c], lp[c]);
         }
         const int off = (kb * (N1 / 8) + n / 8) * 32 + (n % 8) * 4;
         *reinterpret_cast<float4*>(B1h + off) = make_float4(hp[0], hp[1], hp[2], hp[3]);
@@ -377,9 +388,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_volume(const DevPlan P, co
 #pragma unroll
           for (int j = 0; j < HALF; ++j) {
             const int n = v * Te + half * HALF + j;
-            const float hi = tf32_hi(G[r][j][v]);
+            float hi, lo;
+            tf32_split(G[r][j][v], hi, lo);
             B2h[kb + (n / 8) * 32 + (n % 8) * 4] = hi;
-            B2l[kb + (n / 8) * 32 + (n % 8) * 4] = G[r][j][v] - hi;
+            B2l[kb + (n / 8) * 32 + (n % 8) * 4] = lo;
           }
         if (half == 0)
           for (int n = NV * Te; n < N1; ++n) {
