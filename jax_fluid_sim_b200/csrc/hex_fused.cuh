@@ -246,21 +246,120 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 5 : 1) k_hex_face(const De
   for (int v = 0; v < NV; ++v) fd.fluxV[((size_t)f * QF2 + q) * NV + v] = (double)(out[v] * (R)w);
 }
 
+// Rotation of the thread <-> line assignment of a pencil pass, so that passes issued back to back
+// without a barrier between them start on different threads.
+__device__ __forceinline__ int rotated(int offset) {
+  return (int)((threadIdx.x + blockDim.x - (unsigned)offset % blockDim.x) % blockDim.x);
+}
+
+// The three reference-gradient fields of C nodal channels at the Q^3 volume points,
+// g[r][c][Q3] = (d/dxi_r of the interpolant), by the sum-factorised passes with the intermediates
+// shared between directions: x (bq, dq), y (bq, dq on the bq branch; bq on the dq branch), z.  Each
+// output goes through the same three 1-D products as a separate tensor3 per direction, so the values
+// are the same; the barriers are three instead of nine.  s: 2 C N^2 Q + 3 C N Q^2 values of scratch.
+template <int C, int N, int Q, typename T>
+__device__ __forceinline__ void grad3(const T* V, T* g, T* s, const T* bq, const T* dq) {
+  T* Bx = s;
+  T* Dx = Bx + C * N * N * Q;
+  T* BB = Dx + C * N * N * Q;
+  T* BD = BB + C * N * Q * Q;
+  T* DB = BD + C * N * Q * Q;
+  constexpr int L1 = C * N * N, L2 = C * N * Q, L3 = C * Q * Q, Q3 = Q * Q * Q;
+  const int st = blockDim.x;
+  auto i1 = [](int l) { return l * N; };
+  auto o1 = [](int l) { return l * Q; };
+  pencil<N, Q, false>(V, Bx, bq, L1, 1, 1, i1, o1, rotated(0), st);
+  pencil<N, Q, false>(V, Dx, dq, L1, 1, 1, i1, o1, rotated(L1), st);
+  __syncthreads();
+  auto i2 = [](int l) { return (l / Q) * N * Q + l % Q; };
+  auto o2 = [](int l) { return (l / Q) * Q * Q + l % Q; };
+  pencil<N, Q, false>(Bx, BB, bq, L2, Q, Q, i2, o2, rotated(0), st);
+  pencil<N, Q, false>(Bx, BD, dq, L2, Q, Q, i2, o2, rotated(L2), st);
+  pencil<N, Q, false>(Dx, DB, bq, L2, Q, Q, i2, o2, rotated(2 * L2), st);
+  __syncthreads();
+  auto i3 = [](int l) { return (l / (Q * Q)) * N * Q * Q + l % (Q * Q); };
+  auto o3 = [](int l) { return (l / (Q * Q)) * Q * Q * Q + l % (Q * Q); };
+  pencil<N, Q, false>(DB, g + 0 * C * Q3, bq, L3, Q * Q, Q * Q, i3, o3, rotated(0), st);
+  pencil<N, Q, false>(BD, g + 1 * C * Q3, bq, L3, Q * Q, Q * Q, i3, o3, rotated(L3), st);
+  pencil<N, Q, false>(BB, g + 2 * C * Q3, dq, L3, Q * Q, Q * Q, i3, o3, rotated(2 * L3), st);
+  __syncthreads();
+}
+
+// The weak divergence R[c][N3] = sum_r (transposed gradient of direction r) G[r][c][Q3], by three
+// passes (x, y with three inputs each, then z summing the three terms in the order of three
+// accumulating tensor3 calls: (t0 + t1) + t2), so the values match that form with three barriers
+// instead of nine.  A: 3 C Q^2 N values of scratch; the y-pass results overwrite G.
+template <int C, int N, int Q, typename T>
+__device__ __forceinline__ void div3(T* G, T* R, T* A, const T* bqT, const T* dqT) {
+  constexpr int Q3 = Q * Q * Q, LX = C * Q * Q, LY = C * Q * N, LZ = C * N * N;
+  constexpr int AS = C * Q * Q * N, BS = C * Q * N * N;
+  const int st = blockDim.x;
+  auto ix = [](int l) { return l * Q; };
+  auto ox = [](int l) { return l * N; };
+  pencil<Q, N, false>(G + 0 * C * Q3, A + 0 * AS, dqT, LX, 1, 1, ix, ox, rotated(0), st);
+  pencil<Q, N, false>(G + 1 * C * Q3, A + 1 * AS, bqT, LX, 1, 1, ix, ox, rotated(LX), st);
+  pencil<Q, N, false>(G + 2 * C * Q3, A + 2 * AS, bqT, LX, 1, 1, ix, ox, rotated(2 * LX), st);
+  __syncthreads();
+  T* B = G;                                    // [3][C][Q][N][N]
+  auto iy = [](int l) { return (l / N) * Q * N + l % N; };
+  auto oy = [](int l) { return (l / N) * N * N + l % N; };
+  pencil<Q, N, false>(A + 0 * AS, B + 0 * BS, bqT, LY, N, N, iy, oy, rotated(0), st);
+  pencil<Q, N, false>(A + 1 * AS, B + 1 * BS, dqT, LY, N, N, iy, oy, rotated(LY), st);
+  pencil<Q, N, false>(A + 2 * AS, B + 2 * BS, bqT, LY, N, N, iy, oy, rotated(2 * LY), st);
+  __syncthreads();
+  const T* mb = bqT;                           // read from shared memory (broadcast)
+  const T* md = dqT;
+  for (int line = threadIdx.x; line < LZ; line += st) {
+    const int ib = (line / (N * N)) * Q * N * N + line % (N * N);
+    const int ob = (line / (N * N)) * N * N * N + line % (N * N);
+    T x0[Q], x1[Q], x2[Q];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+      x0[i] = B[0 * BS + ib + i * N * N];
+      x1[i] = B[1 * BS + ib + i * N * N];
+      x2[i] = B[2 * BS + ib + i * N * N];
+    }
+#pragma unroll
+    for (int o = 0; o < N; ++o) {
+      T s0 = T(0), s1 = T(0), s2 = T(0);
+#pragma unroll
+      for (int i = 0; i < Q; ++i) s0 += mb[o * Q + i] * x0[i];
+#pragma unroll
+      for (int i = 0; i < Q; ++i) s1 += mb[o * Q + i] * x1[i];
+#pragma unroll
+      for (int i = 0; i < Q; ++i) s2 += md[o * Q + i] * x2[i];
+      T acc = s0;
+      acc += s1;
+      acc += s2;
+      R[ob + o * N * N] = acc;
+    }
+  }
+  __syncthreads();
+}
+
 // Shared-memory layout of k_hex_element, in units of R.
 template <int P, int NV, bool SPLIT, typename R>
 struct HexElemSmem {
   using D = HexDims<P>;
   static constexpr int N = D::N, Q = D::Q, QF = D::QF, N2 = D::N2, N3 = D::N3, Q3 = D::Q3, QF2 = D::QF2;
-  static constexpr int T = (int)((sizeof(HexTablesT<R>) + sizeof(R) - 1) / sizeof(R));
+  // table size in R, rounded up to 16 bytes so that the arrays after the tables stay 16-byte aligned
+  static constexpr int T = (int)((sizeof(HexTablesT<R>) + 15) / 16 * 16 / sizeof(R));
   static constexpr int C = SPLIT ? 2 * NV : NV;          // residual channels
   static constexpr int U = T, V = U + NV * N3, LF = V + 4 * N3, RR = LF + 12 * N3, W = RR + C * N3;
   // phase scratch (aliased)
   static constexpr int LIFT = 72 * QF2 + 72 * QF * N + 72 * N2 + 12 * N3 + 3 * 12 * N3;
-  static constexpr int C1 = NV > 12 ? NV : 12;
-  static constexpr int VOL1 = NV * Q3 + 12 * Q3 + C1 * N * N * Q + C1 * N * Q * Q;
-  static constexpr int VOL2 = NV * Q3 + 12 * Q3 + (SPLIT ? 6 : 3) * NV * Q3 + NV * Q * Q * N + NV * Q * N * N;
+  // phase C: uq [NV][Q3], gq [12][Q3], then the lift at the points lq [12][Q3] (later Gi, Gv [3][NV][Q3]
+  // each), then contraction scratch
+  static constexpr int VOL_G = cmax(12 * Q3, (SPLIT ? 6 : 3) * NV * Q3);
+  static constexpr int VOL_S = cmax(cmax(NV * N * N * Q + NV * N * Q * Q, 12 * N * N * Q + 12 * N * Q * Q),
+                                    2 * 4 * N * N * Q + 3 * 4 * N * Q * Q);
+  // the scratch lives beyond lq while Gi/Gv are not yet written; div3's x-pass results go to the
+  // dead uq/gq region when they fit there, otherwise beyond Gi/Gv
+  static constexpr int DIV_A = 3 * NV * Q * Q * N;
+  static constexpr int DIV_AT = DIV_A <= NV * Q3 + 12 * Q3 ? 0 : NV * Q3 + 12 * Q3 + VOL_G;
+  static constexpr int VOL2 = cmax(NV * Q3 + 12 * Q3 + cmax(VOL_G, 12 * Q3 + VOL_S), DIV_AT + DIV_A);
   static constexpr int FIN = 6 * C * (QF2 + QF * N) + cmax(6 * C * N2, 4 * NV * N3);
-  static constexpr int TOTAL = W + cmax(cmax(LIFT, VOL1), cmax(VOL2, FIN));
+  static constexpr int TOTAL = W + cmax(LIFT, cmax(VOL2, FIN));
 };
 
 // Lift + volume + finalize of one hexahedron (see the file comment).  SPLIT keeps the inviscid
@@ -376,13 +475,14 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
     }
   }
   __syncthreads();
-  // ---- phase C: volume terms (k_hex_volume with the lift from shared memory)
+  // ---- phase C: volume terms (k_hex_volume's arithmetic with the lift from shared memory; the
+  // gradient and divergence contractions share their intermediate passes, grad3 / div3)
   {
     R* uq = W;                           // [NV][Q3]   U - anchor at volume points
     R* gq = uq + NV * Q3;                // [12][Q3]   gradients of v: reference (3 x 4), then physical + lift
-    R* t1 = gq + 12 * Q3;                // contraction scratch
-    R* t2 = t1 + L::C1 * N * N * Q;
-    tensor3<NV, N, N, N, Q, Q, Q, false>(U, uq, t1, t2, tb->bq, tb->bq, tb->bq);
+    R* lq = gq + 12 * Q3;                // [12][Q3]   nodal lift at the points; Gi, Gv reuse this region
+    R* sc = lq + 12 * Q3;                // contraction scratch (before Gi, Gv are written)
+    tensor3<NV, N, N, N, Q, Q, Q, false>(U, uq, sc, sc + NV * N * N * Q, tb->bq, tb->bq, tb->bq);
     const double* jinv = B.jinv + (size_t)e * Q3 * 9;
     const float* jinv32 = (sizeof(R) == sizeof(float) && B.jinv32) ? B.jinv32 + (size_t)e * Q3 * 9 : nullptr;
     const double* wdet = B.wdet + (size_t)e * Q3;
@@ -393,9 +493,9 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
       deta = (R)B.adet[e];
     }
     if (visc) {
-      tensor3<4, N, N, N, Q, Q, Q, false>(V, gq + 0 * 4 * Q3, t1, t2, tb->dq, tb->bq, tb->bq);
-      tensor3<4, N, N, N, Q, Q, Q, false>(V, gq + 1 * 4 * Q3, t1, t2, tb->bq, tb->dq, tb->bq);
-      tensor3<4, N, N, N, Q, Q, Q, false>(V, gq + 2 * 4 * Q3, t1, t2, tb->bq, tb->bq, tb->dq);
+      tensor3<12, N, N, N, Q, Q, Q, false>(Lf, lq, sc, sc + 12 * N * N * Q, tb->bq, tb->bq, tb->bq);
+      grad3<4, N, Q>(V, gq, sc, tb->bq, tb->dq);
+      // reference -> physical gradient per point, plus the lift at the point
       for (int q = threadIdx.x; q < Q3; q += blockDim.x) {
         R J[9], gr[12];
 #pragma unroll
@@ -405,14 +505,15 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
 #pragma unroll
         for (int m = 0; m < 4; ++m)
 #pragma unroll
-          for (int d = 0; d < 3; ++d)
-            gq[(m * 3 + d) * Q3 + q] = gr[0 * 4 + m] * J[0 * 3 + d] + gr[1 * 4 + m] * J[1 * 3 + d] +
-                                       gr[2 * 4 + m] * J[2 * 3 + d];
+          for (int d = 0; d < 3; ++d) {
+            R x = gr[0 * 4 + m] * J[0 * 3 + d] + gr[1 * 4 + m] * J[1 * 3 + d] + gr[2 * 4 + m] * J[2 * 3 + d];
+            x += lq[(m * 3 + d) * Q3 + q];
+            gq[(m * 3 + d) * Q3 + q] = x;
+          }
       }
       __syncthreads();
-      tensor3<12, N, N, N, Q, Q, Q, true>(Lf, gq, t1, t2, tb->bq, tb->bq, tb->bq);
     }
-    R* Gi = t1;                          // [3][NV][Q3]
+    R* Gi = lq;                          // [3][NV][Q3]
     R* Gv = Gi + 3 * NV * Q3;            // [3][NV][Q3] (SPLIT only)
     R Fa[3][NV];
     {
@@ -466,23 +567,18 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
         }
     }
     __syncthreads();
-    R* s1 = Gi + (SPLIT ? 6 : 3) * NV * Q3;
-    R* s2 = s1 + NV * Q * Q * N;
     R* Ri = Rr;
     R* Rv = Rr + NV * N3;
+    R* A = W + L::DIV_AT;                 // uq and gq are dead: the x-pass results go there if they fit
     if (skip_inv) {
       for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) Ri[idx] = R(0);
       __syncthreads();
     } else {
-      tensor3<NV, Q, Q, Q, N, N, N, false>(Gi + 0 * NV * Q3, Ri, s1, s2, tb->dqT, tb->bqT, tb->bqT);
-      tensor3<NV, Q, Q, Q, N, N, N, true>(Gi + 1 * NV * Q3, Ri, s1, s2, tb->bqT, tb->dqT, tb->bqT);
-      tensor3<NV, Q, Q, Q, N, N, N, true>(Gi + 2 * NV * Q3, Ri, s1, s2, tb->bqT, tb->bqT, tb->dqT);
+      div3<NV, N, Q>(Gi, Ri, A, tb->bqT, tb->dqT);
     }
     if (SPLIT) {
       if (visc) {
-        tensor3<NV, Q, Q, Q, N, N, N, false>(Gv + 0 * NV * Q3, Rv, s1, s2, tb->dqT, tb->bqT, tb->bqT);
-        tensor3<NV, Q, Q, Q, N, N, N, true>(Gv + 1 * NV * Q3, Rv, s1, s2, tb->bqT, tb->dqT, tb->bqT);
-        tensor3<NV, Q, Q, Q, N, N, N, true>(Gv + 2 * NV * Q3, Rv, s1, s2, tb->bqT, tb->bqT, tb->dqT);
+        div3<NV, N, Q>(Gv, Rv, A, tb->bqT, tb->dqT);
       } else {
         for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) Rv[idx] = R(0);
         __syncthreads();

@@ -75,9 +75,32 @@ __device__ __forceinline__ int axis_stride(int a) { return a == 0 ? 1 : (a == 1 
 // sits at in_base(line), its first output at out_base(line); outputs also at stride ostride.
 // The lines are shared among the block's threads, or, with first/step = lane/32, among one warp's
 // lanes; a line's arithmetic does not depend on which thread takes it.
+// A contiguous run of 4 (float) or 2 (double) values at a 16-byte aligned address moves as one
+// 16-byte shared-memory access: a warp's lines then fall on distinct banks, where element-wise
+// accesses at a line stride of 4 floats meet 4-way bank conflicts.
+template <typename T>
+__device__ __forceinline__ bool vec16(const T* p, int stride) {
+  return stride == 1 && (reinterpret_cast<uintptr_t>(p) & 15) == 0;
+}
+__device__ __forceinline__ void load16(const float* p, float* x) {
+  const float4 v = *reinterpret_cast<const float4*>(p);
+  x[0] = v.x, x[1] = v.y, x[2] = v.z, x[3] = v.w;
+}
+__device__ __forceinline__ void load16(const double* p, double* x) {
+  const double2 v = *reinterpret_cast<const double2*>(p);
+  x[0] = v.x, x[1] = v.y;
+}
+__device__ __forceinline__ void store16(float* p, const float* x) {
+  *reinterpret_cast<float4*>(p) = make_float4(x[0], x[1], x[2], x[3]);
+}
+__device__ __forceinline__ void store16(double* p, const double* x) {
+  *reinterpret_cast<double2*>(p) = make_double2(x[0], x[1]);
+}
+
 template <int IN, int OUT, bool ACC, typename T, typename InBase, typename OutBase>
 __device__ __forceinline__ void pencil(const T* in, T* out, const T* M, int lines, int istride, int ostride,
                                        InBase in_base, OutBase out_base, int first = -1, int step = 0) {
+  constexpr int VW = 16 / sizeof(T);               // values per 16-byte access
   T m[OUT * IN];
 #pragma unroll
   for (int k = 0; k < OUT * IN; ++k) m[k] = M[k];
@@ -88,15 +111,40 @@ __device__ __forceinline__ void pencil(const T* in, T* out, const T* M, int line
   for (int line = first; line < lines; line += step) {
     const T* src = in + in_base(line);
     T x[IN];
+    if (IN % VW == 0 && vec16(src, istride)) {
 #pragma unroll
-    for (int i = 0; i < IN; ++i) x[i] = src[i * istride];
+      for (int i = 0; i < IN; i += VW) load16(src + i, &x[i]);
+    } else {
+#pragma unroll
+      for (int i = 0; i < IN; ++i) x[i] = src[i * istride];
+    }
     T* dst = out + out_base(line);
+    T y[OUT];
 #pragma unroll
     for (int o = 0; o < OUT; ++o) {
       T s = T(0);
 #pragma unroll
       for (int i = 0; i < IN; ++i) s += m[o * IN + i] * x[i];
-      if (ACC) dst[o * ostride] += s; else dst[o * ostride] = s;
+      y[o] = s;
+    }
+    if (OUT % VW == 0 && vec16(dst, ostride)) {
+#pragma unroll
+      for (int o = 0; o < OUT; o += VW) {
+        if (ACC) {
+          T cur[VW];
+          load16(dst + o, cur);
+#pragma unroll
+          for (int k = 0; k < VW; ++k) cur[k] += y[o + k];
+          store16(dst + o, cur);
+        } else {
+          store16(dst + o, &y[o]);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int o = 0; o < OUT; ++o) {
+        if (ACC) dst[o * ostride] += y[o]; else dst[o * ostride] = y[o];
+      }
     }
   }
 }
@@ -166,7 +214,8 @@ template <int P, int NV, typename R = double>
 struct HexSmem {
   using D = HexDims<P>;
   static constexpr int N = D::N, Q = D::Q, QF = D::QF, N2 = D::N2, N3 = D::N3, Q3 = D::Q3, QF2 = D::QF2;
-  static constexpr int T = (int)((sizeof(HexTablesT<R>) + sizeof(R) - 1) / sizeof(R));
+  // table size in R, rounded up to 16 bytes so that the arrays after the tables stay 16-byte aligned
+  static constexpr int T = (int)((sizeof(HexTablesT<R>) + 15) / 16 * 16 / sizeof(R));
   static constexpr int MS = N3 + 1;                 // padded row stride of the staged M^-1 (transposed)
   // traces: U, v, then the six faces' slabs, contraction scratch, face values and tangential derivatives
   static constexpr int TR_U = T, TR_V = TR_U + NV * N3, TR_W = TR_V + 4 * N3;
