@@ -364,7 +364,8 @@ def run_ours(args):
     tfile = ROOT / "profiles" / "traffic.json"
     if tfile.exists():
         try:
-            per_elem = json.loads(tfile.read_text()).get(dominant, {}).get("dram_bytes_per_element")
+            table = json.loads(tfile.read_text())
+            per_elem = (table.get("fused", {}) if fused else table).get(dominant, {}).get("dram_bytes_per_element")
             if per_elem:
                 traffic = per_elem * E
         except Exception:
