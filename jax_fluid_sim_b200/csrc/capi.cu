@@ -96,6 +96,8 @@ struct dgb_plan {
   double* hex_lift = nullptr;     // [E][12][N3] nodal BR2 lift scratch
   // fused right-hand side (hex_fused.cuh): on by default, dgb_plan_set_fused
   bool fused = true;
+  // false while a caller needs the float64 viscous traces (the wall-force integral reads them)
+  bool f32_traces = true;
   HexFaceArgs hex_face = {nullptr, nullptr, nullptr};
   // MOOD subcell fallback
   MoodDev mood;
@@ -334,13 +336,25 @@ int run_rhs_hex_fused(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cu
   const size_t sm_tr = sizeof(R) * (size_t)LR::TRACES, sm_el = sizeof(R) * (size_t)LE::TOTAL;
   int rc;
   if (ev) CK(cudaEventRecord(ev[0], st));
-  if ((rc = prepare(k_hex_traces<P, NV, R>, sm_tr))) return rc;
-  k_hex_traces<P, NV, R><<<E, kThreads, sm_tr, st>>>(D, S, 0, p->hex_tables, p->hex_codes);
-  if (ev) CK(cudaEventRecord(ev[1], st));
+  // mixed precision: the viscous traces travel to the face kernel in float32
+  constexpr bool MIXED = sizeof(R) == sizeof(float);
+  const bool f32 = MIXED && D.face[1].trV32 != nullptr && p->f32_traces;
   constexpr int FPC = kThreads / HexDims<P>::QF2;
-  if (D.face[1].F > 0)
-    k_hex_face<P, NV, R><<<blocks_for(D.face[1].F, FPC), kThreads, 0, st>>>(D, p->hex_tables, p->hex_codes,
-                                                                             p->hex_face);
+  const int fgrid = blocks_for(D.face[1].F, FPC);
+  if (f32) {
+    if ((rc = prepare(k_hex_traces<P, NV, R, MIXED>, sm_tr))) return rc;
+    k_hex_traces<P, NV, R, MIXED><<<E, kThreads, sm_tr, st>>>(D, S, 0, p->hex_tables, p->hex_codes);
+  } else {
+    if ((rc = prepare(k_hex_traces<P, NV, R>, sm_tr))) return rc;
+    k_hex_traces<P, NV, R><<<E, kThreads, sm_tr, st>>>(D, S, 0, p->hex_tables, p->hex_codes);
+  }
+  if (ev) CK(cudaEventRecord(ev[1], st));
+  if (D.face[1].F > 0) {
+    if (f32)
+      k_hex_face<P, NV, R, MIXED><<<fgrid, kThreads, 0, st>>>(D, p->hex_tables, p->hex_codes, p->hex_face);
+    else
+      k_hex_face<P, NV, R><<<fgrid, kThreads, 0, st>>>(D, p->hex_tables, p->hex_codes, p->hex_face);
+  }
   if (ev) {
     CK(cudaEventRecord(ev[2], st));
     CK(cudaEventRecord(ev[3], st));
@@ -1392,6 +1406,13 @@ int dgb_plan_finalize(dgb_plan* p) {
     if (p->face_present[1]) {
       if ((rc = to_float32(p, F.jinv, (size_t)F.F * 2 * F.nq * 9, &f))) return rc;
       F.jinv32 = f;
+      if (p->dev.viscous) {
+        double* d;
+        if ((rc = alloc(p, ((size_t)F.F * 2 * F.nq * 4 + 1) / 2, &d))) return rc;
+        F.trV32 = reinterpret_cast<float*>(d);
+        if ((rc = alloc(p, (size_t)F.F * 2 * F.nq * 6, &d))) return rc;
+        F.trG32 = reinterpret_cast<float*>(d);
+      }
     }
   }
   p->finalized = true;
@@ -1515,7 +1536,10 @@ int dgb_wall_forces(dgb_plan* p, const dgb_state* U, const int32_t* wall_tags, i
   memset(&A, 0, sizeof(A));
   const StatePtrs S = to_ptrs(U);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if ((rc = p->dev.nv == 5 ? run_rhs<5>(p, S, A, st) : run_rhs<16>(p, S, A, st))) return rc;
+  p->f32_traces = false;
+  rc = p->dev.nv == 5 ? run_rhs<5>(p, S, A, st) : run_rhs<16>(p, S, A, st);
+  p->f32_traces = true;
+  if (rc) return rc;
   size_t off = 0;
   for (int ft = 0; ft < 2; ++ft) {
     if (!blocks[ft]) continue;

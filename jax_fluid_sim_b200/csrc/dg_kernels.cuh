@@ -80,6 +80,10 @@ struct FaceDev {
   double* liftF;          // [F][2][nq][12] br2 * B_f r_f per side
   double* fluxV;          // [F][nq][NV]    viscous normal flux times w
   const float* jinv32;    // float32 copy of jinv (mixed-precision plans; else null)
+  // float32 traces of the viscous variables and their gradients, written and read by the fused
+  // hexahedron kernels of mixed-precision plans (else null)
+  float* trV32;           // [F][2][nq][4]
+  float* trG32;           // [F][2][nq][12]
 };
 
 struct DevPlan {

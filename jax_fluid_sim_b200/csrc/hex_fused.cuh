@@ -88,8 +88,8 @@ struct HexFaceArgs {
 };
 
 // R: arithmetic of the local lifts and the viscous face flux (float in precision mode 1; HLLC and
-// the jumps are float64 in both modes).
-template <int P, int NV, typename R = double>
+// the jumps are float64 in both modes).  F32: the viscous traces come from trV32 / trG32.
+template <int P, int NV, typename R = double, bool F32 = false>
 __global__ void __launch_bounds__(kThreads, NV <= 5 ? 5 : 1) k_hex_face(const DevPlan P_, const HexTables tables,
                                                                        const HexCodes codes, const HexFaceArgs A) {
   using D = HexDims<P>;
@@ -156,10 +156,10 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 5 : 1) k_hex_face(const De
   double vo[4], vn[4];
   if (live) {
 #pragma unroll
-    for (int m = 0; m < 4; ++m) vo[m] = fd.trV[so * 4 + m];
+    for (int m = 0; m < 4; ++m) vo[m] = F32 ? (double)fd.trV32[so * 4 + m] : fd.trV[so * 4 + m];
     if (nb >= 0) {
 #pragma unroll
-      for (int m = 0; m < 4; ++m) vn[m] = fd.trV[sn * 4 + m];
+      for (int m = 0; m < 4; ++m) vn[m] = F32 ? (double)fd.trV32[sn * 4 + m] : fd.trV[sn * 4 + m];
     } else if (P_.ph.has_boundary) {
       const CaseView cv = case_view(P_.ph, P_.blk[0].ecase, fd.ol[f]);
       viscous_ghost<NV>(P_.ph, cv.far, cv.wall_T, UL, n, fd.tag[f], vn);
@@ -227,7 +227,7 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 5 : 1) k_hex_face(const De
 #pragma unroll
     for (int v = 0; v < NV; ++v) U[v] = (R)fd.trP[ss * NV + v];
 #pragma unroll
-    for (int c = 0; c < 12; ++c) g[c] = (R)fd.trG[ss * 12 + c] + lift[c];
+    for (int c = 0; c < 12; ++c) g[c] = (F32 ? (R)fd.trG32[ss * 12 + c] : (R)fd.trG[ss * 12 + c]) + lift[c];
     if (s == 0) {
       viscous_flux<NV>(P_.ph, cv.mu, cv.kappa, U, g, Fo);
     } else {

@@ -267,7 +267,8 @@ __device__ __forceinline__ void stage_minv(const double* Mg, const int* lex2node
 // --------------------------------------------------------------------------------------------
 // Face traces of one hexahedron: anchor-form U, viscous variables, their raw physical
 // gradients, for each of the six faces, in the owner's face-point order.
-template <int P, int NV, typename R = double>
+// F32: the viscous traces go to the float32 buffers trV32 / trG32 (fused form, mixed precision).
+template <int P, int NV, typename R = double, bool F32 = false>
 __global__ void __launch_bounds__(kThreads) k_hex_traces(const DevPlan P_, const StatePtrs S, int b,
                                                         const HexTables tables, const HexCodes codes) {
   using D = HexDims<P>;
@@ -367,7 +368,8 @@ __global__ void __launch_bounds__(kThreads) k_hex_traces(const DevPlan P_, const
     for (int idx = threadIdx.x; idx < 6 * QF2 * 4; idx += blockDim.x) {
       const int lf = idx / (QF2 * 4), q = (idx / 4) % QF2, m = idx % 4;
       const int c = codes.perm[fperm[lf] + q];
-      fd.trV[((size_t)fslot[lf] + q) * 4 + m] = (double)fv[(lf * 4 + m) * QF2 + c];
+      if (F32) fd.trV32[((size_t)fslot[lf] + q) * 4 + m] = (float)fv[(lf * 4 + m) * QF2 + c];
+      else fd.trV[((size_t)fslot[lf] + q) * 4 + m] = (double)fv[(lf * 4 + m) * QF2 + c];
     }
     for (int idx = threadIdx.x; idx < 6 * QF2 * 12; idx += blockDim.x) {
       const int lf = idx / (QF2 * 12), q = (idx / 12) % QF2, m = (idx % 12) / 3, d = idx % 3;
@@ -389,7 +391,8 @@ __global__ void __launch_bounds__(kThreads) k_hex_traces(const DevPlan P_, const
         const double* J = fd.jinv + pt * 9;
         J0 = (R)J[0 * 3 + d], J1 = (R)J[1 * 3 + d], J2 = (R)J[2 * 3 + d];
       }
-      fd.trG[pt * 12 + m * 3 + d] = (double)(gx * J0 + gy * J1 + gz * J2);
+      if (F32) fd.trG32[pt * 12 + m * 3 + d] = (float)(gx * J0 + gy * J1 + gz * J2);
+      else fd.trG[pt * 12 + m * 3 + d] = (double)(gx * J0 + gy * J1 + gz * J2);
     }
   }
 }
