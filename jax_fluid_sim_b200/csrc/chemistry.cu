@@ -19,7 +19,17 @@
 // so every warp-uniform table read is a constant-cache broadcast.  Per thread, the
 // augmented Newton matrix [I - dt J | -R] (ns x ns+1) and the species vectors that the
 // reaction loops index through the stoichiometry lists live in shared memory with a
-// stride of one thread, so a warp's accesses fall in distinct banks.
+// stride of one thread, so a warp's accesses fall in distinct banks.  The net rates
+// accumulate in the matrix's last column.  At 176 doubles a node, a CTA of one warp takes
+// 45 KB, and five CTAs share an SM.
+//
+// Work saved against a literal evaluation, each with the same result up to rounding:
+//  - a reaction whose stoichiometric coefficients are all whole numbers up to 3 forms
+//    prod C^nu by multiplication instead of exp(sum nu log C) (the clip at |.| = 700 is
+//    applied to the product);
+//  - the temperature inversion stops once an update moves T by at most 1e-13 T: Newton on
+//    e(T) converges quadratically, so the remaining iterations of the fixed count change T
+//    only in its last bits.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <string.h>
@@ -34,14 +44,20 @@ int set_error(int code, const std::string& msg);
 
 namespace {
 
-constexpr int kThreads = 64;
+constexpr int kThreads = 32;
 constexpr int kMaxList = 6;
 constexpr double kClipExp = 700.0, kMinKc = 1.0e-300, kMinC = 1.0e-100;
+// exp(-700) and exp(700): the clip of the mass-action exponent applied to a product
+constexpr double kExpLo = 9.8597628436862264e-305, kExpHi = 1.0142320547350045e304;
+// the temperature inversion's convergence test (relative step)
+constexpr double kTStop = 1.0e-13;
 constexpr double kRUniv = 8.31446261815324, kPStd = 101325.0;
 
 struct Reaction {
   double A, b, theta, dn;                 // Arrhenius; sum of net stoichiometry
   int fmode, rmode, third, nf, nr, nd;    // temperature modes, third-body flag, list sizes
+  int whole;                              // every nu' and nu'' a whole number in 1..3
+  int f_pw[3], r_pw[3];                   // those whole numbers
   int f_sp[3], r_sp[3], d_sp[kMaxList];   // species of nu', nu'', nu''-nu' (ascending)
   double f_nu[3], r_nu[3], d_nu[kMaxList];
 };
@@ -76,13 +92,12 @@ struct Slots {
   double* base;
   int stride;
   __device__ double& A(int i, int j) const { return base[(i * (NS + 1) + j) * stride]; }
-  __device__ double& logC(int q) const { return base[(NS * (NS + 1) + q) * stride]; }
+  __device__ double& om(int q) const { return A(q, NS); }                              // net rates
+  __device__ double& C(int q) const { return base[(NS * (NS + 1) + q) * stride]; }     // max(C, 1e-100)
   __device__ double& dlog(int q) const { return base[(NS * (NS + 2) + q) * stride]; }
-  __device__ double& dC(int q) const { return base[(NS * (NS + 3) + q) * stride]; }
-  __device__ double& g(int q) const { return base[(NS * (NS + 4) + q) * stride]; }
-  __device__ double& om(int q) const { return base[(NS * (NS + 5) + q) * stride]; }
-  __device__ double& r0(int q) const { return base[(NS * (NS + 6) + q) * stride]; }   // Newton's rho0
-  static constexpr int kDoubles = NS * (NS + 7);
+  __device__ double& g(int q) const { return base[(NS * (NS + 3) + q) * stride]; }
+  __device__ double& r0(int q) const { return base[(NS * (NS + 4) + q) * stride]; }    // Newton's rho0
+  static constexpr int kDoubles = NS * (NS + 5);
 };
 
 // Temperature powers shared by every species at one temperature T: ln T and 1/T.  A species
@@ -172,9 +187,25 @@ __device__ double recover_T(const Tables& M, const double (&rho)[NS], double tar
       cv += Y[q] * ((cp_R(M, q, t) - 1.0) * M.RW[q]);
     }
     const double dT = -(e - target) / jmax(cv, 1.0e-5);
-    T = jclip(T + jclip(dT, -0.5 * T, 0.5 * T), 100.0, 50000.0);
+    const double Tn = jclip(T + jclip(dT, -0.5 * T, 0.5 * T), 100.0, 50000.0);
+    const bool done = fabs(Tn - T) <= kTStop * T;
+    T = Tn;
+    if (done) break;
   }
   return T;
+}
+
+// prod_k C[sp[k]]^pw[k] for whole exponents, clipped to [exp(-700), exp(700)] as the
+// exponential of the summed logarithms is; ok receives d(clip)/d(arg) under JAX's tie rule.
+template <int NS>
+__device__ __forceinline__ double mass_action(const Slots<NS>& sl, int n, const int* sp, const int* pw, double& ok) {
+  double v = 1.0;
+  for (int k = 0; k < n; ++k) {
+    const double c = sl.C(sp[k]);
+    v *= pw[k] == 1 ? c : (pw[k] == 2 ? c * c : c * c * c);
+  }
+  ok = (v > kExpLo && v < kExpHi) ? 1.0 : ((v == kExpLo || v == kExpHi) ? 0.5 : 0.0);
+  return jclip(v, kExpLo, kExpHi);
 }
 
 // Net rates at (rho, T): omega -> sl.om, and, when jac, sum_r dnu[r][s] dq_r/drho_j
@@ -187,9 +218,8 @@ __device__ void rates(const Tables& M, const Slots<NS>& sl, const double (&rho)[
     const double c = jmax(craw, 0.0);
     const double dc = dmax_tie(craw, 0.0) * M.iW[q];
     const double cc = jmax(c, kMinC);
-    sl.logC(q) = log(cc);
+    sl.C(q) = cc;
     sl.dlog(q) = dmax_tie(c, kMinC) * dc / cc;
-    sl.dC(q) = dc;
     sl.om(q) = 0.0;
   }
   const double Tg = jmax(T, 10.0);
@@ -221,11 +251,20 @@ __device__ void rates(const Tables& M, const Slots<NS>& sl, const double (&rho)[
     const double conv = R.dn == 0.0 ? 1.0 : (R.dn == 1.0 ? base : (R.dn == -1.0 ? 1.0 / base : pow(base, R.dn)));
     const double Kc = exp(-jclip(dG, -kClipExp, kClipExp)) * conv;
     const double kr = kf / jmax(Kc, kMinKc);
-    double lf = 0.0, lr = 0.0;
-    for (int k = 0; k < R.nf; ++k) lf += R.f_nu[k] * sl.logC(R.f_sp[k]);
-    for (int k = 0; k < R.nr; ++k) lr += R.r_nu[k] * sl.logC(R.r_sp[k]);
-    const double fwd = exp(jclip(lf, -kClipExp, kClipExp));
-    const double rev = exp(jclip(lr, -kClipExp, kClipExp));
+    double fwd, rev, okf, okr;
+    if (R.whole) {
+      fwd = mass_action(sl, R.nf, R.f_sp, R.f_pw, okf);
+      rev = mass_action(sl, R.nr, R.r_sp, R.r_pw, okr);
+    } else {
+      double lf = 0.0, lr = 0.0;
+      for (int k = 0; k < R.nf; ++k) lf += R.f_nu[k] * log(sl.C(R.f_sp[k]));
+      for (int k = 0; k < R.nr; ++k) lr += R.r_nu[k] * log(sl.C(R.r_sp[k]));
+      fwd = exp(jclip(lf, -kClipExp, kClipExp));
+      rev = exp(jclip(lr, -kClipExp, kClipExp));
+      // d q / d log C_j through the clipped exponentials; the tie rule at |l| == 700
+      okf = fabs(lf) < kClipExp ? 1.0 : (fabs(lf) == kClipExp ? 0.5 : 0.0);
+      okr = fabs(lr) < kClipExp ? 1.0 : (fabs(lr) == kClipExp ? 0.5 : 0.0);
+    }
     double coll = 1.0;
     if (R.third) {
       coll = 0.0;
@@ -236,9 +275,6 @@ __device__ void rates(const Tables& M, const Slots<NS>& sl, const double (&rho)[
     const double qn = qf - qr;
     for (int k = 0; k < R.nd; ++k) sl.om(R.d_sp[k]) += R.d_nu[k] * qn;
     if (!jac) continue;
-    // d q / d log C_j through the clipped exponentials; the tie rule at |l| == 700
-    const double okf = fabs(lf) < kClipExp ? 1.0 : (fabs(lf) == kClipExp ? 0.5 : 0.0);
-    const double okr = fabs(lr) < kClipExp ? 1.0 : (fabs(lr) == kClipExp ? 0.5 : 0.0);
     const double a = kf * fwd * okf * coll, b = kr * rev * okr * coll;
     const double qc = kf * fwd - kr * rev;
     for (int kd = 0; kd < R.nd; ++kd) {
@@ -254,7 +290,10 @@ __device__ void rates(const Tables& M, const Slots<NS>& sl, const double (&rho)[
       }
       if (R.third) {
 #pragma unroll
-        for (int j = 0; j < NS; ++j) sl.A(s, j) += dn * (qc * M.alpha[r][j] * sl.dC(j));
+        for (int j = 0; j < NS; ++j) {
+          const double dC = dmax_tie(rho[j] * M.iW[j], 0.0) * M.iW[j];
+          sl.A(s, j) += dn * (qc * M.alpha[r][j] * dC);
+        }
       }
     }
   }
@@ -281,6 +320,13 @@ __device__ void finish(const Tables& M, const Slots<NS>& sl, const double (&rho)
 #pragma unroll
   for (int q = 0; q < NS; ++q) sl.om(q) = sl.om(q) - (jmax(rho[q], 0.0) / S) * sw;
   if (!jac) return;
+  // per row: Y_i, and dY_i/drho_j off the diagonal (the diagonal adds dmax(rho_i, 0)/S)
+  double Yr[NS], dYo[NS];
+#pragma unroll
+  for (int i = 0; i < NS; ++i) {
+    Yr[i] = jmax(rho[i], 0.0) / S;
+    dYo[i] = -(jmax(rho[i], 0.0) / (S * S)) * dS;
+  }
 #pragma unroll
   for (int j = 0; j < NS; ++j) {
     double col = 0.0;
@@ -292,9 +338,8 @@ __device__ void finish(const Tables& M, const Slots<NS>& sl, const double (&rho)
     }
 #pragma unroll
     for (int i = 0; i < NS; ++i) {
-      const double Yi = jmax(rho[i], 0.0) / S;
-      const double dY = (i == j ? dmax_tie(rho[i], 0.0) / S : 0.0) - (jmax(rho[i], 0.0) / (S * S)) * dS;
-      const double J = sl.A(i, j) - dY * sw - Yi * col;
+      const double dY = i == j ? dmax_tie(rho[i], 0.0) / S + dYo[i] : dYo[i];
+      const double J = sl.A(i, j) - dY * sw - Yr[i] * col;
       sl.A(i, j) = newton ? (i == j ? 1.0 : 0.0) - dt * J : J;
     }
   }
@@ -468,6 +513,10 @@ int launch_react(const Tables& M, const double* U, double* out, long long nodes,
                  const double* dt_elem, cudaStream_t st) {
   const size_t sm = smem_bytes<NS>();
   cudaError_t err = cudaFuncSetAttribute(k_react<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  // the largest shared-memory carve-out, so that five one-warp CTAs share an SM
+  if (err == cudaSuccess)
+    err = cudaFuncSetAttribute(k_react<NS>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               cudaSharedmemCarveoutMaxShared);
   if (err != cudaSuccess) return fail(DGB_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(err));
   const unsigned grid = (unsigned)((nodes + kThreads - 1) / kThreads);
   k_react<NS><<<grid, kThreads, sm, st>>>(M, U, out, nodes, num_nodes, nvars, dt, dt_elem);
@@ -576,6 +625,17 @@ int dgb_chem_create(const dgb_chem_mechanism* m, const dgb_chem_params* prm, dgb
       }
     }
     R.dn = dn;
+    R.whole = 1;
+    for (int k = 0; k < R.nf; ++k) {
+      const double v = R.f_nu[k];
+      R.whole &= (v == 1.0 || v == 2.0 || v == 3.0) ? 1 : 0;
+      R.f_pw[k] = (int)v;
+    }
+    for (int k = 0; k < R.nr; ++k) {
+      const double v = R.r_nu[k];
+      R.whole &= (v == 1.0 || v == 2.0 || v == 3.0) ? 1 : 0;
+      R.r_pw[k] = (int)v;
+    }
   }
   // coupling.py:55-67
   M.iters = prm->max_newton_iters;

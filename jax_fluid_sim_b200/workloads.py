@@ -483,18 +483,41 @@ def reacting_case(scale="full", degree=2, reynolds=2.6e5, precision="float64", m
     bc = FarfieldWallBoundary(solver, far, wall_temperature=REACTING_T_WALL / REACTING_T_INF)
     coupler = ReactingFlowCoupler(dimensionless=True, reference_temperature=REACTING_T_INF,
                                   reference_pressure=REACTING_P_INF, reference_length=0.2, gamma=gamma)
+    return solver, op, bc, coupler, solver.state_blocks_from_primitive_function(
+        op, lambda xyz: reacting_start(xyz, mach, gamma))
+
+
+def reacting_start(xyz, mach=REACTING_MACH, gamma=1.4):
+    """Primitive start of the reacting sphere at the solution nodes xyz (E, N, 3): the normal-shock
+    state in the elements whose centroid lies inside r < 0.65, the free stream elsewhere, species
+    at the free-stream fractions."""
+    far = reacting_farfield(mach, gamma)
     rho2 = (gamma + 1) * mach ** 2 / ((gamma - 1) * mach ** 2 + 2)
     p2 = 1 + 2 * gamma / (gamma + 1) * (mach ** 2 - 1)
+    inside = np.broadcast_to(np.linalg.norm(xyz.mean(axis=1), axis=-1)[:, None] < 0.65, xyz.shape[:-1])
+    W = np.broadcast_to(far, xyz.shape[:-1] + (16,)).copy()
+    W[..., 0] = np.where(inside, rho2, 1.0)
+    W[..., 1] = np.where(inside, far[1] / rho2, far[1])
+    W[..., 4] = np.where(inside, p2, 1.0)
+    return W
 
-    def prim(xyz):
-        inside = np.broadcast_to(np.linalg.norm(xyz.mean(axis=1), axis=-1)[:, None] < 0.65, xyz.shape[:-1])
-        W = np.broadcast_to(far, xyz.shape[:-1] + (16,)).copy()
-        W[..., 0] = np.where(inside, rho2, 1.0)
-        W[..., 1] = np.where(inside, far[1] / rho2, far[1])
-        W[..., 4] = np.where(inside, p2, 1.0)
-        return W
 
-    return solver, op, bc, coupler, solver.state_blocks_from_primitive_function(op, prim)
+def stagnation_shock_x(node_xyz, rho, radius=0.5):
+    """Shock position on the stagnation line (the negative x axis upstream of a sphere of the given
+    radius centred at the origin): walking downstream from the far field over the solution nodes
+    that lie on the axis (nodes shared by elements averaged), the x where the density first reaches
+    the midpoint between its far-field value and its largest value on the line, interpolated
+    linearly between the two nodes that bracket it; NaN while the line holds no compression (its
+    largest density within 1e-6 of the far-field one).  node_xyz (E, N, 3), rho (E, N) numpy."""
+    on = (np.hypot(node_xyz[..., 1], node_xyz[..., 2]) < 1e-9) & (node_xyz[..., 0] <= -radius)
+    x = np.round(node_xyz[..., 0][on], 12)
+    xs, inv = np.unique(x, return_inverse=True)
+    r = np.bincount(inv, weights=rho[on]) / np.bincount(inv)
+    if r.max() <= r[0] * (1.0 + 1e-6):
+        return float("nan")
+    mid = 0.5 * (r[0] + r.max())
+    k = int(np.argmax(r >= mid))
+    return float(xs[k - 1] + (mid - r[k - 1]) / (r[k] - r[k - 1]) * (xs[k] - xs[k - 1]))
 
 
 def species_closure(states):
@@ -617,9 +640,11 @@ def run_ensemble(num_cases=64, elements=(5000, 60000), steps=10, warmup=2, seed=
     for degree in sorted({c["degree"] for c in cases}):
         members = [c for c in cases if c["degree"] == degree]
         built = [_cylinder_case(c) for c in members]
+        free0 = torch.cuda.mem_get_info()[0]
         ens = HybridEnsemble([b[0] for b in built], [b[1] for b in built], [b[2] for b in built],
                              polynomial_degree=degree, precision=precision)
         U = ens.freestream_states()
+        plan_gb = (free0 - torch.cuda.mem_get_info()[0]) / 1e9
         it = integrator(ens.operator)
         dt = it.stable_dt(U, ens.boundary)
         t_ens = timed_steps(it, U, dt, ens.boundary)
@@ -634,7 +659,7 @@ def run_ensemble(num_cases=64, elements=(5000, 60000), steps=10, warmup=2, seed=
         dofs = ens.dofs
         groups.append(dict(degree=degree, cases=len(members), limiter=limiter, precision=precision,
                            elements=sum(bp.E for bp in ens.operator.plan.blocks),
-                           dofs=dofs, dt=dt, ensemble_dof_updates_per_s=dofs * steps / t_ens,
+                           dofs=dofs, dt=dt, device_gb=round(plan_gb, 2), ensemble_dof_updates_per_s=dofs * steps / t_ens,
                            sequential_dof_updates_per_s=dofs * steps / t_seq, speedup=t_seq / t_ens))
         total["dofs"] += dofs
         total["ensemble_seconds"] += t_ens

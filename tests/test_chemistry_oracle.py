@@ -137,3 +137,32 @@ def test_coupler_dimensionless_block():
     out = Coupler(16, True, 220.0, 500.0, 0.1).react_block(U, dt)
     _check_coupler_invariants(U, out)
     assert np.max(np.abs(out - GOLDEN["dimless_out"])[..., 5:] / U[..., :1]) < 1e-5
+
+
+def test_batched_oracle_matches_per_node(mech):
+    """The batched restatement (all nodes at once, used for multi-step fixtures) against the
+    per-node one: rates and Jacobian to round-off; the coupler to round-off where its Newton
+    converges, and within the stiff-matrix bound of 1e-5 of the node density where I - dt J is
+    nearly singular."""
+    from oracle.chemistry import batch_rates, batch_react_block, batch_temperature
+    states, temps = GOLDEN["rate_states"], GOLDEN["rate_temps"]
+    rho = np.repeat(states, len(temps), axis=0)
+    T = np.tile(temps, len(states))
+    w, J = batch_rates(mech, rho, T)
+    for k in range(len(rho)):
+        _, w1, J1 = mech.rates(rho[k], T[k], jacobian=True)
+        assert np.max(np.abs(w[k] - w1)) <= 1e-12 * max(np.max(np.abs(w1)), 1e-300)
+        assert np.max(np.abs(J[k] - J1)) <= 1e-12 * max(np.max(np.abs(J1)), 1e-300)
+    e = np.array([mech.internal_energy(r, t) for r, t in zip(rho, T)])
+    Tb = batch_temperature(mech, rho, e, np.full(len(rho), 1000.0))
+    Tn = np.array([mech.temperature(r, x, 1000.0) for r, x in zip(rho, e)])
+    np.testing.assert_allclose(Tb, Tn, rtol=1e-12)
+    U = GOLDEN["coupler_U"]
+    c = Coupler(16)
+    conv_dt = float(GOLDEN["coupler_conv_dt"])
+    assert np.max(np.abs(batch_react_block(c, U, conv_dt) - c.react_block(U, conv_dt))[..., 5:] / U[..., :1]) < 1e-12
+    U, dt = GOLDEN["dimless_U"], float(GOLDEN["dimless_dt"])
+    cd = Coupler(16, True, 220.0, 500.0, 0.1)
+    out = batch_react_block(cd, U, dt)
+    _check_coupler_invariants(U, out)
+    assert np.max(np.abs(out - GOLDEN["dimless_out"])[..., 5:] / U[..., :1]) < 1e-5

@@ -58,3 +58,37 @@ def test_reacting_step_against_oracle():
         hot = np.argsort(-(ref[k][..., 4] / ref[k][..., 0]).max(axis=1))[:8]
         oref = oc.react_block(ref[k][hot], dt)
         assert np.max(np.abs(reacted[hot][..., 5:] - oref[..., 5:]) / ref[k][hot][..., :1]) <= 1e-5
+
+
+def test_reacting_steps_and_shock_position_against_oracle():
+    """Twenty steps of the reacting sphere (each a checked MOOD step, then the Air-11 source on every
+    node) on the smallest grid from the shocked start, against the oracle's own run
+    (tests/golden/make_golden_reacting.py, the batched oracle coupler): the same admissibility in
+    every step, the bow shock's position on the stagnation line after every step (it forms at the
+    wall and stands off to x = -0.804 within these steps) to 1e-10, and the final state at 2,048
+    seeded nodes: the flow to 1e-10 of each field's largest magnitude, the species to 1e-9 of the
+    node density (measured: 2e-14 and 2e-13)."""
+    from pathlib import Path
+    import jax_fluid_sim_b200 as jfs
+    G = np.load(Path(__file__).resolve().parent / "golden" / "reacting_tiny.npz")
+    solver, op, bc, coupler, U = workloads.reacting_case("tiny", degree=2)
+    integ = jfs.HybridSSPRK3(op, cfl=0.3, limiter=jfs.HybridMOODSubcellLimiter(
+        op, positivity=jfs.HybridPositivityLimiter(op)))
+    dt = float(G["dt"])
+    assert abs(integ.stable_dt(U, bc) - dt) <= 1e-12 * dt
+    xyz = op.solution_node_coordinates["hexahedron"]
+    shock, valid = [workloads.stagnation_shock_x(xyz, U["hexahedron"][..., 0].cpu().numpy())], []
+    for _ in range(int(G["steps"])):
+        U, ok, _, _ = integ.checked_step(U, dt, bc)
+        valid.append(bool(ok))
+        U = {k: coupler.react_block(v, dt) for k, v in U.items()}
+        shock.append(workloads.stagnation_shock_x(xyz, U["hexahedron"][..., 0].cpu().numpy()))
+    assert valid == list(G["valid"])
+    np.testing.assert_allclose(shock, G["shock_x"], rtol=0, atol=1e-10, equal_nan=True)
+    assert np.isnan(shock[0]) and shock[-1] < -0.8
+    got = U["hexahedron"].reshape(-1, U["hexahedron"].shape[-1]).cpu().numpy()[G["sample_index"]]
+    ref = G["sample_state"]
+    flow = (np.abs(got - ref)[:, :5].max(axis=0) / np.abs(ref[:, :5]).max(axis=0)).max()
+    assert flow <= 1e-10, flow
+    species = np.max(np.abs(got - ref)[:, 5:] / ref[:, :1])
+    assert species <= 1e-9, species
