@@ -310,6 +310,53 @@ int dgb_plan_set_subcells(dgb_plan* plan, int block, const dgb_subcell_block_des
 int dgb_plan_set_subcell_faces(dgb_plan* plan, int face_type, const int32_t* osub, const int32_t* nsub);
 int dgb_plan_enable_mood(dgb_plan* plan);
 
+/* The same MOOD tables built on the device (HybridSubcellFV.__init__, hybrid/subcell.py:277-396),
+ * in place of dgb_plan_set_subcells / dgb_plan_set_subcell_faces.  The reference subdivision of
+ * the block's element type is described once, host pointers:
+ *   - the subcells' P2 volume rule (Qs points per subcell, each weight times the subcell's
+ *     affine reference-volume factor), the DG basis and the geometry-basis gradients at the
+ *     mapped points, the geometry basis at the subcell vertices;
+ *   - the subcell vertex lists and the internal and boundary subfaces (3 or 4 vertices, -1 past
+ *     a triangle's third), with the index tables of dgb_subcell_block_desc.
+ * geometry_nodes: host [E][num_geometry_nodes][3], the block's geometry-map nodes.  Per element
+ * the device forms |det J| at the mapped points, the subcell volumes and centres, the
+ * metric-weighted projection, its volume-weighted least-squares left inverse (Gram matrix
+ * inverted by Gauss-Jordan) and the subface normals, areas and centres, one CTA per element.
+ * A Gram matrix that is not positive definite fails with DGB_ERR_ARGUMENT. */
+typedef struct {
+  int num_subcells;               /* S = 64 */
+  int num_points;                 /* Qs */
+  int num_geometry_nodes;         /* ng of the geometry map */
+  int num_vertices;               /* V, subcell vertices */
+  int cell_size;                  /* vertices per subcell: 8, 6 or 4 */
+  int num_internal, num_boundary; /* NI, NB */
+  const double* rule_weights;     /* [S][Qs] */
+  const double* point_basis;      /* [S][Qs][Np] */
+  const double* point_geometry_grad; /* [S][Qs][ng][3] */
+  const double* vertex_geometry;  /* [V][ng] */
+  const int32_t* cells;           /* [S][cell_size] */
+  const int32_t* internal_faces;  /* [NI][4] */
+  const int32_t* boundary_faces;  /* [NB][4] */
+  const int32_t* internal_owner;  /* [NI] */
+  const int32_t* internal_neighbor; /* [NI] */
+  const int32_t* boundary_owner;  /* [NB] */
+  const int32_t* csr_ptr;         /* [S+1] */
+  const int32_t* csr_face;        /* [2 NI] */
+  const double* boundary_basis;   /* [NB][Np] */
+  const int32_t* gather;          /* [NB] */
+  const int32_t* scatter;         /* [NB] */
+} dgb_subcell_reference;
+
+int dgb_plan_build_subcells(dgb_plan* plan, int block, const dgb_subcell_reference* ref,
+                            const double* geometry_nodes);
+/* Neighbour subfaces matched to the owner's by physical centre on the device (subcell.py:
+ * 473-533): osub [F][16] the owner's boundary subfaces, ncand [F][16] the neighbour's boundary
+ * subfaces on its parent face in reference order (-1 on boundary faces), host.  Centres are
+ * taken relative to each side's face centre, so periodic partners match; a face whose 16
+ * nearest partners are not distinct or lie farther than 2e-6 of the face's scale fails with
+ * DGB_ERR_ARGUMENT.  Needs dgb_plan_build_subcells on the blocks of both sides first. */
+int dgb_plan_match_subcell_faces(dgb_plan* plan, int face_type, const int32_t* osub, const int32_t* ncand);
+
 /* HybridSubcellFV.recompute (hybrid/subcell.py:855-950): base state, Euler DG candidate,
  * dt, optional additional rhs (viscous, projected onto the subcells) and troubled flags
  * [E_b] per block (device uint8) -> out (device state).  No positivity limiting. */

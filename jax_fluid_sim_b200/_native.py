@@ -50,6 +50,18 @@ class SubcellBlockDesc(ctypes.Structure):
     ]
 
 
+class SubcellReference(ctypes.Structure):
+    _fields_ = [
+        ("num_subcells", c_int), ("num_points", c_int), ("num_geometry_nodes", c_int), ("num_vertices", c_int),
+        ("cell_size", c_int), ("num_internal", c_int), ("num_boundary", c_int),
+        ("rule_weights", P_double), ("point_basis", P_double), ("point_geometry_grad", P_double),
+        ("vertex_geometry", P_double), ("cells", P_int32), ("internal_faces", P_int32), ("boundary_faces", P_int32),
+        ("internal_owner", P_int32), ("internal_neighbor", P_int32), ("boundary_owner", P_int32),
+        ("csr_ptr", P_int32), ("csr_face", P_int32), ("boundary_basis", P_double), ("gather", P_int32),
+        ("scatter", P_int32),
+    ]
+
+
 class BlockDesc(ctypes.Structure):
     _fields_ = [
         ("element_type", c_int), ("num_elements", c_int), ("num_nodes", c_int), ("num_qp", c_int),
@@ -142,6 +154,8 @@ def lib():
             "dgb_rhs_profile": [c_void_p, ctypes.POINTER(State), ctypes.POINTER(ctypes.c_float), c_void_p],
             "dgb_plan_set_subcells": [c_void_p, c_int, ctypes.POINTER(SubcellBlockDesc)],
             "dgb_plan_set_subcell_faces": [c_void_p, c_int, P_int32, P_int32],
+            "dgb_plan_build_subcells": [c_void_p, c_int, ctypes.POINTER(SubcellReference), P_double],
+            "dgb_plan_match_subcell_faces": [c_void_p, c_int, P_int32, P_int32],
             "dgb_plan_enable_mood": [c_void_p],
             "dgb_chem_create": [ctypes.POINTER(ChemMechanism), ctypes.POINTER(ChemParams), ctypes.POINTER(c_void_p)],
             "dgb_chem_destroy": [c_void_p],

@@ -13,6 +13,7 @@
 #include "hex_kernels.cuh"
 #include "mlp_kernels.cuh"
 #include "mood_kernels.cuh"
+#include "subcell_build.cuh"
 #include "tc_volume.h"
 
 using namespace dgb;
@@ -102,6 +103,8 @@ struct dgb_plan {
   // MOOD subcell fallback
   MoodDev mood;
   bool sub_block_set[DGB_MAX_BLOCKS] = {false, false, false};
+  // boundary subface centres of the device-built subcell tables, kept until the faces are matched
+  double* sub_bdc[DGB_MAX_BLOCKS] = {nullptr, nullptr, nullptr};
   bool sub_face_set[2] = {false, false};
   bool mood_ready = false;
   uint8_t* flags[DGB_MAX_BLOCKS] = {nullptr, nullptr, nullptr};
@@ -1128,35 +1131,6 @@ int dgb_plan_set_hex_affine(dgb_plan* p, const uint8_t* affine, const double* co
   return DGB_OK;
 }
 
-// In-place inverse of the symmetric positive definite n x n matrix A in shared memory by
-// Gauss-Jordan elimination without pivoting (every pivot of an SPD matrix is positive), worked by
-// the whole block; rk, ck: n doubles of shared scratch.  Returns false, uniformly across the
-// block, at a pivot that is not positive and finite.  Ends with the block synchronised.
-__device__ bool gauss_jordan_spd(double* A, int n, double* rk, double* ck) {
-  for (int k = 0; k < n; ++k) {
-    __syncthreads();
-    for (int t = threadIdx.x; t < n; t += blockDim.x) {
-      rk[t] = A[k * n + t];
-      ck[t] = A[t * n + k];
-    }
-    __syncthreads();
-    const double piv = rk[k];
-    if (!(piv > 0.0) || !isfinite(piv)) return false;   // every thread read the same pivot
-    const double r = 1.0 / piv;
-    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
-      const int i = idx / n, j = idx % n;
-      if (i == k)
-        A[idx] = j == k ? r : rk[j] * r;
-      else if (j == k)
-        A[idx] = -ck[i] * r;
-      else
-        A[idx] -= ck[i] * rk[j] * r;
-    }
-  }
-  __syncthreads();
-  return true;
-}
-
 // Inverse mass matrices, one element per CTA (plan set-up; hybrid/geometry.py:181-192):
 // M_e = B^T diag(w|J|) B is formed in shared memory, each entry summed over the volume points in
 // order and mirrored so that M_e is exactly symmetric, inverted in place (gauss_jordan_spd; a
@@ -1467,6 +1441,7 @@ int dgb_plan_destroy(dgb_plan* p) {
   if (p->step_exec) cudaGraphExecDestroy(p->step_exec);
   if (p->capture_stream) cudaStreamDestroy(p->capture_stream);
   for (void* d : p->allocations) cudaFree(d);
+  for (double* d : p->sub_bdc) cudaFree(d);
   delete p;
   return DGB_OK;
 }
@@ -1584,6 +1559,171 @@ int dgb_plan_set_subcells(dgb_plan* p, int b, const dgb_subcell_block_desc* d) {
   return DGB_OK;
 }
 
+int dgb_plan_build_subcells(dgb_plan* p, int b, const dgb_subcell_reference* r, const double* geometry_nodes) {
+  if (!p || !r || b < 0 || b >= p->dev.nblocks || !p->block_set[b]) return fail(DGB_ERR_ARGUMENT, "bad subcell block");
+  const BlockDev& B = p->dev.blk[b];
+  if (r->num_subcells != 64) return fail(DGB_ERR_UNSUPPORTED, "subcell tables need 64 subcells (4 divisions)");
+  if (r->num_points < 1 || r->num_geometry_nodes < 1 || r->num_vertices < 1 || r->num_internal < 1 ||
+      r->num_boundary < 1 || (r->cell_size != 4 && r->cell_size != 6 && r->cell_size != 8))
+    return fail(DGB_ERR_ARGUMENT, "bad subcell reference sizes");
+  if (!r->rule_weights || !r->point_basis || !r->point_geometry_grad || !r->vertex_geometry || !r->cells ||
+      !r->internal_faces || !r->boundary_faces || !r->internal_owner || !r->internal_neighbor || !r->boundary_owner ||
+      !r->csr_ptr || !r->csr_face || !r->boundary_basis || !r->gather || !r->scatter)
+    return fail(DGB_ERR_ARGUMENT, "null subcell reference table");
+  const int S = r->num_subcells, NI = r->num_internal, NB = r->num_boundary, V = r->num_vertices;
+  // every index the device follows stays inside its table
+  for (int k = 0; k < S * r->cell_size; ++k)
+    if (r->cells[k] < 0 || r->cells[k] >= V) return fail(DGB_ERR_ARGUMENT, "subcell vertex out of range");
+  for (int f = 0; f < NI + NB; ++f) {
+    const int32_t* fv = f < NI ? r->internal_faces + f * 4 : r->boundary_faces + (f - NI) * 4;
+    for (int k = 0; k < 4; ++k)
+      if ((k < 3 || fv[k] >= 0) && (fv[k] < 0 || fv[k] >= V)) return fail(DGB_ERR_ARGUMENT, "subface vertex out of range");
+    const int own = f < NI ? r->internal_owner[f] : r->boundary_owner[f - NI];
+    if (own < 0 || own >= S || (f < NI && (r->internal_neighbor[f] < 0 || r->internal_neighbor[f] >= S)))
+      return fail(DGB_ERR_ARGUMENT, "subface subcell out of range");
+  }
+  SubcellBlockDev& C = p->mood.blk[b];
+  if (p->sub_block_set[b]) return fail(DGB_ERR_ARGUMENT, "subcell tables already set for this block");
+  C.S = S;
+  C.NI = NI;
+  C.NB = NB;
+  const size_t E = B.E, Np = B.Np, Qs = r->num_points, ng = r->num_geometry_nodes;
+  int rc;
+  // the index tables the MOOD kernels read, as dgb_plan_set_subcells uploads them
+  if ((rc = upload(p, r->internal_owner, (size_t)NI, &C.iown))) return rc;
+  if ((rc = upload(p, r->internal_neighbor, (size_t)NI, &C.inbr))) return rc;
+  if ((rc = upload(p, r->csr_ptr, (size_t)S + 1, &C.csr_ptr))) return rc;
+  if ((rc = upload(p, r->csr_face, 2 * (size_t)NI, &C.csr_face))) return rc;
+  if ((rc = upload(p, r->boundary_basis, (size_t)NB * Np, &C.bbasis))) return rc;
+  if ((rc = upload(p, r->gather, (size_t)NB, &C.gather))) return rc;
+  if ((rc = upload(p, r->scatter, (size_t)NB, &C.scatter))) return rc;
+  if (E == 0) {
+    p->sub_block_set[b] = true;
+    return DGB_OK;
+  }
+  SubcellRefDev R{S, (int)Qs, (int)ng, V, r->cell_size, NI, NB, (int)Np, nullptr, nullptr, nullptr, nullptr,
+                  nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  if ((rc = upload(p, r->rule_weights, (size_t)S * Qs, &R.rw))) return rc;
+  if ((rc = upload(p, r->point_basis, (size_t)S * Qs * Np, &R.sb))) return rc;
+  if ((rc = upload(p, r->point_geometry_grad, (size_t)S * Qs * ng * 3, &R.gq))) return rc;
+  if ((rc = upload(p, r->vertex_geometry, (size_t)V * ng, &R.vg))) return rc;
+  if ((rc = upload(p, r->cells, (size_t)S * r->cell_size, &R.cells))) return rc;
+  if ((rc = upload(p, r->internal_faces, (size_t)NI * 4, &R.ifaces))) return rc;
+  if ((rc = upload(p, r->boundary_faces, (size_t)NB * 4, &R.bfaces))) return rc;
+  R.iown = C.iown;
+  R.inbr = C.inbr;
+  if ((rc = upload(p, r->boundary_owner, (size_t)NB, &R.bown))) return rc;
+  const size_t smem = subcell_build_smem(R);
+  if (smem > 220 * 1024) return fail(DGB_ERR_UNSUPPORTED, "element too large for the subcell-table kernel");
+  SubcellBuildOut O;
+  double* d;
+  if ((rc = alloc(p, E * S * Np, &d))) return rc;
+  O.P = d;
+  if ((rc = alloc(p, E * Np * S, &d))) return rc;
+  O.R = d;
+  if ((rc = alloc(p, E * S, &d))) return rc;
+  O.vol = d;
+  if ((rc = alloc(p, E * S * 3, &d))) return rc;
+  O.cen = d;
+  if ((rc = alloc(p, E * NI * 3, &d))) return rc;
+  O.in_n = d;
+  if ((rc = alloc(p, E * NI, &d))) return rc;
+  O.in_a = d;
+  if ((rc = alloc(p, E * NB * 3, &d))) return rc;
+  O.bd_n = d;
+  if ((rc = alloc(p, E * NB, &d))) return rc;
+  O.bd_a = d;
+  CK(cudaMalloc(&O.bd_c, E * NB * 3 * sizeof(double)));
+  p->sub_bdc[b] = O.bd_c;
+  double* xyz = nullptr;
+  int* bad = nullptr;
+  int h_bad = 0;
+  cudaError_t err = cudaMalloc(&xyz, E * ng * 3 * sizeof(double));
+  if (err == cudaSuccess) err = cudaMalloc(&bad, sizeof(int));
+  if (err == cudaSuccess) err = cudaMemcpy(xyz, geometry_nodes, E * ng * 3 * sizeof(double), cudaMemcpyHostToDevice);
+  if (err == cudaSuccess) err = cudaMemset(bad, 0, sizeof(int));
+  if (err == cudaSuccess)
+    err = cudaFuncSetAttribute(k_subcell_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err == cudaSuccess) {
+    k_subcell_build<<<(unsigned)E, 256, smem>>>(R, xyz, O, bad);
+    err = cudaGetLastError();
+  }
+  if (err == cudaSuccess) err = cudaMemcpy(&h_bad, bad, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(xyz);
+  cudaFree(bad);
+  if (err != cudaSuccess) return fail(DGB_ERR_CUDA, std::string("subcell tables: ") + cudaGetErrorString(err));
+  if (h_bad)
+    return fail(DGB_ERR_ARGUMENT, "subcell Gram matrix of element " + std::to_string(h_bad - 1) +
+                                      " is not positive definite");
+  C.P = O.P;
+  C.R = O.R;
+  C.vol = O.vol;
+  C.cen = O.cen;
+  C.in_n = O.in_n;
+  C.in_a = O.in_a;
+  C.bd_n = O.bd_n;
+  C.bd_a = O.bd_a;
+  p->sub_block_set[b] = true;
+  return DGB_OK;
+}
+
+int dgb_plan_match_subcell_faces(dgb_plan* p, int ft, const int32_t* osub, const int32_t* ncand) {
+  if (!p || ft < 0 || ft > 1) return fail(DGB_ERR_ARGUMENT, "bad subcell face type");
+  if (!p->face_present[ft]) return fail(DGB_ERR_ARGUMENT, "the plan has no faces of this type");
+  const FaceDev& fd = p->dev.face[ft];
+  const size_t F = fd.F;
+  if (F && (!osub || !ncand)) return fail(DGB_ERR_ARGUMENT, "null subface table");
+  SubcellCentres C;
+  for (int b = 0; b < DGB_MAX_BLOCKS; ++b) {
+    C.c[b] = b < p->dev.nblocks ? p->sub_bdc[b] : nullptr;
+    C.NB[b] = b < p->dev.nblocks ? p->mood.blk[b].NB : 0;
+  }
+  // the host tables index the blocks' boundary subfaces: check them and the blocks they need
+  std::vector<int32_t> ob(F), nb(F);
+  if (F) {
+    CK(cudaMemcpy(ob.data(), fd.ob, F * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(nb.data(), fd.nb, F * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  }
+  for (size_t f = 0; f < F; ++f) {
+    if (nb[f] < 0) continue;
+    for (int side = 0; side < 2; ++side) {
+      const int blk = side ? nb[f] : ob[f];
+      if (blk < 0 || blk >= p->dev.nblocks || !p->sub_block_set[blk] || !p->sub_bdc[blk])
+        return fail(DGB_ERR_ARGUMENT, "build the subcell tables of both sides' blocks first");
+      const int32_t* ids = (side ? ncand : osub) + f * kSub;
+      for (int k = 0; k < kSub; ++k)
+        if (ids[k] < 0 || ids[k] >= C.NB[blk]) return fail(DGB_ERR_ARGUMENT, "boundary subface out of range");
+    }
+  }
+  int rc;
+  const int32_t* d_osub = nullptr;
+  const int32_t* d_cand = nullptr;
+  if ((rc = upload(p, osub, F * kSub, &d_osub))) return rc;
+  if ((rc = upload(p, ncand, F * kSub, &d_cand))) return rc;
+  int32_t* d_nsub = nullptr;
+  if (F) {
+    CK(cudaMalloc(&d_nsub, F * kSub * sizeof(int32_t)));
+    p->allocations.push_back(d_nsub);
+  }
+  int* bad = nullptr;
+  int h_bad = 0;
+  CK(cudaMalloc(&bad, sizeof(int)));
+  cudaError_t err = cudaMemset(bad, 0, sizeof(int));
+  if (err == cudaSuccess && F) {
+    k_subcell_match<<<blocks_for((long)F, 256), 256>>>(fd, C, d_osub, d_cand, d_nsub, bad);
+    err = cudaGetLastError();
+  }
+  if (err == cudaSuccess) err = cudaMemcpy(&h_bad, bad, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(bad);
+  if (err != cudaSuccess) return fail(DGB_ERR_CUDA, std::string("subface matching: ") + cudaGetErrorString(err));
+  if (h_bad) return fail(DGB_ERR_ARGUMENT, "Nonconforming subfaces at face " + std::to_string(h_bad - 1));
+  SubcellFaceDev& SF = p->mood.face[ft];
+  SF.osub = d_osub;
+  SF.nsub = d_nsub;
+  p->sub_face_set[ft] = true;
+  return DGB_OK;
+}
+
 int dgb_plan_set_subcell_faces(dgb_plan* p, int ft, const int32_t* osub, const int32_t* nsub) {
   if (!p || ft < 0 || ft > 1) return fail(DGB_ERR_ARGUMENT, "bad subcell face type");
   SubcellFaceDev& SF = p->mood.face[ft];
@@ -1629,6 +1769,10 @@ int dgb_plan_enable_mood(dgb_plan* p) {
     p->allocations.push_back(a);
     CK(cudaMemset(a, 0, F));
     p->mood.face[ft].active = static_cast<uint8_t*>(a);
+  }
+  for (double*& d : p->sub_bdc) {    // the boundary subface centres were only needed for matching
+    cudaFree(d);
+    d = nullptr;
   }
   p->mood_ready = true;
   return DGB_OK;

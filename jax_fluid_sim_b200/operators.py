@@ -136,12 +136,20 @@ class NativePlan:
         self.fused = True          # the plan's default form of the hexahedron right-hand side
         self._pushed = self._snapshot()
 
-    def enable_mood(self, coupling="reference"):
-        """Upload the MOOD subcell tables once (hybrid/subcell.py:442-471)."""
+    def enable_mood(self, coupling="reference", tables="device"):
+        """Set up the MOOD subcell tables once (hybrid/subcell.py:442-471).  ``tables``: "device"
+        builds them on the GPU from the reference subdivision and the geometry nodes
+        (``dgb_plan_build_subcells``, ``dgb_plan_match_subcell_faces``); "host" uploads the
+        host-built ``SubcellPlan`` (the construction the device build is tested against)."""
         if getattr(self, "mood_coupling", None) == coupling:
             return
         if getattr(self, "mood_coupling", None) is not None:
             raise ValueError("the subcell coupling of a plan is fixed once chosen")
+        if tables not in ("device", "host"):
+            raise ValueError('tables must be "device" or "host"')
+        if tables == "device":
+            self._build_mood_tables(coupling)
+            return
         from .subcell import SubcellPlan
         L = N.lib()
         cache = self.plan.__dict__.setdefault("_subcell_plans", {})     # shared by plans of one mesh
@@ -176,6 +184,38 @@ class NativePlan:
         N.check(L.dgb_plan_enable_mood(self.handle))
         self.mood_coupling = coupling
         self.subcell_plan = sp
+
+    def _build_mood_tables(self, coupling):
+        from .subcell import ReferenceSubcells, device_reference, subface_tables
+        L = N.lib()
+        mesh = self.plan.mesh
+        refs = {b.element_type: ReferenceSubcells(b.element_type) for b in mesh.element_blocks}
+        for b, (bp, block) in enumerate(zip(self.plan.blocks, mesh.element_blocks)):
+            rs = refs[bp.etype]
+            t, xyz = device_reference(mesh, block, self.plan.degree, rs)
+            gather, scatter = rs.coupling_indices(coupling)
+            dbl = {k: N.as_f64(t[k]) for k in ("rule_weights", "point_basis", "point_geometry_grad",
+                                               "vertex_geometry", "boundary_basis")}
+            ints = dict(cells=t["cells"], internal_faces=t["internal_faces"], boundary_faces=t["boundary_faces"],
+                        internal_owner=rs.internal_owner, internal_neighbor=rs.internal_neighbor,
+                        boundary_owner=rs.boundary_owner, csr_ptr=rs.csr_ptr, csr_face=rs.csr_face,
+                        gather=gather, scatter=scatter)
+            ints = {k: N.as_i32(v) for k, v in ints.items()}
+            d = N.SubcellReference(num_subcells=rs.count, num_points=t["rule_weights"].shape[1],
+                                   num_geometry_nodes=xyz.shape[1], num_vertices=len(rs.vertices),
+                                   cell_size=rs.cells.shape[1], num_internal=len(rs.internal_faces),
+                                   num_boundary=len(rs.boundary_faces))
+            for k, a in dbl.items():
+                setattr(d, k, N.dptr(a))
+            for k, a in ints.items():
+                setattr(d, k, N.dptr(a, ctypes.c_int32))
+            N.check(L.dgb_plan_build_subcells(self.handle, b, ctypes.byref(d), N.dptr(N.as_f64(xyz))))
+        for ftype, (osub, ncand) in subface_tables(mesh, refs).items():
+            osub, ncand = N.as_i32(osub), N.as_i32(ncand)
+            N.check(L.dgb_plan_match_subcell_faces(self.handle, FACE_TYPE_ID[ftype], N.dptr(osub, ctypes.c_int32),
+                                                   N.dptr(ncand, ctypes.c_int32)))
+        N.check(L.dgb_plan_enable_mood(self.handle))
+        self.mood_coupling = coupling
 
     def set_tensor_cores(self, enable=True):
         """Run the inviscid volume integrals of the eligible dense blocks (prisms, tetrahedra up to

@@ -319,13 +319,32 @@ def hex_affine_data(plan: Plan, tol=1.0e-10):
     same at every volume point to ``tol`` relative.  Returns (affine uint8[E], coef[E] = sliver
     scale / det J, jinv[E][9], det[E]) in the layout of dgb_plan_set_hex_affine; for those
     elements the inverse mass matrix is coef * (m1i (x) m1i (x) m1i)."""
+    cached = plan.__dict__.get("_hex_affine")
+    if cached is not None and cached[0] == tol:
+        return cached[1]
     bp = plan.blocks[0]
     J = bp.jinv.reshape(bp.E, bp.Nq, 9)
-    dev = np.abs(J - J[:, :1]).max(axis=(1, 2)) / np.maximum(np.abs(J).max(axis=(1, 2)), 1e-300)
-    affine = (dev <= tol).astype(np.uint8)
+    affine, mean = _affine_test(J, tol)
     det = bp.volume.astype(np.float64)              # the reference hexahedron [0, 1]^3 has volume 1
     coef = np.minimum(1.0, bp.volume / 1.0e-4) / det
-    return affine, coef, np.ascontiguousarray(J.mean(axis=1)), det
+    out = affine, coef, mean, det
+    plan._hex_affine = (tol, out)                   # shared by the plans of both precisions
+    return out
+
+
+def _affine_test(J, tol, chunk=512):
+    """Per element of J (E, Nq, 9): whether every point's inverse Jacobian equals the first one's to
+    ``tol`` relative to the largest entry, and the mean over the points; in chunks of elements
+    that stay in the host caches."""
+    E = J.shape[0]
+    affine = np.empty(E, np.uint8)
+    mean = np.empty((E, 9))
+    for a in range(0, E, chunk):
+        Jc = J[a:a + chunk]
+        dev = np.abs(Jc - Jc[:, :1]).max(axis=(1, 2)) / np.maximum(np.abs(Jc).max(axis=(1, 2)), 1e-300)
+        affine[a:a + chunk] = dev <= tol
+        mean[a:a + chunk] = Jc.mean(axis=1)
+    return affine, mean
 
 
 def block_affine_data(bp, tol=1.0e-10):
@@ -335,10 +354,9 @@ def block_affine_data(bp, tol=1.0e-10):
     the layout of dgb_plan_set_block_affine.  For those elements w_q |det J| = w_q * det and the
     inverse mass matrix (hybrid/geometry.py:181-192) is coef * inv(B^T diag(w) B)."""
     J = bp.jinv.reshape(bp.E, bp.Nq, 9)
-    dev = np.abs(J - J[:, :1]).max(axis=(1, 2)) / np.maximum(np.abs(J).max(axis=(1, 2)), 1e-300)
-    affine = (dev <= tol).astype(np.uint8)
+    affine, mean = _affine_test(J, tol)
     w = np.asarray(bp.ref.weights, np.float64)
     det = bp.volume / w.sum()
     coef = np.minimum(1.0, bp.volume / 1.0e-4) / det
     mref = np.einsum("q,qi,qj->ij", w, bp.ref.B, bp.ref.B)
-    return affine, coef, np.ascontiguousarray(J.mean(axis=1)), det, w, np.linalg.inv(mref)
+    return affine, coef, mean, det, w, np.linalg.inv(mref)

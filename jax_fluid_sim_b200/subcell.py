@@ -244,8 +244,56 @@ def _face_metrics(pv, cen, faces, owners, neighbors):
     return N.subcell_face_metrics(pv, cen, faces, owners, neighbors)
 
 
+def _padded_faces(faces):
+    out = np.full((len(faces), 4), -1, np.int32)
+    for k, f in enumerate(faces):
+        out[k, :len(f)] = f
+    return out
+
+
+def device_reference(mesh, block, degree, rs):
+    """Reference tables from which the device builds a block's subcell tables
+    (``dgb_plan_build_subcells``): the subcells' P2 rule (weights times each subcell's reference
+    volume factor), the DG basis and the geometry-basis gradients at the mapped points, the
+    geometry basis at the subcell vertices, the subcell vertex lists and the padded subface
+    vertex lists; plus the block's geometry-map nodes (E, ng, 3)."""
+    ref = RefElement(block.element_type, degree)
+    geo1, xyz_all = mesh.geometry(block)
+    mp, rw = _subcell_rule(rs)
+    flat = mp.reshape(-1, 3)
+    S, Qs = mp.shape[0], mp.shape[1]
+    tables = dict(rule_weights=rw, point_basis=ref.basis(flat).reshape(S, Qs, ref.np),
+                  point_geometry_grad=geo1.basis_gradients(flat), vertex_geometry=geo1.basis(rs.vertices),
+                  cells=rs.cells, internal_faces=_padded_faces(rs.internal_faces),
+                  boundary_faces=_padded_faces(rs.boundary_faces), boundary_basis=ref.basis(rs.boundary_reference_centers))
+    return tables, np.ascontiguousarray(xyz_all, np.float64)
+
+
+def subface_tables(mesh, refs):
+    """Per face type: the owner's 16 boundary subfaces on the parent face (osub) and the
+    neighbour's 16 on its side of it in reference order (ncand, -1 on boundary faces), which the
+    device matches to the owner's by centre (``dgb_plan_match_subcell_faces``)."""
+    out = {}
+    for ftype, fb in mesh.face_blocks.items():
+        F = len(fb.nodes)
+        osub = np.zeros((F, 16), np.int32)
+        ncand = np.full((F, 16), -1, np.int32)
+        for b, block in enumerate(mesh.element_blocks):
+            rs = refs[block.element_type]
+            for lf in range(len(LOCAL_FACES[block.element_type])):
+                ids = np.flatnonzero(rs.boundary_parent == lf).astype(np.int32)
+                if len(ids) != 16:
+                    continue
+                osub[(fb.owner_block == b) & (fb.owner_face == lf)] = ids
+                ncand[(fb.neighbor_block == b) & (fb.neighbor_face == lf)] = ids
+        out[ftype] = (osub, ncand)
+    return out
+
+
 class SubcellPlan:
-    """Subcell tables of a whole mesh plus the per-face subface lists of both sides."""
+    """Subcell tables of a whole mesh plus the per-face subface lists of both sides, built on the
+    host (numpy, the native metrics and the GPU Gram inverses): the construction the device build
+    is tested against."""
 
     def __init__(self, mesh, degree, coupling="reference"):
         self.coupling = coupling
