@@ -148,6 +148,14 @@ int dgb_map_metrics(const double* nodes, const int32_t* index, int count, int nu
                     int num_points, const double* weights, const double* tangents, const double* orientation,
                     double* jacobian, double* det, double* inv_jacobian, double* wdet, double* normals,
                     double* area_weights);
+
+/* (set-up, host threads, no GPU) Affine test of a block's per-point inverse Jacobians
+ * jinv [count][num_points][9] (the isoparametric map is affine when J^-1 is the same at every
+ * point): affine[e] = 1 when every entry equals the first point's to tol relative to the
+ * element's largest |entry|; mean [count][9] the mean over the points.  Used to give affine
+ * elements constant metrics and a tensor-product M^-1 (hybrid/geometry.py:181-192 forms the same
+ * matrices by quadrature). */
+int dgb_affine_test(const double* jinv, int count, int num_points, double tol, uint8_t* affine, double* mean);
 /* Host-side subcell face metrics for the MOOD subcell plan (no GPU; hybrid/subcell.py:336-360).
  * For count elements with the physical subcell vertices vertices[count][num_vertices][3] and subcell
  * centres centers[count][num_subcells][3]: each face f of faces[num_faces][4] (face_sizes[f] = 3 or

@@ -140,6 +140,7 @@ def lib():
             "dgb_spd_inverse": [c_void_p, c_int, c_int, c_void_p, c_void_p],
             "dgb_subcell_face_metrics": [P_double, c_int, c_int, P_int32, P_int32, c_int, P_double, c_int, P_int32,
                                          P_int32, P_double, P_double, P_double],
+            "dgb_affine_test": [P_double, c_int, c_int, c_double, ctypes.POINTER(ctypes.c_uint8), P_double],
             "dgb_map_metrics": [P_double, P_int32, c_int, c_int, P_double, c_int, P_double, P_double, P_double,
                                 P_double, P_double, P_double, P_double, P_double, P_double],
             "dgb_plan_destroy": [c_void_p],
@@ -194,6 +195,17 @@ def dptr(a, ctype=ctypes.c_double):
     """Pointer to a C-contiguous numpy array (the caller keeps the array alive)."""
     assert a.flags["C_CONTIGUOUS"]
     return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def affine_test(J, tol):
+    """(affine uint8[E], mean[E][9]) of per-point inverse Jacobians J (E, Nq, 9) on host threads
+    (``dgb_affine_test``)."""
+    J = as_f64(J)
+    E = J.shape[0]
+    affine = np.empty(E, np.uint8)
+    mean = np.empty((E, 9))
+    check(lib().dgb_affine_test(dptr(J), E, J.shape[1], float(tol), dptr(affine, ctypes.c_uint8), dptr(mean)))
+    return affine, mean
 
 
 def as_f64(a):

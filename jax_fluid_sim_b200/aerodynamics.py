@@ -67,8 +67,10 @@ def face_points(plan):
                 continue
             geo, xyz_b = plan.mesh.geometry(block)
             xyz = xyz_b[fp.owner_local[sel]]                                             # (f, n, 3)
-            N1 = geo.basis(fp.own_pts[sel].reshape(-1, 3))
-            pts[sel] = np.einsum("fqk,fkd->fqd", N1.reshape(len(sel), fp.nq, -1), xyz)
+            # the owner's reference face points are those of its trace code
+            ref_pts = np.stack(plan.codes[(block.element_type, ftype)])                  # (codes, nq, 3)
+            N1 = np.stack([geo.basis(r) for r in ref_pts])                               # (codes, nq, n)
+            pts[sel] = np.einsum("fqk,fkd->fqd", N1[fp.ocode[sel]], xyz)
         out[ftype] = pts
     return out
 

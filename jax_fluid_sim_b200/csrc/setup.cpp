@@ -170,3 +170,29 @@ extern "C" int dgb_subcell_face_metrics(const double* vertices, int count, int n
   });
   return DGB_OK;
 }
+
+// Affine test of a block's per-point inverse Jacobians jinv [count][num_points][9]: an element is
+// affine when every point's entries equal the first point's to tol relative to the element's
+// largest |entry|; mean[count][9] receives the mean over the points (summed in point order).
+extern "C" int dgb_affine_test(const double* jinv, int count, int num_points, double tol, uint8_t* affine,
+                               double* mean) {
+  if (count < 0 || num_points < 1 || !jinv || !affine || !mean)
+    return dgb::set_error(DGB_ERR_ARGUMENT, "bad affine-test argument");
+  const int Q = num_points;
+  parallel_ranges(count, [=](int lo, int hi) {
+    for (int e = lo; e < hi; ++e) {
+      const double* J = jinv + (size_t)e * Q * 9;
+      double dev = 0.0, big = 0.0, s[9] = {};
+      for (int q = 0; q < Q; ++q)
+        for (int k = 0; k < 9; ++k) {
+          const double v = J[q * 9 + k];
+          dev = std::max(dev, std::fabs(v - J[k]));
+          big = std::max(big, std::fabs(v));
+          s[k] += v;
+        }
+      affine[e] = dev / std::max(big, 1e-300) <= tol ? 1 : 0;
+      for (int k = 0; k < 9; ++k) mean[(size_t)e * 9 + k] = s[k] / Q;
+    }
+  });
+  return DGB_OK;
+}

@@ -135,9 +135,14 @@ class HybridMesh:
         """(geometry reference element, node coordinates (E, n, 3)) of a block: the second-order
         map of curved cells, the first-order map otherwise (hybrid/geometry.py:102-110)."""
         from .reference import RefElement
-        if block.geometry_connectivity is not None:
-            return RefElement(block.element_type, 2), self.points[block.geometry_connectivity]
-        return RefElement(block.element_type, 1), self.points[block.connectivity]
+        cache = self.__dict__.setdefault("_geometry", {})
+        key = id(block)
+        if key not in cache:
+            if block.geometry_connectivity is not None:
+                cache[key] = (block, RefElement(block.element_type, 2), self.points[block.geometry_connectivity])
+            else:
+                cache[key] = (block, RefElement(block.element_type, 1), self.points[block.connectivity])
+        return cache[key][1], cache[key][2]
 
     def _boundary_tags(self, source):
         keys, tags = [], []

@@ -77,7 +77,11 @@ class Plan:
         p.E, p.Np, p.Nq = len(block.connectivity), ref.np, ref.nq
         p.nlf = len(LOCAL_FACES[block.element_type])
         p.jinv, p.wdet, p.volume = jinv, wdet, vol
-        p.node_xyz = np.einsum("qi,eid->eqd", geo.basis(ref.nodes), xyz)
+        # one matrix product over all elements: (Np x ng) @ (ng x 3E)
+        G = geo.basis(ref.nodes)
+        p.node_xyz = np.ascontiguousarray(
+            (G @ np.ascontiguousarray(xyz.transpose(1, 0, 2)).reshape(xyz.shape[1], -1))
+            .reshape(G.shape[0], xyz.shape[0], 3).transpose(1, 0, 2))
         p.affine = bool(np.all(np.ptp(det, axis=1) <= 1e-13 * np.abs(det).max(axis=1)))
         return p
 
@@ -100,8 +104,6 @@ class Plan:
         fp.owner_block, fp.owner_local = fb.owner_block.copy(), fb.owner_local.copy()
         fp.nbr_block, fp.nbr_local = fb.neighbor_block.copy(), fb.neighbor_local.copy()
         fp.tags = fb.boundary_tags.copy()
-        own_pts = np.empty((F, nq, 3))
-        nbr_pts = np.full((F, nq, 3), np.nan)
         ocode = np.empty(F, np.int32)
         ncode = np.full(F, -1, np.int32)
         normals = np.empty((F, nq, 3))
@@ -118,7 +120,6 @@ class Plan:
                     continue
                 corners = CORNERS[block.element_type][list(loc)]
                 pts = shapes @ corners
-                own_pts[sel] = pts
                 ocode[sel] = self._code(block.element_type, ftype, pts)
                 if ftype == "triangle":
                     tu = np.broadcast_to(corners[1] - corners[0], pts.shape)
@@ -142,22 +143,30 @@ class Plan:
             onodes = canon[fb.nodes[internal]]
             nnodes = canon[fb.neighbor_nodes[internal]]
             perm = np.argmax(onodes[:, :, None] == nnodes[:, None, :], axis=2)   # owner corner j -> nbr corner perm[j]
-            keys = np.concatenate([fb.neighbor_block[internal][:, None], fb.neighbor_face[internal][:, None],
-                                   perm], axis=1)
-            uniq, inverse = np.unique(keys, axis=0, return_inverse=True)
-            inverse = inverse.ravel()
-            for u, (b, lf, *pm) in enumerate(uniq.tolist()):
+            # (neighbour block, neighbour face, corner permutation) as one integer key: the same
+            # order as sorting the tuples
+            key = fb.neighbor_block[internal].astype(np.int64) * 8 + fb.neighbor_face[internal]
+            for j in range(k):
+                key = key * 4 + perm[:, j]
+            ukey, inverse = np.unique(key, return_inverse=True)
+            uniq = []
+            for u in ukey.tolist():
+                pm = []
+                for _ in range(k):
+                    pm.append(u % 4)
+                    u //= 4
+                uniq.append((u // 8, u % 8, *pm[::-1]))
+            for u, (b, lf, *pm) in enumerate(uniq):
                 block = mesh.element_blocks[b]
                 etype = block.element_type
                 corners = CORNERS[etype][list(LOCAL_FACES[etype][lf])][list(pm)]
                 pts = shapes @ corners
                 faces = internal[inverse == u]
-                nbr_pts[faces] = pts
                 ncode[faces] = self._code(etype, ftype, pts)
                 geo, xyz_b = mesh.geometry(block)
                 jinv_side[faces, 1] = N.map_metrics(xyz_b, geo.basis_gradients(pts), index=fb.neighbor_local[faces],
                                                     outputs=("inv_jacobian",))[0]
-        fp.own_pts, fp.nbr_pts, fp.ocode, fp.ncode = own_pts, nbr_pts, ocode, ncode
+        fp.ocode, fp.ncode = ocode, ncode
         fp.normals, fp.weights, fp.jinv_side = normals, weights, jinv_side
         return fp
 
@@ -332,19 +341,10 @@ def hex_affine_data(plan: Plan, tol=1.0e-10):
     return out
 
 
-def _affine_test(J, tol, chunk=512):
+def _affine_test(J, tol):
     """Per element of J (E, Nq, 9): whether every point's inverse Jacobian equals the first one's to
-    ``tol`` relative to the largest entry, and the mean over the points; in chunks of elements
-    that stay in the host caches."""
-    E = J.shape[0]
-    affine = np.empty(E, np.uint8)
-    mean = np.empty((E, 9))
-    for a in range(0, E, chunk):
-        Jc = J[a:a + chunk]
-        dev = np.abs(Jc - Jc[:, :1]).max(axis=(1, 2)) / np.maximum(np.abs(Jc).max(axis=(1, 2)), 1e-300)
-        affine[a:a + chunk] = dev <= tol
-        mean[a:a + chunk] = Jc.mean(axis=1)
-    return affine, mean
+    ``tol`` relative to the largest entry, and the mean over the points (host threads)."""
+    return N.affine_test(J, tol)
 
 
 def block_affine_data(bp, tol=1.0e-10):

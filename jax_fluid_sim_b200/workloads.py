@@ -616,6 +616,7 @@ def run_ensemble(num_cases=64, elements=(5000, 60000), steps=10, warmup=2, seed=
     same dt and step count (checked SSP-RK3 with the MOOD limiter, or with ``limiter="positivity"``
     the positivity limiter alone, which needs no subcell tables).  Returns per group and in total
     the DOF-updates/s of both, timed with CUDA events after ``warmup`` untimed steps."""
+    import gc
     import torch
     from .ensemble import HybridEnsemble
     from .limiter import HybridMOODSubcellLimiter, HybridPositivityLimiter
@@ -656,6 +657,7 @@ def run_ensemble(num_cases=64, elements=(5000, 60000), steps=10, warmup=2, seed=
             Uc = solver.uniform_state_blocks(far[0], far[1:4], far[4])
             t_seq += timed_steps(integrator(op), Uc, dt, bc)
             del solver, op, Uc
+            gc.collect()                  # free the case's device plan before the next one
         dofs = ens.dofs
         groups.append(dict(degree=degree, cases=len(members), limiter=limiter, precision=precision,
                            elements=sum(bp.E for bp in ens.operator.plan.blocks),
@@ -664,7 +666,10 @@ def run_ensemble(num_cases=64, elements=(5000, 60000), steps=10, warmup=2, seed=
         total["dofs"] += dofs
         total["ensemble_seconds"] += t_ens
         total["sequential_seconds"] += t_seq
+        # the group's plan (tens of GB) must be gone before the next group's is built: the
+        # integrator's captured graph and the plan refer to each other, so collect the cycle
         del ens, U, it
+        gc.collect()
         torch.cuda.empty_cache()
     total.update(steps=steps, ensemble_dof_updates_per_s=total["dofs"] * steps / total["ensemble_seconds"],
                  sequential_dof_updates_per_s=total["dofs"] * steps / total["sequential_seconds"],
