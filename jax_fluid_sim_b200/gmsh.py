@@ -1,4 +1,4 @@
-"""Gmsh mesh files (MSH 2.2 and 4.1, ASCII) into a ``MeshSource``.
+"""Gmsh mesh files (MSH 2.2 ASCII or binary, MSH 4.1 ASCII) into a ``MeshSource``.
 
 The reference reads its meshes with meshio (hybrid/mesh.py:182-236, mesh_loader.py).  This
 reader keeps what the hybrid path uses: node coordinates, the physical names and, per cell
@@ -174,16 +174,104 @@ def _read_v4(sec, field):
     return np.concatenate(xyz_all), index, records
 
 
+def _node_count(etype):
+    if etype in _CURVED:
+        return {"tetra10": 10, "hexahedron27": 27, "wedge18": 18}[_CURVED[etype]]
+    if etype in _TYPES:
+        return _TYPES[etype][2]
+    raise ValueError(f"unsupported Gmsh element type {etype}")
+
+
+def _read_v2_binary(data):
+    """MSH 2.2 binary (Gmsh reference manual, legacy MSH 2 format): the section headers, the
+    physical names and the counts are text lines; after the format line one int 1 gives the byte
+    order; the nodes are records (int id, 3 doubles); the elements come in blocks, each a header
+    (int type, int count, int number of tags) followed by count records (int id, the tags, the
+    node ids)."""
+    pos = 0
+
+    def line():
+        nonlocal pos
+        end = data.index(b"\n", pos)
+        out = data[pos:end].decode("ascii", "replace").strip()
+        pos = end + 1
+        return out
+
+    def skip_to(tag):
+        nonlocal pos
+        pos = data.index(tag, pos) + len(tag)
+        if pos < len(data) and data[pos:pos + 1] == b"\r":
+            pos += 1
+        if pos < len(data) and data[pos:pos + 1] == b"\n":
+            pos += 1
+
+    order, field, nodes, records = "<", {}, None, []
+    while pos < len(data):
+        head = line()
+        if not head.startswith("$"):
+            continue
+        name = head[1:]
+        if name == "MeshFormat":
+            version, binary, dsize = line().split()[:3]
+            if int(dsize) != 8:
+                raise NotImplementedError("binary MSH files need 8-byte reals")
+            one = data[pos:pos + 4]
+            order = "<" if np.frombuffer(one, "<i4")[0] == 1 else ">"
+            pos += 4
+            skip_to(b"$EndMeshFormat")
+        elif name == "PhysicalNames":
+            count = int(line())
+            field = _physical_names([str(count)] + [line() for _ in range(count)])
+            skip_to(b"$EndPhysicalNames")
+        elif name == "Nodes":
+            count = int(line())
+            rec = np.dtype([("id", order + "i4"), ("xyz", order + "f8", (3,))])
+            nodes = np.frombuffer(data, rec, count, pos)
+            pos += count * rec.itemsize
+            skip_to(b"$EndNodes")
+        elif name == "Elements":
+            count = int(line())
+            seen, by_shape = 0, {}
+            while seen < count:
+                etype, num, ntags = (int(v) for v in np.frombuffer(data, order + "i4", 3, pos))
+                pos += 12
+                k = _node_count(etype)
+                block = np.frombuffer(data, order + "i4", num * (1 + ntags + k), pos).reshape(num, 1 + ntags + k)
+                pos += block.nbytes
+                phys = block[:, 1] if ntags > 0 else np.zeros(num, np.int32)
+                for p in np.unique(phys).tolist():
+                    by_shape.setdefault((etype, p), []).append(block[phys == p, 1 + ntags:])
+                seen += num
+            records = [(t, p, np.concatenate(n).astype(np.int64)) for (t, p), n in by_shape.items()]
+            skip_to(b"$EndElements")
+        else:
+            skip_to(b"$End" + name.encode())
+    if nodes is None:
+        raise ValueError("the mesh has no $Nodes section")
+    ids = nodes["id"].astype(np.int64)
+    index = np.full(ids.max() + 1, -1, np.int64)
+    index[ids] = np.arange(len(ids))
+    return np.ascontiguousarray(nodes["xyz"], np.float64), index, records, field
+
+
 def read_msh(path, periodic_map=None):
-    """Read a Gmsh MSH 2.2 or 4.1 ASCII file into a ``MeshSource`` (optionally with a periodic
-    point map for ``HybridMesh``)."""
-    lines = Path(path).read_text().splitlines()
+    """Read a Gmsh MSH 2.2 (ASCII or binary) or 4.1 ASCII file into a ``MeshSource`` (optionally
+    with a periodic point map for ``HybridMesh``)."""
+    data = Path(path).read_bytes()
+    if not data.lstrip().startswith(b"$MeshFormat"):
+        raise ValueError(f"{path} is not a Gmsh mesh")
+    fmt = data.split(b"\n", 2)[1].split()
+    if len(fmt) >= 2 and int(fmt[1]) != 0:
+        if not fmt[0].decode().startswith("2"):
+            raise NotImplementedError("binary MSH files are read in version 2.2 only; save 4.1 files as ASCII")
+        points, index, records, field = _read_v2_binary(data)
+        cells, phys = _assemble(points, index, records)
+        return MeshSource(points, cells, phys, field, periodic_map)
+    lines = data.decode("ascii", "replace").splitlines()
     sec = _sections(lines)
     if "MeshFormat" not in sec:
         raise ValueError(f"{path} is not a Gmsh mesh")
     version, binary = sec["MeshFormat"][0].split()[:2]
-    if int(binary) != 0:
-        raise NotImplementedError("binary MSH files are not supported; save as ASCII")
     field = _physical_names(sec.get("PhysicalNames"))
     if version.startswith("2"):
         points, index, records = _read_v2(sec, field)
@@ -195,11 +283,13 @@ def read_msh(path, periodic_map=None):
     return MeshSource(points, cells, phys, field, periodic_map)
 
 
-def write_msh22(path, source):
-    """Write a ``MeshSource`` as an MSH 2.2 ASCII file (first-order cells, and complete
+def write_msh22(path, source, binary=False):
+    """Write a ``MeshSource`` as an MSH 2.2 file, ASCII or binary (first-order cells, and complete
     second-order cells given in meshio's node order, written in Gmsh's)."""
     codes = {"triangle": 2, "quad": 3, "tetra": 4, "hexahedron": 5, "wedge": 6,
              "tetra10": 11, "hexahedron27": 12, "wedge18": 13}
+    if binary:
+        return _write_msh22_binary(path, source, codes)
     out = ["$MeshFormat", "2.2 0 8", "$EndMeshFormat", "$PhysicalNames", str(len(source.field_data))]
     for name, (tag, dim) in source.field_data.items():
         out.append(f'{dim} {tag} "{name}"')
@@ -218,6 +308,37 @@ def write_msh22(path, source):
             k += 1
     out.append("$EndElements")
     Path(path).write_text("\n".join(out) + "\n")
+
+
+def _write_msh22_binary(path, source, codes):
+    out = [b"$MeshFormat\n2.2 1 8\n", np.array([1], "<i4").tobytes(), b"\n$EndMeshFormat\n",
+           f"$PhysicalNames\n{len(source.field_data)}\n".encode()]
+    for name, (tag, dim) in source.field_data.items():
+        out.append(f'{dim} {tag} "{name}"\n'.encode())
+    pts = np.asarray(source.points, np.float64)
+    rec = np.zeros(len(pts), np.dtype([("id", "<i4"), ("xyz", "<f8", (3,))]))
+    rec["id"] = np.arange(1, len(pts) + 1)
+    rec["xyz"] = pts
+    out += [b"$EndPhysicalNames\n", f"$Nodes\n{len(pts)}\n".encode(), rec.tobytes(), b"\n$EndNodes\n",
+            f"$Elements\n{sum(len(c) for _, c in source.cells)}\n".encode()]
+    k = 1
+    for (ctype, conn), phys in zip(source.cells, source.physical):
+        conn = np.asarray(conn, np.int64)
+        if ctype in _GMSH_P2:
+            to_gmsh = np.empty(conn.shape[1], np.int64)
+            to_gmsh[gmsh_to_meshio(ctype)] = np.arange(conn.shape[1])
+            conn = conn[:, to_gmsh]
+        n = len(conn)
+        if n == 0:
+            continue
+        block = np.empty((n, 3 + conn.shape[1]), "<i4")
+        block[:, 0] = np.arange(k, k + n)
+        block[:, 1] = block[:, 2] = np.asarray(phys, np.int64)
+        block[:, 3:] = conn + 1
+        out += [np.array([codes[ctype], n, 2], "<i4").tobytes(), block.tobytes()]
+        k += n
+    out.append(b"\n$EndElements\n")
+    Path(path).write_bytes(b"".join(out))
 
 
 read_gmsh = read_msh     # the name HybridMesh(path) uses

@@ -1,6 +1,7 @@
-"""Gmsh MSH 2.2 / 4.1 ASCII reading: a written file reads back to the same mesh (points, cells,
-physical tags and names, hence the same face tables), hand-written 4.1 and second-order files
-parse, and complete second-order cells come back in meshio's node order."""
+"""Gmsh MSH 2.2 (ASCII and binary) / 4.1 ASCII reading: a written file reads back to the same mesh
+(points, cells, physical tags and names, hence the same face tables), hand-written 4.1 and
+second-order files parse, complete second-order cells come back in meshio's node order, and a
+binary file written by Gmsh itself parses."""
 
 import numpy as np
 import pytest
@@ -26,6 +27,48 @@ def test_msh22_round_trip(tmp_path, source):
     np.testing.assert_array_equal(back.points, source.points)
     assert back.field_data == source.field_data
     _same_faces(source, back)
+
+
+@pytest.mark.parametrize("source", [meshgen.mixed_block(jitter=0.1, seed=3), meshgen.smoke_mesh()])
+def test_msh22_binary_round_trip(tmp_path, source):
+    path = tmp_path / "m.msh"
+    gmsh.write_msh22(path, source, binary=True)
+    assert path.read_bytes().startswith(b"$MeshFormat\n2.2 1 8\n")
+    back = gmsh.read_msh(path)
+    np.testing.assert_array_equal(back.points, source.points)
+    assert back.field_data == source.field_data
+    # the reader groups cells by (type, physical tag), so compare each type's cells as a set
+    got = dict(back.cells)
+    for ctype, conn in source.cells:
+        np.testing.assert_array_equal(np.unique(got[ctype], axis=0), np.unique(conn, axis=0))
+    _same_faces(source, back)
+
+
+def test_msh22_binary_written_by_gmsh(tmp_path):
+    """A slice of the reference's binary mesh mesh/sr71_pure_hex.msh (tests/golden/make_gmsh_binary.py:
+    600 hexahedra, the 120 boundary quadrilaterals among their nodes, 1,902 nodes, records as Gmsh
+    wrote them): counts, names and tags, positive cell volumes, and the same mesh as its ASCII
+    rewrite."""
+    from pathlib import Path
+    from jax_fluid_sim_b200.mesh import _cell_geometry
+    src = gmsh.read_msh(Path(__file__).parent / "golden" / "gmsh_sr71_binary.msh")
+    assert len(src.points) == 1902
+    kinds = dict(src.cells)
+    assert len(kinds["hexahedron"]) == 600 and len(kinds["quad"]) == 120
+    assert {"inlet", "outlet", "walls", "airfoil_wall", "fluid"} <= set(src.field_data)
+    assert np.all(src.physical[0] == src.field_data["fluid"][0])
+    surface = {v[0] for v in src.field_data.values() if v[1] == 2}
+    assert set(np.unique(src.physical[1]).tolist()) <= surface
+    _, vol = _cell_geometry(np.asarray(src.points), "hexahedron", kinds["hexahedron"])
+    assert np.all(vol > 0.0)
+    path = tmp_path / "ascii.msh"
+    gmsh.write_msh22(path, src)
+    back = gmsh.read_msh(path)
+    np.testing.assert_array_equal(back.points, src.points)
+    for (ta, ca), (tb, cb), pa, pb in zip(src.cells, back.cells, src.physical, back.physical):
+        assert ta == tb
+        np.testing.assert_array_equal(ca, cb)
+        np.testing.assert_array_equal(pa, pb)
 
 
 def test_reference_shim_writer_reads_back(tmp_path):
