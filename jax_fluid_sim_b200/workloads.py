@@ -608,6 +608,12 @@ def _cylinder_case(case, gamma=1.4):
     return meshgen.cylinder_o_grid(case["n_theta"], case["n_radial"]), far, far[1] / case["reynolds"]
 
 
+# device bytes per element of a viscous hexahedron ensemble plan and its step buffers (measured
+# about 52 KB at P2 in float64 and 63 KB in mixed precision; P3 scales with the node count), with
+# room for the step's buffers
+ENSEMBLE_BYTES_PER_ELEMENT = {1: 40e3, 2: 80e3, 3: 170e3}
+
+
 def run_ensemble(num_cases=64, elements=(5000, 60000), steps=10, warmup=2, seed=0, precision="float64", cfl=0.3,
                  limiter="mood"):
     """The ensemble configuration: the cases of ``ensemble_cases`` grouped by degree, each group
@@ -641,14 +647,47 @@ def run_ensemble(num_cases=64, elements=(5000, 60000), steps=10, warmup=2, seed=
     for degree in sorted({c["degree"] for c in cases}):
         members = [c for c in cases if c["degree"] == degree]
         built = [_cylinder_case(c) for c in members]
-        free0 = torch.cuda.mem_get_info()[0]
-        ens = HybridEnsemble([b[0] for b in built], [b[1] for b in built], [b[2] for b in built],
-                             polynomial_degree=degree, precision=precision)
-        U = ens.freestream_states()
-        plan_gb = (free0 - torch.cuda.mem_get_info()[0]) / 1e9
-        it = integrator(ens.operator)
-        dt = it.stable_dt(U, ens.boundary)
-        t_ens = timed_steps(it, U, dt, ens.boundary)
+        # one ensemble per group when its plan fits the device, else consecutive sub-ensembles that
+        # do (device bytes per element of a viscous hexahedron plan at this degree, with margin)
+        budget = 0.7 * torch.cuda.mem_get_info()[0] / ENSEMBLE_BYTES_PER_ELEMENT[degree]
+        chunks, cur, size = [], [], 0
+        for b, c in zip(built, members):
+            n = c["n_theta"] * c["n_radial"]
+            if cur and size + n > budget:
+                chunks.append(cur)
+                cur, size = [], 0
+            cur.append(b)
+            size += n
+        chunks.append(cur)
+        # one dt for the whole group: the smallest stable dt of its sub-ensembles
+        ens_list, plan_gb = [], 0.0
+        dt = float("inf")
+        for part in chunks:
+            free0 = torch.cuda.mem_get_info()[0]
+            ens = HybridEnsemble([b[0] for b in part], [b[1] for b in part], [b[2] for b in part],
+                                 polynomial_degree=degree, precision=precision)
+            U = ens.freestream_states()
+            plan_gb = max(plan_gb, (free0 - torch.cuda.mem_get_info()[0]) / 1e9)
+            it = integrator(ens.operator)
+            dt = min(dt, it.stable_dt(U, ens.boundary))
+            if len(chunks) == 1:
+                ens_list.append((ens, U, it))
+            del ens, U, it
+            gc.collect()
+        t_ens, dofs = 0.0, 0
+        for part in chunks:
+            if len(chunks) == 1:
+                ens, U, it = ens_list.pop()
+            else:
+                ens = HybridEnsemble([b[0] for b in part], [b[1] for b in part], [b[2] for b in part],
+                                     polynomial_degree=degree, precision=precision)
+                U = ens.freestream_states()
+                it = integrator(ens.operator)
+            t_ens += timed_steps(it, U, dt, ens.boundary)
+            dofs += ens.dofs
+            del ens, U, it
+            gc.collect()
+            torch.cuda.empty_cache()
         t_seq, ok = 0.0, True
         for src, far, mu in built:
             solver = HybridCompressibleSolver(HybridMesh(src), polynomial_degree=degree, dynamic_viscosity=mu)
@@ -658,17 +697,13 @@ def run_ensemble(num_cases=64, elements=(5000, 60000), steps=10, warmup=2, seed=
             t_seq += timed_steps(integrator(op), Uc, dt, bc)
             del solver, op, Uc
             gc.collect()                  # free the case's device plan before the next one
-        dofs = ens.dofs
         groups.append(dict(degree=degree, cases=len(members), limiter=limiter, precision=precision,
-                           elements=sum(bp.E for bp in ens.operator.plan.blocks),
+                           elements=int(sum(c["n_theta"] * c["n_radial"] for c in members)), ensembles=len(chunks),
                            dofs=dofs, dt=dt, device_gb=round(plan_gb, 2), ensemble_dof_updates_per_s=dofs * steps / t_ens,
                            sequential_dof_updates_per_s=dofs * steps / t_seq, speedup=t_seq / t_ens))
         total["dofs"] += dofs
         total["ensemble_seconds"] += t_ens
         total["sequential_seconds"] += t_seq
-        # the group's plan (tens of GB) must be gone before the next group's is built: the
-        # integrator's captured graph and the plan refer to each other, so collect the cycle
-        del ens, U, it
         gc.collect()
         torch.cuda.empty_cache()
     total.update(steps=steps, ensemble_dof_updates_per_s=total["dofs"] * steps / total["ensemble_seconds"],
