@@ -373,6 +373,35 @@ int run_rhs_hex_fused(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cu
   return DGB_OK;
 }
 
+// The fused element kernel alone, split residuals, on the face buffers of the last right-hand side.
+template <int P, int NV, typename R>
+int run_hex_element_pass(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStream_t st) {
+  using LE = HexElemSmem<P, NV, true, R>;
+  const size_t sm_el = sizeof(R) * (size_t)LE::TOTAL;
+  int rc;
+  if ((rc = prepare(k_hex_element<P, NV, true, R>, sm_el))) return rc;
+  k_hex_element<P, NV, true, R><<<p->dev.blk[0].E, kThreads, sm_el, st>>>(p->dev, S, p->hex_tables, p->hex_codes, A);
+  CK(cudaGetLastError());
+  return DGB_OK;
+}
+
+// The viscous residual of the flagged elements only (p->vis), for the subcell scheme: the fused
+// element kernel with the inviscid terms skipped, on the face data of the stage's right-hand side.
+template <int NV>
+int run_viscous_flagged(dgb_plan* p, const StatePtrs& S, cudaStream_t st) {
+  FinalizeArgs V;
+  memset(&V, 0, sizeof(V));
+  V.out_vis[0] = p->vis[0];
+  V.skip_inviscid = p->flags[0];
+  V.only = p->flags[0];
+  const bool f32 = p->prm.precision == 1;
+  switch (p->dev.degree) {
+    case 1: return f32 ? run_hex_element_pass<1, NV, float>(p, S, V, st) : run_hex_element_pass<1, NV, double>(p, S, V, st);
+    case 2: return f32 ? run_hex_element_pass<2, NV, float>(p, S, V, st) : run_hex_element_pass<2, NV, double>(p, S, V, st);
+    default: return f32 ? run_hex_element_pass<3, NV, float>(p, S, V, st) : run_hex_element_pass<3, NV, double>(p, S, V, st);
+  }
+}
+
 template <int NV, bool SPLIT, typename R>
 int run_rhs_hex_deg(dgb_plan* p, const StatePtrs& S, const FinalizeArgs& A, cudaStream_t st, cudaEvent_t* ev) {
   if (p->fused) {
@@ -746,6 +775,10 @@ int run_step_mood(dgb_plan* p, const StatePtrs& U0, double dt, dgb_status* statu
   const StatePtrs* cur[3] = {&U0, &S1, &S2};
   const StatePtrs* dst[3] = {&S1, &S2, &U0};
   const FlagPtrs F = flag_ptrs(p->flags);
+  // fused hexahedron path with viscous terms: the stage's right-hand side is formed as one
+  // residual (one divergence pass per element), and the viscous residual that the subcell scheme
+  // needs is formed afterwards for the flagged elements only
+  const bool vis_after = p->hex && p->fused && P.viscous;
   int rc;
   for (int s = 0; s < 3; ++s) {
     FinalizeArgs A;
@@ -758,14 +791,18 @@ int run_step_mood(dgb_plan* p, const StatePtrs& U0, double dt, dgb_status* statu
       A.base[b] = U0.b[b];
       A.dst[b] = p->unl[b];
       A.euler[b] = p->eul[b];
-      A.out_vis[b] = p->vis[b];
+      A.out_vis[b] = vis_after ? nullptr : p->vis[b];
     }
     // the predictor reads the stage's base state: it decides before the high-order update, and
-    // in learned mode its elements skip the inviscid part of that update (fused hexahedron path)
+    // in learned mode its elements skip that update (fused hexahedron path): the subcell scheme
+    // replaces it and needs only their viscous residual
     if (p->pred_mode && (rc = run_predict<NV>(p, *cur[s], st))) return rc;
-    if (p->pred_mode == 1 && p->hex && p->fused) A.skip_inviscid = p->pred_flags[0];
+    if (p->pred_mode == 1 && p->hex && p->fused) {
+      if (vis_after) A.skip = p->pred_flags[0]; else A.skip_inviscid = p->pred_flags[0];
+    }
     if ((rc = run_rhs<NV>(p, *cur[s], A, st))) return rc;
     if ((rc = run_troubled<NV>(p, UNL, nullptr, p->flags, st, true))) return rc;
+    if (vis_after && (rc = run_viscous_flagged<NV>(p, *cur[s], st))) return rc;
     if ((rc = run_subcell<NV>(p, *cur[s], p->eul, p->vis, dt, F, p->rec, st))) return rc;
     if ((rc = run_positivity<NV>(p, REC, st))) return rc;
     for (int b = 0; b < P.nblocks; ++b) {

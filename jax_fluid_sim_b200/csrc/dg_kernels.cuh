@@ -662,6 +662,10 @@ struct FinalizeArgs {
   // the subcell scheme, which uses only their viscous residual); null: none.  Read by the fused
   // hexahedron element kernel.
   const uint8_t* skip_inviscid;
+  // element selection of the fused hexahedron element kernel (null: every element): only the
+  // elements flagged in `only`, none of those flagged in `skip`
+  const uint8_t* only;
+  const uint8_t* skip;
 };
 
 // Shared memory per element (in R values) of k_finalize: face partials [nlf][Np][NV] and the

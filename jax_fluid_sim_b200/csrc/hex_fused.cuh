@@ -386,6 +386,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
   const BlockDev& B = P_.blk[b];
   const FaceDev& fd = P_.face[1];
   const int e = blockIdx.x;
+  if ((A.only && !A.only[e]) || (A.skip && A.skip[e])) return;     // uniform across the CTA
   const CaseView cv = case_view(P_.ph, B.ecase, e);
   load_tables<P>(tables, tb);
   const double* Ug = S.b[b] + (size_t)e * N3 * NV;
