@@ -258,7 +258,7 @@ def run_ours(args):
     dt = integ0.stable_dt(U0, bc)                   # one fixed dt for every run (same trajectory)
     # execution form of the hexahedron right-hand side per precision (fused three-launch or
     # six-launch), the faster on the start state
-    forms = {m: ops[m].autotune_form(U0, bc) for m in precisions}
+    forms = {m: ops[m].autotune_form(U0, bc, mood=args.limiter == "mood") for m in precisions}
 
     # training data: plain steps from the start, labelled by the a-posteriori detector
     predictor, train = None, None

@@ -379,6 +379,11 @@ int dgb_subcell_recompute(dgb_plan* plan, const dgb_state* base, const dgb_state
  * lift is part of the volume stage and its entry is 0).  Synchronises the stream. */
 enum { DGB_RHS_STAGES = 6 };
 int dgb_rhs_profile(dgb_plan* plan, const dgb_state* U, float* ms_out, void* stream);
+/* The same for the right-hand side as an SSP-RK stage forms it (the stage update fused into
+ * the last kernel, with dt = 0 into plan scratch), split = 1 with the viscous residual kept
+ * apart as the MOOD step of the six-launch form needs it, split = 0 as one residual (the
+ * MOOD step of the fused form, and every step without MOOD). */
+int dgb_rhs_profile_stage(dgb_plan* plan, const dgb_state* U, int split, float* ms_out, void* stream);
 
 /* Allocation-free CFL time step for one element block.  No counterpart in the reference.
  *
@@ -483,7 +488,8 @@ int dgb_mlp_train_step(float* weights, float* grad, float* adam_m, float* adam_v
                        const float* norm, const float* features, const uint8_t* labels, const int* index,
                        int batch, float pos_weight, float lr, int step, float* loss, void* stream);
 /* Use the predictor inside dgb_ssprk3_step's MOOD stages: mode 0 off, 1 learned (predicted
- * elements skip the a-posteriori test and go to the subcell scheme), 2 evaluate (every element
+ * elements skip the a-posteriori test and go to the subcell scheme; on the fused hexahedron
+ * path they also skip their high-order update), 2 evaluate (every element
  * is tested and the step is the plain one; the prediction is only counted).  The weight and
  * norm arrays must outlive their use. */
 int dgb_plan_set_predictor(dgb_plan* plan, const void* weights_f16, const float* norm, float threshold, int mode);

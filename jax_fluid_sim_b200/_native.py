@@ -153,6 +153,8 @@ def lib():
             "dgb_ssprk3_step": [c_void_p, ctypes.POINTER(State), c_double, c_void_p, c_void_p],
             "dgb_ssprk3_step_graph": [c_void_p, ctypes.POINTER(State), c_double, c_void_p, c_void_p],
             "dgb_rhs_profile": [c_void_p, ctypes.POINTER(State), ctypes.POINTER(ctypes.c_float), c_void_p],
+            "dgb_rhs_profile_stage": [c_void_p, ctypes.POINTER(State), c_int, ctypes.POINTER(ctypes.c_float),
+                                      c_void_p],
             "dgb_plan_set_subcells": [c_void_p, c_int, ctypes.POINTER(SubcellBlockDesc)],
             "dgb_plan_set_subcell_faces": [c_void_p, c_int, P_int32, P_int32],
             "dgb_plan_build_subcells": [c_void_p, c_int, ctypes.POINTER(SubcellReference), P_double],

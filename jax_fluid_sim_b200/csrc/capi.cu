@@ -1904,16 +1904,9 @@ int dgb_plan_predictor_counts(dgb_plan* p, int64_t* out, int reset) {
   return DGB_OK;
 }
 
-int dgb_rhs_profile(dgb_plan* p, const dgb_state* U, float* ms_out, void* stream) {
+namespace {
+int profile_rhs(dgb_plan* p, const dgb_state* U, const FinalizeArgs& A, float* ms_out, void* stream) {
   int rc;
-  if ((rc = check_ready(p)) || (rc = check_state(p, U, "U"))) return rc;
-  if (!ms_out) return fail(DGB_ERR_ARGUMENT, "ms_out is null");
-  FinalizeArgs A;
-  memset(&A, 0, sizeof(A));
-  for (int b = 0; b < DGB_MAX_BLOCKS; ++b) {
-    A.out_inv[b] = p->stage1[b];      // scratch outputs
-    A.out_vis[b] = p->stage2[b];
-  }
   cudaEvent_t ev[DGB_RHS_STAGES + 1];
   for (auto& e : ev) CK(cudaEventCreate(&e));
   const StatePtrs S = to_ptrs(U);
@@ -1925,6 +1918,36 @@ int dgb_rhs_profile(dgb_plan* p, const dgb_state* U, float* ms_out, void* stream
   }
   for (auto& e : ev) cudaEventDestroy(e);
   return rc;
+}
+}  // namespace
+
+int dgb_rhs_profile(dgb_plan* p, const dgb_state* U, float* ms_out, void* stream) {
+  int rc;
+  if ((rc = check_ready(p)) || (rc = check_state(p, U, "U"))) return rc;
+  if (!ms_out) return fail(DGB_ERR_ARGUMENT, "ms_out is null");
+  FinalizeArgs A;
+  memset(&A, 0, sizeof(A));
+  for (int b = 0; b < DGB_MAX_BLOCKS; ++b) {
+    A.out_inv[b] = p->stage1[b];      // scratch outputs
+    A.out_vis[b] = p->stage2[b];
+  }
+  return profile_rhs(p, U, A, ms_out, stream);
+}
+
+int dgb_rhs_profile_stage(dgb_plan* p, const dgb_state* U, int split, float* ms_out, void* stream) {
+  int rc;
+  if ((rc = check_ready(p)) || (rc = check_state(p, U, "U"))) return rc;
+  if (!ms_out) return fail(DGB_ERR_ARGUMENT, "ms_out is null");
+  FinalizeArgs A;
+  memset(&A, 0, sizeof(A));
+  A.stage = 1;
+  A.beta = 1.0;                       // dst = U + 0 * rhs: the stage update's arithmetic, dt = 0
+  for (int b = 0; b < DGB_MAX_BLOCKS; ++b) {
+    A.base[b] = U->block[b];
+    A.dst[b] = p->stage1[b];
+    A.out_vis[b] = split ? p->stage2[b] : nullptr;
+  }
+  return profile_rhs(p, U, A, ms_out, stream);
 }
 
 int dgb_stable_dt(dgb_plan* p, const dgb_state* U, double cfl, double* dt_out, void* stream) {

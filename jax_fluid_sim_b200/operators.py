@@ -356,10 +356,12 @@ class HybridEulerOperator:
                 out[kernel] = row
         return out
 
-    def autotune_form(self, states, boundary_state=None, reps=3):
-        """Sum-factorised hexahedron path: time one right-hand side in the step's split form
-        (dgb_rhs_profile, CUDA events around each launch) in the fused (three-launch) and in the
-        six-launch form on ``states``, best of ``reps``, and keep the faster form in the plan.
+    def autotune_form(self, states, boundary_state=None, reps=3, mood=True):
+        """Sum-factorised hexahedron path: time one right-hand side as an SSP-RK stage forms it
+        (``dgb_rhs_profile_stage``, CUDA events around each launch) in the fused (three-launch) and
+        in the six-launch form on ``states``, best of ``reps``, and keep the faster form in the plan.
+        With ``mood`` the six-launch form keeps the viscous residual apart, as its MOOD step does;
+        the fused form's MOOD step forms one residual and the viscous one for flagged elements only.
         Returns {"fused": ms, "six_launch": ms, "chosen": form}; an empty dict elsewhere."""
         if not self.native.sum_factorised:
             return {}
@@ -370,9 +372,11 @@ class HybridEulerOperator:
         out = {}
         for name, fused in (("fused", True), ("six_launch", False)):
             self.native.set_fused(fused)
+            split = int(bool(mood) and not fused and self.viscous)
             best = float("inf")
             for _ in range(int(reps) + 1):       # the first run loads the kernels
-                N.check(N.lib().dgb_rhs_profile(self.native.handle, ctypes.byref(st), ms, _stream_ptr()))
+                N.check(N.lib().dgb_rhs_profile_stage(self.native.handle, ctypes.byref(st), split, ms,
+                                                      _stream_ptr()))
                 best = min(best, float(sum(ms)))
             out[name] = best
         out["chosen"] = "fused" if out["fused"] <= out["six_launch"] else "six_launch"

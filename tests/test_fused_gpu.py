@@ -81,3 +81,33 @@ def test_fused_mood_step_matches_six_launch_form(precision):
     tol = 1e-12 if precision == "float64" else 1e-5
     for k in a:
         assert _rel(a[k], b[k]) <= tol
+
+
+@pytest.mark.parametrize("precision", ["float64", "mixed"])
+def test_mood_step_forms_agree_and_form_autotune(precision):
+    """The checked MOOD step in the fused form (one residual per element, the viscous residual
+    formed afterwards for the flagged elements only) against the six-launch form (split
+    residuals), from the shocked start of the benchmark's sphere at its smallest size, where the
+    subcell scheme runs: the same admissibility and the same state to 1e-12 of each field's largest
+    magnitude in float64, 1e-5 in mixed precision.  Then the form autotuner times both forms as the
+    step forms its right-hand side and keeps the faster."""
+    import jax_fluid_sim_b200 as jfs
+    from jax_fluid_sim_b200 import workloads
+    solver, op, bc, U = workloads.sphere_case("tiny", 3, precision)
+    integ = jfs.HybridSSPRK3(op, cfl=0.3, limiter=jfs.HybridMOODSubcellLimiter(
+        op, positivity=jfs.HybridPositivityLimiter(op)))
+    dt = integ.stable_dt(U, bc)
+    outs = []
+    for fused in (True, False):
+        op.native.set_fused(fused)
+        V, ok, _, _ = integ.checked_step({k: v.clone() for k, v in U.items()}, dt, bc)
+        outs.append((V, bool(ok)))
+    assert outs[0][1] == outs[1][1]
+    bar = 1e-12 if precision == "float64" else 1e-5
+    for k in U:
+        a, b = outs[0][0][k].cpu().numpy(), outs[1][0][k].cpu().numpy()
+        err = (np.abs(a - b).max(axis=(0, 1)) / np.maximum(np.abs(b).max(axis=(0, 1)), 1e-300)).max()
+        assert err <= bar, err
+    r = op.autotune_form(U, bc, reps=1)
+    assert r["fused"] > 0 and r["six_launch"] > 0 and r["chosen"] in ("fused", "six_launch")
+    assert op.native.fused == (r["chosen"] == "fused")

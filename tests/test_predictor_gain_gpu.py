@@ -2,11 +2,12 @@
 sphere grid (smallest size, 416 P3 hexahedra) from its shocked start.
 
 1. Skipping is exact.  When every element is predicted troubled (threshold below 0) the
-   learned step sends them all to the subcell scheme without their inviscid high-order update
-   and without the a-posteriori test; the plain step with a detector that flags every element
+   learned step sends them all to the subcell scheme without their high-order update and
+   without the a-posteriori test; the plain step with a detector that flags every element
    (sensor threshold below 0) recomputes the same elements after computing that update.  The
-   subcell scheme uses only the base state and the viscous residual of a troubled element, so
-   the two steps must agree bit for bit.
+   subcell scheme uses only the base state and the viscous residual of a troubled element
+   (formed for the flagged elements by the same kernel in both steps), so the two steps must
+   agree bit for bit.
 2. The trained network gains.  Trained on ten plain steps, in evaluate mode (the plain step,
    every element still tested) it predicts at least half of the detector's flags, i.e. those
    elements' failed high-order attempts are the ones the learned step skips; the learned step
