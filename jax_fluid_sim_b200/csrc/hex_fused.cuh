@@ -431,10 +431,17 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
     R* bs = tmp + CH * QF * N;        // [6][12][N2]
     R* ball = bs + CH * N2;           // [12][N3]
     R* ax = ball + 12 * N3;           // affine scratch [3][12][N3]
-    for (int idx = threadIdx.x; idx < 6 * QF2 * 12; idx += blockDim.x) {
-      const int lf = idx / (QF2 * 12), q = (idx / 12) % QF2, c = idx % 12;
-      jc[(lf * 12 + c) * QF2 + codes.perm[fperm[lf] + q]] =
-          (R)fd.jumpW[((size_t)(fface[lf] >> 1) * QF2 + q) * 12 + c];
+    // one face point per thread: its 12 jump components (contiguous) to the canonical point
+    for (int it = threadIdx.x; it < 6 * QF2; it += blockDim.x) {
+      const int lf = it / QF2, q = it % QF2;
+      const int cp = codes.perm[fperm[lf] + q];
+      const double2* src = reinterpret_cast<const double2*>(fd.jumpW + ((size_t)(fface[lf] >> 1) * QF2 + q) * 12);
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        const double2 v = src[k];
+        jc[(lf * 12 + 2 * k) * QF2 + cp] = (R)v.x;
+        jc[(lf * 12 + 2 * k + 1) * QF2 + cp] = (R)v.y;
+      }
     }
     __syncthreads();
     tensor2<CH, QF, QF, N, N>(jc, bs, tmp, tb->bfT, tb->bfT);
@@ -591,18 +598,24 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
   R* tmp = hc + 6 * C * QF2;                    // [6][C][QF][N]
   R* hs = tmp + 6 * C * QF * N;                 // [6][C][N2]; reused for the M^-1 partial sums
   const size_t base = (size_t)e * N3 * NV;
-  for (int idx = threadIdx.x; idx < 6 * QF2 * NV; idx += blockDim.x) {
-    const int lf = idx / (QF2 * NV), q = (idx / NV) % QF2, v = idx % NV;
+  // one face point per thread: its NV inviscid and NV viscous flux values (contiguous)
+  for (int it = threadIdx.x; it < 6 * QF2; it += blockDim.x) {
+    const int lf = it / QF2, q = it % QF2;
     const int f = fface[lf] >> 1, side = fface[lf] & 1;
     const double si = side == 0 ? -1.0 : 1.0;
-    const double hi = skip_inv ? 0.0 : si * fd.fluxI[((size_t)fslot[lf] + q) * NV + v];
-    const double hv = visc ? -si * fd.fluxV[((size_t)f * QF2 + q) * NV + v] : 0.0;
     const int c = codes.perm[fperm[lf] + q];
-    if (SPLIT) {
-      hc[(lf * C + v) * QF2 + c] = (R)hi;
-      hc[(lf * C + NV + v) * QF2 + c] = (R)hv;
-    } else {
-      hc[(lf * C + v) * QF2 + c] = (R)(hi + hv);
+    const double* fi = fd.fluxI + ((size_t)fslot[lf] + q) * NV;
+    const double* fv = fd.fluxV + ((size_t)f * QF2 + q) * NV;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      const double hi = skip_inv ? 0.0 : si * fi[v];
+      const double hv = visc ? -si * fv[v] : 0.0;
+      if (SPLIT) {
+        hc[(lf * C + v) * QF2 + c] = (R)hi;
+        hc[(lf * C + NV + v) * QF2 + c] = (R)hv;
+      } else {
+        hc[(lf * C + v) * QF2 + c] = (R)(hi + hv);
+      }
     }
   }
   __syncthreads();

@@ -354,10 +354,13 @@ __global__ void __launch_bounds__(kThreads) k_hex_traces(const DevPlan P_, const
   } else {
     tensor2<6 * NV, N, N, QF, QF>(slabs, fo, ftmp, tb->bf, tb->bf);
   }
-  for (int idx = threadIdx.x; idx < 6 * QF2 * NV; idx += blockDim.x) {
-    const int lf = idx / (QF2 * NV), q = (idx / NV) % QF2, v = idx % NV;
+  // one face point per thread from here on: its values are contiguous in the face buffers
+  for (int it = threadIdx.x; it < 6 * QF2; it += blockDim.x) {
+    const int lf = it / QF2, q = it % QF2;
     const int c = codes.perm[fperm[lf] + q];
-    fd.trA[((size_t)fslot[lf] + q) * NV + v] = anchor[v] + (double)fo[(lf * NV + v) * QF2 + c];
+    double* dst = fd.trA + ((size_t)fslot[lf] + q) * NV;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) dst[v] = anchor[v] + (double)fo[(lf * NV + v) * QF2 + c];
   }
   // the anchor state per face side, for the face kernel's anchor flux
   for (int idx = threadIdx.x; idx < 6 * NV; idx += blockDim.x)
@@ -365,34 +368,40 @@ __global__ void __launch_bounds__(kThreads) k_hex_traces(const DevPlan P_, const
   if (visc) {
     const R* fv = fo + 6 * NV * QF2;          // [6][4][QF2]
     const R* gn = fv + 24 * QF2;              // [6][4][QF2]
-    for (int idx = threadIdx.x; idx < 6 * QF2 * 4; idx += blockDim.x) {
-      const int lf = idx / (QF2 * 4), q = (idx / 4) % QF2, m = idx % 4;
+    for (int it = threadIdx.x; it < 6 * QF2; it += blockDim.x) {
+      const int lf = it / QF2, q = it % QF2;
       const int c = codes.perm[fperm[lf] + q];
-      if (F32) fd.trV32[((size_t)fslot[lf] + q) * 4 + m] = (float)fv[(lf * 4 + m) * QF2 + c];
-      else fd.trV[((size_t)fslot[lf] + q) * 4 + m] = (double)fv[(lf * 4 + m) * QF2 + c];
-    }
-    for (int idx = threadIdx.x; idx < 6 * QF2 * 12; idx += blockDim.x) {
-      const int lf = idx / (QF2 * 12), q = (idx / 12) % QF2, m = (idx % 12) / 3, d = idx % 3;
+      const size_t pt = (size_t)fslot[lf] + q;
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        if (F32) fd.trV32[pt * 4 + m] = (float)fv[(lf * 4 + m) * QF2 + c];
+        else fd.trV[pt * 4 + m] = (double)fv[(lf * 4 + m) * QF2 + c];
+      }
       int a0, end, a1, a2;
       hex_face_axes(lf, a0, end, a1, a2);
-      const int c = codes.perm[fperm[lf] + q];
-      const int k = (lf * 4 + m) * QF2 + c;
-      const R gnv = gn[k], g1v = g1[k], g2v = g2[k];
-      // reference gradient component along axis r: normal (a0) or tangential (a1 < a2)
-      const R gx = a0 == 0 ? gnv : g1v;
-      const R gy = a0 == 1 ? gnv : (a0 == 0 ? g1v : g2v);
-      const R gz = a0 == 2 ? gnv : g2v;
-      const size_t pt = (size_t)fslot[lf] + q;
-      R J0, J1, J2;
+      R J[9];
       if (sizeof(R) == sizeof(float) && fd.jinv32) {
-        const float* J = fd.jinv32 + pt * 9;
-        J0 = (R)J[0 * 3 + d], J1 = (R)J[1 * 3 + d], J2 = (R)J[2 * 3 + d];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) J[k] = (R)fd.jinv32[pt * 9 + k];
       } else {
-        const double* J = fd.jinv + pt * 9;
-        J0 = (R)J[0 * 3 + d], J1 = (R)J[1 * 3 + d], J2 = (R)J[2 * 3 + d];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) J[k] = (R)fd.jinv[pt * 9 + k];
       }
-      if (F32) fd.trG32[pt * 12 + m * 3 + d] = (float)(gx * J0 + gy * J1 + gz * J2);
-      else fd.trG[pt * 12 + m * 3 + d] = (double)(gx * J0 + gy * J1 + gz * J2);
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const int k = (lf * 4 + m) * QF2 + c;
+        const R gnv = gn[k], g1v = g1[k], g2v = g2[k];
+        // reference gradient component along axis r: normal (a0) or tangential (a1 < a2)
+        const R gx = a0 == 0 ? gnv : g1v;
+        const R gy = a0 == 1 ? gnv : (a0 == 0 ? g1v : g2v);
+        const R gz = a0 == 2 ? gnv : g2v;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const R x = gx * J[0 * 3 + d] + gy * J[1 * 3 + d] + gz * J[2 * 3 + d];
+          if (F32) fd.trG32[pt * 12 + m * 3 + d] = (float)x;
+          else fd.trG[pt * 12 + m * 3 + d] = (double)x;
+        }
+      }
     }
   }
 }
