@@ -763,12 +763,12 @@ int run_predict(dgb_plan* p, const StatePtrs& S, cudaStream_t st) {
 template <int NV>
 int run_step_mood(dgb_plan* p, const StatePtrs& U0, double dt, dgb_status* status, cudaStream_t st) {
   const DevPlan& P = p->dev;
-  StatePtrs S1, S2, UNL, REC;
+  StatePtrs S1, S2, UNL, EUL;
   for (int b = 0; b < DGB_MAX_BLOCKS; ++b) {
     S1.b[b] = p->stage1[b];
     S2.b[b] = p->stage2[b];
     UNL.b[b] = p->unl[b];
-    REC.b[b] = p->rec[b];
+    EUL.b[b] = p->eul[b];
   }
   const double alphas[3] = {0.0, 0.75, 1.0 / 3.0};
   const double betas[3] = {1.0, 0.25, 2.0 / 3.0};
@@ -803,11 +803,13 @@ int run_step_mood(dgb_plan* p, const StatePtrs& U0, double dt, dgb_status* statu
     if ((rc = run_rhs<NV>(p, *cur[s], A, st))) return rc;
     if ((rc = run_troubled<NV>(p, UNL, nullptr, p->flags, st, true))) return rc;
     if (vis_after && (rc = run_viscous_flagged<NV>(p, *cur[s], st))) return rc;
-    if ((rc = run_subcell<NV>(p, *cur[s], p->eul, p->vis, dt, F, p->rec, st))) return rc;
-    if ((rc = run_positivity<NV>(p, REC, st))) return rc;
+    // the subcell update lands in place in the Euler candidate: elements that are neither
+    // troubled nor corrected at a face keep theirs without a copy
+    if ((rc = run_subcell<NV>(p, *cur[s], p->eul, p->vis, dt, F, p->eul, st))) return rc;
+    if ((rc = run_positivity<NV>(p, EUL, st))) return rc;
     for (int b = 0; b < P.nblocks; ++b) {
       const size_t n = (size_t)P.blk[b].E * P.blk[b].Np * NV;
-      k_blend<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(U0.b[b], p->rec[b], alphas[s], betas[s], dst[s]->b[b], n);
+      k_blend<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(U0.b[b], p->eul[b], alphas[s], betas[s], dst[s]->b[b], n);
     }
     if ((rc = run_positivity<NV>(p, *dst[s], st))) return rc;
     if ((rc = run_admissibility<NV>(p, *dst[s], status, 0, st))) return rc;

@@ -289,7 +289,8 @@ __global__ void __launch_bounds__(kThreads) k_mood_faces(const DevPlan P, const 
 }
 
 // --------------------------------------------------------------------------------------------
-// out = troubled ? bound-limited reconstruction of the FV update : candidate + corrections.
+// out = troubled ? bound-limited reconstruction of the FV update : candidate + corrections.  out may
+// be cand (in place): a troubled element's update does not read its candidate.
 template <int NV>
 __global__ void __launch_bounds__(kThreads) k_mood_update(const DevPlan P, const MoodDev M, int b, const FlagPtrs Fl,
                                                          const double* cand, const double* visc, double dt,
@@ -327,6 +328,7 @@ __global__ void __launch_bounds__(kThreads) k_mood_update(const DevPlan P, const
       if (hit) atomicOr(&any, 1);
     }
     __syncthreads();
+    if (out == cand && !any) return;     // in place: an element without corrections keeps its candidate
     for (int idx = threadIdx.x; idx < Np * NV; idx += blockDim.x)
       out[base + idx] = any ? cand[base + idx] + corr[idx % NV] : cand[base + idx];
     return;
