@@ -319,32 +319,26 @@ __global__ void __launch_bounds__(kThreads) k_hex_traces(const DevPlan P_, const
     }
   }
   __syncthreads();
-  const int nch = visc ? CH : 6 * NV;
-  for (int idx = threadIdx.x; idx < nch * N2; idx += blockDim.x) {
-    const int j1 = idx % N, j2 = (idx / N) % N, c = idx / N2;
-    int lf, m, kind;                   // kind 0: U, 1: v, 2: dv/dn
-    if (c < 6 * NV) {
-      lf = c / NV, m = c % NV, kind = 0;
-    } else if (c < 6 * NV + 24) {
-      lf = (c - 6 * NV) / 4, m = (c - 6 * NV) % 4, kind = 1;
-    } else {
-      lf = (c - 6 * NV - 24) / 4, m = (c - 6 * NV - 24) % 4, kind = 2;
-    }
+  // one face node (face, j1, j2) per thread: all its channels
+  for (int it = threadIdx.x; it < 6 * N2; it += blockDim.x) {
+    const int lf = it / N2, j = it % N2, j1 = j % N, j2 = j / N;
     int a0, end, a1, a2;
     hex_face_axes(lf, a0, end, a1, a2);
     const int st0 = axis_stride<N>(a0), off = j1 * axis_stride<N>(a1) + j2 * axis_stride<N>(a2);
-    R val;
-    if (kind == 0) {
-      val = U[m * N3 + end * st0 + off];
-    } else if (kind == 1) {
-      val = V[m * N3 + end * st0 + off];
-    } else {
-      const R* dn = end ? tb->d1 : tb->d0;
-      val = R(0);
+    const int at = end * st0 + off;
 #pragma unroll
-      for (int j0 = 0; j0 < N; ++j0) val += dn[j0] * V[m * N3 + j0 * st0 + off];
+    for (int m = 0; m < NV; ++m) slabs[(lf * NV + m) * N2 + j] = U[m * N3 + at];
+    if (visc) {
+      const R* dn = end ? tb->d1 : tb->d0;
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        slabs[(6 * NV + lf * 4 + m) * N2 + j] = V[m * N3 + at];
+        R val = R(0);
+#pragma unroll
+        for (int j0 = 0; j0 < N; ++j0) val += dn[j0] * V[m * N3 + j0 * st0 + off];
+        slabs[(6 * NV + 24 + lf * 4 + m) * N2 + j] = val;
+      }
     }
-    slabs[idx] = val;
   }
   __syncthreads();
   if (visc) {
