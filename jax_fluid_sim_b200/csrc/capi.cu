@@ -707,7 +707,7 @@ int run_subcell(dgb_plan* p, const StatePtrs& cur, double* const* cand, double* 
   }
   for (int ft = 0; ft < 2; ++ft)
     if (p->face_present[ft])
-      k_mood_faces<NV><<<blocks_for((long)P.face[ft].F * 32, kThreads), kThreads, 0, st>>>(P, M, cur, ft, F);
+      k_mood_faces<NV><<<blocks_for((long)P.face[ft].F, kThreads), kThreads, 0, st>>>(P, M, cur, ft, F);
   for (int b = 0; b < P.nblocks; ++b) {
     const SubcellBlockDev& C = M.blk[b];
     const size_t sm = sizeof(double) * ((size_t)C.S * NV * 2 + (size_t)P.blk[b].Np * NV);

@@ -7,7 +7,8 @@
 //   k_mood_fv      troubled element: subcell means (projection), Green-Gauss gradients,
 //                  constant/TVD/CWENO-Z face states with admissibility clamps, HLLC on the
 //                  internal subfaces, internal residual per subcell (gather, no atomics).
-//   k_mood_faces   one warp per parent face with a troubled side: lanes 0-15 the 16
+//   k_mood_faces   each warp screens 32 parent faces, then works those with a troubled side
+//                  one at a time (mood_face): lanes 0-15 the 16
 //                  DG-FV coupling subfaces (FV mean on a troubled side, DG value at the
 //                  subface centre otherwise), lanes 16-31 the DG face flux integrated with
 //                  the face rule; stores subface fluxes and (new - old) face flux.
@@ -196,20 +197,15 @@ __device__ void dg_at_subface(const double* Ue, const double* basis_row, int Np,
   }
 }
 
+// One parent face with a troubled side, worked by a whole warp (lane: see k_mood_faces).
 template <int NV>
-__global__ void __launch_bounds__(kThreads) k_mood_faces(const DevPlan P, const MoodDev M, const StatePtrs S, int ft,
-                                                        const FlagPtrs Fl) {
+__device__ __forceinline__ void mood_face(const DevPlan& P, const MoodDev& M, const StatePtrs& S, int ft, int f,
+                                          const FlagPtrs& Fl, int lane) {
   const FaceDev& fd = P.face[ft];
   const SubcellFaceDev& sf = M.face[ft];
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (warp >= fd.F) return;
-  const int f = warp;
   const int ob = fd.ob[f], ol = fd.ol[f], nb = fd.nb[f], nl = fd.nl[f];
   const bool tro = Fl.f[ob][ol] != 0;
   const bool trn = nb >= 0 && Fl.f[nb][nl] != 0;
-  const bool active = tro || trn;
-  if (lane == 0) sf.active[f] = active;
-  if (!active) return;
   double Fv[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) Fv[v] = 0.0;
@@ -288,6 +284,31 @@ __global__ void __launch_bounds__(kThreads) k_mood_faces(const DevPlan P, const 
   }
 }
 
+// Each warp screens 32 parent faces (one per lane) for a troubled side, records which are active,
+// then works its active faces one after another with the whole warp.
+template <int NV>
+__global__ void __launch_bounds__(kThreads) k_mood_faces(const DevPlan P, const MoodDev M, const StatePtrs S, int ft,
+                                                        const FlagPtrs Fl) {
+  const FaceDev& fd = P.face[ft];
+  const SubcellFaceDev& sf = M.face[ft];
+  const int lane = threadIdx.x & 31;
+  const long f0 = ((long)blockIdx.x * blockDim.x + threadIdx.x) & ~31L;
+  if (f0 >= fd.F) return;                       // whole warps leave together
+  const long f = f0 + lane;
+  bool active = false;
+  if (f < fd.F) {
+    const int ob = fd.ob[f], ol = fd.ol[f], nb = fd.nb[f], nl = fd.nl[f];
+    active = Fl.f[ob][ol] != 0 || (nb >= 0 && Fl.f[nb][nl] != 0);
+    sf.active[f] = active;
+  }
+  unsigned todo = __ballot_sync(0xffffffffu, active);
+  while (todo) {
+    const int k = __ffs(todo) - 1;
+    todo &= todo - 1;
+    mood_face<NV>(P, M, S, ft, (int)(f0 + k), Fl, lane);
+  }
+}
+
 // --------------------------------------------------------------------------------------------
 // out = troubled ? bound-limited reconstruction of the FV update : candidate + corrections.  out may
 // be cand (in place): a troubled element's update does not read its candidate.
@@ -302,33 +323,38 @@ __global__ void __launch_bounds__(kThreads) k_mood_update(const DevPlan P, const
   const size_t base = (size_t)e * Np * NV;
   const double* vol = C.vol + (size_t)e * Sn;
   __shared__ double vtot;
-  if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int k = 0; k < Sn; ++k) s += vol[k];
-    vtot = s;
-  }
   if (!Fl.f[b][e]) {
-    // conservative correction from active faces where this element is not troubled
+    // conservative correction from active faces where this element is not troubled; the element
+    // volume is summed only when one is
     __shared__ double corr[DGB_MAX_VARS];
     __shared__ int any;
     if (threadIdx.x == 0) any = 0;
     __syncthreads();
+    if (threadIdx.x < B.nlf) {
+      int ft, f, side;
+      decode_face(B.elem_face[e * B.nlf + threadIdx.x], ft, f, side);
+      if (M.face[ft].active[f]) atomicOr(&any, 1);
+    }
+    __syncthreads();
+    if (out == cand && !any) return;     // in place: an element without corrections keeps its candidate
+    if (any && threadIdx.x == 0) {
+      double s = 0.0;
+      for (int k = 0; k < Sn; ++k) s += vol[k];
+      vtot = s;
+    }
+    __syncthreads();
     if (threadIdx.x < NV) {
       double c = 0.0;
-      int hit = 0;
       for (int lf = 0; lf < B.nlf; ++lf) {
         int ft, f, side;
         decode_face(B.elem_face[e * B.nlf + lf], ft, f, side);
         if (!M.face[ft].active[f]) continue;
-        hit = 1;
         const double d = M.face[ft].dflux[(size_t)f * NV + threadIdx.x];
         c += side == 0 ? -dt * d / vtot : dt * d / vtot;
       }
       corr[threadIdx.x] = c;
-      if (hit) atomicOr(&any, 1);
     }
     __syncthreads();
-    if (out == cand && !any) return;     // in place: an element without corrections keeps its candidate
     for (int idx = threadIdx.x; idx < Np * NV; idx += blockDim.x)
       out[base + idx] = any ? cand[base + idx] + corr[idx % NV] : cand[base + idx];
     return;
