@@ -700,6 +700,7 @@ int run_subcell(dgb_plan* p, const StatePtrs& cur, double* const* cand, double* 
   M.recon = p->prm.reconstruction;
   int rc;
   for (int b = 0; b < P.nblocks; ++b) {
+    if (P.blk[b].E == 0) continue;
     const SubcellBlockDev& C = M.blk[b];
     const size_t sm = sizeof(double) * ((size_t)P.blk[b].Np * NV + (size_t)C.S * NV * 4 + (size_t)C.NI * NV);
     if ((rc = prepare(k_mood_fv<NV>, sm))) return rc;
@@ -709,6 +710,7 @@ int run_subcell(dgb_plan* p, const StatePtrs& cur, double* const* cand, double* 
     if (p->face_present[ft])
       k_mood_faces<NV><<<blocks_for((long)P.face[ft].F, kThreads), kThreads, 0, st>>>(P, M, cur, ft, F);
   for (int b = 0; b < P.nblocks; ++b) {
+    if (P.blk[b].E == 0) continue;
     const SubcellBlockDev& C = M.blk[b];
     const size_t sm = sizeof(double) * ((size_t)C.S * NV * 2 + (size_t)P.blk[b].Np * NV);
     if ((rc = prepare(k_mood_update<NV>, sm))) return rc;
