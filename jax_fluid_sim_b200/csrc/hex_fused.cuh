@@ -90,7 +90,7 @@ struct HexFaceArgs {
 // R: arithmetic of the local lifts and the viscous face flux (float in precision mode 1; HLLC and
 // the jumps are float64 in both modes).  F32: the viscous traces come from trV32 / trG32.
 template <int P, int NV, typename R = double, bool F32 = false>
-__global__ void __launch_bounds__(kThreads, NV <= 5 ? 5 : 1) k_hex_face(const DevPlan P_, const HexTables tables,
+__global__ void __launch_bounds__(kThreads, NV <= 5 ? 6 : 1) k_hex_face(const DevPlan P_, const HexTables tables,
                                                                        const HexCodes codes, const HexFaceArgs A) {
   using D = HexDims<P>;
   constexpr int N = D::N, QF = D::QF, QF2 = D::QF2;
