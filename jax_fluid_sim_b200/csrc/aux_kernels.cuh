@@ -154,6 +154,59 @@ __device__ bool nodal_certificate(const double* __restrict__ Ug, int Np, const P
   return certificate_from_range(mn, mx, ph, L, rho_floor, p_floor, rel);
 }
 
+// The SSP-RK stage blend out = alpha * base + beta * x of one element (as k_blend forms it), written
+// to out, with the warp-level nodal range of the result (warp_nodal_range's layout and result).
+template <int NV, int NP>
+__device__ __forceinline__ bool warp_blend_range(const double* __restrict__ base, const double* __restrict__ x,
+                                                 double alpha, double beta, double* __restrict__ out,
+                                                 double (&mn)[5], double (&mx)[5]) {
+#pragma unroll
+  for (int v = 0; v < 5; ++v) {
+    mn[v] = INFINITY;
+    mx[v] = -INFINITY;
+  }
+  bool fin = true;
+#pragma unroll
+  for (int l0 = 0; l0 < NP; l0 += 32) {
+    const int l = l0 + (threadIdx.x & 31);
+    if (l < NP) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        const double y = alpha * base[l * NV + v] + beta * x[l * NV + v];
+        out[l * NV + v] = y;
+        fin &= isfinite(y);
+        if (v < 5) {
+          mn[v] = fmin(mn[v], y);
+          mx[v] = fmax(mx[v], y);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < 5; ++v)
+    for (int o = 16; o > 0; o >>= 1) {
+      mn[v] = fmin(mn[v], __shfl_xor_sync(0xffffffff, mn[v], o));
+      mx[v] = fmax(mx[v], __shfl_xor_sync(0xffffffff, mx[v], o));
+    }
+  return __all_sync(0xffffffff, fin);
+}
+
+// k_certify on the stage blend: out = alpha * base + beta * x is written and certified in one pass.
+template <int NV, int NP>
+__global__ void __launch_bounds__(kThreads) k_blend_certify(const double* __restrict__ base,
+                                                           const double* __restrict__ x, double alpha, double beta,
+                                                           double* __restrict__ out, int E, const Physics ph,
+                                                           double L, double rho_floor, double p_floor, double rel,
+                                                           int* __restrict__ list, int* __restrict__ count) {
+  const long long e = (long long)blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
+  if (e >= E) return;
+  double mn[5], mx[5];
+  const size_t o = (size_t)e * NP * NV;
+  const bool fin = warp_blend_range<NV, NP>(base + o, x + o, alpha, beta, out + o, mn, mx);
+  if ((threadIdx.x & 31) == 0 && !(fin && certificate_from_range(mn, mx, ph, L, rho_floor, p_floor, rel)))
+    list[atomicAdd(count, 1)] = (int)e;
+}
+
 // Certificate pre-pass, one warp per element of NP nodes: elements of block U that the
 // certificate does not clear are appended to list (in no fixed order; each is then processed on
 // its own, so results do not depend on it).  *count must be zero before the launch.

@@ -580,6 +580,27 @@ int run_positivity_hex(dgb_plan* p, const StatePtrs& S, cudaStream_t st) {
   return DGB_OK;
 }
 
+// The stage blend dst = alpha * base + beta * x followed by positivity on the sum-factorised path,
+// with the blend fused into the certificate pre-pass.
+template <int P, int NV>
+int run_blend_positivity_hex(dgb_plan* p, const double* base, const double* x, double alpha, double beta, double* dst,
+                             cudaStream_t st) {
+  const BlockDev& B = p->dev.blk[0];
+  if (B.E == 0) return DGB_OK;
+  CK(cudaMemsetAsync(p->cert_count, 0, sizeof(int), st));
+  k_blend_certify<NV, HexDims<P>::N3><<<blocks_for(B.E, kThreads / 32), kThreads, 0, st>>>(
+      base, x, alpha, beta, dst, B.E, p->dev.ph, p->lim.lebesgue, p->lim.density_floor, p->lim.pressure_floor,
+      p->lim.relative_floor, p->cert_list, p->cert_count);
+  StatePtrs S;
+  for (int b = 0; b < DGB_MAX_BLOCKS; ++b) S.b[b] = nullptr;
+  S.b[0] = dst;
+  const size_t sm = sizeof(double) * (size_t)hex_positivity_smem<P, NV>();
+  k_hex_positivity<P, NV><<<p->pos_grid, kThreads, sm, st>>>(p->dev, S, 0, p->hex_tables, p->lim, p->cert_list,
+                                                             p->cert_count);
+  CK(cudaGetLastError());
+  return DGB_OK;
+}
+
 // Resident CTAs of k_hex_troubled over the whole GPU (set-up; at most one per element).
 template <int P, int NV>
 int hex_troubled_grid(dgb_plan* p) {
@@ -809,11 +830,18 @@ int run_step_mood(dgb_plan* p, const StatePtrs& U0, double dt, dgb_status* statu
     // troubled nor corrected at a face keep theirs without a copy
     if ((rc = run_subcell<NV>(p, *cur[s], p->eul, p->vis, dt, F, p->eul, st))) return rc;
     if ((rc = run_positivity<NV>(p, EUL, st))) return rc;
-    for (int b = 0; b < P.nblocks; ++b) {
-      const size_t n = (size_t)P.blk[b].E * P.blk[b].Np * NV;
-      k_blend<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(U0.b[b], p->eul[b], alphas[s], betas[s], dst[s]->b[b], n);
+    if (p->hex) {
+      rc = p->dev.degree == 1 ? run_blend_positivity_hex<1, NV>(p, U0.b[0], p->eul[0], alphas[s], betas[s], dst[s]->b[0], st)
+         : p->dev.degree == 2 ? run_blend_positivity_hex<2, NV>(p, U0.b[0], p->eul[0], alphas[s], betas[s], dst[s]->b[0], st)
+                              : run_blend_positivity_hex<3, NV>(p, U0.b[0], p->eul[0], alphas[s], betas[s], dst[s]->b[0], st);
+      if (rc) return rc;
+    } else {
+      for (int b = 0; b < P.nblocks; ++b) {
+        const size_t n = (size_t)P.blk[b].E * P.blk[b].Np * NV;
+        k_blend<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(U0.b[b], p->eul[b], alphas[s], betas[s], dst[s]->b[b], n);
+      }
+      if ((rc = run_positivity<NV>(p, *dst[s], st))) return rc;
     }
-    if ((rc = run_positivity<NV>(p, *dst[s], st))) return rc;
     if ((rc = run_admissibility<NV>(p, *dst[s], status, 0, st))) return rc;
   }
   return DGB_OK;
