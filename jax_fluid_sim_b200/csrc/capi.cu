@@ -99,7 +99,7 @@ struct dgb_plan {
   bool fused = true;
   // false while a caller needs the float64 viscous traces (the wall-force integral reads them)
   bool f32_traces = true;
-  HexFaceArgs hex_face = {nullptr, nullptr, nullptr};
+  HexFaceArgs hex_face = {nullptr, nullptr, nullptr, nullptr};
   // MOOD subcell fallback
   MoodDev mood;
   bool sub_block_set[DGB_MAX_BLOCKS] = {false, false, false};
@@ -190,9 +190,9 @@ int prepare(K kernel, size_t smem) {
 
 int blocks_for(long n, int per) { return (int)((n + per - 1) / per); }
 
-template <int P>
-void launch_hex_lop(dgb_plan* p, const int* elems, int count, double* lop) {
-  k_hex_lop<P, double><<<count * 6, 128>>>(p->dev, p->hex_tables, elems, count, lop);
+template <int P, typename T>
+void launch_hex_lop(dgb_plan* p, const int* elems, int count, T* lop) {
+  k_hex_lop<P, T><<<count * 6, 128>>>(p->dev, p->hex_tables, elems, count, lop);
 }
 
 // Tables of the fused face kernel (set-up): the local face of every face side, and the local-lift
@@ -220,20 +220,36 @@ int build_hex_face_tables(dgb_plan* p) {
   const int* dindex = nullptr;
   int rc;
   if ((rc = upload(p, index.data(), index.size(), &dindex))) return rc;
+  // float64 operators for float64 plans; mixed plans round them to float32 when they store them,
+  // as the float32 face kernel does when it reads them, so they keep only that copy
   double* lop = nullptr;
+  float* lop32 = nullptr;
   if (!elems.empty()) {
     const int* delems = nullptr;
     if ((rc = upload(p, elems.data(), elems.size(), &delems))) return rc;
-    if ((rc = alloc(p, elems.size() * 6 * (size_t)QF2 * QF2, &lop))) return rc;
-    switch (p->dev.degree) {
-      case 1: launch_hex_lop<1>(p, delems, (int)elems.size(), lop); break;
-      case 2: launch_hex_lop<2>(p, delems, (int)elems.size(), lop); break;
-      default: launch_hex_lop<3>(p, delems, (int)elems.size(), lop); break;
+    const size_t n = elems.size() * 6 * (size_t)QF2 * QF2;
+    const int cnt = (int)elems.size();
+    if (p->prm.precision == 1) {
+      if ((rc = alloc(p, (n + 1) / 2, &lop))) return rc;
+      lop32 = reinterpret_cast<float*>(lop);
+      lop = nullptr;
+      switch (p->dev.degree) {
+        case 1: launch_hex_lop<1>(p, delems, cnt, lop32); break;
+        case 2: launch_hex_lop<2>(p, delems, cnt, lop32); break;
+        default: launch_hex_lop<3>(p, delems, cnt, lop32); break;
+      }
+    } else {
+      if ((rc = alloc(p, n, &lop))) return rc;
+      switch (p->dev.degree) {
+        case 1: launch_hex_lop<1>(p, delems, cnt, lop); break;
+        case 2: launch_hex_lop<2>(p, delems, cnt, lop); break;
+        default: launch_hex_lop<3>(p, delems, cnt, lop); break;
+      }
     }
     CK(cudaGetLastError());
   }
   CK(cudaDeviceSynchronize());
-  p->hex_face = HexFaceArgs{face_lf, dindex, lop};
+  p->hex_face = HexFaceArgs{face_lf, dindex, lop, lop32};
   return DGB_OK;
 }
 

@@ -84,7 +84,8 @@ __global__ void k_hex_lop(const DevPlan P_, const HexTables tables, const int* _
 struct HexFaceArgs {
   const int8_t* face_lf;      // [F][2]
   const int* lop_index;       // [E], -1 for affine elements
-  const double* lop;          // [count][6][QF2][QF2]
+  const double* lop;          // [count][6][QF2][QF2], float64 plans
+  const float* lop32;         // the same in float32, mixed-precision plans
 };
 
 // R: arithmetic of the local lifts and the viscous face flux (float in precision mode 1; HLLC and
@@ -208,9 +209,11 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 6 : 1) k_hex_face(const De
 #pragma unroll
       for (int c = 0; c < 12; ++c) lift[c] *= scale;
     } else {
-      const double* L = A.lop + ((size_t)li * 6 + lf) * QF2 * QF2 + (size_t)cq * QF2;
+      const size_t lo = ((size_t)li * 6 + lf) * QF2 * QF2 + (size_t)cq * QF2;
       for (int qp = 0; qp < QF2; ++qp) {
-        const R kk = (R)__ldg(L + perm[qp]);
+        R kk;
+        if constexpr (sizeof(R) == sizeof(float)) kk = __ldg(A.lop32 + lo + perm[qp]);
+        else kk = (R)__ldg(A.lop + lo + perm[qp]);
 #pragma unroll
         for (int c = 0; c < 12; ++c) lift[c] += kk * jf[qp * 12 + c];
       }
