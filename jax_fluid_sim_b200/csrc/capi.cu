@@ -1465,8 +1465,17 @@ int dgb_plan_finalize(dgb_plan* p) {
     if (p->face_present[1]) {
       if ((rc = to_float32(p, F.jinv, (size_t)F.F * 2 * F.nq * 9, &f))) return rc;
       F.jinv32 = f;
+      {
+        double* d;
+        if ((rc = alloc(p, ((size_t)F.F * 2 * F.nq * p->dev.nv + 1) / 2, &d))) return rc;
+        F.fluxI32 = reinterpret_cast<float*>(d);
+      }
       if (p->dev.viscous) {
         double* d;
+        if ((rc = alloc(p, ((size_t)F.F * F.nq * p->dev.nv + 1) / 2, &d))) return rc;
+        F.fluxV32 = reinterpret_cast<float*>(d);
+        if ((rc = alloc(p, (size_t)F.F * F.nq * 6, &d))) return rc;
+        F.jumpW32 = reinterpret_cast<float*>(d);
         if ((rc = alloc(p, ((size_t)F.F * 2 * F.nq * 4 + 1) / 2, &d))) return rc;
         F.trV32 = reinterpret_cast<float*>(d);
         if ((rc = alloc(p, (size_t)F.F * 2 * F.nq * 6, &d))) return rc;

@@ -84,6 +84,11 @@ struct FaceDev {
   // hexahedron kernels of mixed-precision plans (else null)
   float* trV32;           // [F][2][nq][4]
   float* trG32;           // [F][2][nq][12]
+  // float32 face fluxes and BR2 jumps of the fused hexahedron kernels of mixed-precision plans (the
+  // element kernel rounds them to float32 anyway)
+  float* fluxI32;         // [F][2][nq][NV]
+  float* fluxV32;         // [F][nq][NV]
+  float* jumpW32;         // [F][nq][12]
 };
 
 struct DevPlan {

@@ -96,6 +96,7 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 6 : 1) k_hex_face(const De
   using D = HexDims<P>;
   constexpr int N = D::N, QF = D::QF, QF2 = D::QF2;
   constexpr int FPC = kThreads / QF2;                // faces per CTA
+  constexpr bool RF = sizeof(R) == sizeof(float);    // float32 face fluxes and jumps (mixed precision)
   // jumps of each face's points, [face][point][12]; the face stride is padded by two doubles so
   // that the faces sharing a warp read different banks
   constexpr int JS = QF2 * 12 + 2;
@@ -142,7 +143,10 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 6 : 1) k_hex_face(const De
       for (int v = 0; v < NV; ++v) a[v] = fd.anc[((size_t)f * 2 + 0) * NV + v];
       normal_flux<NV>(P_.ph, a, n, Fa);
 #pragma unroll
-      for (int v = 0; v < NV; ++v) fd.fluxI[so * NV + v] = (Fh[v] - Fa[v]) * w;
+      for (int v = 0; v < NV; ++v) {
+        if (RF) fd.fluxI32[so * NV + v] = (float)((Fh[v] - Fa[v]) * w);
+        else fd.fluxI[so * NV + v] = (Fh[v] - Fa[v]) * w;
+      }
     }
     if (nb >= 0) {
       double a[NV];
@@ -150,7 +154,10 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 6 : 1) k_hex_face(const De
       for (int v = 0; v < NV; ++v) a[v] = fd.anc[((size_t)f * 2 + 1) * NV + v];
       normal_flux<NV>(P_.ph, a, n, Fa);
 #pragma unroll
-      for (int v = 0; v < NV; ++v) fd.fluxI[sn * NV + v] = (Fh[v] - Fa[v]) * w;
+      for (int v = 0; v < NV; ++v) {
+        if (RF) fd.fluxI32[sn * NV + v] = (float)((Fh[v] - Fa[v]) * w);
+        else fd.fluxI[sn * NV + v] = (Fh[v] - Fa[v]) * w;
+      }
     }
   }
   if (!P_.viscous) return;
@@ -167,13 +174,14 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 6 : 1) k_hex_face(const De
     } else {
       viscous_vars<NV>(P_.ph, UL, vn);
     }
-    double* out = fd.jumpW + ((size_t)f * QF2 + q) * 12;
+    const size_t jo = ((size_t)f * QF2 + q) * 12;
 #pragma unroll
     for (int m = 0; m < 4; ++m)
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         const double j = 0.5 * w * (vn[m] - vo[m]) * n[d];
-        out[m * 3 + d] = j;
+        if (RF) fd.jumpW32[jo + m * 3 + d] = (float)j;
+        else fd.jumpW[jo + m * 3 + d] = j;
         jmp[slot * JS + q * 12 + m * 3 + d] = (R)j;
       }
   }
@@ -246,7 +254,10 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 6 : 1) k_hex_face(const De
     out[v] = Fo[0 * NV + v] * (R)n[0] + Fo[1 * NV + v] * (R)n[1] + Fo[2 * NV + v] * (R)n[2];
   if (nb < 0 && P_.ph.has_boundary && tag_in(fd.tag[f], P_.ph.wall, P_.ph.n_wall)) out[4] = R(0);
 #pragma unroll
-  for (int v = 0; v < NV; ++v) fd.fluxV[((size_t)f * QF2 + q) * NV + v] = (double)(out[v] * (R)w);
+  for (int v = 0; v < NV; ++v) {
+    if (RF) fd.fluxV32[((size_t)f * QF2 + q) * NV + v] = (float)(out[v] * (R)w);
+    else fd.fluxV[((size_t)f * QF2 + q) * NV + v] = (double)(out[v] * (R)w);
+  }
 }
 
 // Rotation of the thread <-> line assignment of a pencil pass, so that passes issued back to back
@@ -438,12 +449,25 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
     for (int it = threadIdx.x; it < 6 * QF2; it += blockDim.x) {
       const int lf = it / QF2, q = it % QF2;
       const int cp = codes.perm[fperm[lf] + q];
-      const double2* src = reinterpret_cast<const double2*>(fd.jumpW + ((size_t)(fface[lf] >> 1) * QF2 + q) * 12);
+      const size_t jo = ((size_t)(fface[lf] >> 1) * QF2 + q) * 12;
+      if constexpr (sizeof(R) == sizeof(float)) {
+        const float4* src = reinterpret_cast<const float4*>(fd.jumpW32 + jo);
 #pragma unroll
-      for (int k = 0; k < 6; ++k) {
-        const double2 v = src[k];
-        jc[(lf * 12 + 2 * k) * QF2 + cp] = (R)v.x;
-        jc[(lf * 12 + 2 * k + 1) * QF2 + cp] = (R)v.y;
+        for (int k = 0; k < 3; ++k) {
+          const float4 v = src[k];
+          jc[(lf * 12 + 4 * k) * QF2 + cp] = v.x;
+          jc[(lf * 12 + 4 * k + 1) * QF2 + cp] = v.y;
+          jc[(lf * 12 + 4 * k + 2) * QF2 + cp] = v.z;
+          jc[(lf * 12 + 4 * k + 3) * QF2 + cp] = v.w;
+        }
+      } else {
+        const double2* src = reinterpret_cast<const double2*>(fd.jumpW + jo);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+          const double2 v = src[k];
+          jc[(lf * 12 + 2 * k) * QF2 + cp] = (R)v.x;
+          jc[(lf * 12 + 2 * k + 1) * QF2 + cp] = (R)v.y;
+        }
       }
     }
     __syncthreads();
@@ -607,17 +631,28 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
     const int f = fface[lf] >> 1, side = fface[lf] & 1;
     const double si = side == 0 ? -1.0 : 1.0;
     const int c = codes.perm[fperm[lf] + q];
-    const double* fi = fd.fluxI + ((size_t)fslot[lf] + q) * NV;
-    const double* fv = fd.fluxV + ((size_t)f * QF2 + q) * NV;
+    const size_t ki = ((size_t)fslot[lf] + q) * NV, kv = ((size_t)f * QF2 + q) * NV;
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-      const double hi = skip_inv ? 0.0 : si * fi[v];
-      const double hv = visc ? -si * fv[v] : 0.0;
-      if (SPLIT) {
-        hc[(lf * C + v) * QF2 + c] = (R)hi;
-        hc[(lf * C + NV + v) * QF2 + c] = (R)hv;
+      if constexpr (sizeof(R) == sizeof(float)) {
+        // float32 fluxes of the mixed-precision face kernel
+        const R hi = skip_inv ? R(0) : (R)si * fd.fluxI32[ki + v];
+        const R hv = visc ? -(R)si * fd.fluxV32[kv + v] : R(0);
+        if (SPLIT) {
+          hc[(lf * C + v) * QF2 + c] = hi;
+          hc[(lf * C + NV + v) * QF2 + c] = hv;
+        } else {
+          hc[(lf * C + v) * QF2 + c] = hi + hv;
+        }
       } else {
-        hc[(lf * C + v) * QF2 + c] = (R)(hi + hv);
+        const double hi = skip_inv ? 0.0 : si * fd.fluxI[ki + v];
+        const double hv = visc ? -si * fd.fluxV[kv + v] : 0.0;
+        if (SPLIT) {
+          hc[(lf * C + v) * QF2 + c] = (R)hi;
+          hc[(lf * C + NV + v) * QF2 + c] = (R)hv;
+        } else {
+          hc[(lf * C + v) * QF2 + c] = (R)(hi + hv);
+        }
       }
     }
   }
