@@ -168,6 +168,31 @@ int dgb_subcell_face_metrics(const double* vertices, int count, int num_vertices
                              const int32_t* face_sizes, int num_faces, const double* centers, int num_subcells,
                              const int32_t* owners, const int32_t* neighbors, double* normals, double* areas,
                              double* face_centers);
+
+/* (set-up, host threads, no GPU) Face pairing of one face type (hybrid/mesh.py:378-459: every
+ * (block, cell, local face) is visited in order and equal sorted corner keys are paired).  keys
+ * [n][k] are the visits' sorted corner ids, visit [n] their distinct visiting order.  Writes the
+ * faces in the reference's order, internal faces by their second visit and then boundary faces by
+ * their first: owner[f] (the first visit's row), neighbor[f] (the second visit's row, -1 at the
+ * boundary), *count faces (at most n).  A key visited more than twice is DGB_ERR_ARGUMENT with
+ * the reference's message. */
+int dgb_pair_faces(const int64_t* keys, int k, int64_t n, const int64_t* visit, int64_t* owner, int64_t* neighbor,
+                   int64_t* count);
+/* (set-up, host, no GPU) Numeric sections of Gmsh ASCII meshes (the reference reads them with
+ * meshio, hybrid/mesh.py:182-236).  text/len: the section body after its "$Nodes" or "$Elements"
+ * line.  MSH 2.2: dgb_msh2_nodes reads n records "id x y z" into ids [n], xyz [n][3];
+ * dgb_msh2_elements reads n records "id type ntags tags... nodes..." into type [n], phys [n] (the
+ * first tag, 0 without tags) and node ids nodes [cap] with offsets [n + 1].  MSH 4.1 (the body
+ * starts with the section's count line): dgb_msh4_nodes reads the entity blocks' node tags and
+ * coordinates (parametric coordinates skipped); dgb_msh4_elements gives each element its type,
+ * its entity's dimension and tag, and its node ids.  Malformed records, counts that disagree with
+ * the header and node lists beyond cap are DGB_ERR_ARGUMENT. */
+int dgb_msh2_nodes(const char* text, int64_t len, int64_t n, int64_t* ids, double* xyz);
+int dgb_msh2_elements(const char* text, int64_t len, int64_t n, int32_t* type, int32_t* phys, int64_t* offsets,
+                      int64_t* nodes, int64_t cap);
+int dgb_msh4_nodes(const char* text, int64_t len, int64_t n, int64_t* ids, double* xyz);
+int dgb_msh4_elements(const char* text, int64_t len, int64_t n, int32_t* type, int32_t* entity_dim,
+                      int32_t* entity_tag, int64_t* offsets, int64_t* nodes, int64_t cap);
 /* Optional sum-factorised path for a mesh of one hexahedron block (hexahedron bases are
  * tensor products of the 1-D Lagrange basis on the nodes 0, 1, interior: hybrid/elements.py:
  * 199-274, 325-456).  line_tables: 173 doubles, in order bq[5][4], dq[5][4] (1-D basis and

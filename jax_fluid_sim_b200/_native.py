@@ -16,6 +16,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libdgb200.so"
 c_int, c_double, c_void_p = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
 P_double = ctypes.POINTER(ctypes.c_double)
 P_int32 = ctypes.POINTER(ctypes.c_int32)
+P_int64 = ctypes.POINTER(ctypes.c_int64)
 
 
 class Params(ctypes.Structure):
@@ -141,6 +142,13 @@ def lib():
             "dgb_subcell_face_metrics": [P_double, c_int, c_int, P_int32, P_int32, c_int, P_double, c_int, P_int32,
                                          P_int32, P_double, P_double, P_double],
             "dgb_affine_test": [P_double, c_int, c_int, c_double, ctypes.POINTER(ctypes.c_uint8), P_double],
+            "dgb_pair_faces": [P_int64, c_int, ctypes.c_int64, P_int64, P_int64, P_int64, P_int64],
+            "dgb_msh2_nodes": [ctypes.c_char_p, ctypes.c_int64, ctypes.c_int64, P_int64, P_double],
+            "dgb_msh2_elements": [ctypes.c_char_p, ctypes.c_int64, ctypes.c_int64, P_int32, P_int32, P_int64,
+                                  P_int64, ctypes.c_int64],
+            "dgb_msh4_nodes": [ctypes.c_char_p, ctypes.c_int64, ctypes.c_int64, P_int64, P_double],
+            "dgb_msh4_elements": [ctypes.c_char_p, ctypes.c_int64, ctypes.c_int64, P_int32, P_int32, P_int32,
+                                  P_int64, P_int64, ctypes.c_int64],
             "dgb_map_metrics": [P_double, P_int32, c_int, c_int, P_double, c_int, P_double, P_double, P_double,
                                 P_double, P_double, P_double, P_double, P_double, P_double],
             "dgb_plan_destroy": [c_void_p],
@@ -208,6 +216,50 @@ def affine_test(J, tol):
     mean = np.empty((E, 9))
     check(lib().dgb_affine_test(dptr(J), E, J.shape[1], float(tol), dptr(affine, ctypes.c_uint8), dptr(mean)))
     return affine, mean
+
+
+def pair_faces(keys, visit):
+    """(owner rows, neighbour rows, -1 at the boundary) of the faces of one face type, in the
+    reference's face order, from the visits' sorted corner keys (n, k) and visiting order (n,)
+    (``dgb_pair_faces``, host threads)."""
+    keys = np.ascontiguousarray(keys, np.int64)
+    visit = np.ascontiguousarray(visit, np.int64)
+    n, k = keys.shape
+    owner = np.empty(max(n, 1), np.int64)
+    neighbor = np.empty(max(n, 1), np.int64)
+    count = ctypes.c_int64(0)
+    check(lib().dgb_pair_faces(dptr(keys, ctypes.c_int64), k, n, dptr(visit, ctypes.c_int64),
+                               dptr(owner, ctypes.c_int64), dptr(neighbor, ctypes.c_int64), ctypes.byref(count)))
+    return owner[:count.value], neighbor[:count.value]
+
+
+def msh_nodes(body, count, version):
+    """(node ids (n,), coordinates (n, 3)) of a Gmsh ASCII $Nodes section body (bytes after the
+    "$Nodes" line; for MSH 2.2 after the count line): ``dgb_msh2_nodes`` / ``dgb_msh4_nodes``."""
+    ids = np.empty(max(count, 1), np.int64)
+    xyz = np.empty((max(count, 1), 3))
+    fn = lib().dgb_msh2_nodes if version == 2 else lib().dgb_msh4_nodes
+    check(fn(body, len(body), count, dptr(ids, ctypes.c_int64), dptr(xyz)))
+    return ids[:count], xyz[:count]
+
+
+def msh_elements(body, count, version, cap):
+    """Element records of a Gmsh ASCII $Elements section body, at most cap node ids in all: MSH 2.2
+    (type, physical tag, offsets, node ids); MSH 4.1 (type, entity dimension, entity tag, offsets,
+    node ids) (``dgb_msh2_elements`` / ``dgb_msh4_elements``)."""
+    n = max(count, 1)
+    cap = max(int(cap), 1)
+    t, a, b = (np.empty(n, np.int32) for _ in range(3))
+    offsets = np.empty(n + 1, np.int64)
+    nodes = np.empty(cap, np.int64)
+    P32, P64 = ctypes.c_int32, ctypes.c_int64
+    if version == 2:
+        check(lib().dgb_msh2_elements(body, len(body), count, dptr(t, P32), dptr(a, P32), dptr(offsets, P64),
+                                      dptr(nodes, P64), cap))
+        return t[:count], a[:count], offsets[:count + 1], nodes[:offsets[count]]
+    check(lib().dgb_msh4_elements(body, len(body), count, dptr(t, P32), dptr(a, P32), dptr(b, P32),
+                                  dptr(offsets, P64), dptr(nodes, P64), cap))
+    return t[:count], a[:count], b[:count], offsets[:count + 1], nodes[:offsets[count]]
 
 
 def as_f64(a):

@@ -20,7 +20,7 @@ LIB = PKG / "libdgb200.so"
 OBJ = PKG / "_build"
 SOURCES = [PKG / "csrc" / "capi.cu", PKG / "csrc" / "tc_volume.cu",
            PKG / "csrc" / "noalloc.cu", PKG / "csrc" / "chemistry.cu", PKG / "csrc" / "raster.cu",
-           PKG / "csrc" / "setup.cpp"]
+           PKG / "csrc" / "setup.cpp", PKG / "csrc" / "mesh_io.cpp"]
 HEADERS = sorted((PKG / "csrc").glob("*.cuh")) + sorted((PKG / "csrc").glob("*.h")) + [ROOT / "include" / "dgb200.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -16,6 +16,7 @@ from pathlib import Path
 
 import numpy as np
 
+from . import _native
 from .meshgen import MeshSource
 
 # Gmsh element type -> (cell type name, corner count, total node count)
@@ -70,19 +71,27 @@ def gmsh_to_meshio(ctype):
 _ORDER = ("hexahedron", "hexahedron27", "wedge", "wedge18", "tetra", "tetra10", "quad", "triangle")
 
 
-def _sections(lines):
-    out, i = {}, 0
-    while i < len(lines):
-        line = lines[i].strip()
-        if line.startswith("$") and not line.startswith("$End"):
-            name = line[1:]
-            j = i + 1
-            while not lines[j].strip().startswith("$End" + name):
-                j += 1
-            out[name] = lines[i + 1:j]
-            i = j
-        i += 1
+def _ascii_sections(data):
+    """{name: body bytes} of an ASCII mesh: the bytes between a "$Name" line and its "$EndName"."""
+    out, pos, n = {}, 0, len(data)
+    while pos < n:
+        eol = data.find(b"\n", pos)
+        eol = n if eol < 0 else eol
+        line = data[pos:eol].strip()
+        if line.startswith(b"$") and not line.startswith(b"$End"):
+            tag = b"\n$End" + line[1:]
+            end = data.find(tag, eol)
+            if end < 0:
+                raise ValueError(f"section {line.decode('ascii', 'replace')} has no end")
+            out[line[1:].decode("ascii", "replace")] = data[eol + 1:end + 1]
+            eol = data.find(b"\n", end + 1)
+            eol = n if eol < 0 else eol
+        pos = eol + 1
     return out
+
+
+def _lines(body):
+    return body.decode("ascii", "replace").splitlines() if body is not None else None
 
 
 def _physical_names(sec):
@@ -117,25 +126,41 @@ def _assemble(points, node_index, records):
     return cells, phys
 
 
-def _read_v2(sec, field):
-    nodes = np.array([line.split() for line in sec["Nodes"][1:1 + int(sec["Nodes"][0])]], dtype=np.float64)
-    ids = nodes[:, 0].astype(np.int64)
+def _records(etype, phys, offsets, nodes):
+    """(gmsh type, physical tag, node ids (n, k)) per (type, tag) pair in the order the pairs first
+    appear, each pair's elements in file order."""
+    key = (etype.astype(np.int64) << 32) | (phys.astype(np.int64) & 0xFFFFFFFF)
+    _, first, inv = np.unique(key, return_index=True, return_inverse=True)
+    out = []
+    for g in np.argsort(first, kind="stable"):
+        rows = np.flatnonzero(inv == g)
+        k = offsets[rows + 1] - offsets[rows]
+        if np.any(k != k[0]):
+            raise ValueError(f"Gmsh element type {int(etype[rows[0]])} has records of different lengths")
+        out.append((int(etype[rows[0]]), int(phys[rows[0]]), nodes[offsets[rows][:, None] + np.arange(k[0])]))
+    return out
+
+
+def _node_index(ids):
     index = np.full(ids.max() + 1, -1, np.int64)
     index[ids] = np.arange(len(ids))
-    by_shape = {}
-    for line in sec["Elements"][1:1 + int(sec["Elements"][0])]:
-        v = [int(x) for x in line.split()]
-        etype, ntags = v[1], v[2]
-        phys = v[3] if ntags > 0 else 0
-        by_shape.setdefault((etype, phys), []).append(v[3 + ntags:])
-    records = [(t, p, np.asarray(n, np.int64)) for (t, p), n in by_shape.items()]
-    return nodes[:, 1:4], index, records
+    return index
 
 
-def _read_v4(sec, field):
-    # $Entities: physical tags of each (dim, entity)
+def _read_v2(sec):
+    """MSH 2.2 ASCII: the node and element records parsed on the host (``dgb_msh2_*``)."""
+    head, _, body = sec["Nodes"].partition(b"\n")
+    ids, xyz = _native.msh_nodes(body, int(head), 2)
+    head, _, body = sec["Elements"].partition(b"\n")
+    etype, phys, offsets, nodes = _native.msh_elements(body, int(head), 2, len(body) // 2 + 1)
+    return xyz, _node_index(ids), _records(etype, phys, offsets, nodes)
+
+
+def _read_v4(sec):
+    """MSH 4.1 ASCII: the entities' physical tags here, the node and element blocks parsed on the
+    host (``dgb_msh4_*``)."""
     phys_of = {}
-    ent = sec.get("Entities")
+    ent = _lines(sec.get("Entities"))
     if ent:
         counts = [int(x) for x in ent[0].split()]
         row = 1
@@ -147,31 +172,16 @@ def _read_v4(sec, field):
                 nfix = 4 if dim == 0 else 7              # point: tag x y z; others: tag + bounding box
                 nphys = int(v[nfix])
                 phys_of[(dim, tag)] = int(v[nfix + 1]) if nphys > 0 else 0
-    head = [int(x) for x in sec["Nodes"][0].split()]
-    nblocks, row = head[0], 1
-    tags_all, xyz_all = [], []
-    for _ in range(nblocks):
-        _, _, parametric, count = (int(x) for x in sec["Nodes"][row].split())
-        row += 1
-        tags_all.append(np.asarray([int(sec["Nodes"][row + k]) for k in range(count)], np.int64))
-        row += count
-        xyz = np.array([sec["Nodes"][row + k].split() for k in range(count)], dtype=np.float64).reshape(count, -1)
-        xyz_all.append(xyz[:, :3])
-        row += count
-    ids = np.concatenate(tags_all)
-    index = np.full(ids.max() + 1, -1, np.int64)
-    index[ids] = np.arange(len(ids))
-    head = [int(x) for x in sec["Elements"][0].split()]
-    nblocks, row = head[0], 1
-    by_shape = {}
-    for _ in range(nblocks):
-        dim, tag, etype, count = (int(x) for x in sec["Elements"][row].split())
-        row += 1
-        data = np.array([sec["Elements"][row + k].split() for k in range(count)], dtype=np.int64)
-        row += count
-        by_shape.setdefault((etype, phys_of.get((dim, tag), 0)), []).append(data[:, 1:])
-    records = [(t, p, np.concatenate(n)) for (t, p), n in by_shape.items()]
-    return np.concatenate(xyz_all), index, records
+    body = sec["Nodes"]
+    ids, xyz = _native.msh_nodes(body, int(body.split(None, 2)[1]), 4)
+    body = sec["Elements"]
+    etype, edim, etag, offsets, nodes = _native.msh_elements(body, int(body.split(None, 2)[1]), 4,
+                                                             len(body) // 2 + 1)
+    ent_key = (edim.astype(np.int64) << 32) | (etag.astype(np.int64) & 0xFFFFFFFF)
+    uniq, inv = np.unique(ent_key, return_inverse=True)
+    phys = np.asarray([phys_of.get((int(u >> 32), int(np.int32(u & 0xFFFFFFFF))), 0) for u in uniq],
+                      np.int32)[inv] if len(uniq) else np.zeros(0, np.int32)
+    return xyz, _node_index(ids), _records(etype, phys, offsets, nodes)
 
 
 def _node_count(etype):
@@ -267,16 +277,15 @@ def read_msh(path, periodic_map=None):
         points, index, records, field = _read_v2_binary(data)
         cells, phys = _assemble(points, index, records)
         return MeshSource(points, cells, phys, field, periodic_map)
-    lines = data.decode("ascii", "replace").splitlines()
-    sec = _sections(lines)
+    sec = _ascii_sections(data)
     if "MeshFormat" not in sec:
         raise ValueError(f"{path} is not a Gmsh mesh")
-    version, binary = sec["MeshFormat"][0].split()[:2]
-    field = _physical_names(sec.get("PhysicalNames"))
+    version, binary = _lines(sec["MeshFormat"])[0].split()[:2]
+    field = _physical_names(_lines(sec.get("PhysicalNames")))
     if version.startswith("2"):
-        points, index, records = _read_v2(sec, field)
+        points, index, records = _read_v2(sec)
     elif version.startswith("4"):
-        points, index, records = _read_v4(sec, field)
+        points, index, records = _read_v4(sec)
     else:
         raise NotImplementedError(f"MSH version {version}")
     cells, phys = _assemble(points, index, records)

@@ -5,8 +5,9 @@ element blocks are ordered hexahedron -> wedge -> tetra; a face's owner is
 the first (block, cell, local face) in that visiting order; internal faces are
 listed in the order their second visitor arrives, boundary faces afterwards in
 first-visit order; the face normal comes from the owner's corners and points
-toward the neighbour centre.  The pairing here is done with one sort instead of
-a Python dictionary walk, and reproduces the reference's face order exactly.
+toward the neighbour centre.  The pairing is one parallel sort of the visits by
+(sorted corner key, visit) on the host cores (``dgb_pair_faces``) instead of a
+Python dictionary walk, and reproduces the reference's face order exactly.
 
 Periodicity (not in the reference): ``MeshSource.periodic_map`` gives each
 point a canonical id used for face keys and neighbour alignment.
@@ -17,6 +18,7 @@ from pathlib import Path
 
 import numpy as np
 
+from . import _native
 from .meshgen import MeshSource
 from .reference import LOCAL_FACES
 
@@ -177,32 +179,12 @@ class HybridMesh:
                 continue
             blk, loc, lface, nodes, visit = (np.concatenate([r[i] for r in recs[k]]) for i in range(5))
             key = np.sort(self.canon[nodes], axis=1)
-            # group equal keys together, visits in order within a group
-            srt = np.lexsort((visit,) + tuple(key[:, j] for j in range(k - 1, -1, -1)))
-            ks = key[srt]
-            new_group = np.ones(len(ks), bool)
-            new_group[1:] = np.any(ks[1:] != ks[:-1], axis=1)
-            gid = np.cumsum(new_group) - 1
-            count = np.bincount(gid)
-            if np.any(count > 2):
-                raise ValueError("A face is shared by more than two cells")
-            first = srt[new_group]
-            second = np.full(len(first), -1)
-            pairs = np.flatnonzero(~new_group)
-            second[gid[pairs]] = srt[pairs]
-            internal = second >= 0
-            # internal faces ordered by the second visit, boundary faces by the first
-            sort_key = np.where(internal, visit[np.maximum(second, 0)], 0)
-            i_idx = np.flatnonzero(internal)
-            i_idx = i_idx[np.argsort(sort_key[i_idx], kind="stable")]
-            b_idx = np.flatnonzero(~internal)
-            b_idx = b_idx[np.argsort(visit[first[b_idx]], kind="stable")]
-            sel = np.concatenate([i_idx, b_idx])
-            own, nbr = first[sel], second[sel]
+            # pairs equal keys; faces in the reference's order (host threads)
+            own, nbr = _native.pair_faces(key, visit)
             has_n = nbr >= 0
             nbr_c = np.where(has_n, nbr, 0)
             fnodes = nodes[own]
-            tags = np.full(len(sel), -1, np.int32)
+            tags = np.full(len(own), -1, np.int32)
             bkeys = key[own[~has_n]]
             tags[~has_n] = [boundary_tags.get(tuple(r), -1) for r in bkeys.tolist()]
             ob, ol = blk[own].astype(np.int32), loc[own].astype(np.int32)
