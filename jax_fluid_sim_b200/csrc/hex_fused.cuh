@@ -266,6 +266,25 @@ __device__ __forceinline__ int rotated(int offset) {
   return (int)((threadIdx.x + blockDim.x - (unsigned)offset % blockDim.x) % blockDim.x);
 }
 
+// K (even) consecutive shared-memory values at p into r by float2 / double2 loads (p 8-byte aligned
+// for float, 16-byte aligned for double).
+template <int K, typename T>
+__device__ __forceinline__ void lds_pairs(const T* p, T* r) {
+  static_assert(K % 2 == 0, "lds_pairs loads pairs");
+#pragma unroll
+  for (int k = 0; k < K / 2; ++k) {
+    if constexpr (sizeof(T) == sizeof(float)) {
+      const float2 v = reinterpret_cast<const float2*>(p)[k];
+      r[2 * k] = v.x;
+      r[2 * k + 1] = v.y;
+    } else {
+      const double2 v = reinterpret_cast<const double2*>(p)[k];
+      r[2 * k] = v.x;
+      r[2 * k + 1] = v.y;
+    }
+  }
+}
+
 // The three reference-gradient fields of C nodal channels at the Q^3 volume points,
 // g[r][c][Q3] = (d/dxi_r of the interpolant), by the sum-factorised passes with the intermediates
 // shared between directions: x (bq, dq), y (bq, dq on the bq branch; bq on the dq branch), z.  Each
@@ -359,7 +378,9 @@ struct HexElemSmem {
   // table size in R, rounded up to 16 bytes so that the arrays after the tables stay 16-byte aligned
   static constexpr int T = (int)((sizeof(HexTablesT<R>) + 15) / 16 * 16 / sizeof(R));
   static constexpr int C = SPLIT ? 2 * NV : NV;          // residual channels
-  static constexpr int U = T, V = U + NV * N3, LF = V + 4 * N3, RR = LF + 12 * N3, W = RR + C * N3;
+  static constexpr int U = T, V = U + NV * N3, LF = V + 4 * N3, RR = LF + 12 * N3;
+  // the phase scratch starts on a 16-byte boundary (N3 = 27 leaves RR + C N3 odd)
+  static constexpr int W = (RR + C * N3 + 3) / 4 * 4;
   // phase scratch (aliased)
   static constexpr int LIFT = 72 * QF2 + 72 * QF * N + 72 * N2 + 12 * N3 + 3 * 12 * N3;
   // phase C: uq [NV][Q3], gq [12][Q3], then the lift at the points lq [12][Q3] (later Gi, Gv [3][NV][Q3]
@@ -482,7 +503,8 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
         hex_face_axes(lf, a0, end, a1, a2);
         if (xyz[a0] == end) acc += bs[(lf * 12 + c) * N2 + xyz[a2] * N + xyz[a1]];
       }
-      ball[idx] = acc;
+      // non-affine elements: node-major rows [N3][12] for the dense M^-1 (pair loads per node)
+      ball[aff ? idx : l * 12 + c] = acc;
     }
     __syncthreads();
     if (aff) {
@@ -498,8 +520,10 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
           for (int j = 0; j < N3; ++j) {
             const R m = (R)__ldg(M + (size_t)j * N3 + i);
             const int lj = node2lex[j];
+            R bj[6];
+            lds_pairs<6>(ball + lj * 12 + c0, bj);
 #pragma unroll
-            for (int k = 0; k < 6; ++k) sacc[k] += m * ball[(c0 + k) * N3 + lj];
+            for (int k = 0; k < 6; ++k) sacc[k] += m * bj[k];
           }
           const int li = node2lex[i];
 #pragma unroll
@@ -658,6 +682,12 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
   }
   __syncthreads();
   tensor2<6 * C, QF, QF, N, N>(hc, hs, tmp, tb->bfT, tb->bfT);
+  // non-affine elements: the residuals go to node-major rows RrT [N3][CS] (inviscid channels, then
+  // from CSH the viscous ones) in the dead hc/tmp region, for pair loads in the dense M^-1
+  constexpr int CSH = (NV + 1) / 2 * 2;
+  constexpr int CS = SPLIT ? 2 * CSH : CSH;
+  static_assert(CS * N3 <= 6 * C * (QF2 + QF * N), "the residual rows must end before hs");
+  R* RrT = W;
   for (int idx = threadIdx.x; idx < C * N3; idx += blockDim.x) {
     const int c = idx / N3, l = idx % N3;
     const int xyz[3] = {l % N, (l / N) % N, l / N2};
@@ -668,7 +698,10 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
       hex_face_axes(lf, a0, end, a1, a2);
       if (xyz[a0] == end) acc += hs[(lf * C + c) * N2 + xyz[a2] * N + xyz[a1]];
     }
-    Rr[idx] = acc;
+    if (aff)
+      Rr[idx] = acc;
+    else
+      RrT[l * CS + (c < NV ? c : CSH + c - NV)] = acc;
   }
   __syncthreads();
   auto emit = [&](size_t o, double ri, double rv) {
@@ -698,6 +731,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
   constexpr int NG = (NV + VB - 1) / VB;
   constexpr int HALVES = NG * N3 * 2 <= kThreads ? 2 : 1;
   constexpr int JH = (N3 + HALVES - 1) / HALVES;
+  constexpr int KP = (VB + 1) / 2 * 2;
   R* part = hs;                                       // [HALVES][2][NV][N3]
   auto apply = [&](const auto* M) {
     for (int idx = threadIdx.x; idx < HALVES * NG * N3; idx += blockDim.x) {
@@ -711,11 +745,14 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
       for (int j = h * JH; j < j1; ++j) {
         const R m = (R)__ldg(M + (size_t)j * N3 + i);
         const int lj = node2lex[j];
+        R xi[KP], xv[KP];
+        lds_pairs<KP>(RrT + lj * CS + v0, xi);
+        if (SPLIT) lds_pairs<KP>(RrT + lj * CS + CSH + v0, xv);
 #pragma unroll
         for (int k = 0; k < VB; ++k) {
           if (v0 + k < NV) {
-            ri[k] += m * Rr[(v0 + k) * N3 + lj];
-            if (SPLIT) rv[k] += m * Rr[(NV + v0 + k) * N3 + lj];
+            ri[k] += m * xi[k];
+            if (SPLIT) rv[k] += m * xv[k];
           }
         }
       }
