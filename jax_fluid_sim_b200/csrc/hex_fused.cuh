@@ -97,10 +97,10 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 6 : 1) k_hex_face(const De
   constexpr int N = D::N, QF = D::QF, QF2 = D::QF2;
   constexpr int FPC = kThreads / QF2;                // faces per CTA
   constexpr bool RF = sizeof(R) == sizeof(float);    // float32 face fluxes and jumps (mixed precision)
-  // jumps of each face's points, [face][point][12]; the face stride is padded by two doubles so
-  // that the faces sharing a warp read different banks
-  constexpr int JS = QF2 * 12 + 2;
-  __shared__ R jmp[FPC * JS];
+  // jumps of each face's points, [face][point][12]; the face stride is padded to a 16-byte
+  // multiple (two doubles or four floats) so that a point's 12 jumps are read by 16-byte loads
+  constexpr int JS = QF2 * 12 + (sizeof(R) == sizeof(float) ? 4 : 2);
+  __shared__ __align__(16) R jmp[FPC * JS];
   __shared__ R K[QF][QF];                            // bf m1i bf^T
   const FaceDev& fd = P_.face[1];
   const int slot = threadIdx.x / QF2, q = threadIdx.x % QF2;
@@ -198,6 +198,35 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 6 : 1) k_hex_face(const De
     const uint8_t* perm = codes.perm + (size_t)code * QF2;
     const int lf = A.face_lf[(size_t)f * 2 + s];
     const int cq = perm[q];
+    // the side's face-point permutation in registers (one 16-byte load for P3 faces), so that the
+    // operator loads of the lift loop do not wait on the permutation loads one by one
+    unsigned wd[4] = {0u, 0u, 0u, 0u};
+    if constexpr (QF2 == 16) {
+      const uint4 raw = __ldg(reinterpret_cast<const uint4*>(perm));
+      wd[0] = raw.x, wd[1] = raw.y, wd[2] = raw.z, wd[3] = raw.w;
+    }
+    auto pm = [&](int k) -> int {
+      if constexpr (QF2 == 16) return (int)((wd[k / 4] >> (8 * (k % 4))) & 0xFFu);
+      else return perm[k];
+    };
+    // the 12 jumps of face point qp (16-byte loads from the padded rows)
+    auto jrow = [&](int qp, R* r) {
+      if constexpr (sizeof(R) == sizeof(float)) {
+        const float4* p4 = reinterpret_cast<const float4*>(jf + qp * 12);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const float4 v = p4[k];
+          r[4 * k] = v.x, r[4 * k + 1] = v.y, r[4 * k + 2] = v.z, r[4 * k + 3] = v.w;
+        }
+      } else {
+        const double2* p2 = reinterpret_cast<const double2*>(jf + qp * 12);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+          const double2 v = p2[k];
+          r[2 * k] = v.x, r[2 * k + 1] = v.y;
+        }
+      }
+    };
     R lift[12];
 #pragma unroll
     for (int c = 0; c < 12; ++c) lift[c] = R(0);
@@ -208,22 +237,28 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 6 : 1) k_hex_face(const De
       hex_face_axes(lf, a0, end, a1, a2);
       const R scale = (R)(P_.ph.br2 * B.acoef[e] * tables.m1i[end * N + end]);
       const int c1 = cq % QF, c2 = cq / QF;
-      for (int qp = 0; qp < QF2; ++qp) {
-        const int cp = perm[qp];
-        const R kk = K[c1][cp % QF] * K[c2][cp / QF];
 #pragma unroll
-        for (int c = 0; c < 12; ++c) lift[c] += kk * jf[qp * 12 + c];
+      for (int qp = 0; qp < QF2; ++qp) {
+        const int cp = pm(qp);
+        const R kk = K[c1][cp % QF] * K[c2][cp / QF];
+        R jv[12];
+        jrow(qp, jv);
+#pragma unroll
+        for (int c = 0; c < 12; ++c) lift[c] += kk * jv[c];
       }
 #pragma unroll
       for (int c = 0; c < 12; ++c) lift[c] *= scale;
     } else {
       const size_t lo = ((size_t)li * 6 + lf) * QF2 * QF2 + (size_t)cq * QF2;
+#pragma unroll
       for (int qp = 0; qp < QF2; ++qp) {
         R kk;
-        if constexpr (sizeof(R) == sizeof(float)) kk = __ldg(A.lop32 + lo + perm[qp]);
-        else kk = (R)__ldg(A.lop + lo + perm[qp]);
+        if constexpr (sizeof(R) == sizeof(float)) kk = __ldg(A.lop32 + lo + pm(qp));
+        else kk = (R)__ldg(A.lop + lo + pm(qp));
+        R jv[12];
+        jrow(qp, jv);
 #pragma unroll
-        for (int c = 0; c < 12; ++c) lift[c] += kk * jf[qp * 12 + c];
+        for (int c = 0; c < 12; ++c) lift[c] += kk * jv[c];
       }
 #pragma unroll
       for (int c = 0; c < 12; ++c) lift[c] *= (R)P_.ph.br2;
