@@ -342,9 +342,32 @@ __global__ void __launch_bounds__(kThreads) k_hex_traces(const DevPlan P_, const
   }
   __syncthreads();
   if (visc) {
-    tensor2<CH, N, N, QF, QF>(slabs, fo, ftmp, tb->bf, tb->bf);
-    tensor2<24, N, N, QF, QF>(slabs + 6 * NV * N2, g1, ftmp, tb->df, tb->bf);
-    tensor2<24, N, N, QF, QF>(slabs + 6 * NV * N2, g2, ftmp, tb->bf, tb->df);
+    if constexpr ((NV + 4) * N3 >= 24 * N * QF) {
+      // The three face contractions with two barriers instead of six: the x-passes (bf on every
+      // channel; df on the 24 v channels, into the U/V region, dead after the slab gather), then the
+      // y-passes (bf -> fo; bf on the df pass -> g1; df on the bf pass of the v channels -> g2).  Each
+      // output goes through the same two 1-D products as in three tensor2 calls.  Consecutive passes
+      // start on rotated threads so that the lines spread evenly.
+      R* xd = U;                                   // [24][N][QF]
+      const R* vsl = slabs + 6 * NV * N2;
+      const int st = blockDim.x;
+      auto rot = [st](int off) { return (int)((threadIdx.x + st - off % st) % st); };
+      auto i1 = [](int l) { return l * N; };
+      auto o1 = [](int l) { return l * QF; };
+      pencil<N, QF, false>(slabs, ftmp, tb->bf, CH * N, 1, 1, i1, o1, rot(0), st);
+      pencil<N, QF, false>(vsl, xd, tb->df, 24 * N, 1, 1, i1, o1, rot(CH * N), st);
+      __syncthreads();
+      auto i2 = [](int l) { return (l / QF) * N * QF + l % QF; };
+      auto o2 = [](int l) { return (l / QF) * QF * QF + l % QF; };
+      pencil<N, QF, false>(ftmp, fo, tb->bf, CH * QF, QF, QF, i2, o2, rot(0), st);
+      pencil<N, QF, false>(xd, g1, tb->bf, 24 * QF, QF, QF, i2, o2, rot(CH * QF), st);
+      pencil<N, QF, false>(ftmp + 6 * NV * N * QF, g2, tb->df, 24 * QF, QF, QF, i2, o2, rot(CH * QF + 24 * QF), st);
+      __syncthreads();
+    } else {
+      tensor2<CH, N, N, QF, QF>(slabs, fo, ftmp, tb->bf, tb->bf);
+      tensor2<24, N, N, QF, QF>(slabs + 6 * NV * N2, g1, ftmp, tb->df, tb->bf);
+      tensor2<24, N, N, QF, QF>(slabs + 6 * NV * N2, g2, ftmp, tb->bf, tb->df);
+    }
   } else {
     tensor2<6 * NV, N, N, QF, QF>(slabs, fo, ftmp, tb->bf, tb->bf);
   }
