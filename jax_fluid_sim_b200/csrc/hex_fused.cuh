@@ -301,23 +301,21 @@ __device__ __forceinline__ int rotated(int offset) {
   return (int)((threadIdx.x + blockDim.x - (unsigned)offset % blockDim.x) % blockDim.x);
 }
 
-// K (even) consecutive shared-memory values at p into r by float2 / double2 loads (p 8-byte aligned
-// for float, 16-byte aligned for double).
+// K consecutive shared-memory values at p (16-byte aligned) into r: 16-byte loads, then an 8-byte
+// load of a float pair, then single values.
 template <int K, typename T>
-__device__ __forceinline__ void lds_pairs(const T* p, T* r) {
-  static_assert(K % 2 == 0, "lds_pairs loads pairs");
+__device__ __forceinline__ void lds_vec(const T* p, T* r) {
+  constexpr int VA = 16 / sizeof(T), K16 = K / VA * VA;
 #pragma unroll
-  for (int k = 0; k < K / 2; ++k) {
-    if constexpr (sizeof(T) == sizeof(float)) {
-      const float2 v = reinterpret_cast<const float2*>(p)[k];
-      r[2 * k] = v.x;
-      r[2 * k + 1] = v.y;
-    } else {
-      const double2 v = reinterpret_cast<const double2*>(p)[k];
-      r[2 * k] = v.x;
-      r[2 * k + 1] = v.y;
-    }
+  for (int k = 0; k < K16; k += VA) load16(p + k, r + k);
+  constexpr int K8 = (sizeof(T) == sizeof(float) && K - K16 >= 2) ? K16 + 2 : K16;
+  if constexpr (K8 > K16) {
+    const float2 v = *reinterpret_cast<const float2*>(p + K16);
+    r[K16] = v.x;
+    r[K16 + 1] = v.y;
   }
+#pragma unroll
+  for (int k = K8; k < K; ++k) r[k] = p[k];
 }
 
 // The three reference-gradient fields of C nodal channels at the Q^3 volume points,
@@ -501,6 +499,10 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
     R* bs = tmp + CH * QF * N;        // [6][12][N2]
     R* ball = bs + CH * N2;           // [12][N3]
     R* ax = ball + 12 * N3;           // affine scratch [3][12][N3]
+    // dense-lift row groups of the non-affine elements: 6 channels padded to 16 bytes; the rows
+    // (2 LR N3 values) reach into ax, which only affine elements use
+    constexpr int LR = (6 * (int)sizeof(R) + 15) / 16 * 16 / (int)sizeof(R);
+    static_assert(2 * LR <= 48, "the dense-lift rows must fit in ball and ax");
     // one face point per thread: its 12 jump components (contiguous) to the canonical point
     for (int it = threadIdx.x; it < 6 * QF2; it += blockDim.x) {
       const int lf = it / QF2, q = it % QF2;
@@ -538,8 +540,9 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
         hex_face_axes(lf, a0, end, a1, a2);
         if (xyz[a0] == end) acc += bs[(lf * 12 + c) * N2 + xyz[a2] * N + xyz[a1]];
       }
-      // non-affine elements: node-major rows [N3][12] for the dense M^-1 (pair loads per node)
-      ball[aff ? idx : l * 12 + c] = acc;
+      // non-affine elements: rows of two 16-byte aligned groups of 6 channels (LR apart) in element
+      // node order, for 16-byte loads in the dense M^-1 (summed in node order)
+      ball[aff ? idx : tb->lex2node[l] * 2 * LR + (c / 6) * LR + c % 6] = acc;
     }
     __syncthreads();
     if (aff) {
@@ -549,14 +552,13 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
     } else {
       auto dense_lift = [&](const auto* M) {
         for (int idx = threadIdx.x; idx < 2 * N3; idx += blockDim.x) {
-          const int i = idx % N3, c0 = (idx / N3) * 6;
+          const int i = idx % N3, g = idx / N3, c0 = g * 6;
           R sacc[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
 #pragma unroll 4
           for (int j = 0; j < N3; ++j) {
             const R m = (R)__ldg(M + (size_t)j * N3 + i);
-            const int lj = node2lex[j];
             R bj[6];
-            lds_pairs<6>(ball + lj * 12 + c0, bj);
+            lds_vec<6>(ball + j * 2 * LR + g * LR, bj);
 #pragma unroll
             for (int k = 0; k < 6; ++k) sacc[k] += m * bj[k];
           }
@@ -717,9 +719,10 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
   }
   __syncthreads();
   tensor2<6 * C, QF, QF, N, N>(hc, hs, tmp, tb->bfT, tb->bfT);
-  // non-affine elements: the residuals go to node-major rows RrT [N3][CS] (inviscid channels, then
-  // from CSH the viscous ones) in the dead hc/tmp region, for pair loads in the dense M^-1
-  constexpr int CSH = (NV + 1) / 2 * 2;
+  // non-affine elements: the residuals go to rows RrT [N3][CS] in element node order (inviscid
+  // channels, then from CSH the viscous ones) in the dead hc/tmp region, for pair loads in the
+  // dense M^-1
+  constexpr int CSH = (NV + 16 / (int)sizeof(R) - 1) / (16 / (int)sizeof(R)) * (16 / (int)sizeof(R));
   constexpr int CS = SPLIT ? 2 * CSH : CSH;
   static_assert(CS * N3 <= 6 * C * (QF2 + QF * N), "the residual rows must end before hs");
   R* RrT = W;
@@ -736,7 +739,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
     if (aff)
       Rr[idx] = acc;
     else
-      RrT[l * CS + (c < NV ? c : CSH + c - NV)] = acc;
+      RrT[tb->lex2node[l] * CS + (c < NV ? c : CSH + c - NV)] = acc;
   }
   __syncthreads();
   auto emit = [&](size_t o, double ri, double rv) {
@@ -766,7 +769,6 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
   constexpr int NG = (NV + VB - 1) / VB;
   constexpr int HALVES = NG * N3 * 2 <= kThreads ? 2 : 1;
   constexpr int JH = (N3 + HALVES - 1) / HALVES;
-  constexpr int KP = (VB + 1) / 2 * 2;
   R* part = hs;                                       // [HALVES][2][NV][N3]
   auto apply = [&](const auto* M) {
     for (int idx = threadIdx.x; idx < HALVES * NG * N3; idx += blockDim.x) {
@@ -779,10 +781,9 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
 #pragma unroll 4
       for (int j = h * JH; j < j1; ++j) {
         const R m = (R)__ldg(M + (size_t)j * N3 + i);
-        const int lj = node2lex[j];
-        R xi[KP], xv[KP];
-        lds_pairs<KP>(RrT + lj * CS + v0, xi);
-        if (SPLIT) lds_pairs<KP>(RrT + lj * CS + CSH + v0, xv);
+        R xi[VB], xv[VB];
+        lds_vec<VB>(RrT + j * CS + v0, xi);
+        if (SPLIT) lds_vec<VB>(RrT + j * CS + CSH + v0, xv);
 #pragma unroll
         for (int k = 0; k < VB; ++k) {
           if (v0 + k < NV) {

@@ -389,10 +389,16 @@ __global__ void __launch_bounds__(kThreads) k_hex_traces(const DevPlan P_, const
       const int lf = it / QF2, q = it % QF2;
       const int c = codes.perm[fperm[lf] + q];
       const size_t pt = (size_t)fslot[lf] + q;
+      // a point's 4 values and 12 gradients are contiguous: 16-byte stores
+      R tv[4];
 #pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        if (F32) fd.trV32[pt * 4 + m] = (float)fv[(lf * 4 + m) * QF2 + c];
-        else fd.trV[pt * 4 + m] = (double)fv[(lf * 4 + m) * QF2 + c];
+      for (int m = 0; m < 4; ++m) tv[m] = fv[(lf * 4 + m) * QF2 + c];
+      if (F32) {
+        *reinterpret_cast<float4*>(fd.trV32 + pt * 4) = make_float4((float)tv[0], (float)tv[1], (float)tv[2], (float)tv[3]);
+      } else {
+        double2* t2 = reinterpret_cast<double2*>(fd.trV + pt * 4);
+        t2[0] = make_double2((double)tv[0], (double)tv[1]);
+        t2[1] = make_double2((double)tv[2], (double)tv[3]);
       }
       int a0, end, a1, a2;
       hex_face_axes(lf, a0, end, a1, a2);
@@ -404,6 +410,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_traces(const DevPlan P_, const
 #pragma unroll
         for (int k = 0; k < 9; ++k) J[k] = (R)fd.jinv[pt * 9 + k];
       }
+      R gout[12];
 #pragma unroll
       for (int m = 0; m < 4; ++m) {
         const int k = (lf * 4 + m) * QF2 + c;
@@ -413,11 +420,17 @@ __global__ void __launch_bounds__(kThreads) k_hex_traces(const DevPlan P_, const
         const R gy = a0 == 1 ? gnv : (a0 == 0 ? g1v : g2v);
         const R gz = a0 == 2 ? gnv : g2v;
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          const R x = gx * J[0 * 3 + d] + gy * J[1 * 3 + d] + gz * J[2 * 3 + d];
-          if (F32) fd.trG32[pt * 12 + m * 3 + d] = (float)x;
-          else fd.trG[pt * 12 + m * 3 + d] = (double)x;
-        }
+        for (int d = 0; d < 3; ++d) gout[m * 3 + d] = gx * J[0 * 3 + d] + gy * J[1 * 3 + d] + gz * J[2 * 3 + d];
+      }
+      if (F32) {
+        float4* g4 = reinterpret_cast<float4*>(fd.trG32 + pt * 12);
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+          g4[k] = make_float4((float)gout[4 * k], (float)gout[4 * k + 1], (float)gout[4 * k + 2], (float)gout[4 * k + 3]);
+      } else {
+        double2* g2d = reinterpret_cast<double2*>(fd.trG + pt * 12);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) g2d[k] = make_double2((double)gout[2 * k], (double)gout[2 * k + 1]);
       }
     }
   }
