@@ -175,15 +175,32 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 6 : 1) k_hex_face(const De
       viscous_vars<NV>(P_.ph, UL, vn);
     }
     const size_t jo = ((size_t)f * QF2 + q) * 12;
+    // a point's 12 jumps are contiguous in the face buffer and in jmp: 16-byte stores
+    R jr[12];
 #pragma unroll
     for (int m = 0; m < 4; ++m)
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        const double j = 0.5 * w * (vn[m] - vo[m]) * n[d];
-        if (RF) fd.jumpW32[jo + m * 3 + d] = (float)j;
-        else fd.jumpW[jo + m * 3 + d] = j;
-        jmp[slot * JS + q * 12 + m * 3 + d] = (R)j;
+      for (int d = 0; d < 3; ++d) jr[m * 3 + d] = (R)(0.5 * w * (vn[m] - vo[m]) * n[d]);
+    R* js = &jmp[slot * JS + q * 12];
+    if constexpr (RF) {
+      float4* g4 = reinterpret_cast<float4*>(fd.jumpW32 + jo);
+      float4* s4 = reinterpret_cast<float4*>(js);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const float4 v = make_float4(jr[4 * k], jr[4 * k + 1], jr[4 * k + 2], jr[4 * k + 3]);
+        g4[k] = v;
+        s4[k] = v;
       }
+    } else {
+      double2* g2 = reinterpret_cast<double2*>(fd.jumpW + jo);
+      double2* s2 = reinterpret_cast<double2*>(js);
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        const double2 v = make_double2(jr[2 * k], jr[2 * k + 1]);
+        g2[k] = v;
+        s2[k] = v;
+      }
+    }
   }
   __syncthreads();
   if (!live) return;
