@@ -162,12 +162,21 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 6 : 1) k_hex_face(const De
   }
   if (!P_.viscous) return;
   double vo[4], vn[4];
+  // a face point's 4 viscous values: one 16-byte load (float32) or two (float64)
+  auto load_v = [&](size_t pt, double* out) {
+    if constexpr (F32) {
+      const float4 t = __ldg(reinterpret_cast<const float4*>(fd.trV32 + pt * 4));
+      out[0] = t.x, out[1] = t.y, out[2] = t.z, out[3] = t.w;
+    } else {
+      const double2* t = reinterpret_cast<const double2*>(fd.trV + pt * 4);
+      const double2 a = t[0], b2 = t[1];
+      out[0] = a.x, out[1] = a.y, out[2] = b2.x, out[3] = b2.y;
+    }
+  };
   if (live) {
-#pragma unroll
-    for (int m = 0; m < 4; ++m) vo[m] = F32 ? (double)fd.trV32[so * 4 + m] : fd.trV[so * 4 + m];
+    load_v(so, vo);
     if (nb >= 0) {
-#pragma unroll
-      for (int m = 0; m < 4; ++m) vn[m] = F32 ? (double)fd.trV32[sn * 4 + m] : fd.trV[sn * 4 + m];
+      load_v(sn, vn);
     } else if (P_.ph.has_boundary) {
       const CaseView cv = case_view(P_.ph, P_.blk[0].ecase, fd.ol[f]);
       viscous_ghost<NV>(P_.ph, cv.far, cv.wall_T, UL, n, fd.tag[f], vn);
@@ -289,8 +298,24 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 6 : 1) k_hex_face(const De
     R U[NV], g[12];
 #pragma unroll
     for (int v = 0; v < NV; ++v) U[v] = (R)fd.trP[ss * NV + v];
+    // the point's 12 gradients: 16-byte loads
+    if constexpr (F32) {
+      const float4* t = reinterpret_cast<const float4*>(fd.trG32 + ss * 12);
 #pragma unroll
-    for (int c = 0; c < 12; ++c) g[c] = (F32 ? (R)fd.trG32[ss * 12 + c] : (R)fd.trG[ss * 12 + c]) + lift[c];
+      for (int k = 0; k < 3; ++k) {
+        const float4 a = __ldg(t + k);
+        g[4 * k] = (R)a.x, g[4 * k + 1] = (R)a.y, g[4 * k + 2] = (R)a.z, g[4 * k + 3] = (R)a.w;
+      }
+    } else {
+      const double2* t = reinterpret_cast<const double2*>(fd.trG + ss * 12);
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        const double2 a = t[k];
+        g[2 * k] = (R)a.x, g[2 * k + 1] = (R)a.y;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 12; ++c) g[c] += lift[c];
     if (s == 0) {
       viscous_flux<NV>(P_.ph, cv.mu, cv.kappa, U, g, Fo);
     } else {
