@@ -340,7 +340,7 @@ __global__ void __launch_bounds__(kThreads, NV <= 5 ? 6 : 1) k_hex_face(const De
 // Rotation of the thread <-> line assignment of a pencil pass, so that passes issued back to back
 // without a barrier between them start on different threads.
 __device__ __forceinline__ int rotated(int offset) {
-  return (int)((threadIdx.x + blockDim.x - (unsigned)offset % blockDim.x) % blockDim.x);
+  return (int)((threadIdx.x + kThreads - (unsigned)offset % kThreads) % kThreads);
 }
 
 // K consecutive shared-memory values at p (16-byte aligned) into r: 16-byte loads, then an 8-byte
@@ -373,7 +373,7 @@ __device__ __forceinline__ void grad3(const T* V, T* g, T* s, const T* bq, const
   T* BD = BB + C * N * Q * Q;
   T* DB = BD + C * N * Q * Q;
   constexpr int L1 = C * N * N, L2 = C * N * Q, L3 = C * Q * Q, Q3 = Q * Q * Q;
-  const int st = blockDim.x;
+  const int st = kThreads;
   auto i1 = [](int l) { return l * N; };
   auto o1 = [](int l) { return l * Q; };
   pencil<N, Q, false>(V, Bx, bq, L1, 1, 1, i1, o1, rotated(0), st);
@@ -401,7 +401,7 @@ template <int C, int N, int Q, typename T>
 __device__ __forceinline__ void div3(T* G, T* R, T* A, const T* bqT, const T* dqT) {
   constexpr int Q3 = Q * Q * Q, LX = C * Q * Q, LY = C * Q * N, LZ = C * N * N;
   constexpr int AS = C * Q * Q * N, BS = C * Q * N * N;
-  const int st = blockDim.x;
+  const int st = kThreads;
   auto ix = [](int l) { return l * Q; };
   auto ox = [](int l) { return l * N; };
   pencil<Q, N, false>(G + 0 * C * Q3, A + 0 * AS, dqT, LX, 1, 1, ix, ox, rotated(0), st);
@@ -512,8 +512,8 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
     fface[threadIdx.x] = (f << 1) | side;
   }
   __syncthreads();
-  for (int l = threadIdx.x; l < N3; l += blockDim.x) node2lex[tb->lex2node[l]] = l;
-  for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
+  for (int l = threadIdx.x; l < N3; l += kThreads) node2lex[tb->lex2node[l]] = l;
+  for (int idx = threadIdx.x; idx < NV * N3; idx += kThreads) {
     const int v = idx / N3, l = idx % N3;
     U[idx] = (R)(Ug[tb->lex2node[l] * NV + v] - anchor_d[v]);
   }
@@ -525,7 +525,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
   const double* MT = B.minv + (size_t)e * N3 * N3;
   const float* MT32 = (sizeof(R) == sizeof(float) && B.minv32) ? B.minv32 + (size_t)e * N3 * N3 : nullptr;
   if (visc) {
-    for (int l = threadIdx.x; l < N3; l += blockDim.x) {
+    for (int l = threadIdx.x; l < N3; l += kThreads) {
       const int node = tb->lex2node[l];
       double u[NV], vv[4];
 #pragma unroll
@@ -546,7 +546,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
     constexpr int LR = (6 * (int)sizeof(R) + 15) / 16 * 16 / (int)sizeof(R);
     static_assert(2 * LR <= 48, "the dense-lift rows must fit in ball and ax");
     // one face point per thread: its 12 jump components (contiguous) to the canonical point
-    for (int it = threadIdx.x; it < 6 * QF2; it += blockDim.x) {
+    for (int it = threadIdx.x; it < 6 * QF2; it += kThreads) {
       const int lf = it / QF2, q = it % QF2;
       const int cp = codes.perm[fperm[lf] + q];
       const size_t jo = ((size_t)(fface[lf] >> 1) * QF2 + q) * 12;
@@ -572,7 +572,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
     }
     __syncthreads();
     tensor2<CH, QF, QF, N, N>(jc, bs, tmp, tb->bfT, tb->bfT);
-    for (int idx = threadIdx.x; idx < 12 * N3; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < 12 * N3; idx += kThreads) {
       const int c = idx / N3, l = idx % N3;
       const int xyz[3] = {l % N, (l / N) % N, l / N2};
       R acc = R(0);
@@ -590,10 +590,10 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
     if (aff) {
       tensor3<12, N, N, N, N, N, N, false>(ball, Lf, ax, ax + 12 * N3, tb->m1i, tb->m1i, tb->m1i);
       const R cf = (R)B.acoef[e];
-      for (int idx = threadIdx.x; idx < 12 * N3; idx += blockDim.x) Lf[idx] *= cf;
+      for (int idx = threadIdx.x; idx < 12 * N3; idx += kThreads) Lf[idx] *= cf;
     } else {
       auto dense_lift = [&](const auto* M) {
-        for (int idx = threadIdx.x; idx < 2 * N3; idx += blockDim.x) {
+        for (int idx = threadIdx.x; idx < 2 * N3; idx += kThreads) {
           const int i = idx % N3, g = idx / N3, c0 = g * 6;
           R sacc[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
 #pragma unroll 4
@@ -634,7 +634,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
       tensor3<12, N, N, N, Q, Q, Q, false>(Lf, lq, sc, sc + 12 * N * N * Q, tb->bq, tb->bq, tb->bq);
       grad3<4, N, Q>(V, gq, sc, tb->bq, tb->dq);
       // reference -> physical gradient per point, plus the lift at the point
-      for (int q = threadIdx.x; q < Q3; q += blockDim.x) {
+      for (int q = threadIdx.x; q < Q3; q += kThreads) {
         R J[9], gr[12];
 #pragma unroll
         for (int k = 0; k < 9; ++k) J[k] = aff ? Ja[k] : (jinv32 ? (R)jinv32[q * 9 + k] : (R)jinv[q * 9 + k]);
@@ -660,7 +660,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
       normal_flux<NV>(P_.ph, anchor, ey, Fa[1]);
       normal_flux<NV>(P_.ph, anchor, ez, Fa[2]);
     }
-    for (int q = threadIdx.x; q < Q3; q += blockDim.x) {
+    for (int q = threadIdx.x; q < Q3; q += kThreads) {
       R J[9];
 #pragma unroll
       for (int k = 0; k < 9; ++k) J[k] = aff ? Ja[k] : (jinv32 ? (R)jinv32[q * 9 + k] : (R)jinv[q * 9 + k]);
@@ -709,7 +709,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
     R* Rv = Rr + NV * N3;
     R* A = W + L::DIV_AT;                 // uq and gq are dead: the x-pass results go there if they fit
     if (skip_inv) {
-      for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) Ri[idx] = R(0);
+      for (int idx = threadIdx.x; idx < NV * N3; idx += kThreads) Ri[idx] = R(0);
       __syncthreads();
     } else {
       div3<NV, N, Q>(Gi, Ri, A, tb->bqT, tb->dqT);
@@ -718,7 +718,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
       if (visc) {
         div3<NV, N, Q>(Gv, Rv, A, tb->bqT, tb->dqT);
       } else {
-        for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) Rv[idx] = R(0);
+        for (int idx = threadIdx.x; idx < NV * N3; idx += kThreads) Rv[idx] = R(0);
         __syncthreads();
       }
     }
@@ -729,7 +729,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
   R* hs = tmp + 6 * C * QF * N;                 // [6][C][N2]; reused for the M^-1 partial sums
   const size_t base = (size_t)e * N3 * NV;
   // one face point per thread: its NV inviscid and NV viscous flux values (contiguous)
-  for (int it = threadIdx.x; it < 6 * QF2; it += blockDim.x) {
+  for (int it = threadIdx.x; it < 6 * QF2; it += kThreads) {
     const int lf = it / QF2, q = it % QF2;
     const int f = fface[lf] >> 1, side = fface[lf] & 1;
     const double si = side == 0 ? -1.0 : 1.0;
@@ -768,7 +768,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
   constexpr int CS = SPLIT ? 2 * CSH : CSH;
   static_assert(CS * N3 <= 6 * C * (QF2 + QF * N), "the residual rows must end before hs");
   R* RrT = W;
-  for (int idx = threadIdx.x; idx < C * N3; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < C * N3; idx += kThreads) {
     const int c = idx / N3, l = idx % N3;
     const int xyz[3] = {l % N, (l / N) % N, l / N2};
     R acc = Rr[idx];
@@ -799,7 +799,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
   if (aff) {
     tensor3<C, N, N, N, N, N, N, false>(Rr, hs, tmp, hc, tb->m1i, tb->m1i, tb->m1i);
     const R cf = (R)B.acoef[e];
-    for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < NV * N3; idx += kThreads) {
       const int v = idx / N3, l = idx % N3;
       const double ri = (double)(cf * hs[v * N3 + l]);
       const double rv = SPLIT ? (double)(cf * hs[(NV + v) * N3 + l]) : 0.0;
@@ -813,7 +813,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
   constexpr int JH = (N3 + HALVES - 1) / HALVES;
   R* part = hs;                                       // [HALVES][2][NV][N3]
   auto apply = [&](const auto* M) {
-    for (int idx = threadIdx.x; idx < HALVES * NG * N3; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < HALVES * NG * N3; idx += kThreads) {
       const int i = idx % N3, g = (idx / N3) % NG, h = idx / (NG * N3);
       const int v0 = g * VB;
       R ri[VB], rv[VB];
@@ -844,7 +844,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
   };
   if (MT32) apply(MT32); else apply(MT);
   __syncthreads();
-  for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < NV * N3; idx += kThreads) {
     const int v = idx / N3, i = idx % N3;
     R si = part[(0 * NV + v) * N3 + i], sv = part[(1 * NV + v) * N3 + i];
     if (HALVES == 2) {

@@ -105,8 +105,10 @@ __device__ __forceinline__ void pencil(const T* in, T* out, const T* M, int line
 #pragma unroll
   for (int k = 0; k < OUT * IN; ++k) m[k] = M[k];
   if (first < 0) {
+    // every kernel that works a pencil pass with the whole CTA is launched with kThreads threads;
+    // the compile-time stride gives the compiler the trip count
     first = threadIdx.x;
-    step = blockDim.x;
+    step = kThreads;
   }
   for (int line = first; line < lines; line += step) {
     const T* src = in + in_base(line);
@@ -302,13 +304,13 @@ __global__ void __launch_bounds__(kThreads) k_hex_traces(const DevPlan P_, const
     fperm[threadIdx.x] = (side == 0 ? fd.oc[f] : fd.nc[f]) * QF2;
   }
   __syncthreads();
-  for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < NV * N3; idx += kThreads) {
     const int v = idx / N3, l = idx % N3;
     U[idx] = (R)(Ug[tb->lex2node[l] * NV + v] - anchor[v]);
   }
   const bool visc = P_.viscous;
   if (visc) {
-    for (int l = threadIdx.x; l < N3; l += blockDim.x) {
+    for (int l = threadIdx.x; l < N3; l += kThreads) {
       const int node = tb->lex2node[l];
       double u[NV], vv[4];
 #pragma unroll
@@ -320,7 +322,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_traces(const DevPlan P_, const
   }
   __syncthreads();
   // one face node (face, j1, j2) per thread: all its channels
-  for (int it = threadIdx.x; it < 6 * N2; it += blockDim.x) {
+  for (int it = threadIdx.x; it < 6 * N2; it += kThreads) {
     const int lf = it / N2, j = it % N2, j1 = j % N, j2 = j / N;
     int a0, end, a1, a2;
     hex_face_axes(lf, a0, end, a1, a2);
@@ -350,7 +352,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_traces(const DevPlan P_, const
       // start on rotated threads so that the lines spread evenly.
       R* xd = U;                                   // [24][N][QF]
       const R* vsl = slabs + 6 * NV * N2;
-      const int st = blockDim.x;
+      const int st = kThreads;
       auto rot = [st](int off) { return (int)((threadIdx.x + st - off % st) % st); };
       auto i1 = [](int l) { return l * N; };
       auto o1 = [](int l) { return l * QF; };
@@ -372,7 +374,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_traces(const DevPlan P_, const
     tensor2<6 * NV, N, N, QF, QF>(slabs, fo, ftmp, tb->bf, tb->bf);
   }
   // one face point per thread from here on: its values are contiguous in the face buffers
-  for (int it = threadIdx.x; it < 6 * QF2; it += blockDim.x) {
+  for (int it = threadIdx.x; it < 6 * QF2; it += kThreads) {
     const int lf = it / QF2, q = it % QF2;
     const int c = codes.perm[fperm[lf] + q];
     double* dst = fd.trA + ((size_t)fslot[lf] + q) * NV;
@@ -380,12 +382,12 @@ __global__ void __launch_bounds__(kThreads) k_hex_traces(const DevPlan P_, const
     for (int v = 0; v < NV; ++v) dst[v] = anchor[v] + (double)fo[(lf * NV + v) * QF2 + c];
   }
   // the anchor state per face side, for the face kernel's anchor flux
-  for (int idx = threadIdx.x; idx < 6 * NV; idx += blockDim.x)
+  for (int idx = threadIdx.x; idx < 6 * NV; idx += kThreads)
     fd.anc[(size_t)(fslot[idx / NV] / QF2) * NV + idx % NV] = anchor[idx % NV];
   if (visc) {
     const R* fv = fo + 6 * NV * QF2;          // [6][4][QF2]
     const R* gn = fv + 24 * QF2;              // [6][4][QF2]
-    for (int it = threadIdx.x; it < 6 * QF2; it += blockDim.x) {
+    for (int it = threadIdx.x; it < 6 * QF2; it += kThreads) {
       const int lf = it / QF2, q = it % QF2;
       const int c = codes.perm[fperm[lf] + q];
       const size_t pt = (size_t)fslot[lf] + q;
