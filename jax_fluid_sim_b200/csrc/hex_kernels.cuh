@@ -199,7 +199,7 @@ __device__ __forceinline__ void tensor2(const T* in, T* out, T* t, const T* M1, 
 // Gather the N^2 slab of face (a0, end) from lexicographic nodal data X[c][N^3] into slab[c][j2][j1].
 template <int C, int N, typename T>
 __device__ __forceinline__ void face_slab(const T* X, T* slab, int a0, int end, int a1, int a2) {
-  for (int idx = threadIdx.x; idx < C * N * N; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < C * N * N; idx += kThreads) {
     const int j1 = idx % N, j2 = (idx / N) % N, c = idx / (N * N);
     // 1-D node 0 sits at xi=0, node 1 at xi=1
     const int l = end * axis_stride<N>(a0) + j1 * axis_stride<N>(a1) + j2 * axis_stride<N>(a2);
@@ -244,7 +244,7 @@ template <int P>
 __device__ __forceinline__ void load_tables(const HexTables& src, HexTables* dst) {
   const double* s = reinterpret_cast<const double*>(&src);
   double* d = reinterpret_cast<double*>(dst);
-  for (int i = threadIdx.x; i < (int)(sizeof(HexTables) / sizeof(double)); i += blockDim.x) d[i] = s[i];
+  for (int i = threadIdx.x; i < (int)(sizeof(HexTables) / sizeof(double)); i += kThreads) d[i] = s[i];
 }
 
 // float32 copy of the tables for the mixed-precision kernels
@@ -252,15 +252,15 @@ template <int P>
 __device__ __forceinline__ void load_tables(const HexTables& src, HexTablesT<float>* dst) {
   const double* s = reinterpret_cast<const double*>(&src);
   float* d = reinterpret_cast<float*>(dst);
-  for (int i = threadIdx.x; i < kHexTableValues; i += blockDim.x) d[i] = (float)s[i];
-  for (int i = threadIdx.x; i < 64; i += blockDim.x) dst->lex2node[i] = src.lex2node[i];
+  for (int i = threadIdx.x; i < kHexTableValues; i += kThreads) d[i] = (float)s[i];
+  for (int i = threadIdx.x; i < 64; i += kThreads) dst->lex2node[i] = src.lex2node[i];
 }
 
 // Stage M^-1 of one element transposed into shared memory, in lexicographic node order:
 // Mt[lj * MS + li] = M^-1[node(li)][node(lj)].  Global reads are coalesced rows.
 template <int N3, int MS>
 __device__ __forceinline__ void stage_minv(const double* Mg, const int* lex2node, const int* node2lex, double* Mt) {
-  for (int idx = threadIdx.x; idx < N3 * N3; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < N3 * N3; idx += kThreads) {
     const int i = idx / N3, j = idx % N3;          // element node indices
     Mt[node2lex[j] * MS + node2lex[i]] = Mg[idx];
   }
@@ -473,19 +473,19 @@ __global__ void __launch_bounds__(kThreads) k_hex_lift(const DevPlan P_, int b, 
     fjump[threadIdx.x] = f;
   }
   __syncthreads();
-  for (int l = threadIdx.x; l < N3; l += blockDim.x) node2lex[tb->lex2node[l]] = l;
+  for (int l = threadIdx.x; l < N3; l += kThreads) node2lex[tb->lex2node[l]] = l;
   // M^-T of this element in element node order: MT[j][i] = M^-1[i][j] (float32 copy in
   // mixed-precision plans)
   const double* MT = B.minv + (size_t)e * N3 * N3;
   const float* MT32 = (sizeof(R) == sizeof(float) && B.minv32) ? B.minv32 + (size_t)e * N3 * N3 : nullptr;
-  for (int idx = threadIdx.x; idx < 6 * QF2 * 12; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < 6 * QF2 * 12; idx += kThreads) {
     const int lf = idx / (QF2 * 12), q = (idx / 12) % QF2, c = idx % 12;
     jc[(lf * 12 + c) * QF2 + codes.perm[fperm[lf] + q]] = (R)fd.jumpW[((size_t)fjump[lf] * QF2 + q) * 12 + c];
   }
   __syncthreads();
   tensor2<CH, QF, QF, N, N>(jc, bs, tmp, tb->bfT, tb->bfT);
   // b on all nodes: each node gathers the faces holding it, in local-face order (deterministic)
-  for (int idx = threadIdx.x; idx < 12 * N3; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < 12 * N3; idx += kThreads) {
     const int c = idx / N3, l = idx % N3;
     const int xyz[3] = {l % N, (l / N) % N, l / N2};
     R acc = R(0);
@@ -508,10 +508,10 @@ __global__ void __launch_bounds__(kThreads) k_hex_lift(const DevPlan P_, int b, 
     R* at2 = at1 + 12 * N3;
     tensor3<12, N, N, N, N, N, N, false>(ball, ax, at1, at2, tb->m1i, tb->m1i, tb->m1i);
     const R cf = (R)B.acoef[e];
-    for (int idx = threadIdx.x; idx < 12 * N3; idx += blockDim.x) lg[idx] = (double)(cf * ax[idx]);
+    for (int idx = threadIdx.x; idx < 12 * N3; idx += kThreads) lg[idx] = (double)(cf * ax[idx]);
     // M^-1 restricted to each face's slab: coef m1i[end][end] (m1i (x) m1i) over the free axes
     tensor2<CH, N, N, N, N>(bs, rs, tmp, tb->m1i, tb->m1i);
-    for (int idx = threadIdx.x; idx < CH * N2; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < CH * N2; idx += kThreads) {
       int a0, end, a1, a2;
       hex_face_axes(idx / (12 * N2), a0, end, a1, a2);
       rs[idx] *= cf * tb->m1i[end * N + end];
@@ -520,7 +520,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_lift(const DevPlan P_, int b, 
     auto dense_lift = [&](const auto* M) {
       // a thread owns one element node i and half of the 12 components; M rows are read
       // coalesced across consecutive nodes
-      for (int idx = threadIdx.x; idx < 2 * N3; idx += blockDim.x) {
+      for (int idx = threadIdx.x; idx < 2 * N3; idx += kThreads) {
         const int i = idx % N3, c0 = (idx / N3) * 6;
         R sacc[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
 #pragma unroll 4
@@ -535,7 +535,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_lift(const DevPlan P_, int b, 
         for (int k = 0; k < 6; ++k) lg[(c0 + k) * N3 + li] = (double)sacc[k];
       }
       // r_f = M^-1[slab_f, slab_f] b_f for the six faces
-      for (int idx = threadIdx.x; idx < 6 * 2 * N2; idx += blockDim.x) {
+      for (int idx = threadIdx.x; idx < 6 * 2 * N2; idx += kThreads) {
         const int lf = idx / (2 * N2), s_i = idx % N2, c0 = ((idx / N2) % 2) * 6;
         int a0, end, a1, a2;
         hex_face_axes(lf, a0, end, a1, a2);
@@ -558,7 +558,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_lift(const DevPlan P_, int b, 
   __syncthreads();
   // br2 * B_f r_f at every face's points
   tensor2<CH, N, N, QF, QF>(rs, lq, tmp, tb->bf, tb->bf);
-  for (int idx = threadIdx.x; idx < 6 * QF2 * 12; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < 6 * QF2 * 12; idx += kThreads) {
     const int lf = idx / (QF2 * 12), q = (idx / 12) % QF2, c = idx % 12;
     fd.liftF[((size_t)fslot[lf] + q) * 12 + c] =
         P_.ph.br2 * (double)lq[(lf * 12 + c) * QF2 + codes.perm[fperm[lf] + q]];
@@ -596,13 +596,13 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
   }
   __syncthreads();
   // differences to the anchor are formed in float64, then rounded to R
-  for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < NV * N3; idx += kThreads) {
     const int v = idx / N3, l = idx % N3;
     U[idx] = (R)(Ug[tb->lex2node[l] * NV + v] - anchor_d[v]);
   }
   const bool visc = P_.viscous;
   if (visc) {
-    for (int l = threadIdx.x; l < N3; l += blockDim.x) {
+    for (int l = threadIdx.x; l < N3; l += kThreads) {
       const int node = tb->lex2node[l];
       double u[NV], vv[4];
 #pragma unroll
@@ -612,7 +612,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
       for (int m = 0; m < 4; ++m) V[m * N3 + l] = (R)vv[m];
     }
     const double* lg = lift_in + (size_t)e * 12 * N3;
-    for (int idx = threadIdx.x; idx < 12 * N3; idx += blockDim.x) Lf[idx] = (R)lg[idx];
+    for (int idx = threadIdx.x; idx < 12 * N3; idx += kThreads) Lf[idx] = (R)lg[idx];
   }
   __syncthreads();
   R* uq = W;                           // [NV][Q3]   U - anchor at volume points
@@ -636,7 +636,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
     tensor3<4, N, N, N, Q, Q, Q, false>(V, gq + 1 * 4 * Q3, t1, t2, tb->bq, tb->dq, tb->bq);
     tensor3<4, N, N, N, Q, Q, Q, false>(V, gq + 2 * 4 * Q3, t1, t2, tb->bq, tb->bq, tb->dq);
     // reference -> physical gradient, in place per point: g[m*3+d] = sum_r dv_m/dxi_r J^-1[r][d]
-    for (int q = threadIdx.x; q < Q3; q += blockDim.x) {
+    for (int q = threadIdx.x; q < Q3; q += kThreads) {
       R J[9], gr[12];
 #pragma unroll
       for (int k = 0; k < 9; ++k) J[k] = aff ? Ja[k] : (jinv32 ? (R)jinv32[q * 9 + k] : (R)jinv[q * 9 + k]);
@@ -661,7 +661,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
     normal_flux<NV>(P_.ph, anchor, ey, Fa[1]);
     normal_flux<NV>(P_.ph, anchor, ez, Fa[2]);
   }
-  for (int q = threadIdx.x; q < Q3; q += blockDim.x) {
+  for (int q = threadIdx.x; q < Q3; q += kThreads) {
     R J[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) J[k] = aff ? Ja[k] : (jinv32 ? (R)jinv32[q * 9 + k] : (R)jinv[q * 9 + k]);
@@ -716,7 +716,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
   // residuals stay in lexicographic [NV][N3] order for k_hex_finalize
   double* Rig = B.Rinv + (size_t)e * N3 * NV;
   double* Rvg = B.Rvis + (size_t)e * N3 * NV;
-  for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < NV * N3; idx += kThreads) {
     Rig[idx] = (double)Ri[idx];
     if (SPLIT && visc) Rvg[idx] = (double)Rv[idx];
   }
@@ -755,11 +755,11 @@ __global__ void __launch_bounds__(kThreads) k_hex_finalize(const DevPlan P_, con
     fface[threadIdx.x] = (f << 1) | side;
   }
   __syncthreads();
-  for (int l = threadIdx.x; l < N3; l += blockDim.x) node2lex[tb->lex2node[l]] = l;
+  for (int l = threadIdx.x; l < N3; l += kThreads) node2lex[tb->lex2node[l]] = l;
   const size_t base = (size_t)e * N3 * NV;
   const bool visc = P_.viscous;
   // the six faces' fluxes, signed for this side, at the canonical face points
-  for (int idx = threadIdx.x; idx < 6 * QF2 * NV; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < 6 * QF2 * NV; idx += kThreads) {
     const int lf = idx / (QF2 * NV), q = (idx / NV) % QF2, v = idx % NV;
     const int f = fface[lf] >> 1, side = fface[lf] & 1;
     const double si = side == 0 ? -1.0 : 1.0;
@@ -776,7 +776,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_finalize(const DevPlan P_, con
   __syncthreads();
   tensor2<6 * C, QF, QF, N, N>(hc, hs, tmp, tb->bfT, tb->bfT);
   // residual plus the face terms of every face holding the node, faces in local order
-  for (int idx = threadIdx.x; idx < C * N3; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < C * N3; idx += kThreads) {
     const int c = idx / N3, l = idx % N3;
     const int xyz[3] = {l % N, (l / N) % N, l / N2};
     R acc = (R)(c < NV ? B.Rinv[base + c * N3 + l] : ((SPLIT && visc) ? B.Rvis[base + (c - NV) * N3 + l] : 0.0));
@@ -806,7 +806,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_finalize(const DevPlan P_, con
     // affine: M^-1 = coef (m1i (x) m1i (x) m1i), three 1-D passes over the lexicographic residual
     tensor3<C, N, N, N, N, N, N, false>(Rr, hs, tmp, hc, tb->m1i, tb->m1i, tb->m1i);
     const R cf = (R)B.acoef[e];
-    for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < NV * N3; idx += kThreads) {
       const int v = idx / N3, l = idx % N3;
       const double ri = (double)(cf * hs[v * N3 + l]);
       const double rv = SPLIT ? (double)(cf * hs[(NV + v) * N3 + l]) : 0.0;
@@ -825,7 +825,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_finalize(const DevPlan P_, con
   const float* MT32 = (sizeof(R) == sizeof(float) && B.minv32) ? B.minv32 + (size_t)e * N3 * N3 : nullptr;
   R* part = hs;                                       // [HALVES][2][NV][N3]
   auto apply = [&](const auto* M) {
-    for (int idx = threadIdx.x; idx < HALVES * NG * N3; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < HALVES * NG * N3; idx += kThreads) {
       const int i = idx % N3, g = (idx / N3) % NG, h = idx / (NG * N3);
       const int v0 = g * VB;
       R ri[VB], rv[VB];
@@ -854,7 +854,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_finalize(const DevPlan P_, con
   };
   if (MT32) apply(MT32); else apply(MT);
   __syncthreads();
-  for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < NV * N3; idx += kThreads) {
     const int v = idx / N3, i = idx % N3;
     R si = part[(0 * NV + v) * N3 + i], sv = part[(1 * NV + v) * N3 + i];
     if (HALVES == 2) {
@@ -881,7 +881,7 @@ __device__ void hex_cell_mean(const double* vq, const double* __restrict__ wdet,
   double s[NV + 1];
 #pragma unroll
   for (int v = 0; v <= NV; ++v) s[v] = 0.0;
-  for (int q = threadIdx.x; q < Q3; q += blockDim.x) {
+  for (int q = threadIdx.x; q < Q3; q += kThreads) {
     const double w = wdet[q];
 #pragma unroll
     for (int v = 0; v < NV; ++v) s[v] += vq[v * Q3 + q] * w;
@@ -896,7 +896,7 @@ __device__ void hex_cell_mean(const double* vq, const double* __restrict__ wdet,
   __syncthreads();
   if (threadIdx.x < NV) {
     double a = 0.0, w = 0.0;
-    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+    for (int k = 0; k < (int)(kThreads >> 5); ++k) {
       a += part[k][threadIdx.x];
       w += part[k][NV];
     }
@@ -911,7 +911,7 @@ __device__ void hex_samples(const HexTables* tb, const double* Ug, double* U, do
   using D = HexDims<P>;
   constexpr int N = D::N, Q = D::Q, QF = D::QF, N2 = D::N2, N3 = D::N3, Q3 = D::Q3, QF2 = D::QF2;
   constexpr int NS = N3 + Q3 + 6 * QF2;
-  for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < NV * N3; idx += kThreads) {
     const int v = idx / N3, l = idx % N3;
     const double x = Ug[tb->lex2node[l] * NV + v];
     U[idx] = x;
@@ -919,14 +919,14 @@ __device__ void hex_samples(const HexTables* tb, const double* Ug, double* U, do
   }
   __syncthreads();
   tensor3<NV, N, N, N, Q, Q, Q, false>(U, vq, t1, t2, tb->bq, tb->bq, tb->bq);
-  for (int idx = threadIdx.x; idx < NV * Q3; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < NV * Q3; idx += kThreads) {
     const int v = idx / Q3, q = idx % Q3;
     Smp[v * NS + N3 + q] = vq[idx];
   }
   double* slabs = fs;                    // [6][NV][N2]
   double* ftmp = slabs + 6 * NV * N2;    // [6][NV][N][QF]
   double* fo = ftmp + 6 * NV * N * QF;   // [6][NV][QF2]
-  for (int idx = threadIdx.x; idx < 6 * NV * N2; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < 6 * NV * N2; idx += kThreads) {
     const int j1 = idx % N, j2 = (idx / N) % N, c = idx / N2, lf = c / NV, v = c % NV;
     int a0, end, a1, a2;
     hex_face_axes(lf, a0, end, a1, a2);
@@ -934,7 +934,7 @@ __device__ void hex_samples(const HexTables* tb, const double* Ug, double* U, do
   }
   __syncthreads();
   tensor2<6 * NV, N, N, QF, QF>(slabs, fo, ftmp, tb->bf, tb->bf);
-  for (int idx = threadIdx.x; idx < 6 * NV * QF2; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < 6 * NV * QF2; idx += kThreads) {
     const int q = idx % QF2, c = idx / QF2, lf = c / NV, v = c % NV;
     Smp[v * NS + N3 + Q3 + lf * QF2 + q] = fo[idx];
   }
@@ -987,7 +987,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_positivity(const DevPlan P_, c
     const double pfloor = fmax(Lc.pressure_floor, Lc.relative_floor * Wm[4]);
     double rmin = INFINITY;
     bool nan_seen = false;
-    for (int r = threadIdx.x; r < NS; r += blockDim.x) {
+    for (int r = threadIdx.x; r < NS; r += kThreads) {
       const double d = Smp[r];
       nan_seen |= isnan(d);
       rmin = fmin(rmin, d);
@@ -1007,7 +1007,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_positivity(const DevPlan P_, c
     const double upper = sh_upper;
     auto pressure_ok = [&](double theta) -> bool {
       bool ok = true;
-      for (int r = threadIdx.x; r < NS; r += blockDim.x) {
+      for (int r = threadIdx.x; r < NS; r += kThreads) {
         double s[NV];
   #pragma unroll
         for (int v = 0; v < NV; ++v) s[v] = mean[v] + theta * (Smp[v * NS + r] - mean[v]);
@@ -1028,7 +1028,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_positivity(const DevPlan P_, c
       }
       theta = lo;
     }
-    for (int idx = threadIdx.x; idx < NV * N3; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < NV * N3; idx += kThreads) {
       const int v = idx / N3, l = idx % N3;
       Ug[tb->lex2node[l] * NV + v] = mean[v] + theta * (U[idx] - mean[v]);
     }
@@ -1070,7 +1070,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_troubled(const DevPlan P_, con
     const int e = list[item];
     const double* Ug = S.b[b] + (size_t)e * N3 * NV;
     hex_samples<P, NV>(tb, Ug, U, Smp, t1, t2, vq, fs);
-    for (int l = threadIdx.x; l < N3; l += blockDim.x) {
+    for (int l = threadIdx.x; l < N3; l += kThreads) {
       double u[NV], W[NV];
   #pragma unroll
       for (int v = 0; v < NV; ++v) u[v] = U[v * N3 + l];
@@ -1086,7 +1086,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_troubled(const DevPlan P_, con
     hex_cell_mean<NV>(vq, B.wdet + (size_t)e * Q3, Q3, mean, part);
     double hi0 = 0.0, hi1 = 0.0, sc0 = 0.0, sc1 = 0.0;
     if (P >= 2) {
-      for (int i = threadIdx.x; i < N3; i += blockDim.x) {
+      for (int i = threadIdx.x; i < N3; i += kThreads) {
         const double m0 = Mon[i], m1 = Mon[N3 + i];
         const double d0 = m0 - Low[i], d1 = m1 - Low[N3 + i];
         hi0 += d0 * d0;
@@ -1109,7 +1109,7 @@ __global__ void __launch_bounds__(kThreads) k_hex_troubled(const DevPlan P_, con
     }
     __syncthreads();
     bool bad = false;
-    for (int r = threadIdx.x; r <= NS; r += blockDim.x) {
+    for (int r = threadIdx.x; r <= NS; r += kThreads) {
       double s[NV], W[NV];
   #pragma unroll
       for (int v = 0; v < NV; ++v) s[v] = r < NS ? Smp[v * NS + r] : mean[v];

@@ -87,10 +87,10 @@ __global__ void __launch_bounds__(kThreads) k_mood_fv(const DevPlan P, const Moo
   double* g = ub + Sn * NV;             // [S][3][NV]
   double* fi = g + Sn * 3 * NV;         // [NI][NV]
   const double* Ug = S.b[b] + (size_t)e * Np * NV;
-  for (int i = threadIdx.x; i < Np * NV; i += blockDim.x) U[i] = Ug[i];
+  for (int i = threadIdx.x; i < Np * NV; i += kThreads) U[i] = Ug[i];
   __syncthreads();
   const double* Pe = C.P + (size_t)e * Sn * Np;
-  for (int idx = threadIdx.x; idx < Sn * NV; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < Sn * NV; idx += kThreads) {
     const int s = idx / NV, v = idx % NV;
     double acc = 0.0;
     for (int i = 0; i < Np; ++i) acc += Pe[s * Np + i] * U[i * NV + v];
@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(kThreads) k_mood_fv(const DevPlan P, const Moo
   const double* cen = C.cen + (size_t)e * Sn * 3;
   if (M.recon != 0) {
     // Green-Gauss gradient per subcell: sum over its internal subfaces of 0.5 n A (U_nbr - U_own) / V
-    for (int idx = threadIdx.x; idx < Sn * 3 * NV; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < Sn * 3 * NV; idx += kThreads) {
       const int s = idx / (3 * NV), d = (idx / NV) % 3, v = idx % NV;
       double acc = 0.0;
       for (int k = C.csr_ptr[s]; k < C.csr_ptr[s + 1]; ++k) {
@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(kThreads) k_mood_fv(const DevPlan P, const Moo
     }
     __syncthreads();
   }
-  for (int f = threadIdx.x; f < NI; f += blockDim.x) {
+  for (int f = threadIdx.x; f < NI; f += kThreads) {
     const int o = C.iown[f], n = C.inbr[f];
     double UL[NV], UR[NV], Fl[NV];
     if (M.recon == 0) {
@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(kThreads) k_mood_fv(const DevPlan P, const Moo
     for (int v = 0; v < NV; ++v) fi[f * NV + v] = Fl[v] * ar[f];
   }
   __syncthreads();
-  for (int idx = threadIdx.x; idx < Sn * NV; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < Sn * NV; idx += kThreads) {
     const int s = idx / NV, v = idx % NV;
     double acc = 0.0;
     for (int k = C.csr_ptr[s]; k < C.csr_ptr[s + 1]; ++k) {
@@ -292,7 +292,7 @@ __global__ void __launch_bounds__(kThreads) k_mood_faces(const DevPlan P, const 
   const FaceDev& fd = P.face[ft];
   const SubcellFaceDev& sf = M.face[ft];
   const int lane = threadIdx.x & 31;
-  const long f0 = ((long)blockIdx.x * blockDim.x + threadIdx.x) & ~31L;
+  const long f0 = ((long)blockIdx.x * kThreads + threadIdx.x) & ~31L;
   if (f0 >= fd.F) return;                       // whole warps leave together
   const long f = f0 + lane;
   bool active = false;
@@ -355,21 +355,21 @@ __global__ void __launch_bounds__(kThreads) k_mood_update(const DevPlan P, const
       corr[threadIdx.x] = c;
     }
     __syncthreads();
-    for (int idx = threadIdx.x; idx < Np * NV; idx += blockDim.x)
+    for (int idx = threadIdx.x; idx < Np * NV; idx += kThreads)
       out[base + idx] = any ? cand[base + idx] + corr[idx % NV] : cand[base + idx];
     return;
   }
   double* res = smem;                    // [S][NV]
   double* fv = res + Sn * NV;            // [S][NV]
   double* raw = fv + Sn * NV;            // [Np][NV]
-  for (int idx = threadIdx.x; idx < Sn * NV; idx += blockDim.x) res[idx] = C.rsub[(size_t)e * Sn * NV + idx];
+  for (int idx = threadIdx.x; idx < Sn * NV; idx += kThreads) res[idx] = C.rsub[(size_t)e * Sn * NV + idx];
   for (int lf = 0; lf < B.nlf; ++lf) {
     int ft, f, side;
     decode_face(B.elem_face[e * B.nlf + lf], ft, f, side);
     const SubcellFaceDev& sf = M.face[ft];
     const int32_t* sub = side == 0 ? sf.osub : sf.nsub;
     __syncthreads();
-    for (int idx = threadIdx.x; idx < kSub * NV; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < kSub * NV; idx += kThreads) {
       const int j = idx / NV, v = idx % NV;
       const int sc = C.scatter[sub[f * kSub + j]];
       if (sc < 0) continue;
@@ -379,7 +379,7 @@ __global__ void __launch_bounds__(kThreads) k_mood_update(const DevPlan P, const
   }
   __syncthreads();
   const double* Pe = C.P + (size_t)e * Sn * Np;
-  for (int idx = threadIdx.x; idx < Sn * NV; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < Sn * NV; idx += kThreads) {
     const int s = idx / NV, v = idx % NV;
     double x = C.ubar[(size_t)e * Sn * NV + idx] + dt * res[idx] / vol[s];
     if (visc) {
@@ -391,7 +391,7 @@ __global__ void __launch_bounds__(kThreads) k_mood_update(const DevPlan P, const
   }
   __syncthreads();
   const double* Re = C.R + (size_t)e * Np * Sn;
-  for (int idx = threadIdx.x; idx < Np * NV; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < Np * NV; idx += kThreads) {
     const int i = idx / NV, v = idx % NV;
     double acc = 0.0;
     for (int s = 0; s < Sn; ++s) acc += Re[i * Sn + s] * fv[s * NV + v];
