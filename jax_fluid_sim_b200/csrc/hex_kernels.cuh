@@ -221,7 +221,10 @@ struct HexSmem {
   static constexpr int MS = N3 + 1;                 // padded row stride of the staged M^-1 (transposed)
   // traces: U, v, then the six faces' slabs, contraction scratch, face values and tangential derivatives
   static constexpr int TR_U = T, TR_V = TR_U + NV * N3, TR_W = TR_V + 4 * N3;
-  static constexpr int TRACES = TR_W + 6 * (NV + 8) * (N2 + N * QF + QF2) + 2 * 24 * QF2;
+  // The face values alias the slabs when the three face contractions run as one merged pass (every read of
+  // the slabs comes before the barrier after which the face values are written); N2 == QF2 at P1-P3.
+  static constexpr bool TR_ALIAS = (NV + 4) * N3 >= 24 * N * QF && N2 == QF2;
+  static constexpr int TRACES = TR_W + 6 * (NV + 8) * (N2 + N * QF + (TR_ALIAS ? 0 : QF2)) + 2 * 24 * QF2;
   // lift: staged M^-T, b per face on its slab, b on all nodes, scratch
   static constexpr int LI_BS = T, LI_B = LI_BS + 6 * 12 * N2, LI_W = LI_B + 12 * N3;
   static constexpr int LI_X = LI_W + 72 * QF2 + 72 * QF * N + 72 * N2 + 72 * QF2;   // affine scratch
@@ -286,8 +289,9 @@ __global__ void __launch_bounds__(kThreads) k_hex_traces(const DevPlan P_, const
   constexpr int CH = 6 * (NV + 8);
   R* slabs = smem + L::TR_W;
   R* ftmp = slabs + CH * N2;         // tensor2 scratch [CH][N][QF]
-  R* fo = ftmp + CH * N * QF;        // [CH][QF2] values at the canonical face points
-  R* g1 = fo + CH * QF2;             // [6*4][QF2] derivative of v along a1
+  // [CH][QF2] values at the canonical face points (over the slabs when the layout aliases them)
+  R* fo = L::TR_ALIAS ? slabs : ftmp + CH * N * QF;
+  R* g1 = L::TR_ALIAS ? ftmp + CH * N * QF : fo + CH * QF2;   // [6*4][QF2] derivative of v along a1
   R* g2 = g1 + 24 * QF2;             // [6*4][QF2] derivative of v along a2
   __shared__ int fslot[6], fperm[6];
   const BlockDev& B = P_.blk[b];
