@@ -457,7 +457,8 @@ struct HexElemSmem {
   // the phase scratch starts on a 16-byte boundary (N3 = 27 leaves RR + C N3 odd)
   static constexpr int W = (RR + C * N3 + 3) / 4 * 4;
   // phase scratch (aliased)
-  static constexpr int LIFT = 72 * QF2 + 72 * QF * N + 72 * N2 + 12 * N3 + 3 * 12 * N3;
+  // jc, tmp, bs, ball, then the affine elements' tensor3 scratch (two [12][N3] passes)
+  static constexpr int LIFT = 72 * QF2 + 72 * QF * N + 72 * N2 + 12 * N3 + 2 * 12 * N3;
   // phase C: uq [NV][Q3], gq [12][Q3], then the lift at the points lq [12][Q3] (later Gi, Gv [3][NV][Q3]
   // each), then contraction scratch
   static constexpr int VOL_G = cmax(12 * Q3, (SPLIT ? 6 : 3) * NV * Q3);
@@ -540,11 +541,11 @@ __global__ void __launch_bounds__(kThreads, sizeof(R) == sizeof(float) ? 6 : 1) 
     R* tmp = jc + CH * QF2;           // [72][QF][N]
     R* bs = tmp + CH * QF * N;        // [6][12][N2]
     R* ball = bs + CH * N2;           // [12][N3]
-    R* ax = ball + 12 * N3;           // affine scratch [3][12][N3]
+    R* ax = ball + 12 * N3;           // affine scratch [2][12][N3]
     // dense-lift row groups of the non-affine elements: 6 channels padded to 16 bytes; the rows
     // (2 LR N3 values) reach into ax, which only affine elements use
     constexpr int LR = (6 * (int)sizeof(R) + 15) / 16 * 16 / (int)sizeof(R);
-    static_assert(2 * LR <= 48, "the dense-lift rows must fit in ball and ax");
+    static_assert(2 * LR <= 36, "the dense-lift rows must fit in ball and ax");
     // one face point per thread: its 12 jump components (contiguous) to the canonical point
     for (int it = threadIdx.x; it < 6 * QF2; it += kThreads) {
       const int lf = it / QF2, q = it % QF2;
